@@ -1,0 +1,205 @@
+"""Seeded synthetic systems for the TholeDipoleForce hot path.
+
+A :class:`TholeSystem` holds exactly the per-particle parameters and settings
+that the reference kernel wrapper copies out of a ``TholeDipoleForce``
+(platforms/reference/src/ReferenceTholeDipoleKernels.cpp:83-158): charges,
+molecular dipoles, polarizabilities, Thole factors, axis types and axis atoms,
+the Covalent12/Covalent13 lists that set the M and I scales, the nonbonded
+method, box, polarization type and solver knobs.
+
+The generators build the rigid 3-site water systems used for measurement:
+O-H 0.09572 nm, H-O-H 104.52 deg; q(O) = -0.834 e, q(H) = +0.417 e;
+alpha(O) = 1.44e-3 nm^3, alpha(H) = 0.496e-3 nm^3; Thole a = 0.39 on every
+atom; a permanent dipole of 0.005 e*nm along the local z axis of O in a
+Z-then-X frame (Z -> H1, X -> H2).  Within a molecule the permanent field is
+excluded (each atom lists its two partners in Covalent12, list positions 0 and
+1, M scale 0) and induced-induced coupling is kept and Thole-damped
+(Covalent13 empty, I scale 1).  Molecule centres sit on a simple-cubic lattice
+with +-0.02 nm uniform jitter and orientations uniform on SO(3) (normalised
+Gaussian quaternions).  No public dataset exists for this path; these seeded
+inputs stand in for it.
+"""
+from __future__ import annotations
+
+import dataclasses
+import math
+from typing import List, Optional, Sequence
+
+import numpy as np
+
+NO_CUTOFF, PME = 0, 1
+DIRECT, MUTUAL, EXTRAPOLATED = 0, 1, 2
+ZTHENX, BISECTOR, ZBISECT, THREEFOLD, ZONLY, NOAXISTYPE = 0, 1, 2, 3, 4, 5
+
+OH_BOND = 0.09572
+HOH_ANGLE = math.radians(104.52)
+Q_O, Q_H = -0.834, 0.417
+ALPHA_O, ALPHA_H = 1.44e-3, 0.496e-3
+THOLE = 0.39
+DIPOLE_O = 0.005
+MASS_O, MASS_H = 15.999, 1.008
+OPT4 = (-0.154, 0.017, 0.658, 0.474)
+
+
+def _csr(lists: Sequence[Sequence[int]], n: int):
+    off = np.zeros(n + 1, dtype=np.int32)
+    for i in range(n):
+        off[i + 1] = off[i] + len(lists[i])
+    flat = np.array([a for l in lists for a in l], dtype=np.int32)
+    return off, flat
+
+
+@dataclasses.dataclass
+class TholeSystem:
+    positions: np.ndarray          # (n, 3) float64, nm
+    charges: np.ndarray            # (n,)
+    dipoles: np.ndarray            # (n, 3) molecular frame, e*nm
+    polarizabilities: np.ndarray   # (n,)
+    tholes: np.ndarray             # (n,)
+    axis: np.ndarray               # (n, 4) int32: type, Z, X, Y
+    cov12: List[List[int]]
+    cov13: List[List[int]]
+    method: int = NO_CUTOFF
+    box: np.ndarray = dataclasses.field(default_factory=lambda: np.zeros(3))
+    cutoff: float = 1.0
+    ewald_tolerance: float = 1e-4
+    polarization: int = MUTUAL
+    target_eps: float = 1e-5
+    max_iter: int = 60
+    extrap: Optional[Sequence[float]] = None
+    masses: Optional[np.ndarray] = None
+
+    @property
+    def n(self) -> int:
+        return int(self.positions.shape[0])
+
+    def cov12_csr(self):
+        return _csr(self.cov12, self.n)
+
+    def cov13_csr(self):
+        return _csr(self.cov13, self.n)
+
+    def copy(self, **changes) -> "TholeSystem":
+        fields = {f.name: getattr(self, f.name) for f in dataclasses.fields(self)}
+        for k, v in list(fields.items()):
+            if isinstance(v, np.ndarray):
+                fields[k] = v.copy()
+            elif isinstance(v, list):
+                fields[k] = [list(x) for x in v]
+        fields.update(changes)
+        return TholeSystem(**fields)
+
+
+def random_rotations(rng: np.random.Generator, m: int) -> np.ndarray:
+    """m rotation matrices uniform on SO(3) from normalised Gaussian quaternions."""
+    q = rng.standard_normal((m, 4))
+    q /= np.linalg.norm(q, axis=1, keepdims=True)
+    w, x, y, z = q[:, 0], q[:, 1], q[:, 2], q[:, 3]
+    r = np.empty((m, 3, 3))
+    r[:, 0, 0] = 1 - 2 * (y * y + z * z)
+    r[:, 0, 1] = 2 * (x * y - z * w)
+    r[:, 0, 2] = 2 * (x * z + y * w)
+    r[:, 1, 0] = 2 * (x * y + z * w)
+    r[:, 1, 1] = 1 - 2 * (x * x + z * z)
+    r[:, 1, 2] = 2 * (y * z - x * w)
+    r[:, 2, 0] = 2 * (x * z - y * w)
+    r[:, 2, 1] = 2 * (y * z + x * w)
+    r[:, 2, 2] = 1 - 2 * (x * x + y * y)
+    return r
+
+
+def water_body_frame() -> np.ndarray:
+    """(3, 3) body-frame coordinates of O, H1, H2 with the centre of mass at 0."""
+    half = 0.5 * HOH_ANGLE
+    o = np.zeros(3)
+    h1 = np.array([OH_BOND * math.sin(half), 0.0, OH_BOND * math.cos(half)])
+    h2 = np.array([-OH_BOND * math.sin(half), 0.0, OH_BOND * math.cos(half)])
+    xyz = np.stack([o, h1, h2])
+    m = np.array([MASS_O, MASS_H, MASS_H])
+    return xyz - (m[:, None] * xyz).sum(0) / m.sum()
+
+
+def _water_parameters(nw: int):
+    n = 3 * nw
+    charges = np.tile([Q_O, Q_H, Q_H], nw).astype(np.float64)
+    pol = np.tile([ALPHA_O, ALPHA_H, ALPHA_H], nw).astype(np.float64)
+    tholes = np.full(n, THOLE)
+    dip = np.zeros((n, 3))
+    dip[0::3, 2] = DIPOLE_O
+    axis = np.full((n, 4), -1, dtype=np.int32)
+    axis[:, 0] = NOAXISTYPE
+    o = np.arange(nw) * 3
+    axis[o, 0] = ZTHENX
+    axis[o, 1] = o + 1
+    axis[o, 2] = o + 2
+    cov12: List[List[int]] = []
+    for w in range(nw):
+        a = 3 * w
+        cov12 += [[a + 1, a + 2], [a, a + 2], [a, a + 1]]
+    cov13: List[List[int]] = [[] for _ in range(n)]
+    masses = np.tile([MASS_O, MASS_H, MASS_H], nw).astype(np.float64)
+    return charges, dip, pol, tholes, axis, cov12, cov13, masses
+
+
+def place_waters(centres: np.ndarray, rng: np.random.Generator) -> np.ndarray:
+    body = water_body_frame()
+    rot = random_rotations(rng, centres.shape[0])
+    xyz = centres[:, None, :] + np.einsum("mij,aj->mai", rot, body)
+    return xyz.reshape(-1, 3)
+
+
+def water_box(n_side: int, box_nm: float, seed: int = 0, cutoff: float = 0.9,
+              jitter: float = 0.02, polarization: int = MUTUAL, target_eps: float = 1e-6,
+              max_iter: int = 500, method: int = PME) -> TholeSystem:
+    """n_side^3 waters on a lattice in a cubic periodic box of edge box_nm."""
+    rng = np.random.default_rng(seed)
+    nw = n_side ** 3
+    a = box_nm / n_side
+    g = (np.arange(n_side) + 0.5) * a
+    cx, cy, cz = np.meshgrid(g, g, g, indexing="ij")
+    centres = np.stack([cx.ravel(), cy.ravel(), cz.ravel()], axis=1)
+    centres = centres + rng.uniform(-jitter, jitter, size=centres.shape)
+    pos = place_waters(centres, rng)
+    charges, dip, pol, th, axis, cov12, cov13, masses = _water_parameters(nw)
+    return TholeSystem(positions=pos, charges=charges, dipoles=dip, polarizabilities=pol, tholes=th,
+                       axis=axis, cov12=cov12, cov13=cov13, method=method,
+                       box=np.array([box_nm] * 3, dtype=np.float64), cutoff=cutoff,
+                       polarization=polarization, target_eps=target_eps, max_iter=max_iter,
+                       masses=masses)
+
+
+def water_cluster(nw: int, rng: np.random.Generator, spacing: float = 0.31, jitter: float = 0.02,
+                  polarization: int = MUTUAL, target_eps: float = 1e-6, max_iter: int = 500) -> TholeSystem:
+    """nw waters on the first nw sites of the smallest simple-cubic block, NoCutoff."""
+    k = 1
+    while k ** 3 < nw:
+        k += 1
+    g = np.arange(k) * spacing
+    cx, cy, cz = np.meshgrid(g, g, g, indexing="ij")
+    sites = np.stack([cx.ravel(), cy.ravel(), cz.ravel()], axis=1)[:nw]
+    sites = sites + rng.uniform(-jitter, jitter, size=sites.shape)
+    pos = place_waters(sites, rng)
+    charges, dip, pol, th, axis, cov12, cov13, masses = _water_parameters(nw)
+    return TholeSystem(positions=pos, charges=charges, dipoles=dip, polarizabilities=pol, tholes=th,
+                       axis=axis, cov12=cov12, cov13=cov13, method=NO_CUTOFF,
+                       polarization=polarization, target_eps=target_eps, max_iter=max_iter,
+                       masses=masses)
+
+
+def cluster_batch(n_clusters: int = 1024, lo: int = 4, hi: int = 64, seed: int = 3, **kw) -> List[TholeSystem]:
+    rng = np.random.default_rng(seed)
+    sizes = rng.integers(lo, hi + 1, size=n_clusters)
+    return [water_cluster(int(s), rng, **kw) for s in sizes]
+
+
+# The measured configurations (216, 4096 and 32768 waters; cutoffs 0.8 / 0.9 nm).
+def config_small(seed: int = 0, **kw) -> TholeSystem:
+    return water_box(6, 1.8643, seed=seed, cutoff=0.8, **kw)
+
+
+def config_medium(seed: int = 1, **kw) -> TholeSystem:
+    return water_box(16, 4.968, seed=seed, cutoff=0.9, **kw)
+
+
+def config_large(seed: int = 2, **kw) -> TholeSystem:
+    return water_box(32, 9.936, seed=seed, cutoff=0.9, **kw)
