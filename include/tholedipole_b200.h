@@ -1,0 +1,219 @@
+/*
+ * tholedipole_b200.h -- C ABI of the B200 (sm_100a) TholeDipoleForce kernels.
+ *
+ * This is the boundary a CUDA-platform kernel of the TholeDipoleForce plugin
+ * (aehogan/tholedipoleplugin) binds: every entry point replaces one method of
+ * the abstract kernel interface CalcTholeDipoleForceKernel
+ * (openmmapi/include/TholeDipoleKernels.h:46-122) or one stage the reference
+ * platform runs behind it (platforms/reference/src/ReferenceTholeDipoleKernels.cpp).
+ * Plain pointers and sizes only; no C++ or torch types cross it.
+ *
+ * Conventions
+ *  - Every function returns TDP_OK (0) or a negative TDP_ERR_* code; the
+ *    message of the last failure on a handle is tdp_last_error(h) (or
+ *    tdp_last_error(NULL) for failures before a handle exists).  Nothing
+ *    throws across the ABI.
+ *  - A handle is single-stream and not thread-safe: the OpenMM caller
+ *    (TholeDipoleForceImpl, openmmapi/src/TholeDipoleForceImpl.cpp:110-195)
+ *    uses one kernel object from the context's thread.
+ *  - Units are the reference's: nm, e, e*nm, nm^3; energies in e^2/nm and
+ *    forces in e^2/nm^2 (Coulomb prefactor 1, ReferenceTholeDipoleForce.cpp:20-21).
+ *  - Arrays of vectors are AoS, n*3 doubles unless stated otherwise.
+ *  - All device work runs on the handle's stream (tdp_set_stream).
+ */
+#ifndef THOLEDIPOLE_B200_H_
+#define THOLEDIPOLE_B200_H_
+
+#include <stddef.h>
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+#define TDP_ABI_VERSION 1
+
+/* Status codes. */
+#define TDP_OK 0
+#define TDP_ERR_INVALID_ARGUMENT (-1)
+#define TDP_ERR_CUDA (-2)
+#define TDP_ERR_NOT_PME (-3)
+#define TDP_ERR_SIZE_MISMATCH (-4)
+#define TDP_ERR_BOX_TOO_SMALL (-5)
+#define TDP_ERR_NOT_CONVERGED (-6)   /* only returned when TDP_COMPUTE_REQUIRE_CONVERGENCE is set */
+#define TDP_ERR_NON_FINITE (-7)
+#define TDP_ERR_UNSUPPORTED (-8)
+
+/* Enumerations: same values as TholeDipoleForce (openmmapi/include/TholeDipoleForce.h:58-109). */
+#define TDP_NO_CUTOFF 0
+#define TDP_PME 1
+#define TDP_DIRECT 0
+#define TDP_MUTUAL 1
+#define TDP_EXTRAPOLATED 2
+#define TDP_ZTHENX 0
+#define TDP_BISECTOR 1
+#define TDP_ZBISECT 2
+#define TDP_THREEFOLD 3
+#define TDP_ZONLY 4
+#define TDP_NO_AXIS_TYPE 5
+
+/* Arithmetic of the pair kernels.
+ *  MIXED : FP32 pair arithmetic (positions as FP32 offsets from FP64 tile
+ *          centres), FP64 accumulation of every tile's partial sums, FP64 CG
+ *          scalars and FP64 recomputation of the true residual.
+ *  DOUBLE: FP64 pair arithmetic and accumulation throughout ("plain"). */
+#define TDP_PRECISION_MIXED 0
+#define TDP_PRECISION_DOUBLE 1
+
+/* Mutual-polarization solver.  Both stop on the reference's criterion: the
+ * RMS change a Jacobi step would make, sqrt(sum|alpha(E+T mu)-mu|^2 / N)
+ * (ReferenceTholeDipoleForce.cpp:838-846), below the target epsilon.
+ *  CG    : conjugate gradients on the symmetric (alpha^-1 - T) system
+ *          (Jacobi-preconditioned), converging to the same fixed point.
+ *  JACOBI: the reference's own fixed-point iteration, step for step. */
+#define TDP_SOLVER_CG 0
+#define TDP_SOLVER_JACOBI 1
+
+/* Flags of tdp_system_desc.flags. */
+/* The reference reads rInvVec[4] past the end of a 4-element vector in every
+ * dipole-dipole force coefficient (ReferenceTholeDipoleForce.cpp:196 vs
+ * :264,277,323,333).  By default the kernels use 0.0 for that word -- the
+ * value a fresh process of the compiled reference reads, which makes results
+ * reproducible against it.  With this flag they use 1/r^4 instead. */
+#define TDP_FLAG_DD_FORCE_R4 (1u << 0)
+/* Keep the previous call's induced dipoles as the solver's starting point
+ * (the reference restarts from mu0 = alpha*E every call). */
+#define TDP_FLAG_WARM_START (1u << 1)
+
+/* Flags of tdp_compute. */
+#define TDP_COMPUTE_FORCES (1u << 0)
+#define TDP_COMPUTE_ENERGY (1u << 1)
+#define TDP_COMPUTE_REQUIRE_CONVERGENCE (1u << 2)
+
+/* Element types of position / force buffers. */
+#define TDP_F64 0
+#define TDP_F32 1
+
+/* Which dipoles tdp_get_dipoles returns (TholeDipoleKernels.h:91-105). */
+#define TDP_DIPOLES_INDUCED 0
+#define TDP_DIPOLES_LAB_PERMANENT 1
+#define TDP_DIPOLES_TOTAL 2
+
+/* Solver status (tdp_solver_stats). */
+#define TDP_STATUS_CONVERGED 0
+#define TDP_STATUS_MAX_ITERATIONS 1
+#define TDP_STATUS_NON_FINITE 2
+
+typedef struct tdp_handle tdp_handle;
+
+/* Everything ReferenceCalcTholeDipoleForceKernel::initialize copies out of a
+ * TholeDipoleForce (ReferenceTholeDipoleKernels.cpp:83-158). */
+typedef struct tdp_system_desc {
+    int32_t num_particles;
+    const double* charges;              /* n */
+    const double* molecular_dipoles;    /* n*3, local frame */
+    const double* polarizabilities;     /* n */
+    const double* thole_damping;        /* n */
+    const int32_t* axis_types;          /* n */
+    const int32_t* atom_z;              /* n, -1 for none */
+    const int32_t* atom_x;              /* n */
+    const int32_t* atom_y;              /* n */
+    /* Covalent12 (M scale) and Covalent13 (I scale) lists as CSR; offsets have
+     * n+1 entries.  NULL offsets mean empty lists. */
+    const int32_t* covalent12_offsets;
+    const int32_t* covalent12_atoms;
+    const int32_t* covalent13_offsets;
+    const int32_t* covalent13_atoms;
+    int32_t nonbonded_method;           /* TDP_NO_CUTOFF / TDP_PME */
+    int32_t polarization_type;          /* TDP_DIRECT / TDP_MUTUAL / TDP_EXTRAPOLATED */
+    double cutoff;                      /* nm (PME: box must be >= 2*cutoff) */
+    double ewald_error_tolerance;
+    double pme_alpha;                   /* 0 -> chosen from the tolerance */
+    int32_t pme_grid[3];
+    double mutual_target_epsilon;
+    int32_t mutual_max_iterations;
+    int32_t num_extrapolation_coefficients;
+    const double* extrapolation_coefficients;
+    int32_t precision;                  /* TDP_PRECISION_* */
+    int32_t solver;                     /* TDP_SOLVER_* */
+    uint32_t flags;                     /* TDP_FLAG_* */
+} tdp_system_desc;
+
+/* ABI version of the loaded library. */
+int tdp_abi_version(void);
+
+/* Message of the last failure on h (NULL h: the last failure of a create). */
+const char* tdp_last_error(const tdp_handle* h);
+
+/* CalcTholeDipoleForceKernel::initialize (TholeDipoleKernels.h:59); validation
+ * as TholeDipoleForceImpl::initialize (openmmapi/src/TholeDipoleForceImpl.cpp:52-108).
+ * Uploads parameters, builds the exclusion/scale tables and device buffers. */
+int tdp_create(const tdp_system_desc* desc, tdp_handle** out);
+void tdp_destroy(tdp_handle* h);
+
+/* CUDA stream (a cudaStream_t) for all later work; NULL = legacy default stream. */
+int tdp_set_stream(tdp_handle* h, void* stream);
+
+/* Periodic box, 9 doubles (three box vectors, row-major).  Only the diagonal
+ * enters the minimum image (ReferenceTholeDipoleForce.cpp:1414-1423).  PME
+ * requires every diagonal entry >= 1.999999*cutoff
+ * (ReferenceTholeDipoleKernels.cpp:168-172), checked at compute time. */
+int tdp_set_box(tdp_handle* h, const double* box9);
+
+/* CalcTholeDipoleForceKernel::copyParametersToContext (TholeDipoleKernels.h:75,
+ * ReferenceTholeDipoleKernels.cpp:317-339): per-particle parameters and axis
+ * atoms only; num_particles must not change (TDP_ERR_SIZE_MISMATCH). */
+int tdp_update_params(tdp_handle* h, int32_t num_particles, const double* charges,
+                      const double* molecular_dipoles, const double* polarizabilities,
+                      const double* thole_damping, const int32_t* axis_types, const int32_t* atom_z,
+                      const int32_t* atom_x, const int32_t* atom_y);
+
+/* CalcTholeDipoleForceKernel::execute (TholeDipoleKernels.h:68,
+ * ReferenceTholeDipoleKernels.cpp:201-215).  positions: n*3 of pos_dtype, on
+ * the device if on_device else on the host.  With TDP_COMPUTE_FORCES the
+ * forces are ADDED to forces_accum (n*3 of force_dtype, same residency as the
+ * positions); energy (host double) may be NULL. */
+int tdp_compute(tdp_handle* h, const void* positions, int32_t pos_dtype, int32_t on_device,
+                void* forces_accum, int32_t force_dtype, double* energy, uint32_t flags);
+
+/* getInducedDipoles / getLabFramePermanentDipoles / getTotalDipoles
+ * (TholeDipoleKernels.h:91-105) at the given positions (NULL: the positions
+ * of the last tdp_compute).  out: n*3 host doubles. */
+int tdp_get_dipoles(tdp_handle* h, int32_t which, const void* positions, int32_t pos_dtype,
+                    int32_t on_device, double* out);
+
+/* getElectrostaticPotential (TholeDipoleKernels.h:113,
+ * ReferenceTholeDipoleForce.cpp:1315-1372): bare 1/r and 1/r^3 sums of the
+ * charges, lab-frame and induced dipoles at num_points host grid points. */
+int tdp_get_potential(tdp_handle* h, const void* positions, int32_t pos_dtype, int32_t on_device,
+                      const double* grid, int32_t num_points, double* out);
+
+/* getSystemMultipoleMoments (TholeDipoleKernels.h:121,
+ * ReferenceTholeDipoleForce.cpp:1225-1313): 13 values (charge, dipole in
+ * Debye, traceless quadrupole), masses: n host doubles. */
+int tdp_get_moments(tdp_handle* h, const void* positions, int32_t pos_dtype, int32_t on_device,
+                    const double* masses, double* out13);
+
+/* getPMEParameters (TholeDipoleKernels.h:84, ReferenceTholeDipoleKernels.cpp:341-348):
+ * TDP_ERR_NOT_PME unless the method is PME. */
+int tdp_get_pme_parameters(const tdp_handle* h, double* alpha, int32_t* nx, int32_t* ny, int32_t* nz);
+
+/* Solver report of the last solve (ReferenceTholeDipoleForce.h:136-150:
+ * getMutualInducedDipoleIterations / Epsilon / Converged) plus a status. */
+int tdp_solver_stats(const tdp_handle* h, int32_t* iterations, double* epsilon, int32_t* converged,
+                     int32_t* status);
+
+/* Device timing of the last tdp_compute (CUDA events on the handle's stream),
+ * recorded only after tdp_enable_timing(h, 1).  out[TDP_NUM_STAGE_TIMES]:
+ * [0] pack+rotation ms, [1] permanent field ms, [2] induced-dipole solve ms,
+ * [3] energy/force stage ms, [4] torque mapping ms, [5] total ms,
+ * [6] mutual-field matvec launches, [7] summed matvec kernel ms,
+ * [8] energy/force kernel ms, [9] kernel launches of the call. */
+#define TDP_NUM_STAGE_TIMES 10
+int tdp_enable_timing(tdp_handle* h, int32_t enable);
+int tdp_stage_times(const tdp_handle* h, double* out);
+
+#ifdef __cplusplus
+}
+#endif
+#endif

@@ -192,3 +192,26 @@ def small_random_system(n, seed=0, method=S.NO_CUTOFF, polarization=S.MUTUAL, bo
     return S.TholeSystem(positions=pos, charges=q, dipoles=dip, polarizabilities=pol, tholes=th, axis=axis,
                          cov12=cov12, cov13=cov13, method=method, box=np.array([box] * 3), cutoff=0.5 * box * 0.9,
                          polarization=polarization, target_eps=1e-8, max_iter=300, masses=rng.uniform(1, 16, n))
+
+
+def sparse_clumps(n_clumps=12, waters_per_clump=11, box=10.0, seed=21, polarization=S.MUTUAL):
+    """Compact clumps of waters scattered through a large periodic box, stored
+    clump by clump.  Each 32-atom tile is then spatially small while tiles sit
+    up to a box diagonal apart, which exercises both the tile-level minimum
+    image (no per-pair folding) and per-pair folding near the half box."""
+    rng = np.random.default_rng(seed)
+    centres = []
+    for _ in range(n_clumps):
+        c = rng.uniform(0, box, size=3)
+        k = 3
+        g = (np.arange(k) - 1) * 0.31
+        gx, gy, gz = np.meshgrid(g, g, g, indexing="ij")
+        sites = np.stack([gx.ravel(), gy.ravel(), gz.ravel()], 1)[:waters_per_clump]
+        centres.append(c + sites + rng.uniform(-0.02, 0.02, size=sites.shape))
+    centres = np.concatenate(centres)
+    pos = S.place_waters(centres, rng)
+    nw = centres.shape[0]
+    charges, dip, pol, th, axis, cov12, cov13, masses = S._water_parameters(nw)
+    return S.TholeSystem(positions=pos, charges=charges, dipoles=dip, polarizabilities=pol, tholes=th, axis=axis,
+                         cov12=cov12, cov13=cov13, method=S.PME, box=np.array([box] * 3), cutoff=0.9,
+                         polarization=polarization, target_eps=1e-6, max_iter=500, masses=masses)

@@ -1,0 +1,83 @@
+"""C ABI checks that need no GPU: the in-tree library loads, exports every
+entry point that include/*.h declares, and rejects invalid systems in its host
+validation (TholeDipoleForceImpl.cpp:52-108) before touching the device."""
+import ctypes as C
+
+import numpy as np
+import pytest
+
+from tholedipoleplugin_b200 import _capi as A
+from tholedipoleplugin_b200 import build as B
+from tholedipoleplugin_b200 import systems as S
+from tholedipoleplugin_b200.kernel import _DescBuffers
+
+from .fixtures import ammonia
+
+
+@pytest.fixture(scope="module")
+def lib():
+    B.build()
+    return A.lib()
+
+
+def test_exports_every_declared_symbol(lib):
+    declared = A.declared_symbols()
+    assert "tdp_create" in declared and "tdp_compute" in declared
+    for name in declared:
+        assert hasattr(lib, name), name
+    assert set(A.PROTOTYPES) <= set(declared)
+
+
+def test_abi_version(lib):
+    assert lib.tdp_abi_version() == 1
+
+
+def _create(sys_, **kw):
+    buf = _DescBuffers(sys_, 0, 0, 0)
+    for k, v in kw.items():
+        setattr(buf.desc, k, v)
+    h = C.c_void_p()
+    rc = A.lib().tdp_create(C.byref(buf.desc), C.byref(h))
+    return rc, h, buf
+
+
+@pytest.mark.parametrize("mutate,fragment", [
+    (lambda s: s.axis.__setitem__((0, 0), 7), "axis type=7"),
+    (lambda s: s.axis.__setitem__((1, 1), 99), "invalid z axis particle: 99"),
+    (lambda s: s.axis.__setitem__((2, 2), -1), "invalid x axis particle: -1"),
+    (lambda s: s.axis.__setitem__((3, 3), -1), "invalid y axis particle: -1"),
+])
+def test_invalid_axes_rejected(lib, mutate, fragment):
+    s = ammonia()
+    mutate(s)
+    rc, h, _ = _create(s)
+    assert rc == -1
+    assert fragment in lib.tdp_last_error(None).decode()
+
+
+def test_rotation_without_x_atom_rejected(lib):
+    s = ammonia()
+    s.axis[0] = [S.NOAXISTYPE, 1, -1, -1]  # reference would dereference a null particle
+    rc, _, _ = _create(s)
+    assert rc == -1 and "no x axis particle" in lib.tdp_last_error(None).decode()
+
+
+def test_long_covalent_list_rejected(lib):
+    s = ammonia()
+    s.cov12[0] = [1, 2, 3, 4, 5, 6]
+    rc, _, _ = _create(s)
+    assert rc == -1 and "only five scale factors" in lib.tdp_last_error(None).decode()
+
+
+def test_bad_enums_rejected(lib):
+    s = ammonia()
+    assert _create(s, nonbonded_method=2)[0] == -1
+    assert "nonbonded method" in lib.tdp_last_error(None).decode()
+    assert _create(s, polarization_type=5)[0] == -1
+    assert _create(s, precision=9)[0] == -1
+    assert _create(s, solver=9)[0] == -1
+
+
+def test_null_desc(lib):
+    h = C.c_void_p()
+    assert lib.tdp_create(None, C.byref(h)) == -1

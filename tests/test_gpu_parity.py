@@ -1,0 +1,130 @@
+"""GPU kernels (through the C ABI) against the FP64 oracle on the same inputs.
+
+Tolerances:
+  * plain (FP64) form: energy relative 1e-9, forces and induced dipoles RMS
+    relative 1e-8 (rounding-level agreement; the solve runs to 1e-11);
+  * mixed form: energy relative 1e-6 (relative to max(|E|, the Coulomb
+    magnitude sum |q_i q_j|/r_ij) where the total cancels) and RMS relative
+    force error 2e-5 (the accuracy targets for the FP32 path), induced
+    dipoles RMS relative 2e-5;
+  * Jacobi solver: the same iteration count as the reference loop.
+The oracle solves Mutual polarization to 1e-12 so that its own convergence
+error is far below these tolerances."""
+import numpy as np
+import pytest
+
+from oracle import oracle as O
+from tholedipoleplugin_b200 import systems as S
+from tholedipoleplugin_b200.kernel import CudaCalcTholeDipoleForceKernel
+
+from .fixtures import reference_test_systems, small_random_system, sparse_clumps
+from .gpu_util import energy_err, rel_err, rel_rms
+
+pytestmark = pytest.mark.gpu
+
+
+def _systems():
+    out = dict(reference_test_systems())
+    out["random_nocutoff"] = small_random_system(70, seed=11, method=S.NO_CUTOFF)
+    out["random_pme"] = small_random_system(97, seed=12, method=S.PME)
+    out["random_zonly_no_x"] = small_random_system(50, seed=13, method=S.NO_CUTOFF, zonly_without_x=True)
+    out["random_direct"] = small_random_system(65, seed=14, method=S.PME, polarization=S.DIRECT)
+    out["random_extrap"] = small_random_system(66, seed=15, method=S.PME, polarization=S.EXTRAPOLATED)
+    out["water216"] = S.config_small()
+    out["water_cluster"] = S.water_cluster(40, np.random.default_rng(4))
+    out["sparse_clumps"] = sparse_clumps()
+    return out
+
+
+SYSTEMS = _systems()
+_ORACLE = {}
+
+
+def tight(s):
+    return s.copy(target_eps=1e-12, max_iter=5000)
+
+
+def oracle_result(name):
+    if name not in _ORACLE:
+        _ORACLE[name] = O.compute(tight(SYSTEMS[name]), "port")
+    return _ORACLE[name]
+
+
+@pytest.mark.parametrize("name", sorted(SYSTEMS))
+def test_plain_matches_oracle(name):
+    s = SYSTEMS[name]
+    ref = oracle_result(name)
+    with CudaCalcTholeDipoleForceKernel(s.copy(target_eps=1e-11, max_iter=2000), precision="double") as k:
+        e, f = k.execute(s.positions)
+        mu = k.getInducedDipoles()
+        lab = k.getLabFramePermanentDipoles()
+    assert rel_err(e, ref.energy) < 1e-9, (e, ref.energy)
+    assert rel_rms(f, ref.forces) < 1e-8
+    assert rel_rms(mu, ref.induced) < 1e-8
+    assert rel_rms(lab, ref.lab) < 1e-12
+
+
+@pytest.mark.parametrize("name", sorted(SYSTEMS))
+def test_mixed_matches_oracle(name):
+    s = SYSTEMS[name]
+    ref = oracle_result(name)
+    with CudaCalcTholeDipoleForceKernel(s.copy(target_eps=1e-9, max_iter=2000), precision="mixed") as k:
+        e, f = k.execute(s.positions)
+        mu = k.getInducedDipoles()
+    # Energy relative error 1e-6, judged against max(|E|, sum|q_i q_j|/r_ij) so
+    # that random systems whose total energy cancels are not held to a
+    # tolerance below their own term size.
+    assert energy_err(e, ref.energy, s) < 1e-6, (e, ref.energy)
+    assert rel_rms(f, ref.forces) < 2e-5
+    if s.polarization != S.DIRECT or np.abs(ref.induced).max() > 0:
+        assert rel_rms(mu, ref.induced) < 2e-5
+
+
+@pytest.mark.parametrize("name", ["ammonia_mutual", "water4_pme", "triclinic8", "water216", "random_pme"])
+def test_jacobi_matches_reference_loop(name):
+    s = SYSTEMS[name]
+    ref = O.compute(s, "port")
+    with CudaCalcTholeDipoleForceKernel(s, precision="double", solver="jacobi") as k:
+        e, f = k.execute(s.positions)
+        st = k.solverStats()
+    assert st["iterations"] == ref.iterations
+    assert st["converged"] == ref.converged
+    assert rel_err(st["epsilon"], ref.epsilon) < 1e-6
+    assert rel_err(e, ref.energy) < 1e-10
+    assert rel_rms(f, ref.forces) < 1e-9
+
+
+@pytest.mark.parametrize("precision", ["double", "mixed"])
+def test_forces_are_added(precision):
+    s = SYSTEMS["water4_pme"]
+    with CudaCalcTholeDipoleForceKernel(s, precision=precision) as k:
+        base = np.full((s.n, 3), 3.25)
+        e, f = k.execute(s.positions, forces=base.copy())
+        e2, f2 = k.execute(s.positions)
+    assert np.allclose(f - 3.25, f2, rtol=0, atol=1e-12)
+    assert e == e2
+
+
+@pytest.mark.parametrize("precision", ["double", "mixed"])
+def test_queries_match_oracle(precision):
+    s = SYSTEMS["ammonia_mutual"]
+    grid = np.random.default_rng(3).uniform(-0.8, 0.8, size=(33, 3))
+    ts = tight(s)
+    with CudaCalcTholeDipoleForceKernel(s.copy(target_eps=1e-11 if precision == "double" else 1e-9,
+                                                max_iter=2000), precision=precision) as k:
+        pot = k.getElectrostaticPotential(grid, s.positions)
+        mom = k.getSystemMultipoleMoments(s.masses, s.positions)
+        tot = k.getTotalDipoles(s.positions)
+    tol = 1e-9 if precision == "double" else 2e-5
+    assert rel_rms(pot, O.potential(ts, grid, "port")) < tol
+    assert rel_rms(mom, O.moments(ts, "port")) < tol
+    assert rel_rms(tot, O.total_dipoles(ts, "port")) < tol
+
+
+def test_rinv4_power_flag():
+    s = SYSTEMS["water4_pme"]
+    ref = O.compute(tight(s), "port", rinv4_mode=O.RINV4_POWER)
+    with CudaCalcTholeDipoleForceKernel(s.copy(target_eps=1e-11), precision="double", dd_force_r4=True) as k:
+        e, f = k.execute(s.positions)
+    assert rel_err(e, ref.energy) < 1e-9
+    assert rel_rms(f, ref.forces) < 1e-8

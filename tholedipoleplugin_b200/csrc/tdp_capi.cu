@@ -1,0 +1,936 @@
+// tdp_capi.cu -- C ABI (include/tholedipole_b200.h) over the sm_100a kernels:
+// validation, the covalent scale tables, device buffers and the per-call
+// orchestration of rotation -> permanent field -> induced-dipole solve ->
+// energy/force/torque -> torque mapping, in the reference's semantics
+// (aehogan/tholedipoleplugin, platforms/reference/src/ReferenceTholeDipoleForce.cpp,
+// driven as ReferenceCalcTholeDipoleForceKernel does in
+// platforms/reference/src/ReferenceTholeDipoleKernels.cpp).
+#include "tholedipole_b200.h"
+#include "tdp_kernels.cuh"
+
+#include <cuda_runtime.h>
+
+#include <algorithm>
+#include <cmath>
+#include <cstdio>
+#include <cstring>
+#include <map>
+#include <string>
+#include <tuple>
+#include <vector>
+
+using namespace tdp;
+
+namespace {
+
+thread_local std::string g_create_error;
+
+struct TdpError {
+    int code;
+    std::string msg;
+};
+
+#define TDP_CUDA(call)                                                                                      \
+    do {                                                                                                    \
+        cudaError_t e_ = (call);                                                                            \
+        if (e_ != cudaSuccess)                                                                              \
+            throw TdpError{TDP_ERR_CUDA, std::string(#call) + ": " + cudaGetErrorString(e_)};              \
+    } while (0)
+
+template <class T>
+T* dalloc(size_t count, std::vector<void*>& owned) {
+    void* p = nullptr;
+    if (count == 0) count = 1;
+    TDP_CUDA(cudaMalloc(&p, count * sizeof(T)));
+    TDP_CUDA(cudaMemset(p, 0, count * sizeof(T)));
+    owned.push_back(p);
+    return static_cast<T*>(p);
+}
+
+}  // namespace
+
+struct tdp_handle {
+    int n = 0;
+    int method = TDP_NO_CUTOFF;
+    int polarization = TDP_MUTUAL;
+    int precision = TDP_PRECISION_MIXED;
+    int solver = TDP_SOLVER_CG;
+    uint32_t flags = 0;
+    double cutoff = 1.0, ewald_tol = 1e-4, pme_alpha = 0.0;
+    int pme_grid[3] = {0, 0, 0};
+    double target_eps = 1e-5;
+    int max_iter = 60;
+    std::vector<double> extrap;
+    double box[9] = {0, 0, 0, 0, 0, 0, 0, 0, 0};
+    bool have_box = false;
+
+    // Host copies of the per-particle parameters.
+    std::vector<double> charge, dip, alpha, thole;
+    std::vector<int> axis;  // n*4
+
+    Dev d;
+    std::vector<void*> owned;
+    cudaStream_t stream = nullptr;
+    double* h_scal = nullptr;   // pinned scalar readback
+    double* h_forces = nullptr; // pinned n*3
+    double* d_stage = nullptr;  // device staging for host FP32 positions / query inputs
+    size_t stage_bytes = 0;
+    bool mu_prev_valid = false;
+    bool have_results = false;
+
+    int iterations = 0;
+    double epsilon = 1.0e50;
+    int converged = 0;
+    int status = TDP_STATUS_CONVERGED;
+    int matvecs = 0;
+    size_t nscal = 0;  // capacity of the per-iteration scalar arrays
+
+    bool timing = false;
+    cudaEvent_t ev[6] = {nullptr, nullptr, nullptr, nullptr, nullptr, nullptr};
+    std::vector<cudaEvent_t> kev;  // event pairs around matvec / energy kernels
+    std::vector<int> kev_kind;     // 0 matvec, 1 energy, per pair
+    size_t kev_used = 0;
+    double stage_ms[TDP_NUM_STAGE_TIMES] = {};
+    long launches = 0;
+
+    std::string err;
+};
+
+namespace {
+
+int fail(tdp_handle* h, const TdpError& e) {
+    if (h) h->err = e.msg;
+    else g_create_error = e.msg;
+    return e.code;
+}
+
+// ---------------------------------------------------------------------------
+// Validation: TholeDipoleForceImpl::initialize (openmmapi/src/TholeDipoleForceImpl.cpp:52-108)
+// plus the inputs on which the reference dereferences null or out-of-range
+// memory (rotation of an atom with Z set and no X atom, RTDF.cpp:556-568;
+// covalent lists longer than the five scale entries, RTDF.cpp:609-633).
+// ---------------------------------------------------------------------------
+void validate_axes(int n, const int32_t* types, const int32_t* zs, const int32_t* xs, const int32_t* ys) {
+    for (int i = 0; i < n; i++) {
+        int t = types[i], z = zs[i], x = xs[i], y = ys[i];
+        char buf[256];
+        if (t < TDP_ZTHENX || t > TDP_NO_AXIS_TYPE) {
+            snprintf(buf, sizeof buf,
+                     "TholeDipoleForce: axis type=%d not currently handled - only axisTypes[ 0, 1, 2, 3, 4, 5] "
+                     "(ZThenX, Bisector, Z-Bisect, ThreeFold, ZOnly, NoAxisType) currently handled.",
+                     t);
+            throw TdpError{TDP_ERR_INVALID_ARGUMENT, buf};
+        }
+        if (t != TDP_NO_AXIS_TYPE && (z < 0 || z >= n)) {
+            snprintf(buf, sizeof buf, "TholeDipoleForce: invalid z axis particle: %d", z);
+            throw TdpError{TDP_ERR_INVALID_ARGUMENT, buf};
+        }
+        if (t != TDP_NO_AXIS_TYPE && t != TDP_ZONLY && (x < 0 || x >= n)) {
+            snprintf(buf, sizeof buf, "TholeDipoleForce: invalid x axis particle: %d", x);
+            throw TdpError{TDP_ERR_INVALID_ARGUMENT, buf};
+        }
+        if ((t == TDP_ZBISECT || t == TDP_THREEFOLD) && (y < 0 || y >= n)) {
+            snprintf(buf, sizeof buf, "TholeDipoleForce: invalid y axis particle: %d", y);
+            throw TdpError{TDP_ERR_INVALID_ARGUMENT, buf};
+        }
+        if (z >= n || x >= n || y >= n) {
+            snprintf(buf, sizeof buf, "TholeDipoleForce: axis particle index out of range for particle %d", i);
+            throw TdpError{TDP_ERR_INVALID_ARGUMENT, buf};
+        }
+        if (z >= 0 && z != i && t != TDP_ZONLY && x < 0) {
+            snprintf(buf, sizeof buf,
+                     "TholeDipoleForce: particle %d has a z axis particle but no x axis particle (the reference "
+                     "platform dereferences a null particle here)",
+                     i);
+            throw TdpError{TDP_ERR_INVALID_ARGUMENT, buf};
+        }
+    }
+}
+
+double damp_radius2(const std::vector<double>& thole) {
+    // a*u^3 < 50 needs r < t_i t_j (50/min(t_i,t_j))^(1/3) <= tmax^(5/3) 50^(1/3).
+    double tmax = 0.0;
+    bool negative = false;
+    for (double t : thole) {
+        if (t < 0.0 || std::isnan(t)) negative = true;
+        tmax = std::max(tmax, t);
+    }
+    if (negative) return INFINITY;
+    if (tmax == 0.0) return 0.0;
+    double r = std::pow(tmax, 5.0 / 3.0) * std::cbrt(50.0) * 1.001;
+    return r * r;
+}
+
+void upload(void* dst, const void* src, size_t bytes) {
+    if (bytes) TDP_CUDA(cudaMemcpy(dst, src, bytes, cudaMemcpyHostToDevice));
+}
+
+// Per-particle parameters and everything derived from them.
+void upload_params(tdp_handle* h) {
+    int n = h->n;
+    Dev& d = h->d;
+    std::vector<double> sal(n);
+    for (int i = 0; i < n; i++) sal[i] = h->alpha[i] > 0.0 ? std::sqrt(h->alpha[i]) : 0.0;
+    upload(d.charge, h->charge.data(), sizeof(double) * n);
+    upload(d.dip_mol, h->dip.data(), sizeof(double) * 3 * n);
+    upload(d.alpha, h->alpha.data(), sizeof(double) * n);
+    upload(d.salpha, sal.data(), sizeof(double) * n);
+    upload(d.thole, h->thole.data(), sizeof(double) * n);
+    upload(d.axis, h->axis.data(), sizeof(int) * 4 * n);
+    d.pp.damp_r2 = (float)damp_radius2(h->thole);
+
+    // Torque-mapping users (RTDF.cpp:915-1115): which atoms receive force from
+    // the frame of atom i, and in which role.
+    std::vector<std::vector<std::pair<int, int>>> users(n);
+    for (int i = 0; i < n; i++) {
+        int t = h->axis[4 * i], z = h->axis[4 * i + 1], x = h->axis[4 * i + 2], y = h->axis[4 * i + 3];
+        if (t == TDP_NO_AXIS_TYPE) continue;
+        users[i].push_back({i, 0});
+        users[z].push_back({i, 1});
+        if (t != TDP_ZONLY && x >= 0) users[x].push_back({i, 2});
+        if ((t == TDP_ZBISECT || t == TDP_THREEFOLD) && y > -1) users[y].push_back({i, 3});
+    }
+    std::vector<int> off(n + 1, 0);
+    std::vector<int2> flat;
+    for (int a = 0; a < n; a++) {
+        for (auto& u : users[a]) flat.push_back(make_int2(u.first, u.second));
+        off[a + 1] = (int)flat.size();
+    }
+    if (d.users) {
+        cudaFree(d.users);
+        h->owned.erase(std::find(h->owned.begin(), h->owned.end(), (void*)d.users));
+    }
+    d.users = dalloc<int2>(flat.size(), h->owned);
+    upload(d.users_off, off.data(), sizeof(int) * (n + 1));
+    upload(d.users, flat.data(), sizeof(int2) * flat.size());
+}
+
+void refresh_box(tdp_handle* h) {
+    PairParams& P = h->d.pp;
+    P.periodic = h->method == TDP_PME ? 1 : 0;
+    for (int k = 0; k < 3; k++) {
+        double L = h->box[4 * k];
+        if (!P.periodic || !(L > 0.0)) {
+            // getPeriodicDelta skips a zero box dimension (RTDF.cpp:1419).
+            P.box[k] = 0.0;
+            P.inv_box[k] = 0.0;
+            P.half_box_tol[k] = INFINITY;
+        } else {
+            P.box[k] = L;
+            P.inv_box[k] = 1.0 / L;
+            // Pairs whose FP32 displacement lies within 16 ulp of half a box are
+            // re-derived in FP64.
+            int ex;
+            std::frexp(L, &ex);
+            double ulp = std::ldexp(1.0, ex - 24);
+            P.half_box_tol[k] = 0.5 * L - 16.0 * ulp;
+        }
+    }
+}
+
+template <class R>
+void setup_and_solve(tdp_handle* h);
+
+template <class R>
+void run_energy(tdp_handle* h);
+
+void stage_positions(tdp_handle* h, const void* positions, int dtype, int on_device) {
+    Dev& d = h->d;
+    size_t n3 = 3 * (size_t)h->n;
+    if (dtype != TDP_F64 && dtype != TDP_F32) throw TdpError{TDP_ERR_INVALID_ARGUMENT, "unknown position dtype"};
+    if (!positions) throw TdpError{TDP_ERR_INVALID_ARGUMENT, "positions is NULL"};
+    if (on_device) {
+        if (dtype == TDP_F64)
+            TDP_CUDA(cudaMemcpyAsync(d.pos, positions, n3 * 8, cudaMemcpyDeviceToDevice, h->stream));
+        else
+            launch_positions_in(d, positions, 1, h->stream);
+    } else {
+        if (dtype == TDP_F64) {
+            TDP_CUDA(cudaMemcpyAsync(d.pos, positions, n3 * 8, cudaMemcpyHostToDevice, h->stream));
+        } else {
+            TDP_CUDA(cudaMemcpyAsync(h->d_stage, positions, n3 * 4, cudaMemcpyHostToDevice, h->stream));
+            launch_positions_in(d, h->d_stage, 1, h->stream);
+        }
+    }
+}
+
+void check_box(tdp_handle* h) {
+    if (h->method != TDP_PME) return;
+    double minAllowed = 1.999999 * h->cutoff;
+    if (!h->have_box || h->box[0] < minAllowed || h->box[4] < minAllowed || h->box[8] < minAllowed)
+        throw TdpError{TDP_ERR_BOX_TOO_SMALL, "The periodic box size has decreased to less than twice the nonbonded cutoff."};
+}
+
+double read_scalar(tdp_handle* h, const double* dptr) {
+    TDP_CUDA(cudaMemcpyAsync(h->h_scal, dptr, sizeof(double), cudaMemcpyDeviceToHost, h->stream));
+    TDP_CUDA(cudaStreamSynchronize(h->stream));
+    return *h->h_scal;
+}
+
+void record(tdp_handle* h, int k) {
+    if (h->timing) TDP_CUDA(cudaEventRecord(h->ev[k], h->stream));
+}
+
+// Event pair around one pair-kernel launch (kind 0: matvec, 1: energy).
+size_t kernel_begin(tdp_handle* h, int kind) {
+    if (!h->timing) return 0;
+    size_t k = h->kev_used++;
+    if (2 * k + 2 > h->kev.size()) {
+        cudaEvent_t a, b;
+        TDP_CUDA(cudaEventCreate(&a));
+        TDP_CUDA(cudaEventCreate(&b));
+        h->kev.push_back(a);
+        h->kev.push_back(b);
+        h->kev_kind.push_back(kind);
+    }
+    h->kev_kind[k] = kind;
+    TDP_CUDA(cudaEventRecord(h->kev[2 * k], h->stream));
+    return k;
+}
+void kernel_end(tdp_handle* h, size_t k) {
+    if (h->timing) TDP_CUDA(cudaEventRecord(h->kev[2 * k + 1], h->stream));
+}
+
+// One mutual-field matvec (pair kernel), timed and counted.
+template <class R>
+void matvec(tdp_handle* h) {
+    size_t k = kernel_begin(h, 0);
+    launch_field<R>(h->d, 1, h->stream);
+    kernel_end(h, k);
+    h->matvecs++;
+    h->launches++;
+}
+
+// Mutual polarization by conjugate gradients in y = mu / sqrt(alpha):
+// (I - S T S) y = S E with S = diag(sqrt(alpha)), whose fixed point is the
+// reference's Jacobi fixed point mu = alpha (E + T mu).  The stopping test is
+// the reference's epsilon: the RMS change a Jacobi step would make,
+// sqrt(sum alpha |r|^2 / N), confirmed on the true residual before returning.
+template <class R>
+void solve_cg(tdp_handle* h) {
+    Dev& d = h->d;
+    cudaStream_t st = h->stream;
+    const int cap = h->max_iter;
+    int slot = 0;
+    // Residual of the starting point (mu = alpha E, or the previous solution).
+    matvec<R>(h);
+    launch_cg_residual<R>(d, st);
+    launch_cg_p<R>(d, -1, slot, st);
+    h->launches += 2;
+    double eps = read_scalar(h, d.scal_eps + slot);
+    bool is_true = true;
+    int it = 0;
+    h->status = TDP_STATUS_MAX_ITERATIONS;
+    while (true) {
+        if (!std::isfinite(eps)) {
+            h->status = TDP_STATUS_NON_FINITE;
+            break;
+        }
+        if (eps <= h->target_eps || it >= cap || (size_t)slot + 3 >= h->nscal) {
+            if (!is_true) {
+                launch_cg_mu<R>(d, st);
+                matvec<R>(h);
+                launch_cg_residual<R>(d, st);
+                launch_cg_p<R>(d, -1, ++slot, st);
+                h->launches += 3;
+                eps = read_scalar(h, d.scal_eps + slot);
+                is_true = true;
+                continue;
+            }
+            if (eps <= h->target_eps) h->status = TDP_STATUS_CONVERGED;
+            break;
+        }
+        matvec<R>(h);
+        launch_cg_q(d, st);
+        launch_cg_update(d, slot, st);
+        launch_cg_p<R>(d, slot, slot + 1, st);
+        h->launches += 3;
+        slot++;
+        it++;
+        eps = read_scalar(h, d.scal_eps + slot);
+        is_true = false;
+    }
+    launch_cg_mu<R>(d, st);
+    h->launches += 1;
+    h->iterations = it;
+    h->epsilon = eps;
+    h->converged = (h->status == TDP_STATUS_CONVERGED) ? 1 : 0;
+}
+
+// The reference's own Jacobi loop (RTDF.cpp:820-851), sweep for sweep.
+template <class R>
+void solve_jacobi(tdp_handle* h) {
+    Dev& d = h->d;
+    cudaStream_t st = h->stream;
+    double eps = 1.0;
+    int it = 0;
+    for (; it < h->max_iter && eps > h->target_eps; it++) {
+        matvec<R>(h);
+        launch_jacobi<R>(d, st);
+        launch_eps_scalar(d, it, st);
+        h->launches += 2;
+        eps = read_scalar(h, d.scal_eps + it);
+        if (!std::isfinite(eps)) break;
+    }
+    h->iterations = it;
+    h->epsilon = eps;
+    h->converged = eps < h->target_eps ? 1 : 0;
+    h->status = std::isfinite(eps) ? (h->converged ? TDP_STATUS_CONVERGED : TDP_STATUS_MAX_ITERATIONS)
+                                   : TDP_STATUS_NON_FINITE;
+}
+
+// Perturbation-theory extrapolation (RTDF.cpp:853-909).
+template <class R>
+void solve_extrapolated(tdp_handle* h) {
+    Dev& d = h->d;
+    cudaStream_t st = h->stream;
+    int k = (int)h->extrap.size();
+    TDP_CUDA(cudaMemcpyAsync(d.hist, d.mu, sizeof(double) * 3 * h->n, cudaMemcpyDeviceToDevice, st));
+    for (int o = 1; o < k; o++) {
+        matvec<R>(h);
+        launch_extrap_step<R>(d, o, st);
+        h->launches++;
+    }
+    launch_extrap_combine<R>(d, k, d.coef, st);
+    matvec<R>(h);
+    launch_step_eps(d, st);
+    launch_eps_scalar(d, 0, st);
+    h->launches += 3;
+    h->epsilon = read_scalar(h, d.scal_eps);
+    h->iterations = k;
+    h->converged = 1;
+    h->status = std::isfinite(h->epsilon) ? TDP_STATUS_CONVERGED : TDP_STATUS_NON_FINITE;
+}
+
+// setup (RTDF.cpp:1117-1155): rotation, permanent field, induced dipoles.
+template <class R>
+void setup_and_solve(tdp_handle* h) {
+    Dev& d = h->d;
+    cudaStream_t st = h->stream;
+    h->matvecs = 0;
+    h->launches = 0;
+    h->kev_used = 0;
+    record(h, 0);
+    launch_pack<R>(d, st);
+    launch_rotate<R>(d, st);
+    record(h, 1);
+    launch_field<R>(d, 0, st);
+    launch_fixed_done<R>(d, st);
+    h->launches += 4;
+    record(h, 2);
+    if (h->polarization == TDP_DIRECT) {
+        h->iterations = 0;
+        h->epsilon = 1.0e50;
+        h->converged = 1;
+        h->status = TDP_STATUS_CONVERGED;
+    } else if (h->polarization == TDP_MUTUAL) {
+        if (h->solver == TDP_SOLVER_JACOBI) {
+            solve_jacobi<R>(h);
+        } else {
+            if ((h->flags & TDP_FLAG_WARM_START) && h->mu_prev_valid) {
+                TDP_CUDA(cudaMemcpyAsync(d.mu, d.mu_prev, sizeof(double) * 3 * h->n, cudaMemcpyDeviceToDevice, st));
+                launch_warm_start<R>(d, st);
+                h->launches++;
+            }
+            solve_cg<R>(h);
+        }
+        TDP_CUDA(cudaMemcpyAsync(d.mu_prev, d.mu, sizeof(double) * 3 * h->n, cudaMemcpyDeviceToDevice, st));
+        h->mu_prev_valid = h->status == TDP_STATUS_CONVERGED;
+    } else {
+        solve_extrapolated<R>(h);
+    }
+    record(h, 3);
+}
+
+// calculateElectrostatic + mapTorqueToForce (RTDF.cpp:117-124).
+template <class R>
+void run_energy(tdp_handle* h) {
+    Dev& d = h->d;
+    cudaStream_t st = h->stream;
+    launch_pack_ind<R>(d, st);
+    size_t k = kernel_begin(h, 1);
+    launch_energy<R>(d, st);
+    kernel_end(h, k);
+    launch_energy_done(d, st);
+    record(h, 4);
+    launch_torque_gather(d, st);
+    record(h, 5);
+    h->launches += 4;
+}
+
+void finish_timing(tdp_handle* h) {
+    if (!h->timing) return;
+    TDP_CUDA(cudaEventSynchronize(h->ev[5]));
+    float ms;
+    for (int k = 0; k < 5; k++) {
+        TDP_CUDA(cudaEventElapsedTime(&ms, h->ev[k], h->ev[k + 1]));
+        h->stage_ms[k] = ms;
+    }
+    TDP_CUDA(cudaEventElapsedTime(&ms, h->ev[0], h->ev[5]));
+    h->stage_ms[5] = ms;
+    h->stage_ms[6] = h->matvecs;
+    double mv = 0.0, en = 0.0;
+    for (size_t k = 0; k < h->kev_used; k++) {
+        TDP_CUDA(cudaEventElapsedTime(&ms, h->kev[2 * k], h->kev[2 * k + 1]));
+        if (h->kev_kind[k] == 0) mv += ms;
+        else en += ms;
+    }
+    h->stage_ms[7] = mv;
+    h->stage_ms[8] = en;
+    h->stage_ms[9] = (double)h->launches;
+}
+
+void solve_at(tdp_handle* h, const void* positions, int dtype, int on_device) {
+    if (positions) {
+        check_box(h);
+        stage_positions(h, positions, dtype, on_device);
+        if (h->precision == TDP_PRECISION_DOUBLE) setup_and_solve<double>(h);
+        else setup_and_solve<float>(h);
+        h->have_results = true;
+    } else if (!h->have_results) {
+        throw TdpError{TDP_ERR_INVALID_ARGUMENT, "no positions given and no previous evaluation"};
+    }
+}
+
+}  // namespace
+
+extern "C" {
+
+int tdp_abi_version(void) { return TDP_ABI_VERSION; }
+
+const char* tdp_last_error(const tdp_handle* h) { return h ? h->err.c_str() : g_create_error.c_str(); }
+
+int tdp_create(const tdp_system_desc* desc, tdp_handle** out) {
+    if (!out) return TDP_ERR_INVALID_ARGUMENT;
+    *out = nullptr;
+    tdp_handle* h = new tdp_handle();
+    try {
+        if (!desc) throw TdpError{TDP_ERR_INVALID_ARGUMENT, "desc is NULL"};
+        int n = desc->num_particles;
+        if (n < 0) throw TdpError{TDP_ERR_INVALID_ARGUMENT, "num_particles < 0"};
+        if (n > 0 && (!desc->charges || !desc->molecular_dipoles || !desc->polarizabilities ||
+                      !desc->thole_damping || !desc->axis_types || !desc->atom_z || !desc->atom_x || !desc->atom_y))
+            throw TdpError{TDP_ERR_INVALID_ARGUMENT, "a per-particle array is NULL"};
+        if (desc->nonbonded_method < 0 || desc->nonbonded_method > 1)
+            throw TdpError{TDP_ERR_INVALID_ARGUMENT, "TholeDipoleForce: Illegal value for nonbonded method"};
+        if (desc->polarization_type < 0 || desc->polarization_type > 2)
+            throw TdpError{TDP_ERR_INVALID_ARGUMENT, "Polarization type not recognized."};
+        if (desc->precision != TDP_PRECISION_MIXED && desc->precision != TDP_PRECISION_DOUBLE)
+            throw TdpError{TDP_ERR_INVALID_ARGUMENT, "unknown precision"};
+        if (desc->solver != TDP_SOLVER_CG && desc->solver != TDP_SOLVER_JACOBI)
+            throw TdpError{TDP_ERR_INVALID_ARGUMENT, "unknown solver"};
+        validate_axes(n, desc->axis_types, desc->atom_z, desc->atom_x, desc->atom_y);
+
+        h->n = n;
+        h->method = desc->nonbonded_method;
+        h->polarization = desc->polarization_type;
+        h->precision = desc->precision;
+        h->solver = desc->solver;
+        h->flags = desc->flags;
+        h->cutoff = desc->cutoff;
+        h->ewald_tol = desc->ewald_error_tolerance;
+        h->pme_alpha = desc->pme_alpha;
+        for (int k = 0; k < 3; k++) h->pme_grid[k] = desc->pme_grid[k];
+        h->target_eps = desc->mutual_target_epsilon;
+        h->max_iter = std::max(0, desc->mutual_max_iterations);
+        if (desc->num_extrapolation_coefficients > 0 && desc->extrapolation_coefficients)
+            h->extrap.assign(desc->extrapolation_coefficients,
+                             desc->extrapolation_coefficients + desc->num_extrapolation_coefficients);
+        else
+            h->extrap = {-0.154, 0.017, 0.658, 0.474};  // RTDF.cpp:857-864
+        h->charge.assign(desc->charges, desc->charges + n);
+        h->dip.assign(desc->molecular_dipoles, desc->molecular_dipoles + 3 * (size_t)n);
+        h->alpha.assign(desc->polarizabilities, desc->polarizabilities + n);
+        h->thole.assign(desc->thole_damping, desc->thole_damping + n);
+        h->axis.resize(4 * (size_t)n);
+        for (int i = 0; i < n; i++) {
+            h->axis[4 * i] = desc->axis_types[i];
+            h->axis[4 * i + 1] = desc->atom_z[i];
+            h->axis[4 * i + 2] = desc->atom_x[i];
+            h->axis[4 * i + 3] = desc->atom_y[i];
+        }
+
+        // Covalent scales (RTDF.cpp:609-644): pair (i<j) takes _mScale[pos] for
+        // j at list position pos of Covalent12(i) and _iScale[pos] for
+        // Covalent13(i), the last occurrence winning; lists of more than five
+        // entries index past the scale tables in the reference.
+        static const double kM[5] = {0.0, 0.0, 0.0, 0.5, 1.0};
+        static const double kI[5] = {0.0, 1.0, 1.0, 1.0, 1.0};
+        std::map<std::pair<int, int>, std::pair<double, double>> scales;
+        for (int i = 0; i < n; i++) {
+            for (int list = 0; list < 2; list++) {
+                const int32_t* off = list == 0 ? desc->covalent12_offsets : desc->covalent13_offsets;
+                const int32_t* atoms = list == 0 ? desc->covalent12_atoms : desc->covalent13_atoms;
+                if (!off) continue;
+                int b = off[i], e = off[i + 1];
+                if (e - b > 5) {
+                    char buf[200];
+                    snprintf(buf, sizeof buf,
+                             "TholeDipoleForce: particle %d has %d Covalent1%d entries; only five scale factors exist",
+                             i, e - b, list == 0 ? 2 : 3);
+                    throw TdpError{TDP_ERR_INVALID_ARGUMENT, buf};
+                }
+                for (int p = b; p < e; p++) {
+                    int j = atoms[p];
+                    if (j <= i || j >= n) continue;  // only the lower-index atom's list counts
+                    auto it = scales.find({i, j});
+                    if (it == scales.end()) it = scales.insert({{i, j}, {1.0, 1.0}}).first;
+                    if (list == 0) it->second.first = kM[p - b];
+                    else it->second.second = kI[p - b];
+                }
+            }
+        }
+        std::vector<std::vector<std::tuple<int, double, double>>> exc(n);
+        for (auto& kv : scales) {
+            double m = kv.second.first, s = kv.second.second;
+            if (m == 1.0 && s == 1.0) continue;
+            exc[kv.first.first].push_back(std::make_tuple(kv.first.second, m - 1.0, s - 1.0));
+            exc[kv.first.second].push_back(std::make_tuple(kv.first.first, m - 1.0, s - 1.0));
+        }
+        std::vector<int> eoff(n + 1, 0), ej;
+        std::vector<double> em, es;
+        for (int i = 0; i < n; i++) {
+            for (auto& t : exc[i]) {
+                ej.push_back(std::get<0>(t));
+                em.push_back(std::get<1>(t));
+                es.push_back(std::get<2>(t));
+            }
+            eoff[i + 1] = (int)ej.size();
+        }
+
+        // Launch geometry.
+        Dev& d = h->d;
+        d.n = n;
+        d.n_pad = std::max(kBlockI, ((n + kBlockI - 1) / kBlockI) * kBlockI);
+        d.nvb = std::max(1, (n + kVecThreads - 1) / kVecThreads);
+        int n_iblk = d.n_pad / kBlockI;
+        int n_stage = d.n_pad / kJStage;
+        int want = (4 * 148 * 8 + n_iblk - 1) / n_iblk;
+        if (const char* e = getenv("TDP_NSPLIT")) want = std::max(1, atoi(e));
+        want = std::max(1, std::min(want, n_stage));
+        int chunk_stages = (n_stage + want - 1) / want;
+        d.pp.j_chunk = chunk_stages * kJStage;
+        d.nsplit = (n_stage + chunk_stages - 1) / chunk_stages;
+        d.pp.n = n;
+        d.pp.n_tiles = (n + kTile - 1) / kTile;
+        d.pp.mutual = h->polarization == TDP_MUTUAL ? 1 : 0;
+        d.pp.rinv4_power = (h->flags & TDP_FLAG_DD_FORCE_R4) ? 1.0f : 0.0f;
+        d.pp.rinv4_fill = 0.0f;
+
+        size_t rsz = h->precision == TDP_PRECISION_DOUBLE ? sizeof(double4) : sizeof(float4);
+        auto& o = h->owned;
+        d.pos = dalloc<double>(3 * (size_t)d.n_pad, o);
+        d.charge = dalloc<double>(n, o);
+        d.dip_mol = dalloc<double>(3 * (size_t)n, o);
+        d.alpha = dalloc<double>(n, o);
+        d.salpha = dalloc<double>(n, o);
+        d.thole = dalloc<double>(n, o);
+        d.axis = dalloc<int4>(n, o);
+        d.posq = dalloc<char>(rsz * d.n_pad, o);
+        d.dipt = dalloc<char>(rsz * d.n_pad, o);
+        d.vec = dalloc<char>(rsz * d.n_pad, o);
+        d.ind = dalloc<char>(rsz * d.n_pad, o);
+        d.yz = dalloc<double2>(d.n_pad, o);
+        d.tctr = dalloc<double4>(d.n_pad / kTile, o);
+        d.text = dalloc<double4>(d.n_pad / kTile, o);
+        d.exc_off = dalloc<int>(n + 1, o);
+        d.exc_j = dalloc<int>(ej.size(), o);
+        d.exc_m = dalloc<double>(em.size(), o);
+        d.exc_s = dalloc<double>(es.size(), o);
+        d.users_off = dalloc<int>(n + 1, o);
+        size_t n3 = 3 * (size_t)n;
+        d.lab = dalloc<double>(n3, o);
+        d.E = dalloc<double>(n3, o);
+        d.mu = dalloc<double>(n3, o);
+        d.mu_prev = dalloc<double>(n3, o);
+        d.y = dalloc<double>(n3, o);
+        d.r = dalloc<double>(n3, o);
+        d.p = dalloc<double>(n3, o);
+        d.q = dalloc<double>(n3, o);
+        d.hist = dalloc<double>(n3 * h->extrap.size(), o);
+        d.partial = dalloc<double>((size_t)d.nsplit * 6 * d.n_pad, o);
+        d.energy_partial = dalloc<double>((size_t)d.nsplit * n_iblk, o);
+        d.fpair = dalloc<double>(n3, o);
+        d.torque = dalloc<double>(n3, o);
+        d.ftotal = dalloc<double>(n3, o);
+        d.energy = dalloc<double>(1, o);
+        d.rr_part = dalloc<double>(d.nvb, o);
+        d.eps_part = dalloc<double>(d.nvb, o);
+        d.pq_part = dalloc<double>(d.nvb, o);
+        // CG uses one slot per iteration plus one per true-residual check.
+        h->nscal = 2 * (size_t)std::max(h->max_iter, 0) + 64;
+        size_t nscal = h->nscal;
+        d.scal_rr = dalloc<double>(nscal, o);
+        d.scal_eps = dalloc<double>(nscal, o);
+        d.coef = dalloc<double>(h->extrap.size(), o);
+        h->stage_bytes = std::max<size_t>(n3 * sizeof(double), 64 * sizeof(double));
+        h->d_stage = dalloc<double>(h->stage_bytes / sizeof(double), o);
+        upload(d.exc_off, eoff.data(), sizeof(int) * (n + 1));
+        upload(d.exc_j, ej.data(), sizeof(int) * ej.size());
+        upload(d.exc_m, em.data(), sizeof(double) * em.size());
+        upload(d.exc_s, es.data(), sizeof(double) * es.size());
+        upload(d.coef, h->extrap.data(), sizeof(double) * h->extrap.size());
+        upload_params(h);
+        TDP_CUDA(cudaMallocHost(&h->h_scal, 64 * sizeof(double)));
+        TDP_CUDA(cudaMallocHost(&h->h_forces, std::max<size_t>(n3, 1) * sizeof(double)));
+        for (int k = 0; k < 6; k++) TDP_CUDA(cudaEventCreate(&h->ev[k]));
+        refresh_box(h);
+        TDP_CUDA(cudaDeviceSynchronize());
+    } catch (const TdpError& e) {
+        int code = fail(nullptr, e);
+        tdp_destroy(h);
+        return code;
+    } catch (const std::exception& e) {
+        g_create_error = e.what();
+        tdp_destroy(h);
+        return TDP_ERR_INVALID_ARGUMENT;
+    }
+    *out = h;
+    return TDP_OK;
+}
+
+void tdp_destroy(tdp_handle* h) {
+    if (!h) return;
+    for (void* p : h->owned) cudaFree(p);
+    if (h->h_scal) cudaFreeHost(h->h_scal);
+    if (h->h_forces) cudaFreeHost(h->h_forces);
+    for (int k = 0; k < 6; k++)
+        if (h->ev[k]) cudaEventDestroy(h->ev[k]);
+    for (cudaEvent_t e : h->kev) cudaEventDestroy(e);
+    delete h;
+}
+
+int tdp_set_stream(tdp_handle* h, void* stream) {
+    if (!h) return TDP_ERR_INVALID_ARGUMENT;
+    h->stream = static_cast<cudaStream_t>(stream);
+    return TDP_OK;
+}
+
+int tdp_set_box(tdp_handle* h, const double* box9) {
+    if (!h || !box9) return TDP_ERR_INVALID_ARGUMENT;
+    for (int k = 0; k < 9; k++) h->box[k] = box9[k];
+    h->have_box = true;
+    refresh_box(h);
+    return TDP_OK;
+}
+
+int tdp_update_params(tdp_handle* h, int32_t num_particles, const double* charges, const double* molecular_dipoles,
+                      const double* polarizabilities, const double* thole_damping, const int32_t* axis_types,
+                      const int32_t* atom_z, const int32_t* atom_x, const int32_t* atom_y) {
+    if (!h) return TDP_ERR_INVALID_ARGUMENT;
+    try {
+        if (num_particles != h->n)
+            throw TdpError{TDP_ERR_SIZE_MISMATCH, "updateParametersInContext: The number of particles has changed"};
+        int n = h->n;
+        if (n > 0 && (!charges || !molecular_dipoles || !polarizabilities || !thole_damping || !axis_types ||
+                      !atom_z || !atom_x || !atom_y))
+            throw TdpError{TDP_ERR_INVALID_ARGUMENT, "a per-particle array is NULL"};
+        validate_axes(n, axis_types, atom_z, atom_x, atom_y);
+        h->charge.assign(charges, charges + n);
+        h->dip.assign(molecular_dipoles, molecular_dipoles + 3 * (size_t)n);
+        h->alpha.assign(polarizabilities, polarizabilities + n);
+        h->thole.assign(thole_damping, thole_damping + n);
+        for (int i = 0; i < n; i++) {
+            h->axis[4 * i] = axis_types[i];
+            h->axis[4 * i + 1] = atom_z[i];
+            h->axis[4 * i + 2] = atom_x[i];
+            h->axis[4 * i + 3] = atom_y[i];
+        }
+        TDP_CUDA(cudaStreamSynchronize(h->stream));
+        upload_params(h);
+        h->mu_prev_valid = false;
+        h->have_results = false;
+    } catch (const TdpError& e) {
+        return fail(h, e);
+    }
+    return TDP_OK;
+}
+
+int tdp_compute(tdp_handle* h, const void* positions, int32_t pos_dtype, int32_t on_device, void* forces_accum,
+                int32_t force_dtype, double* energy, uint32_t flags) {
+    if (!h) return TDP_ERR_INVALID_ARGUMENT;
+    try {
+        if (h->n == 0) {
+            if (energy) *energy = 0.0;
+            h->iterations = 0;
+            h->converged = 1;
+            return TDP_OK;
+        }
+        if ((flags & TDP_COMPUTE_FORCES) && !forces_accum)
+            throw TdpError{TDP_ERR_INVALID_ARGUMENT, "forces requested but forces_accum is NULL"};
+        if ((flags & TDP_COMPUTE_FORCES) && force_dtype != TDP_F64 && force_dtype != TDP_F32)
+            throw TdpError{TDP_ERR_INVALID_ARGUMENT, "unknown force dtype"};
+        solve_at(h, positions, pos_dtype, on_device);
+        if (h->precision == TDP_PRECISION_DOUBLE) run_energy<double>(h);
+        else run_energy<float>(h);
+        cudaStream_t st = h->stream;
+        size_t n3 = 3 * (size_t)h->n;
+        if (flags & TDP_COMPUTE_FORCES) {
+            if (on_device) {
+                launch_add_forces(h->d, forces_accum, force_dtype == TDP_F32, st);
+                h->launches++;
+            } else {
+                TDP_CUDA(cudaMemcpyAsync(h->h_forces, h->d.ftotal, n3 * sizeof(double), cudaMemcpyDeviceToHost, st));
+            }
+        }
+        if (energy) TDP_CUDA(cudaMemcpyAsync(h->h_scal + 1, h->d.energy, sizeof(double), cudaMemcpyDeviceToHost, st));
+        TDP_CUDA(cudaStreamSynchronize(st));
+        TDP_CUDA(cudaGetLastError());
+        if ((flags & TDP_COMPUTE_FORCES) && !on_device) {
+            if (force_dtype == TDP_F64) {
+                double* acc = static_cast<double*>(forces_accum);
+                for (size_t k = 0; k < n3; k++) acc[k] += h->h_forces[k];
+            } else {
+                float* acc = static_cast<float*>(forces_accum);
+                for (size_t k = 0; k < n3; k++) acc[k] += (float)h->h_forces[k];
+            }
+        }
+        if (energy) *energy = h->h_scal[1];
+        finish_timing(h);
+        if (h->status == TDP_STATUS_NON_FINITE)
+            throw TdpError{TDP_ERR_NON_FINITE, "the induced-dipole solve produced a non-finite residual"};
+        if ((flags & TDP_COMPUTE_REQUIRE_CONVERGENCE) && !h->converged)
+            throw TdpError{TDP_ERR_NOT_CONVERGED, "the induced dipoles did not converge"};
+    } catch (const TdpError& e) {
+        return fail(h, e);
+    }
+    return TDP_OK;
+}
+
+int tdp_get_dipoles(tdp_handle* h, int32_t which, const void* positions, int32_t pos_dtype, int32_t on_device,
+                    double* out) {
+    if (!h || !out) return TDP_ERR_INVALID_ARGUMENT;
+    try {
+        if (which < TDP_DIPOLES_INDUCED || which > TDP_DIPOLES_TOTAL)
+            throw TdpError{TDP_ERR_INVALID_ARGUMENT, "unknown dipole kind"};
+        if (h->n == 0) return TDP_OK;
+        solve_at(h, positions, pos_dtype, on_device);
+        size_t n3 = 3 * (size_t)h->n;
+        cudaStream_t st = h->stream;
+        if (which == TDP_DIPOLES_INDUCED) {
+            TDP_CUDA(cudaMemcpyAsync(out, h->d.mu, n3 * 8, cudaMemcpyDeviceToHost, st));
+            TDP_CUDA(cudaStreamSynchronize(st));
+        } else if (which == TDP_DIPOLES_LAB_PERMANENT) {
+            TDP_CUDA(cudaMemcpyAsync(out, h->d.lab, n3 * 8, cudaMemcpyDeviceToHost, st));
+            TDP_CUDA(cudaStreamSynchronize(st));
+        } else {
+            TDP_CUDA(cudaMemcpyAsync(out, h->d.lab, n3 * 8, cudaMemcpyDeviceToHost, st));
+            TDP_CUDA(cudaMemcpyAsync(h->h_forces, h->d.mu, n3 * 8, cudaMemcpyDeviceToHost, st));
+            TDP_CUDA(cudaStreamSynchronize(st));
+            for (size_t k = 0; k < n3; k++) out[k] += h->h_forces[k];
+        }
+    } catch (const TdpError& e) {
+        return fail(h, e);
+    }
+    return TDP_OK;
+}
+
+int tdp_get_potential(tdp_handle* h, const void* positions, int32_t pos_dtype, int32_t on_device, const double* grid,
+                      int32_t num_points, double* out) {
+    if (!h || (num_points > 0 && (!grid || !out)) || num_points < 0) return TDP_ERR_INVALID_ARGUMENT;
+    try {
+        if (num_points == 0) return TDP_OK;
+        if (h->n == 0) {
+            for (int g = 0; g < num_points; g++) out[g] = 0.0;
+            return TDP_OK;
+        }
+        solve_at(h, positions, pos_dtype, on_device);
+        cudaStream_t st = h->stream;
+        double* dgrid = nullptr;
+        double* dout = nullptr;
+        TDP_CUDA(cudaMallocAsync((void**)&dgrid, sizeof(double) * 3 * num_points, st));
+        TDP_CUDA(cudaMallocAsync((void**)&dout, sizeof(double) * num_points, st));
+        TDP_CUDA(cudaMemcpyAsync(dgrid, grid, sizeof(double) * 3 * num_points, cudaMemcpyHostToDevice, st));
+        launch_potential(h->d, dgrid, num_points, dout, st);
+        TDP_CUDA(cudaMemcpyAsync(out, dout, sizeof(double) * num_points, cudaMemcpyDeviceToHost, st));
+        TDP_CUDA(cudaFreeAsync(dgrid, st));
+        TDP_CUDA(cudaFreeAsync(dout, st));
+        TDP_CUDA(cudaStreamSynchronize(st));
+    } catch (const TdpError& e) {
+        return fail(h, e);
+    }
+    return TDP_OK;
+}
+
+int tdp_get_moments(tdp_handle* h, const void* positions, int32_t pos_dtype, int32_t on_device, const double* masses,
+                    double* out13) {
+    if (!h || !masses || !out13) return TDP_ERR_INVALID_ARGUMENT;
+    try {
+        if (h->n == 0) {
+            for (int k = 0; k < 13; k++) out13[k] = 0.0;
+            return TDP_OK;
+        }
+        solve_at(h, positions, pos_dtype, on_device);
+        cudaStream_t st = h->stream;
+        int nb = h->d.nvb;
+        double* dmass = nullptr;
+        double* scratch = nullptr;
+        double* dout = nullptr;
+        TDP_CUDA(cudaMallocAsync((void**)&dmass, sizeof(double) * h->n, st));
+        TDP_CUDA(cudaMallocAsync((void**)&scratch, sizeof(double) * 14 * nb, st));
+        TDP_CUDA(cudaMallocAsync((void**)&dout, sizeof(double) * 13, st));
+        TDP_CUDA(cudaMemcpyAsync(dmass, masses, sizeof(double) * h->n, cudaMemcpyHostToDevice, st));
+        launch_moments(h->d, dmass, scratch, dout, st);
+        TDP_CUDA(cudaMemcpyAsync(out13, dout, sizeof(double) * 13, cudaMemcpyDeviceToHost, st));
+        TDP_CUDA(cudaFreeAsync(dmass, st));
+        TDP_CUDA(cudaFreeAsync(scratch, st));
+        TDP_CUDA(cudaFreeAsync(dout, st));
+        TDP_CUDA(cudaStreamSynchronize(st));
+    } catch (const TdpError& e) {
+        return fail(h, e);
+    }
+    return TDP_OK;
+}
+
+int tdp_get_pme_parameters(const tdp_handle* h, double* alpha, int32_t* nx, int32_t* ny, int32_t* nz) {
+    if (!h || !alpha || !nx || !ny || !nz) return TDP_ERR_INVALID_ARGUMENT;
+    if (h->method != TDP_PME) {
+        const_cast<tdp_handle*>(h)->err = "getPMEParametersInContext: This Context is not using PME";
+        return TDP_ERR_NOT_PME;
+    }
+    if (h->pme_alpha != 0.0 && h->pme_grid[0] != 0) {
+        *alpha = h->pme_alpha;
+        *nx = h->pme_grid[0];
+        *ny = h->pme_grid[1];
+        *nz = h->pme_grid[2];
+        return TDP_OK;
+    }
+    // OpenMM's documented choice (NonbondedForceImpl::calcPMEParameters, used by
+    // ReferenceTholeDipoleKernels.cpp:143-152): alpha = sqrt(-ln(2 tol))/cutoff,
+    // n_k = ceil(2 alpha L_k / (3 tol^(1/5))), at least 6.
+    double tol = h->ewald_tol;
+    double a = std::sqrt(-std::log(2.0 * tol)) / h->cutoff;
+    int g[3];
+    for (int k = 0; k < 3; k++) {
+        g[k] = (int)std::ceil(2.0 * a * h->box[4 * k] / (3.0 * std::pow(tol, 0.2)));
+        g[k] = std::max(g[k], 6);
+    }
+    *alpha = a;
+    *nx = g[0];
+    *ny = g[1];
+    *nz = g[2];
+    return TDP_OK;
+}
+
+int tdp_solver_stats(const tdp_handle* h, int32_t* iterations, double* epsilon, int32_t* converged, int32_t* status) {
+    if (!h) return TDP_ERR_INVALID_ARGUMENT;
+    if (iterations) *iterations = h->iterations;
+    if (epsilon) *epsilon = h->epsilon;
+    if (converged) *converged = h->converged;
+    if (status) *status = h->status;
+    return TDP_OK;
+}
+
+int tdp_enable_timing(tdp_handle* h, int32_t enable) {
+    if (!h) return TDP_ERR_INVALID_ARGUMENT;
+    h->timing = enable != 0;
+    return TDP_OK;
+}
+
+int tdp_stage_times(const tdp_handle* h, double* out) {
+    if (!h || !out) return TDP_ERR_INVALID_ARGUMENT;
+    for (int k = 0; k < TDP_NUM_STAGE_TIMES; k++) out[k] = h->stage_ms[k];
+    return TDP_OK;
+}
+
+}  // extern "C"

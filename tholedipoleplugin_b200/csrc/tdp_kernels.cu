@@ -1,0 +1,1260 @@
+// tdp_kernels.cu -- sm_100a kernels of the TholeDipoleForce hot path in the
+// reference's semantics (aehogan/tholedipoleplugin,
+// platforms/reference/src/ReferenceTholeDipoleForce.cpp, "RTDF.cpp").
+//
+// Pair kernels (permanent field, mutual-field matvec, energy/force/torque)
+// are all-pairs and ordered: every thread owns one i-atom and visits every
+// j-atom, so no atomics and no j-side reductions are needed and the result is
+// deterministic.  A block owns kBlockI consecutive i-atoms (one 32-atom tile
+// per warp); blockIdx.y splits the j range, and each split writes its partial
+// sums to a scratch buffer that the consumer kernel reduces in a fixed order.
+// j-atoms are staged kJStage at a time in shared memory with 16-byte vector
+// loads and read back as warp-wide broadcasts.
+//
+// Mixed form: positions are FP32 offsets from FP64 32-atom tile centres, so
+// near pairs keep full FP32 precision wherever they are in the box; the
+// minimum image of a tile pair is taken in FP64 and per-pair folding is done
+// only where the tiles' extents reach half a box, with pairs within a few ulp
+// of the half-box boundary re-derived in FP64 so that the image chosen always
+// matches the FP64 reference.  Each thread's per-subtile sums are added to
+// FP64 accumulators.
+#include "tdp_kernels.cuh"
+#include "tdp_pairs.cuh"
+
+#include <math.h>
+
+namespace tdp {
+
+// ---------------------------------------------------------------------------
+// Packing: tile centres/extents and per-atom position records.
+// ---------------------------------------------------------------------------
+template <class R>
+__global__ void k_pack(int n, int n_tiles_pad, const double* __restrict__ pos, const double* __restrict__ charge,
+                       double4* __restrict__ tctr, double4* __restrict__ text,
+                       typename Vec4T<R>::type* __restrict__ posq, double2* __restrict__ yz) {
+    int warp = (blockIdx.x * blockDim.x + threadIdx.x) >> 5;
+    int lane = threadIdx.x & 31;
+    if (warp >= n_tiles_pad) return;
+    int i = warp * kTile + lane;
+    bool valid = i < n;
+    double x = valid ? pos[3 * i] : 0.0, y = valid ? pos[3 * i + 1] : 0.0, z = valid ? pos[3 * i + 2] : 0.0;
+    int cnt = __popc(__ballot_sync(0xffffffffu, valid));
+    double cx = warp_sum(x), cy = warp_sum(y), cz = warp_sum(z);
+    if (cnt > 0) {
+        cx /= cnt;
+        cy /= cnt;
+        cz /= cnt;
+    }
+    double ex = valid ? fabs(x - cx) : 0.0, ey = valid ? fabs(y - cy) : 0.0, ez = valid ? fabs(z - cz) : 0.0;
+    ex = warp_max(ex);
+    ey = warp_max(ey);
+    ez = warp_max(ez);
+    if (lane == 0) {
+        tctr[warp] = make_double4(cx, cy, cz, 0.0);
+        text[warp] = make_double4(ex, ey, ez, 0.0);
+    }
+    double q = valid ? charge[i] : 0.0;
+    typename Vec4T<R>::type p;
+    if (sizeof(R) == 4) {
+        p.x = (R)(valid ? x - cx : 0.0);
+        p.y = (R)(valid ? y - cy : 0.0);
+        p.z = (R)(valid ? z - cz : 0.0);
+    } else {
+        p.x = (R)(valid ? x : cx);
+        p.y = (R)(valid ? y : cy);
+        p.z = (R)(valid ? z : cz);
+    }
+    p.w = (R)q;
+    posq[i] = p;
+    yz[i] = make_double2(y, z);
+}
+
+// ---------------------------------------------------------------------------
+// Local -> lab frame of the permanent dipoles: checkChiral (RTDF.cpp:432-467)
+// then applyRotationMatrixToParticle (RTDF.cpp:477-571), FP64.
+// ---------------------------------------------------------------------------
+struct d3 {
+    double x, y, z;
+};
+__device__ __forceinline__ d3 ld3(const double* p) { return {p[0], p[1], p[2]}; }
+__device__ __forceinline__ d3 operator+(d3 a, d3 b) { return {a.x + b.x, a.y + b.y, a.z + b.z}; }
+__device__ __forceinline__ d3 operator-(d3 a, d3 b) { return {a.x - b.x, a.y - b.y, a.z - b.z}; }
+__device__ __forceinline__ d3 operator*(d3 a, double s) { return {a.x * s, a.y * s, a.z * s}; }
+__device__ __forceinline__ double dot(d3 a, d3 b) { return a.x * b.x + a.y * b.y + a.z * b.z; }
+__device__ __forceinline__ d3 cross(d3 a, d3 b) {
+    return {a.y * b.z - a.z * b.y, a.z * b.x - a.x * b.z, a.x * b.y - a.y * b.x};
+}
+__device__ __forceinline__ double normalize(d3& a) {
+    double nrm = sqrt(dot(a, a));
+    if (nrm > 0.0) a = a * (1.0 / nrm);
+    return nrm;
+}
+
+template <class R>
+__global__ void k_rotate(int n, const double* __restrict__ pos, const double* __restrict__ dip_mol,
+                         const int4* __restrict__ axis, const double* __restrict__ thole, double* __restrict__ lab,
+                         typename Vec4T<R>::type* __restrict__ dipt) {
+    int i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= n) return;
+    d3 d = ld3(dip_mol + 3 * i);
+    int4 ax = axis[i];  // type, z, x, y
+    d3 pi = ld3(pos + 3 * i);
+    if (ax.w > -1 && ax.x == 0 /* ZThenX */) {
+        d3 py = ld3(pos + 3 * ax.w);
+        d3 ad = pi - py, bd = ld3(pos + 3 * ax.y) - py, cd = ld3(pos + 3 * ax.z) - py;
+        if (dot(cross(bd, cd), ad) < 0.0) d.y *= -1.0;
+    }
+    if (ax.y >= 0 && ax.y != i) {
+        d3 vz = ld3(pos + 3 * ax.y) - pi;
+        normalize(vz);
+        d3 vx, vy;
+        if (ax.x == 4 /* ZOnly */) {
+            vx = fabs(vz.x) < 0.866 ? d3{1.0, 0.0, 0.0} : d3{0.0, 1.0, 0.0};
+        } else {
+            vx = ld3(pos + 3 * ax.z) - pi;
+            if (ax.x == 1) {  // Bisector
+                normalize(vx);
+                vz = vz + vx;
+                normalize(vz);
+            } else if (ax.x == 2) {  // ZBisect
+                normalize(vx);
+                vy = ld3(pos + 3 * ax.w) - pi;
+                normalize(vy);
+                vx = vx + vy;
+                normalize(vx);
+            } else if (ax.x == 3) {  // ThreeFold
+                normalize(vx);
+                vy = ld3(pos + 3 * ax.w) - pi;
+                normalize(vy);
+                vz = vz + (vx + vy);
+                normalize(vz);
+            }
+        }
+        double dt = dot(vz, vx);
+        vx = vx - vz * dt;
+        normalize(vx);
+        vy = cross(vz, vx);
+        d3 o;
+        o.x = 0.0 + d.x * vx.x + d.y * vy.x + d.z * vz.x;
+        o.y = 0.0 + d.x * vx.y + d.y * vy.y + d.z * vz.y;
+        o.z = 0.0 + d.x * vx.z + d.y * vy.z + d.z * vz.z;
+        d = o;
+    }
+    lab[3 * i] = d.x;
+    lab[3 * i + 1] = d.y;
+    lab[3 * i + 2] = d.z;
+    typename Vec4T<R>::type v;
+    v.x = (R)d.x;
+    v.y = (R)d.y;
+    v.z = (R)d.z;
+    v.w = (R)thole[i];
+    dipt[i] = v;
+}
+
+// ---------------------------------------------------------------------------
+// Pair-loop machinery.
+// ---------------------------------------------------------------------------
+// Per-(warp, j-subtile) geometry: displacement of the j tile centre from the
+// i tile centre (FP64, minimum image), and which dimensions need per-pair
+// folding.
+struct TileGeom {
+    double dcx, dcy, dcz;
+    bool fold;
+};
+
+__device__ __forceinline__ TileGeom tile_geom(const PairParams& P, double4 cA, double4 eA, double4 cB, double4 eB) {
+    TileGeom g;
+    g.dcx = cB.x - cA.x;
+    g.dcy = cB.y - cA.y;
+    g.dcz = cB.z - cA.z;
+    g.fold = false;
+    if (P.periodic) {
+        g.dcx = fold_d(g.dcx, P.box[0], P.inv_box[0]);
+        g.dcy = fold_d(g.dcy, P.box[1], P.inv_box[1]);
+        g.dcz = fold_d(g.dcz, P.box[2], P.inv_box[2]);
+        g.fold = fabs(g.dcx) + eA.x + eB.x >= P.half_box_tol[0] || fabs(g.dcy) + eA.y + eB.y >= P.half_box_tol[1] ||
+                 fabs(g.dcz) + eA.z + eB.z >= P.half_box_tol[2];
+    }
+    return g;
+}
+
+// Exact FP64 minimum-image displacement p_j - p_i (the reference's own
+// arithmetic), used for exceptions and for FP32 pairs near the half-box.
+__device__ __forceinline__ d3 exact_delta(const PairParams& P, const double* __restrict__ pos, int i, int j) {
+    d3 d = ld3(pos + 3 * j) - ld3(pos + 3 * i);
+    if (P.periodic) {
+        d.x = fold_d(d.x, P.box[0], P.inv_box[0]);
+        d.y = fold_d(d.y, P.box[1], P.inv_box[1]);
+        d.z = fold_d(d.z, P.box[2], P.inv_box[2]);
+    }
+    return d;
+}
+
+// Displacement of j from i inside a j-subtile loop.  For R = float the i offset
+// has already been shifted by the tile displacement; for R = double positions
+// are absolute.
+template <class R, bool FOLD>
+__device__ __forceinline__ void pair_delta(const PairParams& P, const double* __restrict__ pos, int i, int j, R pjx,
+                                           R pjy, R pjz, R oix, R oiy, R oiz, R& dx, R& dy, R& dz) {
+    dx = pjx - oix;
+    dy = pjy - oiy;
+    dz = pjz - oiz;
+    if (FOLD) {
+        if (sizeof(R) == 4) {
+            dx = (R)fold_f((float)dx, (float)P.box[0], (float)P.inv_box[0]);
+            dy = (R)fold_f((float)dy, (float)P.box[1], (float)P.inv_box[1]);
+            dz = (R)fold_f((float)dz, (float)P.box[2], (float)P.inv_box[2]);
+            if ((fabs(dx) > (R)P.half_box_tol[0] || fabs(dy) > (R)P.half_box_tol[1] ||
+                 fabs(dz) > (R)P.half_box_tol[2]) && i < P.n && j < P.n) {
+                d3 e = exact_delta(P, pos, i, j);
+                dx = (R)e.x;
+                dy = (R)e.y;
+                dz = (R)e.z;
+            }
+        } else {
+            dx = (R)fold_d((double)dx, P.box[0], P.inv_box[0]);
+            dy = (R)fold_d((double)dy, P.box[1], P.inv_box[1]);
+            dz = (R)fold_d((double)dz, P.box[2], P.inv_box[2]);
+        }
+    }
+}
+
+template <class R>
+__device__ __forceinline__ R masked_r2(R r2, bool dirty, int i, int j, int n) {
+    if (dirty && (j == i || j >= n)) return (R)INFINITY;
+    return r2;
+}
+
+// ---------------------------------------------------------------------------
+// Field kernels: KIND 0 = permanent field (j records: posq + lab dipole/thole),
+// KIND 1 = mutual-field matvec T*v (j records: posq + v/thole).
+// ---------------------------------------------------------------------------
+template <class R, int KIND, bool FOLD, bool DIRTY>
+__device__ __forceinline__ void field_subtile(const PairParams& P, const double* __restrict__ pos,
+                                              const typename Vec4T<R>::type* __restrict__ sp,
+                                              const typename Vec4T<R>::type* __restrict__ sv, int i, int jbase,
+                                              R oix, R oiy, R oiz, R ti, R damp_r2, R& fx, R& fy, R& fz) {
+#pragma unroll 4
+    for (int jj = 0; jj < kTile; jj++) {
+        typename Vec4T<R>::type pj = sp[jj];
+        typename Vec4T<R>::type vj = sv[jj];
+        int j = jbase + jj;
+        R dx, dy, dz;
+        pair_delta<R, FOLD>(P, pos, i, j, pj.x, pj.y, pj.z, oix, oiy, oiz, dx, dy, dz);
+        R r2 = dx * dx + dy * dy + dz * dz;
+        r2 = masked_r2<R>(r2, DIRTY, i, j, P.n);
+        if (KIND == 0)
+            pair_fixed<R>(dx, dy, dz, r2, pj.w, vj.x, vj.y, vj.z, ti, vj.w, damp_r2, fx, fy, fz);
+        else
+            pair_matvec<R>(dx, dy, dz, r2, vj.x, vj.y, vj.z, ti, vj.w, damp_r2, fx, fy, fz);
+    }
+}
+
+template <class R, int KIND>
+__global__ void __launch_bounds__(kBlockI) k_field(PairParams P, const typename Vec4T<R>::type* __restrict__ posq,
+                                                   const typename Vec4T<R>::type* __restrict__ jvec,
+                                                   const double4* __restrict__ tctr,
+                                                   const double4* __restrict__ text,
+                                                   const double* __restrict__ pos, const int* __restrict__ exc_off,
+                                                   const int* __restrict__ exc_j, const double* __restrict__ exc_scale,
+                                                   int n_pad, double* __restrict__ partial) {
+    typedef typename Vec4T<R>::type V4;
+    __shared__ V4 s_pos[kJStage];
+    __shared__ V4 s_vec[kJStage];
+    __shared__ double4 s_ctr[kJStage / kTile];
+    __shared__ double4 s_ext[kJStage / kTile];
+
+    const int i = blockIdx.x * kBlockI + threadIdx.x;
+    const int A = i >> 5;
+    const V4 pi = posq[i];
+    const R ti = jvec[i].w;
+    const double4 cA = tctr[A];
+    const double4 eA = text[A];
+    const R damp_r2 = (R)P.damp_r2;
+    double ax = 0.0, ay = 0.0, az = 0.0;
+
+    const int jtot = P.n_tiles * kTile;
+    const int jbeg = blockIdx.y * P.j_chunk;
+    const int jend = min(jbeg + P.j_chunk, jtot);
+    for (int j0 = jbeg; j0 < jend; j0 += kJStage) {
+        __syncthreads();
+        for (int k = threadIdx.x; k < kJStage; k += kBlockI) {
+            s_pos[k] = posq[j0 + k];
+            s_vec[k] = jvec[j0 + k];
+        }
+        if (threadIdx.x < kJStage / kTile) {
+            s_ctr[threadIdx.x] = tctr[(j0 >> 5) + threadIdx.x];
+            s_ext[threadIdx.x] = text[(j0 >> 5) + threadIdx.x];
+        }
+        __syncthreads();
+        for (int sub = 0; sub < kJStage / kTile; sub++) {
+            const int B = (j0 >> 5) + sub;
+            if (B >= P.n_tiles) break;
+            TileGeom g = tile_geom(P, cA, eA, s_ctr[sub], s_ext[sub]);
+            R oix, oiy, oiz;
+            if (sizeof(R) == 4) {
+                oix = pi.x - (R)g.dcx;
+                oiy = pi.y - (R)g.dcy;
+                oiz = pi.z - (R)g.dcz;
+            } else {
+                // Absolute positions: shift i by the whole-box image that the
+                // tile-level minimum image chose, (cB - cA) - dc = L*k.
+                oix = pi.x + ((s_ctr[sub].x - cA.x) - g.dcx);
+                oiy = pi.y + ((s_ctr[sub].y - cA.y) - g.dcy);
+                oiz = pi.z + ((s_ctr[sub].z - cA.z) - g.dcz);
+            }
+            const bool dirty = (B == A) || (B == P.n_tiles - 1 && (P.n & (kTile - 1)));
+            R fx = 0, fy = 0, fz = 0;
+            const V4* sp = s_pos + sub * kTile;
+            const V4* sv = s_vec + sub * kTile;
+            const int jbase = B * kTile;
+            if (g.fold) {
+                if (dirty)
+                    field_subtile<R, KIND, true, true>(P, pos, sp, sv, i, jbase, oix, oiy, oiz, ti, damp_r2, fx, fy, fz);
+                else
+                    field_subtile<R, KIND, true, false>(P, pos, sp, sv, i, jbase, oix, oiy, oiz, ti, damp_r2, fx, fy, fz);
+            } else {
+                if (dirty)
+                    field_subtile<R, KIND, false, true>(P, pos, sp, sv, i, jbase, oix, oiy, oiz, ti, damp_r2, fx, fy, fz);
+                else
+                    field_subtile<R, KIND, false, false>(P, pos, sp, sv, i, jbase, oix, oiy, oiz, ti, damp_r2, fx, fy,
+                                                         fz);
+            }
+            ax += (double)fx;
+            ay += (double)fy;
+            az += (double)fz;
+        }
+    }
+    // Covalent scale corrections: the main loop used scale 1 for every pair;
+    // each listed pair adds (scale - 1) times its term (the terms are linear in
+    // the scale).
+    if (blockIdx.y == 0 && i < P.n) {
+        for (int e = exc_off[i]; e < exc_off[i + 1]; e++) {
+            double s = exc_scale[e];
+            if (s == 0.0) continue;
+            int j = exc_j[e];
+            d3 d = exact_delta(P, pos, i, j);
+            R dx = (R)d.x, dy = (R)d.y, dz = (R)d.z;
+            R r2 = dx * dx + dy * dy + dz * dz;
+            V4 vj = jvec[j];
+            R fx = 0, fy = 0, fz = 0;
+            if (KIND == 0)
+                pair_fixed<R>(dx, dy, dz, r2, posq[j].w, vj.x, vj.y, vj.z, ti, vj.w, damp_r2, fx, fy, fz);
+            else
+                pair_matvec<R>(dx, dy, dz, r2, vj.x, vj.y, vj.z, ti, vj.w, damp_r2, fx, fy, fz);
+            ax += s * (double)fx;
+            ay += s * (double)fy;
+            az += s * (double)fz;
+        }
+    }
+    const size_t base = (size_t)blockIdx.y * 3 * n_pad;
+    partial[base + i] = ax;
+    partial[base + n_pad + i] = ay;
+    partial[base + 2 * (size_t)n_pad + i] = az;
+}
+
+// ---------------------------------------------------------------------------
+// Energy / force / torque kernel.
+// ---------------------------------------------------------------------------
+template <class R, bool FOLD, bool DIRTY>
+__device__ __forceinline__ void energy_subtile(const PairParams& P, const double* __restrict__ pos,
+                                               const typename Vec4T<R>::type* __restrict__ sp,
+                                               const typename Vec4T<R>::type* __restrict__ sd,
+                                               const typename Vec4T<R>::type* __restrict__ su,
+                                               const double2* __restrict__ syz, int i, int jbase, R oix, R oiy, R oiz,
+                                               double yi, double zi, const EAtom<R>& me, R damp_r2, R rv4p, R rv4f,
+                                               bool upper, R& fx, R& fy, R& fz, R& tx, R& ty, R& tz, R& en) {
+#pragma unroll 1
+    for (int jj = 0; jj < kTile; jj++) {
+        typename Vec4T<R>::type pj = sp[jj], dj = sd[jj], uj = su[jj];
+        double2 yzj = syz[jj];
+        int j = jbase + jj;
+        R dx, dy, dz;
+        pair_delta<R, FOLD>(P, pos, i, j, pj.x, pj.y, pj.z, oix, oiy, oiz, dx, dy, dz);
+        R r2 = dx * dx + dy * dy + dz * dz;
+        r2 = masked_r2<R>(r2, DIRTY, i, j, P.n);
+        bool yzd = (yi != yzj.x) || (zi != yzj.y);
+        EAtom<R> other;
+        other.q = pj.w;
+        other.mx = dj.x;
+        other.my = dj.y;
+        other.mz = dj.z;
+        other.t = dj.w;
+        other.ux = uj.x;
+        other.uy = uj.y;
+        other.uz = uj.z;
+        // The pair is evaluated in the reference's orientation: I = lower index.
+        if (!upper && (!DIRTY || j > i))
+            pair_energy<R, true>(dx, dy, dz, r2, yzd, me, other, R(1), R(1), damp_r2, rv4p, rv4f, P.mutual, fx, fy,
+                                 fz, tx, ty, tz, en);
+        else
+            pair_energy<R, false>(-dx, -dy, -dz, r2, yzd, other, me, R(1), R(1), damp_r2, rv4p, rv4f, P.mutual, fx, fy,
+                                  fz, tx, ty, tz, en);
+    }
+}
+
+template <class R>
+__global__ void __launch_bounds__(kBlockI) k_energy(PairParams P, const typename Vec4T<R>::type* __restrict__ posq,
+                                                    const typename Vec4T<R>::type* __restrict__ dipt,
+                                                    const typename Vec4T<R>::type* __restrict__ indv,
+                                                    const double2* __restrict__ yz, const double4* __restrict__ tctr,
+                                                    const double4* __restrict__ text, const double* __restrict__ pos,
+                                                    const int* __restrict__ exc_off, const int* __restrict__ exc_j,
+                                                    const double* __restrict__ exc_m, const double* __restrict__ exc_s,
+                                                    int n_pad, double* __restrict__ partial,
+                                                    double* __restrict__ energy_partial) {
+    typedef typename Vec4T<R>::type V4;
+    __shared__ V4 s_pos[kJStage];
+    __shared__ V4 s_dip[kJStage];
+    __shared__ V4 s_ind[kJStage];
+    __shared__ double2 s_yz[kJStage];
+    __shared__ double4 s_ctr[kJStage / kTile];
+    __shared__ double4 s_ext[kJStage / kTile];
+    __shared__ double s_red[kBlockI / 32];
+
+    const int i = blockIdx.x * kBlockI + threadIdx.x;
+    const int A = i >> 5;
+    const V4 pi = posq[i];
+    const V4 di = dipt[i];
+    const V4 ui = indv[i];
+    const double2 yzi = yz[i];
+    EAtom<R> me;
+    me.q = pi.w;
+    me.mx = di.x;
+    me.my = di.y;
+    me.mz = di.z;
+    me.t = di.w;
+    me.ux = ui.x;
+    me.uy = ui.y;
+    me.uz = ui.z;
+    const double4 cA = tctr[A];
+    const double4 eA = text[A];
+    const R damp_r2 = (R)P.damp_r2;
+    const R rv4p = (R)P.rinv4_power, rv4f = (R)P.rinv4_fill;
+    double afx = 0, afy = 0, afz = 0, atx = 0, aty = 0, atz = 0, aen = 0;
+
+    const int jtot = P.n_tiles * kTile;
+    const int jbeg = blockIdx.y * P.j_chunk;
+    const int jend = min(jbeg + P.j_chunk, jtot);
+    for (int j0 = jbeg; j0 < jend; j0 += kJStage) {
+        __syncthreads();
+        for (int k = threadIdx.x; k < kJStage; k += kBlockI) {
+            s_pos[k] = posq[j0 + k];
+            s_dip[k] = dipt[j0 + k];
+            s_ind[k] = indv[j0 + k];
+            s_yz[k] = yz[j0 + k];
+        }
+        if (threadIdx.x < kJStage / kTile) {
+            s_ctr[threadIdx.x] = tctr[(j0 >> 5) + threadIdx.x];
+            s_ext[threadIdx.x] = text[(j0 >> 5) + threadIdx.x];
+        }
+        __syncthreads();
+        for (int sub = 0; sub < kJStage / kTile; sub++) {
+            const int B = (j0 >> 5) + sub;
+            if (B >= P.n_tiles) break;
+            TileGeom g = tile_geom(P, cA, eA, s_ctr[sub], s_ext[sub]);
+            R oix, oiy, oiz;
+            if (sizeof(R) == 4) {
+                oix = pi.x - (R)g.dcx;
+                oiy = pi.y - (R)g.dcy;
+                oiz = pi.z - (R)g.dcz;
+            } else {
+                // Absolute positions: shift i by the whole-box image that the
+                // tile-level minimum image chose, (cB - cA) - dc = L*k.
+                oix = pi.x + ((s_ctr[sub].x - cA.x) - g.dcx);
+                oiy = pi.y + ((s_ctr[sub].y - cA.y) - g.dcy);
+                oiz = pi.z + ((s_ctr[sub].z - cA.z) - g.dcz);
+            }
+            const bool dirty = (B == A) || (B == P.n_tiles - 1 && (P.n & (kTile - 1)));
+            // Outside the diagonal tile every j of the subtile is on one side of i.
+            const bool upper = !dirty && (B < A);
+            R fx = 0, fy = 0, fz = 0, tx = 0, ty = 0, tz = 0, en = 0;
+            const int o = sub * kTile;
+            const int jbase = B * kTile;
+            if (g.fold) {
+                if (dirty)
+                    energy_subtile<R, true, true>(P, pos, s_pos + o, s_dip + o, s_ind + o, s_yz + o, i, jbase, oix, oiy,
+                                                  oiz, yzi.x, yzi.y, me, damp_r2, rv4p, rv4f, upper, fx, fy, fz, tx,
+                                                  ty, tz, en);
+                else
+                    energy_subtile<R, true, false>(P, pos, s_pos + o, s_dip + o, s_ind + o, s_yz + o, i, jbase, oix,
+                                                   oiy, oiz, yzi.x, yzi.y, me, damp_r2, rv4p, rv4f, upper, fx, fy, fz,
+                                                   tx, ty, tz, en);
+            } else {
+                if (dirty)
+                    energy_subtile<R, false, true>(P, pos, s_pos + o, s_dip + o, s_ind + o, s_yz + o, i, jbase, oix,
+                                                   oiy, oiz, yzi.x, yzi.y, me, damp_r2, rv4p, rv4f, upper, fx, fy, fz,
+                                                   tx, ty, tz, en);
+                else
+                    energy_subtile<R, false, false>(P, pos, s_pos + o, s_dip + o, s_ind + o, s_yz + o, i, jbase, oix,
+                                                    oiy, oiz, yzi.x, yzi.y, me, damp_r2, rv4p, rv4f, upper, fx, fy, fz,
+                                                    tx, ty, tz, en);
+            }
+            afx += (double)fx;
+            afy += (double)fy;
+            afz += (double)fz;
+            atx += (double)tx;
+            aty += (double)ty;
+            atz += (double)tz;
+            aen += (double)en;
+        }
+    }
+    if (blockIdx.y == 0 && i < P.n) {
+        for (int e = exc_off[i]; e < exc_off[i + 1]; e++) {
+            int j = exc_j[e];
+            R mS = (R)exc_m[e], iS = (R)exc_s[e];
+            d3 d = exact_delta(P, pos, i, j);
+            R dx = (R)d.x, dy = (R)d.y, dz = (R)d.z;
+            R r2 = dx * dx + dy * dy + dz * dz;
+            V4 pj = posq[j], dj = dipt[j], uj = indv[j];
+            double2 yzj = yz[j];
+            bool yzd = (yzi.x != yzj.x) || (yzi.y != yzj.y);
+            EAtom<R> other;
+            other.q = pj.w;
+            other.mx = dj.x;
+            other.my = dj.y;
+            other.mz = dj.z;
+            other.t = dj.w;
+            other.ux = uj.x;
+            other.uy = uj.y;
+            other.uz = uj.z;
+            R fx = 0, fy = 0, fz = 0, tx = 0, ty = 0, tz = 0, en = 0;
+            if (j > i)
+                pair_energy<R, true>(dx, dy, dz, r2, yzd, me, other, mS, iS, damp_r2, rv4p, rv4f, P.mutual, fx, fy, fz,
+                                     tx, ty, tz, en);
+            else
+                pair_energy<R, false>(-dx, -dy, -dz, r2, yzd, other, me, mS, iS, damp_r2, rv4p, rv4f, P.mutual, fx, fy,
+                                      fz, tx, ty, tz, en);
+            afx += (double)fx;
+            afy += (double)fy;
+            afz += (double)fz;
+            atx += (double)tx;
+            aty += (double)ty;
+            atz += (double)tz;
+            aen += (double)en;
+        }
+    }
+    const size_t base = (size_t)blockIdx.y * 6 * n_pad;
+    partial[base + i] = afx;
+    partial[base + n_pad + i] = afy;
+    partial[base + 2 * (size_t)n_pad + i] = afz;
+    partial[base + 3 * (size_t)n_pad + i] = atx;
+    partial[base + 4 * (size_t)n_pad + i] = aty;
+    partial[base + 5 * (size_t)n_pad + i] = atz;
+    // Block energy (threads beyond n contribute nothing).
+    double ev = (i < P.n) ? aen : 0.0;
+    ev = warp_sum(ev);
+    if ((threadIdx.x & 31) == 0) s_red[threadIdx.x >> 5] = ev;
+    __syncthreads();
+    if (threadIdx.x == 0) {
+        double s = 0.0;
+        for (int w = 0; w < kBlockI / 32; w++) s += s_red[w];
+        energy_partial[(size_t)blockIdx.y * gridDim.x + blockIdx.x] = s;
+    }
+}
+
+// ---------------------------------------------------------------------------
+// Torque -> force, gather form of mapTorqueToForceForParticle
+// (RTDF.cpp:915-1090): atom a sums, over every frame it belongs to, the force
+// its role (I, U=Z, V=X, W=Y) receives.  role: 0 I, 1 U, 2 V, 3 W.
+// ---------------------------------------------------------------------------
+__device__ d3 torque_role_force(const double* __restrict__ pos, int4 ax, int i, int role, d3 T) {
+    const int t = ax.x, iz = ax.y, ix = ax.z, iy = ax.w;
+    d3 zero = {0.0, 0.0, 0.0};
+    if (t == 5) return zero;
+    d3 pi = ld3(pos + 3 * i);
+    d3 U = ld3(pos + 3 * iz) - pi;
+    double normU = normalize(U);
+    d3 V;
+    double normV;
+    if (ix >= 0) {
+        V = ld3(pos + 3 * ix) - pi;
+        normV = normalize(V);
+    } else {  // ZOnly without an X atom (undefined in the reference): the rotation's fixed axis
+        V = fabs(U.x) < 0.866 ? d3{1.0, 0.0, 0.0} : d3{0.0, 1.0, 0.0};
+        normV = 1.0;
+    }
+    d3 W;
+    if (iy > -1 && (t == 2 || t == 3)) W = ld3(pos + 3 * iy) - pi;
+    else W = cross(U, V);
+    double normW = normalize(W);
+    d3 UV = cross(V, U), UW = cross(W, U), VW = cross(W, V);
+    normalize(UV);
+    normalize(UW);
+    normalize(VW);
+    double cosUV = dot(U, V), sinUV = sqrt(1.0 - cosUV * cosUV);
+    double cosUW = dot(U, W), sinUW = sqrt(1.0 - cosUW * cosUW);
+    double cosVW = dot(V, W), sinVW = sqrt(1.0 - cosVW * cosVW);
+    double dphi0 = dot(U, T) * -1.0, dphi1 = dot(V, T) * -1.0, dphi2 = dot(W, T) * -1.0;
+    if (t == 0 || t == 1) {
+        double f1 = dphi1 / (normU * sinUV);
+        double f2 = dphi2 / normU;
+        double f3 = -dphi0 / (normV * sinUV);
+        double f4 = 0.0;
+        if (t == 1) {
+            f2 *= 0.5;
+            f4 = 0.5 * dphi2 / normV;
+        }
+        d3 fU = {UV.x * f1 + f2 * UW.x, UV.y * f1 + f2 * UW.y, UV.z * f1 + f2 * UW.z};
+        d3 fV = {UV.x * f3 + f4 * VW.x, UV.y * f3 + f4 * VW.y, UV.z * f3 + f4 * VW.z};
+        if (role == 0) return fU + fV;
+        if (role == 1) return fU * -1.0;
+        if (role == 2) return fV * -1.0;
+        return zero;
+    }
+    if (t == 2) {
+        d3 Rv = V + W;
+        d3 S = cross(U, Rv);
+        normalize(Rv);
+        normalize(S);
+        d3 UR = cross(Rv, U), US = cross(S, U);
+        normalize(UR);
+        normalize(US);
+        double cosUR = dot(U, Rv), sinUR = sqrt(1.0 - cosUR * cosUR);
+        double cosVS = dot(V, S), sinVS = sqrt(1.0 - cosVS * cosVS);
+        double cosWS = dot(W, S), sinWS = sqrt(1.0 - cosWS * cosWS);
+        d3 t1 = V - S * cosVS, t2 = W - S * cosWS;
+        normalize(t1);
+        normalize(t2);
+        double ut1cos = dot(U, t1), ut1sin = sqrt(1.0 - ut1cos * ut1cos);
+        double ut2cos = dot(U, t2), ut2sin = sqrt(1.0 - ut2cos * ut2cos);
+        double dphiR = dot(Rv, T) * (-1.0);
+        double dphiS = dot(S, T) * (-1.0);
+        double f1 = dphiR / (normU * sinUR);
+        double f2 = dphiS / normU;
+        double f3 = dphi0 / (normV * (ut1sin + ut2sin));
+        double f4 = dphi0 / (normW * (ut1sin + ut2sin));
+        d3 fU = UR * f1 + US * f2;
+        d3 fV = (S * sinVS - t1 * cosVS) * f3;
+        d3 fW = (S * sinWS - t2 * cosWS) * f4;
+        if (role == 0) return (fU + fV) + fW;
+        if (role == 1) return fU * -1.0;
+        if (role == 2) return fV * -1.0;
+        return fW * -1.0;
+    }
+    if (t == 3) {
+        double du[3], dv[3], dw[3];
+        double uwc[3] = {UW.x, UW.y, UW.z}, uvc[3] = {UV.x, UV.y, UV.z}, vwc[3] = {VW.x, VW.y, VW.z};
+        for (int c = 0; c < 3; c++) {
+            du[c] = uwc[c] * dphi2 / (normU * sinUW) + uvc[c] * dphi1 / (normU * sinUV) -
+                    uwc[c] * dphi0 / (normU * sinUW) - uvc[c] * dphi0 / (normU * sinUV);
+            dv[c] = vwc[c] * dphi2 / (normV * sinVW) - uvc[c] * dphi0 / (normV * sinUV) -
+                    vwc[c] * dphi1 / (normV * sinVW) + uvc[c] * dphi1 / (normV * sinUV);
+            dw[c] = -uwc[c] * dphi0 / (normW * sinUW) - vwc[c] * dphi1 / (normW * sinVW) +
+                    uwc[c] * dphi2 / (normW * sinUW) + vwc[c] * dphi2 / (normW * sinVW);
+            du[c] /= 3.0;
+            dv[c] /= 3.0;
+            dw[c] /= 3.0;
+        }
+        if (role == 0) return {du[0] + dv[0] + dw[0], du[1] + dv[1] + dw[1], du[2] + dv[2] + dw[2]};
+        if (role == 1) return {-du[0], -du[1], -du[2]};
+        if (role == 2) return {-dv[0], -dv[1], -dv[2]};
+        if (iy > -1) return {-dw[0], -dw[1], -dw[2]};
+        return zero;
+    }
+    if (t == 4) {
+        d3 du = {UV.x * dphi1 / (normU * sinUV) + UW.x * dphi2 / normU,
+                 UV.y * dphi1 / (normU * sinUV) + UW.y * dphi2 / normU,
+                 UV.z * dphi1 / (normU * sinUV) + UW.z * dphi2 / normU};
+        if (role == 0) return du;
+        if (role == 1) return du * -1.0;
+        return zero;
+    }
+    return zero;
+}
+
+// forces_out = pair forces + torque-mapped forces (FP64, deterministic).
+__global__ void k_torque_gather(int n, const double* __restrict__ pos, const int4* __restrict__ axis,
+                                const double* __restrict__ torque, const int* __restrict__ users_off,
+                                const int2* __restrict__ users, const double* __restrict__ fpair,
+                                double* __restrict__ fout) {
+    int a = blockIdx.x * blockDim.x + threadIdx.x;
+    if (a >= n) return;
+    d3 f = ld3(fpair + 3 * a);
+    for (int k = users_off[a]; k < users_off[a + 1]; k++) {
+        int2 u = users[k];  // (frame atom i, role)
+        d3 T = ld3(torque + 3 * u.x);
+        f = f + torque_role_force(pos, axis[u.x], u.x, u.y, T);
+    }
+    fout[3 * a] = f.x;
+    fout[3 * a + 1] = f.y;
+    fout[3 * a + 2] = f.z;
+}
+
+// ---------------------------------------------------------------------------
+// O(N) vector kernels of the solvers (FP64 vectors, deterministic reductions).
+// ---------------------------------------------------------------------------
+__device__ __forceinline__ d3 sum_partial3(const double* __restrict__ partial, int nsplit, int n_pad, int i) {
+    d3 t = {0.0, 0.0, 0.0};
+    for (int s = 0; s < nsplit; s++) {
+        size_t b = (size_t)s * 3 * n_pad;
+        t.x += partial[b + i];
+        t.y += partial[b + n_pad + i];
+        t.z += partial[b + 2 * (size_t)n_pad + i];
+    }
+    return t;
+}
+
+template <class R>
+__device__ __forceinline__ void store_vec(typename Vec4T<R>::type* v, int i, d3 a, double t) {
+    typename Vec4T<R>::type o;
+    o.x = (R)a.x;
+    o.y = (R)a.y;
+    o.z = (R)a.z;
+    o.w = (R)t;
+    v[i] = o;
+}
+
+// E = sum of permanent-field partials; mu = alpha*E (RTDF.cpp:743-746);
+// packs mu as the next matvec operand; CG start y = sqrt(alpha)*E.
+template <class R>
+__global__ void k_fixed_done(int n, int nsplit, int n_pad, const double* __restrict__ partial,
+                             const double* __restrict__ alpha, const double* __restrict__ salpha,
+                             const double* __restrict__ thole, double* __restrict__ E, double* __restrict__ mu,
+                             double* __restrict__ y, typename Vec4T<R>::type* __restrict__ vec) {
+    int i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= n) return;
+    d3 e = sum_partial3(partial, nsplit, n_pad, i);
+    E[3 * i] = e.x;
+    E[3 * i + 1] = e.y;
+    E[3 * i + 2] = e.z;
+    d3 m = e * alpha[i];
+    mu[3 * i] = m.x;
+    mu[3 * i + 1] = m.y;
+    mu[3 * i + 2] = m.z;
+    d3 yy = e * salpha[i];
+    y[3 * i] = yy.x;
+    y[3 * i + 1] = yy.y;
+    y[3 * i + 2] = yy.z;
+    store_vec<R>(vec, i, m, thole[i]);
+}
+
+// Warm start: y = mu / sqrt(alpha) (0 where alpha = 0); packs mu.
+template <class R>
+__global__ void k_warm_start(int n, const double* __restrict__ salpha, const double* __restrict__ thole,
+                             const double* __restrict__ mu, double* __restrict__ y,
+                             typename Vec4T<R>::type* __restrict__ vec) {
+    int i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= n) return;
+    d3 m = ld3(mu + 3 * i);
+    double s = salpha[i];
+    d3 yy = s > 0.0 ? m * (1.0 / s) : d3{0.0, 0.0, 0.0};
+    y[3 * i] = yy.x;
+    y[3 * i + 1] = yy.y;
+    y[3 * i + 2] = yy.z;
+    store_vec<R>(vec, i, m, thole[i]);
+}
+
+// True residual in y-space: r = sqrt(alpha)*(E + T mu) - y, with mu = sqrt(alpha)*y.
+// p = r, packs sqrt(alpha)*p; block partials of r.r and sum alpha|r|^2.
+template <class R>
+__global__ void k_cg_residual(int n, int nsplit, int n_pad, const double* __restrict__ partial,
+                              const double* __restrict__ E, const double* __restrict__ salpha,
+                              const double* __restrict__ thole, const double* __restrict__ y, double* __restrict__ r,
+                              double* __restrict__ p, typename Vec4T<R>::type* __restrict__ vec,
+                              double* __restrict__ rr_part, double* __restrict__ eps_part) {
+    __shared__ double red[40];
+    int i = blockIdx.x * blockDim.x + threadIdx.x;
+    double rr = 0.0, ee = 0.0;
+    if (i < n) {
+        d3 t = sum_partial3(partial, nsplit, n_pad, i);
+        double s = salpha[i];
+        d3 rv = (ld3(E + 3 * i) + t) * s - ld3(y + 3 * i);
+        r[3 * i] = rv.x;
+        r[3 * i + 1] = rv.y;
+        r[3 * i + 2] = rv.z;
+        p[3 * i] = rv.x;
+        p[3 * i + 1] = rv.y;
+        p[3 * i + 2] = rv.z;
+        store_vec<R>(vec, i, rv * s, thole[i]);
+        rr = dot(rv, rv);
+        ee = s * s * rr;
+    }
+    rr = block_sum(rr, red);
+    ee = block_sum(ee, red);
+    if (threadIdx.x == 0) {
+        rr_part[blockIdx.x] = rr;
+        eps_part[blockIdx.x] = ee;
+    }
+}
+
+// q = p - sqrt(alpha) * (T sqrt(alpha) p); block partials of p.q.
+__global__ void k_cg_q(int n, int nsplit, int n_pad, const double* __restrict__ partial,
+                       const double* __restrict__ salpha, const double* __restrict__ p, double* __restrict__ q,
+                       double* __restrict__ pq_part) {
+    __shared__ double red[40];
+    int i = blockIdx.x * blockDim.x + threadIdx.x;
+    double pq = 0.0;
+    if (i < n) {
+        d3 t = sum_partial3(partial, nsplit, n_pad, i);
+        d3 pv = ld3(p + 3 * i);
+        d3 qv = pv - t * salpha[i];
+        q[3 * i] = qv.x;
+        q[3 * i + 1] = qv.y;
+        q[3 * i + 2] = qv.z;
+        pq = dot(pv, qv);
+    }
+    pq = block_sum(pq, red);
+    if (threadIdx.x == 0) pq_part[blockIdx.x] = pq;
+}
+
+// a = rr/pq; y += a p; r -= a q; block partials of r.r and sum alpha|r|^2.
+__global__ void k_cg_update(int n, int nblk, const double* __restrict__ scal_rr, int slot,
+                            const double* __restrict__ pq_part, const double* __restrict__ salpha,
+                            const double* __restrict__ p, const double* __restrict__ q, double* __restrict__ y,
+                            double* __restrict__ r, double* __restrict__ rr_part, double* __restrict__ eps_part) {
+    __shared__ double red[40];
+    double pq = sum_partials(pq_part, nblk, red);
+    double a = scal_rr[slot] / pq;
+    int i = blockIdx.x * blockDim.x + threadIdx.x;
+    double rr = 0.0, ee = 0.0;
+    if (i < n) {
+        d3 yv = ld3(y + 3 * i) + ld3(p + 3 * i) * a;
+        d3 rv = ld3(r + 3 * i) - ld3(q + 3 * i) * a;
+        y[3 * i] = yv.x;
+        y[3 * i + 1] = yv.y;
+        y[3 * i + 2] = yv.z;
+        r[3 * i] = rv.x;
+        r[3 * i + 1] = rv.y;
+        r[3 * i + 2] = rv.z;
+        double s = salpha[i];
+        rr = dot(rv, rv);
+        ee = s * s * rr;
+    }
+    rr = block_sum(rr, red);
+    ee = block_sum(ee, red);
+    if (threadIdx.x == 0) {
+        rr_part[blockIdx.x] = rr;
+        eps_part[blockIdx.x] = ee;
+    }
+}
+
+// rr' = sum(rr_part) -> scal_rr[slot]; eps -> scal_eps[slot].  With prev >= 0
+// also p = r + (rr'/scal_rr[prev]) p and packs sqrt(alpha)*p for the next
+// matvec.
+template <class R>
+__global__ void k_cg_p(int n, int nblk, int prev, int slot, double* __restrict__ scal_rr,
+                       double* __restrict__ scal_eps, const double* __restrict__ rr_part,
+                       const double* __restrict__ eps_part, const double* __restrict__ salpha,
+                       const double* __restrict__ thole, const double* __restrict__ r, double* __restrict__ p,
+                       typename Vec4T<R>::type* __restrict__ vec) {
+    __shared__ double red[40];
+    double rr = sum_partials(rr_part, nblk, red);
+    double ee = sum_partials(eps_part, nblk, red);
+    if (blockIdx.x == 0 && threadIdx.x == 0) {
+        scal_rr[slot] = rr;
+        scal_eps[slot] = sqrt(ee / (double)n);
+    }
+    if (prev < 0) return;
+    double beta = rr / scal_rr[prev];
+    int i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i < n) {
+        d3 pv = ld3(r + 3 * i) + ld3(p + 3 * i) * beta;
+        p[3 * i] = pv.x;
+        p[3 * i + 1] = pv.y;
+        p[3 * i + 2] = pv.z;
+        store_vec<R>(vec, i, pv * salpha[i], thole[i]);
+    }
+}
+
+// mu = sqrt(alpha) y; packs mu.
+template <class R>
+__global__ void k_cg_mu(int n, const double* __restrict__ salpha, const double* __restrict__ thole,
+                        const double* __restrict__ y, double* __restrict__ mu,
+                        typename Vec4T<R>::type* __restrict__ vec) {
+    int i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= n) return;
+    d3 m = ld3(y + 3 * i) * salpha[i];
+    mu[3 * i] = m.x;
+    mu[3 * i + 1] = m.y;
+    mu[3 * i + 2] = m.z;
+    store_vec<R>(vec, i, m, thole[i]);
+}
+
+// One Jacobi sweep of convergeInducedDipolesByDIIS (RTDF.cpp:838-846):
+// mu' = alpha (E + T mu); block partials of |mu' - mu|^2; packs mu'.
+template <class R>
+__global__ void k_jacobi(int n, int nsplit, int n_pad, const double* __restrict__ partial,
+                         const double* __restrict__ E, const double* __restrict__ alpha,
+                         const double* __restrict__ thole, double* __restrict__ mu,
+                         typename Vec4T<R>::type* __restrict__ vec, double* __restrict__ eps_part) {
+    __shared__ double red[40];
+    int i = blockIdx.x * blockDim.x + threadIdx.x;
+    double ee = 0.0;
+    if (i < n) {
+        d3 t = sum_partial3(partial, nsplit, n_pad, i);
+        d3 nw = (ld3(E + 3 * i) + t) * alpha[i];
+        d3 dl = nw - ld3(mu + 3 * i);
+        ee = dot(dl, dl);
+        mu[3 * i] = nw.x;
+        mu[3 * i + 1] = nw.y;
+        mu[3 * i + 2] = nw.z;
+        store_vec<R>(vec, i, nw, thole[i]);
+    }
+    ee = block_sum(ee, red);
+    if (threadIdx.x == 0) eps_part[blockIdx.x] = ee;
+}
+
+// Extrapolation (RTDF.cpp:876-887): mu = alpha (E + T mu), stored as order k.
+template <class R>
+__global__ void k_extrap_step(int n, int nsplit, int n_pad, const double* __restrict__ partial,
+                              const double* __restrict__ E, const double* __restrict__ alpha,
+                              const double* __restrict__ thole, double* __restrict__ mu, double* __restrict__ hist_k,
+                              typename Vec4T<R>::type* __restrict__ vec) {
+    int i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= n) return;
+    d3 t = sum_partial3(partial, nsplit, n_pad, i);
+    d3 nw = (ld3(E + 3 * i) + t) * alpha[i];
+    mu[3 * i] = nw.x;
+    mu[3 * i + 1] = nw.y;
+    mu[3 * i + 2] = nw.z;
+    hist_k[3 * i] = nw.x;
+    hist_k[3 * i + 1] = nw.y;
+    hist_k[3 * i + 2] = nw.z;
+    store_vec<R>(vec, i, nw, thole[i]);
+}
+
+// mu = sum_k c_k mu_k (RTDF.cpp:890-895); packs mu.
+template <class R>
+__global__ void k_extrap_combine(int n, int korder, const double* __restrict__ coef, const double* __restrict__ hist,
+                                 const double* __restrict__ thole, double* __restrict__ mu,
+                                 typename Vec4T<R>::type* __restrict__ vec) {
+    int i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= n) return;
+    d3 m = {0.0, 0.0, 0.0};
+    for (int k = 0; k < korder; k++) m = m + ld3(hist + (size_t)k * 3 * n + 3 * i) * coef[k];
+    mu[3 * i] = m.x;
+    mu[3 * i + 1] = m.y;
+    mu[3 * i + 2] = m.z;
+    store_vec<R>(vec, i, m, thole[i]);
+}
+
+// Block partials of |alpha (E + T mu) - mu|^2 (RTDF.cpp:898-906).
+__global__ void k_step_eps(int n, int nsplit, int n_pad, const double* __restrict__ partial,
+                           const double* __restrict__ E, const double* __restrict__ alpha,
+                           const double* __restrict__ mu, double* __restrict__ eps_part) {
+    __shared__ double red[40];
+    int i = blockIdx.x * blockDim.x + threadIdx.x;
+    double ee = 0.0;
+    if (i < n) {
+        d3 t = sum_partial3(partial, nsplit, n_pad, i);
+        d3 dl = (ld3(E + 3 * i) + t) * alpha[i] - ld3(mu + 3 * i);
+        ee = dot(dl, dl);
+    }
+    ee = block_sum(ee, red);
+    if (threadIdx.x == 0) eps_part[blockIdx.x] = ee;
+}
+
+// scal[slot] = sqrt(sum(eps_part)/n).
+__global__ void k_eps_scalar(int n, int nblk, const double* __restrict__ eps_part, double* __restrict__ scal,
+                             int slot) {
+    __shared__ double red[40];
+    double ee = sum_partials(eps_part, nblk, red);
+    if (threadIdx.x == 0) scal[slot] = sqrt(ee / (double)n);
+}
+
+// Induced dipoles packed for the energy kernel.
+template <class R>
+__global__ void k_pack_ind(int n, const double* __restrict__ mu, typename Vec4T<R>::type* __restrict__ out) {
+    int i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= n) return;
+    store_vec<R>(out, i, ld3(mu + 3 * i), 0.0);
+}
+
+// Pair forces/torques and the total energy from the energy-kernel partials.
+__global__ void k_energy_done(int n, int nsplit, int n_pad, int n_eblk, const double* __restrict__ partial,
+                              const double* __restrict__ energy_partial, double* __restrict__ fpair,
+                              double* __restrict__ torque, double* __restrict__ energy_out) {
+    __shared__ double red[40];
+    if (blockIdx.x == 0) {
+        double e = sum_partials(energy_partial, n_eblk, red);
+        if (threadIdx.x == 0) *energy_out = e;
+    }
+    int i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= n) return;
+    double f[6] = {0, 0, 0, 0, 0, 0};
+    for (int s = 0; s < nsplit; s++) {
+        size_t b = (size_t)s * 6 * n_pad;
+        for (int c = 0; c < 6; c++) f[c] += partial[b + (size_t)c * n_pad + i];
+    }
+    fpair[3 * i] = f[0];
+    fpair[3 * i + 1] = f[1];
+    fpair[3 * i + 2] = f[2];
+    torque[3 * i] = f[3];
+    torque[3 * i + 1] = f[4];
+    torque[3 * i + 2] = f[5];
+}
+
+// accum += forces (device accumulator of either element type).
+__global__ void k_add_forces(int n3, const double* __restrict__ f, double* __restrict__ acc64,
+                             float* __restrict__ acc32) {
+    int k = blockIdx.x * blockDim.x + threadIdx.x;
+    if (k >= n3) return;
+    if (acc64) acc64[k] += f[k];
+    else acc32[k] += (float)f[k];
+}
+
+// Positions of either element type into the FP64 working copy.
+__global__ void k_positions_in(int n3, const void* __restrict__ src, int is_f32, double* __restrict__ dst) {
+    int k = blockIdx.x * blockDim.x + threadIdx.x;
+    if (k >= n3) return;
+    dst[k] = is_f32 ? (double)((const float*)src)[k] : ((const double*)src)[k];
+}
+
+// Electrostatic potential at grid points, calculateElectrostaticPotential-
+// ForParticleGridPoint (RTDF.cpp:1348-1372), FP64.
+__global__ void k_potential(int n, int ng, PairParams P, const double* __restrict__ pos,
+                            const double* __restrict__ charge, const double* __restrict__ lab,
+                            const double* __restrict__ mu, const double* __restrict__ grid, double* __restrict__ out) {
+    int g = blockIdx.x * blockDim.x + threadIdx.x;
+    if (g >= ng) return;
+    d3 gp = ld3(grid + 3 * g);
+    double pot = 0.0;
+    for (int i = 0; i < n; i++) {
+        d3 dr = ld3(pos + 3 * i) - gp;
+        if (P.periodic) {
+            dr.x = fold_d(dr.x, P.box[0], P.inv_box[0]);
+            dr.y = fold_d(dr.y, P.box[1], P.inv_box[1]);
+            dr.z = fold_d(dr.z, P.box[2], P.inv_box[2]);
+        }
+        double r = sqrt(dot(dr, dr));
+        double rr1 = 1.0 / r, rr2 = rr1 * rr1, rr3 = rr1 * rr2;
+        double p = charge[i] * rr1;
+        double scd = dot(ld3(lab + 3 * i), dr);
+        double scu = dot(ld3(mu + 3 * i), dr);
+        p -= (scd + scu) * rr3;
+        pot += p;
+    }
+    out[g] = pot;
+}
+
+// Block partial sums for the system multipole moments
+// (RTDF.cpp:1243-1283): 0 mass, 1-3 mass-weighted position.
+__global__ void k_com_partials(int n, const double* __restrict__ pos, const double* __restrict__ mass,
+                               double* __restrict__ part) {
+    __shared__ double red[40];
+    int i = blockIdx.x * blockDim.x + threadIdx.x;
+    double v[4] = {0, 0, 0, 0};
+    if (i < n) {
+        double m = mass[i];
+        v[0] = m;
+        v[1] = pos[3 * i] * m;
+        v[2] = pos[3 * i + 1] * m;
+        v[3] = pos[3 * i + 2] * m;
+    }
+    for (int c = 0; c < 4; c++) {
+        double s = block_sum(v[c], red);
+        if (threadIdx.x == 0) part[(size_t)c * gridDim.x + blockIdx.x] = s;
+    }
+}
+
+// 0 netchg, 1-3 dpl, 4 xx, 5 xy, 6 xz, 7 yy, 8 yz, 9 zz.
+__global__ void k_moment_partials(int n, int ncomblk, const double* __restrict__ com_part,
+                                  const double* __restrict__ pos, const double* __restrict__ charge,
+                                  const double* __restrict__ lab, const double* __restrict__ mu,
+                                  double* __restrict__ part) {
+    __shared__ double red[40];
+    double tm = sum_partials(com_part, ncomblk, red);
+    d3 com = {sum_partials(com_part + ncomblk, ncomblk, red), sum_partials(com_part + 2 * ncomblk, ncomblk, red),
+              sum_partials(com_part + 3 * ncomblk, ncomblk, red)};
+    if (tm > 0.0) com = com * (1.0 / tm);
+    int i = blockIdx.x * blockDim.x + threadIdx.x;
+    double v[10] = {0, 0, 0, 0, 0, 0, 0, 0, 0, 0};
+    if (i < n) {
+        double q = charge[i];
+        d3 p = ld3(pos + 3 * i) - com;
+        d3 nd = ld3(lab + 3 * i) + ld3(mu + 3 * i);
+        v[0] = q;
+        d3 dp = p * q + nd;
+        v[1] = dp.x;
+        v[2] = dp.y;
+        v[3] = dp.z;
+        v[4] = p.x * p.x * q + 2.0 * p.x * nd.x;
+        v[5] = p.x * p.y * q + p.x * nd.y + p.y * nd.x;
+        v[6] = p.x * p.z * q + p.x * nd.z + p.z * nd.x;
+        v[7] = p.y * p.y * q + 2.0 * p.y * nd.y;
+        v[8] = p.y * p.z * q + p.y * nd.z + p.z * nd.y;
+        v[9] = p.z * p.z * q + 2.0 * p.z * nd.z;
+    }
+    for (int c = 0; c < 10; c++) {
+        double s = block_sum(v[c], red);
+        if (threadIdx.x == 0) part[(size_t)c * gridDim.x + blockIdx.x] = s;
+    }
+}
+
+__global__ void k_moment_final(int nblk, const double* __restrict__ part, double* __restrict__ out13) {
+    __shared__ double red[40];
+    double s[10];
+    for (int c = 0; c < 10; c++) s[c] = sum_partials(part + (size_t)c * nblk, nblk, red);
+    if (threadIdx.x != 0) return;
+    double xx = s[4], xy = s[5], xz = s[6], yy = s[7], yz = s[8], zz = s[9];
+    double qave = (xx + yy + zz) / 3.0;
+    double o[13];
+    o[4] = 0.5 * (xx - qave);
+    o[5] = 0.5 * xy;
+    o[6] = 0.5 * xz;
+    o[8] = 0.5 * (yy - qave);
+    o[9] = 0.5 * yz;
+    o[12] = 0.5 * (zz - qave);
+    o[7] = o[5];
+    o[10] = o[6];
+    o[11] = o[9];
+    double debye = 4.80321;
+    o[0] = s[0];
+    o[1] = s[1] * (10.0 * debye);
+    o[2] = s[2] * (10.0 * debye);
+    o[3] = s[3] * (10.0 * debye);
+    debye *= 3.0;
+    for (int k = 4; k < 13; k++) o[k] *= 100.0 * debye;
+    for (int k = 0; k < 13; k++) out13[k] = o[k];
+}
+
+// ---------------------------------------------------------------------------
+// Launchers.
+// ---------------------------------------------------------------------------
+static inline int nblk(int n, int t) { return (n + t - 1) / t; }
+
+template <class R>
+void launch_pack(const Dev& d, cudaStream_t st) {
+    int threads = 128;
+    int warps = d.n_pad / kTile;
+    k_pack<R><<<nblk(warps * 32, threads), threads, 0, st>>>(
+        d.n, warps, d.pos, d.charge, d.tctr, d.text, (typename Vec4T<R>::type*)d.posq, d.yz);
+}
+
+template <class R>
+void launch_rotate(const Dev& d, cudaStream_t st) {
+    k_rotate<R><<<nblk(d.n, kVecThreads), kVecThreads, 0, st>>>(d.n, d.pos, d.dip_mol, d.axis, d.thole, d.lab,
+                                                                 (typename Vec4T<R>::type*)d.dipt);
+}
+
+template <class R>
+void launch_field(const Dev& d, int kind, cudaStream_t st) {
+    dim3 grid(d.n_pad / kBlockI, d.nsplit);
+    typedef typename Vec4T<R>::type V4;
+    if (kind == 0)
+        k_field<R, 0><<<grid, kBlockI, 0, st>>>(d.pp, (const V4*)d.posq, (const V4*)d.dipt, d.tctr, d.text, d.pos,
+                                               d.exc_off, d.exc_j, d.exc_m, d.n_pad, d.partial);
+    else
+        k_field<R, 1><<<grid, kBlockI, 0, st>>>(d.pp, (const V4*)d.posq, (const V4*)d.vec, d.tctr, d.text, d.pos,
+                                               d.exc_off, d.exc_j, d.exc_s, d.n_pad, d.partial);
+}
+
+template <class R>
+void launch_energy(const Dev& d, cudaStream_t st) {
+    dim3 grid(d.n_pad / kBlockI, d.nsplit);
+    typedef typename Vec4T<R>::type V4;
+    k_energy<R><<<grid, kBlockI, 0, st>>>(d.pp, (const V4*)d.posq, (const V4*)d.dipt, (const V4*)d.ind, d.yz, d.tctr,
+                                          d.text, d.pos, d.exc_off, d.exc_j, d.exc_m, d.exc_s, d.n_pad, d.partial,
+                                          d.energy_partial);
+}
+
+#define TDP_INSTANTIATE(R)                                                                                  \
+    template void launch_pack<R>(const Dev&, cudaStream_t);                                                 \
+    template void launch_rotate<R>(const Dev&, cudaStream_t);                                               \
+    template void launch_field<R>(const Dev&, int, cudaStream_t);                                           \
+    template void launch_energy<R>(const Dev&, cudaStream_t);
+
+TDP_INSTANTIATE(float)
+TDP_INSTANTIATE(double)
+
+template <class R>
+void launch_fixed_done(const Dev& d, cudaStream_t st) {
+    k_fixed_done<R><<<nblk(d.n, kVecThreads), kVecThreads, 0, st>>>(d.n, d.nsplit, d.n_pad, d.partial, d.alpha,
+                                                                     d.salpha, d.thole, d.E, d.mu, d.y,
+                                                                     (typename Vec4T<R>::type*)d.vec);
+}
+template <class R>
+void launch_warm_start(const Dev& d, cudaStream_t st) {
+    k_warm_start<R><<<nblk(d.n, kVecThreads), kVecThreads, 0, st>>>(d.n, d.salpha, d.thole, d.mu, d.y,
+                                                                     (typename Vec4T<R>::type*)d.vec);
+}
+template <class R>
+void launch_cg_residual(const Dev& d, cudaStream_t st) {
+    k_cg_residual<R><<<d.nvb, kVecThreads, 0, st>>>(d.n, d.nsplit, d.n_pad, d.partial, d.E, d.salpha, d.thole, d.y,
+                                                    d.r, d.p, (typename Vec4T<R>::type*)d.vec, d.rr_part, d.eps_part);
+}
+void launch_cg_q(const Dev& d, cudaStream_t st) {
+    k_cg_q<<<d.nvb, kVecThreads, 0, st>>>(d.n, d.nsplit, d.n_pad, d.partial, d.salpha, d.p, d.q, d.pq_part);
+}
+void launch_cg_update(const Dev& d, int slot, cudaStream_t st) {
+    k_cg_update<<<d.nvb, kVecThreads, 0, st>>>(d.n, d.nvb, d.scal_rr, slot, d.pq_part, d.salpha, d.p, d.q, d.y, d.r,
+                                               d.rr_part, d.eps_part);
+}
+template <class R>
+void launch_cg_p(const Dev& d, int prev, int slot, cudaStream_t st) {
+    k_cg_p<R><<<d.nvb, kVecThreads, 0, st>>>(d.n, d.nvb, prev, slot, d.scal_rr, d.scal_eps, d.rr_part, d.eps_part, d.salpha,
+                                             d.thole, d.r, d.p, (typename Vec4T<R>::type*)d.vec);
+}
+template <class R>
+void launch_cg_mu(const Dev& d, cudaStream_t st) {
+    k_cg_mu<R><<<d.nvb, kVecThreads, 0, st>>>(d.n, d.salpha, d.thole, d.y, d.mu, (typename Vec4T<R>::type*)d.vec);
+}
+template <class R>
+void launch_jacobi(const Dev& d, cudaStream_t st) {
+    k_jacobi<R><<<d.nvb, kVecThreads, 0, st>>>(d.n, d.nsplit, d.n_pad, d.partial, d.E, d.alpha, d.thole, d.mu,
+                                               (typename Vec4T<R>::type*)d.vec, d.eps_part);
+}
+template <class R>
+void launch_extrap_step(const Dev& d, int k, cudaStream_t st) {
+    k_extrap_step<R><<<d.nvb, kVecThreads, 0, st>>>(d.n, d.nsplit, d.n_pad, d.partial, d.E, d.alpha, d.thole, d.mu,
+                                                    d.hist + (size_t)k * 3 * d.n, (typename Vec4T<R>::type*)d.vec);
+}
+template <class R>
+void launch_extrap_combine(const Dev& d, int korder, const double* coef, cudaStream_t st) {
+    k_extrap_combine<R><<<d.nvb, kVecThreads, 0, st>>>(d.n, korder, coef, d.hist, d.thole, d.mu,
+                                                       (typename Vec4T<R>::type*)d.vec);
+}
+void launch_step_eps(const Dev& d, cudaStream_t st) {
+    k_step_eps<<<d.nvb, kVecThreads, 0, st>>>(d.n, d.nsplit, d.n_pad, d.partial, d.E, d.alpha, d.mu, d.eps_part);
+}
+void launch_eps_scalar(const Dev& d, int slot, cudaStream_t st) {
+    k_eps_scalar<<<1, kVecThreads, 0, st>>>(d.n, d.nvb, d.eps_part, d.scal_eps, slot);
+}
+template <class R>
+void launch_pack_ind(const Dev& d, cudaStream_t st) {
+    k_pack_ind<R><<<d.nvb, kVecThreads, 0, st>>>(d.n, d.mu, (typename Vec4T<R>::type*)d.ind);
+}
+void launch_energy_done(const Dev& d, cudaStream_t st) {
+    int n_eblk = (d.n_pad / kBlockI) * d.nsplit;
+    k_energy_done<<<d.nvb, kVecThreads, 0, st>>>(d.n, d.nsplit, d.n_pad, n_eblk, d.partial, d.energy_partial, d.fpair,
+                                                 d.torque, d.energy);
+}
+void launch_torque_gather(const Dev& d, cudaStream_t st) {
+    k_torque_gather<<<d.nvb, kVecThreads, 0, st>>>(d.n, d.pos, d.axis, d.torque, d.users_off, d.users, d.fpair,
+                                                   d.ftotal);
+}
+void launch_add_forces(const Dev& d, void* acc, int is_f32, cudaStream_t st) {
+    int n3 = 3 * d.n;
+    k_add_forces<<<nblk(n3, kVecThreads), kVecThreads, 0, st>>>(n3, d.ftotal, is_f32 ? nullptr : (double*)acc,
+                                                                 is_f32 ? (float*)acc : nullptr);
+}
+void launch_positions_in(const Dev& d, const void* src, int is_f32, cudaStream_t st) {
+    int n3 = 3 * d.n;
+    k_positions_in<<<nblk(n3, kVecThreads), kVecThreads, 0, st>>>(n3, src, is_f32, d.pos);
+}
+void launch_potential(const Dev& d, const double* grid, int ng, double* out, cudaStream_t st) {
+    k_potential<<<nblk(ng, 128), 128, 0, st>>>(d.n, ng, d.pp, d.pos, d.charge, d.lab, d.mu, grid, out);
+}
+void launch_moments(const Dev& d, const double* mass, double* scratch, double* out13, cudaStream_t st) {
+    int nb = d.nvb;
+    k_com_partials<<<nb, kVecThreads, 0, st>>>(d.n, d.pos, mass, scratch);
+    k_moment_partials<<<nb, kVecThreads, 0, st>>>(d.n, nb, scratch, d.pos, d.charge, d.lab, d.mu, scratch + 4 * nb);
+    k_moment_final<<<1, kVecThreads, 0, st>>>(nb, scratch + 4 * nb, out13);
+}
+
+#define TDP_INSTANTIATE2(R)                                                         \
+    template void launch_fixed_done<R>(const Dev&, cudaStream_t);                   \
+    template void launch_warm_start<R>(const Dev&, cudaStream_t);                   \
+    template void launch_cg_residual<R>(const Dev&, cudaStream_t);                  \
+    template void launch_cg_p<R>(const Dev&, int, int, cudaStream_t);               \
+    template void launch_cg_mu<R>(const Dev&, cudaStream_t);                        \
+    template void launch_jacobi<R>(const Dev&, cudaStream_t);                       \
+    template void launch_extrap_step<R>(const Dev&, int, cudaStream_t);             \
+    template void launch_extrap_combine<R>(const Dev&, int, const double*, cudaStream_t); \
+    template void launch_pack_ind<R>(const Dev&, cudaStream_t);
+
+TDP_INSTANTIATE2(float)
+TDP_INSTANTIATE2(double)
+
+}  // namespace tdp

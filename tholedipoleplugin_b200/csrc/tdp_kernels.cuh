@@ -1,0 +1,86 @@
+// tdp_kernels.cuh -- device state and kernel launchers shared by the C ABI
+// layer (tdp_capi.cu) and the kernels (tdp_kernels.cu).
+#pragma once
+
+#include "tdp_common.cuh"
+
+namespace tdp {
+
+// All device buffers of one system (sizes: n atoms, n_pad = n rounded up to
+// kBlockI, nsplit j-splits of the pair kernels, nvb blocks of the O(N) kernels).
+struct Dev {
+    int n = 0, n_pad = 0, nsplit = 1, nvb = 1;
+    PairParams pp{};
+    // Inputs.
+    double* pos = nullptr;       // n_pad*3 (FP64 working copy of the positions)
+    double* charge = nullptr;    // n
+    double* dip_mol = nullptr;   // n*3 molecular-frame dipoles
+    double* alpha = nullptr;     // n
+    double* salpha = nullptr;    // n, sqrt(alpha)
+    double* thole = nullptr;     // n
+    int4* axis = nullptr;        // n: type, Z, X, Y
+    // Packed pair-kernel records, Vec4<R> of n_pad entries.
+    void* posq = nullptr;        // mixed: (offset from tile centre, q); plain: (x, y, z, q)
+    void* dipt = nullptr;        // (lab dipole, thole)
+    void* vec = nullptr;         // (matvec operand, thole)
+    void* ind = nullptr;         // (induced dipole, 0)
+    double2* yz = nullptr;       // n_pad raw (y, z) for the QI frame test
+    double4* tctr = nullptr;     // n_pad/32 tile centres
+    double4* text = nullptr;     // n_pad/32 tile half-extents
+    // Covalent scale exceptions (both directions), CSR over atoms.
+    int* exc_off = nullptr;
+    int* exc_j = nullptr;
+    double* exc_m = nullptr;     // M scale - 1
+    double* exc_s = nullptr;     // I scale - 1
+    // Torque-mapping users: for atom a, (frame atom, role) entries.
+    int* users_off = nullptr;
+    int2* users = nullptr;
+    // Working vectors (n*3 doubles).
+    double* lab = nullptr;
+    double* E = nullptr;
+    double* mu = nullptr;
+    double* mu_prev = nullptr;
+    double* y = nullptr;
+    double* r = nullptr;
+    double* p = nullptr;
+    double* q = nullptr;
+    double* hist = nullptr;      // extrapolation orders, korder*n*3
+    double* partial = nullptr;   // nsplit*6*n_pad pair-kernel partial sums (scratch)
+    double* energy_partial = nullptr;
+    double* fpair = nullptr;
+    double* torque = nullptr;
+    double* ftotal = nullptr;
+    double* energy = nullptr;    // 1
+    double* rr_part = nullptr;   // nvb
+    double* eps_part = nullptr;
+    double* pq_part = nullptr;
+    double* scal_rr = nullptr;   // per-iteration scalars
+    double* scal_eps = nullptr;
+    double* coef = nullptr;      // extrapolation coefficients
+};
+
+template <class R> void launch_pack(const Dev& d, cudaStream_t st);
+template <class R> void launch_rotate(const Dev& d, cudaStream_t st);
+template <class R> void launch_field(const Dev& d, int kind, cudaStream_t st);
+template <class R> void launch_energy(const Dev& d, cudaStream_t st);
+template <class R> void launch_fixed_done(const Dev& d, cudaStream_t st);
+template <class R> void launch_warm_start(const Dev& d, cudaStream_t st);
+template <class R> void launch_cg_residual(const Dev& d, cudaStream_t st);
+void launch_cg_q(const Dev& d, cudaStream_t st);
+void launch_cg_update(const Dev& d, int slot, cudaStream_t st);
+template <class R> void launch_cg_p(const Dev& d, int prev, int slot, cudaStream_t st);
+template <class R> void launch_cg_mu(const Dev& d, cudaStream_t st);
+template <class R> void launch_jacobi(const Dev& d, cudaStream_t st);
+template <class R> void launch_extrap_step(const Dev& d, int k, cudaStream_t st);
+template <class R> void launch_extrap_combine(const Dev& d, int korder, const double* coef, cudaStream_t st);
+void launch_step_eps(const Dev& d, cudaStream_t st);
+void launch_eps_scalar(const Dev& d, int slot, cudaStream_t st);
+template <class R> void launch_pack_ind(const Dev& d, cudaStream_t st);
+void launch_energy_done(const Dev& d, cudaStream_t st);
+void launch_torque_gather(const Dev& d, cudaStream_t st);
+void launch_add_forces(const Dev& d, void* acc, int is_f32, cudaStream_t st);
+void launch_positions_in(const Dev& d, const void* src, int is_f32, cudaStream_t st);
+void launch_potential(const Dev& d, const double* grid, int ng, double* out, cudaStream_t st);
+void launch_moments(const Dev& d, const double* mass, double* scratch, double* out13, cudaStream_t st);
+
+}  // namespace tdp

@@ -1,0 +1,260 @@
+// tdp_pairs.cuh -- per-pair arithmetic of the TholeDipoleForce hot path, in
+// the reference's semantics (aehogan/tholedipoleplugin,
+// platforms/reference/src/ReferenceTholeDipoleForce.cpp, "RTDF.cpp").  R is
+// float (mixed form) or double (plain form).  Every function works on the
+// displacement d = p_j - p_i already minimum-imaged; a masked pair (self or
+// padding) arrives with r2 = +inf, which makes rinv = 0 and every term zero.
+#pragma once
+
+#include "tdp_common.cuh"
+
+namespace tdp {
+
+// Thole damping of 1/r^3 and 3/r^5 as getAndScaleInverseRs (RTDF.cpp:646-676).
+// Pairs with r2 >= damp_r2 have a*u^3 >= 50 and are left undamped there too.
+template <class R>
+__device__ __forceinline__ void damp_field(R r2, R rinv, R ti, R tj, R damp_r2, R& rr3, R& rr5) {
+    if (r2 < damp_r2) {
+        R dmp = ti * tj;
+        if (dmp != R(0)) {
+            R pgamma = ti < tj ? ti : tj;
+            R r = r2 * rinv;
+            R ratio = r / dmp;
+            ratio = ratio * ratio * ratio;
+            R damp = -pgamma * ratio;
+            if (damp > R(-50)) {
+                R e = exp_r(damp);
+                rr3 *= R(1) - e;
+                rr5 *= R(1) - (R(1) - damp) * e;
+            }
+        }
+    }
+}
+
+// One term of the mutual field (T mu)_i, calculateInducedDipolePairIxn with
+// rr3 -> -rr3 (RTDF.cpp:766-818), I scale applied by the caller.
+template <class R>
+__device__ __forceinline__ void pair_matvec(R dx, R dy, R dz, R r2, R vx, R vy, R vz, R ti, R tj, R damp_r2,
+                                            R& fx, R& fy, R& fz) {
+    R rinv = rsqrt_r(r2);
+    R rinv2 = rinv * rinv;
+    R rr3 = rinv * rinv2;
+    R rr5 = R(3) * rr3 * rinv2;
+    damp_field(r2, rinv, ti, tj, damp_r2, rr3, rr5);
+    R dd = rr5 * (vx * dx + vy * dy + vz * dz);
+    fx += dd * dx - rr3 * vx;
+    fy += dd * dy - rr3 * vy;
+    fz += dd * dz - rr3 * vz;
+}
+
+// One term of the permanent field at i from the charge and lab-frame dipole of
+// j, calculateFixedDipoleFieldPairIxn (RTDF.cpp:678-713), M scale applied by
+// the caller:  E_i -= d (rr3 q_j - rr5 mu_j.d) + mu_j rr3.
+template <class R>
+__device__ __forceinline__ void pair_fixed(R dx, R dy, R dz, R r2, R qj, R mx, R my, R mz, R ti, R tj, R damp_r2,
+                                           R& fx, R& fy, R& fz) {
+    R rinv = rsqrt_r(r2);
+    R rinv2 = rinv * rinv;
+    R rr3 = rinv * rinv2;
+    R rr5 = R(3) * rr3 * rinv2;
+    damp_field(r2, rinv, ti, tj, damp_r2, rr3, rr5);
+    R f = rr3 * qj - rr5 * (mx * dx + my * dy + mz * dz);
+    fx -= dx * f + mx * rr3;
+    fy -= dy * f + my * rr3;
+    fz -= dz * f + mz * rr3;
+}
+
+// Inputs of one particle to the pair energy routine.
+template <class R>
+struct EAtom {
+    R q, mx, my, mz;   // charge, lab-frame permanent dipole
+    R ux, uy, uz;      // induced dipole
+    R t;               // Thole factor
+};
+
+// calculateElectrostaticPairIxn (RTDF.cpp:129-366) with formQIRotationMatrix
+// (:573-607), in its canonical orientation I = lower index, K = higher index,
+// d = p_K - p_I.  The QI frame has rows [X, Y, Z] with Z along d, and the
+// multipole algebra below treats component 0 as the bond axis and back-rotates
+// with the permuted matrix of :150-159, exactly as the reference does.
+// SIDE_I adds the force and torque on I (and the pair energy); otherwise the
+// force and torque on K.  Linear in (mScale, iScale).
+template <class R, bool SIDE_I>
+__device__ __forceinline__ void pair_energy(R dx, R dy, R dz, R r2, bool yz_differ, const EAtom<R>& I,
+                                            const EAtom<R>& K, R mS, R iS, R damp_r2, R rv4_power, R rv4_fill,
+                                            bool mutual, R& fx, R& fy, R& fz, R& tx, R& ty, R& tz, R& en) {
+    R rinv = rsqrt_r(r2);
+    // QI frame.
+    R zx = dx * rinv, zy = dy * rinv, zz = dz * rinv;
+    R xx = zx, xy = zy, xz = zz;
+    if (yz_differ) xx += R(1);
+    else xy += R(1);
+    R dt = zx * xx + zy * xy + zz * xz;
+    xx -= zx * dt;
+    xy -= zy * dt;
+    xz -= zz * dt;
+    R xn2 = xx * xx + xy * xy + xz * xz;
+    if (xn2 > R(0)) {
+        R s = R(1) / sqrt_r(xn2);
+        xx *= s;
+        xy *= s;
+        xz *= s;
+    }
+    R yx = zy * xz - zz * xy, yy = zz * xx - zx * xz, yz = zx * xy - zy * xx;
+
+    R uI0 = xx * I.ux + xy * I.uy + xz * I.uz;
+    R uI1 = yx * I.ux + yy * I.uy + yz * I.uz;
+    R uI2 = zx * I.ux + zy * I.uy + zz * I.uz;
+    R uJ0 = xx * K.ux + xy * K.uy + xz * K.uz;
+    R uJ1 = yx * K.ux + yy * K.uy + yz * K.uz;
+    R uJ2 = zx * K.ux + zy * K.uy + zz * K.uz;
+    R QI0 = I.q, QJ0 = K.q;
+    R QI1 = xx * I.mx + xy * I.my + xz * I.mz;
+    R QI2 = yx * I.mx + yy * I.my + yz * I.mz;
+    R QI3 = zx * I.mx + zy * I.my + zz * I.mz;
+    R QJ1 = xx * K.mx + xy * K.my + xz * K.mz;
+    R QJ2 = yx * K.mx + yy * K.my + yz * K.mz;
+    R QJ3 = zx * K.mx + zy * K.my + zz * K.mz;
+
+    R rv1 = rinv;
+    R rv2 = rv1 * rinv;
+    R rv3 = rv2 * rinv;
+    // rInvVec[4]: read past the end of the reference's 4-element vector.
+    R rv4 = rv4_power * (rv3 * rinv) + rv4_fill;
+
+    // Thole factors; beyond damp_r2 every factor is exactly 1 in the reference too.
+    R tc = R(1), td0 = R(1), td1 = R(1), dtc = R(1), dtd0 = R(1), dtd1 = R(1);
+    if (r2 < damp_r2) {
+        R dmp = I.t * K.t;
+        if (fabs(dmp) > R(1.0e-5)) {
+            R a = I.t < K.t ? I.t : K.t;
+            R r = r2 * rinv;
+            R u = r / dmp;
+            R au3 = a * u * u * u;
+            R e = exp_r(-au3);
+            tc = R(1) - e;
+            td0 = R(1) - e * (R(1) + R(1.5) * au3);
+            td1 = R(1) - e;
+            dtc = R(1) - e * (R(1) + R(1.5) * au3);
+            dtd0 = R(1) - e * (R(1) + au3 + R(1.5) * au3 * au3);
+            dtd1 = R(1) - e * (R(1) + au3);
+        }
+    }
+
+    R Vij0, Vij1, Vij2, Vij3, Vji0, Vji1, Vji2, Vji3;
+    R VijR0, VijR1, VijR2, VijR3, VjiR0, VjiR1, VjiR2, VjiR3;
+    R Vijd0, Vijd1, Vijd2, Vjid0, Vjid1, Vjid2;
+
+    R eP = rv1 * mS;
+    R dP = R(-0.5) * mS * rv2;
+    Vij0 = eP * QJ0;
+    Vji0 = eP * QI0;
+    VijR0 = dP * QJ0;
+    VjiR0 = dP * QI0;
+
+    eP = rv2 * mS;
+    R eU = rv2 * iS * tc;
+    dP = -rv3 * mS;
+    R dU = R(-2) * rv3 * iS * dtc;
+    Vij0 += -(eP * QJ1 + eU * uJ0);
+    Vji1 = -(eP * QI0);
+    VijR0 += -(dP * QJ1 + dU * uJ0);
+    VjiR1 = -(dP * QI0);
+    Vjid0 = -(eU * QI0);
+    Vij1 = eP * QJ0;
+    Vji0 += eP * QI1 + eU * uI0;
+    VijR1 = dP * QJ0;
+    VjiR0 += dP * QI1 + dU * uI0;
+    Vijd0 = eU * QJ0;
+
+    eP = R(-2) * rv3 * mS;
+    eU = R(-2) * rv3 * iS * td0;
+    dP = R(3) * rv4 * mS;
+    dU = R(6) * rv4 * iS * dtd0;
+    Vij1 += eP * QJ1 + eU * uJ0;
+    Vji1 += eP * QI1 + eU * uI0;
+    VijR1 += dP * QJ1 + dU * uJ0;
+    VjiR1 += dP * QI1 + dU * uI0;
+    Vijd0 += eU * QJ1;
+    Vjid0 += eU * QI1;
+
+    eP = rv3 * mS;
+    eU = rv3 * iS * td1;
+    dP = R(-1.5) * rv4 * mS;
+    dU = R(-3) * rv4 * iS * dtd1;
+    Vij2 = eP * QJ2 + eU * uJ1;
+    Vji2 = eP * QI2 + eU * uI1;
+    VijR2 = dP * QJ2 + dU * uJ1;
+    VjiR2 = dP * QI2 + dU * uI1;
+    Vijd1 = eU * QJ2;
+    Vjid1 = eU * QI2;
+    Vij3 = eP * QJ3 + eU * uJ2;
+    Vji3 = eP * QI3 + eU * uI2;
+    VijR3 = dP * QJ3 + dU * uJ2;
+    VjiR3 = dP * QI3 + dU * uI2;
+    Vijd2 = eU * QJ3;
+    Vjid2 = eU * QI3;
+
+    R fIZ = QI0 * VijR0 + QI1 * VijR1 + QI2 * VijR2 + QI3 * VijR3;
+    R fJZ = QJ0 * VjiR0 + QJ1 * VjiR1 + QJ2 * VjiR2 + QJ3 * VjiR3;
+    R EIX = QI3 * Vij1 - QI1 * Vij3;
+    R EIY = QI1 * Vij2 - QI2 * Vij1;
+    R EJX = QJ3 * Vji1 - QJ1 * Vji3;
+    R EJY = QJ1 * Vji2 - QJ2 * Vji1;
+    R iEIX = uI2 * Vijd0 - uI0 * Vijd2;
+    R iEJX = uJ2 * Vjid0 - uJ0 * Vjid2;
+    R iEIY = uI0 * Vijd1 - uI1 * Vijd0;
+    R iEJY = uJ0 * Vjid1 - uJ1 * Vjid0;
+    if (mutual) {
+        R eC = R(-4) * rv3 * iS * td0;
+        R dC = R(6) * rv4 * iS * dtd0;
+        iEIX += eC * uI2 * uJ0;
+        iEJX += eC * uJ2 * uI0;
+        iEIY -= eC * uI1 * uJ0;
+        iEJY -= eC * uJ1 * uI0;
+        fIZ += dC * uI0 * uJ0;
+        fJZ += dC * uJ0 * uI0;
+        eC = R(2) * rv3 * iS * td1;
+        dC = R(-3) * rv4 * iS * dtd1;
+        iEIX -= eC * uI0 * uJ2;
+        iEJX -= eC * uJ0 * uI2;
+        iEIY += eC * uI0 * uJ1;
+        iEJY += eC * uJ0 * uI1;
+        fIZ += dC * (uI1 * uJ1 + uI2 * uJ2);
+        fJZ += dC * (uJ1 * uI1 + uJ2 * uI2);
+    }
+    R qf0 = rinv * (EIY + EJY + iEIY + iEJY);
+    R qf1 = -rinv * (EIX + EJX + iEIX + iEJX);
+    R qf2 = -(fJZ + fIZ);
+    // Back rotation with the reference's permuted matrix: rows (Y.y, Z.y, X.y),
+    // (Y.z, Z.z, X.z), (Y.x, Z.x, X.x).
+    R fvx = yy * qf0 + zy * qf1 + xy * qf2;
+    R fvy = yz * qf0 + zz * qf1 + xz * qf2;
+    R fvz = yx * qf0 + zx * qf1 + xx * qf2;
+    if (SIDE_I) {
+        R EIZ = QI2 * Vij3 - QI3 * Vij2;
+        R q0 = -EIX, q1 = -EIY, q2 = -EIZ;
+        tx += yy * q0 + zy * q1 + xy * q2;
+        ty += yz * q0 + zz * q1 + xz * q2;
+        tz += yx * q0 + zx * q1 + xx * q2;
+        fx -= fvx;
+        fy -= fvy;
+        fz -= fvz;
+        R e = R(0.5) * (QI0 * Vij0 + QJ0 * Vji0);
+        e += R(0.5) * (QI1 * Vij1 + QJ1 * Vji1);
+        e += R(0.5) * (QI2 * Vij2 + QJ2 * Vji2);
+        e += R(0.5) * (QI3 * Vij3 + QJ3 * Vji3);
+        en += e;
+    } else {
+        R EJZ = QJ2 * Vji3 - QJ3 * Vji2;
+        R q0 = -EJX, q1 = -EJY, q2 = -EJZ;
+        tx += yy * q0 + zy * q1 + xy * q2;
+        ty += yz * q0 + zz * q1 + xz * q2;
+        tz += yx * q0 + zx * q1 + xx * q2;
+        fx += fvx;
+        fy += fvy;
+        fz += fvz;
+    }
+}
+
+}  // namespace tdp
