@@ -188,6 +188,29 @@ int tdp_get_dipoles(tdp_handle* h, int32_t which, const void* positions, int32_t
 int tdp_get_potential(tdp_handle* h, const void* positions, int32_t pos_dtype, int32_t on_device,
                       const double* grid, int32_t num_points, double* out);
 
+/* Electrostatic potential at grid points that allocates no device memory.
+ * No counterpart in the reference: it exists for callers that cannot call
+ * cudaMalloc -- a host program whose pool allocator owns all device memory,
+ * or a loop that must not hit the implicit device synchronisation of
+ * cudaMalloc/cudaFree.  Same sums as tdp_get_potential (bare 1/r and 1/r^3
+ * of the charges and the total dipoles, minimum image when periodic != 0 with
+ * the box diagonal box3, a host array), but every input and output is a
+ * device pointer the caller owns: positions and total_dipoles (n*3),
+ * charges (n), grid (num_points*3), out (num_points), and no handle is needed.
+ * Its scratch (per-atom-chunk partial sums) is one file-scope device array of
+ * TDP_NOALLOC_SCRATCH_DOUBLES doubles (8 MiB) that every GPU loading this
+ * library keeps until exit; num_points above that count is rejected with
+ * TDP_ERR_INVALID_ARGUMENT.  The first call on a device looks up the array's
+ * device address (cudaGetSymbolAddress) with that device current, so make it
+ * before any stream capture.  All calls share the array and leave their
+ * partial sums in it (every slot a call reads, it first writes, so nothing
+ * needs clearing); calls that overlap on the GPU race on it.  Errors:
+ * tdp_last_error(NULL). */
+#define TDP_NOALLOC_SCRATCH_DOUBLES (1 << 20)
+int tdp_potential_noalloc(int32_t num_particles, const double* positions, const double* charges,
+                          const double* total_dipoles, int32_t num_points, const double* grid, int32_t periodic,
+                          const double* box3, double* out, void* stream);
+
 /* getSystemMultipoleMoments (TholeDipoleKernels.h:121,
  * ReferenceTholeDipoleForce.cpp:1225-1313): 13 values (charge, dipole in
  * Debye, traceless quadrupole), masses: n host doubles. */

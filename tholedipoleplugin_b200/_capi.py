@@ -69,6 +69,8 @@ PROTOTYPES = {
     "tdp_get_dipoles": (C.c_int, [C.c_void_p, C.c_int32, C.c_void_p, C.c_int32, C.c_int32, _dp]),
     "tdp_get_potential": (C.c_int, [C.c_void_p, C.c_void_p, C.c_int32, C.c_int32, _dp, C.c_int32, _dp]),
     "tdp_get_moments": (C.c_int, [C.c_void_p, C.c_void_p, C.c_int32, C.c_int32, _dp, _dp]),
+    "tdp_potential_noalloc": (C.c_int, [C.c_int32, C.c_void_p, C.c_void_p, C.c_void_p, C.c_int32, C.c_void_p,
+                                        C.c_int32, _dp, C.c_void_p, C.c_void_p]),
     "tdp_get_pme_parameters": (C.c_int, [C.c_void_p, _dp, _ip, _ip, _ip]),
     "tdp_solver_stats": (C.c_int, [C.c_void_p, _ip, _dp, _ip, _ip]),
     "tdp_enable_timing": (C.c_int, [C.c_void_p, C.c_int32]),

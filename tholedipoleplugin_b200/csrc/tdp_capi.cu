@@ -21,6 +21,11 @@
 
 using namespace tdp;
 
+namespace tdp {
+const char* noalloc_error_message();
+void noalloc_clear_error();
+}  // namespace tdp
+
 namespace {
 
 thread_local std::string g_create_error;
@@ -99,8 +104,12 @@ struct tdp_handle {
 namespace {
 
 int fail(tdp_handle* h, const TdpError& e) {
-    if (h) h->err = e.msg;
-    else g_create_error = e.msg;
+    if (h) {
+        h->err = e.msg;
+    } else {
+        g_create_error = e.msg;
+        noalloc_clear_error();
+    }
     return e.code;
 }
 
@@ -498,7 +507,11 @@ extern "C" {
 
 int tdp_abi_version(void) { return TDP_ABI_VERSION; }
 
-const char* tdp_last_error(const tdp_handle* h) { return h ? h->err.c_str() : g_create_error.c_str(); }
+const char* tdp_last_error(const tdp_handle* h) {
+    if (h) return h->err.c_str();
+    const char* na = noalloc_error_message();
+    return na[0] ? na : g_create_error.c_str();
+}
 
 int tdp_create(const tdp_system_desc* desc, tdp_handle** out) {
     if (!out) return TDP_ERR_INVALID_ARGUMENT;
@@ -682,6 +695,7 @@ int tdp_create(const tdp_system_desc* desc, tdp_handle** out) {
         return code;
     } catch (const std::exception& e) {
         g_create_error = e.what();
+        noalloc_clear_error();
         tdp_destroy(h);
         return TDP_ERR_INVALID_ARGUMENT;
     }
