@@ -28,6 +28,7 @@ def energy_scale(s):
     return float((q[:, None] * q[None, :])[iu] @ (1.0 / r[iu]))
 
 
-def energy_err(e, ref, s):
-    """Energy error relative to max(|E|, Coulomb magnitude scale)."""
-    return abs(e - ref) / max(abs(ref), energy_scale(s) if len(s.charges) <= 2000 else abs(ref))
+def energy_err(e, ref, s, floor=1e-3):
+    """Energy error relative to max(|E|, floor * Coulomb magnitude scale)."""
+    scale = energy_scale(s) if len(s.charges) <= 4000 else 0.0
+    return abs(e - ref) / max(abs(ref), floor * scale)

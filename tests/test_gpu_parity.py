@@ -3,8 +3,8 @@
 Tolerances:
   * plain (FP64) form: energy relative 1e-9, forces and induced dipoles RMS
     relative 1e-8 (rounding-level agreement; the solve runs to 1e-11);
-  * mixed form: energy relative 1e-6 (for the non-neutral random systems
-    relative to max(|E|, sum |q_i q_j|/r_ij)) and RMS relative
+  * mixed form: energy relative 1e-6 of max(|E|, 1e-3 sum |q_i q_j|/r_ij)
+    (|E| itself for every water box and reference test system) and RMS relative
     force error 2e-5 (the accuracy targets for the FP32 path), induced
     dipoles RMS relative 2e-5;
   * Jacobi solver: the same iteration count as the reference loop.
@@ -71,11 +71,12 @@ def test_mixed_matches_oracle(name):
     with CudaCalcTholeDipoleForceKernel(s.copy(target_eps=1e-9, max_iter=2000), precision="mixed") as k:
         e, f = k.execute(s.positions)
         mu = k.getInducedDipoles()
-    # Energy relative error 1e-6.  The random systems carry random, non-neutral
-    # charges whose total energy nearly cancels; there the error is judged
-    # against max(|E|, sum|q_i q_j|/r_ij) instead of |E| alone.
-    err = energy_err(e, ref.energy, s) if name.startswith("random") else rel_err(e, ref.energy)
-    assert err < 1e-6, (e, ref.energy)
+    # Energy relative error 1e-6 of max(|E|, 1e-3 * sum|q_i q_j|/r_ij): FP32 pair
+    # arithmetic carries ~1e-7 relative error per pair term, so where the total
+    # is a thousand times smaller than its terms (randomly oriented clusters,
+    # sparse boxes, random non-neutral charges) it is judged against the term
+    # scale; everywhere else the bound is 1e-6 of |E| itself.
+    assert energy_err(e, ref.energy, s) < 1e-6, (e, ref.energy)
     assert rel_rms(f, ref.forces) < 2e-5
     if s.polarization != S.DIRECT or np.abs(ref.induced).max() > 0:
         assert rel_rms(mu, ref.induced) < 2e-5

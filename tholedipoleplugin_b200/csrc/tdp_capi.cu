@@ -597,16 +597,22 @@ int tdp_create(const tdp_system_desc* desc, tdp_handle** out) {
         for (auto& kv : scales) {
             double m = kv.second.first, s = kv.second.second;
             if (m == 1.0 && s == 1.0) continue;
-            exc[kv.first.first].push_back(std::make_tuple(kv.first.second, m - 1.0, s - 1.0));
-            exc[kv.first.second].push_back(std::make_tuple(kv.first.first, m - 1.0, s - 1.0));
+            exc[kv.first.first].push_back(std::make_tuple(kv.first.second, m, s));
+            exc[kv.first.second].push_back(std::make_tuple(kv.first.first, m, s));
         }
         std::vector<int> eoff(n + 1, 0), ej;
         std::vector<double> em, es;
+        int n_tiles_pad = std::max(kBlockI, ((n + kBlockI - 1) / kBlockI) * kBlockI) / kTile;
+        std::vector<int2> etiles(n_tiles_pad, make_int2(1 << 30, -1));  // empty range
         for (int i = 0; i < n; i++) {
             for (auto& t : exc[i]) {
-                ej.push_back(std::get<0>(t));
+                int j = std::get<0>(t);
+                ej.push_back(j);
                 em.push_back(std::get<1>(t));
                 es.push_back(std::get<2>(t));
+                int2& r = etiles[i / kTile];
+                r.x = std::min(r.x, j / kTile);
+                r.y = std::max(r.y, j / kTile);
             }
             eoff[i + 1] = (int)ej.size();
         }
@@ -650,6 +656,7 @@ int tdp_create(const tdp_system_desc* desc, tdp_handle** out) {
         d.exc_j = dalloc<int>(ej.size(), o);
         d.exc_m = dalloc<double>(em.size(), o);
         d.exc_s = dalloc<double>(es.size(), o);
+        d.exc_tiles = dalloc<int2>(etiles.size(), o);
         d.users_off = dalloc<int>(n + 1, o);
         size_t n3 = 3 * (size_t)n;
         d.lab = dalloc<double>(n3, o);
@@ -682,6 +689,7 @@ int tdp_create(const tdp_system_desc* desc, tdp_handle** out) {
         upload(d.exc_j, ej.data(), sizeof(int) * ej.size());
         upload(d.exc_m, em.data(), sizeof(double) * em.size());
         upload(d.exc_s, es.data(), sizeof(double) * es.size());
+        upload(d.exc_tiles, etiles.data(), sizeof(int2) * etiles.size());
         upload(d.coef, h->extrap.data(), sizeof(double) * h->extrap.size());
         upload_params(h);
         TDP_CUDA(cudaMallocHost(&h->h_scal, 64 * sizeof(double)));

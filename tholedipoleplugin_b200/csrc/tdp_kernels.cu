@@ -229,11 +229,30 @@ __device__ __forceinline__ R masked_r2(R r2, bool dirty, int i, int j, int n) {
 // Field kernels: KIND 0 = permanent field (j records: posq + lab dipole/thole),
 // KIND 1 = mutual-field matvec T*v (j records: posq + v/thole).
 // ---------------------------------------------------------------------------
-template <class R, int KIND, bool FOLD, bool DIRTY>
+// Covalent scale of pair (i, j) from i's exception list (scale 1 if absent).
+__device__ __forceinline__ void pair_scales(const int* __restrict__ exc_j, const double* __restrict__ exc_m,
+                                            const double* __restrict__ exc_s, int e0, int e1, int j, double& m,
+                                            double& sc) {
+    m = 1.0;
+    sc = 1.0;
+    for (int e = e0; e < e1; e++)
+        if (exc_j[e] == j) {
+            m = exc_m[e];
+            sc = exc_s[e];
+        }
+}
+
+// SLOW subtiles are the diagonal tile, the ragged last tile and tiles holding
+// covalent partners of the warp's atoms: there self/padding pairs are masked
+// and each pair's M/I scale is applied in place, so excluded terms are never
+// formed.
+template <class R, int KIND, bool FOLD, bool SLOW>
 __device__ __forceinline__ void field_subtile(const PairParams& P, const double* __restrict__ pos,
                                               const typename Vec4T<R>::type* __restrict__ sp,
                                               const typename Vec4T<R>::type* __restrict__ sv, int i, int jbase,
-                                              R oix, R oiy, R oiz, R ti, R damp_r2, R& fx, R& fy, R& fz) {
+                                              R oix, R oiy, R oiz, R ti, R damp_r2, const int* __restrict__ exc_j,
+                                              const double* __restrict__ exc_m, const double* __restrict__ exc_s,
+                                              int e0, int e1, R& fx, R& fy, R& fz) {
 #pragma unroll 4
     for (int jj = 0; jj < kTile; jj++) {
         typename Vec4T<R>::type pj = sp[jj];
@@ -242,11 +261,26 @@ __device__ __forceinline__ void field_subtile(const PairParams& P, const double*
         R dx, dy, dz;
         pair_delta<R, FOLD>(P, pos, i, j, pj.x, pj.y, pj.z, oix, oiy, oiz, dx, dy, dz);
         R r2 = dx * dx + dy * dy + dz * dz;
-        r2 = masked_r2<R>(r2, DIRTY, i, j, P.n);
-        if (KIND == 0)
-            pair_fixed<R>(dx, dy, dz, r2, pj.w, vj.x, vj.y, vj.z, ti, vj.w, damp_r2, fx, fy, fz);
-        else
-            pair_matvec<R>(dx, dy, dz, r2, vj.x, vj.y, vj.z, ti, vj.w, damp_r2, fx, fy, fz);
+        if (SLOW) {
+            r2 = masked_r2<R>(r2, true, i, j, P.n);
+            double m, sc;
+            pair_scales(exc_j, exc_m, exc_s, e0, e1, j, m, sc);
+            R scale = (R)(KIND == 0 ? m : sc);
+            if (scale == R(0)) continue;
+            R tx = 0, ty = 0, tz = 0;
+            if (KIND == 0)
+                pair_fixed<R>(dx, dy, dz, r2, pj.w, vj.x, vj.y, vj.z, ti, vj.w, damp_r2, tx, ty, tz);
+            else
+                pair_matvec<R>(dx, dy, dz, r2, vj.x, vj.y, vj.z, ti, vj.w, damp_r2, tx, ty, tz);
+            fx += scale * tx;
+            fy += scale * ty;
+            fz += scale * tz;
+        } else {
+            if (KIND == 0)
+                pair_fixed<R>(dx, dy, dz, r2, pj.w, vj.x, vj.y, vj.z, ti, vj.w, damp_r2, fx, fy, fz);
+            else
+                pair_matvec<R>(dx, dy, dz, r2, vj.x, vj.y, vj.z, ti, vj.w, damp_r2, fx, fy, fz);
+        }
     }
 }
 
@@ -256,7 +290,8 @@ __global__ void __launch_bounds__(kBlockI) k_field(PairParams P, const typename 
                                                    const double4* __restrict__ tctr,
                                                    const double4* __restrict__ text,
                                                    const double* __restrict__ pos, const int* __restrict__ exc_off,
-                                                   const int* __restrict__ exc_j, const double* __restrict__ exc_scale,
+                                                   const int* __restrict__ exc_j, const double* __restrict__ exc_m,
+                                                   const double* __restrict__ exc_s, const int2* __restrict__ exc_tiles,
                                                    int n_pad, double* __restrict__ partial) {
     typedef typename Vec4T<R>::type V4;
     __shared__ V4 s_pos[kJStage];
@@ -270,6 +305,9 @@ __global__ void __launch_bounds__(kBlockI) k_field(PairParams P, const typename 
     const R ti = jvec[i].w;
     const double4 cA = tctr[A];
     const double4 eA = text[A];
+    const int2 etile = exc_tiles[A];
+    const int e0 = i < P.n ? exc_off[i] : 0;
+    const int e1 = i < P.n ? exc_off[i + 1] : 0;
     const R damp_r2 = (R)P.damp_r2;
     double ax = 0.0, ay = 0.0, az = 0.0;
 
@@ -303,48 +341,30 @@ __global__ void __launch_bounds__(kBlockI) k_field(PairParams P, const typename 
                 oiy = pi.y + ((s_ctr[sub].y - cA.y) - g.dcy);
                 oiz = pi.z + ((s_ctr[sub].z - cA.z) - g.dcz);
             }
-            const bool dirty = (B == A) || (B == P.n_tiles - 1 && (P.n & (kTile - 1)));
+            const bool slow = (B == A) || (B == P.n_tiles - 1 && (P.n & (kTile - 1))) ||
+                              (B >= etile.x && B <= etile.y);
             R fx = 0, fy = 0, fz = 0;
             const V4* sp = s_pos + sub * kTile;
             const V4* sv = s_vec + sub * kTile;
             const int jbase = B * kTile;
             if (g.fold) {
-                if (dirty)
-                    field_subtile<R, KIND, true, true>(P, pos, sp, sv, i, jbase, oix, oiy, oiz, ti, damp_r2, fx, fy, fz);
+                if (slow)
+                    field_subtile<R, KIND, true, true>(P, pos, sp, sv, i, jbase, oix, oiy, oiz, ti, damp_r2, exc_j,
+                                                       exc_m, exc_s, e0, e1, fx, fy, fz);
                 else
-                    field_subtile<R, KIND, true, false>(P, pos, sp, sv, i, jbase, oix, oiy, oiz, ti, damp_r2, fx, fy, fz);
+                    field_subtile<R, KIND, true, false>(P, pos, sp, sv, i, jbase, oix, oiy, oiz, ti, damp_r2, exc_j,
+                                                        exc_m, exc_s, e0, e1, fx, fy, fz);
             } else {
-                if (dirty)
-                    field_subtile<R, KIND, false, true>(P, pos, sp, sv, i, jbase, oix, oiy, oiz, ti, damp_r2, fx, fy, fz);
+                if (slow)
+                    field_subtile<R, KIND, false, true>(P, pos, sp, sv, i, jbase, oix, oiy, oiz, ti, damp_r2, exc_j,
+                                                        exc_m, exc_s, e0, e1, fx, fy, fz);
                 else
-                    field_subtile<R, KIND, false, false>(P, pos, sp, sv, i, jbase, oix, oiy, oiz, ti, damp_r2, fx, fy,
-                                                         fz);
+                    field_subtile<R, KIND, false, false>(P, pos, sp, sv, i, jbase, oix, oiy, oiz, ti, damp_r2, exc_j,
+                                                         exc_m, exc_s, e0, e1, fx, fy, fz);
             }
             ax += (double)fx;
             ay += (double)fy;
             az += (double)fz;
-        }
-    }
-    // Covalent scale corrections: the main loop used scale 1 for every pair;
-    // each listed pair adds (scale - 1) times its term (the terms are linear in
-    // the scale).
-    if (blockIdx.y == 0 && i < P.n) {
-        for (int e = exc_off[i]; e < exc_off[i + 1]; e++) {
-            double s = exc_scale[e];
-            if (s == 0.0) continue;
-            int j = exc_j[e];
-            d3 d = exact_delta(P, pos, i, j);
-            R dx = (R)d.x, dy = (R)d.y, dz = (R)d.z;
-            R r2 = dx * dx + dy * dy + dz * dz;
-            V4 vj = jvec[j];
-            R fx = 0, fy = 0, fz = 0;
-            if (KIND == 0)
-                pair_fixed<R>(dx, dy, dz, r2, posq[j].w, vj.x, vj.y, vj.z, ti, vj.w, damp_r2, fx, fy, fz);
-            else
-                pair_matvec<R>(dx, dy, dz, r2, vj.x, vj.y, vj.z, ti, vj.w, damp_r2, fx, fy, fz);
-            ax += s * (double)fx;
-            ay += s * (double)fy;
-            az += s * (double)fz;
         }
     }
     const size_t base = (size_t)blockIdx.y * 3 * n_pad;
@@ -356,14 +376,16 @@ __global__ void __launch_bounds__(kBlockI) k_field(PairParams P, const typename 
 // ---------------------------------------------------------------------------
 // Energy / force / torque kernel.
 // ---------------------------------------------------------------------------
-template <class R, bool FOLD, bool DIRTY>
+template <class R, bool FOLD, bool SLOW>
 __device__ __forceinline__ void energy_subtile(const PairParams& P, const double* __restrict__ pos,
                                                const typename Vec4T<R>::type* __restrict__ sp,
                                                const typename Vec4T<R>::type* __restrict__ sd,
                                                const typename Vec4T<R>::type* __restrict__ su,
                                                const double2* __restrict__ syz, int i, int jbase, R oix, R oiy, R oiz,
                                                double yi, double zi, const EAtom<R>& me, R damp_r2, R rv4p, R rv4f,
-                                               bool upper, R& fx, R& fy, R& fz, R& tx, R& ty, R& tz, R& en) {
+                                               bool upper, const int* __restrict__ exc_j,
+                                               const double* __restrict__ exc_m, const double* __restrict__ exc_s,
+                                               int e0, int e1, R& fx, R& fy, R& fz, R& tx, R& ty, R& tz, R& en) {
 #pragma unroll 1
     for (int jj = 0; jj < kTile; jj++) {
         typename Vec4T<R>::type pj = sp[jj], dj = sd[jj], uj = su[jj];
@@ -372,7 +394,15 @@ __device__ __forceinline__ void energy_subtile(const PairParams& P, const double
         R dx, dy, dz;
         pair_delta<R, FOLD>(P, pos, i, j, pj.x, pj.y, pj.z, oix, oiy, oiz, dx, dy, dz);
         R r2 = dx * dx + dy * dy + dz * dz;
-        r2 = masked_r2<R>(r2, DIRTY, i, j, P.n);
+        R mS = R(1), iS = R(1);
+        if (SLOW) {
+            r2 = masked_r2<R>(r2, true, i, j, P.n);
+            double m, sc;
+            pair_scales(exc_j, exc_m, exc_s, e0, e1, j, m, sc);
+            if (m == 0.0 && sc == 0.0) continue;
+            mS = (R)m;
+            iS = (R)sc;
+        }
         bool yzd = (yi != yzj.x) || (zi != yzj.y);
         EAtom<R> other;
         other.q = pj.w;
@@ -384,11 +414,11 @@ __device__ __forceinline__ void energy_subtile(const PairParams& P, const double
         other.uy = uj.y;
         other.uz = uj.z;
         // The pair is evaluated in the reference's orientation: I = lower index.
-        if (!upper && (!DIRTY || j > i))
-            pair_energy<R, true>(dx, dy, dz, r2, yzd, me, other, R(1), R(1), damp_r2, rv4p, rv4f, P.mutual, fx, fy,
-                                 fz, tx, ty, tz, en);
+        if (!upper && (!SLOW || j > i))
+            pair_energy<R, true>(dx, dy, dz, r2, yzd, me, other, mS, iS, damp_r2, rv4p, rv4f, P.mutual, fx, fy, fz,
+                                 tx, ty, tz, en);
         else
-            pair_energy<R, false>(-dx, -dy, -dz, r2, yzd, other, me, R(1), R(1), damp_r2, rv4p, rv4f, P.mutual, fx, fy,
+            pair_energy<R, false>(-dx, -dy, -dz, r2, yzd, other, me, mS, iS, damp_r2, rv4p, rv4f, P.mutual, fx, fy,
                                   fz, tx, ty, tz, en);
     }
 }
@@ -401,7 +431,8 @@ __global__ void __launch_bounds__(kBlockI) k_energy(PairParams P, const typename
                                                     const double4* __restrict__ text, const double* __restrict__ pos,
                                                     const int* __restrict__ exc_off, const int* __restrict__ exc_j,
                                                     const double* __restrict__ exc_m, const double* __restrict__ exc_s,
-                                                    int n_pad, double* __restrict__ partial,
+                                                    const int2* __restrict__ exc_tiles, int n_pad,
+                                                    double* __restrict__ partial,
                                                     double* __restrict__ energy_partial) {
     typedef typename Vec4T<R>::type V4;
     __shared__ V4 s_pos[kJStage];
@@ -429,6 +460,9 @@ __global__ void __launch_bounds__(kBlockI) k_energy(PairParams P, const typename
     me.uz = ui.z;
     const double4 cA = tctr[A];
     const double4 eA = text[A];
+    const int2 etile = exc_tiles[A];
+    const int e0 = i < P.n ? exc_off[i] : 0;
+    const int e1 = i < P.n ? exc_off[i + 1] : 0;
     const R damp_r2 = (R)P.damp_r2;
     const R rv4p = (R)P.rinv4_power, rv4f = (R)P.rinv4_fill;
     double afx = 0, afy = 0, afz = 0, atx = 0, aty = 0, atz = 0, aen = 0;
@@ -465,66 +499,25 @@ __global__ void __launch_bounds__(kBlockI) k_energy(PairParams P, const typename
                 oiy = pi.y + ((s_ctr[sub].y - cA.y) - g.dcy);
                 oiz = pi.z + ((s_ctr[sub].z - cA.z) - g.dcz);
             }
-            const bool dirty = (B == A) || (B == P.n_tiles - 1 && (P.n & (kTile - 1)));
+            const bool slow = (B == A) || (B == P.n_tiles - 1 && (P.n & (kTile - 1))) ||
+                              (B >= etile.x && B <= etile.y);
             // Outside the diagonal tile every j of the subtile is on one side of i.
-            const bool upper = !dirty && (B < A);
+            const bool upper = B < A;
             R fx = 0, fy = 0, fz = 0, tx = 0, ty = 0, tz = 0, en = 0;
             const int o = sub * kTile;
             const int jbase = B * kTile;
+#define TDP_ESUB(F, S)                                                                                              \
+    energy_subtile<R, F, S>(P, pos, s_pos + o, s_dip + o, s_ind + o, s_yz + o, i, jbase, oix, oiy, oiz, yzi.x, yzi.y, \
+                            me, damp_r2, rv4p, rv4f, upper && !(S), exc_j, exc_m, exc_s, e0, e1, fx, fy, fz, tx, ty,  \
+                            tz, en)
             if (g.fold) {
-                if (dirty)
-                    energy_subtile<R, true, true>(P, pos, s_pos + o, s_dip + o, s_ind + o, s_yz + o, i, jbase, oix, oiy,
-                                                  oiz, yzi.x, yzi.y, me, damp_r2, rv4p, rv4f, upper, fx, fy, fz, tx,
-                                                  ty, tz, en);
-                else
-                    energy_subtile<R, true, false>(P, pos, s_pos + o, s_dip + o, s_ind + o, s_yz + o, i, jbase, oix,
-                                                   oiy, oiz, yzi.x, yzi.y, me, damp_r2, rv4p, rv4f, upper, fx, fy, fz,
-                                                   tx, ty, tz, en);
+                if (slow) TDP_ESUB(true, true);
+                else TDP_ESUB(true, false);
             } else {
-                if (dirty)
-                    energy_subtile<R, false, true>(P, pos, s_pos + o, s_dip + o, s_ind + o, s_yz + o, i, jbase, oix,
-                                                   oiy, oiz, yzi.x, yzi.y, me, damp_r2, rv4p, rv4f, upper, fx, fy, fz,
-                                                   tx, ty, tz, en);
-                else
-                    energy_subtile<R, false, false>(P, pos, s_pos + o, s_dip + o, s_ind + o, s_yz + o, i, jbase, oix,
-                                                    oiy, oiz, yzi.x, yzi.y, me, damp_r2, rv4p, rv4f, upper, fx, fy, fz,
-                                                    tx, ty, tz, en);
+                if (slow) TDP_ESUB(false, true);
+                else TDP_ESUB(false, false);
             }
-            afx += (double)fx;
-            afy += (double)fy;
-            afz += (double)fz;
-            atx += (double)tx;
-            aty += (double)ty;
-            atz += (double)tz;
-            aen += (double)en;
-        }
-    }
-    if (blockIdx.y == 0 && i < P.n) {
-        for (int e = exc_off[i]; e < exc_off[i + 1]; e++) {
-            int j = exc_j[e];
-            R mS = (R)exc_m[e], iS = (R)exc_s[e];
-            d3 d = exact_delta(P, pos, i, j);
-            R dx = (R)d.x, dy = (R)d.y, dz = (R)d.z;
-            R r2 = dx * dx + dy * dy + dz * dz;
-            V4 pj = posq[j], dj = dipt[j], uj = indv[j];
-            double2 yzj = yz[j];
-            bool yzd = (yzi.x != yzj.x) || (yzi.y != yzj.y);
-            EAtom<R> other;
-            other.q = pj.w;
-            other.mx = dj.x;
-            other.my = dj.y;
-            other.mz = dj.z;
-            other.t = dj.w;
-            other.ux = uj.x;
-            other.uy = uj.y;
-            other.uz = uj.z;
-            R fx = 0, fy = 0, fz = 0, tx = 0, ty = 0, tz = 0, en = 0;
-            if (j > i)
-                pair_energy<R, true>(dx, dy, dz, r2, yzd, me, other, mS, iS, damp_r2, rv4p, rv4f, P.mutual, fx, fy, fz,
-                                     tx, ty, tz, en);
-            else
-                pair_energy<R, false>(-dx, -dy, -dz, r2, yzd, other, me, mS, iS, damp_r2, rv4p, rv4f, P.mutual, fx, fy,
-                                      fz, tx, ty, tz, en);
+#undef TDP_ESUB
             afx += (double)fx;
             afy += (double)fy;
             afz += (double)fz;
@@ -1134,10 +1127,12 @@ void launch_field(const Dev& d, int kind, cudaStream_t st) {
     typedef typename Vec4T<R>::type V4;
     if (kind == 0)
         k_field<R, 0><<<grid, kBlockI, 0, st>>>(d.pp, (const V4*)d.posq, (const V4*)d.dipt, d.tctr, d.text, d.pos,
-                                               d.exc_off, d.exc_j, d.exc_m, d.n_pad, d.partial);
+                                               d.exc_off, d.exc_j, d.exc_m, d.exc_s, d.exc_tiles, d.n_pad,
+                                               d.partial);
     else
         k_field<R, 1><<<grid, kBlockI, 0, st>>>(d.pp, (const V4*)d.posq, (const V4*)d.vec, d.tctr, d.text, d.pos,
-                                               d.exc_off, d.exc_j, d.exc_s, d.n_pad, d.partial);
+                                               d.exc_off, d.exc_j, d.exc_m, d.exc_s, d.exc_tiles, d.n_pad,
+                                               d.partial);
 }
 
 template <class R>
@@ -1145,8 +1140,8 @@ void launch_energy(const Dev& d, cudaStream_t st) {
     dim3 grid(d.n_pad / kBlockI, d.nsplit);
     typedef typename Vec4T<R>::type V4;
     k_energy<R><<<grid, kBlockI, 0, st>>>(d.pp, (const V4*)d.posq, (const V4*)d.dipt, (const V4*)d.ind, d.yz, d.tctr,
-                                          d.text, d.pos, d.exc_off, d.exc_j, d.exc_m, d.exc_s, d.n_pad, d.partial,
-                                          d.energy_partial);
+                                          d.text, d.pos, d.exc_off, d.exc_j, d.exc_m, d.exc_s, d.exc_tiles, d.n_pad,
+                                          d.partial, d.energy_partial);
 }
 
 #define TDP_INSTANTIATE(R)                                                                                  \

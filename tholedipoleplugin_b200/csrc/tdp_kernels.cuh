@@ -30,8 +30,9 @@ struct Dev {
     // Covalent scale exceptions (both directions), CSR over atoms.
     int* exc_off = nullptr;
     int* exc_j = nullptr;
-    double* exc_m = nullptr;     // M scale - 1
-    double* exc_s = nullptr;     // I scale - 1
+    double* exc_m = nullptr;     // M scale of the pair
+    double* exc_s = nullptr;     // I scale of the pair
+    int2* exc_tiles = nullptr;   // per 32-atom tile: lowest and highest tile holding a listed partner
     // Torque-mapping users: for atom a, (frame atom, role) entries.
     int* users_off = nullptr;
     int2* users = nullptr;
