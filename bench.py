@@ -64,7 +64,8 @@ def parse():
     p.add_argument("--steps", type=int, default=20)
     p.add_argument("--warmup", type=int, default=3)
     p.add_argument("--impl", default="ours", choices=["ours", "reference"])
-    p.add_argument("--config", default="large", choices=["small", "medium", "large"])
+    p.add_argument("--config", default="large", choices=["small", "medium", "profile", "large"],
+                   help="small 648, medium 12,288, profile 41,472 (24^3 waters, kernel profiling), large 98,304 atoms")
     p.add_argument("--no-extras", action="store_true", help="only the timed MD (used under ncu)")
     return p.parse_args()
 
@@ -224,7 +225,7 @@ def run_reference(args):
     import multiprocessing as mp
     from oracle import oracle as O
     from tholedipoleplugin_b200 import systems as S
-    n_atoms = {"small": 648, "medium": 12288, "large": 98304}[args.config]
+    n_atoms = {"small": 648, "medium": 12288, "profile": 41472, "large": 98304}[args.config]
     cores = len(os.sched_getaffinity(0)) if hasattr(os, "sched_getaffinity") else os.cpu_count()
     base = {"metric": "ns/day", "unit": "ns/day", "impl": "reference", "n_gpus": args.gpus, "steps": args.steps,
             "warmup": args.warmup, "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
@@ -310,8 +311,9 @@ def run_ours(args):
         dist.all_reduce(t, op=dist.ReduceOp.MAX)
         return float(t.item())
 
-    make = {"small": S.config_small, "medium": S.config_medium, "large": S.config_large}[args.config]
-    system = make(seed={"small": 0, "medium": 1, "large": 2}[args.config] + 100 * rank)
+    make = {"small": S.config_small, "medium": S.config_medium, "large": S.config_large,
+            "profile": lambda seed: S.water_box(24, 9.936 * 24 / 32, seed=seed, cutoff=0.9)}[args.config]
+    system = make(seed={"small": 0, "medium": 1, "profile": 5, "large": 2}[args.config] + 100 * rank)
     n = system.n
     pairs = n * (n - 1) / 2
     K, W = args.steps, args.warmup

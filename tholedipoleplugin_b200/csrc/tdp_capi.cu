@@ -72,6 +72,16 @@ struct tdp_handle {
     // Host copies of the per-particle parameters.
     std::vector<double> charge, dip, alpha, thole;
     std::vector<int> axis;  // n*4
+    // Covalent scale exceptions by atom: (partner, M scale, I scale).
+    std::vector<std::vector<std::tuple<int, double, double>>> exc_user;
+    size_t n_exc = 0;
+    // Molecules (connected by covalent lists and axis atoms), CSR in index order;
+    // the field kernels order molecules along a Morton curve.
+    std::vector<int> comp_off, comp_atoms;
+    bool sorted = false;
+    int since_sort = 0;
+    int resort_interval = 1000;
+    std::vector<double> hpos;
 
     Dev d;
     std::vector<void*> owned;
@@ -235,6 +245,129 @@ void refresh_box(tdp_handle* h) {
             P.half_box_tol[k] = 0.5 * L - 16.0 * ulp;
         }
     }
+}
+
+// Union-find molecules over the covalent lists and axis atoms.
+void build_components(tdp_handle* h, const tdp_system_desc* desc) {
+    int n = h->n;
+    std::vector<int> parent(n);
+    for (int i = 0; i < n; i++) parent[i] = i;
+    auto find = [&](int a) {
+        while (parent[a] != a) a = parent[a] = parent[parent[a]];
+        return a;
+    };
+    auto unite = [&](int a, int b) {
+        if (a < 0 || b < 0 || a >= n || b >= n) return;
+        a = find(a);
+        b = find(b);
+        if (a != b) parent[std::max(a, b)] = std::min(a, b);
+    };
+    for (int i = 0; i < n; i++) {
+        unite(i, h->axis[4 * i + 1]);
+        unite(i, h->axis[4 * i + 2]);
+        unite(i, h->axis[4 * i + 3]);
+        for (int list = 0; list < 2; list++) {
+            const int32_t* off = list == 0 ? desc->covalent12_offsets : desc->covalent13_offsets;
+            const int32_t* atoms = list == 0 ? desc->covalent12_atoms : desc->covalent13_atoms;
+            if (!off) continue;
+            for (int p = off[i]; p < off[i + 1]; p++) unite(i, atoms[p]);
+        }
+    }
+    std::vector<int> root(n), count(n, 0);
+    for (int i = 0; i < n; i++) count[root[i] = find(i)]++;
+    std::vector<int> cid(n, -1);
+    int nc = 0;
+    for (int i = 0; i < n; i++)
+        if (root[i] == i) cid[i] = nc++;
+    h->comp_off.assign(nc + 1, 0);
+    for (int i = 0; i < n; i++) h->comp_off[cid[root[i]] + 1]++;
+    for (int c = 0; c < nc; c++) h->comp_off[c + 1] += h->comp_off[c];
+    std::vector<int> fill(h->comp_off.begin(), h->comp_off.end() - 1);
+    h->comp_atoms.assign(n, 0);
+    for (int i = 0; i < n; i++) h->comp_atoms[fill[cid[root[i]]]++] = i;
+}
+
+static inline uint64_t spread21(uint64_t v) {
+    v &= 0x1fffff;
+    v = (v | v << 32) & 0x1f00000000ffffull;
+    v = (v | v << 16) & 0x1f0000ff0000ffull;
+    v = (v | v << 8) & 0x100f00f00f00f00full;
+    v = (v | v << 4) & 0x10c30c30c30c30c3ull;
+    v = (v | v << 2) & 0x1249249249249249ull;
+    return v;
+}
+
+// Orders molecules along a Morton curve of their centroids (wrapped into the
+// box when periodic) and uploads order/rank plus the slot-indexed exception
+// tables.  Only the field kernels' memory layout changes; results are the
+// same up to summation order.
+void sort_atoms(tdp_handle* h) {
+    int n = h->n;
+    Dev& d = h->d;
+    h->hpos.resize(3 * (size_t)n);
+    TDP_CUDA(cudaMemcpyAsync(h->hpos.data(), d.pos, sizeof(double) * 3 * n, cudaMemcpyDeviceToHost, h->stream));
+    TDP_CUDA(cudaStreamSynchronize(h->stream));
+    int nc = (int)h->comp_off.size() - 1;
+    std::vector<double> cen(3 * (size_t)nc, 0.0);
+    double lo[3] = {INFINITY, INFINITY, INFINITY}, hi[3] = {-INFINITY, -INFINITY, -INFINITY};
+    for (int c = 0; c < nc; c++) {
+        int a0 = h->comp_off[c], a1 = h->comp_off[c + 1];
+        for (int k = 0; k < 3; k++) {
+            double sum = 0.0;
+            for (int a = a0; a < a1; a++) sum += h->hpos[3 * (size_t)h->comp_atoms[a] + k];
+            double v = sum / (a1 - a0);
+            double L = d.pp.box[k];
+            if (d.pp.periodic && L > 0.0) v -= L * std::floor(v / L);
+            if (!std::isfinite(v)) v = 0.0;
+            cen[3 * (size_t)c + k] = v;
+            lo[k] = std::min(lo[k], v);
+            hi[k] = std::max(hi[k], v);
+        }
+    }
+    std::vector<std::pair<uint64_t, int>> keys(nc);
+    for (int c = 0; c < nc; c++) {
+        uint64_t key = 0;
+        for (int k = 0; k < 3; k++) {
+            double span = hi[k] - lo[k];
+            double f = span > 0.0 ? (cen[3 * (size_t)c + k] - lo[k]) / span : 0.0;
+            uint64_t q = (uint64_t)std::min(std::max(f, 0.0) * 2097151.0, 2097151.0);
+            key |= spread21(q) << k;
+        }
+        keys[c] = {key, c};
+    }
+    std::stable_sort(keys.begin(), keys.end());
+    std::vector<int> order(d.n_pad, -1), rank(n);
+    int k = 0;
+    for (auto& kc : keys)
+        for (int a = h->comp_off[kc.second]; a < h->comp_off[kc.second + 1]; a++) {
+            int i = h->comp_atoms[a];
+            order[k] = i;
+            rank[i] = k++;
+        }
+    std::vector<int> off(n + 1, 0), ej;
+    std::vector<double> em, es;
+    std::vector<int2> etiles(d.n_pad / kTile, make_int2(1 << 30, -1));
+    for (int slot = 0; slot < n; slot++) {
+        for (auto& t : h->exc_user[order[slot]]) {
+            int js = rank[std::get<0>(t)];
+            ej.push_back(js);
+            em.push_back(std::get<1>(t));
+            es.push_back(std::get<2>(t));
+            int2& r = etiles[slot / kTile];
+            r.x = std::min(r.x, js / kTile);
+            r.y = std::max(r.y, js / kTile);
+        }
+        off[slot + 1] = (int)ej.size();
+    }
+    upload(d.order, order.data(), sizeof(int) * order.size());
+    upload(d.rank, rank.data(), sizeof(int) * n);
+    upload(d.exs_off, off.data(), sizeof(int) * (n + 1));
+    upload(d.exs_j, ej.data(), sizeof(int) * ej.size());
+    upload(d.exs_m, em.data(), sizeof(double) * em.size());
+    upload(d.exs_s, es.data(), sizeof(double) * es.size());
+    upload(d.exs_tiles, etiles.data(), sizeof(int2) * etiles.size());
+    h->sorted = true;
+    h->since_sort = 0;
 }
 
 template <class R>
@@ -493,6 +626,7 @@ void solve_at(tdp_handle* h, const void* positions, int dtype, int on_device) {
     if (positions) {
         check_box(h);
         stage_positions(h, positions, dtype, on_device);
+        if (!h->sorted || ++h->since_sort >= h->resort_interval) sort_atoms(h);
         if (h->precision == TDP_PRECISION_DOUBLE) setup_and_solve<double>(h);
         else setup_and_solve<float>(h);
         h->have_results = true;
@@ -593,7 +727,8 @@ int tdp_create(const tdp_system_desc* desc, tdp_handle** out) {
                 }
             }
         }
-        std::vector<std::vector<std::tuple<int, double, double>>> exc(n);
+        std::vector<std::vector<std::tuple<int, double, double>>>& exc = h->exc_user;
+        exc.assign(n, {});
         for (auto& kv : scales) {
             double m = kv.second.first, s = kv.second.second;
             if (m == 1.0 && s == 1.0) continue;
@@ -647,7 +782,6 @@ int tdp_create(const tdp_system_desc* desc, tdp_handle** out) {
         d.axis = dalloc<int4>(n, o);
         d.posq = dalloc<char>(rsz * d.n_pad, o);
         d.dipt = dalloc<char>(rsz * d.n_pad, o);
-        d.vec = dalloc<char>(rsz * d.n_pad, o);
         d.ind = dalloc<char>(rsz * d.n_pad, o);
         d.yz = dalloc<double2>(d.n_pad, o);
         d.tctr = dalloc<double4>(d.n_pad / kTile, o);
@@ -690,6 +824,22 @@ int tdp_create(const tdp_system_desc* desc, tdp_handle** out) {
         upload(d.exc_m, em.data(), sizeof(double) * em.size());
         upload(d.exc_s, es.data(), sizeof(double) * es.size());
         upload(d.exc_tiles, etiles.data(), sizeof(int2) * etiles.size());
+        h->n_exc = ej.size();
+        build_components(h, desc);
+        if (const char* e = getenv("TDP_RESORT_INTERVAL")) h->resort_interval = std::max(1, atoi(e));
+        d.order = dalloc<int>(d.n_pad, o);
+        d.rank = dalloc<int>(n, o);
+        d.pos_s = dalloc<double>(3 * (size_t)d.n_pad, o);
+        d.posq_s = dalloc<char>(rsz * d.n_pad, o);
+        d.dipt_s = dalloc<char>(rsz * d.n_pad, o);
+        d.vec_s = dalloc<char>(rsz * d.n_pad, o);
+        d.tctr_s = dalloc<double4>(d.n_pad / kTile, o);
+        d.text_s = dalloc<double4>(d.n_pad / kTile, o);
+        d.exs_off = dalloc<int>(n + 1, o);
+        d.exs_j = dalloc<int>(ej.size(), o);
+        d.exs_m = dalloc<double>(em.size(), o);
+        d.exs_s = dalloc<double>(es.size(), o);
+        d.exs_tiles = dalloc<int2>(d.n_pad / kTile, o);
         upload(d.coef, h->extrap.data(), sizeof(double) * h->extrap.size());
         upload_params(h);
         TDP_CUDA(cudaMallocHost(&h->h_scal, 64 * sizeof(double)));

@@ -69,6 +69,52 @@ __global__ void k_pack(int n, int n_tiles_pad, const double* __restrict__ pos, c
     yz[i] = make_double2(y, z);
 }
 
+// Same records in the spatially sorted order of the field kernels: slot k
+// holds atom order[k]; also the FP64 positions by slot.
+template <class R>
+__global__ void k_pack_sorted(int n_tiles_pad, const int* __restrict__ order, const double* __restrict__ pos,
+                              const double* __restrict__ charge, double4* __restrict__ tctr,
+                              double4* __restrict__ text, typename Vec4T<R>::type* __restrict__ posq,
+                              double* __restrict__ pos_s) {
+    int warp = (blockIdx.x * blockDim.x + threadIdx.x) >> 5;
+    int lane = threadIdx.x & 31;
+    if (warp >= n_tiles_pad) return;
+    int k = warp * kTile + lane;
+    int i = order[k];
+    bool valid = i >= 0;
+    double x = valid ? pos[3 * i] : 0.0, y = valid ? pos[3 * i + 1] : 0.0, z = valid ? pos[3 * i + 2] : 0.0;
+    int cnt = __popc(__ballot_sync(0xffffffffu, valid));
+    double cx = warp_sum(x), cy = warp_sum(y), cz = warp_sum(z);
+    if (cnt > 0) {
+        cx /= cnt;
+        cy /= cnt;
+        cz /= cnt;
+    }
+    double ex = valid ? fabs(x - cx) : 0.0, ey = valid ? fabs(y - cy) : 0.0, ez = valid ? fabs(z - cz) : 0.0;
+    ex = warp_max(ex);
+    ey = warp_max(ey);
+    ez = warp_max(ez);
+    if (lane == 0) {
+        tctr[warp] = make_double4(cx, cy, cz, 0.0);
+        text[warp] = make_double4(ex, ey, ez, 0.0);
+    }
+    typename Vec4T<R>::type p;
+    if (sizeof(R) == 4) {
+        p.x = (R)(valid ? x - cx : 0.0);
+        p.y = (R)(valid ? y - cy : 0.0);
+        p.z = (R)(valid ? z - cz : 0.0);
+    } else {
+        p.x = (R)(valid ? x : cx);
+        p.y = (R)(valid ? y : cy);
+        p.z = (R)(valid ? z : cz);
+    }
+    p.w = (R)(valid ? charge[i] : 0.0);
+    posq[k] = p;
+    pos_s[3 * k] = valid ? x : cx;
+    pos_s[3 * k + 1] = valid ? y : cy;
+    pos_s[3 * k + 2] = valid ? z : cz;
+}
+
 // ---------------------------------------------------------------------------
 // Local -> lab frame of the permanent dipoles: checkChiral (RTDF.cpp:432-467)
 // then applyRotationMatrixToParticle (RTDF.cpp:477-571), FP64.
@@ -93,7 +139,8 @@ __device__ __forceinline__ double normalize(d3& a) {
 template <class R>
 __global__ void k_rotate(int n, const double* __restrict__ pos, const double* __restrict__ dip_mol,
                          const int4* __restrict__ axis, const double* __restrict__ thole, double* __restrict__ lab,
-                         typename Vec4T<R>::type* __restrict__ dipt) {
+                         typename Vec4T<R>::type* __restrict__ dipt, const int* __restrict__ rank,
+                         typename Vec4T<R>::type* __restrict__ dipt_s) {
     int i = blockIdx.x * blockDim.x + threadIdx.x;
     if (i >= n) return;
     d3 d = ld3(dip_mol + 3 * i);
@@ -149,6 +196,7 @@ __global__ void k_rotate(int n, const double* __restrict__ pos, const double* __
     v.z = (R)d.z;
     v.w = (R)thole[i];
     dipt[i] = v;
+    dipt_s[rank[i]] = v;
 }
 
 // ---------------------------------------------------------------------------
@@ -160,6 +208,7 @@ __global__ void k_rotate(int n, const double* __restrict__ pos, const double* __
 struct TileGeom {
     double dcx, dcy, dcz;
     bool fold;
+    bool near;  // some pair may be within the Thole damping range
 };
 
 __device__ __forceinline__ TileGeom tile_geom(const PairParams& P, double4 cA, double4 eA, double4 cB, double4 eB) {
@@ -175,6 +224,12 @@ __device__ __forceinline__ TileGeom tile_geom(const PairParams& P, double4 cA, d
         g.fold = fabs(g.dcx) + eA.x + eB.x >= P.half_box_tol[0] || fabs(g.dcy) + eA.y + eB.y >= P.half_box_tol[1] ||
                  fabs(g.dcz) + eA.z + eB.z >= P.half_box_tol[2];
     }
+    // Smallest distance any pair of the two tiles can have (per dimension the
+    // gap between the tiles' boxes; folded pairs are never closer).
+    double gx = fmax(fabs(g.dcx) - eA.x - eB.x, 0.0);
+    double gy = fmax(fabs(g.dcy) - eA.y - eB.y, 0.0);
+    double gz = fmax(fabs(g.dcz) - eA.z - eB.z, 0.0);
+    g.near = g.fold || gx * gx + gy * gy + gz * gz < (double)P.damp_r2;
     return g;
 }
 
@@ -229,30 +284,25 @@ __device__ __forceinline__ R masked_r2(R r2, bool dirty, int i, int j, int n) {
 // Field kernels: KIND 0 = permanent field (j records: posq + lab dipole/thole),
 // KIND 1 = mutual-field matvec T*v (j records: posq + v/thole).
 // ---------------------------------------------------------------------------
-// Covalent scale of pair (i, j) from i's exception list (scale 1 if absent).
-__device__ __forceinline__ void pair_scales(const int* __restrict__ exc_j, const double* __restrict__ exc_m,
-                                            const double* __restrict__ exc_s, int e0, int e1, int j, double& m,
-                                            double& sc) {
-    m = 1.0;
-    sc = 1.0;
-    for (int e = e0; e < e1; e++)
-        if (exc_j[e] == j) {
-            m = exc_m[e];
-            sc = exc_s[e];
-        }
-}
-
 // SLOW subtiles are the diagonal tile, the ragged last tile and tiles holding
 // covalent partners of the warp's atoms: there self/padding pairs are masked
 // and each pair's M/I scale is applied in place, so excluded terms are never
 // formed.
-template <class R, int KIND, bool FOLD, bool SLOW>
+template <class R, int KIND, bool FOLD, bool SLOW, bool DAMP>
 __device__ __forceinline__ void field_subtile(const PairParams& P, const double* __restrict__ pos,
                                               const typename Vec4T<R>::type* __restrict__ sp,
                                               const typename Vec4T<R>::type* __restrict__ sv, int i, int jbase,
                                               R oix, R oiy, R oiz, R ti, R damp_r2, const int* __restrict__ exc_j,
                                               const double* __restrict__ exc_m, const double* __restrict__ exc_s,
                                               int e0, int e1, R& fx, R& fy, R& fz) {
+    // Bit jj set: j = jbase + jj is one of i's covalent partners; those pairs
+    // are left out of the loop and added once below with their scale.
+    unsigned partners = 0u;
+    if (SLOW)
+        for (int e = e0; e < e1; e++) {
+            unsigned off = (unsigned)(exc_j[e] - jbase);
+            if (off < (unsigned)kTile) partners |= 1u << off;
+        }
 #pragma unroll 4
     for (int jj = 0; jj < kTile; jj++) {
         typename Vec4T<R>::type pj = sp[jj];
@@ -261,25 +311,32 @@ __device__ __forceinline__ void field_subtile(const PairParams& P, const double*
         R dx, dy, dz;
         pair_delta<R, FOLD>(P, pos, i, j, pj.x, pj.y, pj.z, oix, oiy, oiz, dx, dy, dz);
         R r2 = dx * dx + dy * dy + dz * dz;
-        if (SLOW) {
-            r2 = masked_r2<R>(r2, true, i, j, P.n);
-            double m, sc;
-            pair_scales(exc_j, exc_m, exc_s, e0, e1, j, m, sc);
-            R scale = (R)(KIND == 0 ? m : sc);
+        if (SLOW && (j == i || j >= P.n || ((partners >> jj) & 1u))) r2 = (R)INFINITY;
+        if (KIND == 0)
+            pair_fixed<R, DAMP>(dx, dy, dz, r2, pj.w, vj.x, vj.y, vj.z, ti, vj.w, damp_r2, fx, fy, fz);
+        else
+            pair_matvec<R, DAMP>(dx, dy, dz, r2, vj.x, vj.y, vj.z, ti, vj.w, damp_r2, fx, fy, fz);
+    }
+    if (SLOW) {
+#pragma unroll 1
+        for (int e = e0; e < e1; e++) {
+            unsigned off = (unsigned)(exc_j[e] - jbase);
+            if (off >= (unsigned)kTile) continue;
+            R scale = (R)(KIND == 0 ? exc_m[e] : exc_s[e]);
             if (scale == R(0)) continue;
+            typename Vec4T<R>::type pj = sp[off];
+            typename Vec4T<R>::type vj = sv[off];
+            R dx, dy, dz;
+            pair_delta<R, FOLD>(P, pos, i, jbase + off, pj.x, pj.y, pj.z, oix, oiy, oiz, dx, dy, dz);
+            R r2 = dx * dx + dy * dy + dz * dz;
             R tx = 0, ty = 0, tz = 0;
             if (KIND == 0)
-                pair_fixed<R>(dx, dy, dz, r2, pj.w, vj.x, vj.y, vj.z, ti, vj.w, damp_r2, tx, ty, tz);
+                pair_fixed<R, true>(dx, dy, dz, r2, pj.w, vj.x, vj.y, vj.z, ti, vj.w, damp_r2, tx, ty, tz);
             else
-                pair_matvec<R>(dx, dy, dz, r2, vj.x, vj.y, vj.z, ti, vj.w, damp_r2, tx, ty, tz);
+                pair_matvec<R, true>(dx, dy, dz, r2, vj.x, vj.y, vj.z, ti, vj.w, damp_r2, tx, ty, tz);
             fx += scale * tx;
             fy += scale * ty;
             fz += scale * tz;
-        } else {
-            if (KIND == 0)
-                pair_fixed<R>(dx, dy, dz, r2, pj.w, vj.x, vj.y, vj.z, ti, vj.w, damp_r2, fx, fy, fz);
-            else
-                pair_matvec<R>(dx, dy, dz, r2, vj.x, vj.y, vj.z, ti, vj.w, damp_r2, fx, fy, fz);
         }
     }
 }
@@ -347,21 +404,20 @@ __global__ void __launch_bounds__(kBlockI) k_field(PairParams P, const typename 
             const V4* sp = s_pos + sub * kTile;
             const V4* sv = s_vec + sub * kTile;
             const int jbase = B * kTile;
-            if (g.fold) {
-                if (slow)
-                    field_subtile<R, KIND, true, true>(P, pos, sp, sv, i, jbase, oix, oiy, oiz, ti, damp_r2, exc_j,
-                                                       exc_m, exc_s, e0, e1, fx, fy, fz);
-                else
-                    field_subtile<R, KIND, true, false>(P, pos, sp, sv, i, jbase, oix, oiy, oiz, ti, damp_r2, exc_j,
-                                                        exc_m, exc_s, e0, e1, fx, fy, fz);
+#define TDP_FSUB(F, S, D)                                                                                        \
+    field_subtile<R, KIND, F, S, D>(P, pos, sp, sv, i, jbase, oix, oiy, oiz, ti, damp_r2, exc_j, exc_m, exc_s, e0, e1, \
+                                    fx, fy, fz)
+            if (slow) {
+                if (g.fold) TDP_FSUB(true, true, true);
+                else TDP_FSUB(false, true, true);
+            } else if (g.fold) {
+                TDP_FSUB(true, false, true);
+            } else if (g.near) {
+                TDP_FSUB(false, false, true);
             } else {
-                if (slow)
-                    field_subtile<R, KIND, false, true>(P, pos, sp, sv, i, jbase, oix, oiy, oiz, ti, damp_r2, exc_j,
-                                                        exc_m, exc_s, e0, e1, fx, fy, fz);
-                else
-                    field_subtile<R, KIND, false, false>(P, pos, sp, sv, i, jbase, oix, oiy, oiz, ti, damp_r2, exc_j,
-                                                         exc_m, exc_s, e0, e1, fx, fy, fz);
+                TDP_FSUB(false, false, false);
             }
+#undef TDP_FSUB
             ax += (double)fx;
             ay += (double)fy;
             az += (double)fz;
@@ -381,29 +437,47 @@ __device__ __forceinline__ void energy_subtile(const PairParams& P, const double
                                                const typename Vec4T<R>::type* __restrict__ sp,
                                                const typename Vec4T<R>::type* __restrict__ sd,
                                                const typename Vec4T<R>::type* __restrict__ su,
-                                               const double2* __restrict__ syz, int i, int jbase, R oix, R oiy, R oiz,
+                                               const double2* __restrict__ yz, int i, int jbase, R oix, R oiy, R oiz,
                                                double yi, double zi, const EAtom<R>& me, R damp_r2, R rv4p, R rv4f,
                                                bool upper, const int* __restrict__ exc_j,
                                                const double* __restrict__ exc_m, const double* __restrict__ exc_s,
                                                int e0, int e1, R& fx, R& fy, R& fz, R& tx, R& ty, R& tz, R& en) {
+    unsigned partners = 0u;
+    if (SLOW)
+        for (int e = e0; e < e1; e++) {
+            unsigned off = (unsigned)(exc_j[e] - jbase);
+            if (off < (unsigned)kTile) partners |= 1u << off;
+        }
+    // jj < kTile: the loop over the subtile (scale 1, partners masked out);
+    // afterwards, in SLOW subtiles, each covalent partner once with its scales.
+    int e = e0;
 #pragma unroll 1
-    for (int jj = 0; jj < kTile; jj++) {
-        typename Vec4T<R>::type pj = sp[jj], dj = sd[jj], uj = su[jj];
-        double2 yzj = syz[jj];
-        int j = jbase + jj;
+    for (int jj = 0; jj < kTile || (SLOW && e < e1); jj++) {
+        R mS = R(1), iS = R(1);
+        int jo = jj;
+        bool extra = jj >= kTile;
+        if (SLOW && extra) {
+            unsigned off = (unsigned)(exc_j[e] - jbase);
+            mS = (R)exc_m[e];
+            iS = (R)exc_s[e];
+            e++;
+            if (off >= (unsigned)kTile || (mS == R(0) && iS == R(0))) continue;
+            jo = (int)off;
+        }
+        typename Vec4T<R>::type pj = sp[jo], dj = sd[jo], uj = su[jo];
+        int j = jbase + jo;
         R dx, dy, dz;
         pair_delta<R, FOLD>(P, pos, i, j, pj.x, pj.y, pj.z, oix, oiy, oiz, dx, dy, dz);
         R r2 = dx * dx + dy * dy + dz * dz;
-        R mS = R(1), iS = R(1);
-        if (SLOW) {
-            r2 = masked_r2<R>(r2, true, i, j, P.n);
-            double m, sc;
-            pair_scales(exc_j, exc_m, exc_s, e0, e1, j, m, sc);
-            if (m == 0.0 && sc == 0.0) continue;
-            mS = (R)m;
-            iS = (R)sc;
+        if (SLOW && !extra && (j == i || j >= P.n || ((partners >> jj) & 1u))) r2 = (R)INFINITY;
+        // formQIRotationMatrix's test on the raw positions, pI.y != pK.y ||
+        // pI.z != pK.z (RTDF.cpp:584): displacements above 1e-5 nm decide it;
+        // below that the raw FP64 coordinates are compared.
+        bool yzd = fabs(dy) > R(1e-5) || fabs(dz) > R(1e-5);
+        if (!yzd) {
+            double2 yzj = yz[min(j, P.n_tiles * kTile - 1)];
+            yzd = (yi != yzj.x) || (zi != yzj.y);
         }
-        bool yzd = (yi != yzj.x) || (zi != yzj.y);
         EAtom<R> other;
         other.q = pj.w;
         other.mx = dj.x;
@@ -438,7 +512,6 @@ __global__ void __launch_bounds__(kBlockI) k_energy(PairParams P, const typename
     __shared__ V4 s_pos[kJStage];
     __shared__ V4 s_dip[kJStage];
     __shared__ V4 s_ind[kJStage];
-    __shared__ double2 s_yz[kJStage];
     __shared__ double4 s_ctr[kJStage / kTile];
     __shared__ double4 s_ext[kJStage / kTile];
     __shared__ double s_red[kBlockI / 32];
@@ -476,7 +549,6 @@ __global__ void __launch_bounds__(kBlockI) k_energy(PairParams P, const typename
             s_pos[k] = posq[j0 + k];
             s_dip[k] = dipt[j0 + k];
             s_ind[k] = indv[j0 + k];
-            s_yz[k] = yz[j0 + k];
         }
         if (threadIdx.x < kJStage / kTile) {
             s_ctr[threadIdx.x] = tctr[(j0 >> 5) + threadIdx.x];
@@ -507,7 +579,7 @@ __global__ void __launch_bounds__(kBlockI) k_energy(PairParams P, const typename
             const int o = sub * kTile;
             const int jbase = B * kTile;
 #define TDP_ESUB(F, S)                                                                                              \
-    energy_subtile<R, F, S>(P, pos, s_pos + o, s_dip + o, s_ind + o, s_yz + o, i, jbase, oix, oiy, oiz, yzi.x, yzi.y, \
+    energy_subtile<R, F, S>(P, pos, s_pos + o, s_dip + o, s_ind + o, yz, i, jbase, oix, oiy, oiz, yzi.x, yzi.y,       \
                             me, damp_r2, rv4p, rv4f, upper && !(S), exc_j, exc_m, exc_s, e0, e1, fx, fy, fz, tx, ty,  \
                             tz, en)
             if (g.fold) {
@@ -677,6 +749,7 @@ __global__ void k_torque_gather(int n, const double* __restrict__ pos, const int
 // ---------------------------------------------------------------------------
 // O(N) vector kernels of the solvers (FP64 vectors, deterministic reductions).
 // ---------------------------------------------------------------------------
+// Sum of the j-split partials of the field kernels for slot k.
 __device__ __forceinline__ d3 sum_partial3(const double* __restrict__ partial, int nsplit, int n_pad, int i) {
     d3 t = {0.0, 0.0, 0.0};
     for (int s = 0; s < nsplit; s++) {
@@ -701,13 +774,13 @@ __device__ __forceinline__ void store_vec(typename Vec4T<R>::type* v, int i, d3 
 // E = sum of permanent-field partials; mu = alpha*E (RTDF.cpp:743-746);
 // packs mu as the next matvec operand; CG start y = sqrt(alpha)*E.
 template <class R>
-__global__ void k_fixed_done(int n, int nsplit, int n_pad, const double* __restrict__ partial,
+__global__ void k_fixed_done(int n, const int* __restrict__ rank, int nsplit, int n_pad, const double* __restrict__ partial,
                              const double* __restrict__ alpha, const double* __restrict__ salpha,
                              const double* __restrict__ thole, double* __restrict__ E, double* __restrict__ mu,
                              double* __restrict__ y, typename Vec4T<R>::type* __restrict__ vec) {
     int i = blockIdx.x * blockDim.x + threadIdx.x;
     if (i >= n) return;
-    d3 e = sum_partial3(partial, nsplit, n_pad, i);
+    d3 e = sum_partial3(partial, nsplit, n_pad, rank[i]);
     E[3 * i] = e.x;
     E[3 * i + 1] = e.y;
     E[3 * i + 2] = e.z;
@@ -719,12 +792,12 @@ __global__ void k_fixed_done(int n, int nsplit, int n_pad, const double* __restr
     y[3 * i] = yy.x;
     y[3 * i + 1] = yy.y;
     y[3 * i + 2] = yy.z;
-    store_vec<R>(vec, i, m, thole[i]);
+    store_vec<R>(vec, rank[i], m, thole[i]);
 }
 
 // Warm start: y = mu / sqrt(alpha) (0 where alpha = 0); packs mu.
 template <class R>
-__global__ void k_warm_start(int n, const double* __restrict__ salpha, const double* __restrict__ thole,
+__global__ void k_warm_start(int n, const int* __restrict__ rank, const double* __restrict__ salpha, const double* __restrict__ thole,
                              const double* __restrict__ mu, double* __restrict__ y,
                              typename Vec4T<R>::type* __restrict__ vec) {
     int i = blockIdx.x * blockDim.x + threadIdx.x;
@@ -735,13 +808,13 @@ __global__ void k_warm_start(int n, const double* __restrict__ salpha, const dou
     y[3 * i] = yy.x;
     y[3 * i + 1] = yy.y;
     y[3 * i + 2] = yy.z;
-    store_vec<R>(vec, i, m, thole[i]);
+    store_vec<R>(vec, rank[i], m, thole[i]);
 }
 
 // True residual in y-space: r = sqrt(alpha)*(E + T mu) - y, with mu = sqrt(alpha)*y.
 // p = r, packs sqrt(alpha)*p; block partials of r.r and sum alpha|r|^2.
 template <class R>
-__global__ void k_cg_residual(int n, int nsplit, int n_pad, const double* __restrict__ partial,
+__global__ void k_cg_residual(int n, const int* __restrict__ rank, int nsplit, int n_pad, const double* __restrict__ partial,
                               const double* __restrict__ E, const double* __restrict__ salpha,
                               const double* __restrict__ thole, const double* __restrict__ y, double* __restrict__ r,
                               double* __restrict__ p, typename Vec4T<R>::type* __restrict__ vec,
@@ -750,7 +823,7 @@ __global__ void k_cg_residual(int n, int nsplit, int n_pad, const double* __rest
     int i = blockIdx.x * blockDim.x + threadIdx.x;
     double rr = 0.0, ee = 0.0;
     if (i < n) {
-        d3 t = sum_partial3(partial, nsplit, n_pad, i);
+        d3 t = sum_partial3(partial, nsplit, n_pad, rank[i]);
         double s = salpha[i];
         d3 rv = (ld3(E + 3 * i) + t) * s - ld3(y + 3 * i);
         r[3 * i] = rv.x;
@@ -759,7 +832,7 @@ __global__ void k_cg_residual(int n, int nsplit, int n_pad, const double* __rest
         p[3 * i] = rv.x;
         p[3 * i + 1] = rv.y;
         p[3 * i + 2] = rv.z;
-        store_vec<R>(vec, i, rv * s, thole[i]);
+        store_vec<R>(vec, rank[i], rv * s, thole[i]);
         rr = dot(rv, rv);
         ee = s * s * rr;
     }
@@ -772,14 +845,14 @@ __global__ void k_cg_residual(int n, int nsplit, int n_pad, const double* __rest
 }
 
 // q = p - sqrt(alpha) * (T sqrt(alpha) p); block partials of p.q.
-__global__ void k_cg_q(int n, int nsplit, int n_pad, const double* __restrict__ partial,
+__global__ void k_cg_q(int n, const int* __restrict__ rank, int nsplit, int n_pad, const double* __restrict__ partial,
                        const double* __restrict__ salpha, const double* __restrict__ p, double* __restrict__ q,
                        double* __restrict__ pq_part) {
     __shared__ double red[40];
     int i = blockIdx.x * blockDim.x + threadIdx.x;
     double pq = 0.0;
     if (i < n) {
-        d3 t = sum_partial3(partial, nsplit, n_pad, i);
+        d3 t = sum_partial3(partial, nsplit, n_pad, rank[i]);
         d3 pv = ld3(p + 3 * i);
         d3 qv = pv - t * salpha[i];
         q[3 * i] = qv.x;
@@ -826,7 +899,7 @@ __global__ void k_cg_update(int n, int nblk, const double* __restrict__ scal_rr,
 // also p = r + (rr'/scal_rr[prev]) p and packs sqrt(alpha)*p for the next
 // matvec.
 template <class R>
-__global__ void k_cg_p(int n, int nblk, int prev, int slot, double* __restrict__ scal_rr,
+__global__ void k_cg_p(int n, const int* __restrict__ rank, int nblk, int prev, int slot, double* __restrict__ scal_rr,
                        double* __restrict__ scal_eps, const double* __restrict__ rr_part,
                        const double* __restrict__ eps_part, const double* __restrict__ salpha,
                        const double* __restrict__ thole, const double* __restrict__ r, double* __restrict__ p,
@@ -846,13 +919,13 @@ __global__ void k_cg_p(int n, int nblk, int prev, int slot, double* __restrict__
         p[3 * i] = pv.x;
         p[3 * i + 1] = pv.y;
         p[3 * i + 2] = pv.z;
-        store_vec<R>(vec, i, pv * salpha[i], thole[i]);
+        store_vec<R>(vec, rank[i], pv * salpha[i], thole[i]);
     }
 }
 
 // mu = sqrt(alpha) y; packs mu.
 template <class R>
-__global__ void k_cg_mu(int n, const double* __restrict__ salpha, const double* __restrict__ thole,
+__global__ void k_cg_mu(int n, const int* __restrict__ rank, const double* __restrict__ salpha, const double* __restrict__ thole,
                         const double* __restrict__ y, double* __restrict__ mu,
                         typename Vec4T<R>::type* __restrict__ vec) {
     int i = blockIdx.x * blockDim.x + threadIdx.x;
@@ -861,13 +934,13 @@ __global__ void k_cg_mu(int n, const double* __restrict__ salpha, const double* 
     mu[3 * i] = m.x;
     mu[3 * i + 1] = m.y;
     mu[3 * i + 2] = m.z;
-    store_vec<R>(vec, i, m, thole[i]);
+    store_vec<R>(vec, rank[i], m, thole[i]);
 }
 
 // One Jacobi sweep of convergeInducedDipolesByDIIS (RTDF.cpp:838-846):
 // mu' = alpha (E + T mu); block partials of |mu' - mu|^2; packs mu'.
 template <class R>
-__global__ void k_jacobi(int n, int nsplit, int n_pad, const double* __restrict__ partial,
+__global__ void k_jacobi(int n, const int* __restrict__ rank, int nsplit, int n_pad, const double* __restrict__ partial,
                          const double* __restrict__ E, const double* __restrict__ alpha,
                          const double* __restrict__ thole, double* __restrict__ mu,
                          typename Vec4T<R>::type* __restrict__ vec, double* __restrict__ eps_part) {
@@ -875,14 +948,14 @@ __global__ void k_jacobi(int n, int nsplit, int n_pad, const double* __restrict_
     int i = blockIdx.x * blockDim.x + threadIdx.x;
     double ee = 0.0;
     if (i < n) {
-        d3 t = sum_partial3(partial, nsplit, n_pad, i);
+        d3 t = sum_partial3(partial, nsplit, n_pad, rank[i]);
         d3 nw = (ld3(E + 3 * i) + t) * alpha[i];
         d3 dl = nw - ld3(mu + 3 * i);
         ee = dot(dl, dl);
         mu[3 * i] = nw.x;
         mu[3 * i + 1] = nw.y;
         mu[3 * i + 2] = nw.z;
-        store_vec<R>(vec, i, nw, thole[i]);
+        store_vec<R>(vec, rank[i], nw, thole[i]);
     }
     ee = block_sum(ee, red);
     if (threadIdx.x == 0) eps_part[blockIdx.x] = ee;
@@ -890,13 +963,13 @@ __global__ void k_jacobi(int n, int nsplit, int n_pad, const double* __restrict_
 
 // Extrapolation (RTDF.cpp:876-887): mu = alpha (E + T mu), stored as order k.
 template <class R>
-__global__ void k_extrap_step(int n, int nsplit, int n_pad, const double* __restrict__ partial,
+__global__ void k_extrap_step(int n, const int* __restrict__ rank, int nsplit, int n_pad, const double* __restrict__ partial,
                               const double* __restrict__ E, const double* __restrict__ alpha,
                               const double* __restrict__ thole, double* __restrict__ mu, double* __restrict__ hist_k,
                               typename Vec4T<R>::type* __restrict__ vec) {
     int i = blockIdx.x * blockDim.x + threadIdx.x;
     if (i >= n) return;
-    d3 t = sum_partial3(partial, nsplit, n_pad, i);
+    d3 t = sum_partial3(partial, nsplit, n_pad, rank[i]);
     d3 nw = (ld3(E + 3 * i) + t) * alpha[i];
     mu[3 * i] = nw.x;
     mu[3 * i + 1] = nw.y;
@@ -904,12 +977,12 @@ __global__ void k_extrap_step(int n, int nsplit, int n_pad, const double* __rest
     hist_k[3 * i] = nw.x;
     hist_k[3 * i + 1] = nw.y;
     hist_k[3 * i + 2] = nw.z;
-    store_vec<R>(vec, i, nw, thole[i]);
+    store_vec<R>(vec, rank[i], nw, thole[i]);
 }
 
 // mu = sum_k c_k mu_k (RTDF.cpp:890-895); packs mu.
 template <class R>
-__global__ void k_extrap_combine(int n, int korder, const double* __restrict__ coef, const double* __restrict__ hist,
+__global__ void k_extrap_combine(int n, const int* __restrict__ rank, int korder, const double* __restrict__ coef, const double* __restrict__ hist,
                                  const double* __restrict__ thole, double* __restrict__ mu,
                                  typename Vec4T<R>::type* __restrict__ vec) {
     int i = blockIdx.x * blockDim.x + threadIdx.x;
@@ -919,18 +992,18 @@ __global__ void k_extrap_combine(int n, int korder, const double* __restrict__ c
     mu[3 * i] = m.x;
     mu[3 * i + 1] = m.y;
     mu[3 * i + 2] = m.z;
-    store_vec<R>(vec, i, m, thole[i]);
+    store_vec<R>(vec, rank[i], m, thole[i]);
 }
 
 // Block partials of |alpha (E + T mu) - mu|^2 (RTDF.cpp:898-906).
-__global__ void k_step_eps(int n, int nsplit, int n_pad, const double* __restrict__ partial,
+__global__ void k_step_eps(int n, const int* __restrict__ rank, int nsplit, int n_pad, const double* __restrict__ partial,
                            const double* __restrict__ E, const double* __restrict__ alpha,
                            const double* __restrict__ mu, double* __restrict__ eps_part) {
     __shared__ double red[40];
     int i = blockIdx.x * blockDim.x + threadIdx.x;
     double ee = 0.0;
     if (i < n) {
-        d3 t = sum_partial3(partial, nsplit, n_pad, i);
+        d3 t = sum_partial3(partial, nsplit, n_pad, rank[i]);
         d3 dl = (ld3(E + 3 * i) + t) * alpha[i] - ld3(mu + 3 * i);
         ee = dot(dl, dl);
     }
@@ -1113,25 +1186,29 @@ void launch_pack(const Dev& d, cudaStream_t st) {
     int warps = d.n_pad / kTile;
     k_pack<R><<<nblk(warps * 32, threads), threads, 0, st>>>(
         d.n, warps, d.pos, d.charge, d.tctr, d.text, (typename Vec4T<R>::type*)d.posq, d.yz);
+    k_pack_sorted<R><<<nblk(warps * 32, threads), threads, 0, st>>>(
+        warps, d.order, d.pos, d.charge, d.tctr_s, d.text_s, (typename Vec4T<R>::type*)d.posq_s, d.pos_s);
 }
 
 template <class R>
 void launch_rotate(const Dev& d, cudaStream_t st) {
     k_rotate<R><<<nblk(d.n, kVecThreads), kVecThreads, 0, st>>>(d.n, d.pos, d.dip_mol, d.axis, d.thole, d.lab,
-                                                                 (typename Vec4T<R>::type*)d.dipt);
+                                                                 (typename Vec4T<R>::type*)d.dipt, d.rank,
+                                                                 (typename Vec4T<R>::type*)d.dipt_s);
 }
 
 template <class R>
 void launch_field(const Dev& d, int kind, cudaStream_t st) {
     dim3 grid(d.n_pad / kBlockI, d.nsplit);
     typedef typename Vec4T<R>::type V4;
+    // Field kernels run on the spatially sorted records.
     if (kind == 0)
-        k_field<R, 0><<<grid, kBlockI, 0, st>>>(d.pp, (const V4*)d.posq, (const V4*)d.dipt, d.tctr, d.text, d.pos,
-                                               d.exc_off, d.exc_j, d.exc_m, d.exc_s, d.exc_tiles, d.n_pad,
+        k_field<R, 0><<<grid, kBlockI, 0, st>>>(d.pp, (const V4*)d.posq_s, (const V4*)d.dipt_s, d.tctr_s, d.text_s,
+                                               d.pos_s, d.exs_off, d.exs_j, d.exs_m, d.exs_s, d.exs_tiles, d.n_pad,
                                                d.partial);
     else
-        k_field<R, 1><<<grid, kBlockI, 0, st>>>(d.pp, (const V4*)d.posq, (const V4*)d.vec, d.tctr, d.text, d.pos,
-                                               d.exc_off, d.exc_j, d.exc_m, d.exc_s, d.exc_tiles, d.n_pad,
+        k_field<R, 1><<<grid, kBlockI, 0, st>>>(d.pp, (const V4*)d.posq_s, (const V4*)d.vec_s, d.tctr_s, d.text_s,
+                                               d.pos_s, d.exs_off, d.exs_j, d.exs_m, d.exs_s, d.exs_tiles, d.n_pad,
                                                d.partial);
 }
 
@@ -1155,22 +1232,22 @@ TDP_INSTANTIATE(double)
 
 template <class R>
 void launch_fixed_done(const Dev& d, cudaStream_t st) {
-    k_fixed_done<R><<<nblk(d.n, kVecThreads), kVecThreads, 0, st>>>(d.n, d.nsplit, d.n_pad, d.partial, d.alpha,
+    k_fixed_done<R><<<nblk(d.n, kVecThreads), kVecThreads, 0, st>>>(d.n, d.rank, d.nsplit, d.n_pad, d.partial, d.alpha,
                                                                      d.salpha, d.thole, d.E, d.mu, d.y,
-                                                                     (typename Vec4T<R>::type*)d.vec);
+                                                                     (typename Vec4T<R>::type*)d.vec_s);
 }
 template <class R>
 void launch_warm_start(const Dev& d, cudaStream_t st) {
-    k_warm_start<R><<<nblk(d.n, kVecThreads), kVecThreads, 0, st>>>(d.n, d.salpha, d.thole, d.mu, d.y,
-                                                                     (typename Vec4T<R>::type*)d.vec);
+    k_warm_start<R><<<nblk(d.n, kVecThreads), kVecThreads, 0, st>>>(d.n, d.rank, d.salpha, d.thole, d.mu, d.y,
+                                                                     (typename Vec4T<R>::type*)d.vec_s);
 }
 template <class R>
 void launch_cg_residual(const Dev& d, cudaStream_t st) {
-    k_cg_residual<R><<<d.nvb, kVecThreads, 0, st>>>(d.n, d.nsplit, d.n_pad, d.partial, d.E, d.salpha, d.thole, d.y,
-                                                    d.r, d.p, (typename Vec4T<R>::type*)d.vec, d.rr_part, d.eps_part);
+    k_cg_residual<R><<<d.nvb, kVecThreads, 0, st>>>(d.n, d.rank, d.nsplit, d.n_pad, d.partial, d.E, d.salpha, d.thole, d.y,
+                                                    d.r, d.p, (typename Vec4T<R>::type*)d.vec_s, d.rr_part, d.eps_part);
 }
 void launch_cg_q(const Dev& d, cudaStream_t st) {
-    k_cg_q<<<d.nvb, kVecThreads, 0, st>>>(d.n, d.nsplit, d.n_pad, d.partial, d.salpha, d.p, d.q, d.pq_part);
+    k_cg_q<<<d.nvb, kVecThreads, 0, st>>>(d.n, d.rank, d.nsplit, d.n_pad, d.partial, d.salpha, d.p, d.q, d.pq_part);
 }
 void launch_cg_update(const Dev& d, int slot, cudaStream_t st) {
     k_cg_update<<<d.nvb, kVecThreads, 0, st>>>(d.n, d.nvb, d.scal_rr, slot, d.pq_part, d.salpha, d.p, d.q, d.y, d.r,
@@ -1178,30 +1255,30 @@ void launch_cg_update(const Dev& d, int slot, cudaStream_t st) {
 }
 template <class R>
 void launch_cg_p(const Dev& d, int prev, int slot, cudaStream_t st) {
-    k_cg_p<R><<<d.nvb, kVecThreads, 0, st>>>(d.n, d.nvb, prev, slot, d.scal_rr, d.scal_eps, d.rr_part, d.eps_part, d.salpha,
-                                             d.thole, d.r, d.p, (typename Vec4T<R>::type*)d.vec);
+    k_cg_p<R><<<d.nvb, kVecThreads, 0, st>>>(d.n, d.rank, d.nvb, prev, slot, d.scal_rr, d.scal_eps, d.rr_part, d.eps_part, d.salpha,
+                                             d.thole, d.r, d.p, (typename Vec4T<R>::type*)d.vec_s);
 }
 template <class R>
 void launch_cg_mu(const Dev& d, cudaStream_t st) {
-    k_cg_mu<R><<<d.nvb, kVecThreads, 0, st>>>(d.n, d.salpha, d.thole, d.y, d.mu, (typename Vec4T<R>::type*)d.vec);
+    k_cg_mu<R><<<d.nvb, kVecThreads, 0, st>>>(d.n, d.rank, d.salpha, d.thole, d.y, d.mu, (typename Vec4T<R>::type*)d.vec_s);
 }
 template <class R>
 void launch_jacobi(const Dev& d, cudaStream_t st) {
-    k_jacobi<R><<<d.nvb, kVecThreads, 0, st>>>(d.n, d.nsplit, d.n_pad, d.partial, d.E, d.alpha, d.thole, d.mu,
-                                               (typename Vec4T<R>::type*)d.vec, d.eps_part);
+    k_jacobi<R><<<d.nvb, kVecThreads, 0, st>>>(d.n, d.rank, d.nsplit, d.n_pad, d.partial, d.E, d.alpha, d.thole, d.mu,
+                                               (typename Vec4T<R>::type*)d.vec_s, d.eps_part);
 }
 template <class R>
 void launch_extrap_step(const Dev& d, int k, cudaStream_t st) {
-    k_extrap_step<R><<<d.nvb, kVecThreads, 0, st>>>(d.n, d.nsplit, d.n_pad, d.partial, d.E, d.alpha, d.thole, d.mu,
-                                                    d.hist + (size_t)k * 3 * d.n, (typename Vec4T<R>::type*)d.vec);
+    k_extrap_step<R><<<d.nvb, kVecThreads, 0, st>>>(d.n, d.rank, d.nsplit, d.n_pad, d.partial, d.E, d.alpha, d.thole, d.mu,
+                                                    d.hist + (size_t)k * 3 * d.n, (typename Vec4T<R>::type*)d.vec_s);
 }
 template <class R>
 void launch_extrap_combine(const Dev& d, int korder, const double* coef, cudaStream_t st) {
-    k_extrap_combine<R><<<d.nvb, kVecThreads, 0, st>>>(d.n, korder, coef, d.hist, d.thole, d.mu,
-                                                       (typename Vec4T<R>::type*)d.vec);
+    k_extrap_combine<R><<<d.nvb, kVecThreads, 0, st>>>(d.n, d.rank, korder, coef, d.hist, d.thole, d.mu,
+                                                       (typename Vec4T<R>::type*)d.vec_s);
 }
 void launch_step_eps(const Dev& d, cudaStream_t st) {
-    k_step_eps<<<d.nvb, kVecThreads, 0, st>>>(d.n, d.nsplit, d.n_pad, d.partial, d.E, d.alpha, d.mu, d.eps_part);
+    k_step_eps<<<d.nvb, kVecThreads, 0, st>>>(d.n, d.rank, d.nsplit, d.n_pad, d.partial, d.E, d.alpha, d.mu, d.eps_part);
 }
 void launch_eps_scalar(const Dev& d, int slot, cudaStream_t st) {
     k_eps_scalar<<<1, kVecThreads, 0, st>>>(d.n, d.nvb, d.eps_part, d.scal_eps, slot);

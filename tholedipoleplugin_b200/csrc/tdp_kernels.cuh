@@ -22,7 +22,6 @@ struct Dev {
     // Packed pair-kernel records, Vec4<R> of n_pad entries.
     void* posq = nullptr;        // mixed: (offset from tile centre, q); plain: (x, y, z, q)
     void* dipt = nullptr;        // (lab dipole, thole)
-    void* vec = nullptr;         // (matvec operand, thole)
     void* ind = nullptr;         // (induced dipole, 0)
     double2* yz = nullptr;       // n_pad raw (y, z) for the QI frame test
     double4* tctr = nullptr;     // n_pad/32 tile centres
@@ -33,6 +32,21 @@ struct Dev {
     double* exc_m = nullptr;     // M scale of the pair
     double* exc_s = nullptr;     // I scale of the pair
     int2* exc_tiles = nullptr;   // per 32-atom tile: lowest and highest tile holding a listed partner
+    // Spatially sorted copies for the field kernels (permanent field, matvec):
+    // slot k holds atom order[k] (-1 for padding), atom i sits in slot rank[i].
+    int* order = nullptr;        // n_pad
+    int* rank = nullptr;         // n
+    double* pos_s = nullptr;     // n_pad*3
+    void* posq_s = nullptr;      // Vec4<R>: (offset from tile centre, q)
+    void* dipt_s = nullptr;      // Vec4<R>: (lab dipole, thole)
+    void* vec_s = nullptr;       // Vec4<R>: (matvec operand, thole)
+    double4* tctr_s = nullptr;
+    double4* text_s = nullptr;
+    int* exs_off = nullptr;      // exceptions by slot, partners as slots
+    int* exs_j = nullptr;
+    double* exs_m = nullptr;
+    double* exs_s = nullptr;
+    int2* exs_tiles = nullptr;
     // Torque-mapping users: for atom a, (frame atom, role) entries.
     int* users_off = nullptr;
     int2* users = nullptr;

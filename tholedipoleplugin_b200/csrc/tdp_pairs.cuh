@@ -19,7 +19,7 @@ __device__ __forceinline__ void damp_field(R r2, R rinv, R ti, R tj, R damp_r2, 
         if (dmp != R(0)) {
             R pgamma = ti < tj ? ti : tj;
             R r = r2 * rinv;
-            R ratio = r / dmp;
+            R ratio = sizeof(R) == 4 ? (R)__fdividef((float)r, (float)dmp) : r / dmp;
             ratio = ratio * ratio * ratio;
             R damp = -pgamma * ratio;
             if (damp > R(-50)) {
@@ -33,14 +33,14 @@ __device__ __forceinline__ void damp_field(R r2, R rinv, R ti, R tj, R damp_r2, 
 
 // One term of the mutual field (T mu)_i, calculateInducedDipolePairIxn with
 // rr3 -> -rr3 (RTDF.cpp:766-818), I scale applied by the caller.
-template <class R>
+template <class R, bool DAMP = true>
 __device__ __forceinline__ void pair_matvec(R dx, R dy, R dz, R r2, R vx, R vy, R vz, R ti, R tj, R damp_r2,
                                             R& fx, R& fy, R& fz) {
     R rinv = rsqrt_r(r2);
     R rinv2 = rinv * rinv;
     R rr3 = rinv * rinv2;
     R rr5 = R(3) * rr3 * rinv2;
-    damp_field(r2, rinv, ti, tj, damp_r2, rr3, rr5);
+    if (DAMP) damp_field(r2, rinv, ti, tj, damp_r2, rr3, rr5);
     R dd = rr5 * (vx * dx + vy * dy + vz * dz);
     fx += dd * dx - rr3 * vx;
     fy += dd * dy - rr3 * vy;
@@ -50,14 +50,14 @@ __device__ __forceinline__ void pair_matvec(R dx, R dy, R dz, R r2, R vx, R vy, 
 // One term of the permanent field at i from the charge and lab-frame dipole of
 // j, calculateFixedDipoleFieldPairIxn (RTDF.cpp:678-713), M scale applied by
 // the caller:  E_i -= d (rr3 q_j - rr5 mu_j.d) + mu_j rr3.
-template <class R>
+template <class R, bool DAMP = true>
 __device__ __forceinline__ void pair_fixed(R dx, R dy, R dz, R r2, R qj, R mx, R my, R mz, R ti, R tj, R damp_r2,
                                            R& fx, R& fy, R& fz) {
     R rinv = rsqrt_r(r2);
     R rinv2 = rinv * rinv;
     R rr3 = rinv * rinv2;
     R rr5 = R(3) * rr3 * rinv2;
-    damp_field(r2, rinv, ti, tj, damp_r2, rr3, rr5);
+    if (DAMP) damp_field(r2, rinv, ti, tj, damp_r2, rr3, rr5);
     R f = rr3 * qj - rr5 * (mx * dx + my * dy + mz * dz);
     fx -= dx * f + mx * rr3;
     fy -= dy * f + my * rr3;
@@ -95,7 +95,7 @@ __device__ __forceinline__ void pair_energy(R dx, R dy, R dz, R r2, bool yz_diff
     xz -= zz * dt;
     R xn2 = xx * xx + xy * xy + xz * xz;
     if (xn2 > R(0)) {
-        R s = R(1) / sqrt_r(xn2);
+        R s = rsqrt_r(xn2);
         xx *= s;
         xy *= s;
         xz *= s;
@@ -129,7 +129,7 @@ __device__ __forceinline__ void pair_energy(R dx, R dy, R dz, R r2, bool yz_diff
         if (fabs(dmp) > R(1.0e-5)) {
             R a = I.t < K.t ? I.t : K.t;
             R r = r2 * rinv;
-            R u = r / dmp;
+            R u = sizeof(R) == 4 ? (R)__fdividef((float)r, (float)dmp) : r / dmp;
             R au3 = a * u * u * u;
             R e = exp_r(-au3);
             tc = R(1) - e;
