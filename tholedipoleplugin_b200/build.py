@@ -32,8 +32,19 @@ def _stale() -> bool:
     return any(os.path.getmtime(d) > t for d in deps if os.path.isfile(d))
 
 
+def _adapter_stale() -> bool:
+    outs = [ADAPTER_LIB, ADAPTER_DRIVER]
+    if not all(os.path.exists(o) for o in outs):
+        return True
+    t = min(os.path.getmtime(o) for o in outs)
+    deps = [LIB] + [os.path.join(dp, f) for dp, _, fs in os.walk(ADAPTER) for f in fs]
+    return any(os.path.getmtime(d) > t for d in deps if os.path.isfile(d))
+
+
 def build(force: bool = False, verbose: bool = False) -> str:
     if not force and not _stale():
+        if _adapter_stale():
+            build_adapter(verbose)
         return LIB
     objs = []
     build_dir = os.path.join(HERE, "_build")
@@ -54,7 +65,33 @@ def build(force: bool = False, verbose: bool = False) -> str:
     tmp = LIB + ".tmp"
     subprocess.run([nvcc(), *ARCH, "-shared", "-o", tmp, *objs, "-lcudart"], check=True)
     os.replace(tmp, LIB)
+    build_adapter(verbose)
     return LIB
+
+
+ADAPTER = os.path.join(HERE, "openmm_adapter")
+ADAPTER_LIB = os.path.join(HERE, "libtholedipole_b200_openmm.so")
+ADAPTER_DRIVER = os.path.join(HERE, "_build", "adapter_driver")
+
+
+def build_adapter(verbose: bool = False) -> str:
+    """The OpenMM-facing kernel adapter (CudaCalcTholeDipoleForceKernel, its
+    factory and registration symbols) over the C ABI, built here against the
+    OpenMM stand-in headers, plus its test driver."""
+    inc = ["-I", os.path.join(ADAPTER, "standin"), "-I", os.path.join(ADAPTER, "plugin"), "-I", ADAPTER,
+           "-I", os.path.join(ROOT, "include")]
+    srcs = [os.path.join(ADAPTER, f) for f in ("CudaTholeDipoleKernels.cpp", "CudaTholeDipoleKernelFactory.cpp")]
+    srcs += [os.path.join(ADAPTER, "plugin", "TholeDipoleForce.cpp"), os.path.join(ADAPTER, "standin", "openmm_standin.cpp")]
+    cmd = ["g++", "-std=c++17", "-O2", "-fPIC", "-shared", *inc, "-o", ADAPTER_LIB, *srcs, "-L", HERE,
+           "-ltholedipole_b200", "-Wl,-rpath,$ORIGIN"]
+    if verbose:
+        print(" ".join(cmd), file=sys.stderr)
+    subprocess.run(cmd, check=True)
+    os.makedirs(os.path.dirname(ADAPTER_DRIVER), exist_ok=True)
+    cmd = ["g++", "-std=c++17", "-O2", *inc, "-o", ADAPTER_DRIVER, os.path.join(ADAPTER, "adapter_driver.cpp"),
+           "-L", HERE, "-ltholedipole_b200_openmm", "-ltholedipole_b200", "-Wl,-rpath," + HERE]
+    subprocess.run(cmd, check=True)
+    return ADAPTER_LIB
 
 
 if __name__ == "__main__":
