@@ -226,6 +226,18 @@ int tdp_get_pme_parameters(const tdp_handle* h, double* alpha, int32_t* nx, int3
 int tdp_solver_stats(const tdp_handle* h, int32_t* iterations, double* epsilon, int32_t* converged,
                      int32_t* status);
 
+/* Reverse mode of the last tdp_compute (its positions and parameters):
+ * gradients of  L = dL_dE * E + sum_i dL_dF_i . F_i  (F the total force,
+ * torque mapping included) with respect to every particle's charge,
+ * polarizability, Thole factor and molecular-frame dipole.  dL_dF: n*3 host
+ * doubles (NULL = zero); grads: n*6 host doubles, per particle
+ * (dq, dalpha, dthole, dmu_mol_x, dmu_mol_y, dmu_mol_z).  Mutual polarization
+ * costs one adjoint solve of the same symmetric (alpha^-1 - T) system; pair
+ * damping terms are recomputed, not stored.  The plugin has no counterpart:
+ * this is the backward of the torch.autograd.Function in the Python layer.
+ * Direct and Mutual polarization (TDP_ERR_UNSUPPORTED for Extrapolated). */
+int tdp_adjoint(tdp_handle* h, const double* dL_dF, double dL_dE, double* grads);
+
 /* Device timing of the last tdp_compute (CUDA events on the handle's stream),
  * recorded only after tdp_enable_timing(h, 1).  out[TDP_NUM_STAGE_TIMES]:
  * [0] pack+rotation ms, [1] permanent field ms, [2] induced-dipole solve ms,

@@ -73,6 +73,7 @@ PROTOTYPES = {
                                         C.c_int32, _dp, C.c_void_p, C.c_void_p]),
     "tdp_get_pme_parameters": (C.c_int, [C.c_void_p, _dp, _ip, _ip, _ip]),
     "tdp_solver_stats": (C.c_int, [C.c_void_p, _ip, _dp, _ip, _ip]),
+    "tdp_adjoint": (C.c_int, [C.c_void_p, C.c_void_p, C.c_double, _dp]),
     "tdp_enable_timing": (C.c_int, [C.c_void_p, C.c_int32]),
     "tdp_stage_times": (C.c_int, [C.c_void_p, _dp]),
     "tdp_md_kick_drift": (C.c_int, [C.c_int32, C.c_double, C.c_double, C.c_double, C.c_double, C.c_double,

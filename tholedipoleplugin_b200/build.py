@@ -12,7 +12,7 @@ HERE = os.path.dirname(os.path.abspath(__file__))
 ROOT = os.path.dirname(HERE)
 CSRC = os.path.join(HERE, "csrc")
 LIB = os.path.join(HERE, "libtholedipole_b200.so")
-SOURCES = ["tdp_kernels.cu", "tdp_capi.cu", "tdp_md.cu", "tdp_noalloc.cu"]
+SOURCES = ["tdp_kernels.cu", "tdp_capi.cu", "tdp_md.cu", "tdp_noalloc.cu", "tdp_adjoint.cu"]
 ARCH = ["-gencode", "arch=compute_100a,code=sm_100a"]
 
 

@@ -108,6 +108,11 @@ struct tdp_handle {
     double stage_ms[TDP_NUM_STAGE_TIMES] = {};
     long launches = 0;
 
+    // Adjoint work buffers (allocated on first use).
+    double* adj = nullptr;
+    double adj_eps = 0.0;
+    int adj_iterations = 0;
+
     std::string err;
 };
 
@@ -635,9 +640,114 @@ void solve_at(tdp_handle* h, const void* positions, int dtype, int on_device) {
     }
 }
 
+// Reverse mode of one evaluation (tdp_adjoint.cu has the kernels and the
+// derivation).  Needs the state of the last evaluation (positions, lab-frame
+// and induced dipoles, permanent field); leaves it as it was.
+template <class R>
+void run_adjoint(tdp_handle* h, const double* g_host, double gE, double* out_host) {
+    Dev& d = h->d;
+    cudaStream_t st = h->stream;
+    const int n = h->n;
+    const size_t n3 = 3 * (size_t)n;
+    if (!h->adj) h->adj = dalloc<double>(n3 * 10 + 8 * (size_t)n + 5 * (size_t)n + n + 6 * (size_t)n, h->owned);
+    double* g = h->adj;
+    double* gt = g + n3;
+    double* amu = gt + n3;
+    double* lam = amu + n3;
+    double* glab = lam + n3;
+    double* gmol = glab + n3;
+    double* mu_fwd = gmol + n3;
+    double* E_fwd = mu_fwd + n3;
+    double* amu_tlam = E_fwd + n3;
+    double* e_tmu = amu_tlam + n3;
+    double* a8 = e_tmu + n3;
+    double* b5 = a8 + 8 * (size_t)n;
+    double* ct = b5 + 5 * (size_t)n;
+    double* out = ct + n;
+    if (g_host) TDP_CUDA(cudaMemcpyAsync(g, g_host, n3 * 8, cudaMemcpyHostToDevice, st));
+    else TDP_CUDA(cudaMemsetAsync(g, 0, n3 * 8, st));
+    TDP_CUDA(cudaMemcpyAsync(mu_fwd, d.mu, n3 * 8, cudaMemcpyDeviceToDevice, st));
+    TDP_CUDA(cudaMemcpyAsync(E_fwd, d.E, n3 * 8, cudaMemcpyDeviceToDevice, st));
+    launch_torque_vjp(d, g, gt, st);
+    launch_adjoint_pair(d, g, gt, gE, a8, st);
+    launch_adjoint_split(d, a8, nullptr, amu, nullptr, st);
+    if (h->polarization == TDP_MUTUAL) {
+        // One solve of the same symmetric system: A lambda = a_mu.  Target:
+        // 1e-12 of the RMS of alpha * a_mu (the solver's Jacobi-step units).
+        std::vector<double> ha(n3);
+        TDP_CUDA(cudaMemcpyAsync(ha.data(), amu, n3 * 8, cudaMemcpyDeviceToHost, st));
+        TDP_CUDA(cudaStreamSynchronize(st));
+        double s2 = 0.0;
+        for (size_t k = 0; k < n3; k++) s2 += (h->alpha[k / 3] * ha[k]) * (h->alpha[k / 3] * ha[k]);
+        double rms = std::sqrt(s2 / std::max(n, 1));
+        int it0 = h->iterations, conv0 = h->converged, st0 = h->status, mv0 = h->matvecs;
+        double eps0 = h->epsilon, tgt0 = h->target_eps;
+        int cap0 = h->max_iter;
+        h->target_eps = std::max(rms * 1e-12, 1e-300);
+        h->max_iter = std::max(cap0, 1000);
+        launch_rhs_init<R>(d, amu, st);
+        solve_cg<R>(h);
+        h->adj_eps = h->epsilon;
+        h->adj_iterations = h->iterations;
+        h->iterations = it0;
+        h->converged = conv0;
+        h->status = st0;
+        h->epsilon = eps0;
+        h->matvecs = mv0;
+        h->target_eps = tgt0;
+        h->max_iter = cap0;
+        TDP_CUDA(cudaMemcpyAsync(lam, d.mu, n3 * 8, cudaMemcpyDeviceToDevice, st));
+        TDP_CUDA(cudaMemcpyAsync(d.mu, mu_fwd, n3 * 8, cudaMemcpyDeviceToDevice, st));
+        TDP_CUDA(cudaMemcpyAsync(d.E, E_fwd, n3 * 8, cudaMemcpyDeviceToDevice, st));
+        launch_adjoint_fixed(d, lam, b5, st);
+        launch_adjoint_matvec_t(d, lam, ct, st);
+        launch_set_operand<R>(d, lam, st);
+        launch_field<R>(d, 1, st);
+        launch_add_field(d, amu, amu_tlam, st);
+        launch_set_operand<R>(d, mu_fwd, st);
+        launch_field<R>(d, 1, st);
+        launch_add_field(d, E_fwd, e_tmu, st);
+    } else {
+        // Direct: mu = alpha E, so lambda = alpha a_mu and dL/dalpha = a_mu . E.
+        std::vector<double> ha(n3);
+        TDP_CUDA(cudaMemcpyAsync(ha.data(), amu, n3 * 8, cudaMemcpyDeviceToHost, st));
+        TDP_CUDA(cudaStreamSynchronize(st));
+        for (size_t k = 0; k < n3; k++) ha[k] *= h->alpha[k / 3];
+        TDP_CUDA(cudaMemcpyAsync(lam, ha.data(), n3 * 8, cudaMemcpyHostToDevice, st));
+        TDP_CUDA(cudaStreamSynchronize(st));
+        launch_adjoint_fixed(d, lam, b5, st);
+        TDP_CUDA(cudaMemsetAsync(ct, 0, sizeof(double) * n, st));
+        TDP_CUDA(cudaMemcpyAsync(amu_tlam, amu, n3 * 8, cudaMemcpyDeviceToDevice, st));
+        TDP_CUDA(cudaMemcpyAsync(e_tmu, E_fwd, n3 * 8, cudaMemcpyDeviceToDevice, st));
+        h->adj_eps = 0.0;
+        h->adj_iterations = 0;
+    }
+    launch_adjoint_split(d, a8, b5, amu, glab, st);
+    launch_rotation_vjp(d, glab, gmol, st);
+    launch_adjoint_assemble(d, a8, b5, ct, amu_tlam, e_tmu, gmol, out, st);
+    TDP_CUDA(cudaMemcpyAsync(out_host, out, sizeof(double) * 6 * n, cudaMemcpyDeviceToHost, st));
+    TDP_CUDA(cudaStreamSynchronize(st));
+    TDP_CUDA(cudaGetLastError());
+}
+
 }  // namespace
 
 extern "C" {
+
+int tdp_adjoint(tdp_handle* h, const double* dL_dF, double dL_dE, double* grads) {
+    if (!h || !grads) return TDP_ERR_INVALID_ARGUMENT;
+    try {
+        if (h->n == 0) return TDP_OK;
+        if (!h->have_results) throw TdpError{TDP_ERR_INVALID_ARGUMENT, "tdp_adjoint needs a previous tdp_compute"};
+        if (h->polarization == TDP_EXTRAPOLATED)
+            throw TdpError{TDP_ERR_UNSUPPORTED, "tdp_adjoint supports Direct and Mutual polarization"};
+        if (h->precision == TDP_PRECISION_DOUBLE) run_adjoint<double>(h, dL_dF, dL_dE, grads);
+        else run_adjoint<float>(h, dL_dF, dL_dE, grads);
+    } catch (const TdpError& e) {
+        return fail(h, e);
+    }
+    return TDP_OK;
+}
 
 int tdp_abi_version(void) { return TDP_ABI_VERSION; }
 

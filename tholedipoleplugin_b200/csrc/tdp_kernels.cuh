@@ -98,4 +98,19 @@ void launch_positions_in(const Dev& d, const void* src, int is_f32, cudaStream_t
 void launch_potential(const Dev& d, const double* grid, int ng, double* out, cudaStream_t st);
 void launch_moments(const Dev& d, const double* mass, double* scratch, double* out13, cudaStream_t st);
 
+// Adjoint (tdp_adjoint.cu).
+void launch_torque_vjp(const Dev& d, const double* g, double* gt, cudaStream_t st);
+void launch_adjoint_pair(const Dev& d, const double* g, const double* gT, double gE, double* a8, cudaStream_t st);
+void launch_adjoint_fixed(const Dev& d, const double* lam, double* b5, cudaStream_t st);
+void launch_adjoint_matvec_t(const Dev& d, const double* lam, double* ct, cudaStream_t st);
+void launch_rotation_vjp(const Dev& d, const double* glab, double* gmol, cudaStream_t st);
+void launch_adjoint_split(const Dev& d, const double* a8, const double* b5, double* amu, double* glab,
+                          cudaStream_t st);
+void launch_add_field(const Dev& d, const double* base, double* out, cudaStream_t st);
+template <class R> void launch_rhs_init(const Dev& d, const double* rhs, cudaStream_t st);
+template <class R> void launch_set_operand(const Dev& d, const double* x, cudaStream_t st);
+void launch_adjoint_assemble(const Dev& d, const double* a8, const double* b5, const double* ct,
+                             const double* amu_tlam, const double* e_tmu, const double* gmol, double* out,
+                             cudaStream_t st);
+
 }  // namespace tdp

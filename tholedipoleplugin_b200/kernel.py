@@ -226,6 +226,15 @@ class CudaCalcTholeDipoleForceKernel:
         self._check(self._lib.tdp_get_pme_parameters(self._h, C.byref(a), C.byref(nx), C.byref(ny), C.byref(nz)))
         return a.value, nx.value, ny.value, nz.value
 
+    def adjoint(self, dL_dF=None, dL_dE: float = 0.0) -> np.ndarray:
+        """Per-particle gradients (dq, dalpha, dthole, dmu_mol[3]) of
+        dL_dE * E + sum dL_dF . F at the last execute()'s positions."""
+        out = np.zeros((self.n, 6))
+        g = None if dL_dF is None else np.ascontiguousarray(np.asarray(dL_dF, dtype=np.float64).reshape(self.n, 3))
+        self._check(self._lib.tdp_adjoint(self._h, None if g is None else g.ctypes.data_as(C.c_void_p),
+                                          float(dL_dE), _dptr(out)))
+        return out
+
     def solverStats(self):
         it, conv, st = C.c_int32(), C.c_int32(), C.c_int32()
         eps = C.c_double()
