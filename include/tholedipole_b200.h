@@ -248,6 +248,53 @@ int tdp_adjoint(tdp_handle* h, const double* dL_dF, double dL_dE, double* grads)
 int tdp_enable_timing(tdp_handle* h, int32_t enable);
 int tdp_stage_times(const tdp_handle* h, double* out);
 
+/* ---------------------------------------------------------------------------
+ * Cluster batches.  No reference counterpart: the reference evaluates one
+ * System per context (ReferenceCalcTholeDipoleForceKernel::execute,
+ * platforms/reference/src/ReferenceTholeDipoleKernels.cpp); a batch evaluates
+ * many independent NoCutoff systems -- the clusters -- in one persistent
+ * launch, each with exactly the per-system semantics of tdp_compute.
+ *
+ * desc describes all clusters' particles concatenated; cluster c owns the
+ * particles [cluster_offsets[c], cluster_offsets[c+1]) and every axis atom and
+ * covalent partner of a particle must lie in its cluster.  Indices in desc are
+ * global.  Requirements: nonbonded_method TDP_NO_CUTOFF, solver TDP_SOLVER_CG;
+ * precision as for tdp_create.  The largest cluster must fit one CTA's shared
+ * memory (about 300 bytes per particle in the mixed form); otherwise
+ * TDP_ERR_UNSUPPORTED.  Errors: tdp_batch_last_error(b), or (NULL) for create.
+ * ------------------------------------------------------------------------- */
+typedef struct tdp_batch tdp_batch;
+
+int tdp_batch_create(const tdp_system_desc* desc, int32_t num_clusters, const int32_t* cluster_offsets,
+                     tdp_batch** out);
+void tdp_batch_destroy(tdp_batch* b);
+const char* tdp_batch_last_error(const tdp_batch* b);
+int tdp_batch_set_stream(tdp_batch* b, void* stream);
+
+/* One evaluation of every cluster: positions (n*3 doubles) in; forces (n*3,
+ * WRITTEN, torque mapping included) and per-cluster energies (num_clusters)
+ * out, either may be NULL.  on_device: all three pointers are device memory
+ * (no host synchronisation beyond the timing event) rather than host memory.
+ * The first call picks the tile shape (CTA size, lanes per particle) by timing
+ * every candidate on this batch, then captures the launch in a CUDA graph that
+ * every call replays. */
+int tdp_batch_compute(tdp_batch* b, const double* positions, int32_t on_device, double* forces, double* energies);
+
+/* Induced dipoles of the last compute, n*3 host doubles. */
+int tdp_batch_get_induced_dipoles(tdp_batch* b, double* out);
+
+/* Per-cluster solver report of the last compute: CG iterations (Extrapolated:
+ * the order) and the final RMS dipole change; either may be NULL. */
+int tdp_batch_solver_stats(tdp_batch* b, int32_t* iterations, double* epsilons);
+
+/* Tile shape chosen by the autotuner (0s before the first compute) and the
+ * device time of the last launch in ms. */
+int tdp_batch_tile(const tdp_batch* b, int32_t* threads, int32_t* lanes, int32_t* ctas, double* last_ms);
+
+/* The autotuner's candidates and their measured ms per launch (-1: not
+ * timed); fills up to capacity entries, returns the number of candidates. */
+int tdp_batch_tile_candidates(const tdp_batch* b, int32_t capacity, int32_t* threads, int32_t* lanes, double* ms);
+
 #ifdef __cplusplus
 }
 #endif

@@ -81,3 +81,51 @@ def test_bad_enums_rejected(lib):
 def test_null_desc(lib):
     h = C.c_void_p()
     assert lib.tdp_create(None, C.byref(h)) == -1
+
+
+# -- cluster batches: host validation runs before any device work ----------
+def _batch_create(clusters, offsets=None, edit=None, **kw):
+    sys_, offs = S.concat_clusters(clusters)
+    if offsets is not None:
+        offs = np.asarray(offsets, dtype=np.int32)
+    if edit is not None:
+        edit(sys_)
+    buf = _DescBuffers(sys_, 0, 0, 0)
+    for k, v in kw.items():
+        setattr(buf.desc, k, v)
+    offs = np.ascontiguousarray(offs, dtype=np.int32)
+    h = C.c_void_p()
+    rc = A.lib().tdp_batch_create(C.byref(buf.desc), len(offs) - 1, offs.ctypes.data_as(C.POINTER(C.c_int32)),
+                                  C.byref(h))
+    return rc, A.lib().tdp_batch_last_error(None).decode()
+
+
+def test_batch_rejects_periodic_and_jacobi(lib):
+    cl = [ammonia(), ammonia()]
+    rc, msg = _batch_create(cl, nonbonded_method=S.PME)
+    assert rc == A.TDP_ERR_UNSUPPORTED and "NoCutoff" in msg
+    rc, msg = _batch_create(cl, solver=A.SOLVER_JACOBI)
+    assert rc == A.TDP_ERR_UNSUPPORTED and "conjugate gradients" in msg
+
+
+def test_batch_rejects_bad_offsets(lib):
+    cl = [ammonia(), ammonia()]
+    n = sum(c.n for c in cl)
+    rc, msg = _batch_create(cl, offsets=[0, 5, n - 1])
+    assert rc == -1 and "from 0 to num_particles" in msg
+    rc, msg = _batch_create(cl, offsets=[0, n, 4, n])
+    assert rc == -1 and "non-decreasing" in msg
+
+
+def test_batch_rejects_links_across_clusters(lib):
+    a, b = ammonia(), ammonia()
+    a.cov12[0] = a.cov12[0] + [a.n + 1]  # partner index lands in the second cluster
+    rc, msg = _batch_create([a, b])
+    assert rc == -1 and "another cluster" in msg
+    n_a = ammonia().n
+
+    def z_into_first(sys_):
+        sys_.axis[n_a, 1] = 1  # first atom of the second cluster takes its Z atom from the first
+
+    rc, msg = _batch_create([ammonia(), ammonia()], edit=z_into_first)
+    assert rc == -1 and "another cluster" in msg

@@ -14,6 +14,7 @@ HERE = os.path.dirname(os.path.abspath(__file__))
 LIB_PATH = os.path.join(HERE, "libtholedipole_b200.so")
 
 TDP_OK = 0
+TDP_ERR_INVALID_ARGUMENT, TDP_ERR_CUDA, TDP_ERR_UNSUPPORTED = -1, -2, -8
 ERRORS = {
     -1: "invalid argument", -2: "CUDA error", -3: "not PME", -4: "size mismatch", -5: "box too small",
     -6: "not converged", -7: "non-finite", -8: "unsupported",
@@ -83,6 +84,15 @@ PROTOTYPES = {
     "tdp_md_constrain_velocities": (C.c_int, [C.c_int32, C.c_double, C.c_double, C.c_double, C.c_double,
                                               C.c_void_p, C.c_void_p, C.c_void_p]),
     "tdp_md_kinetic_energy": (C.c_int, [C.c_int32, C.c_double, C.c_double, C.c_void_p, C.c_void_p, C.c_void_p]),
+    "tdp_batch_create": (C.c_int, [C.POINTER(SystemDesc), C.c_int32, _ip, C.POINTER(C.c_void_p)]),
+    "tdp_batch_destroy": (None, [C.c_void_p]),
+    "tdp_batch_last_error": (C.c_char_p, [C.c_void_p]),
+    "tdp_batch_set_stream": (C.c_int, [C.c_void_p, C.c_void_p]),
+    "tdp_batch_compute": (C.c_int, [C.c_void_p, C.c_void_p, C.c_int32, C.c_void_p, C.c_void_p]),
+    "tdp_batch_get_induced_dipoles": (C.c_int, [C.c_void_p, _dp]),
+    "tdp_batch_solver_stats": (C.c_int, [C.c_void_p, _ip, _dp]),
+    "tdp_batch_tile": (C.c_int, [C.c_void_p, _ip, _ip, _ip, _dp]),
+    "tdp_batch_tile_candidates": (C.c_int, [C.c_void_p, C.c_int32, _ip, _ip, _dp]),
 }
 
 

@@ -12,7 +12,9 @@ HERE = os.path.dirname(os.path.abspath(__file__))
 ROOT = os.path.dirname(HERE)
 CSRC = os.path.join(HERE, "csrc")
 LIB = os.path.join(HERE, "libtholedipole_b200.so")
-SOURCES = ["tdp_kernels.cu", "tdp_capi.cu", "tdp_md.cu", "tdp_noalloc.cu", "tdp_adjoint.cu"]
+SOURCES = ["tdp_kernels.cu", "tdp_capi.cu", "tdp_md.cu", "tdp_noalloc.cu", "tdp_adjoint.cu", "tdp_batch.cu"]
+# Sources whose FP32 pair arithmetic is compiled with subnormal flushing.
+FTZ = {"tdp_kernels.cu", "tdp_batch.cu"}
 ARCH = ["-gencode", "arch=compute_100a,code=sm_100a"]
 
 
@@ -56,7 +58,7 @@ def build(force: bool = False, verbose: bool = False) -> str:
         # The pair kernels never see subnormal FP32 operands (squared distances
         # are >= ~1e-4 nm^2 or masked to +inf), so flushing subnormals removes
         # the fix-up around every reciprocal square root.
-        extra = ["-ftz=true"] if src == "tdp_kernels.cu" else []
+        extra = ["-ftz=true"] if src in FTZ else []
         cmd = common + extra + ["-c", os.path.join(CSRC, src), "-o", obj]
         if verbose:
             print(" ".join(cmd), file=sys.stderr)

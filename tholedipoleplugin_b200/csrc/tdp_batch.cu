@@ -1,0 +1,984 @@
+// tdp_batch.cu -- many isolated clusters (NoCutoff systems) evaluated in one
+// persistent launch: the tdp_batch_* entry points of include/tholedipole_b200.h.
+//
+// Device side.  Each CTA pulls clusters from a work queue ordered by
+// decreasing size and keeps the whole cluster in shared memory: FP64
+// positions, parameters, permanent field, induced dipoles and the CG vectors,
+// plus centroid-relative float4 (or double4) records for the pair arithmetic.
+// Inside the CTA it runs the reference evaluation end to end -- lab-frame
+// rotation, permanent field, induced dipoles, pair energy/force/torque and
+// torque mapping (ReferenceTholeDipoleForce.cpp, "RTDF.cpp", :117-124 and
+// :1117-1155) -- with the per-pair device functions of the box kernels
+// (tdp_pairs.cuh, tdp_frames.cuh), so the semantics are the same by
+// construction.  Mutual polarization is the box path's conjugate gradient in
+// y = mu/sqrt(alpha) with FP64 vectors and block reductions, the reference's
+// RMS-dipole-change stopping test and a true-residual check before accepting.
+//
+// Tile shape.  An atom i is served by a group of L consecutive lanes (L a
+// power of two, L*n <= threads): lane l takes j = l, l+L, ... and the group
+// reduces by shuffles, so small clusters still occupy the CTA.  The CTA size
+// and the largest L are the tile shape; tdp_batch_compute picks them on the
+// first call by timing every candidate on the batch itself.
+//
+// Host side.  The launch (queue reset + kernel) is captured once in a CUDA
+// graph and replayed; one call is: positions in, graph, then forces and
+// per-cluster energies out.
+#include "tholedipole_b200.h"
+#include "tdp_frames.cuh"
+#include "tdp_host.h"
+#include "tdp_pairs.cuh"
+
+#include <cuda_runtime.h>
+
+#include <algorithm>
+#include <cstdlib>
+#include <numeric>
+#include <string>
+#include <vector>
+
+namespace tdp {
+namespace {
+
+struct BatchArgs {
+    int num_clusters;
+    int max_atoms, max_exc, korder, lmax;
+    int polarization;  // TDP_DIRECT / TDP_MUTUAL / TDP_EXTRAPOLATED
+    int max_iter;
+    double target_eps;
+    double damp_r2;
+    double rinv4_power, rinv4_fill;
+    const int* order;   // clusters by decreasing size
+    const int* coff;    // num_clusters+1 atom offsets
+    const double* pos;  // n*3
+    const double* charge;
+    const double* dip_mol;
+    const double* alpha;
+    const double* thole;
+    const int4* axis;   // (type, z, x, y), global indices
+    const int* exc_off;
+    const int* exc_j;
+    const double* exc_m;
+    const double* exc_s;
+    const int* users_off;
+    const int2* users;  // (frame atom, role), global
+    const double* coef; // extrapolation coefficients
+    int* queue;
+    double* forces;     // n*3, written
+    double* mu_out;     // n*3 induced dipoles
+    double* energy;     // per cluster
+    int* iters;         // per cluster
+    double* eps;        // per cluster
+};
+
+__host__ __device__ inline size_t align_up(size_t x, size_t a) { return (x + a - 1) / a * a; }
+
+// Per-atom double slots of the work region: CG (y, r, p, q) or the
+// extrapolation history plus one field; forces and torques afterwards.
+__host__ __device__ inline int work_slots(int korder) { return 3 * korder + 3 > 12 ? 3 * korder + 3 : 12; }
+
+template <class R>
+__host__ __device__ inline size_t batch_smem(int M, int X, int korder) {
+    typedef typename Vec4T<R>::type V4;
+    size_t b = 0;
+    b += sizeof(double) * ((size_t)M * (3 + 3 + 3 + 1 + 1 + work_slots(korder)) + 64);
+    b = align_up(b, 32);
+    b += sizeof(V4) * 3 * (size_t)M;
+    b = align_up(b, 16);
+    b += sizeof(int4) * (size_t)M;
+    b += sizeof(int) * ((size_t)M + 1 + (size_t)X);
+    b = align_up(b, 8);
+    b += sizeof(R) * 2 * (size_t)X;
+    return align_up(b, 16);
+}
+
+template <class R>
+struct Cl {
+    typedef typename Vec4T<R>::type V4;
+    double *pos, *E, *mu, *alpha, *salpha, *w, *red;
+    V4 *posq, *dipt, *vec;
+    int4* axis;
+    int *eoff, *ej;
+    R *em, *es;
+    int M;
+};
+
+template <class R>
+__device__ Cl<R> carve(char* base, int M, int X, int korder) {
+    typedef typename Vec4T<R>::type V4;
+    Cl<R> c;
+    c.M = M;
+    double* d = reinterpret_cast<double*>(base);
+    c.pos = d; d += 3 * M;
+    c.E = d; d += 3 * M;
+    c.mu = d; d += 3 * M;
+    c.alpha = d; d += M;
+    c.salpha = d; d += M;
+    c.w = d; d += (size_t)work_slots(korder) * M;
+    c.red = d; d += 64;
+    size_t off = align_up((size_t)(reinterpret_cast<char*>(d) - base), 32);
+    V4* v = reinterpret_cast<V4*>(base + off);
+    c.posq = v; v += M;
+    c.dipt = v; v += M;
+    c.vec = v; v += M;
+    off = align_up((size_t)(reinterpret_cast<char*>(v) - base), 16);
+    int4* a = reinterpret_cast<int4*>(base + off);
+    c.axis = a; a += M;
+    int* ip = reinterpret_cast<int*>(a);
+    c.eoff = ip; ip += M + 1;
+    c.ej = ip; ip += X;
+    off = align_up((size_t)(reinterpret_cast<char*>(ip) - base), 8);
+    R* rp = reinterpret_cast<R*>(base + off);
+    c.em = rp; rp += X;
+    c.es = rp;
+    return c;
+}
+
+// Block sum in a fixed order (deterministic for a given CTA size).
+__device__ __forceinline__ double bsum(double v, double* red) {
+    v = warp_sum(v);
+    const int lane = threadIdx.x & 31, w = threadIdx.x >> 5;
+    __syncthreads();
+    if (lane == 0) red[w] = v;
+    __syncthreads();
+    double s = 0.0;
+    const int nw = blockDim.x >> 5;
+    for (int k = 0; k < nw; k++) s += red[k];
+    return s;
+}
+
+template <class T>
+__device__ __forceinline__ T group_sum(T v, int L) {
+    for (int o = L >> 1; o > 0; o >>= 1) v += __shfl_xor_sync(0xffffffffu, v, o);
+    return v;
+}
+
+// Lane-group decomposition of the pair loops for an n-atom cluster.
+struct Groups {
+    int L, G, g, l;
+};
+__device__ __forceinline__ Groups groups(int n, int lmax) {
+    Groups q;
+    int L = 1;
+    while (L * 2 <= lmax && L * 2 * n <= (int)blockDim.x) L *= 2;
+    q.L = L;
+    q.G = blockDim.x / L;
+    q.g = threadIdx.x / L;
+    q.l = threadIdx.x % L;
+    return q;
+}
+
+// (M, I) scales of the pair (i, j) from i's local exception list.
+template <class R>
+__device__ __forceinline__ void pair_scales(const Cl<R>& c, int i, int j, R& m, R& s) {
+    m = R(1);
+    s = R(1);
+    for (int e = c.eoff[i]; e < c.eoff[i + 1]; e++)
+        if (c.ej[e] == j) {
+            m = c.em[e];
+            s = c.es[e];
+        }
+}
+
+// out[i] = sum_j I_ij T_ij v_j with v in c.vec (the mutual field of the operand).
+template <class R>
+__device__ void cluster_matvec(const Cl<R>& c, int n, const Groups& gp, R damp_r2, double* out) {
+    typedef typename Vec4T<R>::type V4;
+    for (int base = 0; base < n; base += gp.G) {
+        const int i = base + gp.g;
+        R fx = 0, fy = 0, fz = 0;
+        if (i < n) {
+            const V4 pi = c.posq[i];
+            const R ti = c.vec[i].w;
+            for (int j = gp.l; j < n; j += gp.L) {
+                if (j == i) continue;
+                R m, s;
+                pair_scales(c, i, j, m, s);
+                if (s == R(0)) continue;
+                const V4 pj = c.posq[j], vj = c.vec[j];
+                const R dx = pj.x - pi.x, dy = pj.y - pi.y, dz = pj.z - pi.z;
+                const R r2 = dx * dx + dy * dy + dz * dz;
+                R tx = 0, ty = 0, tz = 0;
+                pair_matvec<R>(dx, dy, dz, r2, vj.x, vj.y, vj.z, ti, vj.w, damp_r2, tx, ty, tz);
+                fx += s * tx;
+                fy += s * ty;
+                fz += s * tz;
+            }
+        }
+        double ax = group_sum((double)fx, gp.L), ay = group_sum((double)fy, gp.L), az = group_sum((double)fz, gp.L);
+        if (i < n && gp.l == 0) {
+            out[3 * i] = ax;
+            out[3 * i + 1] = ay;
+            out[3 * i + 2] = az;
+        }
+    }
+}
+
+template <class R>
+__device__ __forceinline__ void set_vec(const Cl<R>& c, int i, double x, double y, double z) {
+    typename Vec4T<R>::type v = c.vec[i];
+    v.x = (R)x;
+    v.y = (R)y;
+    v.z = (R)z;
+    c.vec[i] = v;
+}
+
+// CG residual of y: r = S (E + T mu) - y (T mu already in tq), p = r, operand
+// S p; returns r.r and writes sum alpha |r|^2 into *ee.
+template <class R>
+__device__ double cg_residual(const Cl<R>& c, int n, const double* y, double* r, double* p, const double* tq,
+                              double* ee) {
+    double rr = 0.0, e2 = 0.0;
+    for (int i = threadIdx.x; i < n; i += blockDim.x) {
+        const double sa = c.salpha[i];
+        for (int k = 0; k < 3; k++) {
+            const double rv = (c.E[3 * i + k] + tq[3 * i + k]) * sa - y[3 * i + k];
+            r[3 * i + k] = rv;
+            p[3 * i + k] = rv;
+            rr += rv * rv;
+            e2 += sa * sa * rv * rv;
+        }
+        set_vec(c, i, sa * p[3 * i], sa * p[3 * i + 1], sa * p[3 * i + 2]);
+    }
+    rr = bsum(rr, c.red);
+    *ee = bsum(e2, c.red);
+    return rr;
+}
+
+template <class R>
+__global__ void __launch_bounds__(512) k_batch(BatchArgs A) {
+    typedef typename Vec4T<R>::type V4;
+    extern __shared__ __align__(32) char smem_raw[];
+    const Cl<R> c = carve<R>(smem_raw, A.max_atoms, A.max_exc, A.korder);
+    __shared__ int s_slot;
+    const R damp_r2 = (R)A.damp_r2;
+    const R rv4p = (R)A.rinv4_power, rv4f = (R)A.rinv4_fill;
+    while (true) {
+        __syncthreads();
+        if (threadIdx.x == 0) s_slot = atomicAdd(A.queue, 1);
+        __syncthreads();
+        const int slot = s_slot;
+        if (slot >= A.num_clusters) break;
+        const int cid = A.order[slot];
+        const int a0 = A.coff[cid], n = A.coff[cid + 1] - a0;
+        if (n <= 0) {
+            if (threadIdx.x == 0) {
+                A.energy[cid] = 0.0;
+                A.iters[cid] = 0;
+                A.eps[cid] = 0.0;
+            }
+            continue;
+        }
+        const Groups gp = groups(n, A.lmax);
+        const int e0 = A.exc_off[a0];
+
+        // ---- load ------------------------------------------------------------------------
+        double cx = 0, cy = 0, cz = 0;
+        for (int i = threadIdx.x; i < n; i += blockDim.x) {
+            const int gi = a0 + i;
+            for (int k = 0; k < 3; k++) c.pos[3 * i + k] = A.pos[3 * (size_t)gi + k];
+            cx += c.pos[3 * i];
+            cy += c.pos[3 * i + 1];
+            cz += c.pos[3 * i + 2];
+            const int4 ax = A.axis[gi];
+            c.axis[i] = make_int4(ax.x, ax.y >= 0 ? ax.y - a0 : -1, ax.z >= 0 ? ax.z - a0 : -1,
+                                  ax.w >= 0 ? ax.w - a0 : -1);
+            const double al = A.alpha[gi];
+            c.alpha[i] = al;
+            c.salpha[i] = al > 0.0 ? sqrt(al) : 0.0;
+            c.eoff[i] = A.exc_off[gi] - e0;
+            for (int e = A.exc_off[gi]; e < A.exc_off[gi + 1]; e++) {
+                c.ej[e - e0] = A.exc_j[e] - a0;
+                c.em[e - e0] = (R)A.exc_m[e];
+                c.es[e - e0] = (R)A.exc_s[e];
+            }
+        }
+        if (threadIdx.x == 0) c.eoff[n] = A.exc_off[a0 + n] - e0;
+        cx = bsum(cx, c.red) / n;
+        cy = bsum(cy, c.red) / n;
+        cz = bsum(cz, c.red) / n;
+        for (int i = threadIdx.x; i < n; i += blockDim.x) {
+            V4 pq;
+            if (sizeof(R) == 4) {
+                pq.x = (R)(c.pos[3 * i] - cx);
+                pq.y = (R)(c.pos[3 * i + 1] - cy);
+                pq.z = (R)(c.pos[3 * i + 2] - cz);
+            } else {
+                pq.x = (R)c.pos[3 * i];
+                pq.y = (R)c.pos[3 * i + 1];
+                pq.z = (R)c.pos[3 * i + 2];
+            }
+            pq.w = (R)A.charge[a0 + i];
+            c.posq[i] = pq;
+        }
+        __syncthreads();
+
+        // ---- lab-frame dipoles (RTDF.cpp:432-571) ------------------------------------------
+        for (int i = threadIdx.x; i < n; i += blockDim.x) {
+            double Rm[3][3], sy;
+            frame_rows(c.pos, c.axis[i], i, Rm, sy);
+            const double* dm = A.dip_mol + 3 * (size_t)(a0 + i);
+            const double d0 = dm[0], d1 = sy * dm[1], d2 = dm[2];
+            double lab[3];
+            for (int k = 0; k < 3; k++) lab[k] = 0.0 + d0 * Rm[0][k] + d1 * Rm[1][k] + d2 * Rm[2][k];
+            V4 dv;
+            dv.x = (R)lab[0];
+            dv.y = (R)lab[1];
+            dv.z = (R)lab[2];
+            dv.w = (R)A.thole[a0 + i];
+            c.dipt[i] = dv;
+        }
+        __syncthreads();
+
+        // ---- permanent field (RTDF.cpp:678-746): E, mu = alpha E --------------------------
+        for (int base = 0; base < n; base += gp.G) {
+            const int i = base + gp.g;
+            R fx = 0, fy = 0, fz = 0;
+            if (i < n) {
+                const V4 pi = c.posq[i];
+                const R ti = c.dipt[i].w;
+                for (int j = gp.l; j < n; j += gp.L) {
+                    if (j == i) continue;
+                    R m, s;
+                    pair_scales(c, i, j, m, s);
+                    if (m == R(0)) continue;
+                    const V4 pj = c.posq[j], dj = c.dipt[j];
+                    const R dx = pj.x - pi.x, dy = pj.y - pi.y, dz = pj.z - pi.z;
+                    const R r2 = dx * dx + dy * dy + dz * dz;
+                    R tx = 0, ty = 0, tz = 0;
+                    pair_fixed<R>(dx, dy, dz, r2, pj.w, dj.x, dj.y, dj.z, ti, dj.w, damp_r2, tx, ty, tz);
+                    fx += m * tx;
+                    fy += m * ty;
+                    fz += m * tz;
+                }
+            }
+            const double ex = group_sum((double)fx, gp.L), ey = group_sum((double)fy, gp.L),
+                         ez = group_sum((double)fz, gp.L);
+            if (i < n && gp.l == 0) {
+                c.E[3 * i] = ex;
+                c.E[3 * i + 1] = ey;
+                c.E[3 * i + 2] = ez;
+            }
+        }
+        __syncthreads();
+        for (int i = threadIdx.x; i < n; i += blockDim.x) {
+            const double al = c.alpha[i];
+            for (int k = 0; k < 3; k++) c.mu[3 * i + k] = al * c.E[3 * i + k];
+            V4 v;
+            v.x = (R)c.mu[3 * i];
+            v.y = (R)c.mu[3 * i + 1];
+            v.z = (R)c.mu[3 * i + 2];
+            v.w = c.dipt[i].w;
+            c.vec[i] = v;
+        }
+        __syncthreads();
+
+        // ---- induced dipoles ---------------------------------------------------------------
+        int it = 0;
+        double eps = 1.0e50;
+        const int n3 = 3 * n;
+        if (A.polarization == TDP_MUTUAL) {
+            double* y = c.w;
+            double* r = c.w + 3 * c.M;
+            double* p = c.w + 6 * c.M;
+            double* q = c.w + 9 * c.M;
+            for (int k = threadIdx.x; k < n3; k += blockDim.x) y[k] = c.salpha[k / 3] * c.E[k];
+            cluster_matvec(c, n, gp, damp_r2, q);
+            __syncthreads();
+            double ee;
+            double rr = cg_residual(c, n, y, r, p, q, &ee);
+            eps = sqrt(ee / n);
+            bool is_true = true;
+            while (true) {
+                if (!(eps <= 1.0e300)) break;  // non-finite
+                if (eps <= A.target_eps || it >= A.max_iter) {
+                    if (is_true) break;
+                    // Accept only on the true residual of the current iterate.
+                    for (int i = threadIdx.x; i < n; i += blockDim.x) {
+                        const double sa = c.salpha[i];
+                        set_vec(c, i, sa * y[3 * i], sa * y[3 * i + 1], sa * y[3 * i + 2]);
+                    }
+                    __syncthreads();
+                    cluster_matvec(c, n, gp, damp_r2, q);
+                    __syncthreads();
+                    rr = cg_residual(c, n, y, r, p, q, &ee);
+                    eps = sqrt(ee / n);
+                    is_true = true;
+                    continue;
+                }
+                __syncthreads();
+                cluster_matvec(c, n, gp, damp_r2, q);  // T S p
+                __syncthreads();
+                double pq = 0.0;
+                for (int k = threadIdx.x; k < n3; k += blockDim.x) {
+                    const double qv = p[k] - c.salpha[k / 3] * q[k];
+                    q[k] = qv;
+                    pq += p[k] * qv;
+                }
+                pq = bsum(pq, c.red);
+                const double a = rr / pq;
+                double rr2 = 0.0, e2 = 0.0;
+                for (int k = threadIdx.x; k < n3; k += blockDim.x) {
+                    const double sa = c.salpha[k / 3];
+                    y[k] += a * p[k];
+                    const double rv = r[k] - a * q[k];
+                    r[k] = rv;
+                    rr2 += rv * rv;
+                    e2 += sa * sa * rv * rv;
+                }
+                rr2 = bsum(rr2, c.red);
+                eps = sqrt(bsum(e2, c.red) / n);
+                const double beta = rr2 / rr;
+                rr = rr2;
+                for (int i = threadIdx.x; i < n; i += blockDim.x) {
+                    const double sa = c.salpha[i];
+                    for (int k = 0; k < 3; k++) p[3 * i + k] = r[3 * i + k] + beta * p[3 * i + k];
+                    set_vec(c, i, sa * p[3 * i], sa * p[3 * i + 1], sa * p[3 * i + 2]);
+                }
+                it++;
+                is_true = false;
+            }
+            __syncthreads();
+            for (int k = threadIdx.x; k < n3; k += blockDim.x) c.mu[k] = c.salpha[k / 3] * y[k];
+        } else if (A.polarization == TDP_EXTRAPOLATED) {
+            // Perturbation-theory extrapolation (RTDF.cpp:853-909).
+            double* hist = c.w;                               // korder slots of 3M
+            double* fld = c.w + (size_t)A.korder * 3 * c.M;   // 3M
+            for (int k = threadIdx.x; k < n3; k += blockDim.x) hist[k] = c.mu[k];
+            for (int o = 1; o < A.korder; o++) {
+                __syncthreads();
+                cluster_matvec(c, n, gp, damp_r2, fld);
+                __syncthreads();
+                for (int i = threadIdx.x; i < n; i += blockDim.x) {
+                    for (int k = 0; k < 3; k++) {
+                        const double v = (c.E[3 * i + k] + fld[3 * i + k]) * c.alpha[i];
+                        c.mu[3 * i + k] = v;
+                        hist[(size_t)o * 3 * c.M + 3 * i + k] = v;
+                    }
+                    set_vec(c, i, c.mu[3 * i], c.mu[3 * i + 1], c.mu[3 * i + 2]);
+                }
+            }
+            __syncthreads();
+            for (int i = threadIdx.x; i < n; i += blockDim.x) {
+                for (int k = 0; k < 3; k++) {
+                    double acc = 0.0;
+                    for (int o = 0; o < A.korder; o++) acc += hist[(size_t)o * 3 * c.M + 3 * i + k] * A.coef[o];
+                    c.mu[3 * i + k] = acc;
+                }
+                set_vec(c, i, c.mu[3 * i], c.mu[3 * i + 1], c.mu[3 * i + 2]);
+            }
+            __syncthreads();
+            cluster_matvec(c, n, gp, damp_r2, fld);
+            __syncthreads();
+            double e2 = 0.0;
+            for (int k = threadIdx.x; k < n3; k += blockDim.x) {
+                const double dl = (c.E[k] + fld[k]) * c.alpha[k / 3] - c.mu[k];
+                e2 += dl * dl;
+            }
+            eps = sqrt(bsum(e2, c.red) / n);
+            it = A.korder;
+        }
+        __syncthreads();
+
+        // ---- energy, forces, torques (RTDF.cpp:129-393) ------------------------------------
+        // The operand records now carry the induced dipoles.
+        for (int i = threadIdx.x; i < n; i += blockDim.x) set_vec(c, i, c.mu[3 * i], c.mu[3 * i + 1], c.mu[3 * i + 2]);
+        __syncthreads();
+        double* frc = c.w;
+        double* trq = c.w + 3 * c.M;
+        double en = 0.0;
+        for (int base = 0; base < n; base += gp.G) {
+            const int i = base + gp.g;
+            double f[6] = {0, 0, 0, 0, 0, 0};
+            if (i < n) {
+                const V4 pi = c.posq[i], di = c.dipt[i], ui = c.vec[i];
+                const EAtom<R> me{pi.w, di.x, di.y, di.z, ui.x, ui.y, ui.z, di.w};
+                const double yi = c.pos[3 * i + 1], zi = c.pos[3 * i + 2];
+                for (int j = gp.l; j < n; j += gp.L) {
+                    if (j == i) continue;
+                    R m, s;
+                    pair_scales(c, i, j, m, s);
+                    if (m == R(0) && s == R(0)) continue;
+                    const V4 pj = c.posq[j], dj = c.dipt[j], uj = c.vec[j];
+                    const EAtom<R> other{pj.w, dj.x, dj.y, dj.z, uj.x, uj.y, uj.z, dj.w};
+                    const R dx = pj.x - pi.x, dy = pj.y - pi.y, dz = pj.z - pi.z;
+                    const R r2 = dx * dx + dy * dy + dz * dz;
+                    // formQIRotationMatrix's test on the raw positions (RTDF.cpp:584).
+                    bool yzd = fabs(dy) > R(1e-5) || fabs(dz) > R(1e-5);
+                    if (!yzd) yzd = (yi != c.pos[3 * j + 1]) || (zi != c.pos[3 * j + 2]);
+                    R fx = 0, fy = 0, fz = 0, tx = 0, ty = 0, tz = 0, e = 0;
+                    if (i < j)
+                        pair_energy<R, true>(dx, dy, dz, r2, yzd, me, other, m, s, damp_r2, rv4p, rv4f,
+                                             A.polarization == TDP_MUTUAL, fx, fy, fz, tx, ty, tz, e);
+                    else
+                        pair_energy<R, false>(-dx, -dy, -dz, r2, yzd, other, me, m, s, damp_r2, rv4p, rv4f,
+                                              A.polarization == TDP_MUTUAL, fx, fy, fz, tx, ty, tz, e);
+                    f[0] += fx;
+                    f[1] += fy;
+                    f[2] += fz;
+                    f[3] += tx;
+                    f[4] += ty;
+                    f[5] += tz;
+                    en += e;
+                }
+            }
+            for (int k = 0; k < 6; k++) f[k] = group_sum(f[k], gp.L);
+            if (i < n && gp.l == 0) {
+                for (int k = 0; k < 3; k++) {
+                    frc[3 * i + k] = f[k];
+                    trq[3 * i + k] = f[3 + k];
+                }
+            }
+        }
+        en = bsum(en, c.red);  // its barriers also order the frc/trq writes before the gather
+
+        // ---- torque mapping (RTDF.cpp:915-1115), gathered per receiving atom -------------
+        for (int a = threadIdx.x; a < n; a += blockDim.x) {
+            const int ga = a0 + a;
+            d3 F = {frc[3 * a], frc[3 * a + 1], frc[3 * a + 2]};
+            for (int k = A.users_off[ga]; k < A.users_off[ga + 1]; k++) {
+                const int2 u = A.users[k];
+                const int fi = u.x - a0;
+                const d3 T = {trq[3 * fi], trq[3 * fi + 1], trq[3 * fi + 2]};
+                F = F + torque_role_force(c.pos, c.axis[fi], fi, u.y, T);
+            }
+            A.forces[3 * (size_t)ga] = F.x;
+            A.forces[3 * (size_t)ga + 1] = F.y;
+            A.forces[3 * (size_t)ga + 2] = F.z;
+            for (int k = 0; k < 3; k++) A.mu_out[3 * (size_t)ga + k] = c.mu[3 * a + k];
+        }
+        if (threadIdx.x == 0) {
+            A.energy[cid] = en;
+            A.iters[cid] = it;
+            A.eps[cid] = eps;
+        }
+    }
+}
+
+}  // namespace
+}  // namespace tdp
+
+using namespace tdp;
+
+// ---------------------------------------------------------------------------
+// Host side.
+// ---------------------------------------------------------------------------
+struct tdp_batch {
+    int n = 0, nc = 0;
+    int precision = TDP_PRECISION_MIXED;
+    int polarization = TDP_MUTUAL;
+    int max_atoms = 0, max_exc = 0;
+    std::vector<int> coff;
+    std::vector<double> extrap;
+    BatchArgs args{};
+    std::vector<void*> owned;
+    cudaStream_t stream = nullptr;
+    int device = 0, num_sms = 148;
+    size_t smem_optin = 0;
+    // Tile shape: CTA size, largest lanes per atom, CTAs in the persistent grid.
+    bool tuned = false;
+    int threads = 128, lmax = 8, ctas = 148;
+    double tile_ms = 0.0;
+    std::vector<double> tune_ms;  // per candidate, in tdp_batch_tile_candidates order
+    cudaGraph_t graph = nullptr;
+    cudaGraphExec_t exec = nullptr;
+    cudaEvent_t ev0 = nullptr, ev1 = nullptr;
+    double last_ms = 0.0;
+    bool have_results = false;
+    std::string err;
+};
+
+namespace {
+
+thread_local std::string g_batch_create_error;
+
+struct TileShape {
+    int threads, lmax;
+};
+const TileShape kShapes[] = {{64, 4},  {64, 16},  {128, 4},  {128, 8},  {128, 16}, {128, 32},
+                             {256, 4}, {256, 8},  {256, 16}, {256, 32}, {512, 8},  {512, 32}};
+constexpr int kNumShapes = sizeof(kShapes) / sizeof(kShapes[0]);
+
+int batch_fail(tdp_batch* b, const TdpError& e) {
+    if (b) b->err = e.msg;
+    else g_batch_create_error = e.msg;
+    return e.code;
+}
+
+size_t smem_for(const tdp_batch* b) {
+    int korder = std::max(1, (int)b->extrap.size());
+    int M = std::max(1, b->max_atoms);
+    return b->precision == TDP_PRECISION_DOUBLE ? batch_smem<double>(M, b->max_exc, korder)
+                                                : batch_smem<float>(M, b->max_exc, korder);
+}
+
+const void* kernel_for(const tdp_batch* b) {
+    return b->precision == TDP_PRECISION_DOUBLE ? (const void*)k_batch<double> : (const void*)k_batch<float>;
+}
+
+// CTAs of the persistent grid for a CTA size: every resident slot, at most one per cluster.
+int grid_for(tdp_batch* b, int threads) {
+    size_t smem = smem_for(b);
+    const void* k = kernel_for(b);
+    TDP_CUDA(cudaFuncSetAttribute(k, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
+    int per_sm = 0;
+    TDP_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k, threads, smem));
+    if (per_sm < 1) return 0;
+    return std::max(1, std::min(b->nc, per_sm * b->num_sms));
+}
+
+void launch(tdp_batch* b, int threads, int lmax, int ctas, cudaStream_t st) {
+    BatchArgs a = b->args;
+    a.lmax = lmax;
+    size_t smem = smem_for(b);
+    TDP_CUDA(cudaMemsetAsync(a.queue, 0, sizeof(int), st));
+    if (b->precision == TDP_PRECISION_DOUBLE) k_batch<double><<<ctas, threads, smem, st>>>(a);
+    else k_batch<float><<<ctas, threads, smem, st>>>(a);
+    TDP_CUDA(cudaGetLastError());
+}
+
+void drop_graph(tdp_batch* b) {
+    if (b->exec) cudaGraphExecDestroy(b->exec);
+    if (b->graph) cudaGraphDestroy(b->graph);
+    b->exec = nullptr;
+    b->graph = nullptr;
+}
+
+void build_graph(tdp_batch* b) {
+    drop_graph(b);
+    cudaStream_t cap = nullptr;
+    TDP_CUDA(cudaStreamCreateWithFlags(&cap, cudaStreamNonBlocking));
+    cudaError_t e = cudaStreamBeginCapture(cap, cudaStreamCaptureModeThreadLocal);
+    if (e == cudaSuccess) {
+        try {
+            launch(b, b->threads, b->lmax, b->ctas, cap);
+        } catch (const TdpError&) {
+            cudaGraph_t g = nullptr;
+            cudaStreamEndCapture(cap, &g);
+            if (g) cudaGraphDestroy(g);
+            cudaStreamDestroy(cap);
+            throw;
+        }
+        e = cudaStreamEndCapture(cap, &b->graph);
+    }
+    cudaStreamDestroy(cap);
+    if (e != cudaSuccess) throw TdpError{TDP_ERR_CUDA, std::string("graph capture: ") + cudaGetErrorString(e)};
+    TDP_CUDA(cudaGraphInstantiate(&b->exec, b->graph, 0));
+}
+
+double time_launch(tdp_batch* b, int threads, int lmax, int ctas, int reps) {
+    TDP_CUDA(cudaEventRecord(b->ev0, b->stream));
+    for (int r = 0; r < reps; r++) launch(b, threads, lmax, ctas, b->stream);
+    TDP_CUDA(cudaEventRecord(b->ev1, b->stream));
+    TDP_CUDA(cudaEventSynchronize(b->ev1));
+    float ms = 0.f;
+    TDP_CUDA(cudaEventElapsedTime(&ms, b->ev0, b->ev1));
+    return ms / reps;
+}
+
+// The autotuner: time every tile shape that fits on the batch (one warm-up
+// launch, then two timed) and keep the fastest.  TDP_BATCH_TILE="threads,lanes"
+// pins the shape instead.
+void autotune(tdp_batch* b) {
+    b->tune_ms.assign(kNumShapes, -1.0);
+    int pin_t = 0, pin_l = 0;
+    if (const char* env = getenv("TDP_BATCH_TILE")) sscanf(env, "%d,%d", &pin_t, &pin_l);
+    double best = 1e300;
+    int best_k = -1;
+    for (int k = 0; k < kNumShapes; k++) {
+        const TileShape s = kShapes[k];
+        if (pin_t && (s.threads != pin_t || s.lmax != pin_l)) continue;
+        int ctas = grid_for(b, s.threads);
+        if (ctas <= 0) continue;
+        launch(b, s.threads, s.lmax, ctas, b->stream);
+        double ms = time_launch(b, s.threads, s.lmax, ctas, 2);
+        b->tune_ms[k] = ms;
+        if (ms < best) {
+            best = ms;
+            best_k = k;
+        }
+    }
+    if (best_k < 0) throw TdpError{TDP_ERR_UNSUPPORTED, "no tile shape fits the largest cluster"};
+    b->threads = kShapes[best_k].threads;
+    b->lmax = kShapes[best_k].lmax;
+    b->ctas = grid_for(b, b->threads);
+    b->tile_ms = best;
+    b->tuned = true;
+    build_graph(b);
+}
+
+}  // namespace
+
+extern "C" {
+
+const char* tdp_batch_last_error(const tdp_batch* b) { return b ? b->err.c_str() : g_batch_create_error.c_str(); }
+
+void tdp_batch_destroy(tdp_batch* b) {
+    if (!b) return;
+    drop_graph(b);
+    if (b->ev0) cudaEventDestroy(b->ev0);
+    if (b->ev1) cudaEventDestroy(b->ev1);
+    for (void* p : b->owned) cudaFree(p);
+    delete b;
+}
+
+int tdp_batch_create(const tdp_system_desc* desc, int32_t num_clusters, const int32_t* cluster_offsets,
+                     tdp_batch** out) {
+    if (!out) return TDP_ERR_INVALID_ARGUMENT;
+    *out = nullptr;
+    tdp_batch* b = new tdp_batch();
+    try {
+        if (!desc) throw TdpError{TDP_ERR_INVALID_ARGUMENT, "desc is NULL"};
+        const int n = desc->num_particles;
+        if (n < 0 || num_clusters < 0) throw TdpError{TDP_ERR_INVALID_ARGUMENT, "negative size"};
+        if (!cluster_offsets) throw TdpError{TDP_ERR_INVALID_ARGUMENT, "cluster_offsets is NULL"};
+        if (n > 0 && (!desc->charges || !desc->molecular_dipoles || !desc->polarizabilities ||
+                      !desc->thole_damping || !desc->axis_types || !desc->atom_z || !desc->atom_x || !desc->atom_y))
+            throw TdpError{TDP_ERR_INVALID_ARGUMENT, "a per-particle array is NULL"};
+        if (desc->nonbonded_method != TDP_NO_CUTOFF)
+            throw TdpError{TDP_ERR_UNSUPPORTED, "cluster batches are isolated systems: NoCutoff only"};
+        if (desc->polarization_type < 0 || desc->polarization_type > 2)
+            throw TdpError{TDP_ERR_INVALID_ARGUMENT, "Polarization type not recognized."};
+        if (desc->precision != TDP_PRECISION_MIXED && desc->precision != TDP_PRECISION_DOUBLE)
+            throw TdpError{TDP_ERR_INVALID_ARGUMENT, "unknown precision"};
+        if (desc->solver != TDP_SOLVER_CG)
+            throw TdpError{TDP_ERR_UNSUPPORTED, "cluster batches solve Mutual polarization by conjugate gradients"};
+        if (cluster_offsets[0] != 0 || cluster_offsets[num_clusters] != n)
+            throw TdpError{TDP_ERR_INVALID_ARGUMENT, "cluster_offsets must run from 0 to num_particles"};
+        for (int c = 0; c < num_clusters; c++)
+            if (cluster_offsets[c + 1] < cluster_offsets[c])
+                throw TdpError{TDP_ERR_INVALID_ARGUMENT, "cluster_offsets must be non-decreasing"};
+        validate_axes(n, desc->axis_types, desc->atom_z, desc->atom_x, desc->atom_y);
+
+        b->n = n;
+        b->nc = num_clusters;
+        b->precision = desc->precision;
+        b->polarization = desc->polarization_type;
+        b->coff.assign(cluster_offsets, cluster_offsets + num_clusters + 1);
+        std::vector<int> cl_of(n);
+        for (int c = 0; c < num_clusters; c++)
+            for (int i = b->coff[c]; i < b->coff[c + 1]; i++) cl_of[i] = c;
+        auto same = [&](int i, int j, const char* what) {
+            if (j >= 0 && cl_of[j] != cl_of[i]) {
+                char buf[200];
+                snprintf(buf, sizeof buf, "particle %d: %s particle %d lies in another cluster", i, what, j);
+                throw TdpError{TDP_ERR_INVALID_ARGUMENT, buf};
+            }
+        };
+        std::vector<int> axis(4 * (size_t)n);
+        for (int i = 0; i < n; i++) {
+            axis[4 * i] = desc->axis_types[i];
+            axis[4 * i + 1] = desc->atom_z[i];
+            axis[4 * i + 2] = desc->atom_x[i];
+            axis[4 * i + 3] = desc->atom_y[i];
+            if (desc->axis_types[i] != TDP_NO_AXIS_TYPE) {
+                same(i, desc->atom_z[i], "axis");
+                same(i, desc->atom_x[i], "axis");
+                if (desc->axis_types[i] == TDP_ZBISECT || desc->axis_types[i] == TDP_THREEFOLD)
+                    same(i, desc->atom_y[i], "axis");
+            }
+        }
+        auto exc = covalent_exceptions(n, desc->covalent12_offsets, desc->covalent12_atoms,
+                                       desc->covalent13_offsets, desc->covalent13_atoms);
+        std::vector<int> eoff(n + 1, 0), ej;
+        std::vector<double> em, es;
+        for (int i = 0; i < n; i++) {
+            for (auto& t : exc[i]) {
+                same(i, std::get<0>(t), "covalent");
+                ej.push_back(std::get<0>(t));
+                em.push_back(std::get<1>(t));
+                es.push_back(std::get<2>(t));
+            }
+            eoff[i + 1] = (int)ej.size();
+        }
+        std::vector<int> uoff;
+        std::vector<int2> users;
+        torque_users(n, axis, uoff, users);
+
+        std::vector<int> order(num_clusters);
+        std::iota(order.begin(), order.end(), 0);
+        std::stable_sort(order.begin(), order.end(), [&](int x, int y) {
+            return b->coff[x + 1] - b->coff[x] > b->coff[y + 1] - b->coff[y];
+        });
+        for (int c = 0; c < num_clusters; c++) {
+            b->max_atoms = std::max(b->max_atoms, b->coff[c + 1] - b->coff[c]);
+            b->max_exc = std::max(b->max_exc, eoff[b->coff[c + 1]] - eoff[b->coff[c]]);
+        }
+        if (desc->num_extrapolation_coefficients > 0 && desc->extrapolation_coefficients)
+            b->extrap.assign(desc->extrapolation_coefficients,
+                             desc->extrapolation_coefficients + desc->num_extrapolation_coefficients);
+        else
+            b->extrap = {-0.154, 0.017, 0.658, 0.474};  // RTDF.cpp:857-864
+
+        TDP_CUDA(cudaGetDevice(&b->device));
+        TDP_CUDA(cudaDeviceGetAttribute(&b->num_sms, cudaDevAttrMultiProcessorCount, b->device));
+        int optin = 0;
+        TDP_CUDA(cudaDeviceGetAttribute(&optin, cudaDevAttrMaxSharedMemoryPerBlockOptin, b->device));
+        b->smem_optin = (size_t)optin;
+        if (smem_for(b) > b->smem_optin) {
+            char buf[220];
+            snprintf(buf, sizeof buf,
+                     "largest cluster (%d atoms, %d exceptions) needs %zu bytes of shared memory; %d available",
+                     b->max_atoms, b->max_exc, smem_for(b), optin);
+            throw TdpError{TDP_ERR_UNSUPPORTED, buf};
+        }
+
+        BatchArgs& a = b->args;
+        a.num_clusters = num_clusters;
+        a.max_atoms = std::max(1, b->max_atoms);
+        a.max_exc = b->max_exc;
+        a.korder = std::max(1, (int)b->extrap.size());
+        a.polarization = b->polarization;
+        a.max_iter = std::max(0, desc->mutual_max_iterations);
+        a.target_eps = desc->mutual_target_epsilon;
+        std::vector<double> th(desc->thole_damping, desc->thole_damping + n);
+        a.damp_r2 = damp_radius2(th);
+        const bool r4 = (desc->flags & TDP_FLAG_DD_FORCE_R4) != 0;
+        a.rinv4_power = r4 ? 1.0 : 0.0;
+        a.rinv4_fill = 0.0;
+
+        auto& o = b->owned;
+        int* d_order = dalloc<int>(num_clusters, o);
+        int* d_coff = dalloc<int>(num_clusters + 1, o);
+        double* d_pos = dalloc<double>(3 * (size_t)n, o);
+        double* d_q = dalloc<double>(n, o);
+        double* d_dm = dalloc<double>(3 * (size_t)n, o);
+        double* d_al = dalloc<double>(n, o);
+        double* d_th = dalloc<double>(n, o);
+        int4* d_ax = dalloc<int4>(n, o);
+        int* d_eoff = dalloc<int>(n + 1, o);
+        int* d_ej = dalloc<int>(ej.size(), o);
+        double* d_em = dalloc<double>(em.size(), o);
+        double* d_es = dalloc<double>(es.size(), o);
+        int* d_uoff = dalloc<int>(n + 1, o);
+        int2* d_users = dalloc<int2>(users.size(), o);
+        double* d_coef = dalloc<double>(b->extrap.size(), o);
+        a.queue = dalloc<int>(1, o);
+        a.forces = dalloc<double>(3 * (size_t)n, o);
+        a.mu_out = dalloc<double>(3 * (size_t)n, o);
+        a.energy = dalloc<double>(num_clusters, o);
+        a.iters = dalloc<int>(num_clusters, o);
+        a.eps = dalloc<double>(num_clusters, o);
+        upload(d_order, order.data(), sizeof(int) * num_clusters);
+        upload(d_coff, b->coff.data(), sizeof(int) * (num_clusters + 1));
+        upload(d_q, desc->charges, sizeof(double) * n);
+        upload(d_dm, desc->molecular_dipoles, sizeof(double) * 3 * n);
+        upload(d_al, desc->polarizabilities, sizeof(double) * n);
+        upload(d_th, desc->thole_damping, sizeof(double) * n);
+        upload(d_ax, axis.data(), sizeof(int) * 4 * n);
+        upload(d_eoff, eoff.data(), sizeof(int) * (n + 1));
+        upload(d_ej, ej.data(), sizeof(int) * ej.size());
+        upload(d_em, em.data(), sizeof(double) * em.size());
+        upload(d_es, es.data(), sizeof(double) * es.size());
+        upload(d_uoff, uoff.data(), sizeof(int) * (n + 1));
+        upload(d_users, users.data(), sizeof(int2) * users.size());
+        upload(d_coef, b->extrap.data(), sizeof(double) * b->extrap.size());
+        a.order = d_order;
+        a.coff = d_coff;
+        a.pos = d_pos;
+        a.charge = d_q;
+        a.dip_mol = d_dm;
+        a.alpha = d_al;
+        a.thole = d_th;
+        a.axis = d_ax;
+        a.exc_off = d_eoff;
+        a.exc_j = d_ej;
+        a.exc_m = d_em;
+        a.exc_s = d_es;
+        a.users_off = d_uoff;
+        a.users = d_users;
+        a.coef = d_coef;
+        TDP_CUDA(cudaEventCreate(&b->ev0));
+        TDP_CUDA(cudaEventCreate(&b->ev1));
+    } catch (const TdpError& e) {
+        int code = batch_fail(nullptr, e);
+        tdp_batch_destroy(b);
+        return code;
+    }
+    *out = b;
+    return TDP_OK;
+}
+
+int tdp_batch_set_stream(tdp_batch* b, void* stream) {
+    if (!b) return TDP_ERR_INVALID_ARGUMENT;
+    b->stream = static_cast<cudaStream_t>(stream);
+    return TDP_OK;
+}
+
+int tdp_batch_compute(tdp_batch* b, const double* positions, int32_t on_device, double* forces, double* energies) {
+    if (!b) return TDP_ERR_INVALID_ARGUMENT;
+    try {
+        if (b->n > 0 && !positions) throw TdpError{TDP_ERR_INVALID_ARGUMENT, "positions is NULL"};
+        if (b->nc == 0) return TDP_OK;
+        cudaStream_t st = b->stream;
+        const size_t n3 = 3 * (size_t)b->n;
+        if (n3)
+            TDP_CUDA(cudaMemcpyAsync((void*)b->args.pos, positions, sizeof(double) * n3,
+                                     on_device ? cudaMemcpyDeviceToDevice : cudaMemcpyHostToDevice, st));
+        if (!b->tuned) autotune(b);
+        TDP_CUDA(cudaEventRecord(b->ev0, st));
+        TDP_CUDA(cudaGraphLaunch(b->exec, st));
+        TDP_CUDA(cudaEventRecord(b->ev1, st));
+        const cudaMemcpyKind kind = on_device ? cudaMemcpyDeviceToDevice : cudaMemcpyDeviceToHost;
+        if (forces && n3) TDP_CUDA(cudaMemcpyAsync(forces, b->args.forces, sizeof(double) * n3, kind, st));
+        if (energies) TDP_CUDA(cudaMemcpyAsync(energies, b->args.energy, sizeof(double) * b->nc, kind, st));
+        TDP_CUDA(cudaEventSynchronize(b->ev1));
+        float ms = 0.f;
+        TDP_CUDA(cudaEventElapsedTime(&ms, b->ev0, b->ev1));
+        b->last_ms = ms;
+        if (!on_device) TDP_CUDA(cudaStreamSynchronize(st));
+        TDP_CUDA(cudaGetLastError());
+        b->have_results = true;
+    } catch (const TdpError& e) {
+        return batch_fail(b, e);
+    }
+    return TDP_OK;
+}
+
+int tdp_batch_get_induced_dipoles(tdp_batch* b, double* out) {
+    if (!b || !out) return TDP_ERR_INVALID_ARGUMENT;
+    try {
+        if (!b->have_results) throw TdpError{TDP_ERR_INVALID_ARGUMENT, "no tdp_batch_compute yet"};
+        if (b->n)
+            TDP_CUDA(cudaMemcpyAsync(out, b->args.mu_out, sizeof(double) * 3 * b->n, cudaMemcpyDeviceToHost, b->stream));
+        TDP_CUDA(cudaStreamSynchronize(b->stream));
+    } catch (const TdpError& e) {
+        return batch_fail(b, e);
+    }
+    return TDP_OK;
+}
+
+int tdp_batch_solver_stats(tdp_batch* b, int32_t* iterations, double* epsilons) {
+    if (!b) return TDP_ERR_INVALID_ARGUMENT;
+    try {
+        if (!b->have_results) throw TdpError{TDP_ERR_INVALID_ARGUMENT, "no tdp_batch_compute yet"};
+        if (iterations && b->nc)
+            TDP_CUDA(cudaMemcpyAsync(iterations, b->args.iters, sizeof(int) * b->nc, cudaMemcpyDeviceToHost, b->stream));
+        if (epsilons && b->nc)
+            TDP_CUDA(cudaMemcpyAsync(epsilons, b->args.eps, sizeof(double) * b->nc, cudaMemcpyDeviceToHost, b->stream));
+        TDP_CUDA(cudaStreamSynchronize(b->stream));
+    } catch (const TdpError& e) {
+        return batch_fail(b, e);
+    }
+    return TDP_OK;
+}
+
+int tdp_batch_tile(const tdp_batch* b, int32_t* threads, int32_t* lanes, int32_t* ctas, double* last_ms) {
+    if (!b) return TDP_ERR_INVALID_ARGUMENT;
+    if (threads) *threads = b->tuned ? b->threads : 0;
+    if (lanes) *lanes = b->tuned ? b->lmax : 0;
+    if (ctas) *ctas = b->tuned ? b->ctas : 0;
+    if (last_ms) *last_ms = b->last_ms;
+    return TDP_OK;
+}
+
+int tdp_batch_tile_candidates(const tdp_batch* b, int32_t capacity, int32_t* threads, int32_t* lanes, double* ms) {
+    if (!b) return TDP_ERR_INVALID_ARGUMENT;
+    for (int k = 0; k < kNumShapes && k < capacity; k++) {
+        if (threads) threads[k] = kShapes[k].threads;
+        if (lanes) lanes[k] = kShapes[k].lmax;
+        if (ms) ms[k] = k < (int)b->tune_ms.size() ? b->tune_ms[k] : -1.0;
+    }
+    return kNumShapes;
+}
+
+}  // extern "C"

@@ -6,6 +6,7 @@
 // driven as ReferenceCalcTholeDipoleForceKernel does in
 // platforms/reference/src/ReferenceTholeDipoleKernels.cpp).
 #include "tholedipole_b200.h"
+#include "tdp_host.h"
 #include "tdp_kernels.cuh"
 
 #include <cuda_runtime.h>
@@ -29,28 +30,6 @@ void noalloc_clear_error();
 namespace {
 
 thread_local std::string g_create_error;
-
-struct TdpError {
-    int code;
-    std::string msg;
-};
-
-#define TDP_CUDA(call)                                                                                      \
-    do {                                                                                                    \
-        cudaError_t e_ = (call);                                                                            \
-        if (e_ != cudaSuccess)                                                                              \
-            throw TdpError{TDP_ERR_CUDA, std::string(#call) + ": " + cudaGetErrorString(e_)};              \
-    } while (0)
-
-template <class T>
-T* dalloc(size_t count, std::vector<void*>& owned) {
-    void* p = nullptr;
-    if (count == 0) count = 1;
-    TDP_CUDA(cudaMalloc(&p, count * sizeof(T)));
-    TDP_CUDA(cudaMemset(p, 0, count * sizeof(T)));
-    owned.push_back(p);
-    return static_cast<T*>(p);
-}
 
 }  // namespace
 
@@ -128,67 +107,6 @@ int fail(tdp_handle* h, const TdpError& e) {
     return e.code;
 }
 
-// ---------------------------------------------------------------------------
-// Validation: TholeDipoleForceImpl::initialize (openmmapi/src/TholeDipoleForceImpl.cpp:52-108)
-// plus the inputs on which the reference dereferences null or out-of-range
-// memory (rotation of an atom with Z set and no X atom, RTDF.cpp:556-568;
-// covalent lists longer than the five scale entries, RTDF.cpp:609-633).
-// ---------------------------------------------------------------------------
-void validate_axes(int n, const int32_t* types, const int32_t* zs, const int32_t* xs, const int32_t* ys) {
-    for (int i = 0; i < n; i++) {
-        int t = types[i], z = zs[i], x = xs[i], y = ys[i];
-        char buf[256];
-        if (t < TDP_ZTHENX || t > TDP_NO_AXIS_TYPE) {
-            snprintf(buf, sizeof buf,
-                     "TholeDipoleForce: axis type=%d not currently handled - only axisTypes[ 0, 1, 2, 3, 4, 5] "
-                     "(ZThenX, Bisector, Z-Bisect, ThreeFold, ZOnly, NoAxisType) currently handled.",
-                     t);
-            throw TdpError{TDP_ERR_INVALID_ARGUMENT, buf};
-        }
-        if (t != TDP_NO_AXIS_TYPE && (z < 0 || z >= n)) {
-            snprintf(buf, sizeof buf, "TholeDipoleForce: invalid z axis particle: %d", z);
-            throw TdpError{TDP_ERR_INVALID_ARGUMENT, buf};
-        }
-        if (t != TDP_NO_AXIS_TYPE && t != TDP_ZONLY && (x < 0 || x >= n)) {
-            snprintf(buf, sizeof buf, "TholeDipoleForce: invalid x axis particle: %d", x);
-            throw TdpError{TDP_ERR_INVALID_ARGUMENT, buf};
-        }
-        if ((t == TDP_ZBISECT || t == TDP_THREEFOLD) && (y < 0 || y >= n)) {
-            snprintf(buf, sizeof buf, "TholeDipoleForce: invalid y axis particle: %d", y);
-            throw TdpError{TDP_ERR_INVALID_ARGUMENT, buf};
-        }
-        if (z >= n || x >= n || y >= n) {
-            snprintf(buf, sizeof buf, "TholeDipoleForce: axis particle index out of range for particle %d", i);
-            throw TdpError{TDP_ERR_INVALID_ARGUMENT, buf};
-        }
-        if (z >= 0 && z != i && t != TDP_ZONLY && x < 0) {
-            snprintf(buf, sizeof buf,
-                     "TholeDipoleForce: particle %d has a z axis particle but no x axis particle (the reference "
-                     "platform dereferences a null particle here)",
-                     i);
-            throw TdpError{TDP_ERR_INVALID_ARGUMENT, buf};
-        }
-    }
-}
-
-double damp_radius2(const std::vector<double>& thole) {
-    // a*u^3 < 50 needs r < t_i t_j (50/min(t_i,t_j))^(1/3) <= tmax^(5/3) 50^(1/3).
-    double tmax = 0.0;
-    bool negative = false;
-    for (double t : thole) {
-        if (t < 0.0 || std::isnan(t)) negative = true;
-        tmax = std::max(tmax, t);
-    }
-    if (negative) return INFINITY;
-    if (tmax == 0.0) return 0.0;
-    double r = std::pow(tmax, 5.0 / 3.0) * std::cbrt(50.0) * 1.001;
-    return r * r;
-}
-
-void upload(void* dst, const void* src, size_t bytes) {
-    if (bytes) TDP_CUDA(cudaMemcpy(dst, src, bytes, cudaMemcpyHostToDevice));
-}
-
 // Per-particle parameters and everything derived from them.
 void upload_params(tdp_handle* h) {
     int n = h->n;
@@ -203,23 +121,11 @@ void upload_params(tdp_handle* h) {
     upload(d.axis, h->axis.data(), sizeof(int) * 4 * n);
     d.pp.damp_r2 = (float)damp_radius2(h->thole);
 
-    // Torque-mapping users (RTDF.cpp:915-1115): which atoms receive force from
-    // the frame of atom i, and in which role.
-    std::vector<std::vector<std::pair<int, int>>> users(n);
-    for (int i = 0; i < n; i++) {
-        int t = h->axis[4 * i], z = h->axis[4 * i + 1], x = h->axis[4 * i + 2], y = h->axis[4 * i + 3];
-        if (t == TDP_NO_AXIS_TYPE) continue;
-        users[i].push_back({i, 0});
-        users[z].push_back({i, 1});
-        if (t != TDP_ZONLY && x >= 0) users[x].push_back({i, 2});
-        if ((t == TDP_ZBISECT || t == TDP_THREEFOLD) && y > -1) users[y].push_back({i, 3});
-    }
-    std::vector<int> off(n + 1, 0);
+    // Torque-mapping users: which atoms receive force from the frame of atom
+    // i, and in which role.
+    std::vector<int> off;
     std::vector<int2> flat;
-    for (int a = 0; a < n; a++) {
-        for (auto& u : users[a]) flat.push_back(make_int2(u.first, u.second));
-        off[a + 1] = (int)flat.size();
-    }
+    torque_users(n, h->axis, off, flat);
     if (d.users) {
         cudaFree(d.users);
         h->owned.erase(std::find(h->owned.begin(), h->owned.end(), (void*)d.users));
@@ -807,44 +713,9 @@ int tdp_create(const tdp_system_desc* desc, tdp_handle** out) {
             h->axis[4 * i + 3] = desc->atom_y[i];
         }
 
-        // Covalent scales (RTDF.cpp:609-644): pair (i<j) takes _mScale[pos] for
-        // j at list position pos of Covalent12(i) and _iScale[pos] for
-        // Covalent13(i), the last occurrence winning; lists of more than five
-        // entries index past the scale tables in the reference.
-        static const double kM[5] = {0.0, 0.0, 0.0, 0.5, 1.0};
-        static const double kI[5] = {0.0, 1.0, 1.0, 1.0, 1.0};
-        std::map<std::pair<int, int>, std::pair<double, double>> scales;
-        for (int i = 0; i < n; i++) {
-            for (int list = 0; list < 2; list++) {
-                const int32_t* off = list == 0 ? desc->covalent12_offsets : desc->covalent13_offsets;
-                const int32_t* atoms = list == 0 ? desc->covalent12_atoms : desc->covalent13_atoms;
-                if (!off) continue;
-                int b = off[i], e = off[i + 1];
-                if (e - b > 5) {
-                    char buf[200];
-                    snprintf(buf, sizeof buf,
-                             "TholeDipoleForce: particle %d has %d Covalent1%d entries; only five scale factors exist",
-                             i, e - b, list == 0 ? 2 : 3);
-                    throw TdpError{TDP_ERR_INVALID_ARGUMENT, buf};
-                }
-                for (int p = b; p < e; p++) {
-                    int j = atoms[p];
-                    if (j <= i || j >= n) continue;  // only the lower-index atom's list counts
-                    auto it = scales.find({i, j});
-                    if (it == scales.end()) it = scales.insert({{i, j}, {1.0, 1.0}}).first;
-                    if (list == 0) it->second.first = kM[p - b];
-                    else it->second.second = kI[p - b];
-                }
-            }
-        }
         std::vector<std::vector<std::tuple<int, double, double>>>& exc = h->exc_user;
-        exc.assign(n, {});
-        for (auto& kv : scales) {
-            double m = kv.second.first, s = kv.second.second;
-            if (m == 1.0 && s == 1.0) continue;
-            exc[kv.first.first].push_back(std::make_tuple(kv.first.second, m, s));
-            exc[kv.first.second].push_back(std::make_tuple(kv.first.first, m, s));
-        }
+        exc = covalent_exceptions(n, desc->covalent12_offsets, desc->covalent12_atoms, desc->covalent13_offsets,
+                                  desc->covalent13_atoms);
         std::vector<int> eoff(n + 1, 0), ej;
         std::vector<double> em, es;
         int n_tiles_pad = std::max(kBlockI, ((n + kBlockI - 1) / kBlockI) * kBlockI) / kTile;

@@ -192,6 +192,41 @@ def cluster_batch(n_clusters: int = 1024, lo: int = 4, hi: int = 64, seed: int =
     return [water_cluster(int(s), rng, **kw) for s in sizes]
 
 
+def concat_clusters(clusters: Sequence[TholeSystem]):
+    """One TholeSystem holding every cluster's particles in order (axis atoms
+    and covalent partners shifted to global indices) and the n_clusters+1
+    particle offsets.  Settings (polarization, target, limits) come from the
+    first cluster."""
+    offs = np.zeros(len(clusters) + 1, dtype=np.int32)
+    for k, c in enumerate(clusters):
+        offs[k + 1] = offs[k] + c.n
+    if not clusters:
+        z3 = np.zeros((0, 3))
+        return TholeSystem(positions=z3, charges=np.zeros(0), dipoles=z3.copy(), polarizabilities=np.zeros(0),
+                           tholes=np.zeros(0), axis=np.zeros((0, 4), dtype=np.int32), cov12=[], cov13=[]), offs
+    axis = []
+    cov12: List[List[int]] = []
+    cov13: List[List[int]] = []
+    for k, c in enumerate(clusters):
+        a0 = int(offs[k])
+        ax = np.asarray(c.axis, dtype=np.int32).reshape(c.n, 4).copy()
+        ax[:, 1:] = np.where(ax[:, 1:] >= 0, ax[:, 1:] + a0, ax[:, 1:])
+        axis.append(ax)
+        cov12 += [[j + a0 for j in l] for l in c.cov12]
+        cov13 += [[j + a0 for j in l] for l in c.cov13]
+    f = clusters[0]
+    cat = lambda name: np.concatenate([np.asarray(getattr(c, name), dtype=np.float64) for c in clusters])
+    masses = None
+    if all(c.masses is not None for c in clusters):
+        masses = cat("masses")
+    sys_ = TholeSystem(positions=cat("positions").reshape(-1, 3), charges=cat("charges"),
+                       dipoles=cat("dipoles").reshape(-1, 3), polarizabilities=cat("polarizabilities"),
+                       tholes=cat("tholes"), axis=np.concatenate(axis), cov12=cov12, cov13=cov13,
+                       method=NO_CUTOFF, polarization=f.polarization, target_eps=f.target_eps,
+                       max_iter=f.max_iter, extrap=f.extrap, masses=masses)
+    return sys_, offs
+
+
 # The measured configurations (216, 4096 and 32768 waters; cutoffs 0.8 / 0.9 nm).
 def config_small(seed: int = 0, **kw) -> TholeSystem:
     return water_box(6, 1.8643, seed=seed, cutoff=0.8, **kw)
