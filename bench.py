@@ -21,7 +21,12 @@ Reported (one JSON line, rank 0):
                (FP32 SGEMM measured here); roofline_hbm: the same kernel
                against the measured HBM copy bandwidth
   cpu_baseline the reference's own FP64 code (compiled oracle/_ref), 1 core,
-               timed on a 6,144-atom sample and scaled to this box
+               timed on a 6,591-atom sample and scaled to this box
+  clusters     the batched-cluster workload (1024 NoCutoff water clusters of
+               4-64 waters in one persistent launch): clusters/s mixed and
+               plain, device-resident and end to end, the autotuner's table,
+               per-cluster errors against the FP64 oracle, and the compiled
+               reference on one core over 384 of the clusters
 
 `--impl reference` times the reference's CPU implementation on all host cores
 instead (rank 0 only).
@@ -275,6 +280,106 @@ def _recorded_sweeps() -> int:
 
 
 # ---------------------------------------------------------------------------
+# Cluster batches: 1024 isolated water clusters, sizes uniform in [4, 64]
+# waters, NoCutoff, mutual polarization to 1e-6, one persistent launch.
+# ---------------------------------------------------------------------------
+N_CLUSTERS = 1024
+
+
+def _cluster_workload(seed):
+    from tholedipoleplugin_b200 import systems as S
+    return S.cluster_batch(N_CLUSTERS, 4, 64, seed=seed, target_eps=1e-6, max_iter=500)
+
+
+def _ref_clusters(args):
+    """(seconds, clusters) of the compiled reference over a slice of the cluster workload."""
+    sys.path.insert(0, ROOT)
+    from oracle import oracle as O
+    seed, lo, hi = args
+    clusters = _cluster_workload(seed)[lo:hi]
+    t = time.perf_counter()
+    for c in clusters:
+        O.compute(c, "reference", dipoles=False)
+    return time.perf_counter() - t, len(clusters)
+
+
+def run_clusters(args, rank, world, barrier, max_over_ranks, stream):
+    import numpy as np
+    import torch
+    from tholedipoleplugin_b200.batch import ClusterBatch
+
+    clusters = _cluster_workload(3 + 100 * rank)
+    res = {"workload": f"{N_CLUSTERS} isolated water clusters, 4-64 waters each (seeded), NoCutoff, "
+                       "mutual polarization to 1e-6, one persistent graph-captured launch per evaluation"}
+    reps = max(5, args.steps)
+    for prec in ("mixed", "double"):
+        with ClusterBatch(clusters, precision=prec) as b:
+            b.setStream(stream.cuda_stream)
+            b.compute()  # autotunes the tile shape, captures the graph
+            pos = torch.tensor(b.positions, dtype=torch.float64, device="cuda")
+            frc = torch.zeros_like(pos)
+            en = torch.zeros(b.num_clusters, dtype=torch.float64, device="cuda")
+            for _ in range(max(3, args.warmup)):
+                b.compute_device(pos.data_ptr(), frc.data_ptr(), en.data_ptr())
+            torch.cuda.synchronize()
+            barrier()
+            s0, s1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+            s0.record(stream)
+            for _ in range(reps):
+                b.compute_device(pos.data_ptr(), frc.data_ptr(), en.data_ptr())
+            s1.record(stream)
+            torch.cuda.synchronize()
+            t_ms = max_over_ranks(s0.elapsed_time(s1) / reps)
+            # End to end: host positions in, host forces and energies out, every call.
+            hpos = torch.empty((b.n, 3), dtype=torch.float64, pin_memory=True).numpy()
+            hpos[...] = b.positions
+            barrier()
+            t0 = time.perf_counter()
+            for _ in range(reps):
+                b.compute(hpos)
+            t_e2e = max_over_ranks((time.perf_counter() - t0) / reps)
+            it, ep = b.solverStats()
+            tile = b.tile()
+            cand = b.tileCandidates()
+            res[prec] = {"clusters_per_s": world * N_CLUSTERS / (t_ms * 1e-3), "ms_per_launch": t_ms,
+                         "e2e_clusters_per_s": world * N_CLUSTERS / t_e2e, "n_atoms": b.n,
+                         "cg_iterations_mean": float(it.mean()), "cg_iterations_max": int(it.max()),
+                         "max_epsilon": float(ep.max()),
+                         "tile": {"threads": tile["threads"], "lanes_per_atom": tile["lanes"], "ctas": tile["ctas"]},
+                         "autotuner_ms": {f"{c['threads']}x{c['lanes']}": round(c["ms"], 4) for c in cand}}
+            if prec == "mixed":
+                e_mixed, f_mixed = b.compute()
+                offs = b.offsets
+    res["mixed_over_plain"] = res["mixed"]["clusters_per_s"] / res["double"]["clusters_per_s"]
+    # Pair work of one evaluation: every cluster's fixed field, its matvecs and its energy pass.
+    sizes = np.diff(offs).astype(np.float64)
+    pairs = float((sizes * (sizes - 1) / 2).sum())
+    res["unordered_pairs"] = pairs
+    if rank == 0:
+        from oracle import oracle as O
+        # Per-cluster error against the FP64 oracle (converged to 1e-12) on a seeded sample.
+        sample = np.random.default_rng(0).choice(N_CLUSTERS, 32, replace=False)
+        e_rel, f_rel = [], []
+        for k in sample:
+            c = clusters[k]
+            ref = O.compute(c.copy(target_eps=1e-12, max_iter=5000), "port")
+            sl = slice(int(offs[k]), int(offs[k + 1]))
+            e_rel.append(abs(e_mixed[k] - ref.energy) / abs(ref.energy))
+            f_rel.append(rel_rms(f_mixed[sl], ref.forces))
+        res["errors_mixed_vs_fp64_oracle"] = {
+            "clusters_sampled": len(sample), "energy_rel_median": float(np.median(e_rel)),
+            "energy_rel_max": float(np.max(e_rel)), "force_rms_rel_median": float(np.median(f_rel)),
+            "force_rms_rel_max": float(np.max(f_rel)),
+            "note": "batch at the workload's 1e-6 target; oracle converged to 1e-12"}
+        if world == 1 and O.reference_available():
+            t, m = _ref_clusters((3, 0, 384))
+            res["cpu_baseline"] = {"value": m / t, "unit": "clusters/s", "cores": 1, "kind": "reference",
+                                   "sample": f"compiled reference on the first {m} clusters of the workload, "
+                                             f"1 core, {t:.1f}s"}
+    return res
+
+
+# ---------------------------------------------------------------------------
 # Our arm.
 # ---------------------------------------------------------------------------
 def rel_rms(a, b):
@@ -424,6 +529,9 @@ def run_ours(args):
                                "cg_iterations": {"mixed": it_mixed, "plain": it_plain},
                                "what": "rotation + permanent field + CG to 1e-6 from mu0 = alpha E"}
     out["md_ns_per_day_mixed_over_plain"] = value / out["plain"]["ns_per_day"]
+
+    # ---- cluster batches (1024 NoCutoff clusters of 4-64 waters, one launch) -------------
+    out["clusters"] = run_clusters(args, rank, world, barrier, max_over_ranks, stream)
 
     # ---- errors (rank 0) ---------------------------------------------------------------
     if rank == 0:
