@@ -716,10 +716,36 @@ int tdp_create(const tdp_system_desc* desc, tdp_handle** out) {
         std::vector<std::vector<std::tuple<int, double, double>>>& exc = h->exc_user;
         exc = covalent_exceptions(n, desc->covalent12_offsets, desc->covalent12_atoms, desc->covalent13_offsets,
                                   desc->covalent13_atoms);
+        // Launch geometry of the pair kernels: 32-atom tiles in bands of
+        // band_tiles tiles, one CTA per band pair.  Bands are as wide as
+        // possible (16 tiles, so the J records and sums of a band fit shared
+        // memory) while still giving about 16 CTAs per SM.
+        Dev& d = h->d;
+        const int nt = std::max(1, (n + kTile - 1) / kTile);
+        int band = 1;
+        for (int cand : {16, 8, 4, 2}) {
+            long nb = (nt + cand - 1) / cand;
+            if (nb * (nb + 1) / 2 >= 16L * 148) {
+                band = cand;
+                break;
+            }
+        }
+        if (const char* e = getenv("TDP_BAND_TILES")) {
+            int v = atoi(e);
+            if (v == 1 || v == 2 || v == 4 || v == 8 || v == 16) band = v;
+        }
+        const int pad = kTile * std::max(4, band);
+        d.n = n;
+        d.n_pad = std::max(pad, ((n + pad - 1) / pad) * pad);
+        d.nvb = std::max(1, (n + kVecThreads - 1) / kVecThreads);
+        d.pp.band_tiles = band;
+        d.pp.n_bands = (nt + band - 1) / band;
+        d.nsplit = d.pp.n_bands;
+        d.n_eblk = d.pp.n_bands * (d.pp.n_bands + 1) / 2;
+
         std::vector<int> eoff(n + 1, 0), ej;
         std::vector<double> em, es;
-        int n_tiles_pad = std::max(kBlockI, ((n + kBlockI - 1) / kBlockI) * kBlockI) / kTile;
-        std::vector<int2> etiles(n_tiles_pad, make_int2(1 << 30, -1));  // empty range
+        std::vector<int2> etiles(d.n_pad / kTile, make_int2(1 << 30, -1));  // empty range
         for (int i = 0; i < n; i++) {
             for (auto& t : exc[i]) {
                 int j = std::get<0>(t);
@@ -733,19 +759,6 @@ int tdp_create(const tdp_system_desc* desc, tdp_handle** out) {
             eoff[i + 1] = (int)ej.size();
         }
 
-        // Launch geometry.
-        Dev& d = h->d;
-        d.n = n;
-        d.n_pad = std::max(kBlockI, ((n + kBlockI - 1) / kBlockI) * kBlockI);
-        d.nvb = std::max(1, (n + kVecThreads - 1) / kVecThreads);
-        int n_iblk = d.n_pad / kBlockI;
-        int n_stage = d.n_pad / kJStage;
-        int want = (4 * 148 * 8 + n_iblk - 1) / n_iblk;
-        if (const char* e = getenv("TDP_NSPLIT")) want = std::max(1, atoi(e));
-        want = std::max(1, std::min(want, n_stage));
-        int chunk_stages = (n_stage + want - 1) / want;
-        d.pp.j_chunk = chunk_stages * kJStage;
-        d.nsplit = (n_stage + chunk_stages - 1) / chunk_stages;
         d.pp.n = n;
         d.pp.n_tiles = (n + kTile - 1) / kTile;
         d.pp.mutual = h->polarization == TDP_MUTUAL ? 1 : 0;
@@ -784,7 +797,7 @@ int tdp_create(const tdp_system_desc* desc, tdp_handle** out) {
         d.q = dalloc<double>(n3, o);
         d.hist = dalloc<double>(n3 * h->extrap.size(), o);
         d.partial = dalloc<double>((size_t)d.nsplit * 6 * d.n_pad, o);
-        d.energy_partial = dalloc<double>((size_t)d.nsplit * n_iblk, o);
+        d.energy_partial = dalloc<double>((size_t)d.n_eblk, o);
         d.fpair = dalloc<double>(n3, o);
         d.torque = dalloc<double>(n3, o);
         d.ftotal = dalloc<double>(n3, o);

@@ -8,8 +8,6 @@
 namespace tdp {
 
 constexpr int kTile = 32;          // atoms per tile (one warp's i-atoms, one j-subtile)
-constexpr int kBlockI = 128;       // i-atoms (threads) per pair-kernel block
-constexpr int kJStage = 128;       // j-atoms staged in shared memory per step
 constexpr int kVecThreads = 256;   // threads per block of the O(N) vector kernels
 
 template <class R> struct Vec4T;
@@ -28,7 +26,8 @@ struct PairParams {
     float rinv4_power;     // 1: rInvVec[4] = 1/r^4; 0: the constant rinv4_fill
     float rinv4_fill;
     int mutual;            // polarization type is Mutual (adds the Uind-Uind terms)
-    int j_chunk;           // j-atoms per blockIdx.y split (multiple of kJStage)
+    int band_tiles;        // 32-atom tiles per band of the pair kernels (1..16)
+    int n_bands;           // bands covering the n_tiles real tiles
 };
 
 __device__ __forceinline__ float rsqrt_r(float x) { return rsqrtf(x); }

@@ -1,23 +1,13 @@
 // tdp_kernels.cu -- sm_100a kernels of the TholeDipoleForce hot path in the
 // reference's semantics (aehogan/tholedipoleplugin,
-// platforms/reference/src/ReferenceTholeDipoleForce.cpp, "RTDF.cpp").
-//
-// Pair kernels (permanent field, mutual-field matvec, energy/force/torque)
-// are all-pairs and ordered: every thread owns one i-atom and visits every
-// j-atom, so no atomics and no j-side reductions are needed and the result is
-// deterministic.  A block owns kBlockI consecutive i-atoms (one 32-atom tile
-// per warp); blockIdx.y splits the j range, and each split writes its partial
-// sums to a scratch buffer that the consumer kernel reduces in a fixed order.
-// j-atoms are staged kJStage at a time in shared memory with 16-byte vector
-// loads and read back as warp-wide broadcasts.
+// platforms/reference/src/ReferenceTholeDipoleForce.cpp, "RTDF.cpp"): packing
+// of the tile records, lab-frame rotation, the O(N) kernels of the solvers,
+// the torque gather and the queries.  The all-pairs kernels (permanent field,
+// mutual-field matvec, energy/force/torque) are in tdp_sym.cu; they leave
+// per-band partial sums that the consumers here reduce in a fixed order.
 //
 // Mixed form: positions are FP32 offsets from FP64 32-atom tile centres, so
-// near pairs keep full FP32 precision wherever they are in the box; the
-// minimum image of a tile pair is taken in FP64 and per-pair folding is done
-// only where the tiles' extents reach half a box, with pairs within a few ulp
-// of the half-box boundary re-derived in FP64 so that the image chosen always
-// matches the FP64 reference.  Each thread's per-subtile sums are added to
-// FP64 accumulators.
+// near pairs keep full FP32 precision wherever they are in the box.
 #include "tdp_frames.cuh"
 #include "tdp_kernels.cuh"
 #include "tdp_pairs.cuh"
@@ -144,425 +134,6 @@ __global__ void k_rotate(int n, const double* __restrict__ pos, const double* __
     v.w = (R)thole[i];
     dipt[i] = v;
     dipt_s[rank[i]] = v;
-}
-
-// ---------------------------------------------------------------------------
-// Pair-loop machinery.
-// ---------------------------------------------------------------------------
-// Per-(warp, j-subtile) geometry: displacement of the j tile centre from the
-// i tile centre (FP64, minimum image), and which dimensions need per-pair
-// folding.
-struct TileGeom {
-    double dcx, dcy, dcz;
-    bool fold;
-    bool near;  // some pair may be within the Thole damping range
-};
-
-__device__ __forceinline__ TileGeom tile_geom(const PairParams& P, double4 cA, double4 eA, double4 cB, double4 eB) {
-    TileGeom g;
-    g.dcx = cB.x - cA.x;
-    g.dcy = cB.y - cA.y;
-    g.dcz = cB.z - cA.z;
-    g.fold = false;
-    if (P.periodic) {
-        g.dcx = fold_d(g.dcx, P.box[0], P.inv_box[0]);
-        g.dcy = fold_d(g.dcy, P.box[1], P.inv_box[1]);
-        g.dcz = fold_d(g.dcz, P.box[2], P.inv_box[2]);
-        g.fold = fabs(g.dcx) + eA.x + eB.x >= P.half_box_tol[0] || fabs(g.dcy) + eA.y + eB.y >= P.half_box_tol[1] ||
-                 fabs(g.dcz) + eA.z + eB.z >= P.half_box_tol[2];
-    }
-    // Smallest distance any pair of the two tiles can have (per dimension the
-    // gap between the tiles' boxes; folded pairs are never closer).
-    double gx = fmax(fabs(g.dcx) - eA.x - eB.x, 0.0);
-    double gy = fmax(fabs(g.dcy) - eA.y - eB.y, 0.0);
-    double gz = fmax(fabs(g.dcz) - eA.z - eB.z, 0.0);
-    g.near = g.fold || gx * gx + gy * gy + gz * gz < (double)P.damp_r2;
-    return g;
-}
-
-// Exact FP64 minimum-image displacement p_j - p_i (the reference's own
-// arithmetic), used for exceptions and for FP32 pairs near the half-box.
-__device__ __forceinline__ d3 exact_delta(const PairParams& P, const double* __restrict__ pos, int i, int j) {
-    d3 d = ld3(pos + 3 * j) - ld3(pos + 3 * i);
-    if (P.periodic) {
-        d.x = fold_d(d.x, P.box[0], P.inv_box[0]);
-        d.y = fold_d(d.y, P.box[1], P.inv_box[1]);
-        d.z = fold_d(d.z, P.box[2], P.inv_box[2]);
-    }
-    return d;
-}
-
-// Displacement of j from i inside a j-subtile loop.  For R = float the i offset
-// has already been shifted by the tile displacement; for R = double positions
-// are absolute.
-template <class R, bool FOLD>
-__device__ __forceinline__ void pair_delta(const PairParams& P, const double* __restrict__ pos, int i, int j, R pjx,
-                                           R pjy, R pjz, R oix, R oiy, R oiz, R& dx, R& dy, R& dz) {
-    dx = pjx - oix;
-    dy = pjy - oiy;
-    dz = pjz - oiz;
-    if (FOLD) {
-        if (sizeof(R) == 4) {
-            dx = (R)fold_f((float)dx, (float)P.box[0], (float)P.inv_box[0]);
-            dy = (R)fold_f((float)dy, (float)P.box[1], (float)P.inv_box[1]);
-            dz = (R)fold_f((float)dz, (float)P.box[2], (float)P.inv_box[2]);
-            if ((fabs(dx) > (R)P.half_box_tol[0] || fabs(dy) > (R)P.half_box_tol[1] ||
-                 fabs(dz) > (R)P.half_box_tol[2]) && i < P.n && j < P.n) {
-                d3 e = exact_delta(P, pos, i, j);
-                dx = (R)e.x;
-                dy = (R)e.y;
-                dz = (R)e.z;
-            }
-        } else {
-            dx = (R)fold_d((double)dx, P.box[0], P.inv_box[0]);
-            dy = (R)fold_d((double)dy, P.box[1], P.inv_box[1]);
-            dz = (R)fold_d((double)dz, P.box[2], P.inv_box[2]);
-        }
-    }
-}
-
-template <class R>
-__device__ __forceinline__ R masked_r2(R r2, bool dirty, int i, int j, int n) {
-    if (dirty && (j == i || j >= n)) return (R)INFINITY;
-    return r2;
-}
-
-// ---------------------------------------------------------------------------
-// Field kernels: KIND 0 = permanent field (j records: posq + lab dipole/thole),
-// KIND 1 = mutual-field matvec T*v (j records: posq + v/thole).
-// ---------------------------------------------------------------------------
-// SLOW subtiles are the diagonal tile, the ragged last tile and tiles holding
-// covalent partners of the warp's atoms: there self/padding pairs are masked
-// and each pair's M/I scale is applied in place, so excluded terms are never
-// formed.
-template <class R, int KIND, bool FOLD, bool SLOW, bool DAMP>
-__device__ __forceinline__ void field_subtile(const PairParams& P, const double* __restrict__ pos,
-                                              const typename Vec4T<R>::type* __restrict__ sp,
-                                              const typename Vec4T<R>::type* __restrict__ sv, int i, int jbase,
-                                              R oix, R oiy, R oiz, R ti, R damp_r2, const int* __restrict__ exc_j,
-                                              const double* __restrict__ exc_m, const double* __restrict__ exc_s,
-                                              int e0, int e1, R& fx, R& fy, R& fz) {
-    // Bit jj set: j = jbase + jj is one of i's covalent partners; those pairs
-    // are left out of the loop and added once below with their scale.
-    unsigned partners = 0u;
-    if (SLOW)
-        for (int e = e0; e < e1; e++) {
-            unsigned off = (unsigned)(exc_j[e] - jbase);
-            if (off < (unsigned)kTile) partners |= 1u << off;
-        }
-#pragma unroll 4
-    for (int jj = 0; jj < kTile; jj++) {
-        typename Vec4T<R>::type pj = sp[jj];
-        typename Vec4T<R>::type vj = sv[jj];
-        int j = jbase + jj;
-        R dx, dy, dz;
-        pair_delta<R, FOLD>(P, pos, i, j, pj.x, pj.y, pj.z, oix, oiy, oiz, dx, dy, dz);
-        R r2 = dx * dx + dy * dy + dz * dz;
-        if (SLOW && (j == i || j >= P.n || ((partners >> jj) & 1u))) r2 = (R)INFINITY;
-        if (KIND == 0)
-            pair_fixed<R, DAMP>(dx, dy, dz, r2, pj.w, vj.x, vj.y, vj.z, ti, vj.w, damp_r2, fx, fy, fz);
-        else
-            pair_matvec<R, DAMP>(dx, dy, dz, r2, vj.x, vj.y, vj.z, ti, vj.w, damp_r2, fx, fy, fz);
-    }
-    if (SLOW) {
-#pragma unroll 1
-        for (int e = e0; e < e1; e++) {
-            unsigned off = (unsigned)(exc_j[e] - jbase);
-            if (off >= (unsigned)kTile) continue;
-            R scale = (R)(KIND == 0 ? exc_m[e] : exc_s[e]);
-            if (scale == R(0)) continue;
-            typename Vec4T<R>::type pj = sp[off];
-            typename Vec4T<R>::type vj = sv[off];
-            R dx, dy, dz;
-            pair_delta<R, FOLD>(P, pos, i, jbase + off, pj.x, pj.y, pj.z, oix, oiy, oiz, dx, dy, dz);
-            R r2 = dx * dx + dy * dy + dz * dz;
-            R tx = 0, ty = 0, tz = 0;
-            if (KIND == 0)
-                pair_fixed<R, true>(dx, dy, dz, r2, pj.w, vj.x, vj.y, vj.z, ti, vj.w, damp_r2, tx, ty, tz);
-            else
-                pair_matvec<R, true>(dx, dy, dz, r2, vj.x, vj.y, vj.z, ti, vj.w, damp_r2, tx, ty, tz);
-            fx += scale * tx;
-            fy += scale * ty;
-            fz += scale * tz;
-        }
-    }
-}
-
-template <class R, int KIND>
-__global__ void __launch_bounds__(kBlockI) k_field(PairParams P, const typename Vec4T<R>::type* __restrict__ posq,
-                                                   const typename Vec4T<R>::type* __restrict__ jvec,
-                                                   const double4* __restrict__ tctr,
-                                                   const double4* __restrict__ text,
-                                                   const double* __restrict__ pos, const int* __restrict__ exc_off,
-                                                   const int* __restrict__ exc_j, const double* __restrict__ exc_m,
-                                                   const double* __restrict__ exc_s, const int2* __restrict__ exc_tiles,
-                                                   int n_pad, double* __restrict__ partial) {
-    typedef typename Vec4T<R>::type V4;
-    __shared__ V4 s_pos[kJStage];
-    __shared__ V4 s_vec[kJStage];
-    __shared__ double4 s_ctr[kJStage / kTile];
-    __shared__ double4 s_ext[kJStage / kTile];
-
-    const int i = blockIdx.x * kBlockI + threadIdx.x;
-    const int A = i >> 5;
-    const V4 pi = posq[i];
-    const R ti = jvec[i].w;
-    const double4 cA = tctr[A];
-    const double4 eA = text[A];
-    const int2 etile = exc_tiles[A];
-    const int e0 = i < P.n ? exc_off[i] : 0;
-    const int e1 = i < P.n ? exc_off[i + 1] : 0;
-    const R damp_r2 = (R)P.damp_r2;
-    double ax = 0.0, ay = 0.0, az = 0.0;
-
-    const int jtot = P.n_tiles * kTile;
-    const int jbeg = blockIdx.y * P.j_chunk;
-    const int jend = min(jbeg + P.j_chunk, jtot);
-    for (int j0 = jbeg; j0 < jend; j0 += kJStage) {
-        __syncthreads();
-        for (int k = threadIdx.x; k < kJStage; k += kBlockI) {
-            s_pos[k] = posq[j0 + k];
-            s_vec[k] = jvec[j0 + k];
-        }
-        if (threadIdx.x < kJStage / kTile) {
-            s_ctr[threadIdx.x] = tctr[(j0 >> 5) + threadIdx.x];
-            s_ext[threadIdx.x] = text[(j0 >> 5) + threadIdx.x];
-        }
-        __syncthreads();
-        for (int sub = 0; sub < kJStage / kTile; sub++) {
-            const int B = (j0 >> 5) + sub;
-            if (B >= P.n_tiles) break;
-            TileGeom g = tile_geom(P, cA, eA, s_ctr[sub], s_ext[sub]);
-            R oix, oiy, oiz;
-            if (sizeof(R) == 4) {
-                oix = pi.x - (R)g.dcx;
-                oiy = pi.y - (R)g.dcy;
-                oiz = pi.z - (R)g.dcz;
-            } else {
-                // Absolute positions: shift i by the whole-box image that the
-                // tile-level minimum image chose, (cB - cA) - dc = L*k.
-                oix = pi.x + ((s_ctr[sub].x - cA.x) - g.dcx);
-                oiy = pi.y + ((s_ctr[sub].y - cA.y) - g.dcy);
-                oiz = pi.z + ((s_ctr[sub].z - cA.z) - g.dcz);
-            }
-            const bool slow = (B == A) || (B == P.n_tiles - 1 && (P.n & (kTile - 1))) ||
-                              (B >= etile.x && B <= etile.y);
-            R fx = 0, fy = 0, fz = 0;
-            const V4* sp = s_pos + sub * kTile;
-            const V4* sv = s_vec + sub * kTile;
-            const int jbase = B * kTile;
-#define TDP_FSUB(F, S, D)                                                                                        \
-    field_subtile<R, KIND, F, S, D>(P, pos, sp, sv, i, jbase, oix, oiy, oiz, ti, damp_r2, exc_j, exc_m, exc_s, e0, e1, \
-                                    fx, fy, fz)
-            if (slow) {
-                if (g.fold) TDP_FSUB(true, true, true);
-                else TDP_FSUB(false, true, true);
-            } else if (g.fold) {
-                TDP_FSUB(true, false, true);
-            } else if (g.near) {
-                TDP_FSUB(false, false, true);
-            } else {
-                TDP_FSUB(false, false, false);
-            }
-#undef TDP_FSUB
-            ax += (double)fx;
-            ay += (double)fy;
-            az += (double)fz;
-        }
-    }
-    const size_t base = (size_t)blockIdx.y * 3 * n_pad;
-    partial[base + i] = ax;
-    partial[base + n_pad + i] = ay;
-    partial[base + 2 * (size_t)n_pad + i] = az;
-}
-
-// ---------------------------------------------------------------------------
-// Energy / force / torque kernel.
-// ---------------------------------------------------------------------------
-template <class R, bool FOLD, bool SLOW>
-__device__ __forceinline__ void energy_subtile(const PairParams& P, const double* __restrict__ pos,
-                                               const typename Vec4T<R>::type* __restrict__ sp,
-                                               const typename Vec4T<R>::type* __restrict__ sd,
-                                               const typename Vec4T<R>::type* __restrict__ su,
-                                               const double2* __restrict__ yz, int i, int jbase, R oix, R oiy, R oiz,
-                                               double yi, double zi, const EAtom<R>& me, R damp_r2, R rv4p, R rv4f,
-                                               bool upper, const int* __restrict__ exc_j,
-                                               const double* __restrict__ exc_m, const double* __restrict__ exc_s,
-                                               int e0, int e1, R& fx, R& fy, R& fz, R& tx, R& ty, R& tz, R& en) {
-    unsigned partners = 0u;
-    if (SLOW)
-        for (int e = e0; e < e1; e++) {
-            unsigned off = (unsigned)(exc_j[e] - jbase);
-            if (off < (unsigned)kTile) partners |= 1u << off;
-        }
-    // jj < kTile: the loop over the subtile (scale 1, partners masked out);
-    // afterwards, in SLOW subtiles, each covalent partner once with its scales.
-    int e = e0;
-#pragma unroll 1
-    for (int jj = 0; jj < kTile || (SLOW && e < e1); jj++) {
-        R mS = R(1), iS = R(1);
-        int jo = jj;
-        bool extra = jj >= kTile;
-        if (SLOW && extra) {
-            unsigned off = (unsigned)(exc_j[e] - jbase);
-            mS = (R)exc_m[e];
-            iS = (R)exc_s[e];
-            e++;
-            if (off >= (unsigned)kTile || (mS == R(0) && iS == R(0))) continue;
-            jo = (int)off;
-        }
-        typename Vec4T<R>::type pj = sp[jo], dj = sd[jo], uj = su[jo];
-        int j = jbase + jo;
-        R dx, dy, dz;
-        pair_delta<R, FOLD>(P, pos, i, j, pj.x, pj.y, pj.z, oix, oiy, oiz, dx, dy, dz);
-        R r2 = dx * dx + dy * dy + dz * dz;
-        if (SLOW && !extra && (j == i || j >= P.n || ((partners >> jj) & 1u))) r2 = (R)INFINITY;
-        // formQIRotationMatrix's test on the raw positions, pI.y != pK.y ||
-        // pI.z != pK.z (RTDF.cpp:584): displacements above 1e-5 nm decide it;
-        // below that the raw FP64 coordinates are compared.
-        bool yzd = fabs(dy) > R(1e-5) || fabs(dz) > R(1e-5);
-        if (!yzd) {
-            double2 yzj = yz[min(j, P.n_tiles * kTile - 1)];
-            yzd = (yi != yzj.x) || (zi != yzj.y);
-        }
-        EAtom<R> other;
-        other.q = pj.w;
-        other.mx = dj.x;
-        other.my = dj.y;
-        other.mz = dj.z;
-        other.t = dj.w;
-        other.ux = uj.x;
-        other.uy = uj.y;
-        other.uz = uj.z;
-        // The pair is evaluated in the reference's orientation: I = lower index.
-        if (!upper && (!SLOW || j > i))
-            pair_energy<R, true>(dx, dy, dz, r2, yzd, me, other, mS, iS, damp_r2, rv4p, rv4f, P.mutual, fx, fy, fz,
-                                 tx, ty, tz, en);
-        else
-            pair_energy<R, false>(-dx, -dy, -dz, r2, yzd, other, me, mS, iS, damp_r2, rv4p, rv4f, P.mutual, fx, fy,
-                                  fz, tx, ty, tz, en);
-    }
-}
-
-template <class R>
-__global__ void __launch_bounds__(kBlockI) k_energy(PairParams P, const typename Vec4T<R>::type* __restrict__ posq,
-                                                    const typename Vec4T<R>::type* __restrict__ dipt,
-                                                    const typename Vec4T<R>::type* __restrict__ indv,
-                                                    const double2* __restrict__ yz, const double4* __restrict__ tctr,
-                                                    const double4* __restrict__ text, const double* __restrict__ pos,
-                                                    const int* __restrict__ exc_off, const int* __restrict__ exc_j,
-                                                    const double* __restrict__ exc_m, const double* __restrict__ exc_s,
-                                                    const int2* __restrict__ exc_tiles, int n_pad,
-                                                    double* __restrict__ partial,
-                                                    double* __restrict__ energy_partial) {
-    typedef typename Vec4T<R>::type V4;
-    __shared__ V4 s_pos[kJStage];
-    __shared__ V4 s_dip[kJStage];
-    __shared__ V4 s_ind[kJStage];
-    __shared__ double4 s_ctr[kJStage / kTile];
-    __shared__ double4 s_ext[kJStage / kTile];
-    __shared__ double s_red[kBlockI / 32];
-
-    const int i = blockIdx.x * kBlockI + threadIdx.x;
-    const int A = i >> 5;
-    const V4 pi = posq[i];
-    const V4 di = dipt[i];
-    const V4 ui = indv[i];
-    const double2 yzi = yz[i];
-    EAtom<R> me;
-    me.q = pi.w;
-    me.mx = di.x;
-    me.my = di.y;
-    me.mz = di.z;
-    me.t = di.w;
-    me.ux = ui.x;
-    me.uy = ui.y;
-    me.uz = ui.z;
-    const double4 cA = tctr[A];
-    const double4 eA = text[A];
-    const int2 etile = exc_tiles[A];
-    const int e0 = i < P.n ? exc_off[i] : 0;
-    const int e1 = i < P.n ? exc_off[i + 1] : 0;
-    const R damp_r2 = (R)P.damp_r2;
-    const R rv4p = (R)P.rinv4_power, rv4f = (R)P.rinv4_fill;
-    double afx = 0, afy = 0, afz = 0, atx = 0, aty = 0, atz = 0, aen = 0;
-
-    const int jtot = P.n_tiles * kTile;
-    const int jbeg = blockIdx.y * P.j_chunk;
-    const int jend = min(jbeg + P.j_chunk, jtot);
-    for (int j0 = jbeg; j0 < jend; j0 += kJStage) {
-        __syncthreads();
-        for (int k = threadIdx.x; k < kJStage; k += kBlockI) {
-            s_pos[k] = posq[j0 + k];
-            s_dip[k] = dipt[j0 + k];
-            s_ind[k] = indv[j0 + k];
-        }
-        if (threadIdx.x < kJStage / kTile) {
-            s_ctr[threadIdx.x] = tctr[(j0 >> 5) + threadIdx.x];
-            s_ext[threadIdx.x] = text[(j0 >> 5) + threadIdx.x];
-        }
-        __syncthreads();
-        for (int sub = 0; sub < kJStage / kTile; sub++) {
-            const int B = (j0 >> 5) + sub;
-            if (B >= P.n_tiles) break;
-            TileGeom g = tile_geom(P, cA, eA, s_ctr[sub], s_ext[sub]);
-            R oix, oiy, oiz;
-            if (sizeof(R) == 4) {
-                oix = pi.x - (R)g.dcx;
-                oiy = pi.y - (R)g.dcy;
-                oiz = pi.z - (R)g.dcz;
-            } else {
-                // Absolute positions: shift i by the whole-box image that the
-                // tile-level minimum image chose, (cB - cA) - dc = L*k.
-                oix = pi.x + ((s_ctr[sub].x - cA.x) - g.dcx);
-                oiy = pi.y + ((s_ctr[sub].y - cA.y) - g.dcy);
-                oiz = pi.z + ((s_ctr[sub].z - cA.z) - g.dcz);
-            }
-            const bool slow = (B == A) || (B == P.n_tiles - 1 && (P.n & (kTile - 1))) ||
-                              (B >= etile.x && B <= etile.y);
-            // Outside the diagonal tile every j of the subtile is on one side of i.
-            const bool upper = B < A;
-            R fx = 0, fy = 0, fz = 0, tx = 0, ty = 0, tz = 0, en = 0;
-            const int o = sub * kTile;
-            const int jbase = B * kTile;
-#define TDP_ESUB(F, S)                                                                                              \
-    energy_subtile<R, F, S>(P, pos, s_pos + o, s_dip + o, s_ind + o, yz, i, jbase, oix, oiy, oiz, yzi.x, yzi.y,       \
-                            me, damp_r2, rv4p, rv4f, upper && !(S), exc_j, exc_m, exc_s, e0, e1, fx, fy, fz, tx, ty,  \
-                            tz, en)
-            if (g.fold) {
-                if (slow) TDP_ESUB(true, true);
-                else TDP_ESUB(true, false);
-            } else {
-                if (slow) TDP_ESUB(false, true);
-                else TDP_ESUB(false, false);
-            }
-#undef TDP_ESUB
-            afx += (double)fx;
-            afy += (double)fy;
-            afz += (double)fz;
-            atx += (double)tx;
-            aty += (double)ty;
-            atz += (double)tz;
-            aen += (double)en;
-        }
-    }
-    const size_t base = (size_t)blockIdx.y * 6 * n_pad;
-    partial[base + i] = afx;
-    partial[base + n_pad + i] = afy;
-    partial[base + 2 * (size_t)n_pad + i] = afz;
-    partial[base + 3 * (size_t)n_pad + i] = atx;
-    partial[base + 4 * (size_t)n_pad + i] = aty;
-    partial[base + 5 * (size_t)n_pad + i] = atz;
-    // Block energy (threads beyond n contribute nothing).
-    double ev = (i < P.n) ? aen : 0.0;
-    ev = warp_sum(ev);
-    if ((threadIdx.x & 31) == 0) s_red[threadIdx.x >> 5] = ev;
-    __syncthreads();
-    if (threadIdx.x == 0) {
-        double s = 0.0;
-        for (int w = 0; w < kBlockI / 32; w++) s += s_red[w];
-        energy_partial[(size_t)blockIdx.y * gridDim.x + blockIdx.x] = s;
-    }
 }
 
 // forces_out = pair forces + torque-mapped forces (FP64, deterministic).
@@ -1034,35 +605,9 @@ void launch_rotate(const Dev& d, cudaStream_t st) {
                                                                  (typename Vec4T<R>::type*)d.dipt_s);
 }
 
-template <class R>
-void launch_field(const Dev& d, int kind, cudaStream_t st) {
-    dim3 grid(d.n_pad / kBlockI, d.nsplit);
-    typedef typename Vec4T<R>::type V4;
-    // Field kernels run on the spatially sorted records.
-    if (kind == 0)
-        k_field<R, 0><<<grid, kBlockI, 0, st>>>(d.pp, (const V4*)d.posq_s, (const V4*)d.dipt_s, d.tctr_s, d.text_s,
-                                               d.pos_s, d.exs_off, d.exs_j, d.exs_m, d.exs_s, d.exs_tiles, d.n_pad,
-                                               d.partial);
-    else
-        k_field<R, 1><<<grid, kBlockI, 0, st>>>(d.pp, (const V4*)d.posq_s, (const V4*)d.vec_s, d.tctr_s, d.text_s,
-                                               d.pos_s, d.exs_off, d.exs_j, d.exs_m, d.exs_s, d.exs_tiles, d.n_pad,
-                                               d.partial);
-}
-
-template <class R>
-void launch_energy(const Dev& d, cudaStream_t st) {
-    dim3 grid(d.n_pad / kBlockI, d.nsplit);
-    typedef typename Vec4T<R>::type V4;
-    k_energy<R><<<grid, kBlockI, 0, st>>>(d.pp, (const V4*)d.posq, (const V4*)d.dipt, (const V4*)d.ind, d.yz, d.tctr,
-                                          d.text, d.pos, d.exc_off, d.exc_j, d.exc_m, d.exc_s, d.exc_tiles, d.n_pad,
-                                          d.partial, d.energy_partial);
-}
-
 #define TDP_INSTANTIATE(R)                                                                                  \
     template void launch_pack<R>(const Dev&, cudaStream_t);                                                 \
-    template void launch_rotate<R>(const Dev&, cudaStream_t);                                               \
-    template void launch_field<R>(const Dev&, int, cudaStream_t);                                           \
-    template void launch_energy<R>(const Dev&, cudaStream_t);
+    template void launch_rotate<R>(const Dev&, cudaStream_t);
 
 TDP_INSTANTIATE(float)
 TDP_INSTANTIATE(double)
@@ -1125,9 +670,8 @@ void launch_pack_ind(const Dev& d, cudaStream_t st) {
     k_pack_ind<R><<<d.nvb, kVecThreads, 0, st>>>(d.n, d.mu, (typename Vec4T<R>::type*)d.ind);
 }
 void launch_energy_done(const Dev& d, cudaStream_t st) {
-    int n_eblk = (d.n_pad / kBlockI) * d.nsplit;
-    k_energy_done<<<d.nvb, kVecThreads, 0, st>>>(d.n, d.nsplit, d.n_pad, n_eblk, d.partial, d.energy_partial, d.fpair,
-                                                 d.torque, d.energy);
+    k_energy_done<<<d.nvb, kVecThreads, 0, st>>>(d.n, d.nsplit, d.n_pad, d.n_eblk, d.partial, d.energy_partial,
+                                                 d.fpair, d.torque, d.energy);
 }
 void launch_torque_gather(const Dev& d, cudaStream_t st) {
     k_torque_gather<<<d.nvb, kVecThreads, 0, st>>>(d.n, d.pos, d.axis, d.torque, d.users_off, d.users, d.fpair,

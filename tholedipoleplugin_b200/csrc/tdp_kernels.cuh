@@ -6,10 +6,12 @@
 
 namespace tdp {
 
-// All device buffers of one system (sizes: n atoms, n_pad = n rounded up to
-// kBlockI, nsplit j-splits of the pair kernels, nvb blocks of the O(N) kernels).
+// All device buffers of one system (sizes: n atoms, n_pad = n rounded up to a
+// whole number of bands, nsplit partial-sum slots of the pair kernels = one per
+// band, n_eblk energy partials = one per band pair, nvb blocks of the O(N)
+// kernels).
 struct Dev {
-    int n = 0, n_pad = 0, nsplit = 1, nvb = 1;
+    int n = 0, n_pad = 0, nsplit = 1, nvb = 1, n_eblk = 1;
     PairParams pp{};
     // Inputs.
     double* pos = nullptr;       // n_pad*3 (FP64 working copy of the positions)

@@ -77,12 +77,14 @@ struct EAtom {
 // d = p_K - p_I.  The QI frame has rows [X, Y, Z] with Z along d, and the
 // multipole algebra below treats component 0 as the bond axis and back-rotates
 // with the permuted matrix of :150-159, exactly as the reference does.
-// SIDE_I adds the force and torque on I (and the pair energy); otherwise the
-// force and torque on K.  Linear in (mScale, iScale).
-template <class R, bool SIDE_I>
-__device__ __forceinline__ void pair_energy(R dx, R dy, R dz, R r2, bool yz_differ, const EAtom<R>& I,
-                                            const EAtom<R>& K, R mS, R iS, R damp_r2, R rv4_power, R rv4_fill,
-                                            bool mutual, R& fx, R& fy, R& fz, R& tx, R& ty, R& tz, R& en) {
+// SIDES = 1 adds the force and torque on I (and the pair energy) to f/t;
+// SIDES = 2 adds the force and torque on K to f/t; SIDES = 3 adds I's to f/t,
+// K's to g/u and the pair energy.  Linear in (mScale, iScale).
+template <class R, int SIDES>
+__device__ __forceinline__ void pair_energy_sides(R dx, R dy, R dz, R r2, bool yz_differ, const EAtom<R>& I,
+                                                  const EAtom<R>& K, R mS, R iS, R damp_r2, R rv4_power,
+                                                  R rv4_fill, bool mutual, R& fx, R& fy, R& fz, R& tx, R& ty, R& tz,
+                                                  R& gx, R& gy, R& gz, R& ux, R& uy, R& uz, R& en) {
     R rinv = rsqrt_r(r2);
     // QI frame.
     R zx = dx * rinv, zy = dy * rinv, zz = dz * rinv;
@@ -231,7 +233,7 @@ __device__ __forceinline__ void pair_energy(R dx, R dy, R dz, R r2, bool yz_diff
     R fvx = yy * qf0 + zy * qf1 + xy * qf2;
     R fvy = yz * qf0 + zz * qf1 + xz * qf2;
     R fvz = yx * qf0 + zx * qf1 + xx * qf2;
-    if (SIDE_I) {
+    if (SIDES & 1) {
         R EIZ = QI2 * Vij3 - QI3 * Vij2;
         R q0 = -EIX, q1 = -EIY, q2 = -EIZ;
         tx += yy * q0 + zy * q1 + xy * q2;
@@ -245,16 +247,77 @@ __device__ __forceinline__ void pair_energy(R dx, R dy, R dz, R r2, bool yz_diff
         e += R(0.5) * (QI2 * Vij2 + QJ2 * Vji2);
         e += R(0.5) * (QI3 * Vij3 + QJ3 * Vji3);
         en += e;
-    } else {
+    }
+    if (SIDES & 2) {
         R EJZ = QJ2 * Vji3 - QJ3 * Vji2;
         R q0 = -EJX, q1 = -EJY, q2 = -EJZ;
-        tx += yy * q0 + zy * q1 + xy * q2;
-        ty += yz * q0 + zz * q1 + xz * q2;
-        tz += yx * q0 + zx * q1 + xx * q2;
-        fx += fvx;
-        fy += fvy;
-        fz += fvz;
+        R& ox = SIDES == 3 ? ux : tx;
+        R& oy = SIDES == 3 ? uy : ty;
+        R& oz = SIDES == 3 ? uz : tz;
+        R& px = SIDES == 3 ? gx : fx;
+        R& py = SIDES == 3 ? gy : fy;
+        R& pz = SIDES == 3 ? gz : fz;
+        ox += yy * q0 + zy * q1 + xy * q2;
+        oy += yz * q0 + zz * q1 + xz * q2;
+        oz += yx * q0 + zx * q1 + xx * q2;
+        px += fvx;
+        py += fvy;
+        pz += fvz;
     }
+}
+
+// One side of the pair: SIDE_I adds the force and torque on I and the pair
+// energy; otherwise the force and torque on K.
+template <class R, bool SIDE_I>
+__device__ __forceinline__ void pair_energy(R dx, R dy, R dz, R r2, bool yz_differ, const EAtom<R>& I,
+                                            const EAtom<R>& K, R mS, R iS, R damp_r2, R rv4_power, R rv4_fill,
+                                            bool mutual, R& fx, R& fy, R& fz, R& tx, R& ty, R& tz, R& en) {
+    R d0 = 0, d1 = 0, d2 = 0, d3 = 0, d4 = 0, d5 = 0;
+    pair_energy_sides<R, SIDE_I ? 1 : 2>(dx, dy, dz, r2, yz_differ, I, K, mS, iS, damp_r2, rv4_power, rv4_fill,
+                                         mutual, fx, fy, fz, tx, ty, tz, d0, d1, d2, d3, d4, d5, en);
+}
+
+// Both sides of the mutual-field pair: the field at i from v_j and the field
+// at j from v_i (the dipole-field tensor is even in d), I scale applied by the
+// caller.
+template <class R, bool DAMP = true>
+__device__ __forceinline__ void pair_matvec2(R dx, R dy, R dz, R r2, R vix, R viy, R viz, R vjx, R vjy, R vjz, R ti,
+                                             R tj, R damp_r2, R& fix, R& fiy, R& fiz, R& fjx, R& fjy, R& fjz) {
+    R rinv = rsqrt_r(r2);
+    R rinv2 = rinv * rinv;
+    R rr3 = rinv * rinv2;
+    R rr5 = R(3) * rr3 * rinv2;
+    if (DAMP) damp_field(r2, rinv, ti, tj, damp_r2, rr3, rr5);
+    R ddj = rr5 * (vjx * dx + vjy * dy + vjz * dz);
+    R ddi = rr5 * (vix * dx + viy * dy + viz * dz);
+    fix += ddj * dx - rr3 * vjx;
+    fiy += ddj * dy - rr3 * vjy;
+    fiz += ddj * dz - rr3 * vjz;
+    fjx += ddi * dx - rr3 * vix;
+    fjy += ddi * dy - rr3 * viy;
+    fjz += ddi * dz - rr3 * viz;
+}
+
+// Both sides of the permanent-field pair (calculateFixedDipoleFieldPairIxn,
+// RTDF.cpp:678-713), M scale applied by the caller:
+//   E_i -= d (rr3 q_j - rr5 mu_j.d) + mu_j rr3,  E_j += d (rr3 q_i + rr5 mu_i.d) - mu_i rr3.
+template <class R, bool DAMP = true>
+__device__ __forceinline__ void pair_fixed2(R dx, R dy, R dz, R r2, R qi, R mix, R miy, R miz, R qj, R mjx, R mjy,
+                                            R mjz, R ti, R tj, R damp_r2, R& fix, R& fiy, R& fiz, R& fjx, R& fjy,
+                                            R& fjz) {
+    R rinv = rsqrt_r(r2);
+    R rinv2 = rinv * rinv;
+    R rr3 = rinv * rinv2;
+    R rr5 = R(3) * rr3 * rinv2;
+    if (DAMP) damp_field(r2, rinv, ti, tj, damp_r2, rr3, rr5);
+    R a = rr3 * qj - rr5 * (mjx * dx + mjy * dy + mjz * dz);
+    R b = rr3 * qi + rr5 * (mix * dx + miy * dy + miz * dz);
+    fix -= dx * a + mjx * rr3;
+    fiy -= dy * a + mjy * rr3;
+    fiz -= dz * a + mjz * rr3;
+    fjx += dx * b - mix * rr3;
+    fjy += dy * b - miy * rr3;
+    fjz += dz * b - miz * rr3;
 }
 
 }  // namespace tdp

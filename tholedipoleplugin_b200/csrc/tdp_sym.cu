@@ -1,0 +1,814 @@
+// tdp_sym.cu -- the all-pairs kernels of the box path (permanent field,
+// mutual-field matvec, energy/force/torque), each unordered pair evaluated
+// once with both of its sides.
+//
+// Work decomposition.  Atoms form 32-atom tiles and tiles form bands of
+// band_tiles tiles.  One CTA (4 warps) owns a band pair (p, q), p <= q, and
+// evaluates every tile pair (I in band p, J in band q, I <= J).  A warp holds
+// the 32 atoms of I in registers (lane = atom) and walks the 32 atoms of J
+// along the diagonals of the 32x32 tile: at step s lane l pairs with atom
+// (l + s) mod 32 of J, read from shared memory, and the J-side sums travel
+// with it, one lane per step, by shuffles, so after 32 steps lane l holds the
+// J-side sums of atom l.  The J-side sums of band q collect in FP64 in shared
+// memory; the four warps of a CTA visit different J tiles in every round
+// (a staggered schedule with a barrier per round), so no two warps add to the
+// same atom at once and the order of the additions is fixed.
+//
+// Output.  Partial sums go to slot s of a [n_bands][components][n_pad] FP64
+// buffer: CTA (p, q) writes the I-side sums of band p into slot q and the
+// J-side sums of band q into slot p (on the diagonal, p == q, both into slot
+// p).  Every (slot, atom) is written by exactly one CTA, and the consumers sum
+// the slots of an atom in slot order, so results are bitwise deterministic.
+//
+// Tile pairs are classified as in the reference's arithmetic requires: FOLD
+// where the tiles' extents reach half a box (per-pair minimum image with an
+// FP64 fallback near the half-box boundary), DAMP where some pair may lie
+// within the Thole damping range, SLOW on the diagonal tile, the ragged last
+// tile and tiles holding covalent partners.  In SLOW tile pairs, self and
+// padding pairs and the partners are masked out of the diagonal walk; each
+// partner pair is then evaluated once per side with its M/I scales.
+#include "tdp_frames.cuh"
+#include "tdp_kernels.cuh"
+#include "tdp_pairs.cuh"
+
+#include <math.h>
+
+namespace tdp {
+
+namespace {
+
+constexpr int kSymWarps = 4;
+constexpr int kSymThreads = 32 * kSymWarps;
+constexpr unsigned kFull = 0xffffffffu;
+
+// Band pair of CTA k, enumerated q = 0, 1, ... and p = 0..q: k = q(q+1)/2 + p.
+__device__ __forceinline__ void band_pair(int k, int& p, int& q) {
+    int qq = (int)((sqrt(8.0 * (double)k + 1.0) - 1.0) * 0.5);
+    while ((qq + 1) * (qq + 2) / 2 <= k) qq++;
+    while (qq * (qq + 1) / 2 > k) qq--;
+    q = qq;
+    p = k - qq * (qq + 1) / 2;
+}
+
+// Geometry of a tile pair: displacement of J's centre from I's (FP64, minimum
+// image), whether any pair needs per-pair folding, whether any pair can be
+// within the damping range.
+struct TileGeom {
+    double dcx, dcy, dcz;
+    bool fold;
+    bool near;
+};
+
+__device__ __forceinline__ TileGeom tile_geom(const PairParams& P, double4 cA, double4 eA, double4 cB, double4 eB) {
+    TileGeom g;
+    g.dcx = cB.x - cA.x;
+    g.dcy = cB.y - cA.y;
+    g.dcz = cB.z - cA.z;
+    g.fold = false;
+    if (P.periodic) {
+        g.dcx = fold_d(g.dcx, P.box[0], P.inv_box[0]);
+        g.dcy = fold_d(g.dcy, P.box[1], P.inv_box[1]);
+        g.dcz = fold_d(g.dcz, P.box[2], P.inv_box[2]);
+        g.fold = fabs(g.dcx) + eA.x + eB.x >= P.half_box_tol[0] || fabs(g.dcy) + eA.y + eB.y >= P.half_box_tol[1] ||
+                 fabs(g.dcz) + eA.z + eB.z >= P.half_box_tol[2];
+    }
+    // Smallest distance any pair of the two tiles can have (per dimension the
+    // gap between the tiles' boxes; folded pairs are never closer).
+    double gx = fmax(fabs(g.dcx) - eA.x - eB.x, 0.0);
+    double gy = fmax(fabs(g.dcy) - eA.y - eB.y, 0.0);
+    double gz = fmax(fabs(g.dcz) - eA.z - eB.z, 0.0);
+    g.near = g.fold || gx * gx + gy * gy + gz * gz < (double)P.damp_r2;
+    return g;
+}
+
+// Exact FP64 minimum-image displacement p_j - p_i (the reference's own
+// arithmetic), for FP32 pairs near the half-box.
+__device__ __forceinline__ d3 exact_delta(const PairParams& P, const double* __restrict__ pos, int i, int j) {
+    d3 d = ld3(pos + 3 * j) - ld3(pos + 3 * i);
+    if (P.periodic) {
+        d.x = fold_d(d.x, P.box[0], P.inv_box[0]);
+        d.y = fold_d(d.y, P.box[1], P.inv_box[1]);
+        d.z = fold_d(d.z, P.box[2], P.inv_box[2]);
+    }
+    return d;
+}
+
+// p_j - p_i from j's record (its own tile frame) and i's record shifted into
+// that frame.
+template <class R, bool FOLD>
+__device__ __forceinline__ void pair_delta(const PairParams& P, const double* __restrict__ pos, int i, int j, R pjx,
+                                           R pjy, R pjz, R oix, R oiy, R oiz, R& dx, R& dy, R& dz) {
+    dx = pjx - oix;
+    dy = pjy - oiy;
+    dz = pjz - oiz;
+    if (FOLD) {
+        if (sizeof(R) == 4) {
+            dx = (R)fold_f((float)dx, (float)P.box[0], (float)P.inv_box[0]);
+            dy = (R)fold_f((float)dy, (float)P.box[1], (float)P.inv_box[1]);
+            dz = (R)fold_f((float)dz, (float)P.box[2], (float)P.inv_box[2]);
+            if ((fabs(dx) > (R)P.half_box_tol[0] || fabs(dy) > (R)P.half_box_tol[1] ||
+                 fabs(dz) > (R)P.half_box_tol[2]) && i < P.n && j < P.n) {
+                d3 e = exact_delta(P, pos, i, j);
+                dx = (R)e.x;
+                dy = (R)e.y;
+                dz = (R)e.z;
+            }
+        } else {
+            dx = (R)fold_d((double)dx, P.box[0], P.inv_box[0]);
+            dy = (R)fold_d((double)dy, P.box[1], P.inv_box[1]);
+            dz = (R)fold_d((double)dz, P.box[2], P.inv_box[2]);
+        }
+    }
+}
+
+// The record of an I-tile atom shifted into J's frame.  FP32: offsets from the
+// tile centres, shifted by the minimum-image centre displacement; FP64:
+// absolute positions, shifted by the whole-box image the tile pair chose.
+template <class R>
+__device__ __forceinline__ void shift_into(const TileGeom& g, double4 cA, double4 cB, R px, R py, R pz, R& ox, R& oy,
+                                           R& oz) {
+    if (sizeof(R) == 4) {
+        ox = px - (R)g.dcx;
+        oy = py - (R)g.dcy;
+        oz = pz - (R)g.dcz;
+    } else {
+        ox = px + (R)((cB.x - cA.x) - g.dcx);
+        oy = py + (R)((cB.y - cA.y) - g.dcy);
+        oz = pz + (R)((cB.z - cA.z) - g.dcz);
+    }
+}
+
+// Pairs of the diagonal walk that are left out: self, padding, listed
+// partners, and on the diagonal tile the second visit of every pair (steps
+// 17..31 and the upper half of step 16 repeat steps 15..1 and 16).
+__device__ __forceinline__ bool skip_pair(int s, int lane, int i, int j, int n, unsigned partners, int jj, bool diag) {
+    bool skip = i >= n || j >= n || ((partners >> jj) & 1u);
+    if (diag) skip = skip || s == 0 || s > 16 || (s == 16 && lane >= 16);
+    return skip;
+}
+
+// Bits of the J-tile atoms listed as covalent partners of atom i.
+__device__ __forceinline__ unsigned partner_bits(const int* __restrict__ exc_j, int e0, int e1, int jbase) {
+    unsigned b = 0u;
+    for (int e = e0; e < e1; e++) {
+        unsigned off = (unsigned)(exc_j[e] - jbase);
+        if (off < 32u) b |= 1u << off;
+    }
+    return b;
+}
+
+// ---------------------------------------------------------------------------
+// Field kernels: KIND 0 = permanent field (records: posq + lab dipole/thole),
+// KIND 1 = mutual-field matvec T*v (records: posq + v/thole).
+// ---------------------------------------------------------------------------
+template <class R, int KIND, bool FOLD, bool SLOW, bool DAMP>
+__device__ __forceinline__ void field_walk(const PairParams& P, const double* __restrict__ pos,
+                                           const typename Vec4T<R>::type* __restrict__ sp,
+                                           const typename Vec4T<R>::type* __restrict__ sv, int lane, int i, int jbase,
+                                           R oix, R oiy, R oiz, R qi, typename Vec4T<R>::type vi, bool diag,
+                                           unsigned partners, R damp_r2, R& fx, R& fy, R& fz, R& gx, R& gy, R& gz) {
+    const int nxt = (lane + 1) & 31;
+#pragma unroll 2
+    for (int s = 0; s < 32; s++) {
+        const int jj = (lane + s) & 31;
+        const typename Vec4T<R>::type pj = sp[jj];
+        const typename Vec4T<R>::type vj = sv[jj];
+        const int j = jbase + jj;
+        R dx, dy, dz;
+        pair_delta<R, FOLD>(P, pos, i, j, pj.x, pj.y, pj.z, oix, oiy, oiz, dx, dy, dz);
+        R r2 = dx * dx + dy * dy + dz * dz;
+        if (SLOW && skip_pair(s, lane, i, j, P.n, partners, jj, diag)) r2 = (R)INFINITY;
+        if (KIND == 0)
+            pair_fixed2<R, DAMP>(dx, dy, dz, r2, qi, vi.x, vi.y, vi.z, pj.w, vj.x, vj.y, vj.z, vi.w, vj.w, damp_r2, fx,
+                                 fy, fz, gx, gy, gz);
+        else
+            pair_matvec2<R, DAMP>(dx, dy, dz, r2, vi.x, vi.y, vi.z, vj.x, vj.y, vj.z, vi.w, vj.w, damp_r2, fx, fy, fz,
+                                  gx, gy, gz);
+        gx = __shfl_sync(kFull, gx, nxt);
+        gy = __shfl_sync(kFull, gy, nxt);
+        gz = __shfl_sync(kFull, gz, nxt);
+    }
+}
+
+// Two I tiles against the same J tile: every J record read from shared
+// memory and every shuffle of the J-side sums serves two pairs, and the two
+// pair evaluations are independent instruction streams.
+template <class R, int KIND, bool FOLD, bool SLOW, bool DAMP>
+__device__ __forceinline__ void field_walk2(const PairParams& P, const double* __restrict__ pos,
+                                            const typename Vec4T<R>::type* __restrict__ sp,
+                                            const typename Vec4T<R>::type* __restrict__ sv, int lane, int jbase,
+                                            int ia, R oax, R oay, R oaz, R qa, typename Vec4T<R>::type va, bool diag_a,
+                                            unsigned part_a, int ib, R obx, R oby, R obz, R qb,
+                                            typename Vec4T<R>::type vb, bool diag_b, unsigned part_b, R damp_r2,
+                                            R* fa, R* fb, R* g) {
+    const int nxt = (lane + 1) & 31;
+#pragma unroll 2
+    for (int s = 0; s < 32; s++) {
+        const int jj = (lane + s) & 31;
+        const typename Vec4T<R>::type pj = sp[jj];
+        const typename Vec4T<R>::type vj = sv[jj];
+        const int j = jbase + jj;
+        R dax, day, daz, dbx, dby, dbz;
+        pair_delta<R, FOLD>(P, pos, ia, j, pj.x, pj.y, pj.z, oax, oay, oaz, dax, day, daz);
+        pair_delta<R, FOLD>(P, pos, ib, j, pj.x, pj.y, pj.z, obx, oby, obz, dbx, dby, dbz);
+        R ra = dax * dax + day * day + daz * daz;
+        R rb = dbx * dbx + dby * dby + dbz * dbz;
+        if (SLOW) {
+            if (skip_pair(s, lane, ia, j, P.n, part_a, jj, diag_a)) ra = (R)INFINITY;
+            if (skip_pair(s, lane, ib, j, P.n, part_b, jj, diag_b)) rb = (R)INFINITY;
+        }
+        if (KIND == 0) {
+            pair_fixed2<R, DAMP>(dax, day, daz, ra, qa, va.x, va.y, va.z, pj.w, vj.x, vj.y, vj.z, va.w, vj.w,
+                                 damp_r2, fa[0], fa[1], fa[2], g[0], g[1], g[2]);
+            pair_fixed2<R, DAMP>(dbx, dby, dbz, rb, qb, vb.x, vb.y, vb.z, pj.w, vj.x, vj.y, vj.z, vb.w, vj.w,
+                                 damp_r2, fb[0], fb[1], fb[2], g[0], g[1], g[2]);
+        } else {
+            pair_matvec2<R, DAMP>(dax, day, daz, ra, va.x, va.y, va.z, vj.x, vj.y, vj.z, va.w, vj.w, damp_r2, fa[0],
+                                  fa[1], fa[2], g[0], g[1], g[2]);
+            pair_matvec2<R, DAMP>(dbx, dby, dbz, rb, vb.x, vb.y, vb.z, vj.x, vj.y, vj.z, vb.w, vj.w, damp_r2, fb[0],
+                                  fb[1], fb[2], g[0], g[1], g[2]);
+        }
+        g[0] = __shfl_sync(kFull, g[0], nxt);
+        g[1] = __shfl_sync(kFull, g[1], nxt);
+        g[2] = __shfl_sync(kFull, g[2], nxt);
+    }
+}
+
+// Partner pairs of a SLOW tile pair, each side once with its scale (M for
+// the permanent field, I for the matvec): lane l adds, for its I atom, the
+// partners in J, and for atom l of J (not on the diagonal tile), the partners
+// in I.
+template <class R, int KIND, bool FOLD>
+__device__ __forceinline__ void field_partners(const PairParams& P, const double* __restrict__ pos,
+                                               const typename Vec4T<R>::type* __restrict__ posq,
+                                               const typename Vec4T<R>::type* __restrict__ jvec,
+                                               const typename Vec4T<R>::type* __restrict__ sp,
+                                               const typename Vec4T<R>::type* __restrict__ sv,
+                                               const int* __restrict__ exc_off, const int* __restrict__ exc_j,
+                                               const double* __restrict__ exc_m, const double* __restrict__ exc_s,
+                                               const TileGeom& g, double4 cA, double4 cB, int lane, int i, int ibase,
+                                               int jbase, int e0, int e1, R oix, R oiy, R oiz, R qi,
+                                               typename Vec4T<R>::type vi, bool diag, R damp_r2, R& fx, R& fy, R& fz,
+                                               R& gx, R& gy, R& gz) {
+    typedef typename Vec4T<R>::type V4;
+#pragma unroll 1
+    for (int e = e0; e < e1; e++) {
+        unsigned off = (unsigned)(exc_j[e] - jbase);
+        if (off >= 32u) continue;
+        R sc = (R)(KIND == 0 ? exc_m[e] : exc_s[e]);
+        if (sc == R(0)) continue;
+        const V4 pj = sp[off], vj = sv[off];
+        R dx, dy, dz;
+        pair_delta<R, FOLD>(P, pos, i, jbase + off, pj.x, pj.y, pj.z, oix, oiy, oiz, dx, dy, dz);
+        R r2 = dx * dx + dy * dy + dz * dz;
+        R tx = 0, ty = 0, tz = 0;
+        if (KIND == 0) pair_fixed<R, true>(dx, dy, dz, r2, pj.w, vj.x, vj.y, vj.z, vi.w, vj.w, damp_r2, tx, ty, tz);
+        else pair_matvec<R, true>(dx, dy, dz, r2, vj.x, vj.y, vj.z, vi.w, vj.w, damp_r2, tx, ty, tz);
+        fx += sc * tx;
+        fy += sc * ty;
+        fz += sc * tz;
+    }
+    if (diag) return;
+    const int jl = jbase + lane;
+    if (jl >= P.n) return;
+    const V4 pl = sp[lane], vl = sv[lane];
+#pragma unroll 1
+    for (int e = exc_off[jl]; e < exc_off[jl + 1]; e++) {
+        const int a = exc_j[e];
+        if ((unsigned)(a - ibase) >= 32u) continue;
+        R sc = (R)(KIND == 0 ? exc_m[e] : exc_s[e]);
+        if (sc == R(0)) continue;
+        const V4 pa = posq[a], va = jvec[a];
+        R ox, oy, oz;
+        shift_into<R>(g, cA, cB, pa.x, pa.y, pa.z, ox, oy, oz);
+        R dx, dy, dz;  // p_a - p_jl
+        pair_delta<R, FOLD>(P, pos, jl, a, ox, oy, oz, pl.x, pl.y, pl.z, dx, dy, dz);
+        R r2 = dx * dx + dy * dy + dz * dz;
+        R tx = 0, ty = 0, tz = 0;
+        if (KIND == 0) pair_fixed<R, true>(dx, dy, dz, r2, pa.w, va.x, va.y, va.z, vl.w, va.w, damp_r2, tx, ty, tz);
+        else pair_matvec<R, true>(dx, dy, dz, r2, va.x, va.y, va.z, vl.w, va.w, damp_r2, tx, ty, tz);
+        gx += sc * tx;
+        gy += sc * ty;
+        gz += sc * tz;
+    }
+}
+
+// One I tile of a warp (lane = atom) and its state against the current J
+// tile.  The tile's centre and extent stay in shared memory (s_ic, s_ie).
+template <class R>
+struct ISlot {
+    typename Vec4T<R>::type pi, vi;
+    int2 et;
+    int Il, I, i, e0, e1;
+    bool act;
+    // Against the current J tile.
+    bool valid, diag, slow, fold, near;
+    unsigned partners;
+    R ox, oy, oz;
+};
+
+template <class R>
+__device__ __forceinline__ void load_slot(ISlot<R>& a, const PairParams& P, int p, int BT, int Il, int lane,
+                                          const typename Vec4T<R>::type* __restrict__ posq,
+                                          const typename Vec4T<R>::type* __restrict__ jvec,
+                                          const int* __restrict__ exc_off, const int2* __restrict__ exc_tiles) {
+    a.Il = Il;
+    a.I = p * BT + Il;
+    a.act = Il < BT && a.I < P.n_tiles;
+    a.i = a.I * 32 + lane;
+    a.pi = {};
+    a.vi = {};
+    a.et = make_int2(1 << 30, -1);
+    a.e0 = a.e1 = 0;
+    if (a.act) {
+        a.pi = posq[a.i];
+        a.vi = jvec[a.i];
+        a.et = exc_tiles[a.I];
+        if (a.i < P.n) {
+            a.e0 = exc_off[a.i];
+            a.e1 = exc_off[a.i + 1];
+        }
+    }
+}
+
+template <class R>
+__device__ __forceinline__ void slot_against(ISlot<R>& a, const PairParams& P, bool same_band, int J, int Jl,
+                                             double4 cA, double4 eA, double4 cB, double4 eB,
+                                             const int* __restrict__ exc_j) {
+    a.valid = a.act && J < P.n_tiles && (!same_band || Jl >= a.Il);
+    if (!a.valid) return;
+    const TileGeom g = tile_geom(P, cA, eA, cB, eB);
+    shift_into<R>(g, cA, cB, a.pi.x, a.pi.y, a.pi.z, a.ox, a.oy, a.oz);
+    a.fold = g.fold;
+    a.near = g.near;
+    a.diag = a.I == J;
+    a.slow = a.diag || (J == P.n_tiles - 1 && (P.n & 31)) || (J >= a.et.x && J <= a.et.y);
+    a.partners = a.slow ? partner_bits(exc_j, a.e0, a.e1, J * 32) : 0u;
+}
+
+template <class R, int KIND>
+__global__ void __launch_bounds__(kSymThreads, 4) k_field_sym(
+    PairParams P, const typename Vec4T<R>::type* __restrict__ posq, const typename Vec4T<R>::type* __restrict__ jvec,
+    const double4* __restrict__ tctr, const double4* __restrict__ text, const double* __restrict__ pos,
+    const int* __restrict__ exc_off, const int* __restrict__ exc_j, const double* __restrict__ exc_m,
+    const double* __restrict__ exc_s, const int2* __restrict__ exc_tiles, int n_pad, double* __restrict__ partial) {
+    typedef typename Vec4T<R>::type V4;
+    extern __shared__ __align__(16) unsigned char smem[];
+    const int BT = P.band_tiles, NA = BT * 32;
+    double* s_acc = reinterpret_cast<double*>(smem);              // 3 * NA: J-side sums of band q
+    double* s_iacc = s_acc + 3 * NA;                               // 6 * kSymThreads: I-side sums, two slots
+    double4* s_ctr = reinterpret_cast<double4*>(s_iacc + 6 * kSymThreads);  // BT
+    double4* s_ext = s_ctr + BT;                                   // BT
+    double4* s_ic = s_ext + BT;                                    // 2 * kSymWarps: the warps' I tiles
+    double4* s_ie = s_ic + 2 * kSymWarps;
+    V4* s_pos = reinterpret_cast<V4*>(s_ie + 2 * kSymWarps);       // NA
+    V4* s_vec = s_pos + NA;                                        // NA
+
+    int p, q;
+    band_pair(blockIdx.x, p, q);
+    const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+    const int qa0 = q * NA;
+    for (int k = threadIdx.x; k < NA; k += kSymThreads) {
+        s_pos[k] = posq[qa0 + k];
+        s_vec[k] = jvec[qa0 + k];
+        s_acc[3 * k] = 0.0;
+        s_acc[3 * k + 1] = 0.0;
+        s_acc[3 * k + 2] = 0.0;
+    }
+    for (int k = threadIdx.x; k < BT; k += kSymThreads) {
+        s_ctr[k] = tctr[q * BT + k];
+        s_ext[k] = text[q * BT + k];
+    }
+    double* my = s_iacc + 6 * threadIdx.x;
+    __syncthreads();
+
+    const R damp_r2 = (R)P.damp_r2;
+    const int stride = BT >= kSymWarps ? BT / kSymWarps : 1;
+    // A warp's I tiles are warp, warp + 4, warp + 8, ...; a round takes two of them.
+    const int rounds = (BT + 2 * kSymWarps - 1) / (2 * kSymWarps);
+    for (int r = 0; r < rounds; r++) {
+        ISlot<R> a, b;
+        load_slot<R>(a, P, p, BT, warp + 2 * kSymWarps * r, lane, posq, jvec, exc_off, exc_tiles);
+        load_slot<R>(b, P, p, BT, warp + 2 * kSymWarps * r + kSymWarps, lane, posq, jvec, exc_off, exc_tiles);
+        if (lane < 2) {
+            const ISlot<R>& s1 = lane == 0 ? a : b;
+            s_ic[2 * warp + lane] = s1.act ? tctr[s1.I] : make_double4(0, 0, 0, 0);
+            s_ie[2 * warp + lane] = s1.act ? text[s1.I] : make_double4(0, 0, 0, 0);
+        }
+        __syncwarp();
+        for (int c = 0; c < 6; c++) my[c] = 0.0;
+        for (int t = 0; t < BT; t++) {
+            const int Jl = (t + warp * stride) % BT;
+            const int J = q * BT + Jl;
+            const double4 cB = s_ctr[Jl], eB = s_ext[Jl];
+            slot_against<R>(a, P, p == q, J, Jl, s_ic[2 * warp], s_ie[2 * warp], cB, eB, exc_j);
+            slot_against<R>(b, P, p == q, J, Jl, s_ic[2 * warp + 1], s_ie[2 * warp + 1], cB, eB, exc_j);
+            if (a.valid || b.valid) {
+                const int jbase = J * 32;
+                const V4* sp = s_pos + Jl * 32;
+                const V4* sv = s_vec + Jl * 32;
+                R fa[3] = {0, 0, 0}, fb[3] = {0, 0, 0}, g[3] = {0, 0, 0};
+                if (a.valid && b.valid) {
+                    const bool slow = a.slow || b.slow, fold = a.fold || b.fold;
+                    const bool near = a.near || b.near;
+#define TDP_FWALK2(F, S, D)                                                                                        \
+    field_walk2<R, KIND, F, S, D>(P, pos, sp, sv, lane, jbase, a.i, a.ox, a.oy, a.oz, a.pi.w, a.vi, a.diag,     \
+                                  a.partners, b.i, b.ox, b.oy, b.oz, b.pi.w, b.vi, b.diag, b.partners, damp_r2, fa, \
+                                  fb, g)
+                    if (slow) {
+                        if (fold) TDP_FWALK2(true, true, true);
+                        else TDP_FWALK2(false, true, true);
+                    } else if (fold) {
+                        TDP_FWALK2(true, false, true);
+                    } else if (near) {
+                        TDP_FWALK2(false, false, true);
+                    } else {
+                        TDP_FWALK2(false, false, false);
+                    }
+#undef TDP_FWALK2
+                } else {
+                    const ISlot<R>& s1 = a.valid ? a : b;
+                    R* f1 = a.valid ? fa : fb;
+#define TDP_FWALK(F, S, D)                                                                                        \
+    field_walk<R, KIND, F, S, D>(P, pos, sp, sv, lane, s1.i, jbase, s1.ox, s1.oy, s1.oz, s1.pi.w, s1.vi, s1.diag, \
+                                 s1.partners, damp_r2, f1[0], f1[1], f1[2], g[0], g[1], g[2])
+                    if (s1.slow) {
+                        if (s1.fold) TDP_FWALK(true, true, true);
+                        else TDP_FWALK(false, true, true);
+                    } else if (s1.fold) {
+                        TDP_FWALK(true, false, true);
+                    } else if (s1.near) {
+                        TDP_FWALK(false, false, true);
+                    } else {
+                        TDP_FWALK(false, false, false);
+                    }
+#undef TDP_FWALK
+                }
+                // Partner pairs of each SLOW slot, each side once.
+                for (int k = 0; k < 2; k++) {
+                    const ISlot<R>& s1 = k == 0 ? a : b;
+                    if (!s1.valid || !s1.slow) continue;
+                    R* f1 = k == 0 ? fa : fb;
+                    const double4 cA = s_ic[2 * warp + k];
+                    const TileGeom g1 = tile_geom(P, cA, s_ie[2 * warp + k], cB, eB);
+                    if (s1.fold)
+                        field_partners<R, KIND, true>(P, pos, posq, jvec, sp, sv, exc_off, exc_j, exc_m, exc_s, g1, cA,
+                                                      cB, lane, s1.i, s1.I * 32, jbase, s1.e0, s1.e1, s1.ox, s1.oy,
+                                                      s1.oz, s1.pi.w, s1.vi, s1.diag, damp_r2, f1[0], f1[1], f1[2],
+                                                      g[0], g[1], g[2]);
+                    else
+                        field_partners<R, KIND, false>(P, pos, posq, jvec, sp, sv, exc_off, exc_j, exc_m, exc_s, g1,
+                                                       cA, cB, lane, s1.i, s1.I * 32, jbase, s1.e0, s1.e1, s1.ox,
+                                                       s1.oy, s1.oz, s1.pi.w, s1.vi, s1.diag, damp_r2, f1[0], f1[1],
+                                                       f1[2], g[0], g[1], g[2]);
+                }
+                // This warp alone visits tile Jl in this round.
+                double* acc = s_acc + 3 * (Jl * 32 + lane);
+                for (int c = 0; c < 3; c++) {
+                    acc[c] += (double)g[c];
+                    my[c] += (double)fa[c];
+                    my[3 + c] += (double)fb[c];
+                }
+            }
+            __syncthreads();
+        }
+        for (int k = 0; k < 2; k++) {
+            const ISlot<R>& s1 = k == 0 ? a : b;
+            if (!s1.act) continue;
+            if (p == q) {
+                double* acc = s_acc + 3 * (s1.Il * 32 + lane);
+                for (int c = 0; c < 3; c++) acc[c] += my[3 * k + c];
+            } else {
+                const size_t base = (size_t)q * 3 * n_pad;
+                for (int c = 0; c < 3; c++) partial[base + (size_t)c * n_pad + s1.i] = my[3 * k + c];
+            }
+        }
+        __syncthreads();
+    }
+    const size_t base = (size_t)p * 3 * n_pad;
+    for (int k = threadIdx.x; k < NA; k += kSymThreads)
+        for (int c = 0; c < 3; c++) partial[base + (size_t)c * n_pad + qa0 + k] = s_acc[3 * k + c];
+}
+
+// ---------------------------------------------------------------------------
+// Energy / force / torque kernel (index order: within a tile pair I < J every
+// lane's atom has the lower index, the reference's orientation I = lower).
+// ---------------------------------------------------------------------------
+template <class R>
+__device__ __forceinline__ EAtom<R> eatom(typename Vec4T<R>::type pq, typename Vec4T<R>::type d,
+                                          typename Vec4T<R>::type u) {
+    EAtom<R> a;
+    a.q = pq.w;
+    a.mx = d.x;
+    a.my = d.y;
+    a.mz = d.z;
+    a.t = d.w;
+    a.ux = u.x;
+    a.uy = u.y;
+    a.uz = u.z;
+    return a;
+}
+
+// formQIRotationMatrix's test on the raw positions, pI.y != pK.y || pI.z !=
+// pK.z (RTDF.cpp:584): displacements above 1e-5 nm decide it; below that the
+// raw FP64 coordinates are compared.
+template <class R>
+__device__ __forceinline__ bool yz_differ(R dy, R dz, const double2* __restrict__ yz, int i, int j, int nmax) {
+    bool d = fabs(dy) > R(1e-5) || fabs(dz) > R(1e-5);
+    if (!d) {
+        const double2 a = yz[min(i, nmax)], b = yz[min(j, nmax)];
+        d = (a.x != b.x) || (a.y != b.y);
+    }
+    return d;
+}
+
+template <class R, bool FOLD, bool SLOW>
+__device__ __forceinline__ void energy_walk(const PairParams& P, const double* __restrict__ pos,
+                                            const double2* __restrict__ yz,
+                                            const typename Vec4T<R>::type* __restrict__ sp,
+                                            const typename Vec4T<R>::type* __restrict__ sd,
+                                            const typename Vec4T<R>::type* __restrict__ su, int lane, int i,
+                                            int jbase, R oix, R oiy, R oiz, const EAtom<R>& me, bool diag,
+                                            unsigned partners, R damp_r2, R rv4p, R rv4f, R f[6], R g[6], R& en) {
+    const int nxt = (lane + 1) & 31;
+    const int nmax = P.n_tiles * 32 - 1;
+#pragma unroll 1
+    for (int s = 0; s < 32; s++) {
+        const int jj = (lane + s) & 31;
+        const int j = jbase + jj;
+        const EAtom<R> other = eatom<R>(sp[jj], sd[jj], su[jj]);
+        R dx, dy, dz;
+        pair_delta<R, FOLD>(P, pos, i, j, sp[jj].x, sp[jj].y, sp[jj].z, oix, oiy, oiz, dx, dy, dz);
+        R r2 = dx * dx + dy * dy + dz * dz;
+        if (SLOW && skip_pair(s, lane, i, j, P.n, partners, jj, diag)) r2 = (R)INFINITY;
+        const bool yzd = yz_differ<R>(dy, dz, yz, i, j, nmax);
+        if (!SLOW || !diag) {
+            pair_energy_sides<R, 3>(dx, dy, dz, r2, yzd, me, other, R(1), R(1), damp_r2, rv4p, rv4f, P.mutual != 0,
+                                    f[0], f[1], f[2], f[3], f[4], f[5], g[0], g[1], g[2], g[3], g[4], g[5], en);
+        } else {
+            // Diagonal tile: the lane's atom is the lower index iff lane + s < 32.
+            const bool lo = lane + s < 32;
+            const EAtom<R> A = lo ? me : other;
+            const EAtom<R> B = lo ? other : me;
+            const R sg = lo ? R(1) : R(-1);
+            R a[6] = {0, 0, 0, 0, 0, 0}, b[6] = {0, 0, 0, 0, 0, 0};
+            pair_energy_sides<R, 3>(sg * dx, sg * dy, sg * dz, r2, yzd, A, B, R(1), R(1), damp_r2, rv4p, rv4f,
+                                    P.mutual != 0, a[0], a[1], a[2], a[3], a[4], a[5], b[0], b[1], b[2], b[3], b[4],
+                                    b[5], en);
+#pragma unroll
+            for (int c = 0; c < 6; c++) {
+                f[c] += lo ? a[c] : b[c];
+                g[c] += lo ? b[c] : a[c];
+            }
+        }
+#pragma unroll
+        for (int c = 0; c < 6; c++) g[c] = __shfl_sync(kFull, g[c], nxt);
+    }
+}
+
+// Partner pairs of a SLOW tile pair with their (M, I) scales, each side once:
+// the lane's I atom with its partners in J (the pair energy is counted on the
+// lower-index side), and atom l of J (off the diagonal) with its partners in I.
+template <class R, bool FOLD>
+__device__ __forceinline__ void energy_partners(
+    const PairParams& P, const double* __restrict__ pos, const double2* __restrict__ yz,
+    const typename Vec4T<R>::type* __restrict__ posq, const typename Vec4T<R>::type* __restrict__ dipt,
+    const typename Vec4T<R>::type* __restrict__ indv, const typename Vec4T<R>::type* __restrict__ sp,
+    const typename Vec4T<R>::type* __restrict__ sd, const typename Vec4T<R>::type* __restrict__ su,
+    const int* __restrict__ exc_off, const int* __restrict__ exc_j, const double* __restrict__ exc_m,
+    const double* __restrict__ exc_s, const TileGeom& geo, double4 cA, double4 cB, int lane, int i, int ibase,
+    int jbase, int e0, int e1, R oix, R oiy, R oiz, const EAtom<R>& me, bool diag, R damp_r2, R rv4p, R rv4f, R f[6],
+    R g[6], R& en) {
+    typedef typename Vec4T<R>::type V4;
+    const int nmax = P.n_tiles * 32 - 1;
+#pragma unroll 1
+    for (int e = e0; e < e1; e++) {
+        unsigned off = (unsigned)(exc_j[e] - jbase);
+        if (off >= 32u) continue;
+        const R mS = (R)exc_m[e], iS = (R)exc_s[e];
+        if (mS == R(0) && iS == R(0)) continue;
+        const int j = jbase + (int)off;
+        const EAtom<R> other = eatom<R>(sp[off], sd[off], su[off]);
+        R dx, dy, dz;
+        pair_delta<R, FOLD>(P, pos, i, j, sp[off].x, sp[off].y, sp[off].z, oix, oiy, oiz, dx, dy, dz);
+        const R r2 = dx * dx + dy * dy + dz * dz;
+        const bool yzd = yz_differ<R>(dy, dz, yz, i, j, nmax);
+        if (j > i)
+            pair_energy<R, true>(dx, dy, dz, r2, yzd, me, other, mS, iS, damp_r2, rv4p, rv4f, P.mutual != 0, f[0],
+                                 f[1], f[2], f[3], f[4], f[5], en);
+        else
+            pair_energy<R, false>(-dx, -dy, -dz, r2, yzd, other, me, mS, iS, damp_r2, rv4p, rv4f, P.mutual != 0,
+                                  f[0], f[1], f[2], f[3], f[4], f[5], en);
+    }
+    if (diag) return;
+    const int jl = jbase + lane;
+    if (jl >= P.n) return;
+    const EAtom<R> mine = eatom<R>(sp[lane], sd[lane], su[lane]);
+    R dummy = 0;
+#pragma unroll 1
+    for (int e = exc_off[jl]; e < exc_off[jl + 1]; e++) {
+        const int a = exc_j[e];
+        if ((unsigned)(a - ibase) >= 32u) continue;
+        const R mS = (R)exc_m[e], iS = (R)exc_s[e];
+        if (mS == R(0) && iS == R(0)) continue;
+        const V4 pa = posq[a];
+        const EAtom<R> A = eatom<R>(pa, dipt[a], indv[a]);
+        R ox, oy, oz;
+        shift_into<R>(geo, cA, cB, pa.x, pa.y, pa.z, ox, oy, oz);
+        R dx, dy, dz;  // p_jl - p_a: a (tile I < J) is the lower index
+        pair_delta<R, FOLD>(P, pos, a, jl, sp[lane].x, sp[lane].y, sp[lane].z, ox, oy, oz, dx, dy, dz);
+        const R r2 = dx * dx + dy * dy + dz * dz;
+        const bool yzd = yz_differ<R>(dy, dz, yz, a, jl, nmax);
+        pair_energy<R, false>(dx, dy, dz, r2, yzd, A, mine, mS, iS, damp_r2, rv4p, rv4f, P.mutual != 0, g[0], g[1],
+                              g[2], g[3], g[4], g[5], dummy);
+    }
+}
+
+template <class R>
+__global__ void __launch_bounds__(kSymThreads, 3) k_energy_sym(
+    PairParams P, const typename Vec4T<R>::type* __restrict__ posq, const typename Vec4T<R>::type* __restrict__ dipt,
+    const typename Vec4T<R>::type* __restrict__ indv, const double2* __restrict__ yz, const double4* __restrict__ tctr,
+    const double4* __restrict__ text, const double* __restrict__ pos, const int* __restrict__ exc_off,
+    const int* __restrict__ exc_j, const double* __restrict__ exc_m, const double* __restrict__ exc_s,
+    const int2* __restrict__ exc_tiles, int n_pad, double* __restrict__ partial, double* __restrict__ energy_partial) {
+    typedef typename Vec4T<R>::type V4;
+    extern __shared__ __align__(16) unsigned char smem[];
+    const int BT = P.band_tiles, NA = BT * 32;
+    double* s_acc = reinterpret_cast<double*>(smem);              // 6 * NA: J-side sums of band q
+    double* s_iacc = s_acc + 6 * NA;                               // 7 * kSymThreads: I-side sums and energy
+    double4* s_ctr = reinterpret_cast<double4*>(s_iacc + 7 * kSymThreads);
+    double4* s_ext = s_ctr + BT;
+    V4* s_pos = reinterpret_cast<V4*>(s_ext + BT);
+    V4* s_dip = s_pos + NA;
+    V4* s_ind = s_dip + NA;
+
+    int p, q;
+    band_pair(blockIdx.x, p, q);
+    const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+    const int qa0 = q * NA;
+    for (int k = threadIdx.x; k < NA; k += kSymThreads) {
+        s_pos[k] = posq[qa0 + k];
+        s_dip[k] = dipt[qa0 + k];
+        s_ind[k] = indv[qa0 + k];
+        for (int c = 0; c < 6; c++) s_acc[6 * k + c] = 0.0;
+    }
+    for (int k = threadIdx.x; k < BT; k += kSymThreads) {
+        s_ctr[k] = tctr[q * BT + k];
+        s_ext[k] = text[q * BT + k];
+    }
+    double* my = s_iacc + 7 * threadIdx.x;
+    my[6] = 0.0;
+    __syncthreads();
+
+    const R damp_r2 = (R)P.damp_r2;
+    const R rv4p = (R)P.rinv4_power, rv4f = (R)P.rinv4_fill;
+    const int stride = BT >= kSymWarps ? BT / kSymWarps : 1;
+    const int rounds = (BT + kSymWarps - 1) / kSymWarps;
+    for (int r = 0; r < rounds; r++) {
+        const int Il = warp + kSymWarps * r;
+        const int I = p * BT + Il;
+        const bool wact = Il < BT && I < P.n_tiles;
+        const int ibase = I * 32;
+        const int i = ibase + lane;
+        V4 pi = {}, di = {}, ui = {};
+        double4 cA = {}, eA = {};
+        int2 et = make_int2(1 << 30, -1);
+        int e0 = 0, e1 = 0;
+        if (wact) {
+            pi = posq[i];
+            di = dipt[i];
+            ui = indv[i];
+            cA = tctr[I];
+            eA = text[I];
+            et = exc_tiles[I];
+            if (i < P.n) {
+                e0 = exc_off[i];
+                e1 = exc_off[i + 1];
+            }
+        }
+        const EAtom<R> me = eatom<R>(pi, di, ui);
+        for (int c = 0; c < 6; c++) my[c] = 0.0;
+        for (int t = 0; t < BT; t++) {
+            const int Jl = (t + warp * stride) % BT;
+            const int J = q * BT + Jl;
+            if (wact && J < P.n_tiles && (p != q || Jl >= Il)) {
+                const double4 cB = s_ctr[Jl];
+                const TileGeom g = tile_geom(P, cA, eA, cB, s_ext[Jl]);
+                R oix, oiy, oiz;
+                shift_into<R>(g, cA, cB, pi.x, pi.y, pi.z, oix, oiy, oiz);
+                const bool diag = I == J;
+                const bool slow = diag || (J == P.n_tiles - 1 && (P.n & 31)) || (J >= et.x && J <= et.y);
+                const int jbase = J * 32;
+                const V4* sp = s_pos + Jl * 32;
+                const V4* sd = s_dip + Jl * 32;
+                const V4* su = s_ind + Jl * 32;
+                const unsigned partners = slow ? partner_bits(exc_j, e0, e1, jbase) : 0u;
+                R f[6] = {0, 0, 0, 0, 0, 0}, gg[6] = {0, 0, 0, 0, 0, 0}, en = 0;
+                if (slow) {
+                    if (g.fold) {
+                        energy_walk<R, true, true>(P, pos, yz, sp, sd, su, lane, i, jbase, oix, oiy, oiz, me, diag,
+                                                   partners, damp_r2, rv4p, rv4f, f, gg, en);
+                        energy_partners<R, true>(P, pos, yz, posq, dipt, indv, sp, sd, su, exc_off, exc_j, exc_m,
+                                                 exc_s, g, cA, cB, lane, i, ibase, jbase, e0, e1, oix, oiy, oiz, me,
+                                                 diag, damp_r2, rv4p, rv4f, f, gg, en);
+                    } else {
+                        energy_walk<R, false, true>(P, pos, yz, sp, sd, su, lane, i, jbase, oix, oiy, oiz, me, diag,
+                                                    partners, damp_r2, rv4p, rv4f, f, gg, en);
+                        energy_partners<R, false>(P, pos, yz, posq, dipt, indv, sp, sd, su, exc_off, exc_j, exc_m,
+                                                  exc_s, g, cA, cB, lane, i, ibase, jbase, e0, e1, oix, oiy, oiz, me,
+                                                  diag, damp_r2, rv4p, rv4f, f, gg, en);
+                    }
+                } else if (g.fold) {
+                    energy_walk<R, true, false>(P, pos, yz, sp, sd, su, lane, i, jbase, oix, oiy, oiz, me, diag,
+                                                partners, damp_r2, rv4p, rv4f, f, gg, en);
+                } else {
+                    energy_walk<R, false, false>(P, pos, yz, sp, sd, su, lane, i, jbase, oix, oiy, oiz, me, diag,
+                                                 partners, damp_r2, rv4p, rv4f, f, gg, en);
+                }
+                double* acc = s_acc + 6 * (Jl * 32 + lane);
+                for (int c = 0; c < 6; c++) {
+                    acc[c] += (double)gg[c];
+                    my[c] += (double)f[c];
+                }
+                my[6] += (double)en;
+            }
+            __syncthreads();
+        }
+        if (wact) {
+            if (p == q) {
+                double* acc = s_acc + 6 * (Il * 32 + lane);
+                for (int c = 0; c < 6; c++) acc[c] += my[c];
+            } else {
+                const size_t b = (size_t)q * 6 * n_pad;
+                for (int c = 0; c < 6; c++) partial[b + (size_t)c * n_pad + i] = my[c];
+            }
+        }
+        __syncthreads();
+    }
+    const size_t b = (size_t)p * 6 * n_pad;
+    for (int k = threadIdx.x; k < NA; k += kSymThreads)
+        for (int c = 0; c < 6; c++) partial[b + (size_t)c * n_pad + qa0 + k] = s_acc[6 * k + c];
+    // CTA energy, summed in thread order (padding atoms contribute exactly 0).
+    double e = warp_sum(my[6]);
+    __shared__ double s_red[kSymWarps];
+    if (lane == 0) s_red[warp] = e;
+    __syncthreads();
+    if (threadIdx.x == 0) {
+        double s = 0.0;
+        for (int w = 0; w < kSymWarps; w++) s += s_red[w];
+        energy_partial[blockIdx.x] = s;
+    }
+}
+
+template <class R>
+size_t field_smem(int BT) {
+    const int NA = 32 * BT;
+    return sizeof(double) * (3 * NA + 6 * kSymThreads) + sizeof(double4) * (2 * BT + 4 * kSymWarps) +
+           sizeof(typename Vec4T<R>::type) * 2 * NA;
+}
+
+template <class R>
+size_t energy_smem(int BT) {
+    const int NA = 32 * BT;
+    return sizeof(double) * (6 * NA + 7 * kSymThreads) + sizeof(double4) * 2 * BT +
+           sizeof(typename Vec4T<R>::type) * 3 * NA;
+}
+
+int band_pairs(const Dev& d) { return d.pp.n_bands * (d.pp.n_bands + 1) / 2; }
+
+}  // namespace
+
+template <class R>
+void launch_field(const Dev& d, int kind, cudaStream_t st) {
+    typedef typename Vec4T<R>::type V4;
+    const size_t smem = field_smem<R>(d.pp.band_tiles);
+    // Field kernels run on the spatially sorted records.
+    if (kind == 0) {
+        cudaFuncSetAttribute(k_field_sym<R, 0>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+        k_field_sym<R, 0><<<band_pairs(d), kSymThreads, smem, st>>>(
+            d.pp, (const V4*)d.posq_s, (const V4*)d.dipt_s, d.tctr_s, d.text_s, d.pos_s, d.exs_off, d.exs_j, d.exs_m,
+            d.exs_s, d.exs_tiles, d.n_pad, d.partial);
+    } else {
+        cudaFuncSetAttribute(k_field_sym<R, 1>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+        k_field_sym<R, 1><<<band_pairs(d), kSymThreads, smem, st>>>(
+            d.pp, (const V4*)d.posq_s, (const V4*)d.vec_s, d.tctr_s, d.text_s, d.pos_s, d.exs_off, d.exs_j, d.exs_m,
+            d.exs_s, d.exs_tiles, d.n_pad, d.partial);
+    }
+}
+
+template <class R>
+void launch_energy(const Dev& d, cudaStream_t st) {
+    typedef typename Vec4T<R>::type V4;
+    const size_t smem = energy_smem<R>(d.pp.band_tiles);
+    cudaFuncSetAttribute(k_energy_sym<R>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+    k_energy_sym<R><<<band_pairs(d), kSymThreads, smem, st>>>(
+        d.pp, (const V4*)d.posq, (const V4*)d.dipt, (const V4*)d.ind, d.yz, d.tctr, d.text, d.pos, d.exc_off, d.exc_j,
+        d.exc_m, d.exc_s, d.exc_tiles, d.n_pad, d.partial, d.energy_partial);
+}
+
+template void launch_field<float>(const Dev&, int, cudaStream_t);
+template void launch_field<double>(const Dev&, int, cudaStream_t);
+template void launch_energy<float>(const Dev&, cudaStream_t);
+template void launch_energy<double>(const Dev&, cudaStream_t);
+
+}  // namespace tdp
