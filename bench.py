@@ -574,10 +574,10 @@ def run_ours(args):
         dominant = "energy" if en_ms >= mv_ms else "matvec"
         if dominant == "energy":
             flops, avg, bytes_ = pairs * FLOP_ENERGY_PAIR, en_avg, n * BYTES_ENERGY_ATOM
-            kname = "k_energy<float>"
+            kname = "k_energy_sym<float>"
         else:
             flops, avg, bytes_ = pairs * FLOP_MATVEC_PAIR, mv_avg, n * BYTES_MATVEC_ATOM
-            kname = "k_field<float,1>"
+            kname = "k_field_sym<float,1>"
         ach = flops / (avg * 1e-3) / 1e12
         hbm_peak = peaks.get("hbm_gbs", 6650.0)
         out["roofline"] = {"bound": "fp32", "kernel": kname, "achieved": ach, "peak": fp32, "unit": "TFLOP/s",

@@ -718,12 +718,15 @@ int tdp_create(const tdp_system_desc* desc, tdp_handle** out) {
                                   desc->covalent13_atoms);
         // Launch geometry of the pair kernels: 32-atom tiles in bands of
         // band_tiles tiles, one CTA per band pair.  Bands are as wide as
-        // possible (16 tiles, so the J records and sums of a band fit shared
-        // memory) while still giving about 16 CTAs per SM.
+        // possible -- 16 tiles (8 in FP64, whose records and sums are twice as
+        // large) so that four CTAs' J records and sums fit one SM's shared
+        // memory -- while still giving about 16 CTAs per SM.
         Dev& d = h->d;
         const int nt = std::max(1, (n + kTile - 1) / kTile);
+        const int widest = h->precision == TDP_PRECISION_DOUBLE ? 8 : 16;
         int band = 1;
         for (int cand : {16, 8, 4, 2}) {
+            if (cand > widest) continue;
             long nb = (nt + cand - 1) / cand;
             if (nb * (nb + 1) / 2 >= 16L * 148) {
                 band = cand;
@@ -732,7 +735,7 @@ int tdp_create(const tdp_system_desc* desc, tdp_handle** out) {
         }
         if (const char* e = getenv("TDP_BAND_TILES")) {
             int v = atoi(e);
-            if (v == 1 || v == 2 || v == 4 || v == 8 || v == 16) band = v;
+            if ((v == 1 || v == 2 || v == 4 || v == 8 || v == 16) && v <= widest) band = v;
         }
         const int pad = kTile * std::max(4, band);
         d.n = n;

@@ -72,12 +72,13 @@ __device__ __forceinline__ TileGeom tile_geom(const PairParams& P, double4 cA, d
         g.fold = fabs(g.dcx) + eA.x + eB.x >= P.half_box_tol[0] || fabs(g.dcy) + eA.y + eB.y >= P.half_box_tol[1] ||
                  fabs(g.dcz) + eA.z + eB.z >= P.half_box_tol[2];
     }
-    // Smallest distance any pair of the two tiles can have (per dimension the
-    // gap between the tiles' boxes; folded pairs are never closer).
+    // Smallest minimum-image distance any pair of the two tiles can have: per
+    // dimension the periodic distance is a metric, so it is at least the
+    // centres' folded distance minus both extents.
     double gx = fmax(fabs(g.dcx) - eA.x - eB.x, 0.0);
     double gy = fmax(fabs(g.dcy) - eA.y - eB.y, 0.0);
     double gz = fmax(fabs(g.dcz) - eA.z - eB.z, 0.0);
-    g.near = g.fold || gx * gx + gy * gy + gz * gz < (double)P.damp_r2;
+    g.near = gx * gx + gy * gy + gz * gz < (double)P.damp_r2;
     return g;
 }
 
@@ -355,14 +356,14 @@ __global__ void __launch_bounds__(kSymThreads, 4) k_field_sym(
     typedef typename Vec4T<R>::type V4;
     extern __shared__ __align__(16) unsigned char smem[];
     const int BT = P.band_tiles, NA = BT * 32;
-    double* s_acc = reinterpret_cast<double*>(smem);              // 3 * NA: J-side sums of band q
-    double* s_iacc = s_acc + 3 * NA;                               // 6 * kSymThreads: I-side sums, two slots
+    double* s_iacc = reinterpret_cast<double*>(smem);              // 6 * kSymThreads: I-side sums, two slots
     double4* s_ctr = reinterpret_cast<double4*>(s_iacc + 6 * kSymThreads);  // BT
     double4* s_ext = s_ctr + BT;                                   // BT
     double4* s_ic = s_ext + BT;                                    // 2 * kSymWarps: the warps' I tiles
     double4* s_ie = s_ic + 2 * kSymWarps;
     V4* s_pos = reinterpret_cast<V4*>(s_ie + 2 * kSymWarps);       // NA
     V4* s_vec = s_pos + NA;                                        // NA
+    R* s_acc = reinterpret_cast<R*>(s_vec + NA);                   // kSymWarps * 3 * NA: J-side sums per warp
 
     int p, q;
     band_pair(blockIdx.x, p, q);
@@ -371,17 +372,18 @@ __global__ void __launch_bounds__(kSymThreads, 4) k_field_sym(
     for (int k = threadIdx.x; k < NA; k += kSymThreads) {
         s_pos[k] = posq[qa0 + k];
         s_vec[k] = jvec[qa0 + k];
-        s_acc[3 * k] = 0.0;
-        s_acc[3 * k + 1] = 0.0;
-        s_acc[3 * k + 2] = 0.0;
     }
+    for (int k = threadIdx.x; k < kSymWarps * 3 * NA; k += kSymThreads) s_acc[k] = R(0);
     for (int k = threadIdx.x; k < BT; k += kSymThreads) {
         s_ctr[k] = tctr[q * BT + k];
         s_ext[k] = text[q * BT + k];
     }
     double* my = s_iacc + 6 * threadIdx.x;
+    R* wacc = s_acc + warp * 3 * NA;
     __syncthreads();
 
+    // Each warp sums its J-side contributions in its own area, so the warps
+    // never wait for one another until the final combination.
     const R damp_r2 = (R)P.damp_r2;
     const int stride = BT >= kSymWarps ? BT / kSymWarps : 1;
     // A warp's I tiles are warp, warp + 4, warp + 8, ...; a round takes two of them.
@@ -390,6 +392,7 @@ __global__ void __launch_bounds__(kSymThreads, 4) k_field_sym(
         ISlot<R> a, b;
         load_slot<R>(a, P, p, BT, warp + 2 * kSymWarps * r, lane, posq, jvec, exc_off, exc_tiles);
         load_slot<R>(b, P, p, BT, warp + 2 * kSymWarps * r + kSymWarps, lane, posq, jvec, exc_off, exc_tiles);
+        __syncwarp();
         if (lane < 2) {
             const ISlot<R>& s1 = lane == 0 ? a : b;
             s_ic[2 * warp + lane] = s1.act ? tctr[s1.I] : make_double4(0, 0, 0, 0);
@@ -403,91 +406,94 @@ __global__ void __launch_bounds__(kSymThreads, 4) k_field_sym(
             const double4 cB = s_ctr[Jl], eB = s_ext[Jl];
             slot_against<R>(a, P, p == q, J, Jl, s_ic[2 * warp], s_ie[2 * warp], cB, eB, exc_j);
             slot_against<R>(b, P, p == q, J, Jl, s_ic[2 * warp + 1], s_ie[2 * warp + 1], cB, eB, exc_j);
-            if (a.valid || b.valid) {
-                const int jbase = J * 32;
-                const V4* sp = s_pos + Jl * 32;
-                const V4* sv = s_vec + Jl * 32;
-                R fa[3] = {0, 0, 0}, fb[3] = {0, 0, 0}, g[3] = {0, 0, 0};
-                if (a.valid && b.valid) {
-                    const bool slow = a.slow || b.slow, fold = a.fold || b.fold;
-                    const bool near = a.near || b.near;
+            if (!(a.valid || b.valid)) continue;
+            const int jbase = J * 32;
+            const V4* sp = s_pos + Jl * 32;
+            const V4* sv = s_vec + Jl * 32;
+            R fa[3] = {0, 0, 0}, fb[3] = {0, 0, 0}, g[3] = {0, 0, 0};
+            if (a.valid && b.valid) {
+                const bool slow = a.slow || b.slow, fold = a.fold || b.fold;
+                const bool near = a.near || b.near;
 #define TDP_FWALK2(F, S, D)                                                                                        \
     field_walk2<R, KIND, F, S, D>(P, pos, sp, sv, lane, jbase, a.i, a.ox, a.oy, a.oz, a.pi.w, a.vi, a.diag,     \
                                   a.partners, b.i, b.ox, b.oy, b.oz, b.pi.w, b.vi, b.diag, b.partners, damp_r2, fa, \
                                   fb, g)
-                    if (slow) {
-                        if (fold) TDP_FWALK2(true, true, true);
-                        else TDP_FWALK2(false, true, true);
-                    } else if (fold) {
-                        TDP_FWALK2(true, false, true);
-                    } else if (near) {
-                        TDP_FWALK2(false, false, true);
-                    } else {
-                        TDP_FWALK2(false, false, false);
-                    }
-#undef TDP_FWALK2
+                if (slow) {
+                    if (fold) TDP_FWALK2(true, true, true);
+                    else TDP_FWALK2(false, true, true);
+                } else if (fold) {
+                    if (near) TDP_FWALK2(true, false, true);
+                    else TDP_FWALK2(true, false, false);
+                } else if (near) {
+                    TDP_FWALK2(false, false, true);
                 } else {
-                    const ISlot<R>& s1 = a.valid ? a : b;
-                    R* f1 = a.valid ? fa : fb;
+                    TDP_FWALK2(false, false, false);
+                }
+#undef TDP_FWALK2
+            } else {
+                const ISlot<R>& s1 = a.valid ? a : b;
+                R* f1 = a.valid ? fa : fb;
 #define TDP_FWALK(F, S, D)                                                                                        \
     field_walk<R, KIND, F, S, D>(P, pos, sp, sv, lane, s1.i, jbase, s1.ox, s1.oy, s1.oz, s1.pi.w, s1.vi, s1.diag, \
                                  s1.partners, damp_r2, f1[0], f1[1], f1[2], g[0], g[1], g[2])
-                    if (s1.slow) {
-                        if (s1.fold) TDP_FWALK(true, true, true);
-                        else TDP_FWALK(false, true, true);
-                    } else if (s1.fold) {
-                        TDP_FWALK(true, false, true);
-                    } else if (s1.near) {
-                        TDP_FWALK(false, false, true);
-                    } else {
-                        TDP_FWALK(false, false, false);
-                    }
+                if (s1.slow) {
+                    if (s1.fold) TDP_FWALK(true, true, true);
+                    else TDP_FWALK(false, true, true);
+                } else if (s1.fold) {
+                    if (s1.near) TDP_FWALK(true, false, true);
+                    else TDP_FWALK(true, false, false);
+                } else if (s1.near) {
+                    TDP_FWALK(false, false, true);
+                } else {
+                    TDP_FWALK(false, false, false);
+                }
 #undef TDP_FWALK
-                }
-                // Partner pairs of each SLOW slot, each side once.
-                for (int k = 0; k < 2; k++) {
-                    const ISlot<R>& s1 = k == 0 ? a : b;
-                    if (!s1.valid || !s1.slow) continue;
-                    R* f1 = k == 0 ? fa : fb;
-                    const double4 cA = s_ic[2 * warp + k];
-                    const TileGeom g1 = tile_geom(P, cA, s_ie[2 * warp + k], cB, eB);
-                    if (s1.fold)
-                        field_partners<R, KIND, true>(P, pos, posq, jvec, sp, sv, exc_off, exc_j, exc_m, exc_s, g1, cA,
-                                                      cB, lane, s1.i, s1.I * 32, jbase, s1.e0, s1.e1, s1.ox, s1.oy,
-                                                      s1.oz, s1.pi.w, s1.vi, s1.diag, damp_r2, f1[0], f1[1], f1[2],
-                                                      g[0], g[1], g[2]);
-                    else
-                        field_partners<R, KIND, false>(P, pos, posq, jvec, sp, sv, exc_off, exc_j, exc_m, exc_s, g1,
-                                                       cA, cB, lane, s1.i, s1.I * 32, jbase, s1.e0, s1.e1, s1.ox,
-                                                       s1.oy, s1.oz, s1.pi.w, s1.vi, s1.diag, damp_r2, f1[0], f1[1],
-                                                       f1[2], g[0], g[1], g[2]);
-                }
-                // This warp alone visits tile Jl in this round.
-                double* acc = s_acc + 3 * (Jl * 32 + lane);
-                for (int c = 0; c < 3; c++) {
-                    acc[c] += (double)g[c];
-                    my[c] += (double)fa[c];
-                    my[3 + c] += (double)fb[c];
-                }
             }
-            __syncthreads();
+            // Partner pairs of each SLOW slot, each side once.
+            for (int k = 0; k < 2; k++) {
+                const ISlot<R>& s1 = k == 0 ? a : b;
+                if (!s1.valid || !s1.slow) continue;
+                R* f1 = k == 0 ? fa : fb;
+                const double4 cA = s_ic[2 * warp + k];
+                const TileGeom g1 = tile_geom(P, cA, s_ie[2 * warp + k], cB, eB);
+                if (s1.fold)
+                    field_partners<R, KIND, true>(P, pos, posq, jvec, sp, sv, exc_off, exc_j, exc_m, exc_s, g1, cA,
+                                                  cB, lane, s1.i, s1.I * 32, jbase, s1.e0, s1.e1, s1.ox, s1.oy, s1.oz,
+                                                  s1.pi.w, s1.vi, s1.diag, damp_r2, f1[0], f1[1], f1[2], g[0], g[1],
+                                                  g[2]);
+                else
+                    field_partners<R, KIND, false>(P, pos, posq, jvec, sp, sv, exc_off, exc_j, exc_m, exc_s, g1, cA,
+                                                   cB, lane, s1.i, s1.I * 32, jbase, s1.e0, s1.e1, s1.ox, s1.oy,
+                                                   s1.oz, s1.pi.w, s1.vi, s1.diag, damp_r2, f1[0], f1[1], f1[2], g[0],
+                                                   g[1], g[2]);
+            }
+            R* acc = wacc + 3 * (Jl * 32 + lane);
+            for (int c = 0; c < 3; c++) {
+                acc[c] += g[c];
+                my[c] += (double)fa[c];
+                my[3 + c] += (double)fb[c];
+            }
         }
+        // I-side sums: slot q of band p; on the diagonal band, slot p, where
+        // the J-side sums of the same atoms are added below.
         for (int k = 0; k < 2; k++) {
             const ISlot<R>& s1 = k == 0 ? a : b;
             if (!s1.act) continue;
-            if (p == q) {
-                double* acc = s_acc + 3 * (s1.Il * 32 + lane);
-                for (int c = 0; c < 3; c++) acc[c] += my[3 * k + c];
-            } else {
-                const size_t base = (size_t)q * 3 * n_pad;
-                for (int c = 0; c < 3; c++) partial[base + (size_t)c * n_pad + s1.i] = my[3 * k + c];
-            }
+            const size_t base = (size_t)q * 3 * n_pad;
+            for (int c = 0; c < 3; c++) partial[base + (size_t)c * n_pad + s1.i] = my[3 * k + c];
         }
-        __syncthreads();
     }
+    __syncthreads();
     const size_t base = (size_t)p * 3 * n_pad;
-    for (int k = threadIdx.x; k < NA; k += kSymThreads)
-        for (int c = 0; c < 3; c++) partial[base + (size_t)c * n_pad + qa0 + k] = s_acc[3 * k + c];
+    for (int k = threadIdx.x; k < NA; k += kSymThreads) {
+        const int a = qa0 + k;
+        const bool own = p == q && (a >> 5) < P.n_tiles;
+        for (int c = 0; c < 3; c++) {
+            double v = own ? partial[base + (size_t)c * n_pad + a] : 0.0;
+            for (int w = 0; w < kSymWarps; w++) v += (double)s_acc[w * 3 * NA + 3 * k + c];
+            partial[base + (size_t)c * n_pad + a] = v;
+        }
+    }
 }
 
 // ---------------------------------------------------------------------------
@@ -763,8 +769,8 @@ __global__ void __launch_bounds__(kSymThreads, 3) k_energy_sym(
 template <class R>
 size_t field_smem(int BT) {
     const int NA = 32 * BT;
-    return sizeof(double) * (3 * NA + 6 * kSymThreads) + sizeof(double4) * (2 * BT + 4 * kSymWarps) +
-           sizeof(typename Vec4T<R>::type) * 2 * NA;
+    return sizeof(double) * 6 * kSymThreads + sizeof(double4) * (2 * BT + 4 * kSymWarps) +
+           sizeof(typename Vec4T<R>::type) * 2 * NA + sizeof(R) * kSymWarps * 3 * NA;
 }
 
 template <class R>
