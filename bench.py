@@ -154,7 +154,7 @@ def measured_peaks():
 
 def profile_traffic(kernel: str):
     """DRAM bytes per launch from the committed ncu summary (profiles/), or None."""
-    path = os.path.join(ROOT, "profiles", "traffic.txt")
+    path = os.path.join(ROOT, "profiles", "dram_traffic_water98304.txt")
     if not os.path.exists(path):
         return None
     for line in open(path):
@@ -239,7 +239,7 @@ def run_reference(args):
         base["unavailable"] = "compiled reference (oracle/_ref/libtdp_ref.so) not present"
         print(json.dumps(base))
         return
-    sweeps = _recorded_sweeps()
+    sweeps = _recorded_sweeps(args.config)
     ctx = mp.get_context("spawn")
     with ctx.Pool(cores) as pool:
         for _ in range(max(args.warmup, 1)):
@@ -269,14 +269,16 @@ def run_reference(args):
     print(json.dumps(base))
 
 
-def _recorded_sweeps() -> int:
-    path = os.path.join(ROOT, "profiles", "jacobi_sweeps.txt")  # "large <sweeps>" lines from our arm's runs
-    if os.path.exists(path):
-        for line in open(path):
-            f = line.split()
-            if len(f) >= 2 and f[0] == "large":
-                return int(f[1])
-    return 100
+# Jacobi sweeps the reference's loop (RTDF.cpp:820-851) takes to an RMS dipole
+# change below 1e-6 on each seeded box, as counted by the library's Jacobi
+# solver, which runs that loop sweep for sweep (the iteration count is tested
+# against the reference's): 216 waters 39, 4,096 waters 92, 32,768 waters 134
+# (the last re-measured by every default bench run, config.reference_jacobi_sweeps).
+REFERENCE_JACOBI_SWEEPS = {"small": 39, "medium": 92, "large": 134}
+
+
+def _recorded_sweeps(config: str = "large") -> int:
+    return REFERENCE_JACOBI_SWEEPS.get(config, 134)
 
 
 # ---------------------------------------------------------------------------

@@ -218,6 +218,16 @@ def induced_field(sys, mu: np.ndarray, backend: str = "port") -> np.ndarray:
     return out
 
 
+def map_torque(sys, torque: np.ndarray) -> np.ndarray:
+    """Forces from per-atom torques by the reference's mapTorqueToForce
+    (RTDF.cpp:915-1115), restated in the port."""
+    pk = _Packed(sys, polarization=0)
+    t = np.ascontiguousarray(torque, dtype=np.float64).reshape(sys.n, 3)
+    out = np.zeros((sys.n, 3))
+    _check(_lib("port").tdpo_map_torque(C.byref(pk.s), _p(t), _p(out)), "map_torque")
+    return out
+
+
 def potential(sys, grid: np.ndarray, backend: str = "port") -> np.ndarray:
     pk = _Packed(sys)
     g = np.ascontiguousarray(grid, dtype=np.float64).reshape(-1, 3)
