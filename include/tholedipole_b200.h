@@ -84,6 +84,24 @@ extern "C" {
 /* Keep the previous call's induced dipoles as the solver's starting point
  * (the reference restarts from mu0 = alpha*E every call). */
 #define TDP_FLAG_WARM_START (1u << 1)
+/* Ewald mode (with TDP_PME only).  The reference has no Ewald sum: its "PME"
+ * is the minimum image over all pairs (ReferenceTholeDipoleForce.cpp:1414-1423)
+ * and alpha/grid are only reported (ReferenceTholeDipoleKernels.cpp:143-152).
+ * With this flag the handle runs a true Ewald sum instead: real space within
+ * the cutoff over a neighbour list of 32-atom tiles, smooth particle-mesh Ewald
+ * of order 5 (the TholeDipoleForce default, TholeDipoleForce.cpp:43) on the
+ * grid tdp_get_pme_parameters reports, and the self and neutralising-plasma
+ * terms.  The fields and induced dipoles are the periodic versions of the
+ * reference's (same Thole damping, M and I scales); the energy is the
+ * variational one, U_perm - 1/2 mu.E_M, and the forces are its exact negative
+ * gradient.  Orthorhombic boxes only; real space, damping corrections
+ * included, stops at the cutoff, where exp(-a u^3) of every pair must be
+ * <= 1e-12 (cutoff^3 >= 27.63 t_max^5); tdp_adjoint is unsupported.
+ * alpha = pme_alpha and the grid = pme_grid when both are set, otherwise
+ * alpha = sqrt(-ln(2 tol))/cutoff and
+ * n_k = the smallest 2,3,5,7-smooth size >= ceil(2 alpha L_k / (3 tol^(1/5)))
+ * (at least 6), fixed at the first evaluation. */
+#define TDP_FLAG_EWALD (1u << 2)
 
 /* Flags of tdp_compute. */
 #define TDP_COMPUTE_FORCES (1u << 0)

@@ -129,3 +129,15 @@ def test_batch_rejects_links_across_clusters(lib):
 
     rc, msg = _batch_create([ammonia(), ammonia()], edit=z_into_first)
     assert rc == -1 and "another cluster" in msg
+
+
+def test_ewald_mode_validation(lib):
+    # TDP_FLAG_EWALD needs the PME method, and Thole damping below 1e-12 at the
+    # cutoff (exp(-rc^3 / t^5): rc >= 0.63 nm for t = 0.39).
+    s = S.config_small()
+    rc, _, _ = _create(s.copy(method=S.NO_CUTOFF), flags=A.FLAG_EWALD)
+    assert rc == -1 and "needs the PME nonbonded method" in lib.tdp_last_error(None).decode()
+    rc, _, _ = _create(s.copy(cutoff=0.6), flags=A.FLAG_EWALD)
+    assert rc == -1 and "Thole damping at the cutoff" in lib.tdp_last_error(None).decode()
+    rc, _, _ = _create(s, flags=A.FLAG_EWALD, ewald_error_tolerance=0.7)
+    assert rc == -1 and "tolerance" in lib.tdp_last_error(None).decode()

@@ -12,10 +12,10 @@ HERE = os.path.dirname(os.path.abspath(__file__))
 ROOT = os.path.dirname(HERE)
 CSRC = os.path.join(HERE, "csrc")
 LIB = os.path.join(HERE, "libtholedipole_b200.so")
-SOURCES = ["tdp_kernels.cu", "tdp_sym.cu", "tdp_capi.cu", "tdp_md.cu", "tdp_noalloc.cu", "tdp_adjoint.cu",
-           "tdp_batch.cu"]
+SOURCES = ["tdp_kernels.cu", "tdp_sym.cu", "tdp_ewald.cu", "tdp_capi.cu", "tdp_md.cu", "tdp_noalloc.cu",
+           "tdp_adjoint.cu", "tdp_batch.cu"]
 # Sources whose FP32 pair arithmetic is compiled with subnormal flushing.
-FTZ = {"tdp_kernels.cu", "tdp_sym.cu", "tdp_batch.cu"}
+FTZ = {"tdp_kernels.cu", "tdp_sym.cu", "tdp_ewald.cu", "tdp_batch.cu"}
 ARCH = ["-gencode", "arch=compute_100a,code=sm_100a"]
 
 
@@ -66,7 +66,7 @@ def build(force: bool = False, verbose: bool = False) -> str:
         subprocess.run(cmd, check=True)
         objs.append(obj)
     tmp = LIB + ".tmp"
-    subprocess.run([nvcc(), *ARCH, "-shared", "-o", tmp, *objs, "-lcudart"], check=True)
+    subprocess.run([nvcc(), *ARCH, "-shared", "-o", tmp, *objs, "-lcudart", "-lcufft"], check=True)
     os.replace(tmp, LIB)
     build_adapter(verbose)
     return LIB

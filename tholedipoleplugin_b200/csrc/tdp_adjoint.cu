@@ -297,7 +297,6 @@ __device__ void visit_pair(const PairParams& P, const AtomData& A, const double*
         acc[a] += l;
     }
     // Thole-factor derivative: dual number seeded on my t.
-    double mq = A.q[me];
     Dual dq[2], dm[2][3], du[2][3];
     for (int s = 0; s < 2; s++) {
         int at = s == 0 ? I : K;
@@ -307,7 +306,6 @@ __device__ void visit_pair(const PairParams& P, const AtomData& A, const double*
             du[s][c] = mk(A.mu[3 * at + c]);
         }
     }
-    (void)mq;
     Dual dtI = mk(tI, meI ? 1.0 : 0.0), dtK = mk(tK, meI ? 0.0 : 1.0);
     Dual l = pair_loss<Dual>(d.x, d.y, d.z, yzd, dq[0], dm[0], du[0], dtI, dq[1], dm[1], du[1], dtK, mS, iS, damp_r2,
                              rv4p, rv4f, P.mutual, gE, gFI, gFK, gTI, gTK);

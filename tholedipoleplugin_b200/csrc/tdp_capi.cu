@@ -6,6 +6,7 @@
 // driven as ReferenceCalcTholeDipoleForceKernel does in
 // platforms/reference/src/ReferenceTholeDipoleKernels.cpp).
 #include "tholedipole_b200.h"
+#include "tdp_ewald.cuh"
 #include "tdp_host.h"
 #include "tdp_kernels.cuh"
 
@@ -87,6 +88,10 @@ struct tdp_handle {
     double stage_ms[TDP_NUM_STAGE_TIMES] = {};
     long launches = 0;
 
+    // Ewald mode (TDP_FLAG_EWALD): neighbour list, PME grid and plans.
+    Ewald* ew = nullptr;
+    double total_charge = 0.0;
+
     // Adjoint work buffers (allocated on first use).
     double* adj = nullptr;
     double adj_eps = 0.0;
@@ -114,6 +119,11 @@ void upload_params(tdp_handle* h) {
     std::vector<double> sal(n);
     for (int i = 0; i < n; i++) sal[i] = h->alpha[i] > 0.0 ? std::sqrt(h->alpha[i]) : 0.0;
     upload(d.charge, h->charge.data(), sizeof(double) * n);
+    // Net charge for the neutralising-plasma term, from the charges as the pair
+    // records hold them (FP32 in the mixed form), which reciprocal space sums.
+    h->total_charge = 0.0;
+    for (int i = 0; i < n; i++)
+        h->total_charge += h->precision == TDP_PRECISION_DOUBLE ? h->charge[i] : (double)(float)h->charge[i];
     upload(d.dip_mol, h->dip.data(), sizeof(double) * 3 * n);
     upload(d.alpha, h->alpha.data(), sizeof(double) * n);
     upload(d.salpha, sal.data(), sizeof(double) * n);
@@ -312,6 +322,9 @@ void check_box(tdp_handle* h) {
     double minAllowed = 1.999999 * h->cutoff;
     if (!h->have_box || h->box[0] < minAllowed || h->box[4] < minAllowed || h->box[8] < minAllowed)
         throw TdpError{TDP_ERR_BOX_TOO_SMALL, "The periodic box size has decreased to less than twice the nonbonded cutoff."};
+    if (h->ew && (h->box[1] != 0.0 || h->box[2] != 0.0 || h->box[3] != 0.0 || h->box[5] != 0.0 || h->box[6] != 0.0 ||
+                  h->box[7] != 0.0))
+        throw TdpError{TDP_ERR_UNSUPPORTED, "the Ewald mode supports orthorhombic boxes only"};
 }
 
 double read_scalar(tdp_handle* h, const double* dptr) {
@@ -348,10 +361,15 @@ void kernel_end(tdp_handle* h, size_t k) {
 template <class R>
 void matvec(tdp_handle* h) {
     size_t k = kernel_begin(h, 0);
-    launch_field<R>(h->d, 1, h->stream);
+    if (h->ew) {
+        ewald_matvec<R>(h->ew, h->d, h->stream);
+        h->launches += ewald_last_launches(h->ew);
+    } else {
+        launch_field<R>(h->d, 1, h->stream);
+        h->launches++;
+    }
     kernel_end(h, k);
     h->matvecs++;
-    h->launches++;
 }
 
 // Mutual polarization by conjugate gradients in y = mu / sqrt(alpha):
@@ -467,9 +485,16 @@ void setup_and_solve(tdp_handle* h) {
     launch_pack<R>(d, st);
     launch_rotate<R>(d, st);
     record(h, 1);
-    launch_field<R>(d, 0, st);
+    if (h->ew) {
+        const double L[3] = {h->box[0], h->box[4], h->box[8]};
+        ewald_prepare(h->ew, d, L, h->cutoff, h->ewald_tol, h->pme_alpha, h->pme_grid, st);
+        ewald_fixed_field<R>(h->ew, d, st);
+        h->launches += 3 + ewald_last_launches(h->ew);
+    } else {
+        launch_field<R>(d, 0, st);
+        h->launches += 4;
+    }
     launch_fixed_done<R>(d, st);
-    h->launches += 4;
     record(h, 2);
     if (h->polarization == TDP_DIRECT) {
         h->iterations = 0;
@@ -500,6 +525,17 @@ template <class R>
 void run_energy(tdp_handle* h) {
     Dev& d = h->d;
     cudaStream_t st = h->stream;
+    if (h->ew) {
+        size_t k = kernel_begin(h, 1);
+        ewald_energy<R>(h->ew, d, h->total_charge, st);
+        kernel_end(h, k);
+        h->launches += ewald_last_launches(h->ew);
+        record(h, 4);
+        launch_torque_gather(d, st);
+        record(h, 5);
+        h->launches += 1;
+        return;
+    }
     launch_pack_ind<R>(d, st);
     size_t k = kernel_begin(h, 1);
     launch_energy<R>(d, st);
@@ -647,6 +683,7 @@ int tdp_adjoint(tdp_handle* h, const double* dL_dF, double dL_dE, double* grads)
         if (!h->have_results) throw TdpError{TDP_ERR_INVALID_ARGUMENT, "tdp_adjoint needs a previous tdp_compute"};
         if (h->polarization == TDP_EXTRAPOLATED)
             throw TdpError{TDP_ERR_UNSUPPORTED, "tdp_adjoint supports Direct and Mutual polarization"};
+        if (h->ew) throw TdpError{TDP_ERR_UNSUPPORTED, "tdp_adjoint does not support the Ewald mode"};
         if (h->precision == TDP_PRECISION_DOUBLE) run_adjoint<double>(h, dL_dF, dL_dE, grads);
         else run_adjoint<float>(h, dL_dF, dL_dE, grads);
     } catch (const TdpError& e) {
@@ -745,6 +782,30 @@ int tdp_create(const tdp_system_desc* desc, tdp_handle** out) {
         d.pp.n_bands = (nt + band - 1) / band;
         d.nsplit = d.pp.n_bands;
         d.n_eblk = d.pp.n_bands * (d.pp.n_bands + 1) / 2;
+        const bool ewald = (h->flags & TDP_FLAG_EWALD) != 0;
+        if (ewald) {
+            if (h->method != TDP_PME)
+                throw TdpError{TDP_ERR_INVALID_ARGUMENT, "TDP_FLAG_EWALD needs the PME nonbonded method"};
+            if (!(h->cutoff > 0.0)) throw TdpError{TDP_ERR_INVALID_ARGUMENT, "the Ewald mode needs a cutoff > 0"};
+            if (!(h->ewald_tol > 0.0 && h->ewald_tol < 0.5) && !(h->pme_alpha > 0.0))
+                throw TdpError{TDP_ERR_INVALID_ARGUMENT, "the Ewald error tolerance must lie in (0, 0.5)"};
+            // Real space stops at the cutoff, damping corrections included: the
+            // least-damped pair at the cutoff (a u^3 = rc^3 / t_max^5) must have
+            // exp(-a u^3) <= 1e-12.
+            double tmax = 0.0;
+            bool bad = false;
+            for (double t : h->thole) {
+                if (!(t >= 0.0)) bad = true;
+                tmax = std::max(tmax, t);
+            }
+            if (bad || (tmax > 0.0 && h->cutoff * h->cutoff * h->cutoff < 27.631021115928547 * std::pow(tmax, 5.0)))
+                throw TdpError{TDP_ERR_INVALID_ARGUMENT,
+                               "Ewald mode: the Thole damping at the cutoff exceeds 1e-12 (cutoff too short for the "
+                               "largest Thole factor)"};
+            // Real space in partial slot 0, reciprocal space + self in slot 1.
+            d.nsplit = 2;
+            d.n_eblk = 1;
+        }
 
         std::vector<int> eoff(n + 1, 0), ej;
         std::vector<double> em, es;
@@ -839,6 +900,7 @@ int tdp_create(const tdp_system_desc* desc, tdp_handle** out) {
         d.exs_tiles = dalloc<int2>(d.n_pad / kTile, o);
         upload(d.coef, h->extrap.data(), sizeof(double) * h->extrap.size());
         upload_params(h);
+        if (ewald) h->ew = ewald_create(d, h->precision);
         TDP_CUDA(cudaMallocHost(&h->h_scal, 64 * sizeof(double)));
         TDP_CUDA(cudaMallocHost(&h->h_forces, std::max<size_t>(n3, 1) * sizeof(double)));
         for (int k = 0; k < 6; k++) TDP_CUDA(cudaEventCreate(&h->ev[k]));
@@ -860,6 +922,7 @@ int tdp_create(const tdp_system_desc* desc, tdp_handle** out) {
 
 void tdp_destroy(tdp_handle* h) {
     if (!h) return;
+    if (h->ew) ewald_destroy(h->ew);
     for (void* p : h->owned) cudaFree(p);
     if (h->h_scal) cudaFreeHost(h->h_scal);
     if (h->h_forces) cudaFreeHost(h->h_forces);
@@ -954,6 +1017,8 @@ int tdp_compute(tdp_handle* h, const void* positions, int32_t pos_dtype, int32_t
                 for (size_t k = 0; k < n3; k++) acc[k] += (float)h->h_forces[k];
             }
         }
+        if (h->ew && ewald_list_overflow(h->ew))
+            throw TdpError{TDP_ERR_CUDA, "Ewald mode: a neighbour-tile list row overflowed its capacity"};
         if (energy) *energy = h->h_scal[1];
         finish_timing(h);
         if (h->status == TDP_STATUS_NON_FINITE)
@@ -979,6 +1044,8 @@ int tdp_get_dipoles(tdp_handle* h, int32_t which, const void* positions, int32_t
         if (which == TDP_DIPOLES_INDUCED) {
             TDP_CUDA(cudaMemcpyAsync(out, h->d.mu, n3 * 8, cudaMemcpyDeviceToHost, st));
             TDP_CUDA(cudaStreamSynchronize(st));
+            if (h->ew && ewald_list_overflow(h->ew))
+                throw TdpError{TDP_ERR_CUDA, "Ewald mode: a neighbour-tile list row overflowed its capacity"};
         } else if (which == TDP_DIPOLES_LAB_PERMANENT) {
             TDP_CUDA(cudaMemcpyAsync(out, h->d.lab, n3 * 8, cudaMemcpyDeviceToHost, st));
             TDP_CUDA(cudaStreamSynchronize(st));
@@ -1056,6 +1123,25 @@ int tdp_get_pme_parameters(const tdp_handle* h, double* alpha, int32_t* nx, int3
     if (h->method != TDP_PME) {
         const_cast<tdp_handle*>(h)->err = "getPMEParametersInContext: This Context is not using PME";
         return TDP_ERR_NOT_PME;
+    }
+    if (h->ew) {
+        // The Ewald mode reports what it runs with: the alpha and grid planned
+        // at its first evaluation (before it, the same rule on the current box).
+        double a = 0.0;
+        int g[3] = {0, 0, 0};
+        ewald_params(h->ew, &a, g);
+        if (g[0] == 0) {
+            a = h->pme_alpha > 0.0 ? h->pme_alpha : std::sqrt(-std::log(2.0 * h->ewald_tol)) / h->cutoff;
+            for (int k = 0; k < 3; k++)
+                g[k] = h->pme_grid[0] > 0 ? h->pme_grid[k]
+                                          : pme_smooth_size(std::max(6, (int)std::ceil(2.0 * a * h->box[4 * k] /
+                                                                                       (3.0 * std::pow(h->ewald_tol, 0.2)))));
+        }
+        *alpha = a;
+        *nx = g[0];
+        *ny = g[1];
+        *nz = g[2];
+        return TDP_OK;
     }
     if (h->pme_alpha != 0.0 && h->pme_grid[0] != 0) {
         *alpha = h->pme_alpha;

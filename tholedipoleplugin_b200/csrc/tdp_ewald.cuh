@@ -1,0 +1,45 @@
+// tdp_ewald.cuh -- the Ewald mode of the box path (TDP_FLAG_EWALD): real space
+// over a neighbour list of 32-atom tiles within the cutoff, smooth particle-mesh
+// Ewald (order 5, cuFFT) for reciprocal space, self and neutralising-plasma
+// terms.  The reference plugin has no Ewald sum (its "PME" is the minimum
+// image over all pairs); this mode is the library's own, defined and checked
+// against the FP64 restatement in oracle/ewald.py.
+#pragma once
+
+#include "tdp_kernels.cuh"
+
+namespace tdp {
+
+struct Ewald;
+
+// State that does not depend on the box (neighbour list, buffers of the
+// atom-side kernels); the grid is planned by ewald_prepare.
+Ewald* ewald_create(const Dev& d, int precision);
+void ewald_destroy(Ewald* e);
+
+// Chooses alpha and the grid on the first call (alpha_in > 0 and grid_in[0] > 0
+// pin them; otherwise alpha = sqrt(-ln(2 tol))/cutoff and n_k = the
+// 2,3,5,7-smooth size at or above ceil(2 alpha L_k / (3 tol^(1/5))), at least
+// 6) and keeps the grid afterwards, as a context keeps its PME grid; the
+// influence function follows every box change.
+void ewald_prepare(Ewald* e, const Dev& d, const double box[3], double cutoff, double tol, double alpha_in,
+                   const int grid_in[3], cudaStream_t st);
+void ewald_params(const Ewald* e, double* alpha, int grid[3]);
+
+// Permanent field E_M of the sorted records into partial slots 0 (real
+// space) and 1 (reciprocal + self); builds the neighbour list first.
+template <class R> void ewald_fixed_field(Ewald* e, const Dev& d, cudaStream_t st);
+// Periodic field T v of the operand in vec_s into partial slots 0 and 1.
+template <class R> void ewald_matvec(Ewald* e, const Dev& d, cudaStream_t st);
+// Energy, forces (fpair) and torques (torque) at the converged dipoles d.mu;
+// plasma = -pi Q^2 / (2 V alpha^2) is added to the energy.
+template <class R> void ewald_energy(Ewald* e, const Dev& d, double total_charge, cudaStream_t st);
+// Nonzero when the last neighbour-list build overflowed a row (valid after the
+// stream has been synchronised).
+int ewald_list_overflow(const Ewald* e);
+// Kernel launches of the last call of each stage (for the launch count).
+int ewald_last_launches(const Ewald* e);
+// Smallest size >= n whose prime factors are 2, 3, 5 and 7 only.
+int pme_smooth_size(int n);
+
+}  // namespace tdp
