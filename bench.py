@@ -72,6 +72,8 @@ def parse():
     p.add_argument("--config", default="large", choices=["small", "medium", "profile", "large"],
                    help="small 648, medium 12,288, profile 41,472 (24^3 waters, kernel profiling), large 98,304 atoms")
     p.add_argument("--no-extras", action="store_true", help="only the timed MD (used under ncu)")
+    p.add_argument("--ewald-md", action="store_true",
+                   help="profiling: the timed MD runs in the Ewald mode (with --no-extras)")
     return p.parse_args()
 
 
@@ -389,6 +391,107 @@ def rel_rms(a, b):
     return float(np.sqrt(np.mean((a - b) ** 2) / np.mean(b ** 2)))
 
 
+def ewald_section(system, K, W, stream, world, barrier, max_over_ranks, rank):
+    """The box in the library's Ewald mode (no reference counterpart: the
+    reference's PME is the all-pairs minimum image): MD ns/day and SCF solves/s
+    for the mixed and plain forms, errors mixed vs plain on this box and both
+    vs the FP64 Ewald oracle (smooth-PME restatement) on 216 waters."""
+    import numpy as np
+    import torch
+    from tholedipoleplugin_b200 import _capi as A
+    from tholedipoleplugin_b200 import systems as S
+    from tholedipoleplugin_b200.kernel import CudaCalcTholeDipoleForceKernel
+    from tholedipoleplugin_b200.md import DeviceRigidWaterMD
+    n = system.n
+    res = {"workload": f"{n}-atom water box, Ewald mode: real space within {system.cutoff} nm over a 32-atom tile "
+                       f"neighbour list + order-5 smooth PME (tolerance {system.ewald_tolerance}), mutual "
+                       "polarization to 1e-6, velocity Verlet 1 fs"}
+
+    def md_rate(precision, steps, warm):
+        md = DeviceRigidWaterMD(system, precision=precision, warm_start=True, seed=11 + rank, ewald=True)
+        md.kernel.enableTiming(True)
+        md.step(warm)
+        torch.cuda.synchronize()
+        barrier()
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        mv_ms, mv_n, en_ms, tot_ms, its, launches = 0.0, 0, 0.0, 0.0, [], 0
+        e0.record(stream)
+        for _ in range(steps):
+            md.step()
+            st = md.kernel.stageTimes()
+            mv_ms += st[7]
+            mv_n += int(st[6])
+            en_ms += st[8]
+            tot_ms += st[5]
+            launches += int(st[9]) + 2
+            its.append(md.kernel.solverStats()["iterations"])
+        e1.record(stream)
+        torch.cuda.synchronize()
+        t = max_over_ranks(e0.elapsed_time(e1))
+        params = md.kernel.getPMEParameters()
+        md.close()
+        return {"ns_per_day": world * steps / (t * 1e-3) * NS_PER_DAY, "ms_per_step": t / steps, "steps": steps,
+                "cg_iterations_mean": statistics.mean(its), "matvec_ms_per_launch": mv_ms / max(mv_n, 1),
+                "matvec_share": mv_ms / t, "energy_force_ms": en_ms / steps, "energy_force_share": en_ms / t,
+                "launches_per_step": launches / steps}, params
+
+    mixed, params = md_rate("mixed", K, max(W, 3))
+    plain, _ = md_rate("double", max(3, K // 2), 3)
+    res["pme"] = {"alpha_per_nm": params[0], "grid": list(params[1:]), "order": 5}
+    res["mixed"] = mixed
+    res["plain"] = plain
+    res["md_ns_per_day_mixed_over_plain"] = mixed["ns_per_day"] / plain["ns_per_day"]
+
+    def solves_per_s(precision, reps):
+        with CudaCalcTholeDipoleForceKernel(system, precision=precision, ewald=True) as k:
+            k.setStream(stream.cuda_stream)
+            dev_pos = torch.tensor(system.positions, dtype=torch.float64, device="cuda")
+            buf = np.zeros((n, 3))
+            for _ in range(2):
+                k.solveDevice(dev_pos.data_ptr(), A.F64, buf)
+            torch.cuda.synchronize()
+            s0, s1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+            s0.record(stream)
+            for _ in range(reps):
+                k.solveDevice(dev_pos.data_ptr(), A.F64, buf)
+            s1.record(stream)
+            torch.cuda.synchronize()
+            return world * reps / (max_over_ranks(s0.elapsed_time(s1)) * 1e-3), k.solverStats()["iterations"]
+
+    reps = max(5, K)
+    sm, im = solves_per_s("mixed", reps)
+    sp, ip = solves_per_s("double", reps)
+    res["scf_solves_per_s"] = {"mixed": sm, "plain": sp, "mixed_over_plain": sm / sp,
+                               "cg_iterations": {"mixed": im, "plain": ip},
+                               "what": "rotation + permanent field + CG to 1e-6 from mu0 = alpha E (Ewald)"}
+    if rank == 0:
+        def rel_rms(a, b):
+            return float(np.sqrt(np.mean((a - b) ** 2) / np.mean(b ** 2)))
+
+        errs = {}
+        with CudaCalcTholeDipoleForceKernel(system.copy(target_eps=1e-9), precision="mixed", ewald=True) as km:
+            em, fm = km.execute(system.positions)
+            mum = km.getInducedDipoles()
+        with CudaCalcTholeDipoleForceKernel(system.copy(target_eps=1e-11), precision="double", ewald=True) as kp:
+            ep, fp = kp.execute(system.positions)
+            mup = kp.getInducedDipoles()
+        errs["mixed_vs_plain_this_box"] = {"energy_rel": abs(em - ep) / abs(ep), "force_rms_rel": rel_rms(fm, fp),
+                                           "induced_rms_rel": rel_rms(mum, mup)}
+        from oracle import ewald as EW
+        small = S.config_small(target_eps=1e-12, max_iter=500)
+        alpha, grid = EW.pme_parameters(small.cutoff, small.ewald_tolerance, small.box)
+        ref = EW.Ewald(small, alpha, recip="pme", grid=grid).evaluate()
+        for prec, eps in (("mixed", 1e-9), ("double", 1e-11)):
+            with CudaCalcTholeDipoleForceKernel(small.copy(target_eps=eps), precision=prec, ewald=True) as k:
+                e, f = k.execute(small.positions)
+                mu = k.getInducedDipoles()
+            errs[f"{prec}_vs_fp64_ewald_oracle_216_waters"] = {
+                "energy_rel": abs(e - ref.energy) / abs(ref.energy), "force_rms_rel": rel_rms(f, ref.forces),
+                "induced_rms_rel": rel_rms(mu, ref.induced)}
+        res["errors"] = errs
+    return res
+
+
 def run_ours(args):
     import numpy as np
     import torch
@@ -427,7 +530,7 @@ def run_ours(args):
     stream = torch.cuda.current_stream()
 
     # ---- mixed form, device-resident MD (the headline) --------------------------------
-    md = DeviceRigidWaterMD(system, precision="mixed", warm_start=True, seed=11 + rank)
+    md = DeviceRigidWaterMD(system, precision="mixed", warm_start=True, seed=11 + rank, ewald=args.ewald_md)
     md.kernel.enableTiming(True)
     md.step(W)
     torch.cuda.synchronize()
@@ -460,7 +563,8 @@ def run_ours(args):
            "ms_per_step": t_ms / K, "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
            "dtype": "f32", "data": "synthetic",
            "config": {"workload": f"{n}-atom rigid water box ({n // 3} waters, {system.box[0]} nm cubic, "
-                                  "minimum-image all-pairs, mutual polarization to 1e-6), velocity Verlet 1 fs, "
+                                  + ("Ewald mode: cutoff + smooth PME" if args.ewald_md else "minimum-image all-pairs")
+                                  + ", mutual polarization to 1e-6), velocity Verlet 1 fs, "
                                   "mixed form (FP32 pair arithmetic, FP64 accumulation/CG)",
                       "n_atoms": n, "parallelism": f"replicas x{world}",
                       "l2": "inputs+working set per pass ~ 10 MB (L2-resident); every step re-reads all of it",
@@ -531,6 +635,9 @@ def run_ours(args):
                                "cg_iterations": {"mixed": it_mixed, "plain": it_plain},
                                "what": "rotation + permanent field + CG to 1e-6 from mu0 = alpha E"}
     out["md_ns_per_day_mixed_over_plain"] = value / out["plain"]["ns_per_day"]
+
+    # ---- Ewald mode (TDP_FLAG_EWALD): the same box with real-space cutoff + smooth PME ---------
+    out["ewald"] = ewald_section(system, K, W, stream, world, barrier, max_over_ranks, rank)
 
     # ---- cluster batches (1024 NoCutoff clusters of 4-64 waters, one launch) -------------
     out["clusters"] = run_clusters(args, rank, world, barrier, max_over_ranks, stream)

@@ -310,9 +310,11 @@ __global__ void __launch_bounds__(kEwThreads) k_ew_field(PairParams P, EwParams 
                                                          double* __restrict__ out) {
     typedef typename Vec4T<R>::type V4;
     __shared__ V4 s_pos[kEwWarps][32], s_vec[kEwWarps][32];
+    __shared__ double s_red[kEwWarps][3][32];
     const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
-    const int I = blockIdx.x * kEwWarps + warp;
-    if (I >= P.n_tiles) return;
+    // One I tile per CTA; warp w takes list entries w, w + 4, ...; the four
+    // partial sums are added in warp order.
+    const int I = blockIdx.x;
     const int i = I * 32 + lane;
     const V4 pi = posq_s[i], vi = src[i];
     const double4 cA = tctr[I];
@@ -320,7 +322,7 @@ __global__ void __launch_bounds__(kEwThreads) k_ew_field(PairParams P, EwParams 
     const R rc2 = (R)E.rc2, damp_r2 = (R)P.damp_r2;
     double fx = 0.0, fy = 0.0, fz = 0.0;
     const int cnt = count[I];
-    for (int t = 0; t < cnt; t++) {
+    for (int t = warp; t < cnt; t += kEwWarps) {
         const int ent = list[(size_t)I * E.cap + t];
         const int J = ent & kTileMask;
         const bool fold = (ent >> 30) & 1, slow = ((unsigned)ent >> 31) & 1u;
@@ -343,6 +345,16 @@ __global__ void __launch_bounds__(kEwThreads) k_ew_field(PairParams P, EwParams 
         fx += (double)tx;
         fy += (double)ty;
         fz += (double)tz;
+    }
+    s_red[warp][0][lane] = fx;
+    s_red[warp][1][lane] = fy;
+    s_red[warp][2][lane] = fz;
+    __syncthreads();
+    if (warp != 0) return;
+    for (int w = 1; w < kEwWarps; w++) {
+        fx += s_red[w][0][lane];
+        fy += s_red[w][1][lane];
+        fz += s_red[w][2][lane];
     }
     if (i < P.n) ew_field_exceptions<R, KIND>(P, E, pos_s, posq_s, src, exs_off, exs_j, exs_m, exs_s, i, (double)vi.w, fx, fy, fz);
     else fx = fy = fz = 0.0;
@@ -467,9 +479,10 @@ __global__ void __launch_bounds__(kEwThreads) k_ew_force(PairParams P, EwParams 
                                                          double* __restrict__ out, double* __restrict__ tile_energy) {
     typedef typename Vec4T<R>::type V4;
     __shared__ V4 s_pos[kEwWarps][32], s_dip[kEwWarps][32], s_ind[kEwWarps][32];
+    __shared__ double s_red[kEwWarps][7][32];
     const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
-    const int I = blockIdx.x * kEwWarps + warp;
-    if (I >= P.n_tiles) return;
+    // One I tile per CTA; warps split the neighbour list (see k_ew_field).
+    const int I = blockIdx.x;
     const int i = I * 32 + lane;
     const V4 pi = posq_s[i], di = dipt_s[i], ui = vec_s[i];
     const double4 cA = tctr[I];
@@ -477,7 +490,7 @@ __global__ void __launch_bounds__(kEwThreads) k_ew_force(PairParams P, EwParams 
     const R rc2 = (R)E.rc2, damp_r2 = (R)P.damp_r2;
     double F[3] = {0, 0, 0}, G[3] = {0, 0, 0}, en = 0.0;
     const int cnt = count[I];
-    for (int t = 0; t < cnt; t++) {
+    for (int t = warp; t < cnt; t += kEwWarps) {
         const int ent = list[(size_t)I * E.cap + t];
         const int J = ent & kTileMask;
         const bool fold = (ent >> 30) & 1, slow = ((unsigned)ent >> 31) & 1u;
@@ -503,6 +516,20 @@ __global__ void __launch_bounds__(kEwThreads) k_ew_force(PairParams P, EwParams 
             G[c] += (double)g[c];
         }
         en += (double)e;
+    }
+    for (int c = 0; c < 3; c++) {
+        s_red[warp][c][lane] = F[c];
+        s_red[warp][3 + c][lane] = G[c];
+    }
+    s_red[warp][6][lane] = en;
+    __syncthreads();
+    if (warp != 0) return;
+    for (int w = 1; w < kEwWarps; w++) {
+        for (int c = 0; c < 3; c++) {
+            F[c] += s_red[w][c][lane];
+            G[c] += s_red[w][3 + c][lane];
+        }
+        en += s_red[w][6][lane];
     }
     if (i < P.n) {
         ew_force_exceptions<R>(P, E, pos_s, posq_s, dipt_s, vec_s, exs_off, exs_j, exs_m, exs_s, i, en, F, G);
@@ -1101,7 +1128,7 @@ void pme_potential(Ewald* e, const Dev& d, FftGrid& g, bool energy, cudaStream_t
 template <class R, int KIND>
 void real_field(Ewald* e, const Dev& d, const void* src, cudaStream_t st) {
     typedef typename Vec4T<R>::type V4;
-    const int blocks = (d.pp.n_tiles + kEwWarps - 1) / kEwWarps;
+    const int blocks = d.pp.n_tiles;
     k_ew_field<R, KIND><<<blocks, kEwThreads, 0, st>>>(d.pp, e->E, (const V4*)d.posq_s, (const V4*)src, d.tctr_s,
                                                       d.pos_s, d.exs_off, d.exs_j, d.exs_m, d.exs_s, e->list, e->count,
                                                       d.n_pad, d.partial);
@@ -1147,7 +1174,7 @@ void ewald_energy(Ewald* e, const Dev& d, double total_charge, cudaStream_t st) 
     typedef typename Vec4T<R>::type V4;
     e->launches = 0;
     k_ew_pack_mu<R><<<nblk((size_t)d.n, kVecThreads), kVecThreads, 0, st>>>(d.n, d.rank, d.mu, d.thole, (V4*)d.vec_s);
-    const int blocks = (d.pp.n_tiles + kEwWarps - 1) / kEwWarps;
+    const int blocks = d.pp.n_tiles;
     k_ew_force<R><<<blocks, kEwThreads, 0, st>>>(d.pp, e->E, (const V4*)d.posq_s, (const V4*)d.dipt_s,
                                                  (const V4*)d.vec_s, d.tctr_s, d.pos_s, d.exs_off, d.exs_j, d.exs_m,
                                                  d.exs_s, e->list, e->count, d.n_pad, d.partial, e->tile_energy);

@@ -235,6 +235,181 @@ __device__ __forceinline__ void field_walk2(const PairParams& P, const double* _
     }
 }
 
+// ---------------------------------------------------------------------------
+// Packed FP32 walk (sm_100 f32x2 arithmetic) of field_walk2 for the mixed
+// form: the pairs of the two I slots ride in the low and high halves of
+// 64-bit registers, so every add/mul/fma instruction serves both pairs.  Same
+// operations in the same order as pair_delta + pair_matvec2 / pair_fixed2 per
+// half (FP32, subnormals flushed as the scalar path is compiled); only SLOW
+// tile pairs (masked pairs, partners) keep the scalar walk.
+// ---------------------------------------------------------------------------
+__device__ __forceinline__ float4 to_f4(float4 v) { return v; }
+__device__ __forceinline__ float4 to_f4(double4 v) { return make_float4((float)v.x, (float)v.y, (float)v.z, (float)v.w); }
+
+typedef unsigned long long f2;
+__device__ __forceinline__ f2 pk2(float lo, float hi) {
+    f2 r;
+    asm("mov.b64 %0, {%1, %2};" : "=l"(r) : "f"(lo), "f"(hi));
+    return r;
+}
+__device__ __forceinline__ f2 bc2(float v) { return pk2(v, v); }
+__device__ __forceinline__ void un2(f2 v, float& lo, float& hi) {
+    asm("mov.b64 {%0, %1}, %2;" : "=f"(lo), "=f"(hi) : "l"(v));
+}
+__device__ __forceinline__ f2 add2(f2 a, f2 b) {
+    f2 d;
+    asm("add.rn.ftz.f32x2 %0, %1, %2;" : "=l"(d) : "l"(a), "l"(b));
+    return d;
+}
+__device__ __forceinline__ f2 sub2(f2 a, f2 b) {
+    f2 d;
+    asm("sub.rn.ftz.f32x2 %0, %1, %2;" : "=l"(d) : "l"(a), "l"(b));
+    return d;
+}
+__device__ __forceinline__ f2 mul2(f2 a, f2 b) {
+    f2 d;
+    asm("mul.rn.ftz.f32x2 %0, %1, %2;" : "=l"(d) : "l"(a), "l"(b));
+    return d;
+}
+__device__ __forceinline__ f2 fma2(f2 a, f2 b, f2 c) {
+    f2 d;
+    asm("fma.rn.ftz.f32x2 %0, %1, %2, %3;" : "=l"(d) : "l"(a), "l"(b), "l"(c));
+    return d;
+}
+// fold_f on both halves: t = rn(d/L) via the 1.5*2^23 constant, d - t L
+// (nL = -L).
+__device__ __forceinline__ f2 fold2(f2 d, f2 nL, f2 invL) {
+    const f2 magic = bc2(12582912.0f), nmagic = bc2(-12582912.0f);
+    f2 t = add2(fma2(d, invL, magic), nmagic);
+    return fma2(t, nL, d);
+}
+
+template <int KIND, bool FOLD, bool DAMP>
+__device__ __forceinline__ void field_walk2_x2(const PairParams& P, const double* __restrict__ pos,
+                                               const float4* __restrict__ sp, const float4* __restrict__ sv, int lane,
+                                               int jbase, int ia, float oax, float oay, float oaz, float qa, float4 va,
+                                               int ib, float obx, float oby, float obz, float qb, float4 vb,
+                                               float damp_r2, float* fa, float* fb, float* g) {
+    const int nxt = (lane + 1) & 31;
+    const f2 OX = pk2(oax, obx), OY = pk2(oay, oby), OZ = pk2(oaz, obz);
+    const f2 VX = pk2(va.x, vb.x), VY = pk2(va.y, vb.y), VZ = pk2(va.z, vb.z);
+    const f2 NVX = pk2(-va.x, -vb.x), NVY = pk2(-va.y, -vb.y), NVZ = pk2(-va.z, -vb.z);
+    const f2 QI = pk2(qa, qb), THREE = bc2(3.0f), NEG = bc2(-1.0f);
+    f2 Lx = 0, Ly = 0, Lz = 0, Ix = 0, Iy = 0, Iz = 0;
+    float tx = 0.f, ty = 0.f, tz = 0.f;
+    if (FOLD) {
+        Lx = bc2(-(float)P.box[0]);
+        Ly = bc2(-(float)P.box[1]);
+        Lz = bc2(-(float)P.box[2]);
+        Ix = bc2((float)P.inv_box[0]);
+        Iy = bc2((float)P.inv_box[1]);
+        Iz = bc2((float)P.inv_box[2]);
+        tx = (float)P.half_box_tol[0];
+        ty = (float)P.half_box_tol[1];
+        tz = (float)P.half_box_tol[2];
+    }
+    // I-side sums (lo: slot a, hi: slot b); KIND 0 accumulates their negatives.
+    f2 FX = 0, FY = 0, FZ = 0;
+#pragma unroll 2
+    for (int s = 0; s < 32; s++) {
+        const int jj = (lane + s) & 31;
+        const float4 pj = sp[jj], vj = sv[jj];
+        f2 DX = sub2(bc2(pj.x), OX), DY = sub2(bc2(pj.y), OY), DZ = sub2(bc2(pj.z), OZ);
+        if (FOLD) {
+            DX = fold2(DX, Lx, Ix);
+            DY = fold2(DY, Ly, Iy);
+            DZ = fold2(DZ, Lz, Iz);
+            float ax, bx, ay, by, az, bz;
+            un2(DX, ax, bx);
+            un2(DY, ay, by);
+            un2(DZ, az, bz);
+            const bool amb_a = fabsf(ax) > tx || fabsf(ay) > ty || fabsf(az) > tz;
+            const bool amb_b = fabsf(bx) > tx || fabsf(by) > ty || fabsf(bz) > tz;
+            if (amb_a || amb_b) {
+                // Within 16 ulp of half a box: the reference's FP64 minimum image.
+                const int j = jbase + jj;
+                if (amb_a && ia < P.n && j < P.n) {
+                    d3 e = exact_delta(P, pos, ia, j);
+                    ax = (float)e.x;
+                    ay = (float)e.y;
+                    az = (float)e.z;
+                }
+                if (amb_b && ib < P.n && j < P.n) {
+                    d3 e = exact_delta(P, pos, ib, j);
+                    bx = (float)e.x;
+                    by = (float)e.y;
+                    bz = (float)e.z;
+                }
+                DX = pk2(ax, bx);
+                DY = pk2(ay, by);
+                DZ = pk2(az, bz);
+            }
+        }
+        const f2 R2 = fma2(DX, DX, fma2(DY, DY, mul2(DZ, DZ)));
+        float r2a, r2b;
+        un2(R2, r2a, r2b);
+        const f2 RINV = pk2(rsqrt_r(r2a), rsqrt_r(r2b));
+        const f2 RINV2 = mul2(RINV, RINV);
+        f2 RR3 = mul2(RINV, RINV2);
+        f2 RR5 = mul2(mul2(THREE, RR3), RINV2);
+        if (DAMP) {
+            if (r2a < damp_r2 || r2b < damp_r2) {
+                float ra, rb, r3a, r3b, r5a, r5b;
+                un2(RINV, ra, rb);
+                un2(RR3, r3a, r3b);
+                un2(RR5, r5a, r5b);
+                damp_field<float>(r2a, ra, va.w, vj.w, damp_r2, r3a, r5a);
+                damp_field<float>(r2b, rb, vb.w, vj.w, damp_r2, r3b, r5b);
+                RR3 = pk2(r3a, r3b);
+                RR5 = pk2(r5a, r5b);
+            }
+        }
+        const f2 NRR3 = mul2(RR3, NEG);
+        float gx, gy, gz, hx, hy, hz;
+        if (KIND == 1) {
+            // pair_matvec2: f_i += (rr5 v_j.d) d - rr3 v_j;  f_j += (rr5 v_i.d) d - rr3 v_i.
+            const f2 VJX = bc2(vj.x), VJY = bc2(vj.y), VJZ = bc2(vj.z);
+            const f2 DDJ = mul2(RR5, fma2(VJX, DX, fma2(VJY, DY, mul2(VJZ, DZ))));
+            const f2 DDI = mul2(RR5, fma2(VX, DX, fma2(VY, DY, mul2(VZ, DZ))));
+            FX = fma2(NRR3, VJX, fma2(DDJ, DX, FX));
+            FY = fma2(NRR3, VJY, fma2(DDJ, DY, FY));
+            FZ = fma2(NRR3, VJZ, fma2(DDJ, DZ, FZ));
+            un2(fma2(DDI, DX, mul2(NRR3, VX)), gx, hx);
+            un2(fma2(DDI, DY, mul2(NRR3, VY)), gy, hy);
+            un2(fma2(DDI, DZ, mul2(NRR3, VZ)), gz, hz);
+        } else {
+            // pair_fixed2: a = rr3 q_j - rr5 m_j.d, b = rr3 q_i + rr5 m_i.d;
+            // f_i -= d a + m_j rr3;  f_j += d b - m_i rr3.
+            const f2 MJX = bc2(vj.x), MJY = bc2(vj.y), MJZ = bc2(vj.z);
+            const f2 A = sub2(mul2(RR3, bc2(pj.w)), mul2(RR5, fma2(MJX, DX, fma2(MJY, DY, mul2(MJZ, DZ)))));
+            const f2 B = fma2(RR5, fma2(VX, DX, fma2(VY, DY, mul2(VZ, DZ))), mul2(RR3, QI));
+            FX = fma2(MJX, RR3, fma2(DX, A, FX));
+            FY = fma2(MJY, RR3, fma2(DY, A, FY));
+            FZ = fma2(MJZ, RR3, fma2(DZ, A, FZ));
+            un2(fma2(DX, B, mul2(NVX, RR3)), gx, hx);
+            un2(fma2(DY, B, mul2(NVY, RR3)), gy, hy);
+            un2(fma2(DZ, B, mul2(NVZ, RR3)), gz, hz);
+        }
+        g[0] += gx + hx;
+        g[1] += gy + hy;
+        g[2] += gz + hz;
+        g[0] = __shfl_sync(kFull, g[0], nxt);
+        g[1] = __shfl_sync(kFull, g[1], nxt);
+        g[2] = __shfl_sync(kFull, g[2], nxt);
+    }
+    float lx, hx2, ly, hy2, lz, hz2;
+    un2(FX, lx, hx2);
+    un2(FY, ly, hy2);
+    un2(FZ, lz, hz2);
+    const float sg = KIND == 0 ? -1.0f : 1.0f;
+    fa[0] += sg * lx;
+    fa[1] += sg * ly;
+    fa[2] += sg * lz;
+    fb[0] += sg * hx2;
+    fb[1] += sg * hy2;
+    fb[2] += sg * hz2;
+}
+
 // Partner pairs of a SLOW tile pair, each side once with its scale (M for
 // the permanent field, I for the matvec): lane l adds, for its I atom, the
 // partners in J, and for atom l of J (not on the diagonal tile), the partners
@@ -418,7 +593,21 @@ __global__ void __launch_bounds__(kSymThreads, 4) k_field_sym(
     field_walk2<R, KIND, F, S, D>(P, pos, sp, sv, lane, jbase, a.i, a.ox, a.oy, a.oz, a.pi.w, a.vi, a.diag,     \
                                   a.partners, b.i, b.ox, b.oy, b.oz, b.pi.w, b.vi, b.diag, b.partners, damp_r2, fa, \
                                   fb, g)
-                if (slow) {
+#define TDP_FWALKX2(F, D)                                                                                          \
+    field_walk2_x2<KIND, F, D>(P, pos, (const float4*)sp, (const float4*)sv, lane, jbase, a.i, (float)a.ox,      \
+                               (float)a.oy, (float)a.oz, (float)a.pi.w, to_f4(a.vi), b.i, (float)b.ox, (float)b.oy, \
+                               (float)b.oz, (float)b.pi.w, to_f4(b.vi), (float)damp_r2, (float*)fa, (float*)fb,    \
+                               (float*)g)
+                if (sizeof(R) == 4 && !slow) {
+                    if (fold) {
+                        if (near) TDP_FWALKX2(true, true);
+                        else TDP_FWALKX2(true, false);
+                    } else if (near) {
+                        TDP_FWALKX2(false, true);
+                    } else {
+                        TDP_FWALKX2(false, false);
+                    }
+                } else if (slow) {
                     if (fold) TDP_FWALK2(true, true, true);
                     else TDP_FWALK2(false, true, true);
                 } else if (fold) {
@@ -430,6 +619,7 @@ __global__ void __launch_bounds__(kSymThreads, 4) k_field_sym(
                     TDP_FWALK2(false, false, false);
                 }
 #undef TDP_FWALK2
+#undef TDP_FWALKX2
             } else {
                 const ISlot<R>& s1 = a.valid ? a : b;
                 R* f1 = a.valid ? fa : fb;

@@ -84,7 +84,7 @@ class DeviceRigidWaterMD:
     """Everything on the GPU; positions/velocities/forces are torch CUDA tensors."""
 
     def __init__(self, system: TholeSystem, precision="mixed", dt: float = 0.001, temperature: float = 300.0,
-                 seed: int = 0, warm_start: bool = True, device: str = "cuda:0"):
+                 seed: int = 0, warm_start: bool = True, device: str = "cuda:0", ewald: bool = False):
         import torch
 
         self.torch = torch
@@ -93,7 +93,7 @@ class DeviceRigidWaterMD:
         self.dt = dt
         self.dev = torch.device(device)
         self.lib = A.lib()
-        self.kernel = CudaCalcTholeDipoleForceKernel(system, precision=precision, warm_start=warm_start)
+        self.kernel = CudaCalcTholeDipoleForceKernel(system, precision=precision, warm_start=warm_start, ewald=ewald)
         self.stream = torch.cuda.current_stream(self.dev)
         self.kernel.setStream(self.stream.cuda_stream)
         self.pos = torch.tensor(system.positions, dtype=torch.float64, device=self.dev).contiguous()
@@ -147,11 +147,11 @@ class HostRigidWaterMD:
     hands host positions to the C ABI and reads forces back."""
 
     def __init__(self, system: TholeSystem, precision="mixed", dt: float = 0.001, temperature: float = 300.0,
-                 seed: int = 0, warm_start: bool = True, pinned: Optional[np.ndarray] = None):
+                 seed: int = 0, warm_start: bool = True, pinned: Optional[np.ndarray] = None, ewald: bool = False):
         self.n = system.n
         self.nw = system.n // 3
         self.dt = dt
-        self.kernel = CudaCalcTholeDipoleForceKernel(system, precision=precision, warm_start=warm_start)
+        self.kernel = CudaCalcTholeDipoleForceKernel(system, precision=precision, warm_start=warm_start, ewald=ewald)
         self.pos = np.array(system.positions, dtype=np.float64) if pinned is None else pinned
         if pinned is not None:
             self.pos[...] = system.positions
