@@ -67,6 +67,7 @@ struct tdp_handle {
     std::vector<void*> owned;
     cudaStream_t stream = nullptr;
     double* h_scal = nullptr;   // pinned scalar readback
+    int* h_fixerr = nullptr;    // pinned copy of the accumulator range flag
     double* h_forces = nullptr; // pinned n*3
     double* d_stage = nullptr;  // device staging for host FP32 positions / query inputs
     size_t stage_bytes = 0;
@@ -481,6 +482,7 @@ void setup_and_solve(tdp_handle* h) {
     h->matvecs = 0;
     h->launches = 0;
     h->kev_used = 0;
+    if (d.fix_err) TDP_CUDA(cudaMemsetAsync(d.fix_err, 0, sizeof(int), st));
     record(h, 0);
     launch_pack<R>(d, st);
     launch_rotate<R>(d, st);
@@ -567,6 +569,21 @@ void finish_timing(tdp_handle* h) {
     h->stage_ms[7] = mv;
     h->stage_ms[8] = en;
     h->stage_ms[9] = (double)h->launches;
+}
+
+// Device-side failure flags of the last evaluation: enqueue their readback
+// before the stream is synchronised, check them after.
+void enqueue_flags(tdp_handle* h) {
+    if (h->d.fix_err)
+        TDP_CUDA(cudaMemcpyAsync(h->h_fixerr, h->d.fix_err, sizeof(int), cudaMemcpyDeviceToHost, h->stream));
+}
+void check_flags(tdp_handle* h) {
+    if (h->ew && ewald_list_overflow(h->ew))
+        throw TdpError{TDP_ERR_CUDA, "Ewald mode: a neighbour-tile list row overflowed its capacity"};
+    if (h->d.fix_err && *h->h_fixerr)
+        throw TdpError{TDP_ERR_NON_FINITE,
+                       "a field or force sum is not finite or exceeds the fixed-point accumulator range "
+                       "(2^23 per band sum; near-coincident particles?)"};
 }
 
 void solve_at(tdp_handle* h, const void* positions, int dtype, int on_device) {
@@ -805,6 +822,17 @@ int tdp_create(const tdp_system_desc* desc, tdp_handle** out) {
             // Real space in partial slot 0, reciprocal space + self in slot 1.
             d.nsplit = 2;
             d.n_eblk = 1;
+        } else if (h->precision == TDP_PRECISION_MIXED) {
+            // Mixed all-pairs form: the band sums go into the fixed-point
+            // accumulator and one flushed slot.  Each atom's word receives at
+            // most 2 n_bands adds of magnitude < 2^23, so with 2^bits units
+            // per e/nm^2 the sum stays below 2^61.
+            d.nsplit = 1;
+            int lg = 0;
+            while ((1L << lg) < 2L * std::max(1, d.pp.n_bands)) lg++;
+            const int bits = std::min(32, 38 - lg);
+            d.fix_scale = std::ldexp(1.0, bits);
+            d.fix_limit = std::ldexp(1.0, 23);
         }
 
         std::vector<int> eoff(n + 1, 0), ej;
@@ -861,6 +889,10 @@ int tdp_create(const tdp_system_desc* desc, tdp_handle** out) {
         d.q = dalloc<double>(n3, o);
         d.hist = dalloc<double>(n3 * h->extrap.size(), o);
         d.partial = dalloc<double>((size_t)d.nsplit * 6 * d.n_pad, o);
+        if (d.fix_scale > 0.0) {
+            d.fixacc = dalloc<unsigned long long>(6 * (size_t)d.n_pad, o);
+            d.fix_err = dalloc<int>(1, o);
+        }
         d.energy_partial = dalloc<double>((size_t)d.n_eblk, o);
         d.fpair = dalloc<double>(n3, o);
         d.torque = dalloc<double>(n3, o);
@@ -902,6 +934,8 @@ int tdp_create(const tdp_system_desc* desc, tdp_handle** out) {
         upload_params(h);
         if (ewald) h->ew = ewald_create(d, h->precision);
         TDP_CUDA(cudaMallocHost(&h->h_scal, 64 * sizeof(double)));
+        TDP_CUDA(cudaMallocHost(&h->h_fixerr, sizeof(int)));
+        *h->h_fixerr = 0;
         TDP_CUDA(cudaMallocHost(&h->h_forces, std::max<size_t>(n3, 1) * sizeof(double)));
         for (int k = 0; k < 6; k++) TDP_CUDA(cudaEventCreate(&h->ev[k]));
         refresh_box(h);
@@ -925,6 +959,7 @@ void tdp_destroy(tdp_handle* h) {
     if (h->ew) ewald_destroy(h->ew);
     for (void* p : h->owned) cudaFree(p);
     if (h->h_scal) cudaFreeHost(h->h_scal);
+    if (h->h_fixerr) cudaFreeHost(h->h_fixerr);
     if (h->h_forces) cudaFreeHost(h->h_forces);
     for (int k = 0; k < 6; k++)
         if (h->ev[k]) cudaEventDestroy(h->ev[k]);
@@ -1006,6 +1041,7 @@ int tdp_compute(tdp_handle* h, const void* positions, int32_t pos_dtype, int32_t
             }
         }
         if (energy) TDP_CUDA(cudaMemcpyAsync(h->h_scal + 1, h->d.energy, sizeof(double), cudaMemcpyDeviceToHost, st));
+        enqueue_flags(h);
         TDP_CUDA(cudaStreamSynchronize(st));
         TDP_CUDA(cudaGetLastError());
         if ((flags & TDP_COMPUTE_FORCES) && !on_device) {
@@ -1017,8 +1053,7 @@ int tdp_compute(tdp_handle* h, const void* positions, int32_t pos_dtype, int32_t
                 for (size_t k = 0; k < n3; k++) acc[k] += (float)h->h_forces[k];
             }
         }
-        if (h->ew && ewald_list_overflow(h->ew))
-            throw TdpError{TDP_ERR_CUDA, "Ewald mode: a neighbour-tile list row overflowed its capacity"};
+        check_flags(h);
         if (energy) *energy = h->h_scal[1];
         finish_timing(h);
         if (h->status == TDP_STATUS_NON_FINITE)
@@ -1041,11 +1076,10 @@ int tdp_get_dipoles(tdp_handle* h, int32_t which, const void* positions, int32_t
         solve_at(h, positions, pos_dtype, on_device);
         size_t n3 = 3 * (size_t)h->n;
         cudaStream_t st = h->stream;
+        enqueue_flags(h);
         if (which == TDP_DIPOLES_INDUCED) {
             TDP_CUDA(cudaMemcpyAsync(out, h->d.mu, n3 * 8, cudaMemcpyDeviceToHost, st));
             TDP_CUDA(cudaStreamSynchronize(st));
-            if (h->ew && ewald_list_overflow(h->ew))
-                throw TdpError{TDP_ERR_CUDA, "Ewald mode: a neighbour-tile list row overflowed its capacity"};
         } else if (which == TDP_DIPOLES_LAB_PERMANENT) {
             TDP_CUDA(cudaMemcpyAsync(out, h->d.lab, n3 * 8, cudaMemcpyDeviceToHost, st));
             TDP_CUDA(cudaStreamSynchronize(st));
@@ -1055,6 +1089,7 @@ int tdp_get_dipoles(tdp_handle* h, int32_t which, const void* positions, int32_t
             TDP_CUDA(cudaStreamSynchronize(st));
             for (size_t k = 0; k < n3; k++) out[k] += h->h_forces[k];
         }
+        check_flags(h);
     } catch (const TdpError& e) {
         return fail(h, e);
     }

@@ -63,6 +63,14 @@ struct Dev {
     double* q = nullptr;
     double* hist = nullptr;      // extrapolation orders, korder*n*3
     double* partial = nullptr;   // nsplit*6*n_pad pair-kernel partial sums (scratch)
+    // Mixed all-pairs form: the field and energy kernels add their per-band
+    // sums into one 64-bit fixed-point accumulator (6*n_pad, units of
+    // 1/fix_scale; integer addition makes the result independent of the order)
+    // that a flush kernel converts into partial slot 0 and clears (nsplit = 1).
+    // A sum of magnitude >= fix_limit sets *fix_err instead of wrapping.
+    unsigned long long* fixacc = nullptr;
+    int* fix_err = nullptr;
+    double fix_scale = 0.0, fix_limit = 0.0;
     double* energy_partial = nullptr;
     double* fpair = nullptr;
     double* torque = nullptr;

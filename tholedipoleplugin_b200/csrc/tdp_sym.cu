@@ -158,6 +158,24 @@ __device__ __forceinline__ unsigned partner_bits(const int* __restrict__ exc_j, 
     return b;
 }
 
+// 64-bit fixed-point accumulator of the mixed form (Dev::fixacc).
+struct FixAcc {
+    unsigned long long* acc;
+    int* err;
+    double scale, limit;
+};
+
+// Adds v to the accumulator word; a sum at or beyond the limit (or not finite)
+// flags the error instead of wrapping.
+__device__ __forceinline__ void fix_add(const FixAcc& F, size_t k, double v) {
+    if (v == 0.0) return;
+    if (!(fabs(v) < F.limit)) {
+        atomicExch(F.err, 1);
+        return;
+    }
+    atomicAdd(F.acc + k, (unsigned long long)__double2ll_rn(v * F.scale));
+}
+
 // ---------------------------------------------------------------------------
 // Field kernels: KIND 0 = permanent field (records: posq + lab dipole/thole),
 // KIND 1 = mutual-field matvec T*v (records: posq + v/thole).
@@ -527,7 +545,8 @@ __global__ void __launch_bounds__(kSymThreads, 4) k_field_sym(
     PairParams P, const typename Vec4T<R>::type* __restrict__ posq, const typename Vec4T<R>::type* __restrict__ jvec,
     const double4* __restrict__ tctr, const double4* __restrict__ text, const double* __restrict__ pos,
     const int* __restrict__ exc_off, const int* __restrict__ exc_j, const double* __restrict__ exc_m,
-    const double* __restrict__ exc_s, const int2* __restrict__ exc_tiles, int n_pad, double* __restrict__ partial) {
+    const double* __restrict__ exc_s, const int2* __restrict__ exc_tiles, int n_pad, double* __restrict__ partial,
+    FixAcc fix) {
     typedef typename Vec4T<R>::type V4;
     extern __shared__ __align__(16) unsigned char smem[];
     const int BT = P.band_tiles, NA = BT * 32;
@@ -666,11 +685,16 @@ __global__ void __launch_bounds__(kSymThreads, 4) k_field_sym(
         }
         // I-side sums: slot q of band p; on the diagonal band, slot p, where
         // the J-side sums of the same atoms are added below.
+        // (Mixed form: added into the fixed-point accumulator instead.)
         for (int k = 0; k < 2; k++) {
             const ISlot<R>& s1 = k == 0 ? a : b;
             if (!s1.act) continue;
-            const size_t base = (size_t)q * 3 * n_pad;
-            for (int c = 0; c < 3; c++) partial[base + (size_t)c * n_pad + s1.i] = my[3 * k + c];
+            if (sizeof(R) == 4) {
+                for (int c = 0; c < 3; c++) fix_add(fix, (size_t)c * n_pad + s1.i, my[3 * k + c]);
+            } else {
+                const size_t base = (size_t)q * 3 * n_pad;
+                for (int c = 0; c < 3; c++) partial[base + (size_t)c * n_pad + s1.i] = my[3 * k + c];
+            }
         }
     }
     __syncthreads();
@@ -679,9 +703,14 @@ __global__ void __launch_bounds__(kSymThreads, 4) k_field_sym(
         const int a = qa0 + k;
         const bool own = p == q && (a >> 5) < P.n_tiles;
         for (int c = 0; c < 3; c++) {
-            double v = own ? partial[base + (size_t)c * n_pad + a] : 0.0;
+            double v = 0.0;
             for (int w = 0; w < kSymWarps; w++) v += (double)s_acc[w * 3 * NA + 3 * k + c];
-            partial[base + (size_t)c * n_pad + a] = v;
+            if (sizeof(R) == 4) {
+                fix_add(fix, (size_t)c * n_pad + a, v);
+            } else {
+                if (own) v += partial[base + (size_t)c * n_pad + a];
+                partial[base + (size_t)c * n_pad + a] = v;
+            }
         }
     }
 }
@@ -826,7 +855,8 @@ __global__ void __launch_bounds__(kSymThreads, 3) k_energy_sym(
     const typename Vec4T<R>::type* __restrict__ indv, const double2* __restrict__ yz, const double4* __restrict__ tctr,
     const double4* __restrict__ text, const double* __restrict__ pos, const int* __restrict__ exc_off,
     const int* __restrict__ exc_j, const double* __restrict__ exc_m, const double* __restrict__ exc_s,
-    const int2* __restrict__ exc_tiles, int n_pad, double* __restrict__ partial, double* __restrict__ energy_partial) {
+    const int2* __restrict__ exc_tiles, int n_pad, double* __restrict__ partial, double* __restrict__ energy_partial,
+    FixAcc fix) {
     typedef typename Vec4T<R>::type V4;
     extern __shared__ __align__(16) unsigned char smem[];
     const int BT = P.band_tiles, NA = BT * 32;
@@ -934,6 +964,8 @@ __global__ void __launch_bounds__(kSymThreads, 3) k_energy_sym(
             if (p == q) {
                 double* acc = s_acc + 6 * (Il * 32 + lane);
                 for (int c = 0; c < 6; c++) acc[c] += my[c];
+            } else if (sizeof(R) == 4) {
+                for (int c = 0; c < 6; c++) fix_add(fix, (size_t)c * n_pad + i, my[c]);
             } else {
                 const size_t b = (size_t)q * 6 * n_pad;
                 for (int c = 0; c < 6; c++) partial[b + (size_t)c * n_pad + i] = my[c];
@@ -943,7 +975,10 @@ __global__ void __launch_bounds__(kSymThreads, 3) k_energy_sym(
     }
     const size_t b = (size_t)p * 6 * n_pad;
     for (int k = threadIdx.x; k < NA; k += kSymThreads)
-        for (int c = 0; c < 6; c++) partial[b + (size_t)c * n_pad + qa0 + k] = s_acc[6 * k + c];
+        for (int c = 0; c < 6; c++) {
+            if (sizeof(R) == 4) fix_add(fix, (size_t)c * n_pad + qa0 + k, s_acc[6 * k + c]);
+            else partial[b + (size_t)c * n_pad + qa0 + k] = s_acc[6 * k + c];
+        }
     // CTA energy, summed in thread order (padding atoms contribute exactly 0).
     double e = warp_sum(my[6]);
     __shared__ double s_red[kSymWarps];
@@ -972,6 +1007,24 @@ size_t energy_smem(int BT) {
 
 int band_pairs(const Dev& d) { return d.pp.n_bands * (d.pp.n_bands + 1) / 2; }
 
+// Fixed-point accumulator -> partial slot 0 (ncomp components of n_pad), clearing it.
+__global__ void k_fix_flush(size_t count, unsigned long long* __restrict__ acc, double inv_scale,
+                            double* __restrict__ out) {
+    size_t k = (size_t)blockIdx.x * blockDim.x + threadIdx.x;
+    if (k >= count) return;
+    long long v = (long long)acc[k];
+    acc[k] = 0ull;
+    out[k] = (double)v * inv_scale;
+}
+
+FixAcc fix_of(const Dev& d) { return FixAcc{d.fixacc, d.fix_err, d.fix_scale, d.fix_limit}; }
+
+void fix_flush(const Dev& d, int ncomp, cudaStream_t st) {
+    if (!d.fixacc) return;
+    const size_t count = (size_t)ncomp * d.n_pad;
+    k_fix_flush<<<(unsigned)((count + 255) / 256), 256, 0, st>>>(count, d.fixacc, 1.0 / d.fix_scale, d.partial);
+}
+
 }  // namespace
 
 template <class R>
@@ -983,13 +1036,14 @@ void launch_field(const Dev& d, int kind, cudaStream_t st) {
         cudaFuncSetAttribute(k_field_sym<R, 0>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
         k_field_sym<R, 0><<<band_pairs(d), kSymThreads, smem, st>>>(
             d.pp, (const V4*)d.posq_s, (const V4*)d.dipt_s, d.tctr_s, d.text_s, d.pos_s, d.exs_off, d.exs_j, d.exs_m,
-            d.exs_s, d.exs_tiles, d.n_pad, d.partial);
+            d.exs_s, d.exs_tiles, d.n_pad, d.partial, fix_of(d));
     } else {
         cudaFuncSetAttribute(k_field_sym<R, 1>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
         k_field_sym<R, 1><<<band_pairs(d), kSymThreads, smem, st>>>(
             d.pp, (const V4*)d.posq_s, (const V4*)d.vec_s, d.tctr_s, d.text_s, d.pos_s, d.exs_off, d.exs_j, d.exs_m,
-            d.exs_s, d.exs_tiles, d.n_pad, d.partial);
+            d.exs_s, d.exs_tiles, d.n_pad, d.partial, fix_of(d));
     }
+    if (sizeof(R) == 4) fix_flush(d, 3, st);
 }
 
 template <class R>
@@ -999,7 +1053,8 @@ void launch_energy(const Dev& d, cudaStream_t st) {
     cudaFuncSetAttribute(k_energy_sym<R>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
     k_energy_sym<R><<<band_pairs(d), kSymThreads, smem, st>>>(
         d.pp, (const V4*)d.posq, (const V4*)d.dipt, (const V4*)d.ind, d.yz, d.tctr, d.text, d.pos, d.exc_off, d.exc_j,
-        d.exc_m, d.exc_s, d.exc_tiles, d.n_pad, d.partial, d.energy_partial);
+        d.exc_m, d.exc_s, d.exc_tiles, d.n_pad, d.partial, d.energy_partial, fix_of(d));
+    if (sizeof(R) == 4) fix_flush(d, 6, st);
 }
 
 template void launch_field<float>(const Dev&, int, cudaStream_t);
