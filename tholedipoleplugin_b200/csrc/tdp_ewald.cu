@@ -297,6 +297,173 @@ __device__ __forceinline__ void ew_field_exceptions(const PairParams& P, const E
     }
 }
 
+// ---------------------------------------------------------------------------
+// Packed FP32 walk of the mixed form (sm_100 f32x2 arithmetic): each step
+// evaluates the lane's I atom against two J atoms, whose records are staged
+// pair-interleaved (x_2m, x_2m+1, y_2m, y_2m+1) so 128-bit shared loads give
+// packed operands directly.  erfc(x) = t P(t) exp(-x^2) with t = 1/(1 + p x):
+// the Hastings form (Abramowitz & Stegun 7.1.26) with coefficients fitted
+// here to erfc on [0, 4.5] in relative error (1.1e-8 in exact arithmetic,
+// 1.2e-6 at x = 4.3 evaluated in FP32), sharing exp(-x^2) with the B kernels.
+// Thole damping uses 1/t precomputed per atom.
+// ---------------------------------------------------------------------------
+typedef unsigned long long f2;
+__device__ __forceinline__ f2 pk2(float lo, float hi) {
+    f2 r;
+    asm("mov.b64 %0, {%1, %2};" : "=l"(r) : "f"(lo), "f"(hi));
+    return r;
+}
+__device__ __forceinline__ f2 bc2(float v) { return pk2(v, v); }
+__device__ __forceinline__ void un2(f2 v, float& lo, float& hi) {
+    asm("mov.b64 {%0, %1}, %2;" : "=f"(lo), "=f"(hi) : "l"(v));
+}
+__device__ __forceinline__ f2 add2(f2 a, f2 b) {
+    f2 d;
+    asm("add.rn.ftz.f32x2 %0, %1, %2;" : "=l"(d) : "l"(a), "l"(b));
+    return d;
+}
+__device__ __forceinline__ f2 sub2(f2 a, f2 b) {
+    f2 d;
+    asm("sub.rn.ftz.f32x2 %0, %1, %2;" : "=l"(d) : "l"(a), "l"(b));
+    return d;
+}
+__device__ __forceinline__ f2 mul2(f2 a, f2 b) {
+    f2 d;
+    asm("mul.rn.ftz.f32x2 %0, %1, %2;" : "=l"(d) : "l"(a), "l"(b));
+    return d;
+}
+__device__ __forceinline__ f2 fma2(f2 a, f2 b, f2 c) {
+    f2 d;
+    asm("fma.rn.ftz.f32x2 %0, %1, %2, %3;" : "=l"(d) : "l"(a), "l"(b), "l"(c));
+    return d;
+}
+
+constexpr float kErfcP = 0.41f;
+__constant__ float c_erfc[8] = {0.2307648634694866f,  0.23957919808529987f, 0.15874078916517892f,
+                                0.3642441184340127f,  -0.29754436616944707f, 0.6117635229498828f,
+                                -0.3865500288941725f, 0.0790019121010213f};
+
+struct EwPackedTile {
+    float4 p0[16], p1[16], v0[16], v1[16];   // (x,x' y,y') (z,z' q,q') (vx,vx' vy,vy') (vz,vz' t,t')
+    float2 it[16];                           // 1/t of the pair
+};
+
+__device__ __forceinline__ void stage_packed(EwPackedTile& T, int lane, float4 p, float4 v) {
+    const int m = lane >> 1, h = lane & 1;
+    float* p0 = reinterpret_cast<float*>(&T.p0[m]);
+    float* p1 = reinterpret_cast<float*>(&T.p1[m]);
+    float* v0 = reinterpret_cast<float*>(&T.v0[m]);
+    float* v1 = reinterpret_cast<float*>(&T.v1[m]);
+    p0[h] = p.x;
+    p0[2 + h] = p.y;
+    p1[h] = p.z;
+    p1[2 + h] = p.w;
+    v0[h] = v.x;
+    v0[2 + h] = v.y;
+    v1[h] = v.z;
+    v1[2 + h] = v.w;
+    reinterpret_cast<float*>(&T.it[m])[h] = 1.0f / v.w;
+}
+
+template <int KIND, bool FOLD>
+__device__ __forceinline__ void ew_field_walk_x2(const PairParams& P, const EwParams& E, const EwPackedTile& T,
+                                                 float ox, float oy, float oz, float ti, float iti, float rc2,
+                                                 float damp_r2, float& fx, float& fy, float& fz) {
+    const f2 OX = bc2(ox), OY = bc2(oy), OZ = bc2(oz);
+    const f2 ALPHA = bc2((float)E.alpha), NA2 = bc2((float)(-E.alpha * E.alpha));
+    const f2 CA = bc2((float)E.ca), A2 = bc2((float)E.a2), ONE = bc2(1.0f), THREE = bc2(3.0f), NEG = bc2(-1.0f);
+    const f2 PP = bc2(kErfcP), ITI = bc2(iti);
+    f2 Lx = 0, Ly = 0, Lz = 0, Ix = 0, Iy = 0, Iz = 0;
+    if (FOLD) {
+        Lx = bc2(-(float)P.box[0]);
+        Ly = bc2(-(float)P.box[1]);
+        Lz = bc2(-(float)P.box[2]);
+        Ix = bc2((float)P.inv_box[0]);
+        Iy = bc2((float)P.inv_box[1]);
+        Iz = bc2((float)P.inv_box[2]);
+    }
+    const f2 MAGIC = bc2(12582912.0f), NMAGIC = bc2(-12582912.0f);
+    f2 FX = 0, FY = 0, FZ = 0;
+#pragma unroll 2
+    for (int m = 0; m < 16; m++) {
+        const float4 a = T.p0[m], b = T.p1[m], c = T.v0[m], d = T.v1[m];
+        const float2 it = T.it[m];
+        f2 DX = sub2(pk2(a.x, a.y), OX), DY = sub2(pk2(a.z, a.w), OY), DZ = sub2(pk2(b.x, b.y), OZ);
+        if (FOLD) {
+            DX = fma2(add2(fma2(DX, Ix, MAGIC), NMAGIC), Lx, DX);
+            DY = fma2(add2(fma2(DY, Iy, MAGIC), NMAGIC), Ly, DY);
+            DZ = fma2(add2(fma2(DZ, Iz, MAGIC), NMAGIC), Lz, DZ);
+        }
+        const f2 R2 = fma2(DX, DX, fma2(DY, DY, mul2(DZ, DZ)));
+        float r2a, r2b;
+        un2(R2, r2a, r2b);
+        const bool act_a = r2a < rc2, act_b = r2b < rc2;
+        if (!__any_sync(kFull, act_a || act_b)) continue;
+        r2a = act_a ? r2a : 1e30f;
+        r2b = act_b ? r2b : 1e30f;
+        const f2 R2S = pk2(r2a, r2b);
+        const f2 RINV = pk2(rsqrtf(r2a), rsqrtf(r2b));
+        const f2 RINV2 = mul2(RINV, RINV);
+        const f2 R = mul2(R2S, RINV);
+        const f2 X = mul2(ALPHA, R);
+        float ea, eb;
+        un2(mul2(NA2, R2S), ea, eb);
+        const f2 EX = pk2(__expf(ea), __expf(eb));
+        float da, db;
+        un2(fma2(PP, X, ONE), da, db);
+        const f2 TT = pk2(__fdividef(1.0f, da), __fdividef(1.0f, db));
+        f2 POLY = bc2(c_erfc[7]);
+#pragma unroll
+        for (int k = 6; k >= 0; k--) POLY = fma2(POLY, TT, bc2(c_erfc[k]));
+        const f2 B0 = mul2(mul2(mul2(POLY, TT), EX), RINV);
+        const f2 G1 = mul2(CA, EX);
+        f2 B1 = mul2(add2(B0, G1), RINV2);
+        f2 B2 = mul2(fma2(THREE, B1, mul2(G1, A2)), RINV2);
+        if (r2a < damp_r2 || r2b < damp_r2) {
+            // -(1 - l3) b1 and -(1 - l5) b2 with u = r / (t_i t_j), a = min(t_i, t_j).
+            const f2 U = mul2(mul2(R, ITI), pk2(it.x, it.y));
+            const f2 AM = pk2(fminf(ti, d.z), fminf(ti, d.w));
+            const f2 AU3 = mul2(AM, mul2(U, mul2(U, U)));
+            float xa, xb;
+            un2(AU3, xa, xb);
+            // Per half: e^{-a u^3} and (1 + a u^3) e^{-a u^3}, zero outside the
+            // damping range (a masked half has u^3 = inf, never multiplied).
+            float eta = 0.0f, etb = 0.0f, wa = 0.0f, wb = 0.0f;
+            if (xa < 50.0f && r2a < damp_r2) {
+                eta = __expf(-xa);
+                wa = (1.0f + xa) * eta;
+            }
+            if (xb < 50.0f && r2b < damp_r2) {
+                etb = __expf(-xb);
+                wb = (1.0f + xb) * etb;
+            }
+            const f2 BB1 = mul2(RINV, RINV2);
+            B1 = sub2(B1, mul2(pk2(eta, etb), BB1));
+            B2 = sub2(B2, mul2(pk2(wa, wb), mul2(mul2(THREE, BB1), RINV2)));
+        }
+        const f2 VX = pk2(c.x, c.y), VY = pk2(c.z, c.w), VZ = pk2(d.x, d.y);
+        const f2 A = mul2(B2, fma2(VX, DX, fma2(VY, DY, mul2(VZ, DZ))));
+        const f2 NB1 = mul2(B1, NEG);
+        if (KIND == 0) {
+            const f2 Q = pk2(b.z, b.w);
+            FX = fma2(A, DX, fma2(NB1, fma2(Q, DX, VX), FX));
+            FY = fma2(A, DY, fma2(NB1, fma2(Q, DY, VY), FY));
+            FZ = fma2(A, DZ, fma2(NB1, fma2(Q, DZ, VZ), FZ));
+        } else {
+            FX = fma2(A, DX, fma2(NB1, VX, FX));
+            FY = fma2(A, DY, fma2(NB1, VY, FY));
+            FZ = fma2(A, DZ, fma2(NB1, VZ, FZ));
+        }
+    }
+    float lo, hi;
+    un2(FX, lo, hi);
+    fx += lo + hi;
+    un2(FY, lo, hi);
+    fy += lo + hi;
+    un2(FZ, lo, hi);
+    fz += lo + hi;
+}
+
 template <class R, int KIND>
 __global__ void __launch_bounds__(kEwThreads) k_ew_field(PairParams P, EwParams E,
                                                          const typename Vec4T<R>::type* __restrict__ posq_s,
@@ -310,6 +477,7 @@ __global__ void __launch_bounds__(kEwThreads) k_ew_field(PairParams P, EwParams 
                                                          double* __restrict__ out) {
     typedef typename Vec4T<R>::type V4;
     __shared__ V4 s_pos[kEwWarps][32], s_vec[kEwWarps][32];
+    __shared__ EwPackedTile s_pk[sizeof(R) == 4 ? kEwWarps : 1];
     __shared__ double s_red[kEwWarps][3][32];
     const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
     // One I tile per CTA; warp w takes list entries w, w + 4, ...; the four
@@ -327,12 +495,27 @@ __global__ void __launch_bounds__(kEwThreads) k_ew_field(PairParams P, EwParams 
         const int J = ent & kTileMask;
         const bool fold = (ent >> 30) & 1, slow = ((unsigned)ent >> 31) & 1u;
         __syncwarp();
-        s_pos[warp][lane] = posq_s[J * 32 + lane];
-        s_vec[warp][lane] = src[J * 32 + lane];
+        const V4 pj = posq_s[J * 32 + lane], vj = src[J * 32 + lane];
+        s_pos[warp][lane] = pj;
+        s_vec[warp][lane] = vj;
+        if constexpr (sizeof(R) == 4) {
+            if (!slow) stage_packed(s_pk[warp], lane, pj, vj);
+        }
         __syncwarp();
         R ox, oy, oz;
         tile_shift<R>(P, cA, tctr[J], pi.x, pi.y, pi.z, ox, oy, oz);
         R tx = 0, ty = 0, tz = 0;
+        if constexpr (sizeof(R) == 4) {
+            if (!slow) {
+                const float iti = 1.0f / (float)vi.w;
+                if (fold) ew_field_walk_x2<KIND, true>(P, E, s_pk[warp], ox, oy, oz, vi.w, iti, rc2, damp_r2, tx, ty, tz);
+                else ew_field_walk_x2<KIND, false>(P, E, s_pk[warp], ox, oy, oz, vi.w, iti, rc2, damp_r2, tx, ty, tz);
+                fx += (double)tx;
+                fy += (double)ty;
+                fz += (double)tz;
+                continue;
+            }
+        }
         if (slow) {
             const unsigned part = partner_bits(exs_j, e0, e1, J * 32);
             if (fold) ew_field_walk<R, KIND, true, true>(P, E, s_pos[warp], s_vec[warp], i, J * 32, ox, oy, oz, vi.w, part, rc2, damp_r2, tx, ty, tz);
@@ -465,6 +648,176 @@ __device__ __forceinline__ void ew_force_exceptions(const PairParams& P, const E
     }
 }
 
+// Packed J-pair records of the force walk: (x,x' y,y') (z,z' q,q')
+// (px,px' py,py') (pz,pz' t,t') (ux,ux' uy,uy') (uz,uz' -,-) and 1/t.
+struct EwPackedForceTile {
+    float4 p0[16], p1[16], d0[16], d1[16], u0[16], u1[16];
+    float2 it[16];
+};
+
+__device__ __forceinline__ void stage_packed_force(EwPackedForceTile& T, int lane, float4 p, float4 dv, float4 u) {
+    const int m = lane >> 1, h = lane & 1;
+    float* p0 = reinterpret_cast<float*>(&T.p0[m]);
+    float* p1 = reinterpret_cast<float*>(&T.p1[m]);
+    float* d0 = reinterpret_cast<float*>(&T.d0[m]);
+    float* d1 = reinterpret_cast<float*>(&T.d1[m]);
+    float* u0 = reinterpret_cast<float*>(&T.u0[m]);
+    float* u1 = reinterpret_cast<float*>(&T.u1[m]);
+    p0[h] = p.x;
+    p0[2 + h] = p.y;
+    p1[h] = p.z;
+    p1[2 + h] = p.w;
+    d0[h] = dv.x;
+    d0[2 + h] = dv.y;
+    d1[h] = dv.z;
+    d1[2 + h] = dv.w;
+    u0[h] = u.x;
+    u0[2 + h] = u.y;
+    u1[h] = u.z;
+    u1[2 + h] = 0.0f;
+    reinterpret_cast<float*>(&T.it[m])[h] = 1.0f / dv.w;
+}
+
+// pair_ewald on both halves: energy, force on i and field at i for kernels K.
+__device__ __forceinline__ void pair_ewald2(f2 DX, f2 DY, f2 DZ, f2 QI, f2 IX, f2 IY, f2 IZ, f2 QJ, f2 JX, f2 JY,
+                                            f2 JZ, f2 K0, f2 K1, f2 K2, f2 K3, f2& EN, f2& FX, f2& FY, f2& FZ,
+                                            f2& GX, f2& GY, f2& GZ) {
+    const f2 NEG = bc2(-1.0f);
+    const f2 DIR = fma2(IX, DX, fma2(IY, DY, mul2(IZ, DZ)));
+    const f2 DJR = fma2(JX, DX, fma2(JY, DY, mul2(JZ, DZ)));
+    const f2 DIDJ = fma2(IX, JX, fma2(IY, JY, mul2(IZ, JZ)));
+    const f2 G0 = mul2(QI, QJ);
+    const f2 G1 = add2(fma2(QJ, DIR, mul2(mul2(QI, DJR), NEG)), DIDJ);
+    const f2 G2 = mul2(mul2(DIR, DJR), NEG);
+    EN = fma2(G0, K0, fma2(G1, K1, fma2(G2, K2, EN)));
+    const f2 NC = mul2(fma2(G0, K1, fma2(G1, K2, mul2(G2, K3))), NEG);
+    const f2 NA = mul2(mul2(DJR, K2), NEG), NB = mul2(mul2(DIR, K2), NEG);
+    const f2 NQI = mul2(QI, NEG);
+    // f -= d c - K1 (q_j d_i - q_i d_j) + a d_i + b d_j
+    FX = fma2(DX, NC, fma2(K1, fma2(QJ, IX, mul2(NQI, JX)), fma2(NA, IX, fma2(NB, JX, FX))));
+    FY = fma2(DY, NC, fma2(K1, fma2(QJ, IY, mul2(NQI, JY)), fma2(NA, IY, fma2(NB, JY, FY))));
+    FZ = fma2(DZ, NC, fma2(K1, fma2(QJ, IZ, mul2(NQI, JZ)), fma2(NA, IZ, fma2(NB, JZ, FZ))));
+    // field += -K1 (q_j d + d_j) + a d
+    const f2 NK1 = mul2(K1, NEG), A = mul2(DJR, K2);
+    GX = fma2(A, DX, fma2(NK1, fma2(QJ, DX, JX), GX));
+    GY = fma2(A, DY, fma2(NK1, fma2(QJ, DY, JY), GY));
+    GZ = fma2(A, DZ, fma2(NK1, fma2(QJ, DZ, JZ), GZ));
+}
+
+template <bool FOLD>
+__device__ __forceinline__ void ew_force_walk_x2(const PairParams& P, const EwParams& E, const EwPackedForceTile& T,
+                                                 float ox, float oy, float oz, float qi, float4 di, float4 ui,
+                                                 float iti, float rc2, float damp_r2, float& en, float* f, float* g) {
+    const f2 OX = bc2(ox), OY = bc2(oy), OZ = bc2(oz);
+    const f2 ALPHA = bc2((float)E.alpha), NA2 = bc2((float)(-E.alpha * E.alpha));
+    const f2 CA = bc2((float)E.ca), A2 = bc2((float)E.a2), ONE = bc2(1.0f), THREE = bc2(3.0f),
+             FIVE = bc2(5.0f), HALF = bc2(0.5f), ZERO = bc2(0.0f);
+    const f2 PP = bc2(kErfcP), ITI = bc2(iti), QI = bc2(qi);
+    const f2 PIX = bc2(di.x), PIY = bc2(di.y), PIZ = bc2(di.z);
+    const f2 TIX = bc2(di.x + ui.x), TIY = bc2(di.y + ui.y), TIZ = bc2(di.z + ui.z);
+    f2 Lx = 0, Ly = 0, Lz = 0, Ix = 0, Iy = 0, Iz = 0;
+    if (FOLD) {
+        Lx = bc2(-(float)P.box[0]);
+        Ly = bc2(-(float)P.box[1]);
+        Lz = bc2(-(float)P.box[2]);
+        Ix = bc2((float)P.inv_box[0]);
+        Iy = bc2((float)P.inv_box[1]);
+        Iz = bc2((float)P.inv_box[2]);
+    }
+    const f2 MAGIC = bc2(12582912.0f), NMAGIC = bc2(-12582912.0f);
+    f2 EN = 0, FX = 0, FY = 0, FZ = 0, GX = 0, GY = 0, GZ = 0;
+#pragma unroll 1
+    for (int m = 0; m < 16; m++) {
+        const float4 a = T.p0[m], b = T.p1[m], c = T.d0[m], d = T.d1[m], u = T.u0[m], v = T.u1[m];
+        const float2 it = T.it[m];
+        f2 DX = sub2(pk2(a.x, a.y), OX), DY = sub2(pk2(a.z, a.w), OY), DZ = sub2(pk2(b.x, b.y), OZ);
+        if (FOLD) {
+            DX = fma2(add2(fma2(DX, Ix, MAGIC), NMAGIC), Lx, DX);
+            DY = fma2(add2(fma2(DY, Iy, MAGIC), NMAGIC), Ly, DY);
+            DZ = fma2(add2(fma2(DZ, Iz, MAGIC), NMAGIC), Lz, DZ);
+        }
+        const f2 R2 = fma2(DX, DX, fma2(DY, DY, mul2(DZ, DZ)));
+        float r2a, r2b;
+        un2(R2, r2a, r2b);
+        const bool act_a = r2a < rc2, act_b = r2b < rc2;
+        if (!__any_sync(kFull, act_a || act_b)) continue;
+        r2a = act_a ? r2a : 1e30f;
+        r2b = act_b ? r2b : 1e30f;
+        const f2 R2S = pk2(r2a, r2b);
+        const f2 RINV = pk2(rsqrtf(r2a), rsqrtf(r2b));
+        const f2 RINV2 = mul2(RINV, RINV);
+        const f2 R = mul2(R2S, RINV);
+        const f2 X = mul2(ALPHA, R);
+        float ea, eb;
+        un2(mul2(NA2, R2S), ea, eb);
+        const f2 EX = pk2(__expf(ea), __expf(eb));
+        float da, db;
+        un2(fma2(PP, X, ONE), da, db);
+        const f2 TT = pk2(__fdividef(1.0f, da), __fdividef(1.0f, db));
+        f2 POLY = bc2(c_erfc[7]);
+#pragma unroll
+        for (int k = 6; k >= 0; k--) POLY = fma2(POLY, TT, bc2(c_erfc[k]));
+        const f2 B0 = mul2(mul2(mul2(POLY, TT), EX), RINV);
+        f2 G1 = mul2(CA, EX);
+        const f2 B1 = mul2(add2(B0, G1), RINV2);
+        G1 = mul2(G1, A2);
+        const f2 B2 = mul2(fma2(THREE, B1, G1), RINV2);
+        G1 = mul2(G1, A2);
+        const f2 B3 = mul2(fma2(FIVE, B2, G1), RINV2);
+        f2 D1 = ZERO, D2 = ZERO, D3 = ZERO;
+        const bool damp = r2a < damp_r2 || r2b < damp_r2;
+        if (damp) {
+            const f2 U = mul2(mul2(R, ITI), pk2(it.x, it.y));
+            const f2 AM = pk2(fminf(di.w, d.z), fminf(di.w, d.w));
+            const f2 AU3 = mul2(AM, mul2(U, mul2(U, U)));
+            float xa, xb;
+            un2(AU3, xa, xb);
+            float e1a = 0.f, e1b = 0.f, e2a = 0.f, e2b = 0.f, e3a = 0.f, e3b = 0.f;
+            if (xa < 50.0f && r2a < damp_r2) {
+                e1a = __expf(-xa);
+                e2a = (1.0f + xa) * e1a;
+                e3a = (1.0f + xa + 0.6f * xa * xa) * e1a;
+            }
+            if (xb < 50.0f && r2b < damp_r2) {
+                e1b = __expf(-xb);
+                e2b = (1.0f + xb) * e1b;
+                e3b = (1.0f + xb + 0.6f * xb * xb) * e1b;
+            }
+            const f2 BB1 = mul2(RINV, RINV2);
+            const f2 BB2 = mul2(mul2(THREE, BB1), RINV2);
+            const f2 BB3 = mul2(mul2(FIVE, BB2), RINV2);
+            D1 = mul2(pk2(e1a, e1b), BB1);
+            D2 = mul2(pk2(e2a, e2b), BB2);
+            D3 = mul2(pk2(e3a, e3b), BB3);
+        }
+        const f2 QJ = pk2(b.z, b.w);
+        const f2 PJX = pk2(c.x, c.y), PJY = pk2(c.z, c.w), PJZ = pk2(d.x, d.y);
+        const f2 TJX = add2(PJX, pk2(u.x, u.y)), TJY = add2(PJY, pk2(u.z, u.w)), TJZ = add2(PJZ, pk2(v.x, v.y));
+        // E(T,T; Be - Kd) + E(P,P; Kd)
+        f2 E2 = ZERO;
+        pair_ewald2(DX, DY, DZ, QI, TIX, TIY, TIZ, QJ, TJX, TJY, TJZ, B0, sub2(B1, D1), sub2(B2, D2), sub2(B3, D3), E2,
+                    FX, FY, FZ, GX, GY, GZ);
+        if (damp)
+            pair_ewald2(DX, DY, DZ, QI, PIX, PIY, PIZ, QJ, PJX, PJY, PJZ, ZERO, D1, D2, D3, E2, FX, FY, FZ, GX, GY, GZ);
+        EN = fma2(HALF, E2, EN);
+    }
+    float lo, hi;
+    un2(EN, lo, hi);
+    en += lo + hi;
+    un2(FX, lo, hi);
+    f[0] += lo + hi;
+    un2(FY, lo, hi);
+    f[1] += lo + hi;
+    un2(FZ, lo, hi);
+    f[2] += lo + hi;
+    un2(GX, lo, hi);
+    g[0] += lo + hi;
+    un2(GY, lo, hi);
+    g[1] += lo + hi;
+    un2(GZ, lo, hi);
+    g[2] += lo + hi;
+}
+
 template <class R>
 __global__ void __launch_bounds__(kEwThreads) k_ew_force(PairParams P, EwParams E,
                                                          const typename Vec4T<R>::type* __restrict__ posq_s,
@@ -479,6 +832,7 @@ __global__ void __launch_bounds__(kEwThreads) k_ew_force(PairParams P, EwParams 
                                                          double* __restrict__ out, double* __restrict__ tile_energy) {
     typedef typename Vec4T<R>::type V4;
     __shared__ V4 s_pos[kEwWarps][32], s_dip[kEwWarps][32], s_ind[kEwWarps][32];
+    __shared__ EwPackedForceTile s_pk[sizeof(R) == 4 ? kEwWarps : 1];
     __shared__ double s_red[kEwWarps][7][32];
     const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
     // One I tile per CTA; warps split the neighbour list (see k_ew_field).
@@ -495,13 +849,30 @@ __global__ void __launch_bounds__(kEwThreads) k_ew_force(PairParams P, EwParams 
         const int J = ent & kTileMask;
         const bool fold = (ent >> 30) & 1, slow = ((unsigned)ent >> 31) & 1u;
         __syncwarp();
-        s_pos[warp][lane] = posq_s[J * 32 + lane];
-        s_dip[warp][lane] = dipt_s[J * 32 + lane];
-        s_ind[warp][lane] = vec_s[J * 32 + lane];
+        const V4 pj = posq_s[J * 32 + lane], dj = dipt_s[J * 32 + lane], uj = vec_s[J * 32 + lane];
+        s_pos[warp][lane] = pj;
+        s_dip[warp][lane] = dj;
+        s_ind[warp][lane] = uj;
+        if constexpr (sizeof(R) == 4) {
+            if (!slow) stage_packed_force(s_pk[warp], lane, pj, dj, uj);
+        }
         __syncwarp();
         R ox, oy, oz;
         tile_shift<R>(P, cA, tctr[J], pi.x, pi.y, pi.z, ox, oy, oz);
         R f[3] = {0, 0, 0}, g[3] = {0, 0, 0}, e = 0;
+        if constexpr (sizeof(R) == 4) {
+            if (!slow) {
+                const float iti = 1.0f / (float)di.w;
+                if (fold) ew_force_walk_x2<true>(P, E, s_pk[warp], ox, oy, oz, pi.w, di, ui, iti, rc2, damp_r2, e, f, g);
+                else ew_force_walk_x2<false>(P, E, s_pk[warp], ox, oy, oz, pi.w, di, ui, iti, rc2, damp_r2, e, f, g);
+                for (int c = 0; c < 3; c++) {
+                    F[c] += (double)f[c];
+                    G[c] += (double)g[c];
+                }
+                en += (double)e;
+                continue;
+            }
+        }
         if (slow) {
             const unsigned part = partner_bits(exs_j, e0, e1, J * 32);
             if (fold) ew_force_walk<R, true, true>(P, E, s_pos[warp], s_dip[warp], s_ind[warp], i, J * 32, ox, oy, oz, pi.w, di, ui, part, rc2, damp_r2, e, f, g);
@@ -677,6 +1048,31 @@ __global__ void k_pme_fix_to_real(size_t ng, unsigned long long* __restrict__ gf
     long long v = (long long)gfix[k];
     gfix[k] = 0ull;
     out[k] = (G)((double)v * kFixInv);
+}
+
+// FP32 version, four words per thread: v 2^-32 = hi + lo 2^-32 with hi the
+// signed upper and lo the unsigned lower 32 bits (two 32-bit conversions).
+__device__ __forceinline__ float fix_to_float(unsigned long long u) {
+    const int hi = (int)(long long)(u >> 32);
+    const unsigned lo = (unsigned)u;
+    return __fmaf_rn((float)lo, 2.3283064365386963e-10f, (float)hi);
+}
+__global__ void k_pme_fix_to_f32x4(size_t ng, unsigned long long* __restrict__ gfix, float* __restrict__ out) {
+    const size_t q = (size_t)blockIdx.x * blockDim.x + threadIdx.x;
+    const size_t k = 4 * q;
+    if (k + 3 < ng) {
+        ulonglong2* g2 = reinterpret_cast<ulonglong2*>(gfix + k);
+        const ulonglong2 a = g2[0], b = g2[1];
+        g2[0] = make_ulonglong2(0ull, 0ull);
+        g2[1] = make_ulonglong2(0ull, 0ull);
+        *reinterpret_cast<float4*>(out + k) =
+            make_float4(fix_to_float(a.x), fix_to_float(a.y), fix_to_float(b.x), fix_to_float(b.y));
+    } else {
+        for (size_t j = k; j < ng; j++) {
+            out[j] = fix_to_float(gfix[j]);
+            gfix[j] = 0ull;
+        }
+    }
 }
 
 template <class R>
@@ -1106,7 +1502,10 @@ void pme_potential(Ewald* e, const Dev& d, FftGrid& g, bool energy, cudaStream_t
                                                                    fix ? nullptr : (double*)g.real);
     e->launches++;
     if (fix) {
-        k_pme_fix_to_real<GT><<<nblk(ng, 256), 256, 0, st>>>(ng, e->gfix, (GT*)g.real);
+        if (sizeof(GT) == 4)
+            k_pme_fix_to_f32x4<<<nblk((ng + 3) / 4, 256), 256, 0, st>>>(ng, e->gfix, (float*)g.real);
+        else
+            k_pme_fix_to_real<GT><<<nblk(ng, 256), 256, 0, st>>>(ng, e->gfix, (GT*)g.real);
         e->launches++;
     }
     check_cufft(cufftSetStream(g.fwd, st), "cufftSetStream");
