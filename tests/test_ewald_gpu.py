@@ -151,3 +151,15 @@ def test_translation_invariance():
     s2 = s.copy(positions=s.positions + np.array([0.37, -1.21, 2.9]))
     e1 = run(s2, "double", 1e-11)[0]
     assert rel_err(e1, e0) < 1e-4
+
+
+def test_mixed_matches_plain_at_tight_tolerance():
+    # Ewald tolerance 1e-6: alpha * cutoff = 3.6, deeper into the tail of the
+    # FP32 erfc approximation of the mixed real-space kernels.
+    s = water216().copy(ewald_tolerance=1e-6)
+    ep, fp, mup, params, _ = run(s, "double", 1e-11)
+    em, fm, mum, _, _ = run(s, "mixed", 1e-9)
+    assert params[1] > 30  # finer grid than at 1e-4
+    assert rel_err(em, ep) < 1e-6
+    assert rel_rms(fm, fp) < 2e-5
+    assert rel_rms(mum, mup) < 2e-5

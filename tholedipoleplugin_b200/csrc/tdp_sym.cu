@@ -57,6 +57,7 @@ struct TileGeom {
     double dcx, dcy, dcz;
     bool fold;
     bool near;
+    unsigned fmask;   // dimensions in which some pair may need folding (bit k: dimension k)
 };
 
 __device__ __forceinline__ TileGeom tile_geom(const PairParams& P, double4 cA, double4 eA, double4 cB, double4 eB) {
@@ -65,10 +66,14 @@ __device__ __forceinline__ TileGeom tile_geom(const PairParams& P, double4 cA, d
     g.dcy = cB.y - cA.y;
     g.dcz = cB.z - cA.z;
     g.fold = false;
+    g.fmask = 0u;
     if (P.periodic) {
         g.dcx = fold_d(g.dcx, P.box[0], P.inv_box[0]);
         g.dcy = fold_d(g.dcy, P.box[1], P.inv_box[1]);
         g.dcz = fold_d(g.dcz, P.box[2], P.inv_box[2]);
+        g.fmask = (fabs(g.dcx) + eA.x + eB.x >= P.half_box_tol[0] ? 1u : 0u) |
+                  (fabs(g.dcy) + eA.y + eB.y >= P.half_box_tol[1] ? 2u : 0u) |
+                  (fabs(g.dcz) + eA.z + eB.z >= P.half_box_tol[2] ? 4u : 0u);
         g.fold = fabs(g.dcx) + eA.x + eB.x >= P.half_box_tol[0] || fabs(g.dcy) + eA.y + eB.y >= P.half_box_tol[1] ||
                  fabs(g.dcz) + eA.z + eB.z >= P.half_box_tol[2];
     }
@@ -307,7 +312,7 @@ __device__ __forceinline__ void field_walk2_x2(const PairParams& P, const double
                                                const float4* __restrict__ sp, const float4* __restrict__ sv, int lane,
                                                int jbase, int ia, float oax, float oay, float oaz, float qa, float4 va,
                                                int ib, float obx, float oby, float obz, float qb, float4 vb,
-                                               float damp_r2, float* fa, float* fb, float* g) {
+                                               unsigned fm, float damp_r2, float* fa, float* fb, float* g) {
     const int nxt = (lane + 1) & 31;
     const f2 OX = pk2(oax, obx), OY = pk2(oay, oby), OZ = pk2(oaz, obz);
     const f2 VX = pk2(va.x, vb.x), VY = pk2(va.y, vb.y), VZ = pk2(va.z, vb.z);
@@ -334,16 +339,32 @@ __device__ __forceinline__ void field_walk2_x2(const PairParams& P, const double
         const float4 pj = sp[jj], vj = sv[jj];
         f2 DX = sub2(bc2(pj.x), OX), DY = sub2(bc2(pj.y), OY), DZ = sub2(bc2(pj.z), OZ);
         if (FOLD) {
-            DX = fold2(DX, Lx, Ix);
-            DY = fold2(DY, Ly, Iy);
-            DZ = fold2(DZ, Lz, Iz);
+            // Only the dimensions of fm can need folding (elsewhere every pair
+            // of the two tiles lies within half a box minus the margin).
+            bool amb_a = false, amb_b = false;
             float ax, bx, ay, by, az, bz;
-            un2(DX, ax, bx);
-            un2(DY, ay, by);
-            un2(DZ, az, bz);
-            const bool amb_a = fabsf(ax) > tx || fabsf(ay) > ty || fabsf(az) > tz;
-            const bool amb_b = fabsf(bx) > tx || fabsf(by) > ty || fabsf(bz) > tz;
+            if (fm & 1u) {
+                DX = fold2(DX, Lx, Ix);
+                un2(DX, ax, bx);
+                amb_a = fabsf(ax) > tx;
+                amb_b = fabsf(bx) > tx;
+            }
+            if (fm & 2u) {
+                DY = fold2(DY, Ly, Iy);
+                un2(DY, ay, by);
+                amb_a = amb_a || fabsf(ay) > ty;
+                amb_b = amb_b || fabsf(by) > ty;
+            }
+            if (fm & 4u) {
+                DZ = fold2(DZ, Lz, Iz);
+                un2(DZ, az, bz);
+                amb_a = amb_a || fabsf(az) > tz;
+                amb_b = amb_b || fabsf(bz) > tz;
+            }
             if (amb_a || amb_b) {
+                un2(DX, ax, bx);
+                un2(DY, ay, by);
+                un2(DZ, az, bz);
                 // Within 16 ulp of half a box: the reference's FP64 minimum image.
                 const int j = jbase + jj;
                 if (amb_a && ia < P.n && j < P.n) {
@@ -497,7 +518,7 @@ struct ISlot {
     bool act;
     // Against the current J tile.
     bool valid, diag, slow, fold, near;
-    unsigned partners;
+    unsigned partners, fmask;
     R ox, oy, oz;
 };
 
@@ -534,6 +555,7 @@ __device__ __forceinline__ void slot_against(ISlot<R>& a, const PairParams& P, b
     const TileGeom g = tile_geom(P, cA, eA, cB, eB);
     shift_into<R>(g, cA, cB, a.pi.x, a.pi.y, a.pi.z, a.ox, a.oy, a.oz);
     a.fold = g.fold;
+    a.fmask = g.fmask;
     a.near = g.near;
     a.diag = a.I == J;
     a.slow = a.diag || (J == P.n_tiles - 1 && (P.n & 31)) || (J >= a.et.x && J <= a.et.y);
@@ -615,8 +637,8 @@ __global__ void __launch_bounds__(kSymThreads, 4) k_field_sym(
 #define TDP_FWALKX2(F, D)                                                                                          \
     field_walk2_x2<KIND, F, D>(P, pos, (const float4*)sp, (const float4*)sv, lane, jbase, a.i, (float)a.ox,      \
                                (float)a.oy, (float)a.oz, (float)a.pi.w, to_f4(a.vi), b.i, (float)b.ox, (float)b.oy, \
-                               (float)b.oz, (float)b.pi.w, to_f4(b.vi), (float)damp_r2, (float*)fa, (float*)fb,    \
-                               (float*)g)
+                               (float)b.oz, (float)b.pi.w, to_f4(b.vi), a.fmask | b.fmask, (float)damp_r2,          \
+                               (float*)fa, (float*)fb, (float*)g)
                 if (sizeof(R) == 4 && !slow) {
                     if (fold) {
                         if (near) TDP_FWALKX2(true, true);
