@@ -94,7 +94,10 @@ extern "C" {
  * terms.  The fields and induced dipoles are the periodic versions of the
  * reference's (same Thole damping, M and I scales); the energy is the
  * variational one, U_perm - 1/2 mu.E_M, and the forces are its exact negative
- * gradient.  Orthorhombic boxes only; real space, damping corrections
+ * gradient (Mutual polarization only, where the energy is stationary in the
+ * induced dipoles; Direct and Extrapolated give TDP_ERR_UNSUPPORTED; frames
+ * whose torque map is the gradient of their rotation, i.e. not ZOnly).
+ * Orthorhombic boxes only; real space, damping corrections
  * included, stops at the cutoff, where exp(-a u^3) of every pair must be
  * <= 1e-12 (cutoff^3 >= 27.63 t_max^5); tdp_adjoint is unsupported.
  * alpha = pme_alpha and the grid = pme_grid when both are set, otherwise
@@ -102,6 +105,16 @@ extern "C" {
  * n_k = the smallest 2,3,5,7-smooth size >= ceil(2 alpha L_k / (3 tol^(1/5)))
  * (at least 6), fixed at the first evaluation. */
 #define TDP_FLAG_EWALD (1u << 2)
+/* Variational mode of a NoCutoff system (TDP_NO_CUTOFF only; PME systems use
+ * TDP_FLAG_EWALD).  Fields and induced dipoles are exactly the reference's;
+ * the energy is the variational one, U_perm - 1/2 mu.E_M, summed over all pairs
+ * with bare kernels, and the forces are its exact negative gradient (the
+ * reference's own forces follow its quasi-internal-frame convention and are
+ * not the gradient of its energy, ReferenceTholeDipoleForce.cpp:129-366).  Runs
+ * on the Ewald mode's real-space kernels with alpha = 0, no cutoff and no
+ * reciprocal space; the same limits as TDP_FLAG_EWALD (Mutual polarization,
+ * no ZOnly frames, no tdp_adjoint). */
+#define TDP_FLAG_VARIATIONAL (1u << 3)
 
 /* Flags of tdp_compute. */
 #define TDP_COMPUTE_FORCES (1u << 0)

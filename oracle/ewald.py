@@ -147,8 +147,11 @@ def bare_kernels(r):
 
 def erfc_kernels(r, alpha, cutoff):
     """B0..B3 of erfc(alpha r)/r (B_{n+1} = ((2n+1) B_n + (2 alpha^2)^(n+1)/(alpha sqrt(pi)) e^(-alpha^2 r^2)) / r^2),
-    zero beyond the cutoff and on the diagonal."""
+    zero beyond the cutoff and on the diagonal; alpha = 0 gives the bare kernels."""
     inside = (r > 0) & (r < cutoff)
+    if alpha == 0.0:
+        z = np.zeros_like(r)
+        return tuple(np.where(inside, b, z) for b in bare_kernels(r))
     rs = np.where(inside, r, 1.0)
     e = np.exp(-(alpha * rs) ** 2) / (alpha * SQRT_PI)
     r2 = rs * rs
@@ -411,16 +414,34 @@ class EwaldResult:
     grid: Optional[tuple] = None
 
 
+class NoRecip:
+    """No reciprocal space (the variational NoCutoff model: bare pairs, no images)."""
+
+    def __init__(self, n):
+        self.n = n
+
+    def energy_field(self, q, dip):
+        return 0.0, np.zeros((self.n, 3))
+
+    def forces(self, q, dip):
+        return np.zeros((self.n, 3))
+
+
 class Ewald:
-    """Dense FP64 Ewald model of one system at its positions (orthorhombic box sys.box)."""
+    """Dense FP64 Ewald model of one system at its positions (orthorhombic box
+    sys.box).  recip="none" with alpha = 0 is the variational model without
+    periodicity (all pairs, bare kernels): the NoCutoff counterpart."""
 
     def __init__(self, sys, alpha: float, cutoff: Optional[float] = None, recip: str = "direct",
                  kmax: Optional[int] = None, grid=None):
         self.sys = sys
         self.alpha = float(alpha)
-        self.cutoff = float(sys.cutoff if cutoff is None else cutoff)
-        self.box = np.asarray(sys.box, dtype=np.float64)
-        if np.any(self.box < 2.0 * self.cutoff * 0.999999):
+        vacuum = recip == "none"
+        self.cutoff = float("inf") if vacuum else float(sys.cutoff if cutoff is None else cutoff)
+        self.box = np.zeros(3) if vacuum else np.asarray(sys.box, dtype=np.float64)
+        if vacuum and self.alpha != 0.0:
+            raise ValueError("recip='none' needs alpha = 0")
+        if not vacuum and np.any(self.box < 2.0 * self.cutoff * 0.999999):
             raise ValueError("box smaller than twice the cutoff")
         self.pos = np.asarray(sys.positions, dtype=np.float64).reshape(-1, 3)
         self.q = np.asarray(sys.charges, dtype=np.float64)
@@ -429,7 +450,10 @@ class Ewald:
         self.n = n
         self.lab = O.lab_dipoles(sys)
         self.M, self.S = scale_matrices(sys)
-        self.d = _displacements(self.pos, self.box)
+        if vacuum:
+            self.d = self.pos[None, :, :] - self.pos[:, None, :]
+        else:
+            self.d = _displacements(self.pos, self.box)
         r = np.sqrt((self.d ** 2).sum(-1))
         np.fill_diagonal(r, 0.0)
         self.r = r
@@ -448,6 +472,8 @@ class Ewald:
             if grid is None:
                 grid = pme_parameters(self.cutoff, sys.ewald_tolerance, self.box)[1]
             self.rec = PmeRecip(self.pos, self.box, self.alpha, grid)
+        elif recip == "none":
+            self.rec = NoRecip(n)
         else:
             raise ValueError(recip)
         self.grid = grid
@@ -534,7 +560,7 @@ class Ewald:
         V = float(np.prod(self.box))
         e_self = -self.alpha / SQRT_PI * float((q * q).sum()) - 2.0 * self.alpha ** 3 / (3.0 * SQRT_PI) * float(
             (tot * tot).sum())
-        e_plasma = -math.pi * Q * Q / (2.0 * V * self.alpha ** 2)
+        e_plasma = -math.pi * Q * Q / (2.0 * V * self.alpha ** 2) if self.alpha > 0.0 else 0.0
         pos_mask = self.pol > 0
         e_ind = 0.5 * float((mu[pos_mask] ** 2 / self.pol[pos_mask, None]).sum())
         energy = e_real + e_rec + e_self + e_plasma + e_ind
@@ -550,6 +576,11 @@ class Ewald:
 def map_torque(sys, torque) -> np.ndarray:
     """Forces from per-atom torques through the reference's torque map (C oracle)."""
     return O.map_torque(sys, torque)
+
+
+def variational_nocutoff(sys) -> EwaldResult:
+    """The variational NoCutoff model (TDP_FLAG_VARIATIONAL): all pairs, bare kernels."""
+    return Ewald(sys, 0.0, recip="none").evaluate()
 
 
 def ewald(sys, alpha: Optional[float] = None, recip: str = "pme", **kw) -> EwaldResult:

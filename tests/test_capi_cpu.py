@@ -141,3 +141,13 @@ def test_ewald_mode_validation(lib):
     assert rc == -1 and "Thole damping at the cutoff" in lib.tdp_last_error(None).decode()
     rc, _, _ = _create(s, flags=A.FLAG_EWALD, ewald_error_tolerance=0.7)
     assert rc == -1 and "tolerance" in lib.tdp_last_error(None).decode()
+
+
+def test_gradient_modes_validation(lib):
+    s = S.config_small()
+    rc, _, _ = _create(s.copy(polarization=S.DIRECT), flags=A.FLAG_EWALD)
+    assert rc == -8 and "Mutual polarization" in lib.tdp_last_error(None).decode()
+    rc, _, _ = _create(s, flags=A.FLAG_VARIATIONAL)
+    assert rc == -1 and "NoCutoff mode" in lib.tdp_last_error(None).decode()
+    rc, _, _ = _create(s.copy(method=S.NO_CUTOFF), flags=A.FLAG_VARIATIONAL | A.FLAG_EWALD)
+    assert rc == -1 and "exclude each other" in lib.tdp_last_error(None).decode()

@@ -72,21 +72,23 @@ def test_water216_matches_oracle(precision, eps, e_tol, f_tol, mu_tol):
 
 
 @pytest.mark.parametrize("precision,tol", [("double", 1e-8), ("mixed", 2e-5)])
-def test_direct_polarization_field(precision, tol):
-    # Direct polarization: mu = alpha E_M, so the induced dipoles expose the
-    # permanent field (real space + PME + self) atom by atom.
+def test_permanent_field(precision, tol):
+    # A Mutual solve capped at zero iterations returns its starting point
+    # mu = alpha E_M, which exposes the permanent field (real space + PME +
+    # self) atom by atom.
     ew, _, _, _ = oracle_pme("w216", water216)
-    s = water216().copy(polarization=S.DIRECT)
+    s = water216().copy(max_iter=0)
     with CudaCalcTholeDipoleForceKernel(s, precision=precision, ewald=True) as k:
         mu = k.getInducedDipoles(s.positions)
     E = ew.fixed_field()
     assert rel_rms(mu, E * s.polarizabilities[:, None]) < tol
-    # Energy and forces of the Direct model against the oracle at mu = alpha E.
-    ref = ew.evaluate(E * s.polarizabilities[:, None], E)
-    with CudaCalcTholeDipoleForceKernel(s, precision=precision, ewald=True) as k:
-        e, f = k.execute(s.positions)
-    assert rel_err(e, ref.energy) < (1e-9 if precision == "double" else 1e-6)
-    assert rel_rms(f, ref.forces) < (1e-8 if precision == "double" else 2e-5)
+
+
+def test_direct_and_extrapolated_rejected():
+    from tholedipoleplugin_b200._capi import TdpError
+    for pol in (S.DIRECT, S.EXTRAPOLATED):
+        with pytest.raises(TdpError, match="Mutual polarization"):
+            CudaCalcTholeDipoleForceKernel(water216().copy(polarization=pol), ewald=True)
 
 
 def test_forces_are_gradient_of_gpu_energy():

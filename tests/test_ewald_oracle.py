@@ -156,3 +156,24 @@ def test_pme_restatement_converges_to_direct_sum():
     e2 = rel(fine.fixed_field(), E_d)
     # Order-5 B-splines: the grid error falls by ~2^5 when the spacing halves.
     assert e1 < 1e-4 and e2 < e1 / 16.0
+
+
+def test_variational_nocutoff_oracle():
+    # recip="none", alpha = 0: the fields and induced dipoles are exactly the
+    # reference's NoCutoff ones, and the forces are the energy's gradient.
+    from tests.fixtures import reference_test_systems
+    backend = "reference" if O.reference_available() else "port"
+    s = dict(reference_test_systems())["ammonia_mutual"].copy(target_eps=1e-13, max_iter=5000)
+    r = EW.variational_nocutoff(s)
+    assert rel(r.fixed_field, O.fixed_field(s, backend)) < 1e-13
+    assert rel(r.induced, O.induced_dipoles(s, backend)[0]) < 1e-9
+    h = 1e-6
+    scale = np.abs(r.forces).max()
+    for i in range(s.n):
+        for c in range(3):
+            e = []
+            for sg in (1.0, -1.0):
+                s2 = s.copy()
+                s2.positions[i, c] += sg * h
+                e.append(EW.variational_nocutoff(s2).energy)
+            assert abs(-(e[0] - e[1]) / (2 * h) - r.forces[i, c]) < 1e-8 * scale

@@ -24,6 +24,7 @@ SOLVER_CG, SOLVER_JACOBI = 0, 1
 FLAG_DD_FORCE_R4 = 1 << 0
 FLAG_WARM_START = 1 << 1
 FLAG_EWALD = 1 << 2
+FLAG_VARIATIONAL = 1 << 3
 COMPUTE_FORCES, COMPUTE_ENERGY, COMPUTE_REQUIRE_CONVERGENCE = 1, 2, 4
 F64, F32 = 0, 1
 DIPOLES_INDUCED, DIPOLES_LAB_PERMANENT, DIPOLES_TOTAL = 0, 1, 2

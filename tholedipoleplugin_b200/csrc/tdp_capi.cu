@@ -799,6 +799,23 @@ int tdp_create(const tdp_system_desc* desc, tdp_handle** out) {
         d.pp.n_bands = (nt + band - 1) / band;
         d.nsplit = d.pp.n_bands;
         d.n_eblk = d.pp.n_bands * (d.pp.n_bands + 1) / 2;
+        const bool variational = (h->flags & TDP_FLAG_VARIATIONAL) != 0;
+        // Both gradient modes rest on the energy being stationary in the induced
+        // dipoles, which holds for Mutual polarization.
+        if ((h->flags & (TDP_FLAG_VARIATIONAL | TDP_FLAG_EWALD)) && h->polarization != TDP_MUTUAL)
+            throw TdpError{TDP_ERR_UNSUPPORTED,
+                           "TDP_FLAG_EWALD and TDP_FLAG_VARIATIONAL need Mutual polarization (their forces are the "
+                           "gradient of an energy that is stationary in the induced dipoles)"};
+        if (variational) {
+            if (h->method != TDP_NO_CUTOFF)
+                throw TdpError{TDP_ERR_INVALID_ARGUMENT,
+                               "TDP_FLAG_VARIATIONAL is the NoCutoff mode; PME systems use TDP_FLAG_EWALD"};
+            if (h->flags & TDP_FLAG_EWALD)
+                throw TdpError{TDP_ERR_INVALID_ARGUMENT, "TDP_FLAG_VARIATIONAL and TDP_FLAG_EWALD exclude each other"};
+            // Real space only: one partial slot.
+            d.nsplit = 1;
+            d.n_eblk = 1;
+        }
         const bool ewald = (h->flags & TDP_FLAG_EWALD) != 0;
         if (ewald) {
             if (h->method != TDP_PME)
@@ -822,7 +839,7 @@ int tdp_create(const tdp_system_desc* desc, tdp_handle** out) {
             // Real space in partial slot 0, reciprocal space + self in slot 1.
             d.nsplit = 2;
             d.n_eblk = 1;
-        } else if (h->precision == TDP_PRECISION_MIXED) {
+        } else if (h->precision == TDP_PRECISION_MIXED && !variational) {
             // Mixed all-pairs form: the band sums go into the fixed-point
             // accumulator and one flushed slot.  Each atom's word receives at
             // most 2 n_bands adds of magnitude < 2^23, so with 2^bits units
@@ -932,7 +949,7 @@ int tdp_create(const tdp_system_desc* desc, tdp_handle** out) {
         d.exs_tiles = dalloc<int2>(d.n_pad / kTile, o);
         upload(d.coef, h->extrap.data(), sizeof(double) * h->extrap.size());
         upload_params(h);
-        if (ewald) h->ew = ewald_create(d, h->precision);
+        if (ewald || variational) h->ew = ewald_create(d, h->precision, variational);
         TDP_CUDA(cudaMallocHost(&h->h_scal, 64 * sizeof(double)));
         TDP_CUDA(cudaMallocHost(&h->h_fixerr, sizeof(int)));
         *h->h_fixerr = 0;

@@ -1240,8 +1240,8 @@ __global__ void k_ew_finish(int n, int n_pad, const int* __restrict__ rank, cons
                             const typename Vec4T<R>::type* __restrict__ posq_s,
                             const typename Vec4T<R>::type* __restrict__ dipt_s,
                             const typename Vec4T<R>::type* __restrict__ vec_s, const double* __restrict__ lab,
-                            const double* __restrict__ pol, double alpha, double selfc, double* __restrict__ fpair,
-                            double* __restrict__ torque, double* __restrict__ epart) {
+                            const double* __restrict__ pol, double alpha, double selfc, int recip,
+                            double* __restrict__ fpair, double* __restrict__ torque, double* __restrict__ epart) {
     __shared__ double red[40];
     const int i = blockIdx.x * blockDim.x + threadIdx.x;
     double e = 0.0;
@@ -1250,8 +1250,12 @@ __global__ void k_ew_finish(int n, int n_pad, const int* __restrict__ rank, cons
         const size_t s1 = 6 * (size_t)n_pad;
         double F[3], G[3];
         for (int c = 0; c < 3; c++) {
-            F[c] = partial[(size_t)c * n_pad + k] + partial[s1 + (size_t)c * n_pad + k];
-            G[c] = partial[(size_t)(3 + c) * n_pad + k] + partial[s1 + (size_t)(3 + c) * n_pad + k];
+            F[c] = partial[(size_t)c * n_pad + k];
+            G[c] = partial[(size_t)(3 + c) * n_pad + k];
+            if (recip) {
+                F[c] += partial[s1 + (size_t)c * n_pad + k];
+                G[c] += partial[s1 + (size_t)(3 + c) * n_pad + k];
+            }
         }
         const typename Vec4T<R>::type P = dipt_s[k], U = vec_s[k];
         const d3 u = {(double)U.x, (double)U.y, (double)U.z};
@@ -1333,6 +1337,7 @@ struct FftGrid {
 
 struct Ewald {
     int precision = TDP_PRECISION_MIXED;
+    bool vacuum = false;   // variational NoCutoff model: real space only, alpha = 0
     std::vector<void*> owned;
     int cap = 0;
     int* list = nullptr;
@@ -1400,12 +1405,13 @@ void influence(Ewald* e, FftGrid& g, cudaStream_t st) {
 
 }  // namespace
 
-Ewald* ewald_create(const Dev& d, int precision) {
+Ewald* ewald_create(const Dev& d, int precision, bool vacuum) {
     Ewald* e = new Ewald();
     try {
         e->precision = precision;
+        e->vacuum = vacuum;
         const int nt = std::max(1, d.pp.n_tiles);
-        e->cap = std::min(nt, 2048);
+        e->cap = vacuum ? nt : std::min(nt, 2048);
         e->list = dalloc<int>((size_t)nt * e->cap, e->owned);
         e->count = dalloc<int>(nt, e->owned);
         e->overflow = dalloc<int>(1, e->owned);
@@ -1425,6 +1431,18 @@ void ewald_destroy(Ewald* e) { delete e; }
 
 void ewald_prepare(Ewald* e, const Dev& d, const double box[3], double cutoff, double tol, double alpha_in,
                    const int grid_in[3], cudaStream_t st) {
+    if (e->vacuum) {
+        e->planned = true;
+        e->alpha = 0.0;
+        e->E.alpha = 0.0;
+        e->E.ca = 0.0;
+        e->E.a2 = 0.0;
+        e->E.rc2 = INFINITY;
+        e->E.selfc = 0.0;
+        e->E.cap = e->cap;
+        e->n_rec_blk = 0;
+        return;
+    }
     for (int k = 0; k < 3; k++)
         if (!(box[k] > 0.0)) throw TdpError{TDP_ERR_INVALID_ARGUMENT, "the Ewald mode needs a periodic box"};
     if (!e->planned) {
@@ -1547,6 +1565,8 @@ void ewald_fixed_field(Ewald* e, const Dev& d, cudaStream_t st) {
     TDP_CUDA(cudaMemcpyAsync(e->h_overflow, e->overflow, sizeof(int), cudaMemcpyDeviceToHost, st));
     e->launches++;
     real_field<R, 0>(e, d, d.dipt_s, st);
+    TDP_CUDA(cudaGetLastError());
+    if (e->vacuum) return;
     pme_potential<R, R, 0>(e, d, e->it, false, st);
     k_pme_gather<R, R, 0, false><<<nblk((size_t)d.n_pad, 128), 128, 0, st>>>(
         e->G, d.n, d.n_pad, e->E.selfc, d.pos_s, (const V4*)d.posq_s, (const V4*)d.dipt_s, (const V4*)d.vec_s,
@@ -1560,6 +1580,8 @@ void ewald_matvec(Ewald* e, const Dev& d, cudaStream_t st) {
     typedef typename Vec4T<R>::type V4;
     e->launches = 0;
     real_field<R, 1>(e, d, d.vec_s, st);
+    TDP_CUDA(cudaGetLastError());
+    if (e->vacuum) return;
     pme_potential<R, R, 1>(e, d, e->it, false, st);
     k_pme_gather<R, R, 1, false><<<nblk((size_t)d.n_pad, 128), 128, 0, st>>>(
         e->G, d.n, d.n_pad, e->E.selfc, d.pos_s, (const V4*)d.posq_s, (const V4*)d.dipt_s, (const V4*)d.vec_s,
@@ -1577,16 +1599,20 @@ void ewald_energy(Ewald* e, const Dev& d, double total_charge, cudaStream_t st) 
     k_ew_force<R><<<blocks, kEwThreads, 0, st>>>(d.pp, e->E, (const V4*)d.posq_s, (const V4*)d.dipt_s,
                                                  (const V4*)d.vec_s, d.tctr_s, d.pos_s, d.exs_off, d.exs_j, d.exs_m,
                                                  d.exs_s, e->list, e->count, d.n_pad, d.partial, e->tile_energy);
-    FftGrid& g = e->energy_grid();
-    pme_potential<R, double, 2>(e, d, g, true, st);
-    k_pme_gather<R, double, 2, true><<<nblk((size_t)d.n_pad, 128), 128, 0, st>>>(
-        e->G, d.n, d.n_pad, e->E.selfc, d.pos_s, (const V4*)d.posq_s, (const V4*)d.dipt_s, (const V4*)d.vec_s,
-        (const double*)g.real, d.partial + 6 * (size_t)d.n_pad);
+    if (!e->vacuum) {
+        FftGrid& g = e->energy_grid();
+        pme_potential<R, double, 2>(e, d, g, true, st);
+        k_pme_gather<R, double, 2, true><<<nblk((size_t)d.n_pad, 128), 128, 0, st>>>(
+            e->G, d.n, d.n_pad, e->E.selfc, d.pos_s, (const V4*)d.posq_s, (const V4*)d.dipt_s, (const V4*)d.vec_s,
+            (const double*)g.real, d.partial + 6 * (size_t)d.n_pad);
+    }
     k_ew_finish<R><<<e->n_atom_blk, kVecThreads, 0, st>>>(d.n, d.n_pad, d.rank, d.partial, (const V4*)d.posq_s,
                                                           (const V4*)d.dipt_s, (const V4*)d.vec_s, d.lab, d.alpha,
-                                                          e->alpha, e->E.selfc, d.fpair, d.torque, e->atom_epart);
+                                                          e->alpha, e->E.selfc, e->vacuum ? 0 : 1, d.fpair, d.torque,
+                                                          e->atom_epart);
     const double V = e->box[0] * e->box[1] * e->box[2];
-    const double plasma = -kPi * total_charge * total_charge / (2.0 * V * e->alpha * e->alpha);
+    const double plasma =
+        e->vacuum ? 0.0 : -kPi * total_charge * total_charge / (2.0 * V * e->alpha * e->alpha);
     k_ew_energy_sum<<<1, kVecThreads, 0, st>>>(d.pp.n_tiles, e->tile_energy, e->n_rec_blk, e->rec_epart,
                                                e->n_atom_blk, e->atom_epart, plasma, d.energy);
     e->launches += 6;

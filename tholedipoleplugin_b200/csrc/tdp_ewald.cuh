@@ -14,7 +14,9 @@ struct Ewald;
 
 // State that does not depend on the box (neighbour list, buffers of the
 // atom-side kernels); the grid is planned by ewald_prepare.
-Ewald* ewald_create(const Dev& d, int precision);
+// vacuum: the variational NoCutoff model (alpha = 0, no cutoff, every tile
+// pair in the list, no reciprocal space).
+Ewald* ewald_create(const Dev& d, int precision, bool vacuum = false);
 void ewald_destroy(Ewald* e);
 
 // Chooses alpha and the grid on the first call (alpha_in > 0 and grid_in[0] > 0

@@ -92,15 +92,17 @@ class CudaCalcTholeDipoleForceKernel:
     Name = "CalcTholeDipoleForce"
 
     def __init__(self, system: TholeSystem, precision="mixed", solver="cg", dd_force_r4: bool = False,
-                 warm_start: bool = False, ewald: bool = False):
+                 warm_start: bool = False, ewald: bool = False, variational: bool = False):
         """``ewald=True`` (PME systems only) runs the library's Ewald mode
         (TDP_FLAG_EWALD: neighbour-list real space + smooth PME) instead of the
-        reference's minimum-image all-pairs sum."""
+        reference's minimum-image all-pairs sum; ``variational=True`` (NoCutoff
+        systems only, TDP_FLAG_VARIATIONAL) gives the variational energy and its
+        exact gradient over all pairs."""
         self._lib = A.lib()
         self.n = system.n
         self.method = int(system.method)
         flags = ((A.FLAG_DD_FORCE_R4 if dd_force_r4 else 0) | (A.FLAG_WARM_START if warm_start else 0)
-                 | (A.FLAG_EWALD if ewald else 0))
+                 | (A.FLAG_EWALD if ewald else 0) | (A.FLAG_VARIATIONAL if variational else 0))
         self._buf = _DescBuffers(system, _precision(precision), _solver(solver), flags)
         h = C.c_void_p()
         A.check(self._lib.tdp_create(C.byref(self._buf.desc), C.byref(h)), None)
