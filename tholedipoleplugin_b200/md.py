@@ -38,46 +38,74 @@ def maxwell_boltzmann(n_waters: int, temperature: float, seed: int) -> np.ndarra
     return v - vcom
 
 
+# Constraints of a rigid water (atoms O, H1, H2): k = 0 (O,H1), 1 (O,H2), 2 (H1,H2).
+_PAIRS = ((0, 1), (0, 2), (1, 2))
+_D = np.array([D_OH, D_OH, D_HH])
+_INV_M = np.array([1.0 / MASS_O, 1.0 / MASS_H, 1.0 / MASS_H])
+
+
+def _coupling() -> np.ndarray:
+    """K[k, l]: how a multiplier of constraint l moves the bond vector of constraint k
+    (x_a += g_l c_{a,l} r_l / m_a with c = +1 for the first atom of l, -1 for the second)."""
+    c = np.zeros((3, 3))
+    for l, (a, b) in enumerate(_PAIRS):
+        c[a, l] = 1.0
+        c[b, l] = -1.0
+    K = np.zeros((3, 3))
+    for k, (a, b) in enumerate(_PAIRS):
+        K[k] = c[a] * _INV_M[a] - c[b] * _INV_M[b]
+    return K
+
+
+_K = _coupling()
+
+
+def _bonds(xw: np.ndarray) -> np.ndarray:
+    """(nw, 3 constraints, 3) bond vectors x_a - x_b."""
+    return np.stack([xw[:, a] - xw[:, b] for a, b in _PAIRS], axis=1)
+
+
+def _apply(xw: np.ndarray, g: np.ndarray, r: np.ndarray, scale: float = 1.0) -> None:
+    """x_a += scale g_l c_{a,l} r_l / m_a for the three constraints of every water."""
+    for l, (a, b) in enumerate(_PAIRS):
+        d = (scale * g[:, l])[:, None] * r[:, l]
+        xw[:, a] += _INV_M[a] * d
+        xw[:, b] -= _INV_M[b] * d
+
+
 def _rattle_host(x: np.ndarray, v: np.ndarray, iters: int = 200, tol: float = 1e-12) -> None:
-    """Project water velocities onto the rigid constraints (numpy, in place)."""
+    """Project water velocities onto the rigid constraints (numpy, in place): the
+    three conditions s_k.(v_a - v_b) = 0 are linear in the multipliers, one 3x3
+    solve per water."""
     xw = x.reshape(-1, 3, 3)
     vw = v.reshape(-1, 3, 3)
-    inv = np.array([1.0 / MASS_O, 1.0 / MASS_H, 1.0 / MASS_H])
-    pairs = ((0, 1, D_OH), (0, 2, D_OH), (1, 2, D_HH))
-    for _ in range(iters):
-        worst = 0.0
-        for a, b, d in pairs:
-            r = xw[:, a] - xw[:, b]
-            dv = vw[:, a] - vw[:, b]
-            rv = np.einsum("ij,ij->i", r, dv)
-            k = rv / (d * d * (inv[a] + inv[b]))
-            vw[:, a] -= (k * inv[a])[:, None] * r
-            vw[:, b] += (k * inv[b])[:, None] * r
-            worst = max(worst, float(np.max(np.abs(rv))) / d if rv.size else 0.0)
-        if worst < tol:
-            break
+    s = _bonds(xw)
+    w = _bonds(vw)
+    A = _K[None, :, :] * np.einsum("nkc,nlc->nkl", s, s)
+    rhs = -np.einsum("nkc,nkc->nk", s, w)
+    h = np.linalg.solve(A, rhs[..., None])[..., 0]
+    _apply(vw, h, s)
 
 
-def _shake_host(x0: np.ndarray, x: np.ndarray, v: np.ndarray, dt: float, iters: int = 200, tol: float = 1e-12):
+def _shake_host(x0: np.ndarray, x: np.ndarray, v: np.ndarray, dt: float, iters: int = 50, tol: float = 1e-12):
+    """Positions onto the rigid constraints (SHAKE with the old bond vectors r0),
+    solving each water's three constraints together by Newton's method, with the
+    matching velocity correction (numpy, in place)."""
     x0w = x0.reshape(-1, 3, 3)
     xw = x.reshape(-1, 3, 3)
     vw = v.reshape(-1, 3, 3)
-    inv = np.array([1.0 / MASS_O, 1.0 / MASS_H, 1.0 / MASS_H])
-    pairs = ((0, 1, D_OH), (0, 2, D_OH), (1, 2, D_HH))
+    r0 = _bonds(x0w)
+    s_free = _bonds(xw)
+    g = np.zeros((xw.shape[0], 3))
     for _ in range(iters):
-        worst = 0.0
-        for a, b, d in pairs:
-            s = xw[:, a] - xw[:, b]
-            r0 = x0w[:, a] - x0w[:, b]
-            diff = d * d - np.einsum("ij,ij->i", s, s)
-            g = diff / (2.0 * np.einsum("ij,ij->i", s, r0) * (inv[a] + inv[b]))
-            xw[:, a] += (g * inv[a])[:, None] * r0
-            xw[:, b] -= (g * inv[b])[:, None] * r0
-            vw[:, a] += (g * inv[a] / dt)[:, None] * r0
-            vw[:, b] -= (g * inv[b] / dt)[:, None] * r0
-            worst = max(worst, float(np.max(np.abs(diff))) / (d * d) if diff.size else 0.0)
-        if worst < tol:
+        s = s_free + np.einsum("kl,nl,nlc->nkc", _K, g, r0)
+        sig = np.einsum("nkc,nkc->nk", s, s) - _D[None, :] ** 2
+        if not sig.size or float(np.max(np.abs(sig) / _D[None, :] ** 2)) < tol:
             break
+        J = 2.0 * _K[None, :, :] * np.einsum("nkc,nlc->nkl", s, r0)
+        g -= np.linalg.solve(J, sig[..., None])[..., 0]
+    _apply(xw, g, r0)
+    _apply(vw, g, r0, 1.0 / dt)
 
 
 class DeviceRigidWaterMD:
