@@ -813,6 +813,310 @@ __device__ __forceinline__ void energy_walk(const PairParams& P, const double* _
     }
 }
 
+// ---------------------------------------------------------------------------
+// Packed FP32 energy walk (mixed form, non-SLOW tile pairs): the lane's I
+// atom against J atoms m and m + 16 of the tile at once (m = (lane + s) & 15,
+// s = 0..15), the pair routine of pair_energy_sides<R, 3> in f32x2 halves.
+// The J-side sums ride packed (lo: atom m, hi: atom m + 16) and rotate one
+// lane per step; after 16 steps lanes l and l ^ 16 hold the two copies of the
+// sums of atoms l & 15 and (l & 15) + 16, added by one xor-16 shuffle.
+// ---------------------------------------------------------------------------
+struct EPackedTile {
+    float4 p0[16], p1[16];   // (x, x', y, y'), (z, z', q, q')   (' = atom m + 16)
+    float4 d0[16], d1[16];   // (mx, mx', my, my'), (mz, mz', t, t')
+    float4 u0[16], u1[16];   // (ux, ux', uy, uy'), (uz, uz', 1/t, 1/t')
+};
+
+__device__ __forceinline__ void stage_epacked(EPackedTile& T, int lane, float4 p, float4 d, float4 u) {
+    const int m = lane & 15, h = lane >> 4;
+    float* p0 = reinterpret_cast<float*>(&T.p0[m]);
+    float* p1 = reinterpret_cast<float*>(&T.p1[m]);
+    float* d0 = reinterpret_cast<float*>(&T.d0[m]);
+    float* d1 = reinterpret_cast<float*>(&T.d1[m]);
+    float* u0 = reinterpret_cast<float*>(&T.u0[m]);
+    float* u1 = reinterpret_cast<float*>(&T.u1[m]);
+    p0[h] = p.x;
+    p0[2 + h] = p.y;
+    p1[h] = p.z;
+    p1[2 + h] = p.w;
+    d0[h] = d.x;
+    d0[2 + h] = d.y;
+    d1[h] = d.z;
+    d1[2 + h] = d.w;
+    u0[h] = u.x;
+    u0[2 + h] = u.y;
+    u1[h] = u.z;
+    u1[2 + h] = 1.0f / d.w;
+}
+
+__device__ __forceinline__ f2 neg2(f2 a) { return mul2(a, bc2(-1.0f)); }
+__device__ __forceinline__ f2 dot2(f2 ax, f2 ay, f2 az, f2 bx, f2 by, f2 bz) {
+    return fma2(ax, bx, fma2(ay, by, mul2(az, bz)));
+}
+
+template <bool FOLD>
+__device__ __forceinline__ void energy_walk_x2(const PairParams& P, const double* __restrict__ pos,
+                                               const double2* __restrict__ yz, const EPackedTile& T, int lane,
+                                               int i, int jbase, float oix, float oiy, float oiz, float4 pi,
+                                               float4 di, float4 ui, unsigned fm, float damp_r2, float rv4p,
+                                               float rv4f, bool mutual, float f[6], float gg[6], float& en) {
+    const int nxt = (lane + 1) & 31;
+    const int nmax = P.n_tiles * 32 - 1;
+    const f2 OX = bc2(oix), OY = bc2(oiy), OZ = bc2(oiz);
+    const f2 QI0 = bc2(pi.w), MIX = bc2(di.x), MIY = bc2(di.y), MIZ = bc2(di.z);
+    const f2 UIX = bc2(ui.x), UIY = bc2(ui.y), UIZ = bc2(ui.z);
+    const float ti = di.w, iti = 1.0f / di.w;
+    const f2 ITI = bc2(iti), ONE = bc2(1.0f), HALF = bc2(0.5f);
+    const f2 RV4P = bc2(rv4p), RV4F = bc2(rv4f);
+    f2 Lx = 0, Ly = 0, Lz = 0, Ix = 0, Iy = 0, Iz = 0;
+    float tx = 0.f, ty = 0.f, tz = 0.f;
+    if (FOLD) {
+        Lx = bc2(-(float)P.box[0]);
+        Ly = bc2(-(float)P.box[1]);
+        Lz = bc2(-(float)P.box[2]);
+        Ix = bc2((float)P.inv_box[0]);
+        Iy = bc2((float)P.inv_box[1]);
+        Iz = bc2((float)P.inv_box[2]);
+        tx = (float)P.half_box_tol[0];
+        ty = (float)P.half_box_tol[1];
+        tz = (float)P.half_box_tol[2];
+    }
+    f2 FX = 0, FY = 0, FZ = 0, TX = 0, TY = 0, TZ = 0, EN = 0;        // I side
+    f2 GX = 0, GY = 0, GZ = 0, UX = 0, UY = 0, UZ = 0;                // J side (packed atoms m, m + 16)
+#pragma unroll 1
+    for (int s = 0; s < 16; s++) {
+        const int m = (lane + s) & 15;
+        const float4 a = T.p0[m], b = T.p1[m], c = T.d0[m], d = T.d1[m], e = T.u0[m], h = T.u1[m];
+        f2 DX = sub2(pk2(a.x, a.y), OX), DY = sub2(pk2(a.z, a.w), OY), DZ = sub2(pk2(b.x, b.y), OZ);
+        const int ja = jbase + m, jb = ja + 16;
+        if (FOLD) {
+            bool amb_a = false, amb_b = false;
+            float ax, bx, ay, by, az, bz;
+            if (fm & 1u) {
+                DX = fold2(DX, Lx, Ix);
+                un2(DX, ax, bx);
+                amb_a = fabsf(ax) > tx;
+                amb_b = fabsf(bx) > tx;
+            }
+            if (fm & 2u) {
+                DY = fold2(DY, Ly, Iy);
+                un2(DY, ay, by);
+                amb_a = amb_a || fabsf(ay) > ty;
+                amb_b = amb_b || fabsf(by) > ty;
+            }
+            if (fm & 4u) {
+                DZ = fold2(DZ, Lz, Iz);
+                un2(DZ, az, bz);
+                amb_a = amb_a || fabsf(az) > tz;
+                amb_b = amb_b || fabsf(bz) > tz;
+            }
+            if (amb_a || amb_b) {
+                un2(DX, ax, bx);
+                un2(DY, ay, by);
+                un2(DZ, az, bz);
+                if (amb_a) {
+                    d3 q = exact_delta(P, pos, i, ja);
+                    ax = (float)q.x;
+                    ay = (float)q.y;
+                    az = (float)q.z;
+                }
+                if (amb_b) {
+                    d3 q = exact_delta(P, pos, i, jb);
+                    bx = (float)q.x;
+                    by = (float)q.y;
+                    bz = (float)q.z;
+                }
+                DX = pk2(ax, bx);
+                DY = pk2(ay, by);
+                DZ = pk2(az, bz);
+            }
+        }
+        const f2 R2 = dot2(DX, DY, DZ, DX, DY, DZ);
+        float r2a, r2b, dya, dyb, dza, dzb;
+        un2(R2, r2a, r2b);
+        un2(DY, dya, dyb);
+        un2(DZ, dza, dzb);
+        const bool yza = yz_differ<float>(dya, dza, yz, i, ja, nmax);
+        const bool yzb = yz_differ<float>(dyb, dzb, yz, i, jb, nmax);
+        const f2 RINV = pk2(rsqrtf(r2a), rsqrtf(r2b));
+        // QI frame: Z along d; X from Z + x^ or y^ (the reference's yz test), Gram-Schmidt; Y = Z x X.
+        const f2 ZX = mul2(DX, RINV), ZY = mul2(DY, RINV), ZZ = mul2(DZ, RINV);
+        f2 XX = add2(ZX, pk2(yza ? 1.0f : 0.0f, yzb ? 1.0f : 0.0f));
+        f2 XY = add2(ZY, pk2(yza ? 0.0f : 1.0f, yzb ? 0.0f : 1.0f));
+        f2 XZ = ZZ;
+        const f2 NDT = neg2(dot2(ZX, ZY, ZZ, XX, XY, XZ));
+        XX = fma2(ZX, NDT, XX);
+        XY = fma2(ZY, NDT, XY);
+        XZ = fma2(ZZ, NDT, XZ);
+        float xna, xnb;
+        un2(dot2(XX, XY, XZ, XX, XY, XZ), xna, xnb);
+        const f2 SN = pk2(xna > 0.0f ? rsqrtf(xna) : 1.0f, xnb > 0.0f ? rsqrtf(xnb) : 1.0f);
+        XX = mul2(XX, SN);
+        XY = mul2(XY, SN);
+        XZ = mul2(XZ, SN);
+        const f2 YX = fma2(ZY, XZ, neg2(mul2(ZZ, XY)));
+        const f2 YY = fma2(ZZ, XX, neg2(mul2(ZX, XZ)));
+        const f2 YZ = fma2(ZX, XY, neg2(mul2(ZY, XX)));
+        // Rotated multipoles.
+        const f2 UJX = pk2(e.x, e.y), UJY = pk2(e.z, e.w), UJZ = pk2(h.x, h.y);
+        const f2 MJX = pk2(c.x, c.y), MJY = pk2(c.z, c.w), MJZ = pk2(d.x, d.y);
+        const f2 uI0 = dot2(XX, XY, XZ, UIX, UIY, UIZ), uI1 = dot2(YX, YY, YZ, UIX, UIY, UIZ),
+                 uI2 = dot2(ZX, ZY, ZZ, UIX, UIY, UIZ);
+        const f2 uJ0 = dot2(XX, XY, XZ, UJX, UJY, UJZ), uJ1 = dot2(YX, YY, YZ, UJX, UJY, UJZ),
+                 uJ2 = dot2(ZX, ZY, ZZ, UJX, UJY, UJZ);
+        const f2 QJ0 = pk2(b.z, b.w);
+        const f2 QI1 = dot2(XX, XY, XZ, MIX, MIY, MIZ), QI2 = dot2(YX, YY, YZ, MIX, MIY, MIZ),
+                 QI3 = dot2(ZX, ZY, ZZ, MIX, MIY, MIZ);
+        const f2 QJ1 = dot2(XX, XY, XZ, MJX, MJY, MJZ), QJ2 = dot2(YX, YY, YZ, MJX, MJY, MJZ),
+                 QJ3 = dot2(ZX, ZY, ZZ, MJX, MJY, MJZ);
+        const f2 rv1 = RINV, rv2 = mul2(RINV, RINV), rv3 = mul2(rv2, RINV);
+        const f2 rv4 = fma2(RV4P, mul2(rv3, RINV), RV4F);
+        // Thole factors (1 beyond damp_r2 or where t_i t_j <= 1e-5, as the reference).
+        f2 tc = ONE, td0 = ONE, td1 = ONE, dtc = ONE, dtd0 = ONE, dtd1 = ONE;
+        if (r2a < damp_r2 || r2b < damp_r2) {
+            const f2 R = mul2(R2, RINV);
+            const f2 U = mul2(mul2(R, ITI), pk2(h.z, h.w));
+            const f2 AM = pk2(fminf(ti, d.z), fminf(ti, d.w));
+            const f2 AU3 = mul2(AM, mul2(U, mul2(U, U)));
+            float xa, xb;
+            un2(AU3, xa, xb);
+            const bool da = r2a < damp_r2 && fabsf(ti * d.z) > 1.0e-5f;
+            const bool db = r2b < damp_r2 && fabsf(ti * d.w) > 1.0e-5f;
+            const f2 EX = pk2(da ? __expf(-xa) : 0.0f, db ? __expf(-xb) : 0.0f);
+            const f2 AUs = pk2(da ? xa : 0.0f, db ? xb : 0.0f);   // no inf/NaN into the products
+            const f2 NEX = neg2(EX);
+            tc = add2(ONE, NEX);
+            td1 = tc;
+            td0 = fma2(NEX, fma2(bc2(1.5f), AUs, ONE), ONE);
+            dtc = td0;
+            dtd0 = fma2(NEX, fma2(mul2(bc2(1.5f), AUs), AUs, add2(ONE, AUs)), ONE);
+            dtd1 = fma2(NEX, add2(ONE, AUs), ONE);
+        }
+        // Interaction terms (mS = iS = 1).
+        f2 eP = rv1, dP = mul2(bc2(-0.5f), rv2);
+        f2 Vij0 = mul2(eP, QJ0), Vji0 = mul2(eP, QI0), VijR0 = mul2(dP, QJ0), VjiR0 = mul2(dP, QI0);
+        eP = rv2;
+        f2 eU = mul2(rv2, tc);
+        dP = neg2(rv3);
+        f2 dU = mul2(mul2(bc2(-2.0f), rv3), dtc);
+        Vij0 = sub2(Vij0, fma2(eP, QJ1, mul2(eU, uJ0)));
+        f2 Vji1 = neg2(mul2(eP, QI0));
+        VijR0 = sub2(VijR0, fma2(dP, QJ1, mul2(dU, uJ0)));
+        f2 VjiR1 = neg2(mul2(dP, QI0));
+        f2 Vjid0 = neg2(mul2(eU, QI0));
+        f2 Vij1 = mul2(eP, QJ0);
+        Vji0 = add2(Vji0, fma2(eP, QI1, mul2(eU, uI0)));
+        f2 VijR1 = mul2(dP, QJ0);
+        VjiR0 = add2(VjiR0, fma2(dP, QI1, mul2(dU, uI0)));
+        f2 Vijd0 = mul2(eU, QJ0);
+        eP = mul2(bc2(-2.0f), rv3);
+        eU = mul2(eP, td0);
+        dP = mul2(bc2(3.0f), rv4);
+        dU = mul2(mul2(bc2(6.0f), rv4), dtd0);
+        Vij1 = add2(Vij1, fma2(eP, QJ1, mul2(eU, uJ0)));
+        Vji1 = add2(Vji1, fma2(eP, QI1, mul2(eU, uI0)));
+        VijR1 = add2(VijR1, fma2(dP, QJ1, mul2(dU, uJ0)));
+        VjiR1 = add2(VjiR1, fma2(dP, QI1, mul2(dU, uI0)));
+        Vijd0 = fma2(eU, QJ1, Vijd0);
+        Vjid0 = fma2(eU, QI1, Vjid0);
+        eP = rv3;
+        eU = mul2(rv3, td1);
+        dP = mul2(bc2(-1.5f), rv4);
+        dU = mul2(mul2(bc2(-3.0f), rv4), dtd1);
+        const f2 Vij2 = fma2(eP, QJ2, mul2(eU, uJ1)), Vji2 = fma2(eP, QI2, mul2(eU, uI1));
+        const f2 VijR2 = fma2(dP, QJ2, mul2(dU, uJ1)), VjiR2 = fma2(dP, QI2, mul2(dU, uI1));
+        const f2 Vijd1 = mul2(eU, QJ2), Vjid1 = mul2(eU, QI2);
+        const f2 Vij3 = fma2(eP, QJ3, mul2(eU, uJ2)), Vji3 = fma2(eP, QI3, mul2(eU, uI2));
+        const f2 VijR3 = fma2(dP, QJ3, mul2(dU, uJ2)), VjiR3 = fma2(dP, QI3, mul2(dU, uI2));
+        const f2 Vijd2 = mul2(eU, QJ3), Vjid2 = mul2(eU, QI3);
+
+        f2 fIZ = fma2(QI0, VijR0, fma2(QI1, VijR1, fma2(QI2, VijR2, mul2(QI3, VijR3))));
+        f2 fJZ = fma2(QJ0, VjiR0, fma2(QJ1, VjiR1, fma2(QJ2, VjiR2, mul2(QJ3, VjiR3))));
+        const f2 EIX = sub2(mul2(QI3, Vij1), mul2(QI1, Vij3));
+        const f2 EIY = sub2(mul2(QI1, Vij2), mul2(QI2, Vij1));
+        const f2 EJX = sub2(mul2(QJ3, Vji1), mul2(QJ1, Vji3));
+        const f2 EJY = sub2(mul2(QJ1, Vji2), mul2(QJ2, Vji1));
+        f2 iEIX = sub2(mul2(uI2, Vijd0), mul2(uI0, Vijd2));
+        f2 iEJX = sub2(mul2(uJ2, Vjid0), mul2(uJ0, Vjid2));
+        f2 iEIY = sub2(mul2(uI0, Vijd1), mul2(uI1, Vijd0));
+        f2 iEJY = sub2(mul2(uJ0, Vjid1), mul2(uJ1, Vjid0));
+        if (mutual) {
+            f2 eC = mul2(mul2(bc2(-4.0f), rv3), td0);
+            f2 dC = mul2(mul2(bc2(6.0f), rv4), dtd0);
+            iEIX = fma2(mul2(eC, uI2), uJ0, iEIX);
+            iEJX = fma2(mul2(eC, uJ2), uI0, iEJX);
+            iEIY = sub2(iEIY, mul2(mul2(eC, uI1), uJ0));
+            iEJY = sub2(iEJY, mul2(mul2(eC, uJ1), uI0));
+            fIZ = fma2(mul2(dC, uI0), uJ0, fIZ);
+            fJZ = fma2(mul2(dC, uJ0), uI0, fJZ);
+            eC = mul2(mul2(bc2(2.0f), rv3), td1);
+            dC = mul2(mul2(bc2(-3.0f), rv4), dtd1);
+            iEIX = sub2(iEIX, mul2(mul2(eC, uI0), uJ2));
+            iEJX = sub2(iEJX, mul2(mul2(eC, uJ0), uI2));
+            iEIY = fma2(mul2(eC, uI0), uJ1, iEIY);
+            iEJY = fma2(mul2(eC, uJ0), uI1, iEJY);
+            const f2 uu = fma2(uI1, uJ1, mul2(uI2, uJ2));
+            fIZ = fma2(dC, uu, fIZ);
+            fJZ = fma2(dC, uu, fJZ);
+        }
+        const f2 qf0 = mul2(RINV, add2(add2(EIY, EJY), add2(iEIY, iEJY)));
+        const f2 qf1 = neg2(mul2(RINV, add2(add2(EIX, EJX), add2(iEIX, iEJX))));
+        const f2 qf2 = neg2(add2(fJZ, fIZ));
+        // Back rotation with the reference's permuted matrix.
+        const f2 fvx = fma2(YY, qf0, fma2(ZY, qf1, mul2(XY, qf2)));
+        const f2 fvy = fma2(YZ, qf0, fma2(ZZ, qf1, mul2(XZ, qf2)));
+        const f2 fvz = fma2(YX, qf0, fma2(ZX, qf1, mul2(XX, qf2)));
+        {
+            const f2 EIZ = sub2(mul2(QI2, Vij3), mul2(QI3, Vij2));
+            const f2 q0 = neg2(EIX), q1 = neg2(EIY), q2 = neg2(EIZ);
+            TX = add2(TX, fma2(YY, q0, fma2(ZY, q1, mul2(XY, q2))));
+            TY = add2(TY, fma2(YZ, q0, fma2(ZZ, q1, mul2(XZ, q2))));
+            TZ = add2(TZ, fma2(YX, q0, fma2(ZX, q1, mul2(XX, q2))));
+            FX = sub2(FX, fvx);
+            FY = sub2(FY, fvy);
+            FZ = sub2(FZ, fvz);
+            f2 eq = fma2(QI0, Vij0, mul2(QJ0, Vji0));
+            eq = fma2(QI1, Vij1, fma2(QJ1, Vji1, eq));
+            eq = fma2(QI2, Vij2, fma2(QJ2, Vji2, eq));
+            eq = fma2(QI3, Vij3, fma2(QJ3, Vji3, eq));
+            EN = fma2(HALF, eq, EN);
+        }
+        {
+            const f2 EJZ = sub2(mul2(QJ2, Vji3), mul2(QJ3, Vji2));
+            const f2 q0 = neg2(EJX), q1 = neg2(EJY), q2 = neg2(EJZ);
+            UX = add2(UX, fma2(YY, q0, fma2(ZY, q1, mul2(XY, q2))));
+            UY = add2(UY, fma2(YZ, q0, fma2(ZZ, q1, mul2(XZ, q2))));
+            UZ = add2(UZ, fma2(YX, q0, fma2(ZX, q1, mul2(XX, q2))));
+            GX = add2(GX, fvx);
+            GY = add2(GY, fvy);
+            GZ = add2(GZ, fvz);
+        }
+        // Rotate the packed J-side sums one lane (64-bit shuffles).
+        GX = __shfl_sync(kFull, GX, nxt);
+        GY = __shfl_sync(kFull, GY, nxt);
+        GZ = __shfl_sync(kFull, GZ, nxt);
+        UX = __shfl_sync(kFull, UX, nxt);
+        UY = __shfl_sync(kFull, UY, nxt);
+        UZ = __shfl_sync(kFull, UZ, nxt);
+    }
+    float lo, hi;
+    const f2* Is[7] = {&FX, &FY, &FZ, &TX, &TY, &TZ, &EN};
+    float* Io[7] = {&f[0], &f[1], &f[2], &f[3], &f[4], &f[5], &en};
+#pragma unroll
+    for (int k = 0; k < 7; k++) {
+        un2(*Is[k], lo, hi);
+        *Io[k] += lo + hi;
+    }
+    // Lane l now holds (atom l & 15, atom (l & 15) + 16); lane l ^ 16 the other copy.
+    const f2 Js[6] = {GX, GY, GZ, UX, UY, UZ};
+#pragma unroll
+    for (int k = 0; k < 6; k++) {
+        un2(Js[k], lo, hi);
+        const float olo = __shfl_xor_sync(kFull, lo, 16), ohi = __shfl_xor_sync(kFull, hi, 16);
+        gg[k] += lane < 16 ? lo + olo : hi + ohi;
+    }
+}
+
 // Partner pairs of a SLOW tile pair with their (M, I) scales, each side once:
 // the lane's I atom with its partners in J (the pair energy is counted on the
 // lower-index side), and atom l of J (off the diagonal) with its partners in I.
@@ -889,6 +1193,7 @@ __global__ void __launch_bounds__(kSymThreads, 3) k_energy_sym(
     V4* s_pos = reinterpret_cast<V4*>(s_ext + BT);
     V4* s_dip = s_pos + NA;
     V4* s_ind = s_dip + NA;
+    __shared__ EPackedTile s_ept[sizeof(R) == 4 ? kSymWarps : 1];   // packed walk's J tile (mixed form)
 
     int p, q;
     band_pair(blockIdx.x, p, q);
@@ -952,7 +1257,23 @@ __global__ void __launch_bounds__(kSymThreads, 3) k_energy_sym(
                 const V4* su = s_ind + Jl * 32;
                 const unsigned partners = slow ? partner_bits(exc_j, e0, e1, jbase) : 0u;
                 R f[6] = {0, 0, 0, 0, 0, 0}, gg[6] = {0, 0, 0, 0, 0, 0}, en = 0;
-                if (slow) {
+                bool packed = false;
+                if constexpr (sizeof(R) == 4) {
+                    if (!slow) {
+                        packed = true;
+                        __syncwarp();
+                        stage_epacked(s_ept[warp], lane, sp[lane], sd[lane], su[lane]);
+                        __syncwarp();
+                        if (g.fold)
+                            energy_walk_x2<true>(P, pos, yz, s_ept[warp], lane, i, jbase, oix, oiy, oiz, pi, di, ui,
+                                                 g.fmask, damp_r2, rv4p, rv4f, P.mutual != 0, f, gg, en);
+                        else
+                            energy_walk_x2<false>(P, pos, yz, s_ept[warp], lane, i, jbase, oix, oiy, oiz, pi, di, ui,
+                                                  g.fmask, damp_r2, rv4p, rv4f, P.mutual != 0, f, gg, en);
+                    }
+                }
+                if (packed) {
+                } else if (slow) {
                     if (g.fold) {
                         energy_walk<R, true, true>(P, pos, yz, sp, sd, su, lane, i, jbase, oix, oiy, oiz, me, diag,
                                                    partners, damp_r2, rv4p, rv4f, f, gg, en);
