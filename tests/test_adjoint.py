@@ -127,3 +127,92 @@ def test_force_matching_gradients_through_autograd():
         pm[k] -= h
         fd = (loss_np(pp) - loss_np(pm)) / (2 * h)
         assert abs(grad[k] - fd) <= 1e-4 * abs(fd), (k, grad[k], fd)
+
+
+def _global_params_tensors(base, params, torch):
+    """Per-particle tensors of the five global water parameters (alpha_O, alpha_H,
+    Thole a, q_O with q_H = -q_O/2, dipole magnitude) for a system of waters."""
+    n = base.n
+    o = torch.zeros(n, dtype=torch.bool)
+    o[0::3] = True
+    q = torch.where(o, params[3], -params[3] / 2)
+    alpha = torch.where(o, params[0], params[1])
+    thole = params[2].expand(n)
+    dip = torch.zeros(n, 3, dtype=torch.float64)
+    dip = dip.index_put((torch.arange(0, n, 3), torch.full((n // 3,), 2)), params[4].expand(n // 3))
+    return q, alpha, thole, dip
+
+
+P0 = np.array([S.ALPHA_O, S.ALPHA_H, S.THOLE, S.Q_O, S.DIPOLE_O])
+P_TARGET = [S.ALPHA_O * 1.1, S.ALPHA_H * 0.9, 0.42, S.Q_O, S.DIPOLE_O]
+
+
+def test_force_matching_gradients_4096_water_box():
+    # The differentiation workload on the 4,096-water box: targets from the FP64
+    # form with alpha_O x1.1, alpha_H x0.9, a = 0.42; loss = mean (F - F_target)^2;
+    # gradients of the five global parameters through the adjoint, against
+    # central differences (relative step 1e-4) of the same FP64 forward, which
+    # the parity tests pin to the reference at 1e-10.
+    import torch
+    from tholedipoleplugin_b200.autograd import thole_dipole
+    from tholedipoleplugin_b200.kernel import CudaCalcTholeDipoleForceKernel
+
+    base = S.config_medium(target_eps=1e-12, max_iter=2000)
+    with CudaCalcTholeDipoleForceKernel(base, precision="double") as k:
+        def forces_at(p):
+            s = _global_system(base, p)
+            k.copyParametersToContext(s)
+            return k.execute(s.positions)[1]
+
+        target = forces_at(P_TARGET)
+
+        def loss_np(p):
+            return float(np.mean((forces_at(p) - target) ** 2))
+
+        params = torch.tensor(P0, dtype=torch.float64, requires_grad=True)
+        q, alpha, thole, dip = _global_params_tensors(base, params, torch)
+        _, forces = thole_dipole(q, alpha, thole, dip, k, base)
+        loss = torch.mean((forces - torch.tensor(target)) ** 2)
+        loss.backward()
+        grad = params.grad.numpy()
+        for j in range(5):
+            h = 1e-4 * abs(P0[j])
+            pp, pm = P0.copy(), P0.copy()
+            pp[j] += h
+            pm[j] -= h
+            fd = (loss_np(pp) - loss_np(pm)) / (2 * h)
+            assert abs(grad[j] - fd) <= 1e-4 * abs(fd), (j, grad[j], fd)
+
+
+def test_force_matching_gradients_256_clusters():
+    # The same gradients over 256 clusters of the cluster workload (4-64 waters,
+    # seeded), against central differences of the FP64 oracle.
+    import torch
+    from tholedipoleplugin_b200.autograd import ClusterGradients, thole_dipole_clusters
+
+    clusters = S.cluster_batch(1024, 4, 64, seed=3, target_eps=1e-12, max_iter=5000)[:256]
+    allw, _ = S.concat_clusters(clusters)
+
+    def oracle_forces(p):
+        return np.concatenate([O.compute(_global_system(c, p), "port").forces for c in clusters])
+
+    target = oracle_forces(P_TARGET)
+
+    def loss_np(p):
+        return float(np.mean((oracle_forces(p) - target) ** 2))
+
+    with ClusterGradients(clusters, precision="double") as batch:
+        params = torch.tensor(P0, dtype=torch.float64, requires_grad=True)
+        q, alpha, thole, dip = _global_params_tensors(allw, params, torch)
+        _, forces = thole_dipole_clusters(q, alpha, thole, dip, batch)
+        loss = torch.mean((forces - torch.tensor(target)) ** 2)
+        loss.backward()
+    grad = params.grad.numpy()
+    assert abs(loss.item() - loss_np(P0)) < 1e-9 * abs(loss.item())
+    for j in range(5):
+        h = 1e-4 * abs(P0[j])
+        pp, pm = P0.copy(), P0.copy()
+        pp[j] += h
+        pm[j] -= h
+        fd = (loss_np(pp) - loss_np(pm)) / (2 * h)
+        assert abs(grad[j] - fd) <= 1e-4 * abs(fd), (j, grad[j], fd)
