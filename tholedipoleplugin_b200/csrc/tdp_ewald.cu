@@ -365,10 +365,35 @@ __device__ __forceinline__ void stage_packed(EwPackedTile& T, int lane, float4 p
     reinterpret_cast<float*>(&T.it[m])[h] = 1.0f / v.w;
 }
 
+// Whether a J atom (record offsets p in J's frame) can lie within the cutoff
+// of any atom of the I tile, whose centre sits at -dc in J's frame with
+// half-extents e: the distance to the I tile's box, minimum image when the
+// tile pair folds, against the cutoff plus 1e-3 nm (no pair the walk would
+// count is dropped by FP32 rounding).
+__device__ __forceinline__ bool near_i_tile(const PairParams& P, float px, float py, float pz, const float* dc,
+                                            const float* e, float rcm2, bool fold) {
+    float a[3] = {px + dc[0], py + dc[1], pz + dc[2]};
+    float g2 = 0.0f;
+#pragma unroll
+    for (int k = 0; k < 3; k++) {
+        if (fold) a[k] = fold_f(a[k], (float)P.box[k], (float)P.inv_box[k]);
+        const float g = fmaxf(fabsf(a[k]) - e[k], 0.0f);
+        g2 += g * g;
+    }
+    return g2 < rcm2;
+}
+
+// Minimum-image displacement of J's tile centre from I's, FP32 (mixed form).
+__device__ __forceinline__ void tile_dc(const PairParams& P, double4 cA, double4 cB, float* dc) {
+    dc[0] = (float)fold1(cB.x - cA.x, P.box[0], P.inv_box[0]);
+    dc[1] = (float)fold1(cB.y - cA.y, P.box[1], P.inv_box[1]);
+    dc[2] = (float)fold1(cB.z - cA.z, P.box[2], P.inv_box[2]);
+}
+
 template <int KIND, bool FOLD>
 __device__ __forceinline__ void ew_field_walk_x2(const PairParams& P, const EwParams& E, const EwPackedTile& T,
                                                  float ox, float oy, float oz, float ti, float iti, float rc2,
-                                                 float damp_r2, float& fx, float& fy, float& fz) {
+                                                 float damp_r2, int nsteps, float& fx, float& fy, float& fz) {
     const f2 OX = bc2(ox), OY = bc2(oy), OZ = bc2(oz);
     const f2 ALPHA = bc2((float)E.alpha), NA2 = bc2((float)(-E.alpha * E.alpha));
     const f2 CA = bc2((float)E.ca), A2 = bc2((float)E.a2), ONE = bc2(1.0f), THREE = bc2(3.0f), NEG = bc2(-1.0f);
@@ -385,7 +410,7 @@ __device__ __forceinline__ void ew_field_walk_x2(const PairParams& P, const EwPa
     const f2 MAGIC = bc2(12582912.0f), NMAGIC = bc2(-12582912.0f);
     f2 FX = 0, FY = 0, FZ = 0;
 #pragma unroll 2
-    for (int m = 0; m < 16; m++) {
+    for (int m = 0; m < nsteps; m++) {
         const float4 a = T.p0[m], b = T.p1[m], c = T.v0[m], d = T.v1[m];
         const float2 it = T.it[m];
         f2 DX = sub2(pk2(a.x, a.y), OX), DY = sub2(pk2(a.z, a.w), OY), DZ = sub2(pk2(b.x, b.y), OZ);
@@ -469,6 +494,7 @@ __global__ void __launch_bounds__(kEwThreads) k_ew_field(PairParams P, EwParams 
                                                          const typename Vec4T<R>::type* __restrict__ posq_s,
                                                          const typename Vec4T<R>::type* __restrict__ src,
                                                          const double4* __restrict__ tctr,
+                                                         const double4* __restrict__ text,
                                                          const double* __restrict__ pos_s,
                                                          const int* __restrict__ exs_off, const int* __restrict__ exs_j,
                                                          const double* __restrict__ exs_m,
@@ -486,6 +512,9 @@ __global__ void __launch_bounds__(kEwThreads) k_ew_field(PairParams P, EwParams 
     const int i = I * 32 + lane;
     const V4 pi = posq_s[i], vi = src[i];
     const double4 cA = tctr[I];
+    const double4 eAd = text[I];
+    const float eA[3] = {(float)eAd.x, (float)eAd.y, (float)eAd.z};
+    const float rcm = (float)sqrt(E.rc2) + 1e-3f;
     const int e0 = i < P.n ? exs_off[i] : 0, e1 = i < P.n ? exs_off[i + 1] : 0;
     const R rc2 = (R)E.rc2, damp_r2 = (R)P.damp_r2;
     double fx = 0.0, fy = 0.0, fz = 0.0;
@@ -494,22 +523,40 @@ __global__ void __launch_bounds__(kEwThreads) k_ew_field(PairParams P, EwParams 
         const int ent = list[(size_t)I * E.cap + t];
         const int J = ent & kTileMask;
         const bool fold = (ent >> 30) & 1, slow = ((unsigned)ent >> 31) & 1u;
+        const double4 cB = tctr[J];
         __syncwarp();
         const V4 pj = posq_s[J * 32 + lane], vj = src[J * 32 + lane];
-        s_pos[warp][lane] = pj;
-        s_vec[warp][lane] = vj;
+        int nsteps = 16;
+        bool staged = false;
         if constexpr (sizeof(R) == 4) {
-            if (!slow) stage_packed(s_pk[warp], lane, pj, vj);
+            if (!slow) {
+                // Only the J atoms within the cutoff of the I tile's box,
+                // compacted; an odd count is padded with a multipole-free copy.
+                float dc[3];
+                tile_dc(P, cA, cB, dc);
+                const bool act = near_i_tile(P, (float)pj.x, (float)pj.y, (float)pj.z, dc, eA, rcm * rcm, fold);
+                const unsigned mk = __ballot_sync(kFull, act);
+                const int nact = __popc(mk), k = __popc(mk & ((1u << lane) - 1u));
+                if (act) stage_packed(s_pk[warp], k, pj, vj);
+                if ((nact & 1) && act && k == nact - 1)
+                    stage_packed(s_pk[warp], nact, make_float4(pj.x, pj.y, pj.z, 0.0f), make_float4(0.0f, 0.0f, 0.0f, vj.w));
+                nsteps = (nact + 1) >> 1;
+                staged = true;
+            }
+        }
+        if (!staged) {
+            s_pos[warp][lane] = pj;
+            s_vec[warp][lane] = vj;
         }
         __syncwarp();
         R ox, oy, oz;
-        tile_shift<R>(P, cA, tctr[J], pi.x, pi.y, pi.z, ox, oy, oz);
+        tile_shift<R>(P, cA, cB, pi.x, pi.y, pi.z, ox, oy, oz);
         R tx = 0, ty = 0, tz = 0;
         if constexpr (sizeof(R) == 4) {
             if (!slow) {
                 const float iti = 1.0f / (float)vi.w;
-                if (fold) ew_field_walk_x2<KIND, true>(P, E, s_pk[warp], ox, oy, oz, vi.w, iti, rc2, damp_r2, tx, ty, tz);
-                else ew_field_walk_x2<KIND, false>(P, E, s_pk[warp], ox, oy, oz, vi.w, iti, rc2, damp_r2, tx, ty, tz);
+                if (fold) ew_field_walk_x2<KIND, true>(P, E, s_pk[warp], ox, oy, oz, vi.w, iti, rc2, damp_r2, nsteps, tx, ty, tz);
+                else ew_field_walk_x2<KIND, false>(P, E, s_pk[warp], ox, oy, oz, vi.w, iti, rc2, damp_r2, nsteps, tx, ty, tz);
                 fx += (double)tx;
                 fy += (double)ty;
                 fz += (double)tz;
@@ -707,7 +754,8 @@ __device__ __forceinline__ void pair_ewald2(f2 DX, f2 DY, f2 DZ, f2 QI, f2 IX, f
 template <bool FOLD>
 __device__ __forceinline__ void ew_force_walk_x2(const PairParams& P, const EwParams& E, const EwPackedForceTile& T,
                                                  float ox, float oy, float oz, float qi, float4 di, float4 ui,
-                                                 float iti, float rc2, float damp_r2, float& en, float* f, float* g) {
+                                                 float iti, float rc2, float damp_r2, int nsteps, float& en, float* f,
+                                                 float* g) {
     const f2 OX = bc2(ox), OY = bc2(oy), OZ = bc2(oz);
     const f2 ALPHA = bc2((float)E.alpha), NA2 = bc2((float)(-E.alpha * E.alpha));
     const f2 CA = bc2((float)E.ca), A2 = bc2((float)E.a2), ONE = bc2(1.0f), THREE = bc2(3.0f),
@@ -727,7 +775,7 @@ __device__ __forceinline__ void ew_force_walk_x2(const PairParams& P, const EwPa
     const f2 MAGIC = bc2(12582912.0f), NMAGIC = bc2(-12582912.0f);
     f2 EN = 0, FX = 0, FY = 0, FZ = 0, GX = 0, GY = 0, GZ = 0;
 #pragma unroll 1
-    for (int m = 0; m < 16; m++) {
+    for (int m = 0; m < nsteps; m++) {
         const float4 a = T.p0[m], b = T.p1[m], c = T.d0[m], d = T.d1[m], u = T.u0[m], v = T.u1[m];
         const float2 it = T.it[m];
         f2 DX = sub2(pk2(a.x, a.y), OX), DY = sub2(pk2(a.z, a.w), OY), DZ = sub2(pk2(b.x, b.y), OZ);
@@ -824,6 +872,7 @@ __global__ void __launch_bounds__(kEwThreads) k_ew_force(PairParams P, EwParams 
                                                          const typename Vec4T<R>::type* __restrict__ dipt_s,
                                                          const typename Vec4T<R>::type* __restrict__ vec_s,
                                                          const double4* __restrict__ tctr,
+                                                         const double4* __restrict__ text,
                                                          const double* __restrict__ pos_s,
                                                          const int* __restrict__ exs_off, const int* __restrict__ exs_j,
                                                          const double* __restrict__ exs_m,
@@ -840,6 +889,9 @@ __global__ void __launch_bounds__(kEwThreads) k_ew_force(PairParams P, EwParams 
     const int i = I * 32 + lane;
     const V4 pi = posq_s[i], di = dipt_s[i], ui = vec_s[i];
     const double4 cA = tctr[I];
+    const double4 eAd = text[I];
+    const float eA[3] = {(float)eAd.x, (float)eAd.y, (float)eAd.z};
+    const float rcm = (float)sqrt(E.rc2) + 1e-3f;
     const int e0 = i < P.n ? exs_off[i] : 0, e1 = i < P.n ? exs_off[i + 1] : 0;
     const R rc2 = (R)E.rc2, damp_r2 = (R)P.damp_r2;
     double F[3] = {0, 0, 0}, G[3] = {0, 0, 0}, en = 0.0;
@@ -848,23 +900,42 @@ __global__ void __launch_bounds__(kEwThreads) k_ew_force(PairParams P, EwParams 
         const int ent = list[(size_t)I * E.cap + t];
         const int J = ent & kTileMask;
         const bool fold = (ent >> 30) & 1, slow = ((unsigned)ent >> 31) & 1u;
+        const double4 cB = tctr[J];
         __syncwarp();
         const V4 pj = posq_s[J * 32 + lane], dj = dipt_s[J * 32 + lane], uj = vec_s[J * 32 + lane];
-        s_pos[warp][lane] = pj;
-        s_dip[warp][lane] = dj;
-        s_ind[warp][lane] = uj;
+        int nsteps = 16;
+        bool staged = false;
         if constexpr (sizeof(R) == 4) {
-            if (!slow) stage_packed_force(s_pk[warp], lane, pj, dj, uj);
+            if (!slow) {
+                // Only the J atoms within the cutoff of the I tile's box,
+                // compacted; an odd count is padded with a multipole-free copy.
+                float dc[3];
+                tile_dc(P, cA, cB, dc);
+                const bool act = near_i_tile(P, (float)pj.x, (float)pj.y, (float)pj.z, dc, eA, rcm * rcm, fold);
+                const unsigned mk = __ballot_sync(kFull, act);
+                const int nact = __popc(mk), k = __popc(mk & ((1u << lane) - 1u));
+                if (act) stage_packed_force(s_pk[warp], k, pj, dj, uj);
+                if ((nact & 1) && act && k == nact - 1)
+                    stage_packed_force(s_pk[warp], nact, make_float4(pj.x, pj.y, pj.z, 0.0f),
+                                       make_float4(0.0f, 0.0f, 0.0f, dj.w), make_float4(0.0f, 0.0f, 0.0f, 0.0f));
+                nsteps = (nact + 1) >> 1;
+                staged = true;
+            }
+        }
+        if (!staged) {
+            s_pos[warp][lane] = pj;
+            s_dip[warp][lane] = dj;
+            s_ind[warp][lane] = uj;
         }
         __syncwarp();
         R ox, oy, oz;
-        tile_shift<R>(P, cA, tctr[J], pi.x, pi.y, pi.z, ox, oy, oz);
+        tile_shift<R>(P, cA, cB, pi.x, pi.y, pi.z, ox, oy, oz);
         R f[3] = {0, 0, 0}, g[3] = {0, 0, 0}, e = 0;
         if constexpr (sizeof(R) == 4) {
             if (!slow) {
                 const float iti = 1.0f / (float)di.w;
-                if (fold) ew_force_walk_x2<true>(P, E, s_pk[warp], ox, oy, oz, pi.w, di, ui, iti, rc2, damp_r2, e, f, g);
-                else ew_force_walk_x2<false>(P, E, s_pk[warp], ox, oy, oz, pi.w, di, ui, iti, rc2, damp_r2, e, f, g);
+                if (fold) ew_force_walk_x2<true>(P, E, s_pk[warp], ox, oy, oz, pi.w, di, ui, iti, rc2, damp_r2, nsteps, e, f, g);
+                else ew_force_walk_x2<false>(P, E, s_pk[warp], ox, oy, oz, pi.w, di, ui, iti, rc2, damp_r2, nsteps, e, f, g);
                 for (int c = 0; c < 3; c++) {
                     F[c] += (double)f[c];
                     G[c] += (double)g[c];
@@ -1547,7 +1618,7 @@ void real_field(Ewald* e, const Dev& d, const void* src, cudaStream_t st) {
     typedef typename Vec4T<R>::type V4;
     const int blocks = d.pp.n_tiles;
     k_ew_field<R, KIND><<<blocks, kEwThreads, 0, st>>>(d.pp, e->E, (const V4*)d.posq_s, (const V4*)src, d.tctr_s,
-                                                      d.pos_s, d.exs_off, d.exs_j, d.exs_m, d.exs_s, e->list, e->count,
+                                                      d.text_s, d.pos_s, d.exs_off, d.exs_j, d.exs_m, d.exs_s, e->list, e->count,
                                                       d.n_pad, d.partial);
     e->launches++;
 }
@@ -1597,7 +1668,7 @@ void ewald_energy(Ewald* e, const Dev& d, double total_charge, cudaStream_t st) 
     k_ew_pack_mu<R><<<nblk((size_t)d.n, kVecThreads), kVecThreads, 0, st>>>(d.n, d.rank, d.mu, d.thole, (V4*)d.vec_s);
     const int blocks = d.pp.n_tiles;
     k_ew_force<R><<<blocks, kEwThreads, 0, st>>>(d.pp, e->E, (const V4*)d.posq_s, (const V4*)d.dipt_s,
-                                                 (const V4*)d.vec_s, d.tctr_s, d.pos_s, d.exs_off, d.exs_j, d.exs_m,
+                                                 (const V4*)d.vec_s, d.tctr_s, d.text_s, d.pos_s, d.exs_off, d.exs_j, d.exs_m,
                                                  d.exs_s, e->list, e->count, d.n_pad, d.partial, e->tile_energy);
     if (!e->vacuum) {
         FftGrid& g = e->energy_grid();
