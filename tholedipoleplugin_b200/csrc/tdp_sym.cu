@@ -259,15 +259,11 @@ __device__ __forceinline__ void field_walk2(const PairParams& P, const double* _
 }
 
 // ---------------------------------------------------------------------------
-// Packed FP32 walk (sm_100 f32x2 arithmetic) of field_walk2 for the mixed
-// form: the pairs of the two I slots ride in the low and high halves of
-// 64-bit registers, so every add/mul/fma instruction serves both pairs.  Same
-// operations in the same order as pair_delta + pair_matvec2 / pair_fixed2 per
-// half (FP32, subnormals flushed as the scalar path is compiled); only SLOW
-// tile pairs (masked pairs, partners) keep the scalar walk.
+// Packed FP32 arithmetic (sm_100 f32x2): two FP32 lanes in one 64-bit
+// register, so every add/mul/fma instruction serves two pairs.  The mixed
+// form's walks use it for every tile pair that is not SLOW (masked pairs,
+// partners), with FP32 subnormals flushed as the scalar walks are compiled.
 // ---------------------------------------------------------------------------
-__device__ __forceinline__ float4 to_f4(float4 v) { return v; }
-__device__ __forceinline__ float4 to_f4(double4 v) { return make_float4((float)v.x, (float)v.y, (float)v.z, (float)v.w); }
 
 typedef unsigned long long f2;
 __device__ __forceinline__ f2 pk2(float lo, float hi) {
@@ -307,17 +303,160 @@ __device__ __forceinline__ f2 fold2(f2 d, f2 nL, f2 invL) {
     return fma2(t, nL, d);
 }
 
+// ---------------------------------------------------------------------------
+// Packed FP32 walk over J-atom pairs: the halves of every 64-bit register are
+// J atoms m and m + 16 of the tile (records pair-interleaved in a per-warp
+// shared tile), so the I-side operands are loop-invariant broadcasts and the
+// J-side sums stay packed.  Lane l takes pair m = (l + s) & 15 at step s and
+// passes its packed J-side sums one lane on; lanes l and l ^ 16 hold two
+// partial copies of the same pair, added by one xor-16 exchange at the end.
+// Each lane carries one or two I atoms (slots a and b), each with the pair
+// arithmetic of pair_delta + pair_matvec2 / pair_fixed2 per half.
+// ---------------------------------------------------------------------------
+struct FPackedTile {
+    float4 p0[16], p1[16];   // (x, x', y, y'), (z, z', q, q')   (' = atom m + 16)
+    float4 v0[16], v1[16];   // (vx, vx', vy, vy'), (vz, vz', t, t')
+};
+
+__device__ __forceinline__ void stage_fpacked(FPackedTile& T, int lane, float4 p, float4 v) {
+    const int m = lane & 15, h = lane >> 4;
+    float* p0 = reinterpret_cast<float*>(&T.p0[m]);
+    float* p1 = reinterpret_cast<float*>(&T.p1[m]);
+    float* v0 = reinterpret_cast<float*>(&T.v0[m]);
+    float* v1 = reinterpret_cast<float*>(&T.v1[m]);
+    p0[h] = p.x;
+    p0[2 + h] = p.y;
+    p1[h] = p.z;
+    p1[2 + h] = p.w;
+    v0[h] = v.x;
+    v0[2 + h] = v.y;
+    v1[h] = v.z;
+    v1[2 + h] = v.w;
+}
+
+// Loop-invariant operands of one I atom.
+struct XSlot {
+    f2 OX, OY, OZ, VX, VY, VZ, Q;
+    float t;
+    int i;
+};
+
+__device__ __forceinline__ XSlot xslot(int i, float ox, float oy, float oz, float q, float4 v) {
+    XSlot x;
+    x.OX = bc2(ox);
+    x.OY = bc2(oy);
+    x.OZ = bc2(oz);
+    x.VX = bc2(v.x);
+    x.VY = bc2(v.y);
+    x.VZ = bc2(v.z);
+    x.Q = bc2(q);
+    x.t = v.w;
+    x.i = i;
+    return x;
+}
+
+// One I atom against J atoms (m, m + 16): I-side sums into F*, J-side into G*.
 template <int KIND, bool FOLD, bool DAMP>
-__device__ __forceinline__ void field_walk2_x2(const PairParams& P, const double* __restrict__ pos,
-                                               const float4* __restrict__ sp, const float4* __restrict__ sv, int lane,
-                                               int jbase, int ia, float oax, float oay, float oaz, float qa, float4 va,
-                                               int ib, float obx, float oby, float obz, float qb, float4 vb,
-                                               unsigned fm, float damp_r2, float* fa, float* fb, float* g) {
+__device__ __forceinline__ void xslot_pairs(const PairParams& P, const double* __restrict__ pos, const XSlot& x,
+                                            int ja, f2 PX, f2 PY, f2 PZ, f2 QJ, f2 VJX, f2 VJY, f2 VJZ, float tja,
+                                            float tjb, unsigned fm, f2 Lx, f2 Ly, f2 Lz, f2 Ix, f2 Iy, f2 Iz,
+                                            float tx, float ty, float tz, float damp_r2, f2& FX, f2& FY, f2& FZ,
+                                            f2& GX, f2& GY, f2& GZ) {
+    const f2 THREE = bc2(3.0f), NEG = bc2(-1.0f);
+    f2 DX = sub2(PX, x.OX), DY = sub2(PY, x.OY), DZ = sub2(PZ, x.OZ);
+    if (FOLD) {
+        bool amb_a = false, amb_b = false;
+        float ax, bx, ay, by, az, bz;
+        if (fm & 1u) {
+            DX = fold2(DX, Lx, Ix);
+            un2(DX, ax, bx);
+            amb_a = fabsf(ax) > tx;
+            amb_b = fabsf(bx) > tx;
+        }
+        if (fm & 2u) {
+            DY = fold2(DY, Ly, Iy);
+            un2(DY, ay, by);
+            amb_a = amb_a || fabsf(ay) > ty;
+            amb_b = amb_b || fabsf(by) > ty;
+        }
+        if (fm & 4u) {
+            DZ = fold2(DZ, Lz, Iz);
+            un2(DZ, az, bz);
+            amb_a = amb_a || fabsf(az) > tz;
+            amb_b = amb_b || fabsf(bz) > tz;
+        }
+        if (amb_a || amb_b) {
+            un2(DX, ax, bx);
+            un2(DY, ay, by);
+            un2(DZ, az, bz);
+            // Within 16 ulp of half a box: the reference's FP64 minimum image.
+            if (amb_a && x.i < P.n && ja < P.n) {
+                d3 e = exact_delta(P, pos, x.i, ja);
+                ax = (float)e.x;
+                ay = (float)e.y;
+                az = (float)e.z;
+            }
+            if (amb_b && x.i < P.n && ja + 16 < P.n) {
+                d3 e = exact_delta(P, pos, x.i, ja + 16);
+                bx = (float)e.x;
+                by = (float)e.y;
+                bz = (float)e.z;
+            }
+            DX = pk2(ax, bx);
+            DY = pk2(ay, by);
+            DZ = pk2(az, bz);
+        }
+    }
+    const f2 R2 = fma2(DX, DX, fma2(DY, DY, mul2(DZ, DZ)));
+    float r2a, r2b;
+    un2(R2, r2a, r2b);
+    const f2 RINV = pk2(rsqrt_r(r2a), rsqrt_r(r2b));
+    const f2 RINV2 = mul2(RINV, RINV);
+    f2 RR3 = mul2(RINV, RINV2);
+    f2 RR5 = mul2(mul2(THREE, RR3), RINV2);
+    if (DAMP) {
+        if (r2a < damp_r2 || r2b < damp_r2) {
+            float ra, rb, r3a, r3b, r5a, r5b;
+            un2(RINV, ra, rb);
+            un2(RR3, r3a, r3b);
+            un2(RR5, r5a, r5b);
+            damp_field<float>(r2a, ra, x.t, tja, damp_r2, r3a, r5a);
+            damp_field<float>(r2b, rb, x.t, tjb, damp_r2, r3b, r5b);
+            RR3 = pk2(r3a, r3b);
+            RR5 = pk2(r5a, r5b);
+        }
+    }
+    const f2 NRR3 = mul2(RR3, NEG);
+    if (KIND == 1) {
+        // pair_matvec2: f_i += (rr5 v_j.d) d - rr3 v_j;  f_j += (rr5 v_i.d) d - rr3 v_i.
+        const f2 DDJ = mul2(RR5, fma2(VJX, DX, fma2(VJY, DY, mul2(VJZ, DZ))));
+        const f2 DDI = mul2(RR5, fma2(x.VX, DX, fma2(x.VY, DY, mul2(x.VZ, DZ))));
+        FX = fma2(NRR3, VJX, fma2(DDJ, DX, FX));
+        FY = fma2(NRR3, VJY, fma2(DDJ, DY, FY));
+        FZ = fma2(NRR3, VJZ, fma2(DDJ, DZ, FZ));
+        GX = fma2(NRR3, x.VX, fma2(DDI, DX, GX));
+        GY = fma2(NRR3, x.VY, fma2(DDI, DY, GY));
+        GZ = fma2(NRR3, x.VZ, fma2(DDI, DZ, GZ));
+    } else {
+        // pair_fixed2: a = rr3 q_j - rr5 m_j.d, b = rr3 q_i + rr5 m_i.d;
+        // f_i -= d a + m_j rr3 (F holds the negative);  f_j += d b - m_i rr3.
+        const f2 A = sub2(mul2(RR3, QJ), mul2(RR5, fma2(VJX, DX, fma2(VJY, DY, mul2(VJZ, DZ)))));
+        const f2 B = fma2(RR5, fma2(x.VX, DX, fma2(x.VY, DY, mul2(x.VZ, DZ))), mul2(RR3, x.Q));
+        FX = fma2(VJX, RR3, fma2(DX, A, FX));
+        FY = fma2(VJY, RR3, fma2(DY, A, FY));
+        FZ = fma2(VJZ, RR3, fma2(DZ, A, FZ));
+        GX = fma2(NRR3, x.VX, fma2(DX, B, GX));
+        GY = fma2(NRR3, x.VY, fma2(DY, B, GY));
+        GZ = fma2(NRR3, x.VZ, fma2(DZ, B, GZ));
+    }
+}
+
+template <int KIND, bool FOLD, bool DAMP>
+__device__ __forceinline__ void field_walk_x4(const PairParams& P, const double* __restrict__ pos,
+                                              const FPackedTile& T, int lane, int jbase, const XSlot& xa,
+                                              const XSlot& xb, bool two, unsigned fm, float damp_r2, float* fa,
+                                              float* fb, float* g) {
     const int nxt = (lane + 1) & 31;
-    const f2 OX = pk2(oax, obx), OY = pk2(oay, oby), OZ = pk2(oaz, obz);
-    const f2 VX = pk2(va.x, vb.x), VY = pk2(va.y, vb.y), VZ = pk2(va.z, vb.z);
-    const f2 NVX = pk2(-va.x, -vb.x), NVY = pk2(-va.y, -vb.y), NVZ = pk2(-va.z, -vb.z);
-    const f2 QI = pk2(qa, qb), THREE = bc2(3.0f), NEG = bc2(-1.0f);
     f2 Lx = 0, Ly = 0, Lz = 0, Ix = 0, Iy = 0, Iz = 0;
     float tx = 0.f, ty = 0.f, tz = 0.f;
     if (FOLD) {
@@ -331,122 +470,49 @@ __device__ __forceinline__ void field_walk2_x2(const PairParams& P, const double
         ty = (float)P.half_box_tol[1];
         tz = (float)P.half_box_tol[2];
     }
-    // I-side sums (lo: slot a, hi: slot b); KIND 0 accumulates their negatives.
-    f2 FX = 0, FY = 0, FZ = 0;
-#pragma unroll 2
-    for (int s = 0; s < 32; s++) {
-        const int jj = (lane + s) & 31;
-        const float4 pj = sp[jj], vj = sv[jj];
-        f2 DX = sub2(bc2(pj.x), OX), DY = sub2(bc2(pj.y), OY), DZ = sub2(bc2(pj.z), OZ);
-        if (FOLD) {
-            // Only the dimensions of fm can need folding (elsewhere every pair
-            // of the two tiles lies within half a box minus the margin).
-            bool amb_a = false, amb_b = false;
-            float ax, bx, ay, by, az, bz;
-            if (fm & 1u) {
-                DX = fold2(DX, Lx, Ix);
-                un2(DX, ax, bx);
-                amb_a = fabsf(ax) > tx;
-                amb_b = fabsf(bx) > tx;
-            }
-            if (fm & 2u) {
-                DY = fold2(DY, Ly, Iy);
-                un2(DY, ay, by);
-                amb_a = amb_a || fabsf(ay) > ty;
-                amb_b = amb_b || fabsf(by) > ty;
-            }
-            if (fm & 4u) {
-                DZ = fold2(DZ, Lz, Iz);
-                un2(DZ, az, bz);
-                amb_a = amb_a || fabsf(az) > tz;
-                amb_b = amb_b || fabsf(bz) > tz;
-            }
-            if (amb_a || amb_b) {
-                un2(DX, ax, bx);
-                un2(DY, ay, by);
-                un2(DZ, az, bz);
-                // Within 16 ulp of half a box: the reference's FP64 minimum image.
-                const int j = jbase + jj;
-                if (amb_a && ia < P.n && j < P.n) {
-                    d3 e = exact_delta(P, pos, ia, j);
-                    ax = (float)e.x;
-                    ay = (float)e.y;
-                    az = (float)e.z;
-                }
-                if (amb_b && ib < P.n && j < P.n) {
-                    d3 e = exact_delta(P, pos, ib, j);
-                    bx = (float)e.x;
-                    by = (float)e.y;
-                    bz = (float)e.z;
-                }
-                DX = pk2(ax, bx);
-                DY = pk2(ay, by);
-                DZ = pk2(az, bz);
-            }
-        }
-        const f2 R2 = fma2(DX, DX, fma2(DY, DY, mul2(DZ, DZ)));
-        float r2a, r2b;
-        un2(R2, r2a, r2b);
-        const f2 RINV = pk2(rsqrt_r(r2a), rsqrt_r(r2b));
-        const f2 RINV2 = mul2(RINV, RINV);
-        f2 RR3 = mul2(RINV, RINV2);
-        f2 RR5 = mul2(mul2(THREE, RR3), RINV2);
-        if (DAMP) {
-            if (r2a < damp_r2 || r2b < damp_r2) {
-                float ra, rb, r3a, r3b, r5a, r5b;
-                un2(RINV, ra, rb);
-                un2(RR3, r3a, r3b);
-                un2(RR5, r5a, r5b);
-                damp_field<float>(r2a, ra, va.w, vj.w, damp_r2, r3a, r5a);
-                damp_field<float>(r2b, rb, vb.w, vj.w, damp_r2, r3b, r5b);
-                RR3 = pk2(r3a, r3b);
-                RR5 = pk2(r5a, r5b);
-            }
-        }
-        const f2 NRR3 = mul2(RR3, NEG);
-        float gx, gy, gz, hx, hy, hz;
-        if (KIND == 1) {
-            // pair_matvec2: f_i += (rr5 v_j.d) d - rr3 v_j;  f_j += (rr5 v_i.d) d - rr3 v_i.
-            const f2 VJX = bc2(vj.x), VJY = bc2(vj.y), VJZ = bc2(vj.z);
-            const f2 DDJ = mul2(RR5, fma2(VJX, DX, fma2(VJY, DY, mul2(VJZ, DZ))));
-            const f2 DDI = mul2(RR5, fma2(VX, DX, fma2(VY, DY, mul2(VZ, DZ))));
-            FX = fma2(NRR3, VJX, fma2(DDJ, DX, FX));
-            FY = fma2(NRR3, VJY, fma2(DDJ, DY, FY));
-            FZ = fma2(NRR3, VJZ, fma2(DDJ, DZ, FZ));
-            un2(fma2(DDI, DX, mul2(NRR3, VX)), gx, hx);
-            un2(fma2(DDI, DY, mul2(NRR3, VY)), gy, hy);
-            un2(fma2(DDI, DZ, mul2(NRR3, VZ)), gz, hz);
-        } else {
-            // pair_fixed2: a = rr3 q_j - rr5 m_j.d, b = rr3 q_i + rr5 m_i.d;
-            // f_i -= d a + m_j rr3;  f_j += d b - m_i rr3.
-            const f2 MJX = bc2(vj.x), MJY = bc2(vj.y), MJZ = bc2(vj.z);
-            const f2 A = sub2(mul2(RR3, bc2(pj.w)), mul2(RR5, fma2(MJX, DX, fma2(MJY, DY, mul2(MJZ, DZ)))));
-            const f2 B = fma2(RR5, fma2(VX, DX, fma2(VY, DY, mul2(VZ, DZ))), mul2(RR3, QI));
-            FX = fma2(MJX, RR3, fma2(DX, A, FX));
-            FY = fma2(MJY, RR3, fma2(DY, A, FY));
-            FZ = fma2(MJZ, RR3, fma2(DZ, A, FZ));
-            un2(fma2(DX, B, mul2(NVX, RR3)), gx, hx);
-            un2(fma2(DY, B, mul2(NVY, RR3)), gy, hy);
-            un2(fma2(DZ, B, mul2(NVZ, RR3)), gz, hz);
-        }
-        g[0] += gx + hx;
-        g[1] += gy + hy;
-        g[2] += gz + hz;
-        g[0] = __shfl_sync(kFull, g[0], nxt);
-        g[1] = __shfl_sync(kFull, g[1], nxt);
-        g[2] = __shfl_sync(kFull, g[2], nxt);
+    f2 FXA = 0, FYA = 0, FZA = 0, FXB = 0, FYB = 0, FZB = 0;   // I side, packed over (m, m + 16)
+    f2 GX = 0, GY = 0, GZ = 0;                                 // J side (packed atoms m, m + 16)
+    // One step is already four independent pairs: no unrolling (the walk's
+    // variants must stay small enough for the instruction cache).
+#pragma unroll 1
+    for (int s = 0; s < 16; s++) {
+        const int m = (lane + s) & 15;
+        const float4 a = T.p0[m], b = T.p1[m], c = T.v0[m], d = T.v1[m];
+        const f2 PX = pk2(a.x, a.y), PY = pk2(a.z, a.w), PZ = pk2(b.x, b.y), QJ = pk2(b.z, b.w);
+        const f2 VJX = pk2(c.x, c.y), VJY = pk2(c.z, c.w), VJZ = pk2(d.x, d.y);
+        xslot_pairs<KIND, FOLD, DAMP>(P, pos, xa, jbase + m, PX, PY, PZ, QJ, VJX, VJY, VJZ, d.z, d.w, fm, Lx, Ly,
+                                      Lz, Ix, Iy, Iz, tx, ty, tz, damp_r2, FXA, FYA, FZA, GX, GY, GZ);
+        if (two)
+            xslot_pairs<KIND, FOLD, DAMP>(P, pos, xb, jbase + m, PX, PY, PZ, QJ, VJX, VJY, VJZ, d.z, d.w, fm, Lx, Ly,
+                                          Lz, Ix, Iy, Iz, tx, ty, tz, damp_r2, FXB, FYB, FZB, GX, GY, GZ);
+        GX = __shfl_sync(kFull, GX, nxt);
+        GY = __shfl_sync(kFull, GY, nxt);
+        GZ = __shfl_sync(kFull, GZ, nxt);
     }
-    float lx, hx2, ly, hy2, lz, hz2;
-    un2(FX, lx, hx2);
-    un2(FY, ly, hy2);
-    un2(FZ, lz, hz2);
     const float sg = KIND == 0 ? -1.0f : 1.0f;
-    fa[0] += sg * lx;
-    fa[1] += sg * ly;
-    fa[2] += sg * lz;
-    fb[0] += sg * hx2;
-    fb[1] += sg * hy2;
-    fb[2] += sg * hz2;
+    float lo, hi;
+    un2(FXA, lo, hi);
+    fa[0] += sg * (lo + hi);
+    un2(FYA, lo, hi);
+    fa[1] += sg * (lo + hi);
+    un2(FZA, lo, hi);
+    fa[2] += sg * (lo + hi);
+    if (two) {
+        un2(FXB, lo, hi);
+        fb[0] += sg * (lo + hi);
+        un2(FYB, lo, hi);
+        fb[1] += sg * (lo + hi);
+        un2(FZB, lo, hi);
+        fb[2] += sg * (lo + hi);
+    }
+    // Lane l now holds (atom l & 15, atom (l & 15) + 16); lane l ^ 16 the other copy.
+    const f2 Js[3] = {GX, GY, GZ};
+#pragma unroll
+    for (int k = 0; k < 3; k++) {
+        un2(Js[k], lo, hi);
+        const float olo = __shfl_xor_sync(kFull, lo, 16), ohi = __shfl_xor_sync(kFull, hi, 16);
+        g[k] += lane < 16 ? lo + olo : hi + ohi;
+    }
 }
 
 // Partner pairs of a SLOW tile pair, each side once with its scale (M for
@@ -580,6 +646,7 @@ __global__ void __launch_bounds__(kSymThreads, 4) k_field_sym(
     V4* s_pos = reinterpret_cast<V4*>(s_ie + 2 * kSymWarps);       // NA
     V4* s_vec = s_pos + NA;                                        // NA
     R* s_acc = reinterpret_cast<R*>(s_vec + NA);                   // kSymWarps * 3 * NA: J-side sums per warp
+    FPackedTile* s_fpt = reinterpret_cast<FPackedTile*>(s_acc + kSymWarps * 3 * NA);  // kSymWarps (FP32 only)
 
     int p, q;
     band_pair(blockIdx.x, p, q);
@@ -627,28 +694,50 @@ __global__ void __launch_bounds__(kSymThreads, 4) k_field_sym(
             const V4* sp = s_pos + Jl * 32;
             const V4* sv = s_vec + Jl * 32;
             R fa[3] = {0, 0, 0}, fb[3] = {0, 0, 0}, g[3] = {0, 0, 0};
-            if (a.valid && b.valid) {
+            bool packed = false;
+            if constexpr (sizeof(R) == 4) {
+                // Non-SLOW tile pairs: the packed walk over J-atom pairs, one or both slots.
+                const bool two = a.valid && b.valid;
+                if (two ? !(a.slow || b.slow) : !(a.valid ? a.slow : b.slow)) {
+                    packed = true;
+                    __syncwarp();
+                    stage_fpacked(s_fpt[warp], lane, sp[lane], sv[lane]);
+                    __syncwarp();
+                    const ISlot<R>& s1 = a.valid ? a : b;
+                    const ISlot<R>& s2 = two ? b : s1;
+                    float* f1 = a.valid ? fa : fb;
+                    const XSlot x1 = xslot(s1.i, s1.ox, s1.oy, s1.oz, s1.pi.w, s1.vi);
+                    const XSlot x2 = xslot(s2.i, s2.ox, s2.oy, s2.oz, s2.pi.w, s2.vi);
+                    const unsigned fm = s1.fmask | s2.fmask;
+                    const bool fold = s1.fold || s2.fold, near = s1.near || s2.near;
+// One inlined copy per slot count (the count is a constant inside each).
+#define TDP_FWALKX4(F, D)                                                                                        \
+    do {                                                                                                         \
+        if (two)                                                                                                 \
+            field_walk_x4<KIND, F, D>(P, pos, s_fpt[warp], lane, jbase, x1, x2, true, fm, damp_r2, f1, fb, g);  \
+        else                                                                                                     \
+            field_walk_x4<KIND, F, D>(P, pos, s_fpt[warp], lane, jbase, x1, x2, false, fm, damp_r2, f1, fb, g); \
+    } while (0)
+                    if (fold) {
+                        if (near) TDP_FWALKX4(true, true);
+                        else TDP_FWALKX4(true, false);
+                    } else if (near) {
+                        TDP_FWALKX4(false, true);
+                    } else {
+                        TDP_FWALKX4(false, false);
+                    }
+#undef TDP_FWALKX4
+                }
+            }
+            if (packed) {
+            } else if (a.valid && b.valid) {
                 const bool slow = a.slow || b.slow, fold = a.fold || b.fold;
                 const bool near = a.near || b.near;
 #define TDP_FWALK2(F, S, D)                                                                                        \
     field_walk2<R, KIND, F, S, D>(P, pos, sp, sv, lane, jbase, a.i, a.ox, a.oy, a.oz, a.pi.w, a.vi, a.diag,     \
                                   a.partners, b.i, b.ox, b.oy, b.oz, b.pi.w, b.vi, b.diag, b.partners, damp_r2, fa, \
                                   fb, g)
-#define TDP_FWALKX2(F, D)                                                                                          \
-    field_walk2_x2<KIND, F, D>(P, pos, (const float4*)sp, (const float4*)sv, lane, jbase, a.i, (float)a.ox,      \
-                               (float)a.oy, (float)a.oz, (float)a.pi.w, to_f4(a.vi), b.i, (float)b.ox, (float)b.oy, \
-                               (float)b.oz, (float)b.pi.w, to_f4(b.vi), a.fmask | b.fmask, (float)damp_r2,          \
-                               (float*)fa, (float*)fb, (float*)g)
-                if (sizeof(R) == 4 && !slow) {
-                    if (fold) {
-                        if (near) TDP_FWALKX2(true, true);
-                        else TDP_FWALKX2(true, false);
-                    } else if (near) {
-                        TDP_FWALKX2(false, true);
-                    } else {
-                        TDP_FWALKX2(false, false);
-                    }
-                } else if (slow) {
+                if (slow) {
                     if (fold) TDP_FWALK2(true, true, true);
                     else TDP_FWALK2(false, true, true);
                 } else if (fold) {
@@ -660,7 +749,6 @@ __global__ void __launch_bounds__(kSymThreads, 4) k_field_sym(
                     TDP_FWALK2(false, false, false);
                 }
 #undef TDP_FWALK2
-#undef TDP_FWALKX2
             } else {
                 const ISlot<R>& s1 = a.valid ? a : b;
                 R* f1 = a.valid ? fa : fb;
@@ -1338,7 +1426,8 @@ template <class R>
 size_t field_smem(int BT) {
     const int NA = 32 * BT;
     return sizeof(double) * 6 * kSymThreads + sizeof(double4) * (2 * BT + 4 * kSymWarps) +
-           sizeof(typename Vec4T<R>::type) * 2 * NA + sizeof(R) * kSymWarps * 3 * NA;
+           sizeof(typename Vec4T<R>::type) * 2 * NA + sizeof(R) * kSymWarps * 3 * NA +
+           (sizeof(R) == 4 ? sizeof(FPackedTile) * kSymWarps : 0);
 }
 
 template <class R>
