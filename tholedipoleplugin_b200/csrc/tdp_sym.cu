@@ -360,32 +360,32 @@ template <int KIND, bool FOLD, bool DAMP>
 __device__ __forceinline__ void xslot_pairs(const PairParams& P, const double* __restrict__ pos, const XSlot& x,
                                             int ja, f2 PX, f2 PY, f2 PZ, f2 QJ, f2 VJX, f2 VJY, f2 VJZ, float tja,
                                             float tjb, unsigned fm, f2 Lx, f2 Ly, f2 Lz, f2 Ix, f2 Iy, f2 Iz,
-                                            float tx, float ty, float tz, float damp_r2, f2& FX, f2& FY, f2& FZ,
+                                            f2 NTx, f2 NTy, f2 NTz, float damp_r2, f2& FX, f2& FY, f2& FZ,
                                             f2& GX, f2& GY, f2& GZ) {
     const f2 THREE = bc2(3.0f), NEG = bc2(-1.0f);
     f2 DX = sub2(PX, x.OX), DY = sub2(PY, x.OY), DZ = sub2(PZ, x.OZ);
     if (FOLD) {
-        bool amb_a = false, amb_b = false;
-        float ax, bx, ay, by, az, bz;
+        // Fold the dimensions of fm.  Q = d^2 - t^2 (t = half a box minus 16
+        // ulp) is negative unless the pair lies within the margin of half a
+        // box; AND-ing the Q words keeps sign bits 31 (low half) and 63 (high
+        // half) set only if every Q of that half is negative.
+        f2 neg = ~0ull;
         if (fm & 1u) {
             DX = fold2(DX, Lx, Ix);
-            un2(DX, ax, bx);
-            amb_a = fabsf(ax) > tx;
-            amb_b = fabsf(bx) > tx;
+            neg &= fma2(DX, DX, NTx);
         }
         if (fm & 2u) {
             DY = fold2(DY, Ly, Iy);
-            un2(DY, ay, by);
-            amb_a = amb_a || fabsf(ay) > ty;
-            amb_b = amb_b || fabsf(by) > ty;
+            neg &= fma2(DY, DY, NTy);
         }
         if (fm & 4u) {
             DZ = fold2(DZ, Lz, Iz);
-            un2(DZ, az, bz);
-            amb_a = amb_a || fabsf(az) > tz;
-            amb_b = amb_b || fabsf(bz) > tz;
+            neg &= fma2(DZ, DZ, NTz);
         }
-        if (amb_a || amb_b) {
+        const f2 flag = ~neg & 0x8000000080000000ull;
+        if (flag) {
+            const bool amb_a = (flag >> 31) & 1ull, amb_b = (flag >> 63) != 0ull;
+            float ax, bx, ay, by, az, bz;
             un2(DX, ax, bx);
             un2(DY, ay, by);
             un2(DZ, az, bz);
@@ -457,8 +457,7 @@ __device__ __forceinline__ void field_walk_x4(const PairParams& P, const double*
                                               const XSlot& xb, bool two, unsigned fm, float damp_r2, float* fa,
                                               float* fb, float* g) {
     const int nxt = (lane + 1) & 31;
-    f2 Lx = 0, Ly = 0, Lz = 0, Ix = 0, Iy = 0, Iz = 0;
-    float tx = 0.f, ty = 0.f, tz = 0.f;
+    f2 Lx = 0, Ly = 0, Lz = 0, Ix = 0, Iy = 0, Iz = 0, NTx = 0, NTy = 0, NTz = 0;
     if (FOLD) {
         Lx = bc2(-(float)P.box[0]);
         Ly = bc2(-(float)P.box[1]);
@@ -466,9 +465,9 @@ __device__ __forceinline__ void field_walk_x4(const PairParams& P, const double*
         Ix = bc2((float)P.inv_box[0]);
         Iy = bc2((float)P.inv_box[1]);
         Iz = bc2((float)P.inv_box[2]);
-        tx = (float)P.half_box_tol[0];
-        ty = (float)P.half_box_tol[1];
-        tz = (float)P.half_box_tol[2];
+        NTx = bc2(-(float)(P.half_box_tol[0] * P.half_box_tol[0]));
+        NTy = bc2(-(float)(P.half_box_tol[1] * P.half_box_tol[1]));
+        NTz = bc2(-(float)(P.half_box_tol[2] * P.half_box_tol[2]));
     }
     f2 FXA = 0, FYA = 0, FZA = 0, FXB = 0, FYB = 0, FZB = 0;   // I side, packed over (m, m + 16)
     f2 GX = 0, GY = 0, GZ = 0;                                 // J side (packed atoms m, m + 16)
@@ -481,10 +480,10 @@ __device__ __forceinline__ void field_walk_x4(const PairParams& P, const double*
         const f2 PX = pk2(a.x, a.y), PY = pk2(a.z, a.w), PZ = pk2(b.x, b.y), QJ = pk2(b.z, b.w);
         const f2 VJX = pk2(c.x, c.y), VJY = pk2(c.z, c.w), VJZ = pk2(d.x, d.y);
         xslot_pairs<KIND, FOLD, DAMP>(P, pos, xa, jbase + m, PX, PY, PZ, QJ, VJX, VJY, VJZ, d.z, d.w, fm, Lx, Ly,
-                                      Lz, Ix, Iy, Iz, tx, ty, tz, damp_r2, FXA, FYA, FZA, GX, GY, GZ);
+                                      Lz, Ix, Iy, Iz, NTx, NTy, NTz, damp_r2, FXA, FYA, FZA, GX, GY, GZ);
         if (two)
             xslot_pairs<KIND, FOLD, DAMP>(P, pos, xb, jbase + m, PX, PY, PZ, QJ, VJX, VJY, VJZ, d.z, d.w, fm, Lx, Ly,
-                                          Lz, Ix, Iy, Iz, tx, ty, tz, damp_r2, FXB, FYB, FZB, GX, GY, GZ);
+                                          Lz, Ix, Iy, Iz, NTx, NTy, NTz, damp_r2, FXB, FYB, FZB, GX, GY, GZ);
         GX = __shfl_sync(kFull, GX, nxt);
         GY = __shfl_sync(kFull, GY, nxt);
         GZ = __shfl_sync(kFull, GZ, nxt);
@@ -628,6 +627,25 @@ __device__ __forceinline__ void slot_against(ISlot<R>& a, const PairParams& P, b
     a.partners = a.slow ? partner_bits(exc_j, a.e0, a.e1, J * 32) : 0u;
 }
 
+// The same from the tile pair's geometry computed beforehand (FP32 form):
+// centre displacement dc in FP32 and flags fmask | fold << 3 | near << 4.
+template <class R>
+__device__ __forceinline__ void slot_against_pre(ISlot<R>& a, const PairParams& P, bool same_band, int J, int Jl,
+                                                 float dcx, float dcy, float dcz, unsigned fl,
+                                                 const int* __restrict__ exc_j) {
+    a.valid = a.act && J < P.n_tiles && (!same_band || Jl >= a.Il);
+    if (!a.valid) return;
+    a.ox = a.pi.x - (R)dcx;
+    a.oy = a.pi.y - (R)dcy;
+    a.oz = a.pi.z - (R)dcz;
+    a.fmask = fl & 7u;
+    a.fold = (fl >> 3) & 1u;
+    a.near = (fl >> 4) & 1u;
+    a.diag = a.I == J;
+    a.slow = a.diag || (J == P.n_tiles - 1 && (P.n & 31)) || (J >= a.et.x && J <= a.et.y);
+    a.partners = a.slow ? partner_bits(exc_j, a.e0, a.e1, J * 32) : 0u;
+}
+
 template <class R, int KIND>
 __global__ void __launch_bounds__(kSymThreads, 4) k_field_sym(
     PairParams P, const typename Vec4T<R>::type* __restrict__ posq, const typename Vec4T<R>::type* __restrict__ jvec,
@@ -682,13 +700,38 @@ __global__ void __launch_bounds__(kSymThreads, 4) k_field_sym(
             s_ie[2 * warp + lane] = s1.act ? text[s1.I] : make_double4(0, 0, 0, 0);
         }
         __syncwarp();
+        // FP32 form: the round's 2 x BT tile-pair geometries (FP64 arithmetic),
+        // one per lane, instead of every lane repeating each of them.
+        float gdx = 0.f, gdy = 0.f, gdz = 0.f;
+        unsigned gfl = 0u;
+        if constexpr (sizeof(R) == 4) {
+            if (lane < 2 * BT) {
+                const int k = lane / BT, Jl = lane - k * BT;
+                const TileGeom g = tile_geom(P, s_ic[2 * warp + k], s_ie[2 * warp + k], s_ctr[Jl], s_ext[Jl]);
+                gdx = (float)g.dcx;
+                gdy = (float)g.dcy;
+                gdz = (float)g.dcz;
+                gfl = g.fmask | (g.fold ? 8u : 0u) | (g.near ? 16u : 0u);
+            }
+        }
         for (int c = 0; c < 6; c++) my[c] = 0.0;
         for (int t = 0; t < BT; t++) {
             const int Jl = (t + warp * stride) % BT;
             const int J = q * BT + Jl;
             const double4 cB = s_ctr[Jl], eB = s_ext[Jl];
-            slot_against<R>(a, P, p == q, J, Jl, s_ic[2 * warp], s_ie[2 * warp], cB, eB, exc_j);
-            slot_against<R>(b, P, p == q, J, Jl, s_ic[2 * warp + 1], s_ie[2 * warp + 1], cB, eB, exc_j);
+            if constexpr (sizeof(R) == 4) {
+                const int la = Jl, lb = BT + Jl;
+                const float ax = __shfl_sync(kFull, gdx, la), ay = __shfl_sync(kFull, gdy, la),
+                            az = __shfl_sync(kFull, gdz, la);
+                const float bx = __shfl_sync(kFull, gdx, lb), by = __shfl_sync(kFull, gdy, lb),
+                            bz = __shfl_sync(kFull, gdz, lb);
+                const unsigned af = __shfl_sync(kFull, gfl, la), bf = __shfl_sync(kFull, gfl, lb);
+                slot_against_pre<R>(a, P, p == q, J, Jl, ax, ay, az, af, exc_j);
+                slot_against_pre<R>(b, P, p == q, J, Jl, bx, by, bz, bf, exc_j);
+            } else {
+                slot_against<R>(a, P, p == q, J, Jl, s_ic[2 * warp], s_ie[2 * warp], cB, eB, exc_j);
+                slot_against<R>(b, P, p == q, J, Jl, s_ic[2 * warp + 1], s_ie[2 * warp + 1], cB, eB, exc_j);
+            }
             if (!(a.valid || b.valid)) continue;
             const int jbase = J * 32;
             const V4* sp = s_pos + Jl * 32;
