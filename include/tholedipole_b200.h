@@ -81,8 +81,11 @@ extern "C" {
  * value a fresh process of the compiled reference reads, which makes results
  * reproducible against it.  With this flag they use 1/r^4 instead. */
 #define TDP_FLAG_DD_FORCE_R4 (1u << 0)
-/* Keep the previous call's induced dipoles as the solver's starting point
- * (the reference restarts from mu0 = alpha*E every call). */
+/* Start the Mutual CG solve from the previous calls' induced dipoles (the
+ * reference restarts from mu0 = alpha*E every call): 2*mu(n-1) - mu(n-2) when
+ * the last two calls converged -- along an MD trajectory a second-order
+ * guess -- else mu(n-1).  The converged result is the same fixed point to the
+ * solver tolerance; only the iteration count changes. */
 #define TDP_FLAG_WARM_START (1u << 1)
 /* Ewald mode (with TDP_PME only).  The reference has no Ewald sum: its "PME"
  * is the minimum image over all pairs (ReferenceTholeDipoleForce.cpp:1414-1423)

@@ -131,3 +131,37 @@ def test_rinv4_power_flag():
         e, f = k.execute(s.positions)
     assert rel_err(e, ref.energy) < 1e-9
     assert rel_rms(f, ref.forces) < 1e-8
+
+
+@pytest.mark.parametrize("precision", ["double", "mixed"])
+def test_warm_start_predictor(precision):
+    # A smooth trajectory (every atom moving at a constant velocity): with
+    # TDP_FLAG_WARM_START the solve starts from mu(n-1) on the second call and
+    # from 2 mu(n-1) - mu(n-2) after that.  The converged dipoles are the
+    # cold-start ones to the solver tolerance, in fewer iterations.  A NoCutoff
+    # cluster keeps the dipoles smooth in the positions (in a minimum-image box
+    # a pair crossing half a box edge switches images discontinuously).
+    s = S.water_cluster(40, np.random.default_rng(4)).copy(target_eps=1e-8, max_iter=500)
+    v = np.random.default_rng(21).standard_normal(s.positions.shape) * 1e-3   # nm per call
+    warm_it, cold_it = [], []
+    with CudaCalcTholeDipoleForceKernel(s, precision=precision, warm_start=True) as kw, \
+            CudaCalcTholeDipoleForceKernel(s, precision=precision) as kc:
+        for step in range(6):
+            p = s.positions + step * v
+            ew, fw = kw.execute(p)
+            ec, fc = kc.execute(p)
+            warm_it.append(kw.solverStats()["iterations"])
+            cold_it.append(kc.solverStats()["iterations"])
+            assert kw.solverStats()["converged"]
+            # (No dipole query on kw here: a query at the same positions is a
+            # call of its own and would become the predictor's last point.)
+            assert rel_rms(fw, fc) < 1e-5
+            # The pair energy is first order in the dipoles, and the two solves
+            # stop at different points inside the 1e-8 tolerance; the mixed
+            # form adds the FP32 rounding of its pair sums on a small total
+            # (about 1.04 in the reference's Coulomb-prefactor-1 units).
+            assert rel_err(ew, ec) < (1e-6 if precision == "double" else 1e-5)
+    # Calls 3.. start from the extrapolated guess: fewer iterations than from
+    # the constant guess of call 2, which needs fewer than a cold start.
+    assert warm_it[1] < cold_it[1], (warm_it, cold_it)
+    assert max(warm_it[2:]) < warm_it[1], (warm_it, cold_it)

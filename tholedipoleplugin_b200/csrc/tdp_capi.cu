@@ -72,6 +72,7 @@ struct tdp_handle {
     double* d_stage = nullptr;  // device staging for host FP32 positions / query inputs
     size_t stage_bytes = 0;
     bool mu_prev_valid = false;
+    bool mu_prev2_valid = false;
     bool have_results = false;
 
     int iterations = 0;
@@ -508,14 +509,24 @@ void setup_and_solve(tdp_handle* h) {
             solve_jacobi<R>(h);
         } else {
             if ((h->flags & TDP_FLAG_WARM_START) && h->mu_prev_valid) {
-                TDP_CUDA(cudaMemcpyAsync(d.mu, d.mu_prev, sizeof(double) * 3 * h->n, cudaMemcpyDeviceToDevice, st));
+                // Linear extrapolation from the last two solutions when both
+                // exist (an O(dt^2) guess along a trajectory), else the last one.
+                if (h->mu_prev2_valid) {
+                    launch_predict(d, st);
+                } else {
+                    TDP_CUDA(cudaMemcpyAsync(d.mu, d.mu_prev, sizeof(double) * 3 * h->n, cudaMemcpyDeviceToDevice,
+                                             st));
+                }
                 launch_warm_start<R>(d, st);
-                h->launches++;
+                h->launches += h->mu_prev2_valid ? 2 : 1;
             }
             solve_cg<R>(h);
         }
+        const bool ok = h->status == TDP_STATUS_CONVERGED;
+        std::swap(d.mu_prev, d.mu_prev2);
         TDP_CUDA(cudaMemcpyAsync(d.mu_prev, d.mu, sizeof(double) * 3 * h->n, cudaMemcpyDeviceToDevice, st));
-        h->mu_prev_valid = h->status == TDP_STATUS_CONVERGED;
+        h->mu_prev2_valid = ok && h->mu_prev_valid;
+        h->mu_prev_valid = ok;
     } else {
         solve_extrapolated<R>(h);
     }
@@ -900,6 +911,7 @@ int tdp_create(const tdp_system_desc* desc, tdp_handle** out) {
         d.E = dalloc<double>(n3, o);
         d.mu = dalloc<double>(n3, o);
         d.mu_prev = dalloc<double>(n3, o);
+        d.mu_prev2 = dalloc<double>(n3, o);
         d.y = dalloc<double>(n3, o);
         d.r = dalloc<double>(n3, o);
         d.p = dalloc<double>(n3, o);
@@ -1023,6 +1035,7 @@ int tdp_update_params(tdp_handle* h, int32_t num_particles, const double* charge
         TDP_CUDA(cudaStreamSynchronize(h->stream));
         upload_params(h);
         h->mu_prev_valid = false;
+        h->mu_prev2_valid = false;
         h->have_results = false;
     } catch (const TdpError& e) {
         return fail(h, e);

@@ -219,6 +219,13 @@ __global__ void k_warm_start(int n, const int* __restrict__ rank, const double* 
     store_vec<R>(vec, rank[i], m, thole[i]);
 }
 
+// Starting point extrapolated from the last two solutions: mu = 2 mu1 - mu2.
+__global__ void k_predict(size_t n3, const double* __restrict__ mu1, const double* __restrict__ mu2,
+                          double* __restrict__ mu) {
+    const size_t k = blockIdx.x * (size_t)blockDim.x + threadIdx.x;
+    if (k < n3) mu[k] = 2.0 * mu1[k] - mu2[k];
+}
+
 // True residual in y-space: r = sqrt(alpha)*(E + T mu) - y, with mu = sqrt(alpha)*y.
 // p = r, packs sqrt(alpha)*p; block partials of r.r and sum alpha|r|^2.
 template <class R>
@@ -617,6 +624,10 @@ void launch_fixed_done(const Dev& d, cudaStream_t st) {
     k_fixed_done<R><<<nblk(d.n, kVecThreads), kVecThreads, 0, st>>>(d.n, d.rank, d.nsplit, d.n_pad, d.partial, d.alpha,
                                                                      d.salpha, d.thole, d.E, d.mu, d.y,
                                                                      (typename Vec4T<R>::type*)d.vec_s);
+}
+void launch_predict(const Dev& d, cudaStream_t st) {
+    const size_t n3 = 3 * (size_t)d.n;
+    k_predict<<<nblk(n3, kVecThreads), kVecThreads, 0, st>>>(n3, d.mu_prev, d.mu_prev2, d.mu);
 }
 template <class R>
 void launch_warm_start(const Dev& d, cudaStream_t st) {

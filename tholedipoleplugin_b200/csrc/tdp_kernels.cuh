@@ -56,7 +56,8 @@ struct Dev {
     double* lab = nullptr;
     double* E = nullptr;
     double* mu = nullptr;
-    double* mu_prev = nullptr;
+    double* mu_prev = nullptr;   // the previous call's converged dipoles
+    double* mu_prev2 = nullptr;  // and the call before's (warm-start predictor)
     double* y = nullptr;
     double* r = nullptr;
     double* p = nullptr;
@@ -90,6 +91,7 @@ template <class R> void launch_field(const Dev& d, int kind, cudaStream_t st);
 template <class R> void launch_energy(const Dev& d, cudaStream_t st);
 template <class R> void launch_fixed_done(const Dev& d, cudaStream_t st);
 template <class R> void launch_warm_start(const Dev& d, cudaStream_t st);
+void launch_predict(const Dev& d, cudaStream_t st);
 template <class R> void launch_cg_residual(const Dev& d, cudaStream_t st);
 void launch_cg_q(const Dev& d, cudaStream_t st);
 void launch_cg_update(const Dev& d, int slot, cudaStream_t st);
