@@ -614,7 +614,7 @@ def run_ours(args):
     hmd.close()
     out["e2e"] = {"value": world * K_e2e / t_e2e * NS_PER_DAY, "unit": "ns/day", "h2d_bytes_per_step": n * 3 * 8,
                   "d2h_bytes_per_step": n * 3 * 8 + 8, "steps": K_e2e,
-                  "what": "host numpy velocity Verlet + SHAKE/RATTLE; tdp_compute on pinned host positions/forces"}
+                  "what": "host velocity Verlet + SHAKE/RATTLE (tdp_md_host_*, host threads); tdp_compute on pinned host positions/forces"}
 
     # ---- plain (FP64) form, same MD -------------------------------------------------
     K_pl = max(3, K // 4)

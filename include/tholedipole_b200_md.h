@@ -35,6 +35,16 @@ int tdp_md_kick(int32_t num_waters, double d_oh, double d_hh, double m_o, double
 int tdp_md_constrain_velocities(int32_t num_waters, double d_oh, double d_hh, double m_o, double m_h,
                                 const double* positions, double* velocities, void* stream);
 
+/* The same two half steps on HOST arrays (positions, velocities, forces of
+ * n*3 doubles in host memory), for an integrator loop that hands host
+ * positions to tdp_compute each step.  Runs on host threads (up to 16, each
+ * over its own range of waters); no CUDA call.  forces may be NULL in
+ * tdp_md_host_kick (RATTLE only). */
+int tdp_md_host_kick_drift(int32_t num_waters, double d_oh, double d_hh, double m_o, double m_h, double dt,
+                           double* positions, double* velocities, const double* forces);
+int tdp_md_host_kick(int32_t num_waters, double d_oh, double d_hh, double m_o, double m_h, double dt,
+                     const double* positions, double* velocities, const double* forces);
+
 /* Kinetic energy sum(m v^2)/2 into *out (device double), for the temperature. */
 int tdp_md_kinetic_energy(int32_t num_waters, double m_o, double m_h, const double* velocities, double* out,
                           void* stream);

@@ -1,6 +1,7 @@
-"""Host-side rigid-water constraints of the e2e MD loop (tholedipoleplugin_b200/md.py):
-matrix SHAKE (Newton on each water's three constraints) and RATTLE (one 3x3
-solve per water), CPU only."""
+"""Host-side rigid-water half steps of the e2e MD loop (tdp_md_host_kick_drift /
+tdp_md_host_kick through tholedipoleplugin_b200/md.py), CPU only: the library's
+per-water SHAKE/RATTLE on host threads against a numpy restatement of classic
+SHAKE, constraint satisfaction and momentum conservation."""
 import numpy as np
 
 from tholedipoleplugin_b200 import md as M
@@ -27,40 +28,55 @@ def _iterative_shake(x0, x, v, dt, iters=2000, tol=1e-14):
             return
 
 
-def _step(seed=0):
-    s = S.water_box(4, 1.242, seed=seed)
+def _state(n_side=4, box=1.242, seed=0):
+    s = S.water_box(n_side, box, seed=seed)
     nw = s.n // 3
-    x = s.positions.copy()
+    x = np.ascontiguousarray(s.positions.copy())
     v = M.maxwell_boltzmann(nw, 300.0, seed)
-    M._rattle_host(x, v)
+    M.host_kick(x, v, None, 0.0)
     f = np.random.default_rng(seed).standard_normal((s.n, 3)) * 100.0
-    inv_m = 1.0 / np.tile([M.MASS_O, M.MASS_H, M.MASS_H], nw)[:, None]
-    dt = 0.002
-    v = v + 0.5 * dt * f * inv_m
-    x0 = x.copy()
-    x = x + dt * v
-    return x0, x, v, dt
+    return x, v, f, 0.002
 
 
-def test_shake_restores_bonds_and_matches_iterative_shake():
-    x0, x, v, dt = _step()
+def test_kick_drift_matches_classic_shake():
+    x, v, f, dt = _state()
+    inv_m = 1.0 / np.tile([M.MASS_O, M.MASS_H, M.MASS_H], x.shape[0] // 3)[:, None]
     xa, va = x.copy(), v.copy()
-    M._shake_host(x0, xa, va, dt)
+    M.host_kick_drift(xa, va, f, dt)
     L = np.sqrt((M._bonds(xa.reshape(-1, 3, 3)) ** 2).sum(-1))
-    assert np.abs(L - M._D[None, :]).max() < 1e-13
-    xb, vb = x.copy(), v.copy()
-    _iterative_shake(x0, xb, vb, dt)
-    assert np.abs(xa - xb).max() < 1e-12
-    assert np.abs(va - vb).max() < 1e-9
+    assert np.abs(L - M._D[None, :]).max() < 1e-11
+    vb = v + 0.5 * dt * f * inv_m
+    xb = x + dt * vb
+    _iterative_shake(x, xb, vb, dt)
+    assert np.abs(xa - xb).max() < 1e-11
+    assert np.abs(va - vb).max() < 1e-8
 
 
 def test_constraint_forces_conserve_momentum():
-    x0, x, v, dt = _step(1)
+    x, v, f, dt = _state(seed=1)
+    f -= f.mean(0)   # no net external force
     m = np.tile([M.MASS_O, M.MASS_H, M.MASS_H], x.shape[0] // 3)[:, None]
     p0 = (m * v).sum(0)
-    M._shake_host(x0, x, v, dt)
-    M._rattle_host(x, v)
-    assert np.abs((m * v).sum(0) - p0).max() < 1e-10
+    M.host_kick_drift(x, v, f, dt)
+    M.host_kick(x, v, f, dt)
+    assert np.abs((m * v).sum(0) - p0).max() < 1e-9
     w = M._bonds(v.reshape(-1, 3, 3))
     s = M._bonds(x.reshape(-1, 3, 3))
-    assert np.abs(np.einsum("nkc,nkc->nk", s, w)).max() < 1e-12
+    assert np.abs(np.einsum("nkc,nkc->nk", s, w)).max() < 1e-10
+
+
+def test_threaded_equals_single_range():
+    # 4,000 waters split across host threads give the same result as the same
+    # waters stepped in small calls (one thread each).
+    x, v, f, dt = _state(16, 4.968, seed=2)
+    xa, va = x.copy(), v.copy()
+    M.host_kick_drift(xa, va, f, dt)
+    M.host_kick(xa, va, f, dt)
+    xb, vb = x.copy(), v.copy()
+    for r in range(0, x.shape[0], 300):
+        sl = slice(r, r + 300)
+        xs, vs, fs = xb[sl].copy(), vb[sl].copy(), f[sl].copy()
+        M.host_kick_drift(xs, vs, fs, dt)
+        M.host_kick(xs, vs, fs, dt)
+        xb[sl], vb[sl] = xs, vs
+    assert np.array_equal(xa, xb) and np.array_equal(va, vb)

@@ -86,6 +86,10 @@ PROTOTYPES = {
     "tdp_md_constrain_velocities": (C.c_int, [C.c_int32, C.c_double, C.c_double, C.c_double, C.c_double,
                                               C.c_void_p, C.c_void_p, C.c_void_p]),
     "tdp_md_kinetic_energy": (C.c_int, [C.c_int32, C.c_double, C.c_double, C.c_void_p, C.c_void_p, C.c_void_p]),
+    "tdp_md_host_kick_drift": (C.c_int, [C.c_int32, C.c_double, C.c_double, C.c_double, C.c_double, C.c_double,
+                                         C.c_void_p, C.c_void_p, C.c_void_p]),
+    "tdp_md_host_kick": (C.c_int, [C.c_int32, C.c_double, C.c_double, C.c_double, C.c_double, C.c_double,
+                                   C.c_void_p, C.c_void_p, C.c_void_p]),
     "tdp_batch_create": (C.c_int, [C.POINTER(SystemDesc), C.c_int32, _ip, C.POINTER(C.c_void_p)]),
     "tdp_batch_destroy": (None, [C.c_void_p]),
     "tdp_batch_last_error": (C.c_char_p, [C.c_void_p]),

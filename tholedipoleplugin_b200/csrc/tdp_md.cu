@@ -1,11 +1,18 @@
-// tdp_md.cu -- rigid-water velocity Verlet (RATTLE) kernels behind
-// include/tholedipole_b200_md.h.  One thread per water; the three distance
-// constraints are iterated (Gauss-Seidel SHAKE/RATTLE) to a relative
-// tolerance of 1e-12 with a fixed iteration cap, so every loop is bounded.
+// tdp_md.cu -- rigid-water velocity Verlet (RATTLE) behind
+// include/tholedipole_b200_md.h: device kernels (one thread per water) and the
+// same per-water steps on host arrays (threads over ranges of waters).  The
+// three distance constraints are iterated (Gauss-Seidel SHAKE/RATTLE) to a
+// relative tolerance of 1e-12 with a fixed iteration cap, so every loop is
+// bounded.
 #include "tholedipole_b200.h"
 #include "tholedipole_b200_md.h"
 
 #include <cuda_runtime.h>
+
+#include <algorithm>
+#include <cmath>
+#include <thread>
+#include <vector>
 
 namespace {
 
@@ -16,21 +23,22 @@ struct W {
     double x[3][3];
 };
 
-__device__ __forceinline__ void load(const double* a, int w, W& o) {
+__host__ __device__ inline void load(const double* a, int w, W& o) {
     for (int k = 0; k < 3; k++)
         for (int c = 0; c < 3; c++) o.x[k][c] = a[9 * w + 3 * k + c];
 }
-__device__ __forceinline__ void store(double* a, int w, const W& o) {
+__host__ __device__ inline void store(double* a, int w, const W& o) {
     for (int k = 0; k < 3; k++)
         for (int c = 0; c < 3; c++) a[9 * w + 3 * k + c] = o.x[k][c];
 }
 
-__constant__ int kPair[3][2] = {{0, 1}, {0, 2}, {1, 2}};
+// Constraint p joins atoms (0, 1), (0, 2), (1, 2).
+__host__ __device__ inline int pair_a(int p) { return p == 2 ? 1 : 0; }
+__host__ __device__ inline int pair_b(int p) { return p == 0 ? 1 : 2; }
 
-__global__ void k_kick_drift(int nw, double doh, double dhh, double mo, double mh, double dt, double* pos,
-                             double* vel, const double* frc) {
-    int w = blockIdx.x * blockDim.x + threadIdx.x;
-    if (w >= nw) return;
+// One water: v += dt/2 F/m, x += dt v, SHAKE along the pre-drift bonds.
+__host__ __device__ inline void kick_drift_one(int w, double doh, double dhh, double mo, double mh, double dt,
+                                               double* pos, double* vel, const double* frc) {
     W x0, v, f;
     load(pos, w, x0);
     load(vel, w, v);
@@ -47,7 +55,7 @@ __global__ void k_kick_drift(int nw, double doh, double dhh, double mo, double m
     for (int it = 0; it < kMaxConstraintIter; it++) {
         bool done = true;
         for (int p = 0; p < 3; p++) {
-            int a = kPair[p][0], b = kPair[p][1];
+            const int a = pair_a(p), b = pair_b(p);
             double s[3], r0[3];
             for (int c = 0; c < 3; c++) {
                 s[c] = x.x[a][c] - x.x[b][c];
@@ -71,11 +79,11 @@ __global__ void k_kick_drift(int nw, double doh, double dhh, double mo, double m
     store(vel, w, v);
 }
 
-__device__ void rattle(const W& x, W& v, const double inv[3], const double d2[3]) {
+__host__ __device__ inline void rattle(const W& x, W& v, const double inv[3], const double d2[3]) {
     for (int it = 0; it < kMaxConstraintIter; it++) {
         bool done = true;
         for (int p = 0; p < 3; p++) {
-            int a = kPair[p][0], b = kPair[p][1];
+            const int a = pair_a(p), b = pair_b(p);
             double r[3], dv[3];
             for (int c = 0; c < 3; c++) {
                 r[c] = x.x[a][c] - x.x[b][c];
@@ -94,10 +102,9 @@ __device__ void rattle(const W& x, W& v, const double inv[3], const double d2[3]
     }
 }
 
-__global__ void k_kick(int nw, double doh, double dhh, double mo, double mh, double dt, const double* pos,
-                       double* vel, const double* frc) {
-    int w = blockIdx.x * blockDim.x + threadIdx.x;
-    if (w >= nw) return;
+// One water: v += dt/2 F/m (frc may be null), then RATTLE.
+__host__ __device__ inline void kick_one(int w, double doh, double dhh, double mo, double mh, double dt,
+                                         const double* pos, double* vel, const double* frc) {
     W x, v, f;
     load(pos, w, x);
     load(vel, w, v);
@@ -110,6 +117,20 @@ __global__ void k_kick(int nw, double doh, double dhh, double mo, double mh, dou
     }
     rattle(x, v, inv, d2);
     store(vel, w, v);
+}
+
+__global__ void k_kick_drift(int nw, double doh, double dhh, double mo, double mh, double dt, double* pos,
+                             double* vel, const double* frc) {
+    int w = blockIdx.x * blockDim.x + threadIdx.x;
+    if (w >= nw) return;
+    kick_drift_one(w, doh, dhh, mo, mh, dt, pos, vel, frc);
+}
+
+__global__ void k_kick(int nw, double doh, double dhh, double mo, double mh, double dt, const double* pos,
+                       double* vel, const double* frc) {
+    int w = blockIdx.x * blockDim.x + threadIdx.x;
+    if (w >= nw) return;
+    kick_one(w, doh, dhh, mo, mh, dt, pos, vel, frc);
 }
 
 __global__ void k_kinetic(int nw, double mo, double mh, const double* vel, double* out) {
@@ -131,6 +152,27 @@ __global__ void k_kinetic(int nw, double mo, double mh, const double* vel, doubl
         __syncthreads();
     }
     if (threadIdx.x == 0) atomicAdd(out, red[0]);
+}
+
+// Host loop over waters, split across up to 16 threads (each water independent).
+template <class F>
+void host_each(int nw, F&& fn) {
+    unsigned hw = std::thread::hardware_concurrency();
+    int nt = (int)std::max(1u, std::min(16u, hw ? hw : 1u));
+    nt = std::min(nt, std::max(1, nw / 1024));
+    if (nt <= 1) {
+        for (int w = 0; w < nw; w++) fn(w);
+        return;
+    }
+    std::vector<std::thread> th;
+    th.reserve(nt);
+    for (int t = 0; t < nt; t++) {
+        const int w0 = (int)((long long)nw * t / nt), w1 = (int)((long long)nw * (t + 1) / nt);
+        th.emplace_back([w0, w1, &fn] {
+            for (int w = w0; w < w1; w++) fn(w);
+        });
+    }
+    for (auto& t : th) t.join();
 }
 
 int status(cudaError_t e) { return e == cudaSuccess ? TDP_OK : TDP_ERR_CUDA; }
@@ -161,6 +203,20 @@ int tdp_md_constrain_velocities(int32_t nw, double doh, double dhh, double mo, d
     if (nw == 0) return TDP_OK;
     k_kick<<<(nw + 127) / 128, 128, 0, (cudaStream_t)stream>>>(nw, doh, dhh, mo, mh, 0.0, pos, vel, nullptr);
     return status(cudaGetLastError());
+}
+
+int tdp_md_host_kick_drift(int32_t nw, double doh, double dhh, double mo, double mh, double dt, double* pos,
+                           double* vel, const double* frc) {
+    if (nw < 0 || !pos || !vel || !frc) return TDP_ERR_INVALID_ARGUMENT;
+    host_each(nw, [=](int w) { kick_drift_one(w, doh, dhh, mo, mh, dt, pos, vel, frc); });
+    return TDP_OK;
+}
+
+int tdp_md_host_kick(int32_t nw, double doh, double dhh, double mo, double mh, double dt, const double* pos,
+                     double* vel, const double* frc) {
+    if (nw < 0 || !pos || !vel) return TDP_ERR_INVALID_ARGUMENT;
+    host_each(nw, [=](int w) { kick_one(w, doh, dhh, mo, mh, dt, pos, vel, frc); });
+    return TDP_OK;
 }
 
 int tdp_md_kinetic_energy(int32_t nw, double mo, double mh, const double* vel, double* out, void* stream) {

@@ -44,68 +44,28 @@ _D = np.array([D_OH, D_OH, D_HH])
 _INV_M = np.array([1.0 / MASS_O, 1.0 / MASS_H, 1.0 / MASS_H])
 
 
-def _coupling() -> np.ndarray:
-    """K[k, l]: how a multiplier of constraint l moves the bond vector of constraint k
-    (x_a += g_l c_{a,l} r_l / m_a with c = +1 for the first atom of l, -1 for the second)."""
-    c = np.zeros((3, 3))
-    for l, (a, b) in enumerate(_PAIRS):
-        c[a, l] = 1.0
-        c[b, l] = -1.0
-    K = np.zeros((3, 3))
-    for k, (a, b) in enumerate(_PAIRS):
-        K[k] = c[a] * _INV_M[a] - c[b] * _INV_M[b]
-    return K
-
-
-_K = _coupling()
-
-
 def _bonds(xw: np.ndarray) -> np.ndarray:
     """(nw, 3 constraints, 3) bond vectors x_a - x_b."""
     return np.stack([xw[:, a] - xw[:, b] for a, b in _PAIRS], axis=1)
 
 
-def _apply(xw: np.ndarray, g: np.ndarray, r: np.ndarray, scale: float = 1.0) -> None:
-    """x_a += scale g_l c_{a,l} r_l / m_a for the three constraints of every water."""
-    for l, (a, b) in enumerate(_PAIRS):
-        d = (scale * g[:, l])[:, None] * r[:, l]
-        xw[:, a] += _INV_M[a] * d
-        xw[:, b] -= _INV_M[b] * d
+def host_kick_drift(pos: np.ndarray, vel: np.ndarray, frc: np.ndarray, dt: float) -> None:
+    """v += dt/2 F/m, x += dt v, SHAKE back onto the rigid-water constraints
+    (tdp_md_host_kick_drift: the device step's arithmetic on host threads)."""
+    for a in (pos, vel, frc):
+        assert a.dtype == np.float64 and a.flags.c_contiguous
+    A.check(A.lib().tdp_md_host_kick_drift(pos.shape[0] // 3, D_OH, D_HH, MASS_O, MASS_H, dt,
+                                           pos.ctypes.data_as(C.c_void_p), vel.ctypes.data_as(C.c_void_p),
+                                           frc.ctypes.data_as(C.c_void_p)), None)
 
 
-def _rattle_host(x: np.ndarray, v: np.ndarray, iters: int = 200, tol: float = 1e-12) -> None:
-    """Project water velocities onto the rigid constraints (numpy, in place): the
-    three conditions s_k.(v_a - v_b) = 0 are linear in the multipliers, one 3x3
-    solve per water."""
-    xw = x.reshape(-1, 3, 3)
-    vw = v.reshape(-1, 3, 3)
-    s = _bonds(xw)
-    w = _bonds(vw)
-    A = _K[None, :, :] * np.einsum("nkc,nlc->nkl", s, s)
-    rhs = -np.einsum("nkc,nkc->nk", s, w)
-    h = np.linalg.solve(A, rhs[..., None])[..., 0]
-    _apply(vw, h, s)
-
-
-def _shake_host(x0: np.ndarray, x: np.ndarray, v: np.ndarray, dt: float, iters: int = 50, tol: float = 1e-12):
-    """Positions onto the rigid constraints (SHAKE with the old bond vectors r0),
-    solving each water's three constraints together by Newton's method, with the
-    matching velocity correction (numpy, in place)."""
-    x0w = x0.reshape(-1, 3, 3)
-    xw = x.reshape(-1, 3, 3)
-    vw = v.reshape(-1, 3, 3)
-    r0 = _bonds(x0w)
-    s_free = _bonds(xw)
-    g = np.zeros((xw.shape[0], 3))
-    for _ in range(iters):
-        s = s_free + np.einsum("kl,nl,nlc->nkc", _K, g, r0)
-        sig = np.einsum("nkc,nkc->nk", s, s) - _D[None, :] ** 2
-        if not sig.size or float(np.max(np.abs(sig) / _D[None, :] ** 2)) < tol:
-            break
-        J = 2.0 * _K[None, :, :] * np.einsum("nkc,nlc->nkl", s, r0)
-        g -= np.linalg.solve(J, sig[..., None])[..., 0]
-    _apply(xw, g, r0)
-    _apply(vw, g, r0, 1.0 / dt)
+def host_kick(pos: np.ndarray, vel: np.ndarray, frc: Optional[np.ndarray], dt: float) -> None:
+    """v += dt/2 F/m (skipped for frc None), then RATTLE (tdp_md_host_kick)."""
+    for a in (pos, vel) + ((frc,) if frc is not None else ()):
+        assert a.dtype == np.float64 and a.flags.c_contiguous
+    fp = frc.ctypes.data_as(C.c_void_p) if frc is not None else None
+    A.check(A.lib().tdp_md_host_kick(pos.shape[0] // 3, D_OH, D_HH, MASS_O, MASS_H, dt,
+                                     pos.ctypes.data_as(C.c_void_p), vel.ctypes.data_as(C.c_void_p), fp), None)
 
 
 class DeviceRigidWaterMD:
@@ -172,7 +132,8 @@ class DeviceRigidWaterMD:
 
 class HostRigidWaterMD:
     """The same integrator as a user-level loop over host arrays: each step
-    hands host positions to the C ABI and reads forces back."""
+    hands host positions to the C ABI and reads forces back.  The half steps
+    (kick, drift, SHAKE/RATTLE) run on host threads (tdp_md_host_*)."""
 
     def __init__(self, system: TholeSystem, precision="mixed", dt: float = 0.001, temperature: float = 300.0,
                  seed: int = 0, warm_start: bool = True, pinned: Optional[np.ndarray] = None, ewald: bool = False):
@@ -184,22 +145,17 @@ class HostRigidWaterMD:
         if pinned is not None:
             self.pos[...] = system.positions
         self.vel = maxwell_boltzmann(self.nw, temperature, seed)
-        self.inv_m = 1.0 / np.tile([MASS_O, MASS_H, MASS_H], self.nw)[:, None]
-        _rattle_host(self.pos, self.vel)
+        host_kick(self.pos, self.vel, None, 0.0)
         self.frc = np.zeros((self.n, 3))
         self.energy, _ = self.kernel.execute(self.pos, forces=self.frc)
         self.steps = 0
 
     def step(self, n: int = 1) -> float:
         for _ in range(n):
-            self.vel += 0.5 * self.dt * self.frc * self.inv_m
-            x0 = self.pos.copy()
-            self.pos += self.dt * self.vel
-            _shake_host(x0, self.pos, self.vel, self.dt)
+            host_kick_drift(self.pos, self.vel, self.frc, self.dt)
             self.frc[...] = 0.0
             self.energy, _ = self.kernel.execute(self.pos, forces=self.frc)
-            self.vel += 0.5 * self.dt * self.frc * self.inv_m
-            _rattle_host(self.pos, self.vel)
+            host_kick(self.pos, self.vel, self.frc, self.dt)
             self.steps += 1
         return self.energy
 
