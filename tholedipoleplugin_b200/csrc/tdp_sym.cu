@@ -1432,7 +1432,11 @@ __global__ void __launch_bounds__(kSymThreads, 3) k_energy_sym(
                 }
                 my[6] += (double)en;
             }
-            __syncthreads();
+            // Within a window of `stride` steps the warps' J tiles are
+            // disjoint ((t + warp * stride) % BT), so the shared J-side sums
+            // need a barrier only between windows; the windows' order fixes the
+            // order of the additions (deterministic).
+            if ((t + 1) % stride == 0 || t + 1 == BT) __syncthreads();
         }
         if (wact) {
             if (p == q) {
