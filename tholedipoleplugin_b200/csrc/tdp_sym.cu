@@ -999,8 +999,7 @@ __device__ __forceinline__ void energy_walk_x2(const PairParams& P, const double
     const float ti = di.w, iti = 1.0f / di.w;
     const f2 ITI = bc2(iti), ONE = bc2(1.0f), HALF = bc2(0.5f);
     const f2 RV4P = bc2(rv4p), RV4F = bc2(rv4f);
-    f2 Lx = 0, Ly = 0, Lz = 0, Ix = 0, Iy = 0, Iz = 0;
-    float tx = 0.f, ty = 0.f, tz = 0.f;
+    f2 Lx = 0, Ly = 0, Lz = 0, Ix = 0, Iy = 0, Iz = 0, NTx = 0, NTy = 0, NTz = 0;
     if (FOLD) {
         Lx = bc2(-(float)P.box[0]);
         Ly = bc2(-(float)P.box[1]);
@@ -1008,9 +1007,9 @@ __device__ __forceinline__ void energy_walk_x2(const PairParams& P, const double
         Ix = bc2((float)P.inv_box[0]);
         Iy = bc2((float)P.inv_box[1]);
         Iz = bc2((float)P.inv_box[2]);
-        tx = (float)P.half_box_tol[0];
-        ty = (float)P.half_box_tol[1];
-        tz = (float)P.half_box_tol[2];
+        NTx = bc2(-(float)(P.half_box_tol[0] * P.half_box_tol[0]));
+        NTy = bc2(-(float)(P.half_box_tol[1] * P.half_box_tol[1]));
+        NTz = bc2(-(float)(P.half_box_tol[2] * P.half_box_tol[2]));
     }
     f2 FX = 0, FY = 0, FZ = 0, TX = 0, TY = 0, TZ = 0, EN = 0;        // I side
     f2 GX = 0, GY = 0, GZ = 0, UX = 0, UY = 0, UZ = 0;                // J side (packed atoms m, m + 16)
@@ -1021,27 +1020,25 @@ __device__ __forceinline__ void energy_walk_x2(const PairParams& P, const double
         f2 DX = sub2(pk2(a.x, a.y), OX), DY = sub2(pk2(a.z, a.w), OY), DZ = sub2(pk2(b.x, b.y), OZ);
         const int ja = jbase + m, jb = ja + 16;
         if (FOLD) {
-            bool amb_a = false, amb_b = false;
-            float ax, bx, ay, by, az, bz;
+            // As in xslot_pairs: one sign-bit AND of the d^2 - t^2 words flags
+            // the pairs within the margin of half a box.
+            f2 neg = ~0ull;
             if (fm & 1u) {
                 DX = fold2(DX, Lx, Ix);
-                un2(DX, ax, bx);
-                amb_a = fabsf(ax) > tx;
-                amb_b = fabsf(bx) > tx;
+                neg &= fma2(DX, DX, NTx);
             }
             if (fm & 2u) {
                 DY = fold2(DY, Ly, Iy);
-                un2(DY, ay, by);
-                amb_a = amb_a || fabsf(ay) > ty;
-                amb_b = amb_b || fabsf(by) > ty;
+                neg &= fma2(DY, DY, NTy);
             }
             if (fm & 4u) {
                 DZ = fold2(DZ, Lz, Iz);
-                un2(DZ, az, bz);
-                amb_a = amb_a || fabsf(az) > tz;
-                amb_b = amb_b || fabsf(bz) > tz;
+                neg &= fma2(DZ, DZ, NTz);
             }
-            if (amb_a || amb_b) {
+            const f2 flag = ~neg & 0x8000000080000000ull;
+            if (flag) {
+                const bool amb_a = (flag >> 31) & 1ull, amb_b = (flag >> 63) != 0ull;
+                float ax, bx, ay, by, az, bz;
                 un2(DX, ax, bx);
                 un2(DY, ay, by);
                 un2(DZ, az, bz);
@@ -1131,9 +1128,9 @@ __device__ __forceinline__ void energy_walk_x2(const PairParams& P, const double
         dP = neg2(rv3);
         f2 dU = mul2(mul2(bc2(-2.0f), rv3), dtc);
         Vij0 = sub2(Vij0, fma2(eP, QJ1, mul2(eU, uJ0)));
-        f2 Vji1 = neg2(mul2(eP, QI0));
+        const f2 Vji1n = mul2(eP, QI0);   // -Vji1 so far (subtracted below: exact)
         VijR0 = sub2(VijR0, fma2(dP, QJ1, mul2(dU, uJ0)));
-        f2 VjiR1 = neg2(mul2(dP, QI0));
+        f2 VjiR1 = mul2(rv3, QI0);        // -(dP QI0), dP = -rv3: exact
         f2 Vjid0 = neg2(mul2(eU, QI0));
         f2 Vij1 = mul2(eP, QJ0);
         Vji0 = add2(Vji0, fma2(eP, QI1, mul2(eU, uI0)));
@@ -1145,7 +1142,7 @@ __device__ __forceinline__ void energy_walk_x2(const PairParams& P, const double
         dP = mul2(bc2(3.0f), rv4);
         dU = mul2(mul2(bc2(6.0f), rv4), dtd0);
         Vij1 = add2(Vij1, fma2(eP, QJ1, mul2(eU, uJ0)));
-        Vji1 = add2(Vji1, fma2(eP, QI1, mul2(eU, uI0)));
+        f2 Vji1 = sub2(fma2(eP, QI1, mul2(eU, uI0)), Vji1n);
         VijR1 = add2(VijR1, fma2(dP, QJ1, mul2(dU, uJ0)));
         VjiR1 = add2(VjiR1, fma2(dP, QI1, mul2(dU, uI0)));
         Vijd0 = fma2(eU, QJ1, Vijd0);
@@ -1190,22 +1187,23 @@ __device__ __forceinline__ void energy_walk_x2(const PairParams& P, const double
             fIZ = fma2(dC, uu, fIZ);
             fJZ = fma2(dC, uu, fJZ);
         }
-        const f2 qf0 = mul2(RINV, add2(add2(EIY, EJY), add2(iEIY, iEJY)));
-        const f2 qf1 = neg2(mul2(RINV, add2(add2(EIX, EJX), add2(iEIX, iEJX))));
-        const f2 qf2 = neg2(add2(fJZ, fIZ));
-        // Back rotation with the reference's permuted matrix.
-        const f2 fvx = fma2(YY, qf0, fma2(ZY, qf1, mul2(XY, qf2)));
-        const f2 fvy = fma2(YZ, qf0, fma2(ZZ, qf1, mul2(XZ, qf2)));
-        const f2 fvz = fma2(YX, qf0, fma2(ZX, qf1, mul2(XX, qf2)));
+        // nqf = -qf (the QI-frame force); every sign flip below is exact.
+        const f2 nqf0 = neg2(mul2(RINV, add2(add2(EIY, EJY), add2(iEIY, iEJY))));
+        const f2 nqf1 = mul2(RINV, add2(add2(EIX, EJX), add2(iEIX, iEJX)));
+        const f2 nqf2 = add2(fJZ, fIZ);
+        // Back rotation with the reference's permuted matrix: nfv = -fv.
+        const f2 nfvx = fma2(YY, nqf0, fma2(ZY, nqf1, mul2(XY, nqf2)));
+        const f2 nfvy = fma2(YZ, nqf0, fma2(ZZ, nqf1, mul2(XZ, nqf2)));
+        const f2 nfvz = fma2(YX, nqf0, fma2(ZX, nqf1, mul2(XX, nqf2)));
         {
             const f2 EIZ = sub2(mul2(QI2, Vij3), mul2(QI3, Vij2));
-            const f2 q0 = neg2(EIX), q1 = neg2(EIY), q2 = neg2(EIZ);
-            TX = add2(TX, fma2(YY, q0, fma2(ZY, q1, mul2(XY, q2))));
-            TY = add2(TY, fma2(YZ, q0, fma2(ZZ, q1, mul2(XZ, q2))));
-            TZ = add2(TZ, fma2(YX, q0, fma2(ZX, q1, mul2(XX, q2))));
-            FX = sub2(FX, fvx);
-            FY = sub2(FY, fvy);
-            FZ = sub2(FZ, fvz);
+            // Torque of the QI-frame vector -E_I, rotated back (sign folded into the sub).
+            TX = sub2(TX, fma2(YY, EIX, fma2(ZY, EIY, mul2(XY, EIZ))));
+            TY = sub2(TY, fma2(YZ, EIX, fma2(ZZ, EIY, mul2(XZ, EIZ))));
+            TZ = sub2(TZ, fma2(YX, EIX, fma2(ZX, EIY, mul2(XX, EIZ))));
+            FX = add2(FX, nfvx);
+            FY = add2(FY, nfvy);
+            FZ = add2(FZ, nfvz);
             f2 eq = fma2(QI0, Vij0, mul2(QJ0, Vji0));
             eq = fma2(QI1, Vij1, fma2(QJ1, Vji1, eq));
             eq = fma2(QI2, Vij2, fma2(QJ2, Vji2, eq));
@@ -1214,13 +1212,12 @@ __device__ __forceinline__ void energy_walk_x2(const PairParams& P, const double
         }
         {
             const f2 EJZ = sub2(mul2(QJ2, Vji3), mul2(QJ3, Vji2));
-            const f2 q0 = neg2(EJX), q1 = neg2(EJY), q2 = neg2(EJZ);
-            UX = add2(UX, fma2(YY, q0, fma2(ZY, q1, mul2(XY, q2))));
-            UY = add2(UY, fma2(YZ, q0, fma2(ZZ, q1, mul2(XZ, q2))));
-            UZ = add2(UZ, fma2(YX, q0, fma2(ZX, q1, mul2(XX, q2))));
-            GX = add2(GX, fvx);
-            GY = add2(GY, fvy);
-            GZ = add2(GZ, fvz);
+            UX = sub2(UX, fma2(YY, EJX, fma2(ZY, EJY, mul2(XY, EJZ))));
+            UY = sub2(UY, fma2(YZ, EJX, fma2(ZZ, EJY, mul2(XZ, EJZ))));
+            UZ = sub2(UZ, fma2(YX, EJX, fma2(ZX, EJY, mul2(XX, EJZ))));
+            GX = sub2(GX, nfvx);
+            GY = sub2(GY, nfvy);
+            GZ = sub2(GZ, nfvz);
         }
         // Rotate the packed J-side sums one lane (64-bit shuffles).
         GX = __shfl_sync(kFull, GX, nxt);
@@ -1371,17 +1368,46 @@ __global__ void __launch_bounds__(kSymThreads, 3) k_energy_sym(
             }
         }
         const EAtom<R> me = eatom<R>(pi, di, ui);
+        // FP32 form: the round's BT tile-pair geometries (FP64 arithmetic), one
+        // per lane, read by shuffles instead of every lane repeating each.
+        float gdx = 0.f, gdy = 0.f, gdz = 0.f;
+        unsigned gfl = 0u;
+        if constexpr (sizeof(R) == 4) {
+            if (wact && lane < BT) {
+                const TileGeom g0 = tile_geom(P, cA, eA, s_ctr[lane], s_ext[lane]);
+                gdx = (float)g0.dcx;
+                gdy = (float)g0.dcy;
+                gdz = (float)g0.dcz;
+                gfl = g0.fmask | (g0.fold ? 8u : 0u);
+            }
+        }
         for (int c = 0; c < 6; c++) my[c] = 0.0;
         for (int t = 0; t < BT; t++) {
             const int Jl = (t + warp * stride) % BT;
             const int J = q * BT + Jl;
             if (wact && J < P.n_tiles && (p != q || Jl >= Il)) {
                 const double4 cB = s_ctr[Jl];
-                const TileGeom g = tile_geom(P, cA, eA, cB, s_ext[Jl]);
-                R oix, oiy, oiz;
-                shift_into<R>(g, cA, cB, pi.x, pi.y, pi.z, oix, oiy, oiz);
                 const bool diag = I == J;
                 const bool slow = diag || (J == P.n_tiles - 1 && (P.n & 31)) || (J >= et.x && J <= et.y);
+                TileGeom g;
+                R oix, oiy, oiz;
+                if constexpr (sizeof(R) == 4) {
+                    const float dx = __shfl_sync(kFull, gdx, Jl), dy = __shfl_sync(kFull, gdy, Jl),
+                                dz = __shfl_sync(kFull, gdz, Jl);
+                    const unsigned fl = __shfl_sync(kFull, gfl, Jl);
+                    oix = pi.x - dx;
+                    oiy = pi.y - dy;
+                    oiz = pi.z - dz;
+                    if (slow) {
+                        g = tile_geom(P, cA, eA, cB, s_ext[Jl]);   // the partner walk's FP64 geometry
+                    } else {
+                        g.fmask = fl & 7u;
+                        g.fold = (fl >> 3) & 1u;
+                    }
+                } else {
+                    g = tile_geom(P, cA, eA, cB, s_ext[Jl]);
+                    shift_into<R>(g, cA, cB, pi.x, pi.y, pi.z, oix, oiy, oiz);
+                }
                 const int jbase = J * 32;
                 const V4* sp = s_pos + Jl * 32;
                 const V4* sd = s_dip + Jl * 32;
