@@ -65,7 +65,54 @@ BYTES_ENERGY_ATOM = 120
 SAMPLE_SIDE = 13
 
 
-def parse():
+class Ranks:
+    """Rank plumbing of one bench process under torchrun (RANK, WORLD_SIZE,
+    LOCAL_RANK, MASTER_ADDR/PORT): with more than one rank, a process group with
+    a short timeout (NCCL on the GPUs; gloo in the multi-process CPU test), a
+    barrier and the maximum of a host float over ranks.  The box workload is
+    replicated -- each rank integrates its own seeded box -- so nothing but these
+    timing reductions crosses ranks, and every rank takes them in the same order."""
+
+    def __init__(self, backend: str = "nccl", timeout_s: int = 600):
+        import torch
+        import torch.distributed as dist
+        self._dist = dist
+        self._torch = torch
+        self.rank = int(os.environ.get("RANK", "0"))
+        self.world = int(os.environ.get("WORLD_SIZE", "1"))
+        self.local = int(os.environ.get("LOCAL_RANK", "0"))
+        if backend == "nccl":
+            torch.cuda.set_device(self.local)
+            self.device = torch.device("cuda", self.local)
+        else:
+            self.device = torch.device("cpu")
+        if self.world > 1:
+            import datetime
+            kw = {"device_id": self.device} if backend == "nccl" else {}
+            dist.init_process_group(backend, timeout=datetime.timedelta(seconds=timeout_s), **kw)
+
+    def barrier(self) -> None:
+        if self.world > 1:
+            self._dist.barrier()
+
+    def max_over_ranks(self, x: float) -> float:
+        if self.world == 1:
+            return x
+        t = self._torch.tensor([x], dtype=self._torch.float64, device=self.device)
+        self._dist.all_reduce(t, op=self._dist.ReduceOp.MAX)
+        return float(t.item())
+
+    def close(self) -> None:
+        if self.world > 1:
+            self._dist.destroy_process_group()
+
+
+def box_seed(config: str, rank: int) -> int:
+    """Seed of rank's replica of the box (each rank integrates a different box)."""
+    return {"small": 0, "medium": 1, "profile": 5, "large": 2}[config] + 100 * rank
+
+
+def parse(argv=None):
     p = argparse.ArgumentParser()
     p.add_argument("--gpus", type=int, default=1)
     p.add_argument("--steps", type=int, default=20)
@@ -76,7 +123,7 @@ def parse():
     p.add_argument("--no-extras", action="store_true", help="only the timed MD (used under ncu)")
     p.add_argument("--ewald-md", action="store_true",
                    help="profiling: the timed MD runs in the Ewald mode (with --no-extras)")
-    return p.parse_args()
+    return p.parse_args(argv)
 
 
 # ---------------------------------------------------------------------------
@@ -517,35 +564,19 @@ def ewald_section(system, K, W, stream, world, barrier, max_over_ranks, rank):
 def run_ours(args):
     import numpy as np
     import torch
-    import torch.distributed as dist
 
     from tholedipoleplugin_b200 import _capi as A
     from tholedipoleplugin_b200 import systems as S
     from tholedipoleplugin_b200.kernel import CudaCalcTholeDipoleForceKernel
     from tholedipoleplugin_b200.md import DeviceRigidWaterMD, HostRigidWaterMD
 
-    rank = int(os.environ.get("RANK", "0"))
-    world = int(os.environ.get("WORLD_SIZE", "1"))
-    local = int(os.environ.get("LOCAL_RANK", "0"))
-    torch.cuda.set_device(local)
-    if world > 1:
-        import datetime
-        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=600), device_id=torch.device("cuda", local))
-
-    def barrier():
-        if world > 1:
-            dist.barrier()
-
-    def max_over_ranks(x: float) -> float:
-        if world == 1:
-            return x
-        t = torch.tensor([x], dtype=torch.float64, device="cuda")
-        dist.all_reduce(t, op=dist.ReduceOp.MAX)
-        return float(t.item())
+    ranks = Ranks("nccl")
+    rank, world, local = ranks.rank, ranks.world, ranks.local
+    barrier, max_over_ranks = ranks.barrier, ranks.max_over_ranks
 
     make = {"small": S.config_small, "medium": S.config_medium, "large": S.config_large,
             "profile": lambda seed: S.water_box(24, 9.936 * 24 / 32, seed=seed, cutoff=0.9)}[args.config]
-    system = make(seed={"small": 0, "medium": 1, "profile": 5, "large": 2}[args.config] + 100 * rank)
+    system = make(seed=box_seed(args.config, rank))
     n = system.n
     pairs = n * (n - 1) / 2
     K, W = args.steps, args.warmup
@@ -596,8 +627,7 @@ def run_ours(args):
     if args.no_extras:
         if rank == 0:
             print(json.dumps(out), flush=True)
-        if world > 1:
-            dist.destroy_process_group()
+        ranks.close()
         return
 
     # ---- e2e: the public C ABI with host buffers --------------------------------------
@@ -754,8 +784,7 @@ def run_ours(args):
             out["cpu_baseline"] = cpu_baseline_single(n, sweeps)
         print(json.dumps(out), flush=True)
     barrier()
-    if world > 1:
-        dist.destroy_process_group()
+    ranks.close()
 
 
 def main():
