@@ -81,6 +81,7 @@ __host__ __device__ inline size_t batch_smem(int M, int X, int korder) {
     typedef typename Vec4T<R>::type V4;
     size_t b = 0;
     b += sizeof(double) * ((size_t)M * (3 + 3 + 3 + 1 + 1 + work_slots(korder)) + 64);
+    b += sizeof(unsigned long long) * (size_t)M;   // exception-partner window masks
     b = align_up(b, 32);
     b += sizeof(V4) * 3 * (size_t)M;
     b = align_up(b, 16);
@@ -95,6 +96,9 @@ template <class R>
 struct Cl {
     typedef typename Vec4T<R>::type V4;
     double *pos, *E, *mu, *alpha, *salpha, *w, *red;
+    // Exception partners of atom i by offset: bit d (d < 63) set if atom
+    // i + d - 32 is listed, bit 63 set if a partner lies outside that window.
+    unsigned long long* emask;
     V4 *posq, *dipt, *vec;
     int4* axis;
     int *eoff, *ej;
@@ -115,6 +119,8 @@ __device__ Cl<R> carve(char* base, int M, int X, int korder) {
     c.salpha = d; d += M;
     c.w = d; d += (size_t)work_slots(korder) * M;
     c.red = d; d += 64;
+    c.emask = reinterpret_cast<unsigned long long*>(d);
+    d += M;
     size_t off = align_up((size_t)(reinterpret_cast<char*>(d) - base), 32);
     V4* v = reinterpret_cast<V4*>(base + off);
     c.posq = v; v += M;
@@ -167,11 +173,15 @@ __device__ __forceinline__ Groups groups(int n, int lmax) {
     return q;
 }
 
-// (M, I) scales of the pair (i, j) from i's local exception list.
+// (M, I) scales of the pair (i, j) from i's local exception list, scanned
+// only when i's partner mask says j can be on it.
 template <class R>
 __device__ __forceinline__ void pair_scales(const Cl<R>& c, int i, int j, R& m, R& s) {
     m = R(1);
     s = R(1);
+    const unsigned long long w = c.emask[i];
+    const unsigned d = (unsigned)(j - i + 32);
+    if (d < 63u ? ((w >> d) & 1ull) == 0ull : (w >> 63) == 0ull) return;
     for (int e = c.eoff[i]; e < c.eoff[i + 1]; e++)
         if (c.ej[e] == j) {
             m = c.em[e];
@@ -286,11 +296,16 @@ __global__ void __launch_bounds__(512) k_batch(BatchArgs A) {
             c.alpha[i] = al;
             c.salpha[i] = al > 0.0 ? sqrt(al) : 0.0;
             c.eoff[i] = A.exc_off[gi] - e0;
+            unsigned long long w = 0ull;
             for (int e = A.exc_off[gi]; e < A.exc_off[gi + 1]; e++) {
-                c.ej[e - e0] = A.exc_j[e] - a0;
+                const int j = A.exc_j[e] - a0;
+                c.ej[e - e0] = j;
                 c.em[e - e0] = (R)A.exc_m[e];
                 c.es[e - e0] = (R)A.exc_s[e];
+                const unsigned d = (unsigned)(j - i + 32);
+                w |= d < 63u ? 1ull << d : 1ull << 63;
             }
+            c.emask[i] = w;
         }
         if (threadIdx.x == 0) c.eoff[n] = A.exc_off[a0 + n] - e0;
         cx = bsum(cx, c.red) / n;
