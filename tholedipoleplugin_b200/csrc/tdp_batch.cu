@@ -152,6 +152,27 @@ __device__ __forceinline__ double bsum(double v, double* red) {
     return s;
 }
 
+// Two block sums in one pass (one pair of barriers), each in the fixed order of bsum.
+__device__ __forceinline__ void bsum2(double& a, double& b, double* red) {
+    a = warp_sum(a);
+    b = warp_sum(b);
+    const int lane = threadIdx.x & 31, w = threadIdx.x >> 5;
+    __syncthreads();
+    if (lane == 0) {
+        red[w] = a;
+        red[32 + w] = b;
+    }
+    __syncthreads();
+    double sa = 0.0, sb = 0.0;
+    const int nw = blockDim.x >> 5;
+    for (int k = 0; k < nw; k++) {
+        sa += red[k];
+        sb += red[32 + k];
+    }
+    a = sa;
+    b = sb;
+}
+
 template <class T>
 __device__ __forceinline__ T group_sum(T v, int L) {
     for (int o = L >> 1; o > 0; o >>= 1) v += __shfl_xor_sync(0xffffffffu, v, o);
@@ -249,8 +270,8 @@ __device__ double cg_residual(const Cl<R>& c, int n, const double* y, double* r,
         }
         set_vec(c, i, sa * p[3 * i], sa * p[3 * i + 1], sa * p[3 * i + 2]);
     }
-    rr = bsum(rr, c.red);
-    *ee = bsum(e2, c.red);
+    bsum2(rr, e2, c.red);
+    *ee = e2;
     return rr;
 }
 
@@ -440,8 +461,8 @@ __global__ void __launch_bounds__(512) k_batch(BatchArgs A) {
                     rr2 += rv * rv;
                     e2 += sa * sa * rv * rv;
                 }
-                rr2 = bsum(rr2, c.red);
-                eps = sqrt(bsum(e2, c.red) / n);
+                bsum2(rr2, e2, c.red);
+                eps = sqrt(e2 / n);
                 const double beta = rr2 / rr;
                 rr = rr2;
                 for (int i = threadIdx.x; i < n; i += blockDim.x) {
