@@ -168,9 +168,14 @@ void host_each(int nw, F&& fn) {
     th.reserve(nt);
     for (int t = 0; t < nt; t++) {
         const int w0 = (int)((long long)nw * t / nt), w1 = (int)((long long)nw * (t + 1) / nt);
-        th.emplace_back([w0, w1, &fn] {
+        try {
+            th.emplace_back([w0, w1, &fn] {
+                for (int w = w0; w < w1; w++) fn(w);
+            });
+        } catch (...) {
+            // No thread available: this range runs on the calling thread.
             for (int w = w0; w < w1; w++) fn(w);
-        });
+        }
     }
     for (auto& t : th) t.join();
 }
