@@ -82,6 +82,7 @@ __host__ __device__ inline size_t batch_smem(int M, int X, int korder) {
     size_t b = 0;
     b += sizeof(double) * ((size_t)M * (3 + 3 + 3 + 1 + 1 + work_slots(korder)) + 64);
     b += sizeof(unsigned long long) * (size_t)M;   // exception-partner window masks
+    b += sizeof(double) * 7 * 512;                  // per-thread partial sums of the pair passes
     b = align_up(b, 32);
     b += sizeof(V4) * 3 * (size_t)M;
     b = align_up(b, 16);
@@ -99,6 +100,7 @@ struct Cl {
     // Exception partners of atom i by offset: bit d (d < 63) set if atom
     // i + d - 32 is listed, bit 63 set if a partner lies outside that window.
     unsigned long long* emask;
+    double* part;   // 7 per thread: partial sums of the pair passes, reduced per atom in lane order
     V4 *posq, *dipt, *vec;
     int4* axis;
     int *eoff, *ej;
@@ -121,6 +123,8 @@ __device__ Cl<R> carve(char* base, int M, int X, int korder) {
     c.red = d; d += 64;
     c.emask = reinterpret_cast<unsigned long long*>(d);
     d += M;
+    c.part = d;
+    d += 7 * 512;
     size_t off = align_up((size_t)(reinterpret_cast<char*>(d) - base), 32);
     V4* v = reinterpret_cast<V4*>(base + off);
     c.posq = v; v += M;
@@ -173,25 +177,35 @@ __device__ __forceinline__ void bsum2(double& a, double& b, double* red) {
     b = sb;
 }
 
-template <class T>
-__device__ __forceinline__ T group_sum(T v, int L) {
-    for (int o = L >> 1; o > 0; o >>= 1) v += __shfl_xor_sync(0xffffffffu, v, o);
-    return v;
-}
 
-// Lane-group decomposition of the pair loops for an n-atom cluster.
-struct Groups {
-    int L, G, g, l;
+// Thread split of a pair pass over the atoms [base, base + na) of a cluster:
+// with T = min(blockDim.x, na * lmax) threads in use, atom base + a gets the
+// contiguous threads [first(a), first(a + 1)), first(a) = ceil(a T / na), so
+// every atom has floor(T / na) or one more lanes and all T threads work.
+// Each thread leaves K partial sums in part; split_sum adds an atom's lanes
+// in lane order (deterministic for a given CTA size and lmax).
+struct Split {
+    int a, l, L, T;
+    bool act;
 };
-__device__ __forceinline__ Groups groups(int n, int lmax) {
-    Groups q;
-    int L = 1;
-    while (L * 2 <= lmax && L * 2 * n <= (int)blockDim.x) L *= 2;
-    q.L = L;
-    q.G = blockDim.x / L;
-    q.g = threadIdx.x / L;
-    q.l = threadIdx.x % L;
+__device__ __forceinline__ int split_first(int a, int na, int T) { return (a * T + na - 1) / na; }
+__device__ __forceinline__ Split split(int na, int lmax) {
+    Split q;
+    q.T = min((int)blockDim.x, na * lmax);
+    const int t = threadIdx.x;
+    q.act = t < q.T;
+    q.a = q.act ? (t * na) / q.T : 0;
+    const int f0 = split_first(q.a, na, q.T);
+    q.l = t - f0;
+    q.L = split_first(q.a + 1, na, q.T) - f0;
     return q;
+}
+// Sum k of atom a (thread a < na calls it after a barrier).
+__device__ __forceinline__ double split_sum(const double* part, int K, int k, int a, int na, int T) {
+    const int f0 = split_first(a, na, T), f1 = split_first(a + 1, na, T);
+    double v = 0.0;
+    for (int u = f0; u < f1; u++) v += part[K * u + k];
+    return v;
 }
 
 // (M, I) scales of the pair (i, j) from i's local exception list, scanned
@@ -212,15 +226,17 @@ __device__ __forceinline__ void pair_scales(const Cl<R>& c, int i, int j, R& m, 
 
 // out[i] = sum_j I_ij T_ij v_j with v in c.vec (the mutual field of the operand).
 template <class R>
-__device__ void cluster_matvec(const Cl<R>& c, int n, const Groups& gp, R damp_r2, double* out) {
+__device__ void cluster_matvec(const Cl<R>& c, int n, int lmax, R damp_r2, double* out) {
     typedef typename Vec4T<R>::type V4;
-    for (int base = 0; base < n; base += gp.G) {
-        const int i = base + gp.g;
+    for (int base = 0; base < n; base += blockDim.x) {
+        const int na = min(n - base, (int)blockDim.x);
+        const Split sp = split(na, lmax);
+        const int i = base + sp.a;
         R fx = 0, fy = 0, fz = 0;
-        if (i < n) {
+        if (sp.act) {
             const V4 pi = c.posq[i];
             const R ti = c.vec[i].w;
-            for (int j = gp.l; j < n; j += gp.L) {
+            for (int j = sp.l; j < n; j += sp.L) {
                 if (j == i) continue;
                 R m, s;
                 pair_scales(c, i, j, m, s);
@@ -235,12 +251,15 @@ __device__ void cluster_matvec(const Cl<R>& c, int n, const Groups& gp, R damp_r
                 fz += s * tz;
             }
         }
-        double ax = group_sum((double)fx, gp.L), ay = group_sum((double)fy, gp.L), az = group_sum((double)fz, gp.L);
-        if (i < n && gp.l == 0) {
-            out[3 * i] = ax;
-            out[3 * i + 1] = ay;
-            out[3 * i + 2] = az;
-        }
+        double* pt = c.part + 3 * threadIdx.x;
+        pt[0] = (double)fx;
+        pt[1] = (double)fy;
+        pt[2] = (double)fz;
+        __syncthreads();
+        if ((int)threadIdx.x < na)
+            for (int k = 0; k < 3; k++)
+                out[3 * (base + threadIdx.x) + k] = split_sum(c.part, 3, k, threadIdx.x, na, sp.T);
+        __syncthreads();
     }
 }
 
@@ -299,7 +318,6 @@ __global__ void __launch_bounds__(512) k_batch(BatchArgs A) {
             }
             continue;
         }
-        const Groups gp = groups(n, A.lmax);
         const int e0 = A.exc_off[a0];
 
         // ---- load ------------------------------------------------------------------------
@@ -366,13 +384,15 @@ __global__ void __launch_bounds__(512) k_batch(BatchArgs A) {
         __syncthreads();
 
         // ---- permanent field (RTDF.cpp:678-746): E, mu = alpha E --------------------------
-        for (int base = 0; base < n; base += gp.G) {
-            const int i = base + gp.g;
+        for (int base = 0; base < n; base += blockDim.x) {
+            const int na = min(n - base, (int)blockDim.x);
+            const Split sp = split(na, A.lmax);
+            const int i = base + sp.a;
             R fx = 0, fy = 0, fz = 0;
-            if (i < n) {
+            if (sp.act) {
                 const V4 pi = c.posq[i];
                 const R ti = c.dipt[i].w;
-                for (int j = gp.l; j < n; j += gp.L) {
+                for (int j = sp.l; j < n; j += sp.L) {
                     if (j == i) continue;
                     R m, s;
                     pair_scales(c, i, j, m, s);
@@ -387,13 +407,15 @@ __global__ void __launch_bounds__(512) k_batch(BatchArgs A) {
                     fz += m * tz;
                 }
             }
-            const double ex = group_sum((double)fx, gp.L), ey = group_sum((double)fy, gp.L),
-                         ez = group_sum((double)fz, gp.L);
-            if (i < n && gp.l == 0) {
-                c.E[3 * i] = ex;
-                c.E[3 * i + 1] = ey;
-                c.E[3 * i + 2] = ez;
-            }
+            double* pt = c.part + 3 * threadIdx.x;
+            pt[0] = (double)fx;
+            pt[1] = (double)fy;
+            pt[2] = (double)fz;
+            __syncthreads();
+            if ((int)threadIdx.x < na)
+                for (int k = 0; k < 3; k++)
+                    c.E[3 * (base + threadIdx.x) + k] = split_sum(c.part, 3, k, threadIdx.x, na, sp.T);
+            __syncthreads();
         }
         __syncthreads();
         for (int i = threadIdx.x; i < n; i += blockDim.x) {
@@ -418,7 +440,7 @@ __global__ void __launch_bounds__(512) k_batch(BatchArgs A) {
             double* p = c.w + 6 * c.M;
             double* q = c.w + 9 * c.M;
             for (int k = threadIdx.x; k < n3; k += blockDim.x) y[k] = c.salpha[k / 3] * c.E[k];
-            cluster_matvec(c, n, gp, damp_r2, q);
+            cluster_matvec(c, n, A.lmax, damp_r2, q);
             __syncthreads();
             double ee;
             double rr = cg_residual(c, n, y, r, p, q, &ee);
@@ -434,7 +456,7 @@ __global__ void __launch_bounds__(512) k_batch(BatchArgs A) {
                         set_vec(c, i, sa * y[3 * i], sa * y[3 * i + 1], sa * y[3 * i + 2]);
                     }
                     __syncthreads();
-                    cluster_matvec(c, n, gp, damp_r2, q);
+                    cluster_matvec(c, n, A.lmax, damp_r2, q);
                     __syncthreads();
                     rr = cg_residual(c, n, y, r, p, q, &ee);
                     eps = sqrt(ee / n);
@@ -442,7 +464,7 @@ __global__ void __launch_bounds__(512) k_batch(BatchArgs A) {
                     continue;
                 }
                 __syncthreads();
-                cluster_matvec(c, n, gp, damp_r2, q);  // T S p
+                cluster_matvec(c, n, A.lmax, damp_r2, q);  // T S p
                 __syncthreads();
                 double pq = 0.0;
                 for (int k = threadIdx.x; k < n3; k += blockDim.x) {
@@ -482,7 +504,7 @@ __global__ void __launch_bounds__(512) k_batch(BatchArgs A) {
             for (int k = threadIdx.x; k < n3; k += blockDim.x) hist[k] = c.mu[k];
             for (int o = 1; o < A.korder; o++) {
                 __syncthreads();
-                cluster_matvec(c, n, gp, damp_r2, fld);
+                cluster_matvec(c, n, A.lmax, damp_r2, fld);
                 __syncthreads();
                 for (int i = threadIdx.x; i < n; i += blockDim.x) {
                     for (int k = 0; k < 3; k++) {
@@ -503,7 +525,7 @@ __global__ void __launch_bounds__(512) k_batch(BatchArgs A) {
                 set_vec(c, i, c.mu[3 * i], c.mu[3 * i + 1], c.mu[3 * i + 2]);
             }
             __syncthreads();
-            cluster_matvec(c, n, gp, damp_r2, fld);
+            cluster_matvec(c, n, A.lmax, damp_r2, fld);
             __syncthreads();
             double e2 = 0.0;
             for (int k = threadIdx.x; k < n3; k += blockDim.x) {
@@ -522,14 +544,16 @@ __global__ void __launch_bounds__(512) k_batch(BatchArgs A) {
         double* frc = c.w;
         double* trq = c.w + 3 * c.M;
         double en = 0.0;
-        for (int base = 0; base < n; base += gp.G) {
-            const int i = base + gp.g;
+        for (int base = 0; base < n; base += blockDim.x) {
+            const int na = min(n - base, (int)blockDim.x);
+            const Split sp = split(na, A.lmax);
+            const int i = base + sp.a;
             double f[6] = {0, 0, 0, 0, 0, 0};
-            if (i < n) {
+            if (sp.act) {
                 const V4 pi = c.posq[i], di = c.dipt[i], ui = c.vec[i];
                 const EAtom<R> me{pi.w, di.x, di.y, di.z, ui.x, ui.y, ui.z, di.w};
                 const double yi = c.pos[3 * i + 1], zi = c.pos[3 * i + 2];
-                for (int j = gp.l; j < n; j += gp.L) {
+                for (int j = sp.l; j < n; j += sp.L) {
                     if (j == i) continue;
                     R m, s;
                     pair_scales(c, i, j, m, s);
@@ -557,13 +581,17 @@ __global__ void __launch_bounds__(512) k_batch(BatchArgs A) {
                     en += e;
                 }
             }
-            for (int k = 0; k < 6; k++) f[k] = group_sum(f[k], gp.L);
-            if (i < n && gp.l == 0) {
+            double* pt = c.part + 6 * threadIdx.x;
+            for (int k = 0; k < 6; k++) pt[k] = f[k];
+            __syncthreads();
+            if ((int)threadIdx.x < na) {
+                const int a = base + threadIdx.x;
                 for (int k = 0; k < 3; k++) {
-                    frc[3 * i + k] = f[k];
-                    trq[3 * i + k] = f[3 + k];
+                    frc[3 * a + k] = split_sum(c.part, 6, k, threadIdx.x, na, sp.T);
+                    trq[3 * a + k] = split_sum(c.part, 6, 3 + k, threadIdx.x, na, sp.T);
                 }
             }
+            __syncthreads();
         }
         en = bsum(en, c.red);  // its barriers also order the frc/trq writes before the gather
 
