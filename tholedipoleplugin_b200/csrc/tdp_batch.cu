@@ -225,6 +225,7 @@ __device__ __forceinline__ void pair_scales(const Cl<R>& c, int i, int j, R& m, 
 }
 
 // out[i] = sum_j I_ij T_ij v_j with v in c.vec (the mutual field of the operand).
+// Ends with a CTA barrier: out is complete and visible on return.
 template <class R>
 __device__ void cluster_matvec(const Cl<R>& c, int n, int lmax, R damp_r2, double* out) {
     typedef typename Vec4T<R>::type V4;
@@ -441,7 +442,6 @@ __global__ void __launch_bounds__(512) k_batch(BatchArgs A) {
             double* q = c.w + 9 * c.M;
             for (int k = threadIdx.x; k < n3; k += blockDim.x) y[k] = c.salpha[k / 3] * c.E[k];
             cluster_matvec(c, n, A.lmax, damp_r2, q);
-            __syncthreads();
             double ee;
             double rr = cg_residual(c, n, y, r, p, q, &ee);
             eps = sqrt(ee / n);
@@ -457,7 +457,6 @@ __global__ void __launch_bounds__(512) k_batch(BatchArgs A) {
                     }
                     __syncthreads();
                     cluster_matvec(c, n, A.lmax, damp_r2, q);
-                    __syncthreads();
                     rr = cg_residual(c, n, y, r, p, q, &ee);
                     eps = sqrt(ee / n);
                     is_true = true;
@@ -465,7 +464,6 @@ __global__ void __launch_bounds__(512) k_batch(BatchArgs A) {
                 }
                 __syncthreads();
                 cluster_matvec(c, n, A.lmax, damp_r2, q);  // T S p
-                __syncthreads();
                 double pq = 0.0;
                 for (int k = threadIdx.x; k < n3; k += blockDim.x) {
                     const double qv = p[k] - c.salpha[k / 3] * q[k];
@@ -505,7 +503,6 @@ __global__ void __launch_bounds__(512) k_batch(BatchArgs A) {
             for (int o = 1; o < A.korder; o++) {
                 __syncthreads();
                 cluster_matvec(c, n, A.lmax, damp_r2, fld);
-                __syncthreads();
                 for (int i = threadIdx.x; i < n; i += blockDim.x) {
                     for (int k = 0; k < 3; k++) {
                         const double v = (c.E[3 * i + k] + fld[3 * i + k]) * c.alpha[i];
@@ -526,7 +523,6 @@ __global__ void __launch_bounds__(512) k_batch(BatchArgs A) {
             }
             __syncthreads();
             cluster_matvec(c, n, A.lmax, damp_r2, fld);
-            __syncthreads();
             double e2 = 0.0;
             for (int k = threadIdx.x; k < n3; k += blockDim.x) {
                 const double dl = (c.E[k] + fld[k]) * c.alpha[k / 3] - c.mu[k];
