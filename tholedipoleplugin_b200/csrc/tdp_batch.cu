@@ -24,6 +24,7 @@
 // graph and replayed; one call is: positions in, graph, then forces and
 // per-cluster energies out.
 #include "tholedipole_b200.h"
+#include "tdp_f32x2.cuh"
 #include "tdp_frames.cuh"
 #include "tdp_host.h"
 #include "tdp_pairs.cuh"
@@ -224,6 +225,72 @@ __device__ __forceinline__ void pair_scales(const Cl<R>& c, int i, int j, R& m, 
         }
 }
 
+// FP32 lane loop of cluster_matvec: the lane's J atoms j and j + L ride in the
+// halves of f32x2 registers (pair_matvec per half, I scale applied per half).
+// A half without a pair (j == i, past the cluster's end, or I scale 0) gets
+// the distance (1, 0, 0) and scale 0, so nothing non-finite enters.
+__device__ __forceinline__ void matvec_lane_x2(const Cl<float>& c, int n, int i, int l, int L, float damp_r2,
+                                               float& fx, float& fy, float& fz) {
+    const float4 pi = c.posq[i];
+    const float ti = c.vec[i].w;
+    const f2 OX = bc2(pi.x), OY = bc2(pi.y), OZ = bc2(pi.z), THREE = bc2(3.0f);
+    f2 FX = 0, FY = 0, FZ = 0;
+    for (int ja = l; ja < n; ja += 2 * L) {
+        const int jb = ja + L;
+        float ma, sa, mb, sb = 0.0f;
+        pair_scales(c, i, ja, ma, sa);
+        if (ja == i) sa = 0.0f;
+        if (jb < n) {
+            pair_scales(c, i, jb, mb, sb);
+            if (jb == i) sb = 0.0f;
+        }
+        const float4 pa = c.posq[ja], va = c.vec[ja];
+        const float4 pb = c.posq[jb < n ? jb : ja], vb = c.vec[jb < n ? jb : ja];
+        float dxa = pa.x - pi.x, dya = pa.y - pi.y, dza = pa.z - pi.z;
+        float dxb = pb.x - pi.x, dyb = pb.y - pi.y, dzb = pb.z - pi.z;
+        if (sa == 0.0f) {
+            dxa = 1.0f;
+            dya = dza = 0.0f;
+        }
+        if (sb == 0.0f) {
+            dxb = 1.0f;
+            dyb = dzb = 0.0f;
+        }
+        const f2 DX = pk2(dxa, dxb), DY = pk2(dya, dyb), DZ = pk2(dza, dzb);
+        const f2 R2 = fma2(DX, DX, fma2(DY, DY, mul2(DZ, DZ)));
+        float r2a, r2b;
+        un2(R2, r2a, r2b);
+        const f2 RINV = pk2(rsqrt_r(r2a), rsqrt_r(r2b));
+        const f2 RINV2 = mul2(RINV, RINV);
+        f2 RR3 = mul2(RINV, RINV2);
+        f2 RR5 = mul2(mul2(THREE, RR3), RINV2);
+        if (r2a < damp_r2 || r2b < damp_r2) {
+            float ra, rb, r3a, r3b, r5a, r5b;
+            un2(RINV, ra, rb);
+            un2(RR3, r3a, r3b);
+            un2(RR5, r5a, r5b);
+            damp_field<float>(r2a, ra, ti, va.w, damp_r2, r3a, r5a);
+            damp_field<float>(r2b, rb, ti, vb.w, damp_r2, r3b, r5b);
+            RR3 = pk2(r3a, r3b);
+            RR5 = pk2(r5a, r5b);
+        }
+        const f2 S = pk2(sa, sb);
+        const f2 VX = pk2(va.x, vb.x), VY = pk2(va.y, vb.y), VZ = pk2(va.z, vb.z);
+        const f2 DD = mul2(RR5, fma2(VX, DX, fma2(VY, DY, mul2(VZ, DZ))));
+        const f2 NRR3 = mul2(RR3, bc2(-1.0f));
+        FX = fma2(S, fma2(NRR3, VX, mul2(DD, DX)), FX);
+        FY = fma2(S, fma2(NRR3, VY, mul2(DD, DY)), FY);
+        FZ = fma2(S, fma2(NRR3, VZ, mul2(DD, DZ)), FZ);
+    }
+    float lo, hi;
+    un2(FX, lo, hi);
+    fx += lo + hi;
+    un2(FY, lo, hi);
+    fy += lo + hi;
+    un2(FZ, lo, hi);
+    fz += lo + hi;
+}
+
 // out[i] = sum_j I_ij T_ij v_j with v in c.vec (the mutual field of the operand).
 // Ends with a CTA barrier: out is complete and visible on return.
 template <class R>
@@ -234,7 +301,9 @@ __device__ void cluster_matvec(const Cl<R>& c, int n, int lmax, R damp_r2, doubl
         const Split sp = split(na, lmax);
         const int i = base + sp.a;
         R fx = 0, fy = 0, fz = 0;
-        if (sp.act) {
+        if constexpr (sizeof(R) == 4) {
+            if (sp.act) matvec_lane_x2(c, n, i, sp.l, sp.L, (float)damp_r2, fx, fy, fz);
+        } else if (sp.act) {
             const V4 pi = c.posq[i];
             const R ti = c.vec[i].w;
             for (int j = sp.l; j < n; j += sp.L) {

@@ -36,6 +36,7 @@
 // |b(m)|^2, C2R FFT, then each atom gathers -grad phi (and for forces the
 // second derivatives) with the same weights.
 #include "tdp_ewald.cuh"
+#include "tdp_f32x2.cuh"
 #include "tdp_frames.cuh"
 #include "tdp_host.h"
 #include "tdp_kernels.cuh"
@@ -307,37 +308,6 @@ __device__ __forceinline__ void ew_field_exceptions(const PairParams& P, const E
 // 1.2e-6 at x = 4.3 evaluated in FP32), sharing exp(-x^2) with the B kernels.
 // Thole damping uses 1/t precomputed per atom.
 // ---------------------------------------------------------------------------
-typedef unsigned long long f2;
-__device__ __forceinline__ f2 pk2(float lo, float hi) {
-    f2 r;
-    asm("mov.b64 %0, {%1, %2};" : "=l"(r) : "f"(lo), "f"(hi));
-    return r;
-}
-__device__ __forceinline__ f2 bc2(float v) { return pk2(v, v); }
-__device__ __forceinline__ void un2(f2 v, float& lo, float& hi) {
-    asm("mov.b64 {%0, %1}, %2;" : "=f"(lo), "=f"(hi) : "l"(v));
-}
-__device__ __forceinline__ f2 add2(f2 a, f2 b) {
-    f2 d;
-    asm("add.rn.ftz.f32x2 %0, %1, %2;" : "=l"(d) : "l"(a), "l"(b));
-    return d;
-}
-__device__ __forceinline__ f2 sub2(f2 a, f2 b) {
-    f2 d;
-    asm("sub.rn.ftz.f32x2 %0, %1, %2;" : "=l"(d) : "l"(a), "l"(b));
-    return d;
-}
-__device__ __forceinline__ f2 mul2(f2 a, f2 b) {
-    f2 d;
-    asm("mul.rn.ftz.f32x2 %0, %1, %2;" : "=l"(d) : "l"(a), "l"(b));
-    return d;
-}
-__device__ __forceinline__ f2 fma2(f2 a, f2 b, f2 c) {
-    f2 d;
-    asm("fma.rn.ftz.f32x2 %0, %1, %2, %3;" : "=l"(d) : "l"(a), "l"(b), "l"(c));
-    return d;
-}
-
 constexpr float kErfcP = 0.41f;
 __constant__ float c_erfc[8] = {0.2307648634694866f,  0.23957919808529987f, 0.15874078916517892f,
                                 0.3642441184340127f,  -0.29754436616944707f, 0.6117635229498828f,
