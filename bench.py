@@ -123,6 +123,9 @@ def parse(argv=None):
     p.add_argument("--no-extras", action="store_true", help="only the timed MD (used under ncu)")
     p.add_argument("--ewald-md", action="store_true",
                    help="profiling: the timed MD runs in the Ewald mode (with --no-extras)")
+    p.add_argument("--clusters-profile", type=int, default=0, metavar="N",
+                   help="profiling: only the batched-cluster workload, N clusters of the same seeded "
+                        "size distribution, mixed form, a few evaluations")
     return p.parse_args(argv)
 
 
@@ -787,10 +790,34 @@ def run_ours(args):
     ranks.close()
 
 
+def run_clusters_profile(args):
+    """A small case of the batched-cluster kernel for ncu: N clusters drawn like
+    the 1024-cluster workload, a few evaluations of the mixed form."""
+    import torch
+    from tholedipoleplugin_b200 import systems as S
+    from tholedipoleplugin_b200.batch import ClusterBatch
+    clusters = S.cluster_batch(args.clusters_profile, 4, 64, seed=3, target_eps=1e-6, max_iter=500)
+    with ClusterBatch(clusters, precision="mixed") as b:
+        b.compute()
+        s0, s1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        torch.cuda.synchronize()
+        s0.record()
+        for _ in range(max(1, args.steps)):
+            b.compute()
+        s1.record()
+        torch.cuda.synchronize()
+        it, _ = b.solverStats()
+        print(json.dumps({"clusters": args.clusters_profile, "atoms": b.n, "tile": b.tile(),
+                          "ms_per_evaluation_incl_copies": s0.elapsed_time(s1) / max(1, args.steps),
+                          "cg_iterations_mean": float(it.mean())}))
+
+
 def main():
     args = parse()
     if args.impl == "reference":
         run_reference(args)
+    elif args.clusters_profile > 0:
+        run_clusters_profile(args)
     else:
         run_ours(args)
 
