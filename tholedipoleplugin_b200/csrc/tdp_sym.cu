@@ -5,20 +5,27 @@
 // Work decomposition.  Atoms form 32-atom tiles and tiles form bands of
 // band_tiles tiles.  One CTA (4 warps) owns a band pair (p, q), p <= q, and
 // evaluates every tile pair (I in band p, J in band q, I <= J).  A warp holds
-// the 32 atoms of I in registers (lane = atom) and walks the 32 atoms of J
-// along the diagonals of the 32x32 tile: at step s lane l pairs with atom
-// (l + s) mod 32 of J, read from shared memory, and the J-side sums travel
-// with it, one lane per step, by shuffles, so after 32 steps lane l holds the
-// J-side sums of atom l.  The J-side sums of band q collect in FP64 in shared
-// memory; the four warps of a CTA visit different J tiles in every round
-// (a staggered schedule with a barrier per round), so no two warps add to the
-// same atom at once and the order of the additions is fixed.
+// the atoms of its I tile(s) in registers (lane = atom) and walks the atoms of
+// J along the diagonals of the tile pair, the J-side sums travelling with them
+// from lane to lane by shuffles, so that at the end each lane holds the
+// J-side sums of "its" J atom.  The scalar walks (FP64 form, and SLOW tile
+// pairs) pair lane l with J atom (l + s) mod 32 at step s.  The mixed form's
+// packed walks (f32x2, tdp_f32x2.cuh) pair lane l with J atoms m and m + 16,
+// m = (l + s) mod 16, in the two halves of each register; lanes l and l ^ 16
+// then hold two copies of the same J sums, added by one xor-16 exchange.
 //
-// Output.  Partial sums go to slot s of a [n_bands][components][n_pad] FP64
-// buffer: CTA (p, q) writes the I-side sums of band p into slot q and the
-// J-side sums of band q into slot p (on the diagonal, p == q, both into slot
-// p).  Every (slot, atom) is written by exactly one CTA, and the consumers sum
-// the slots of an atom in slot order, so results are bitwise deterministic.
+// J-side sums of band q.  Field kernels: each warp sums into its own area of
+// shared memory, the four areas are added in warp order at the end.  Energy
+// kernel: one FP64 area; the warps visit disjoint J tiles within each window
+// of band_tiles / 4 steps and a barrier separates the windows, so the order
+// of the additions is fixed.
+//
+// Output.  Plain form: partial sums go to slot s of a [n_bands][components]
+// [n_pad] FP64 buffer -- CTA (p, q) writes the I-side sums of band p into
+// slot q and the J-side sums of band q into slot p -- and the consumers sum an
+// atom's slots in slot order.  Mixed form: every CTA adds its band sums into
+// one 64-bit fixed-point accumulator (integer addition, independent of the
+// order).  Either way results are bitwise deterministic.
 //
 // Tile pairs are classified as in the reference's arithmetic requires: FOLD
 // where the tiles' extents reach half a box (per-pair minimum image with an
