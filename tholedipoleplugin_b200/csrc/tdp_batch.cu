@@ -14,11 +14,13 @@
 // y = mu/sqrt(alpha) with FP64 vectors and block reductions, the reference's
 // RMS-dipole-change stopping test and a true-residual check before accepting.
 //
-// Tile shape.  An atom i is served by a group of L consecutive lanes (L a
-// power of two, L*n <= threads): lane l takes j = l, l+L, ... and the group
-// reduces by shuffles, so small clusters still occupy the CTA.  The CTA size
-// and the largest L are the tile shape; tdp_batch_compute picks them on the
-// first call by timing every candidate on the batch itself.
+// Tile shape.  A pair pass splits the CTA's threads evenly over the
+// cluster's atoms (floor(T/n) or one more consecutive lanes per atom, at most
+// the lane cap): lane l of atom i takes j = l, l+L, ..., leaves its partial
+// sums in shared memory, and the atom's lanes are added in lane order, so
+// small clusters still occupy the CTA and no thread idles on large ones.  The
+// CTA size and the lane cap are the tile shape; tdp_batch_compute picks them
+// on the first call by timing every candidate on the batch itself.
 //
 // Host side.  The launch (queue reset + kernel) is captured once in a CUDA
 // graph and replayed; one call is: positions in, graph, then forces and
