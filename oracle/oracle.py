@@ -45,9 +45,25 @@ class _Stats(C.Structure):
     _fields_ = [("iterations", C.c_int), ("epsilon", C.c_double), ("converged", C.c_int)]
 
 
+# Where this build script looks for the reference plugin's source tree when
+# TDP_REFERENCE_DIR is not set (the compiled reference is built only if the
+# tree is there; without it the tests use the golden fixtures in tests/golden).
+DEFAULT_REFERENCE_DIR = "/root/reference"
+
+
+def reference_dir() -> Optional[str]:
+    d = os.environ.get("TDP_REFERENCE_DIR", DEFAULT_REFERENCE_DIR)
+    return d if os.path.isdir(d) else None
+
+
 def build() -> None:
-    """Compile the oracle libraries (oracle/Makefile)."""
-    subprocess.run(["make", "-s", "-C", HERE], check=True)
+    """Compile the oracle libraries (oracle/Makefile): the restatement always,
+    the compiled reference where its source tree is present."""
+    cmd = ["make", "-s", "-C", HERE]
+    ref = reference_dir()
+    if ref:
+        cmd.append(f"REF={ref}")
+    subprocess.run(cmd, check=True)
 
 
 _libs = {}
@@ -153,6 +169,23 @@ def compute(sys, backend: str = "port", rinv4_mode: int = RINV4_FILL, rinv4_valu
         res.induced = induced_dipoles(sys, backend)[0]
         res.lab = lab_dipoles(sys, backend)
     return res
+
+
+def compute_full(sys, rinv4_value: float = 0.0) -> Result:
+    """Energy, forces and the induced dipoles of the same solve from the
+    compiled reference (one calculateForceAndEnergy call, RTDF.cpp:100-127),
+    plus the lab-frame dipoles (no solve)."""
+    pk = _Packed(sys)
+    n = sys.n
+    forces = np.zeros((n, 3))
+    mu = np.zeros((n, 3))
+    e = C.c_double(0.0)
+    st = _Stats()
+    lib = _lib("reference")
+    lib.tdpref_compute_full.argtypes = [C.c_void_p, C.c_double, _dp, _dp, _dp, C.c_void_p]
+    _check(lib.tdpref_compute_full(C.byref(pk.s), rinv4_value, C.byref(e), _p(forces), _p(mu), C.byref(st)),
+           "compute_full")
+    return Result(e.value, forces, mu, lab_dipoles(sys, "reference"), st.iterations, st.epsilon, st.converged)
 
 
 def lab_dipoles(sys, backend: str = "port") -> np.ndarray:

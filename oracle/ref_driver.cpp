@@ -133,6 +133,15 @@ ReferenceTholeDipoleForce* make(const tdpo_system* s) {
     return f;
 }
 
+/* Either reference class with its protected induced dipoles readable, so that
+ * one calculateForceAndEnergy call yields energy, forces and the dipoles it
+ * used (the golden fixtures of the large boxes need only one solve). */
+template <class Base>
+struct Exposed : Base {
+    using Base::Base;
+    const vector<Vec3>& induced() const { return this->_inducedDipole; }
+};
+
 void stats(const ReferenceTholeDipoleForce* f, tdpo_stats* st) {
     if (!st) return;
     st->iterations = f->getMutualInducedDipoleIterations();
@@ -164,6 +173,42 @@ int tdpref_compute(const tdpo_system* s, double fill, double* energy, double* fo
                                              in.zs, in.xs, in.ys, in.cov, fv);
         stats(f, st);
         put(fv, forces);
+        delete f;
+    } catch (...) {
+        return 1;
+    }
+    return 0;
+}
+
+/* calculateForceAndEnergy (RTDF.cpp:100-127) plus the induced dipoles of the
+ * same solve (mu, n*3; zeros for Direct are the reference's own values). */
+int tdpref_compute_full(const tdpo_system* s, double fill, double* energy, double* forces, double* mu,
+                        tdpo_stats* st) {
+    g_fill = fill;
+    try {
+        Inputs in = load(s);
+        ReferenceTholeDipoleForce* f;
+        Exposed<ReferenceTholeDipoleForce>* fn = nullptr;
+        Exposed<ReferencePmeTholeDipoleForce>* fp = nullptr;
+        if (s->method == TDPO_PME) {
+            fp = new Exposed<ReferencePmeTholeDipoleForce>();
+            Vec3 box[3] = {Vec3(s->box[0], 0, 0), Vec3(0, s->box[1], 0), Vec3(0, 0, s->box[2])};
+            fp->setPeriodicBoxSize(box);
+            f = fp;
+        } else {
+            fn = new Exposed<ReferenceTholeDipoleForce>(ReferenceTholeDipoleForce::NoCutoff);
+            f = fn;
+        }
+        configure(f, s);
+        vector<Vec3> fv(s->n);
+        for (int i = 0; i < s->n; i++) fv[i] = Vec3(forces[3 * i], forces[3 * i + 1], forces[3 * i + 2]);
+        *energy = f->calculateForceAndEnergy(in.pos, in.charges, in.dipoles, in.polarity, in.tholes, in.axisTypes,
+                                             in.zs, in.xs, in.ys, in.cov, fv);
+        stats(f, st);
+        put(fv, forces);
+        const vector<Vec3>& ind = fp ? fp->induced() : fn->induced();
+        for (int i = 0; i < s->n; i++)
+            for (int c = 0; c < 3; c++) mu[3 * i + c] = i < (int)ind.size() ? ind[i][c] : 0.0;
         delete f;
     } catch (...) {
         return 1;
