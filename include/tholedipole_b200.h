@@ -202,6 +202,16 @@ int tdp_update_params(tdp_handle* h, int32_t num_particles, const double* charge
                       const double* thole_damping, const int32_t* axis_types, const int32_t* atom_z,
                       const int32_t* atom_x, const int32_t* atom_y);
 
+/* The per-particle half of copyParametersToContext (same reference lines as
+ * tdp_update_params): charges (n), molecular_dipoles (n*3),
+ * polarizabilities (n), thole_damping (n), on the device if on_device else on
+ * the host; axis frames and covalent maps stay.  With device arrays the
+ * parameters never pass through the host (the damping radius and net charge
+ * are reduced on the device); this is the forward of the Python layer's
+ * torch.autograd.Function on CUDA tensors. */
+int tdp_update_particle_params(tdp_handle* h, const double* charges, const double* molecular_dipoles,
+                               const double* polarizabilities, const double* thole_damping, int32_t on_device);
+
 /* CalcTholeDipoleForceKernel::execute (TholeDipoleKernels.h:68,
  * ReferenceTholeDipoleKernels.cpp:201-215).  positions: n*3 of pos_dtype, on
  * the device if on_device else on the host.  With TDP_COMPUTE_FORCES the
@@ -209,6 +219,20 @@ int tdp_update_params(tdp_handle* h, int32_t num_particles, const double* charge
  * positions); energy (host double) may be NULL. */
 int tdp_compute(tdp_handle* h, const void* positions, int32_t pos_dtype, int32_t on_device,
                 void* forces_accum, int32_t force_dtype, double* energy, uint32_t flags);
+
+/* execute on the OpenMM CUDA platform's own buffers (what a CUDA-platform
+ * kernel gets from its CudaContext, as CudaTholeDipoleKernelFactory.cpp:68-73
+ * hands it contexts[0]): posq holds x, y, z, q per slot as float4 (single and
+ * mixed precision) or double4 (posq_is_double, double precision) in the
+ * context's current atom order, slot k holding atom atom_index[k]; the forces
+ * are ADDED to the 64-bit fixed-point accumulator force_fixed (2^32 units per
+ * force unit, component c of slot k at k + c * padded_num_atoms, truncated
+ * toward zero) -- the layout the platform sums all forces in.  All pointers
+ * are device memory; the energy (host double, may be NULL) is returned as in
+ * tdp_compute.  The positions are taken as given: molecules must be whole, as
+ * the platform keeps them. */
+int tdp_compute_openmm(tdp_handle* h, const void* posq, int32_t posq_is_double, const int32_t* atom_index,
+                       int32_t padded_num_atoms, long long* force_fixed, double* energy, uint32_t flags);
 
 /* getInducedDipoles / getLabFramePermanentDipoles / getTotalDipoles
  * (TholeDipoleKernels.h:91-105) at the given positions (NULL: the positions
@@ -236,7 +260,10 @@ int tdp_get_potential(tdp_handle* h, const void* positions, int32_t pos_dtype, i
  * library keeps until exit; num_points above that count is rejected with
  * TDP_ERR_INVALID_ARGUMENT.  The first call on a device looks up the array's
  * device address (cudaGetSymbolAddress) with that device current, so make it
- * before any stream capture.  All calls share the array and leave their
+ * before any stream capture; the address is kept for the life of the process,
+ * so do not call this on a device after a cudaDeviceReset of it.  The call
+ * clears any pending non-sticky CUDA error on entry, so that it reports only
+ * its own launch failures.  All calls share the array and leave their
  * partial sums in it (every slot a call reads, it first writes, so nothing
  * needs clearing); calls that overlap on the GPU race on it.  Errors:
  * tdp_last_error(NULL). */
@@ -269,8 +296,14 @@ int tdp_solver_stats(const tdp_handle* h, int32_t* iterations, double* epsilon, 
  * costs one adjoint solve of the same symmetric (alpha^-1 - T) system; pair
  * damping terms are recomputed, not stored.  The plugin has no counterpart:
  * this is the backward of the torch.autograd.Function in the Python layer.
- * Direct and Mutual polarization (TDP_ERR_UNSUPPORTED for Extrapolated). */
+ * Every polarization type; Extrapolated runs its perturbation recursion
+ * (ReferenceTholeDipoleForce.cpp:853-909) backwards instead of a solve.
+ * TDP_ERR_UNSUPPORTED in the Ewald and variational modes. */
 int tdp_adjoint(tdp_handle* h, const double* dL_dF, double dL_dE, double* grads);
+
+/* tdp_adjoint with dL_dF (n*3, NULL = zero) and grads (n*6) in device memory;
+ * nothing is synchronised with the host beyond the adjoint solve's scalars. */
+int tdp_adjoint_device(tdp_handle* h, const double* dL_dF, double dL_dE, double* grads);
 
 /* Device timing of the last tdp_compute (CUDA events on the handle's stream),
  * recorded only after tdp_enable_timing(h, 1).  out[TDP_NUM_STAGE_TIMES]:
@@ -316,6 +349,32 @@ int tdp_batch_compute(tdp_batch* b, const double* positions, int32_t on_device, 
 
 /* Induced dipoles of the last compute, n*3 host doubles. */
 int tdp_batch_get_induced_dipoles(tdp_batch* b, double* out);
+
+/* New per-particle parameters for every cluster (copyParametersToContext of
+ * each cluster at once, ReferenceTholeDipoleKernels.cpp:317-339): charges (n),
+ * molecular_dipoles (n*3), polarizabilities (n), thole_damping (n), on the
+ * device if on_device else on the host.  Axis frames and covalent maps stay.
+ * A change of the largest Thole factor moves the damping radius and
+ * re-captures the launch graph. */
+int tdp_batch_update_params(tdp_batch* b, const double* charges, const double* molecular_dipoles,
+                            const double* polarizabilities, const double* thole_damping, int32_t on_device);
+
+/* Reverse mode of the last tdp_batch_compute, every cluster in one persistent
+ * launch: per cluster c, the gradients of
+ *   L_c = dL_dE[c] * E_c + sum over its particles of dL_dF_i . F_i
+ * with respect to every particle's charge, polarizability, Thole factor and
+ * molecular-frame dipole -- tdp_adjoint (the backward of the Python
+ * layer's torch.autograd.Function) for all clusters at once, one adjoint solve
+ * of each cluster's (alpha^-1 - T) system for Mutual polarization.  dL_dF: n*3
+ * (NULL = zero), dL_dE: num_clusters (NULL = zero), grads: n*6 per particle
+ * (dq, dalpha, dthole, dmu_mol_x, dmu_mol_y, dmu_mol_z); all three on the
+ * device if on_device else on the host.  No reference counterpart.  Direct and
+ * Mutual polarization (TDP_ERR_UNSUPPORTED for Extrapolated). */
+int tdp_batch_adjoint(tdp_batch* b, const double* dL_dF, const double* dL_dE, int32_t on_device, double* grads);
+
+/* Per-cluster adjoint CG iterations and final residual of the last
+ * tdp_batch_adjoint (Mutual; 0 otherwise); either may be NULL. */
+int tdp_batch_adjoint_stats(tdp_batch* b, int32_t* iterations, double* epsilons);
 
 /* Per-cluster solver report of the last compute: CG iterations (Extrapolated:
  * the order) and the final RMS dipole change; either may be NULL. */

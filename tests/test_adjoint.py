@@ -4,7 +4,8 @@ finite differences of the FP64 oracle.
 Per-particle gradients of L = gE*E + g.F (random g, gE) with respect to
 charge, polarizability, Thole factor and the three molecular-dipole
 components are checked on systems that exercise every axis type and both
-solver paths (Mutual: one adjoint solve; Direct: none), with a relative step
+solver paths (Mutual: one adjoint solve; Direct: none; Extrapolated: the
+perturbation recursion run backwards), with a relative step
 of 1e-4 and the oracle converged to 1e-12.  Tolerance: 1e-5 relative to the
 largest gradient of the same kind (FD truncation is ~1e-8 relative here).
 Where two Thole factors tie, min(t_i, t_j) has a kink; the adjoint gives each
@@ -51,12 +52,15 @@ def _value(s, kind, i):
         kind, s.dipoles[i]["xyz".index(kind[1])] if kind[0] == "m" else None)
 
 
-@pytest.mark.parametrize("name", ["ammonia_mutual", "ammonia_direct", "water4_pme", "random_mutual"])
+@pytest.mark.parametrize("name", ["ammonia_mutual", "ammonia_direct", "ammonia_extrapolated", "water4_pme",
+                                  "random_mutual", "random_extrapolated"])
 def test_particle_gradients_match_finite_differences(name):
     from tholedipoleplugin_b200.kernel import CudaCalcTholeDipoleForceKernel
 
-    s = {"ammonia_mutual": ammonia(S.MUTUAL), "ammonia_direct": ammonia(S.DIRECT), "water4_pme": water4(S.MUTUAL),
-         "random_mutual": small_random_system(24, seed=31, method=S.PME)}[name]
+    s = {"ammonia_mutual": ammonia(S.MUTUAL), "ammonia_direct": ammonia(S.DIRECT),
+         "ammonia_extrapolated": ammonia(S.EXTRAPOLATED), "water4_pme": water4(S.MUTUAL),
+         "random_mutual": small_random_system(24, seed=31, method=S.PME),
+         "random_extrapolated": small_random_system(24, seed=32, method=S.PME, polarization=S.EXTRAPOLATED)}[name]
     # Ties t_i == t_j put every pair on the kink of min(t_i, t_j), where a
     # central difference is only first-order accurate; a 5% jitter of the
     # Thole factors moves the evaluation point well off it (gaps >> the

@@ -1,0 +1,47 @@
+"""Both precision forms against the compiled reference's own results at the
+boxes the parity tests cannot reach with the oracle in seconds: 729 waters
+(2,187 atoms, 2.8 nm box) and the 4,096-water box of the 12,288-atom
+workload (4.968 nm), PME flag (minimum image over all pairs), Mutual
+polarization.  The fixtures (tests/golden, made by tests/golden/make_golden.py
+from ReferenceTholeDipoleForce.cpp compiled unmodified) hold the energy,
+forces and induced dipoles of one calculateForceAndEnergy call
+(ReferenceTholeDipoleForce.cpp:100-127) converged to an RMS dipole change of
+1e-12.
+
+Tolerances: the FP64 form 1e-9 relative energy and 1e-8 RMS relative forces
+and dipoles; the mixed form the north star's bounds, 1e-6 relative energy and
+2e-5 RMS relative forces (induced dipoles 2e-5)."""
+import os
+
+import numpy as np
+import pytest
+
+from tholedipoleplugin_b200.kernel import CudaCalcTholeDipoleForceKernel
+
+from .golden.make_golden import box_system, positions_sha
+from .gpu_util import rel_err, rel_rms
+
+pytestmark = pytest.mark.gpu
+
+GOLDEN = os.path.join(os.path.dirname(os.path.abspath(__file__)), "golden")
+
+
+@pytest.mark.parametrize("name", ["water2187", "water12288"])
+@pytest.mark.parametrize("precision", ["double", "mixed"])
+def test_box_matches_compiled_reference(name, precision):
+    g = np.load(os.path.join(GOLDEN, f"{name}.npz"))
+    s = box_system(name)
+    assert positions_sha(s) == str(g["sha"]), "the seeded box changed since the fixture was made"
+    eps = 1e-10 if precision == "double" else 1e-8
+    with CudaCalcTholeDipoleForceKernel(s.copy(target_eps=eps, max_iter=1000), precision=precision) as k:
+        e, f = k.execute(s.positions)
+        mu = k.getInducedDipoles()
+        assert k.solverStats()["converged"]
+    if precision == "double":
+        assert rel_err(e, float(g["energy"])) < 1e-9
+        assert rel_rms(f, g["forces"]) < 1e-8
+        assert rel_rms(mu, g["induced"]) < 1e-8
+    else:
+        assert rel_err(e, float(g["energy"])) < 1e-6
+        assert rel_rms(f, g["forces"]) < 2e-5
+        assert rel_rms(mu, g["induced"]) < 2e-5

@@ -122,3 +122,84 @@ def test_adapter_mixed_precision(tmp_path):
     ref = O.compute(s.copy(target_eps=1e-12), "port")
     assert rel_err(float(r["energy"]), ref.energy) < 1e-6
     assert rel_rms(_arr(r["forces"]).reshape(-1, 3), ref.forces) < 2e-5
+
+
+# ---------------------------------------------------------------------------
+# The adapter compiled against the plugin's own public API (the reference's
+# openmmapi headers, TholeDipoleForce.cpp and TholeDipoleForceImpl.cpp built
+# unmodified by oracle/Makefile into oracle/_ref/reference_api_driver), driven
+# through a Context: TholeDipoleForceImpl::initialize validates and creates
+# the kernel by name, calcForcesAndEnergy gates on the force group, the
+# queries go through the Force's Context methods, and the CUDA platform's
+# buffers (posq, atom index, fixed-point forces) take the device path.
+# ---------------------------------------------------------------------------
+API_DRIVER = os.path.join(os.path.dirname(os.path.dirname(os.path.abspath(__file__))), "oracle", "_ref",
+                          "reference_api_driver")
+api_driver = pytest.mark.skipif(not os.path.exists(API_DRIVER),
+                                reason="the reference-API build of the adapter needs the reference source tree")
+
+
+def _run_api(s, grid, tmp_path, precision, *extra):
+    path = str(tmp_path / "system.txt")
+    _write(s, path, grid)
+    out = subprocess.run([API_DRIVER, path, precision, *extra], check=True, capture_output=True, text=True,
+                         timeout=300).stdout
+    res = {}
+    for line in out.splitlines():
+        tag, _, rest = line.partition(" ")
+        res[tag] = rest
+    return res
+
+
+@pytest.mark.gpu
+@api_driver
+@pytest.mark.parametrize("name,precision", [("water4_pme", "double"), ("ammonia_mutual", "double"),
+                                            ("ammonia_extrapolated", "double"), ("water4_pme", "mixed")])
+def test_reference_api_context_matches_oracle(name, precision, tmp_path):
+    s = {"ammonia_mutual": ammonia(S.MUTUAL), "water4_pme": water4(S.MUTUAL),
+         "ammonia_extrapolated": ammonia(S.EXTRAPOLATED)}[name]
+    s = s.copy(target_eps=1e-12 if precision == "double" else 1e-9, max_iter=3000)
+    grid = np.random.default_rng(6).uniform(-0.5, 0.5, size=(7, 3))
+    r = _run_api(s, grid, tmp_path, precision)
+    ref = O.compute(s.copy(target_eps=1e-12), "port")
+    te, tf = (1e-9, 1e-9) if precision == "double" else (1e-6, 2e-5)
+    e = float(r["energy"])
+    assert rel_err(e, ref.energy) < te
+    assert rel_rms(_arr(r["forces"]).reshape(-1, 3), ref.forces) < tf
+    assert rel_rms(_arr(r["induced"]).reshape(-1, 3), ref.induced) < tf
+    assert rel_rms(_arr(r["lab"]).reshape(-1, 3), ref.lab) < 1e-12
+    assert rel_rms(_arr(r["total"]).reshape(-1, 3), ref.lab + ref.induced) < tf
+    assert rel_rms(_arr(r["potential"]), O.potential(s.copy(target_eps=1e-12), grid, "port")) < tf
+    if s.method == S.PME:
+        assert "pme" in r
+    else:
+        assert r["pme_error"] == "getPMEParametersInContext: This Context is not using PME"
+    # Force groups: the force in group 3 contributes only when group 3 is asked for.
+    assert float(r["energy_other_groups"]) == 0.0
+    assert float(r["energy_own_group"]) == e
+    # The CUDA platform's buffers: same evaluation, forces through the fixed-point accumulator.
+    ed = float(r["energy_device"])
+    fd = _arr(r["forces_device"]).reshape(-1, 3)
+    if precision == "double":
+        assert rel_err(ed, e) < 1e-12
+        assert np.abs(fd - _arr(r["forces"]).reshape(-1, 3)).max() <= 2.0 ** -31
+    else:  # float4 posq: coordinates rounded to FP32
+        assert rel_err(ed, ref.energy) < te and rel_rms(fd, ref.forces) < tf
+    assert rel_rms(_arr(r["induced_device"]).reshape(-1, 3), ref.induced) < tf
+    # updateParametersInContext: kernel.copyParametersToContext + context.systemChanged().
+    assert int(r["system_changed"]) >= 1
+    ref2 = O.compute(_scaled(s).copy(target_eps=1e-12), "port")
+    assert rel_err(float(r["energy_updated"]), ref2.energy) < te
+    assert rel_rms(_arr(r["forces_updated"]).reshape(-1, 3), ref2.forces) < tf
+
+
+@pytest.mark.gpu
+@api_driver
+def test_reference_api_validation_messages(tmp_path):
+    s = water4(S.MUTUAL)
+    r = _run_api(s, np.zeros((1, 3)), tmp_path, "double", "validate")
+    assert r["particles_error"] == ("TholeDipoleForce must have exactly as many particles as the System it "
+                                    "belongs to.")
+    assert r["cutoff_error"] == "TholeDipoleForce: The cutoff distance cannot be greater than half the periodic box size."
+    assert r["axis_error"].startswith("TholeDipoleForce: axis type=7 not currently handled")
+    assert r["zaxis_error"] == f"TholeDipoleForce: invalid z axis particle: {s.n + 5}"

@@ -6,13 +6,17 @@ scratch in a fixed device array (8 MiB, TDP_NOALLOC_SCRATCH_DOUBLES doubles).
 
 Checked through the C ABI against tdp_get_potential (which allocates device
 copies of the grid and the result on every call) on two calls in a row, with
-the tolerance of the other FP64 query tests (1e-9 RMS relative).  This file is
-named so that pytest collects it last; it needs nothing from earlier tests."""
+the tolerance of the other FP64 query tests (1e-9 RMS relative), and against
+the FP64 oracle's potential.  Further cases: a grid of half the scratch size,
+where the split over atoms is capped by the scratch array and every slot is
+reused; an empty particle set (zeros); the legacy default stream.  This file
+is named so that pytest collects it last; it needs nothing from earlier tests."""
 import ctypes as C
 
 import numpy as np
 import pytest
 
+from oracle import oracle as O
 from tholedipoleplugin_b200 import _capi as A
 from tholedipoleplugin_b200 import systems as S
 from tholedipoleplugin_b200.kernel import CudaCalcTholeDipoleForceKernel
@@ -70,3 +74,72 @@ def test_noalloc_rejects_oversized_grid():
                                         None, C.c_void_p(one.data_ptr()), None)
     assert big == -1
     assert b"scratch limit" in A.lib().tdp_last_error(None)
+
+
+def _device(*arrays):
+    import torch
+    dev = torch.device("cuda", 0)
+    return [torch.tensor(np.asarray(a, dtype=np.float64), device=dev) for a in arrays]
+
+
+def test_noalloc_potential_matches_oracle():
+    """The potential of the FP64 oracle (converged dipoles, minimum image) at
+    the same grid points, with the GPU's total dipoles from a tight solve."""
+    import torch
+
+    s = S.config_small()
+    grid = np.random.default_rng(8).uniform(-0.2, 2.0, size=(300, 3))
+    ref = O.potential(s.copy(target_eps=1e-12, max_iter=5000), grid, "port")
+    with CudaCalcTholeDipoleForceKernel(s.copy(target_eps=1e-12, max_iter=2000), precision="double") as k:
+        total = k.getTotalDipoles(s.positions)
+    pos, q, dip, g = _device(s.positions, s.charges, total, grid)
+    out = torch.full((grid.shape[0],), float("nan"), dtype=torch.float64, device="cuda")
+    rc = _call(s.n, pos, q, dip, g, 1, s.box, out, torch.cuda.current_stream().cuda_stream)
+    torch.cuda.synchronize()
+    assert rc == 0, A.lib().tdp_last_error(None)
+    assert rel_rms(out.cpu().numpy(), ref) < 1e-9
+
+
+def test_noalloc_scratch_capped_split():
+    """num_points = half the scratch: the atom split is capped at two chunks by
+    the scratch size, so both halves of the array are written and read; the
+    result must equal the allocating query's, twice in a row."""
+    import torch
+
+    s = S.water_box(9, 2.8, seed=31, cutoff=0.9)   # 2,187 atoms
+    npts = (1 << 20) // 2
+    grid = np.random.default_rng(9).uniform(0.0, 2.8, size=(npts, 3))
+    with CudaCalcTholeDipoleForceKernel(s.copy(target_eps=1e-10, max_iter=2000), precision="double") as k:
+        expected = k.getElectrostaticPotential(grid, s.positions)
+        total = k.getTotalDipoles()
+    pos, q, dip, g = _device(s.positions, s.charges, total, grid)
+    out = torch.empty(npts, dtype=torch.float64, device="cuda")
+    for _ in range(2):
+        out.fill_(float("nan"))
+        rc = _call(s.n, pos, q, dip, g, 1, s.box, out, torch.cuda.current_stream().cuda_stream)
+        torch.cuda.synchronize()
+        assert rc == 0, A.lib().tdp_last_error(None)
+        assert rel_rms(out.cpu().numpy(), expected) < 1e-9
+
+
+def test_noalloc_empty_particles_and_default_stream():
+    import torch
+
+    grid = np.random.default_rng(10).uniform(-1.0, 1.0, size=(33, 3))
+    (g,) = _device(grid)
+    out = torch.full((33,), float("nan"), dtype=torch.float64, device="cuda")
+    rc = A.lib().tdp_potential_noalloc(0, None, None, None, 33, C.c_void_p(g.data_ptr()), 0, None,
+                                       C.c_void_p(out.data_ptr()), None)
+    torch.cuda.synchronize()
+    assert rc == 0 and torch.all(out == 0.0)
+    # Legacy default stream (NULL), non-periodic ammonia, against the allocating query.
+    s = ammonia()
+    with CudaCalcTholeDipoleForceKernel(s.copy(target_eps=1e-11, max_iter=2000), precision="double") as k:
+        expected = k.getElectrostaticPotential(grid, s.positions)
+        total = k.getTotalDipoles()
+    pos, q, dip = _device(s.positions, s.charges, total)
+    out.fill_(float("nan"))
+    rc = _call(s.n, pos, q, dip, g, 0, np.zeros(3), out, None)
+    torch.cuda.synchronize()
+    assert rc == 0, A.lib().tdp_last_error(None)
+    assert rel_rms(out.cpu().numpy(), expected) < 1e-9

@@ -14,7 +14,8 @@ HERE = os.path.dirname(os.path.abspath(__file__))
 LIB_PATH = os.path.join(HERE, "libtholedipole_b200.so")
 
 TDP_OK = 0
-TDP_ERR_INVALID_ARGUMENT, TDP_ERR_CUDA, TDP_ERR_UNSUPPORTED = -1, -2, -8
+TDP_ERR_INVALID_ARGUMENT, TDP_ERR_CUDA, TDP_ERR_NOT_PME, TDP_ERR_SIZE_MISMATCH = -1, -2, -3, -4
+TDP_ERR_BOX_TOO_SMALL, TDP_ERR_NOT_CONVERGED, TDP_ERR_NON_FINITE, TDP_ERR_UNSUPPORTED = -5, -6, -7, -8
 ERRORS = {
     -1: "invalid argument", -2: "CUDA error", -3: "not PME", -4: "size mismatch", -5: "box too small",
     -6: "not converged", -7: "non-finite", -8: "unsupported",
@@ -69,6 +70,8 @@ PROTOTYPES = {
     "tdp_update_params": (C.c_int, [C.c_void_p, C.c_int32, _dp, _dp, _dp, _dp, _ip, _ip, _ip, _ip]),
     "tdp_compute": (C.c_int, [C.c_void_p, C.c_void_p, C.c_int32, C.c_int32, C.c_void_p, C.c_int32, _dp,
                               C.c_uint32]),
+    "tdp_compute_openmm": (C.c_int, [C.c_void_p, C.c_void_p, C.c_int32, C.c_void_p, C.c_int32, C.c_void_p, _dp,
+                                     C.c_uint32]),
     "tdp_get_dipoles": (C.c_int, [C.c_void_p, C.c_int32, C.c_void_p, C.c_int32, C.c_int32, _dp]),
     "tdp_get_potential": (C.c_int, [C.c_void_p, C.c_void_p, C.c_int32, C.c_int32, _dp, C.c_int32, _dp]),
     "tdp_get_moments": (C.c_int, [C.c_void_p, C.c_void_p, C.c_int32, C.c_int32, _dp, _dp]),
@@ -77,6 +80,9 @@ PROTOTYPES = {
     "tdp_get_pme_parameters": (C.c_int, [C.c_void_p, _dp, _ip, _ip, _ip]),
     "tdp_solver_stats": (C.c_int, [C.c_void_p, _ip, _dp, _ip, _ip]),
     "tdp_adjoint": (C.c_int, [C.c_void_p, C.c_void_p, C.c_double, _dp]),
+    "tdp_adjoint_device": (C.c_int, [C.c_void_p, C.c_void_p, C.c_double, C.c_void_p]),
+    "tdp_update_particle_params": (C.c_int, [C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p,
+                                             C.c_int32]),
     "tdp_enable_timing": (C.c_int, [C.c_void_p, C.c_int32]),
     "tdp_stage_times": (C.c_int, [C.c_void_p, _dp]),
     "tdp_md_kick_drift": (C.c_int, [C.c_int32, C.c_double, C.c_double, C.c_double, C.c_double, C.c_double,
@@ -99,6 +105,9 @@ PROTOTYPES = {
     "tdp_batch_solver_stats": (C.c_int, [C.c_void_p, _ip, _dp]),
     "tdp_batch_tile": (C.c_int, [C.c_void_p, _ip, _ip, _ip, _dp]),
     "tdp_batch_tile_candidates": (C.c_int, [C.c_void_p, C.c_int32, _ip, _ip, _dp]),
+    "tdp_batch_update_params": (C.c_int, [C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p, C.c_int32]),
+    "tdp_batch_adjoint": (C.c_int, [C.c_void_p, C.c_void_p, C.c_void_p, C.c_int32, C.c_void_p]),
+    "tdp_batch_adjoint_stats": (C.c_int, [C.c_void_p, _ip, _dp]),
 }
 
 

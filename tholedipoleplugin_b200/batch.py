@@ -85,6 +85,45 @@ class ClusterBatch:
                                          C.c_void_p(energies_ptr))
         self._check(rc, self._h)
 
+    def updateParams(self, charges, dipoles, polarizabilities, tholes) -> None:
+        """New per-particle parameters (host numpy arrays, or CUDA torch tensors
+        of float64 on this batch's device) for every cluster."""
+        arrs = [charges, dipoles, polarizabilities, tholes]
+        if all(hasattr(a, "data_ptr") and getattr(a, "is_cuda", False) for a in arrs):
+            for a in arrs:
+                assert a.dtype.itemsize == 8 and a.is_contiguous()
+            rc = self._lib.tdp_batch_update_params(self._h, *[C.c_void_p(a.data_ptr()) for a in arrs], 1)
+        else:
+            hs = [np.ascontiguousarray(np.asarray(a, dtype=np.float64)) for a in arrs]
+            rc = self._lib.tdp_batch_update_params(self._h, *[h.ctypes.data_as(C.c_void_p) for h in hs], 0)
+        self._check(rc, self._h)
+
+    def adjoint(self, dL_dF=None, dL_dE=None) -> np.ndarray:
+        """Per-particle gradients (dq, dalpha, dthole, dmu_mol[3]) of
+        sum_c dL_dE[c] E_c + sum_i dL_dF_i . F_i at the last compute (host arrays)."""
+        out = np.zeros((self.n, 6))
+        gF = None if dL_dF is None else np.ascontiguousarray(np.asarray(dL_dF, dtype=np.float64).reshape(self.n, 3))
+        gE = None if dL_dE is None else np.ascontiguousarray(np.asarray(dL_dE, dtype=np.float64).reshape(-1))
+        rc = self._lib.tdp_batch_adjoint(self._h, None if gF is None else gF.ctypes.data_as(C.c_void_p),
+                                         None if gE is None else gE.ctypes.data_as(C.c_void_p), 0,
+                                         out.ctypes.data_as(C.c_void_p))
+        self._check(rc, self._h)
+        return out
+
+    def adjoint_device(self, dL_dF_ptr: int, dL_dE_ptr: int, grads_ptr: int) -> None:
+        """Device-resident reverse pass: raw CUDA pointers (n*3, num_clusters,
+        n*6 doubles); 0 for an absent cotangent."""
+        rc = self._lib.tdp_batch_adjoint(self._h, C.c_void_p(dL_dF_ptr or None), C.c_void_p(dL_dE_ptr or None), 1,
+                                         C.c_void_p(grads_ptr))
+        self._check(rc, self._h)
+
+    def adjointStats(self):
+        it = np.zeros(self.num_clusters, dtype=np.int32)
+        eps = np.zeros(self.num_clusters)
+        self._check(self._lib.tdp_batch_adjoint_stats(self._h, it.ctypes.data_as(C.POINTER(C.c_int32)),
+                                                      eps.ctypes.data_as(C.POINTER(C.c_double))), self._h)
+        return it, eps
+
     def inducedDipoles(self) -> np.ndarray:
         out = np.zeros((self.n, 3))
         self._check(self._lib.tdp_batch_get_induced_dipoles(self._h, out.ctypes.data_as(C.POINTER(C.c_double))),

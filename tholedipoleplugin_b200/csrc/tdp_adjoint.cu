@@ -16,6 +16,12 @@
 //   dL/dalpha_i = (a_mu + T lambda)_i . (E + T mu)_i   (= lambda_i.mu_i/alpha_i^2)
 //   dL/dq = a_q + b_q,  dL/dt = a_t + b_t + c_t,
 //   dL/dmu_mol = S R^T (a_mu_lab + b_mu_lab).
+// Extrapolated polarization (:853-909: mu_0 = alpha E, mu_k = alpha (E + T
+// mu_(k-1)), mu = sum_k c_k mu_k) has no solve; its adjoint runs the
+// recursion backwards: gbar_(K-1) = c_(K-1) a_mu, gbar_k = c_k a_mu +
+// T (alpha gbar_(k+1)); then lambda = sum_k alpha gbar_k takes the place of
+// the adjoint solution in b, dL/dalpha = sum_k gbar_k . (E + T mu_(k-1)) and
+// c_t = sum_(k>=1) d/dt of (alpha gbar_k)^T T mu_(k-1).
 // For fixed geometry and damping the pair routine's energy, forces and
 // torques are bilinear in the two atoms' multipoles (every term is one
 // quantity of atom I times one of atom K), so the derivative with respect to
@@ -24,293 +30,10 @@
 // factors and is taken with a one-direction dual number.  Damping terms are
 // recomputed in every pass rather than stored.  Every pair is visited from
 // both atoms (each thread owns one atom), so no atomics are needed.
-#include "tdp_frames.cuh"
-#include "tdp_kernels.cuh"
-
-#include <math.h>
+#include "tdp_adjoint.cuh"
 
 namespace tdp {
 namespace adj {
-
-struct Dual {
-    double v, d;
-};
-__device__ __forceinline__ Dual mk(double v, double d = 0.0) { return {v, d}; }
-__device__ __forceinline__ Dual operator+(Dual a, Dual b) { return {a.v + b.v, a.d + b.d}; }
-__device__ __forceinline__ Dual operator-(Dual a, Dual b) { return {a.v - b.v, a.d - b.d}; }
-__device__ __forceinline__ Dual operator-(Dual a) { return {-a.v, -a.d}; }
-__device__ __forceinline__ Dual operator*(Dual a, Dual b) { return {a.v * b.v, a.v * b.d + a.d * b.v}; }
-__device__ __forceinline__ Dual operator/(Dual a, Dual b) {
-    double iv = 1.0 / b.v;
-    return {a.v * iv, (a.d - a.v * iv * b.d) * iv};
-}
-__device__ __forceinline__ Dual operator+(Dual a, double b) { return {a.v + b, a.d}; }
-__device__ __forceinline__ Dual operator+(double a, Dual b) { return {a + b.v, b.d}; }
-__device__ __forceinline__ Dual operator-(Dual a, double b) { return {a.v - b, a.d}; }
-__device__ __forceinline__ Dual operator-(double a, Dual b) { return {a - b.v, -b.d}; }
-__device__ __forceinline__ Dual operator*(Dual a, double b) { return {a.v * b, a.d * b}; }
-__device__ __forceinline__ Dual operator*(double a, Dual b) { return {a * b.v, a * b.d}; }
-__device__ __forceinline__ Dual& operator+=(Dual& a, Dual b) { return a = a + b; }
-__device__ __forceinline__ Dual& operator-=(Dual& a, Dual b) { return a = a - b; }
-__device__ __forceinline__ Dual dexp(Dual a) {
-    double e = exp(a.v);
-    return {e, e * a.d};
-}
-__device__ __forceinline__ double dexp(double a) { return exp(a); }
-__device__ __forceinline__ double val(double a) { return a; }
-__device__ __forceinline__ double val(Dual a) { return a.v; }
-__device__ __forceinline__ double der(double) { return 0.0; }
-__device__ __forceinline__ double der(Dual a) { return a.d; }
-// min(t_i, t_j) of the damping (RTDF.cpp:206, :662).  It has a kink where the
-// factors are equal; there the symmetric subgradient is used (each side gets
-// half), which is what a central difference sees and which sums to the exact
-// derivative when both factors move together.
-__device__ __forceinline__ double tmin(double a, double b) { return a < b ? a : b; }
-__device__ __forceinline__ Dual tmin(Dual a, Dual b) {
-    if (a.v < b.v) return a;
-    if (b.v < a.v) return b;
-    return {a.v, 0.5 * (a.d + b.d)};
-}
-template <class T> __device__ __forceinline__ T cst(double v);
-template <> __device__ __forceinline__ double cst<double>(double v) { return v; }
-template <> __device__ __forceinline__ Dual cst<Dual>(double v) { return mk(v); }
-
-struct V3 {
-    double x, y, z;
-};
-__device__ __forceinline__ V3 ld(const double* p) { return {p[0], p[1], p[2]}; }
-
-// Thole factors of the pair energy routine (RTDF.cpp:204-220).
-template <class T>
-__device__ __forceinline__ void energy_damping(double r, double r2, double damp_r2, T tI, T tK, T& tc, T& td0, T& td1,
-                                               T& dtc, T& dtd0, T& dtd1) {
-    tc = td0 = td1 = dtc = dtd0 = dtd1 = cst<T>(1.0);
-    if (r2 < damp_r2) {
-        T dmp = tI * tK;
-        if (fabs(val(dmp)) > 1.0e-5) {
-            T a = tmin(tI, tK);
-            T u = cst<T>(r) / dmp;
-            T au3 = a * u * u * u;
-            T e = dexp(-au3);
-            tc = 1.0 - e;
-            td0 = 1.0 - e * (1.0 + 1.5 * au3);
-            td1 = 1.0 - e;
-            dtc = 1.0 - e * (1.0 + 1.5 * au3);
-            dtd0 = 1.0 - e * (1.0 + au3 + 1.5 * au3 * au3);
-            dtd1 = 1.0 - e * (1.0 + au3);
-        }
-    }
-}
-
-// Damped 1/r^3 and 3/r^5 of getAndScaleInverseRs (RTDF.cpp:646-676).
-template <class T>
-__device__ __forceinline__ void field_damping(double r, double r2, double damp_r2, T ti, T tj, T& rr3, T& rr5) {
-    double rI = 1.0 / r, r2I = rI * rI;
-    rr3 = cst<T>(rI * r2I);
-    rr5 = cst<T>(3.0 * rI * r2I * r2I);
-    if (r2 < damp_r2) {
-        T dmp = ti * tj;
-        if (val(dmp) != 0.0) {
-            T pg = tmin(ti, tj);
-            T ratio = cst<T>(r) / dmp;
-            ratio = ratio * ratio * ratio;
-            T damp = -pg * ratio;
-            if (val(damp) > -50.0) {
-                T e = dexp(damp);
-                rr3 = rr3 * (1.0 - e);
-                rr5 = rr5 * (1.0 - (1.0 - damp) * e);
-            }
-        }
-    }
-}
-
-// One pair of calculateElectrostaticPairIxn in its canonical orientation
-// (I lower index, d = p_K - p_I), contracted with the cotangents:
-//   l = gE*energy + cf.qf + ctI.qtI + ctK.qtJ
-// where cf = FR^T (gF_K - gF_I), ctI = FR^T gT_I, ctK = FR^T gT_K are the
-// force/torque cotangents brought into the QI frame.  Same operations and
-// frame convention as pair_energy (tdp_pairs.cuh).
-template <class T>
-__device__ T pair_loss(double dx, double dy, double dz, bool yzd, T qI, const T* mI, const T* uIl, T tI, T qK,
-                       const T* mK, const T* uKl, T tK, double mS, double iS, double damp_r2, double rv4p,
-                       double rv4f, bool mutual, double gE, V3 gFI, V3 gFK, V3 gTI, V3 gTK) {
-    double r2 = dx * dx + dy * dy + dz * dz;
-    double r = sqrt(r2);
-    double rinv = 1.0 / r;
-    double zx = dx * rinv, zy = dy * rinv, zz = dz * rinv;
-    double xx = zx, xy = zy, xz = zz;
-    if (yzd) xx += 1.0;
-    else xy += 1.0;
-    double dt = zx * xx + zy * xy + zz * xz;
-    xx -= zx * dt;
-    xy -= zy * dt;
-    xz -= zz * dt;
-    double xn = sqrt(xx * xx + xy * xy + xz * xz);
-    if (xn > 0.0) {
-        xx /= xn;
-        xy /= xn;
-        xz /= xn;
-    }
-    double yx = zy * xz - zz * xy, yy = zz * xx - zx * xz, yz = zx * xy - zy * xx;
-    // Force rotation rows (Y.y, Z.y, X.y), (Y.z, Z.z, X.z), (Y.x, Z.x, X.x).
-    double FR[3][3] = {{yy, zy, xy}, {yz, zz, xz}, {yx, zx, xx}};
-    double gd[3] = {gFK.x - gFI.x, gFK.y - gFI.y, gFK.z - gFI.z};
-    double gti[3] = {gTI.x, gTI.y, gTI.z}, gtk[3] = {gTK.x, gTK.y, gTK.z};
-    double cf[3], cti[3], ctk[3];
-    for (int b = 0; b < 3; b++) {
-        cf[b] = FR[0][b] * gd[0] + FR[1][b] * gd[1] + FR[2][b] * gd[2];
-        cti[b] = FR[0][b] * gti[0] + FR[1][b] * gti[1] + FR[2][b] * gti[2];
-        ctk[b] = FR[0][b] * gtk[0] + FR[1][b] * gtk[1] + FR[2][b] * gtk[2];
-    }
-    T uI0 = xx * uIl[0] + xy * uIl[1] + xz * uIl[2];
-    T uI1 = yx * uIl[0] + yy * uIl[1] + yz * uIl[2];
-    T uI2 = zx * uIl[0] + zy * uIl[1] + zz * uIl[2];
-    T uJ0 = xx * uKl[0] + xy * uKl[1] + xz * uKl[2];
-    T uJ1 = yx * uKl[0] + yy * uKl[1] + yz * uKl[2];
-    T uJ2 = zx * uKl[0] + zy * uKl[1] + zz * uKl[2];
-    T QI0 = qI, QJ0 = qK;
-    T QI1 = xx * mI[0] + xy * mI[1] + xz * mI[2];
-    T QI2 = yx * mI[0] + yy * mI[1] + yz * mI[2];
-    T QI3 = zx * mI[0] + zy * mI[1] + zz * mI[2];
-    T QJ1 = xx * mK[0] + xy * mK[1] + xz * mK[2];
-    T QJ2 = yx * mK[0] + yy * mK[1] + yz * mK[2];
-    T QJ3 = zx * mK[0] + zy * mK[1] + zz * mK[2];
-    double rv1 = rinv, rv2 = rv1 * rinv, rv3 = rv2 * rinv;
-    double rv4 = rv4p * (rv3 * rinv) + rv4f;
-    T tc, td0, td1, dtc, dtd0, dtd1;
-    energy_damping<T>(r, r2, damp_r2, tI, tK, tc, td0, td1, dtc, dtd0, dtd1);
-
-    double eP = rv1 * mS, dP = -0.5 * mS * rv2;
-    T Vij0 = eP * QJ0, Vji0 = eP * QI0, VijR0 = dP * QJ0, VjiR0 = dP * QI0;
-    eP = rv2 * mS;
-    T eU = (rv2 * iS) * tc;
-    dP = -rv3 * mS;
-    T dU = (-2.0 * rv3 * iS) * dtc;
-    Vij0 = Vij0 - (eP * QJ1 + eU * uJ0);
-    T Vji1 = -(eP * QI0);
-    VijR0 = VijR0 - (dP * QJ1 + dU * uJ0);
-    T VjiR1 = -(dP * QI0);
-    T Vjid0 = -(eU * QI0);
-    T Vij1 = eP * QJ0;
-    Vji0 = Vji0 + eP * QI1 + eU * uI0;
-    T VijR1 = dP * QJ0;
-    VjiR0 = VjiR0 + dP * QI1 + dU * uI0;
-    T Vijd0 = eU * QJ0;
-    eP = -2.0 * rv3 * mS;
-    eU = (-2.0 * rv3 * iS) * td0;
-    dP = 3.0 * rv4 * mS;
-    dU = (6.0 * rv4 * iS) * dtd0;
-    Vij1 = Vij1 + eP * QJ1 + eU * uJ0;
-    Vji1 = Vji1 + eP * QI1 + eU * uI0;
-    VijR1 = VijR1 + dP * QJ1 + dU * uJ0;
-    VjiR1 = VjiR1 + dP * QI1 + dU * uI0;
-    Vijd0 = Vijd0 + eU * QJ1;
-    Vjid0 = Vjid0 + eU * QI1;
-    eP = rv3 * mS;
-    eU = (rv3 * iS) * td1;
-    dP = -1.5 * rv4 * mS;
-    dU = (-3.0 * rv4 * iS) * dtd1;
-    T Vij2 = eP * QJ2 + eU * uJ1, Vji2 = eP * QI2 + eU * uI1;
-    T VijR2 = dP * QJ2 + dU * uJ1, VjiR2 = dP * QI2 + dU * uI1;
-    T Vijd1 = eU * QJ2, Vjid1 = eU * QI2;
-    T Vij3 = eP * QJ3 + eU * uJ2, Vji3 = eP * QI3 + eU * uI2;
-    T VijR3 = dP * QJ3 + dU * uJ2, VjiR3 = dP * QI3 + dU * uI2;
-    T Vijd2 = eU * QJ3, Vjid2 = eU * QI3;
-
-    T energy = 0.5 * (QI0 * Vij0 + QJ0 * Vji0) + 0.5 * (QI1 * Vij1 + QJ1 * Vji1) + 0.5 * (QI2 * Vij2 + QJ2 * Vji2) +
-               0.5 * (QI3 * Vij3 + QJ3 * Vji3);
-    T fIZ = QI0 * VijR0 + QI1 * VijR1 + QI2 * VijR2 + QI3 * VijR3;
-    T fJZ = QJ0 * VjiR0 + QJ1 * VjiR1 + QJ2 * VjiR2 + QJ3 * VjiR3;
-    T EIX = QI3 * Vij1 - QI1 * Vij3, EIY = QI1 * Vij2 - QI2 * Vij1, EIZ = QI2 * Vij3 - QI3 * Vij2;
-    T EJX = QJ3 * Vji1 - QJ1 * Vji3, EJY = QJ1 * Vji2 - QJ2 * Vji1, EJZ = QJ2 * Vji3 - QJ3 * Vji2;
-    T iEIX = uI2 * Vijd0 - uI0 * Vijd2, iEJX = uJ2 * Vjid0 - uJ0 * Vjid2;
-    T iEIY = uI0 * Vijd1 - uI1 * Vijd0, iEJY = uJ0 * Vjid1 - uJ1 * Vjid0;
-    if (mutual) {
-        T eC = (-4.0 * rv3 * iS) * td0;
-        T dC = (6.0 * rv4 * iS) * dtd0;
-        iEIX += eC * uI2 * uJ0;
-        iEJX += eC * uJ2 * uI0;
-        iEIY -= eC * uI1 * uJ0;
-        iEJY -= eC * uJ1 * uI0;
-        fIZ += dC * uI0 * uJ0;
-        fJZ += dC * uJ0 * uI0;
-        eC = (2.0 * rv3 * iS) * td1;
-        dC = (-3.0 * rv4 * iS) * dtd1;
-        iEIX -= eC * uI0 * uJ2;
-        iEJX -= eC * uJ0 * uI2;
-        iEIY += eC * uI0 * uJ1;
-        iEJY += eC * uJ0 * uI1;
-        fIZ += dC * (uI1 * uJ1 + uI2 * uJ2);
-        fJZ += dC * (uJ1 * uI1 + uJ2 * uI2);
-    }
-    T qf0 = rinv * (EIY + EJY + iEIY + iEJY);
-    T qf1 = -rinv * (EIX + EJX + iEIX + iEJX);
-    T qf2 = -(fJZ + fIZ);
-    T l = gE * energy + cf[0] * qf0 + cf[1] * qf1 + cf[2] * qf2;
-    l = l - (cti[0] * EIX + cti[1] * EIY + cti[2] * EIZ) - (ctk[0] * EJX + ctk[1] * EJY + ctk[2] * EJZ);
-    return l;
-}
-
-__device__ __forceinline__ V3 min_image(const PairParams& P, V3 d) {
-    if (P.periodic) {
-        d.x = fold_d(d.x, P.box[0], P.inv_box[0]);
-        d.y = fold_d(d.y, P.box[1], P.inv_box[1]);
-        d.z = fold_d(d.z, P.box[2], P.inv_box[2]);
-    }
-    return d;
-}
-
-struct AtomData {
-    const double* pos;     // n*3
-    const double* q;       // n
-    const double* lab;     // n*3
-    const double* mu;      // n*3
-    const double* thole;   // n
-    const double2* yz;     // raw (y, z) for the QI frame test
-};
-
-// Visits pair (me, j) with scales (mS, iS); accumulates d l / d(my q, lab, mu, t).
-__device__ void visit_pair(const PairParams& P, const AtomData& A, const double* g, const double* gT, double gE,
-                           int me, int j, double mS, double iS, double* acc) {
-    const bool meI = me < j;
-    const int I = meI ? me : j, K = meI ? j : me;
-    V3 d = min_image(P, {A.pos[3 * K] - A.pos[3 * I], A.pos[3 * K + 1] - A.pos[3 * I + 1],
-                         A.pos[3 * K + 2] - A.pos[3 * I + 2]});
-    double2 yzI = A.yz[I], yzK = A.yz[K];
-    bool yzd = (yzI.x != yzK.x) || (yzI.y != yzK.y);
-    V3 gFI = ld(g + 3 * I), gFK = ld(g + 3 * K), gTI = ld(gT + 3 * I), gTK = ld(gT + 3 * K);
-    const double rv4p = P.rinv4_power, rv4f = P.rinv4_fill;
-    const double damp_r2 = P.damp_r2 == 0.0f ? 0.0 : (double)P.damp_r2;
-    // Multipole derivatives: the pair function with my multipoles set to unit vectors.
-    double oq = A.q[meI ? K : I];
-    double om[3] = {A.lab[3 * (meI ? K : I)], A.lab[3 * (meI ? K : I) + 1], A.lab[3 * (meI ? K : I) + 2]};
-    double ou[3] = {A.mu[3 * (meI ? K : I)], A.mu[3 * (meI ? K : I) + 1], A.mu[3 * (meI ? K : I) + 2]};
-    double tI = A.thole[I], tK = A.thole[K];
-    for (int a = 0; a < 7; a++) {
-        double bq = a == 0 ? 1.0 : 0.0;
-        double bm[3] = {a == 1 ? 1.0 : 0.0, a == 2 ? 1.0 : 0.0, a == 3 ? 1.0 : 0.0};
-        double bu[3] = {a == 4 ? 1.0 : 0.0, a == 5 ? 1.0 : 0.0, a == 6 ? 1.0 : 0.0};
-        double l = meI ? pair_loss<double>(d.x, d.y, d.z, yzd, bq, bm, bu, tI, oq, om, ou, tK, mS, iS, damp_r2, rv4p,
-                                           rv4f, P.mutual, gE, gFI, gFK, gTI, gTK)
-                       : pair_loss<double>(d.x, d.y, d.z, yzd, oq, om, ou, tI, bq, bm, bu, tK, mS, iS, damp_r2, rv4p,
-                                           rv4f, P.mutual, gE, gFI, gFK, gTI, gTK);
-        acc[a] += l;
-    }
-    // Thole-factor derivative: dual number seeded on my t.
-    Dual dq[2], dm[2][3], du[2][3];
-    for (int s = 0; s < 2; s++) {
-        int at = s == 0 ? I : K;
-        dq[s] = mk(A.q[at]);
-        for (int c = 0; c < 3; c++) {
-            dm[s][c] = mk(A.lab[3 * at + c]);
-            du[s][c] = mk(A.mu[3 * at + c]);
-        }
-    }
-    Dual dtI = mk(tI, meI ? 1.0 : 0.0), dtK = mk(tK, meI ? 0.0 : 1.0);
-    Dual l = pair_loss<Dual>(d.x, d.y, d.z, yzd, dq[0], dm[0], du[0], dtI, dq[1], dm[1], du[1], dtK, mS, iS, damp_r2,
-                             rv4p, rv4f, P.mutual, gE, gFI, gFK, gTI, gTK);
-    acc[7] += l.d;
-}
 
 // a = d/d(q, lab, mu, t) of gE*E_pair + g.F_pair + gT.tau, per atom.  out: n*8.
 __global__ void k_pair_vjp(PairParams P, AtomData A, const double* __restrict__ g, const double* __restrict__ gT,
@@ -330,79 +53,28 @@ __global__ void k_pair_vjp(PairParams P, AtomData A, const double* __restrict__ 
 // b = d/d(q, lab, t) of lambda . Efix, per atom (out: n*5).  Field at i due to
 // k (RTDF.cpp:698-704): f_ik = -m [d (rr3 q_k - rr5 lab_k.d) + lab_k rr3],
 // d = p_k - p_i.
-template <class T>
-__device__ __forceinline__ T lam_dot_field(V3 d, double r, double r2, double damp_r2, T ti, T tk, double qk,
-                                           const double* labk, V3 lam_i, double m) {
-    T rr3, rr5;
-    field_damping<T>(r, r2, damp_r2, ti, tk, rr3, rr5);
-    double ld = lam_i.x * d.x + lam_i.y * d.y + lam_i.z * d.z;
-    double md = labk[0] * d.x + labk[1] * d.y + labk[2] * d.z;
-    double lm = lam_i.x * labk[0] + lam_i.y * labk[1] + lam_i.z * labk[2];
-    return -m * (ld * (rr3 * qk - rr5 * md) + rr3 * lm);
-}
-
 __global__ void k_fixed_vjp(PairParams P, AtomData A, const double* __restrict__ lam, const int* __restrict__ exc_off,
                             const int* __restrict__ exc_j, const double* __restrict__ exc_m, double* __restrict__ out) {
     int k = blockIdx.x * blockDim.x + threadIdx.x;
     if (k >= P.n) return;
-    const double damp_r2 = (double)P.damp_r2;
     double acc[5] = {0, 0, 0, 0, 0};
-    V3 lk = ld(lam + 3 * k);
-    const double* labk = A.lab + 3 * k;
-    auto visit = [&](int i, double m) {
-        V3 d = min_image(P, {A.pos[3 * k] - A.pos[3 * i], A.pos[3 * k + 1] - A.pos[3 * i + 1],
-                             A.pos[3 * k + 2] - A.pos[3 * i + 2]});  // p_k - p_i
-        double r2 = d.x * d.x + d.y * d.y + d.z * d.z, r = sqrt(r2);
-        V3 li = ld(lam + 3 * i);
-        double rr3, rr5;
-        field_damping<double>(r, r2, damp_r2, A.thole[i], A.thole[k], rr3, rr5);
-        double ldd = li.x * d.x + li.y * d.y + li.z * d.z;
-        acc[0] += -m * rr3 * ldd;  // d(lambda_i . f_ik)/dq_k
-        acc[1] += m * (rr5 * ldd * d.x - rr3 * li.x);
-        acc[2] += m * (rr5 * ldd * d.y - rr3 * li.y);
-        acc[3] += m * (rr5 * ldd * d.z - rr3 * li.z);
-        // t_k enters f_ik and f_ki: dual number on t_k.
-        V3 dn = {-d.x, -d.y, -d.z};
-        Dual tk = mk(A.thole[k], 1.0), ti = mk(A.thole[i]);
-        Dual s1 = lam_dot_field<Dual>(d, r, r2, damp_r2, ti, tk, A.q[k], labk, li, m);
-        Dual s2 = lam_dot_field<Dual>(dn, r, r2, damp_r2, tk, ti, A.q[i], A.lab + 3 * i, lk, m);
-        acc[4] += s1.d + s2.d;
-    };
     for (int i = 0; i < P.n; i++)
-        if (i != k) visit(i, 1.0);
-    for (int e = exc_off[k]; e < exc_off[k + 1]; e++) visit(exc_j[e], exc_m[e] - 1.0);
+        if (i != k) fixed_vjp_visit(P, A, lam, k, i, 1.0, acc);
+    for (int e = exc_off[k]; e < exc_off[k + 1]; e++) fixed_vjp_visit(P, A, lam, k, exc_j[e], exc_m[e] - 1.0, acc);
     for (int c = 0; c < 5; c++) out[5 * k + c] = acc[c];
 }
 
 // c_t = d/dt_k of lambda^T T(t) mu (RTDF.cpp:766-818), per atom.
 __global__ void k_matvec_t_vjp(PairParams P, AtomData A, const double* __restrict__ lam,
                                const int* __restrict__ exc_off, const int* __restrict__ exc_j,
-                               const double* __restrict__ exc_s, double* __restrict__ out) {
+                               const double* __restrict__ exc_s, double* __restrict__ out, int accumulate) {
     int k = blockIdx.x * blockDim.x + threadIdx.x;
     if (k >= P.n) return;
-    const double damp_r2 = (double)P.damp_r2;
     double acc = 0.0;
-    V3 lk = ld(lam + 3 * k), uk = ld(A.mu + 3 * k);
-    auto visit = [&](int j, double s) {
-        V3 d = min_image(P, {A.pos[3 * j] - A.pos[3 * k], A.pos[3 * j + 1] - A.pos[3 * k + 1],
-                             A.pos[3 * j + 2] - A.pos[3 * k + 2]});
-        double r2 = d.x * d.x + d.y * d.y + d.z * d.z, r = sqrt(r2);
-        if (!(r2 < damp_r2)) return;  // undamped pairs do not depend on t
-        Dual rr3, rr5;
-        field_damping<Dual>(r, r2, damp_r2, mk(A.thole[k], 1.0), mk(A.thole[j]), rr3, rr5);
-        V3 lj = ld(lam + 3 * j), uj = ld(A.mu + 3 * j);
-        // lambda_k.(T_kj mu_j) + lambda_j.(T_jk mu_k); T_kj v = -rr3 v + rr5 (v.d) d.
-        double a1 = (lk.x * d.x + lk.y * d.y + lk.z * d.z) * (uj.x * d.x + uj.y * d.y + uj.z * d.z);
-        double b1 = lk.x * uj.x + lk.y * uj.y + lk.z * uj.z;
-        double a2 = (lj.x * d.x + lj.y * d.y + lj.z * d.z) * (uk.x * d.x + uk.y * d.y + uk.z * d.z);
-        double b2 = lj.x * uk.x + lj.y * uk.y + lj.z * uk.z;
-        Dual v = s * (rr5 * (a1 + a2) - rr3 * (b1 + b2));
-        acc += v.d;
-    };
     for (int j = 0; j < P.n; j++)
-        if (j != k) visit(j, 1.0);
-    for (int e = exc_off[k]; e < exc_off[k + 1]; e++) visit(exc_j[e], exc_s[e] - 1.0);
-    out[k] = acc;
+        if (j != k) acc += matvec_t_visit(P, A, lam, k, j, 1.0);
+    for (int e = exc_off[k]; e < exc_off[k + 1]; e++) acc += matvec_t_visit(P, A, lam, k, exc_j[e], exc_s[e] - 1.0);
+    out[k] = accumulate ? out[k] + acc : acc;
 }
 
 }  // namespace adj
@@ -456,12 +128,14 @@ __global__ void k_rotation_vjp(int n, const double* __restrict__ pos, const int4
 __global__ void k_adjoint_assemble(int n, const double* __restrict__ a8, const double* __restrict__ b5,
                                    const double* __restrict__ ct, const double* __restrict__ amu_tlam,
                                    const double* __restrict__ e_tmu, const double* __restrict__ gmol,
-                                   double* __restrict__ out) {
+                                   double* __restrict__ out, const double* __restrict__ galpha) {
     int i = blockIdx.x * blockDim.x + threadIdx.x;
     if (i >= n) return;
     out[6 * i] = a8[8 * i] + b5[5 * i];
     double ga = 0.0;
-    for (int c = 0; c < 3; c++) ga += amu_tlam[3 * i + c] * e_tmu[3 * i + c];
+    if (galpha) ga = galpha[i];
+    else
+        for (int c = 0; c < 3; c++) ga += amu_tlam[3 * i + c] * e_tmu[3 * i + c];
     out[6 * i + 1] = ga;
     out[6 * i + 2] = a8[8 * i + 7] + b5[5 * i + 4] + ct[i];
     for (int c = 0; c < 3; c++) out[6 * i + 3 + c] = gmol[3 * i + c];
@@ -543,8 +217,36 @@ void launch_adjoint_fixed(const Dev& d, const double* lam, double* b5, cudaStrea
     adj::k_fixed_vjp<<<nb(d.n), 128, 0, st>>>(d.pp, A, lam, d.exc_off, d.exc_j, d.exc_m, b5);
 }
 void launch_adjoint_matvec_t(const Dev& d, const double* lam, double* ct, cudaStream_t st) {
-    adj::AtomData A{d.pos, d.charge, d.lab, d.mu, d.thole, d.yz};
-    adj::k_matvec_t_vjp<<<nb(d.n), 128, 0, st>>>(d.pp, A, lam, d.exc_off, d.exc_j, d.exc_s, ct);
+    launch_adjoint_matvec_t_mu(d, lam, d.mu, ct, false, st);
+}
+void launch_adjoint_matvec_t_mu(const Dev& d, const double* lam, const double* mu, double* ct, bool accumulate,
+                                cudaStream_t st) {
+    adj::AtomData A{d.pos, d.charge, d.lab, mu, d.thole, d.yz};
+    adj::k_matvec_t_vjp<<<nb(d.n), 128, 0, st>>>(d.pp, A, lam, d.exc_off, d.exc_j, d.exc_s, ct, accumulate ? 1 : 0);
+}
+
+__global__ void k_lincomb(int n3, double ca, const double* __restrict__ a, double cb, const double* __restrict__ b,
+                          double* __restrict__ out) {
+    int k = blockIdx.x * blockDim.x + threadIdx.x;
+    if (k < n3) out[k] = ca * a[k] + (b ? cb * b[k] : 0.0);
+}
+__global__ void k_dot3_acc(int n, const double* __restrict__ a, const double* __restrict__ b, double* __restrict__ acc) {
+    int i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i < n) acc[i] += a[3 * i] * b[3 * i] + a[3 * i + 1] * b[3 * i + 1] + a[3 * i + 2] * b[3 * i + 2];
+}
+__global__ void k_alpha_mul(int n, const double* __restrict__ alpha, const double* __restrict__ v,
+                            double* __restrict__ out) {
+    int k = blockIdx.x * blockDim.x + threadIdx.x;
+    if (k < 3 * n) out[k] = alpha[k / 3] * v[k];
+}
+void launch_lincomb(int n, double ca, const double* a, double cb, const double* b, double* out, cudaStream_t st) {
+    k_lincomb<<<nb(3 * n), 128, 0, st>>>(3 * n, ca, a, cb, b, out);
+}
+void launch_dot3_acc(int n, const double* a, const double* b, double* acc, cudaStream_t st) {
+    k_dot3_acc<<<nb(n), 128, 0, st>>>(n, a, b, acc);
+}
+void launch_alpha_scale(const Dev& d, const double* v, double* out, cudaStream_t st) {
+    k_alpha_mul<<<nb(3 * d.n), 128, 0, st>>>(d.n, d.alpha, v, out);
 }
 void launch_torque_vjp(const Dev& d, const double* g, double* gt, cudaStream_t st) {
     k_torque_vjp<<<nb(d.n), 128, 0, st>>>(d.n, d.pos, d.axis, g, gt);
@@ -574,8 +276,8 @@ template void launch_set_operand<float>(const Dev&, const double*, cudaStream_t)
 template void launch_set_operand<double>(const Dev&, const double*, cudaStream_t);
 void launch_adjoint_assemble(const Dev& d, const double* a8, const double* b5, const double* ct,
                              const double* amu_tlam, const double* e_tmu, const double* gmol, double* out,
-                             cudaStream_t st) {
-    k_adjoint_assemble<<<nb(d.n), 128, 0, st>>>(d.n, a8, b5, ct, amu_tlam, e_tmu, gmol, out);
+                             cudaStream_t st, const double* galpha) {
+    k_adjoint_assemble<<<nb(d.n), 128, 0, st>>>(d.n, a8, b5, ct, amu_tlam, e_tmu, gmol, out, galpha);
 }
 
 }  // namespace tdp

@@ -30,6 +30,7 @@
 #include "tdp_frames.cuh"
 #include "tdp_host.h"
 #include "tdp_pairs.cuh"
+#include "tdp_adjoint.cuh"
 
 #include <cuda_runtime.h>
 
@@ -366,6 +367,202 @@ __device__ double cg_residual(const Cl<R>& c, int n, const double* y, double* r,
     return rr;
 }
 
+// ---- per-cluster stages shared by the forward (k_batch) and reverse
+// (k_batch_adjoint) kernels; each ends with its writes visible to the CTA.
+
+// Cluster atoms [a0, a0 + n) into shared memory: FP64 positions, local axis
+// atoms, polarizabilities, the local exception list with its partner masks,
+// and the pair records (FP32 relative to the centroid in the mixed form).
+template <class R>
+__device__ __forceinline__ void cluster_load(const Cl<R>& c, const BatchArgs& A, int a0, int n) {
+    typedef typename Vec4T<R>::type V4;
+    const int e0 = A.exc_off[a0];
+    double cx = 0, cy = 0, cz = 0;
+    for (int i = threadIdx.x; i < n; i += blockDim.x) {
+        const int gi = a0 + i;
+        for (int k = 0; k < 3; k++) c.pos[3 * i + k] = A.pos[3 * (size_t)gi + k];
+        cx += c.pos[3 * i];
+        cy += c.pos[3 * i + 1];
+        cz += c.pos[3 * i + 2];
+        const int4 ax = A.axis[gi];
+        c.axis[i] = make_int4(ax.x, ax.y >= 0 ? ax.y - a0 : -1, ax.z >= 0 ? ax.z - a0 : -1,
+                              ax.w >= 0 ? ax.w - a0 : -1);
+        const double al = A.alpha[gi];
+        c.alpha[i] = al;
+        c.salpha[i] = al > 0.0 ? sqrt(al) : 0.0;
+        c.eoff[i] = A.exc_off[gi] - e0;
+        unsigned long long w = 0ull;
+        for (int e = A.exc_off[gi]; e < A.exc_off[gi + 1]; e++) {
+            const int j = A.exc_j[e] - a0;
+            c.ej[e - e0] = j;
+            c.em[e - e0] = (R)A.exc_m[e];
+            c.es[e - e0] = (R)A.exc_s[e];
+            const unsigned d = (unsigned)(j - i + 32);
+            w |= d < 63u ? 1ull << d : 1ull << 63;
+        }
+        c.emask[i] = w;
+    }
+    if (threadIdx.x == 0) c.eoff[n] = A.exc_off[a0 + n] - e0;
+    cx = bsum(cx, c.red) / n;
+    cy = bsum(cy, c.red) / n;
+    cz = bsum(cz, c.red) / n;
+    for (int i = threadIdx.x; i < n; i += blockDim.x) {
+        V4 pq;
+        if (sizeof(R) == 4) {
+            pq.x = (R)(c.pos[3 * i] - cx);
+            pq.y = (R)(c.pos[3 * i + 1] - cy);
+            pq.z = (R)(c.pos[3 * i + 2] - cz);
+        } else {
+            pq.x = (R)c.pos[3 * i];
+            pq.y = (R)c.pos[3 * i + 1];
+            pq.z = (R)c.pos[3 * i + 2];
+        }
+        pq.w = (R)A.charge[a0 + i];
+        c.posq[i] = pq;
+    }
+    __syncthreads();
+}
+
+// Lab-frame permanent dipoles (RTDF.cpp:432-571) into c.dipt (.w: Thole factor).
+template <class R>
+__device__ __forceinline__ void cluster_lab(const Cl<R>& c, const BatchArgs& A, int a0, int n) {
+    typedef typename Vec4T<R>::type V4;
+    for (int i = threadIdx.x; i < n; i += blockDim.x) {
+        double Rm[3][3], sy;
+        frame_rows(c.pos, c.axis[i], i, Rm, sy);
+        const double* dm = A.dip_mol + 3 * (size_t)(a0 + i);
+        const double d0 = dm[0], d1 = sy * dm[1], d2 = dm[2];
+        double lab[3];
+        for (int k = 0; k < 3; k++) lab[k] = 0.0 + d0 * Rm[0][k] + d1 * Rm[1][k] + d2 * Rm[2][k];
+        V4 dv;
+        dv.x = (R)lab[0];
+        dv.y = (R)lab[1];
+        dv.z = (R)lab[2];
+        dv.w = (R)A.thole[a0 + i];
+        c.dipt[i] = dv;
+    }
+    __syncthreads();
+}
+
+// Permanent field into c.E, then mu = alpha E and the operand records = mu.
+template <class R>
+__device__ __forceinline__ void cluster_fixed_field(const Cl<R>& c, const BatchArgs& A, int n, R damp_r2) {
+    typedef typename Vec4T<R>::type V4;
+    for (int base = 0; base < n; base += blockDim.x) {
+        const int na = min(n - base, (int)blockDim.x);
+        const Split sp = split(na, A.lmax);
+        const int i = base + sp.a;
+        R fx = 0, fy = 0, fz = 0;
+        if (sp.act) {
+            const V4 pi = c.posq[i];
+            const R ti = c.dipt[i].w;
+            for (int j = sp.l; j < n; j += sp.L) {
+                if (j == i) continue;
+                R m, s;
+                pair_scales(c, i, j, m, s);
+                if (m == R(0)) continue;
+                const V4 pj = c.posq[j], dj = c.dipt[j];
+                const R dx = pj.x - pi.x, dy = pj.y - pi.y, dz = pj.z - pi.z;
+                const R r2 = dx * dx + dy * dy + dz * dz;
+                R tx = 0, ty = 0, tz = 0;
+                pair_fixed<R>(dx, dy, dz, r2, pj.w, dj.x, dj.y, dj.z, ti, dj.w, damp_r2, tx, ty, tz);
+                fx += m * tx;
+                fy += m * ty;
+                fz += m * tz;
+            }
+        }
+        double* pt = c.part + 3 * threadIdx.x;
+        pt[0] = (double)fx;
+        pt[1] = (double)fy;
+        pt[2] = (double)fz;
+        __syncthreads();
+        if ((int)threadIdx.x < na)
+            for (int k = 0; k < 3; k++)
+                c.E[3 * (base + threadIdx.x) + k] = split_sum(c.part, 3, k, threadIdx.x, na, sp.T);
+        __syncthreads();
+    }
+    __syncthreads();
+    for (int i = threadIdx.x; i < n; i += blockDim.x) {
+        const double al = c.alpha[i];
+        for (int k = 0; k < 3; k++) c.mu[3 * i + k] = al * c.E[3 * i + k];
+        V4 v;
+        v.x = (R)c.mu[3 * i];
+        v.y = (R)c.mu[3 * i + 1];
+        v.z = (R)c.mu[3 * i + 2];
+        v.w = c.dipt[i].w;
+        c.vec[i] = v;
+    }
+    __syncthreads();
+}
+
+// Mutual polarization: CG in y = mu / sqrt(alpha) on (I - S T S) y = S E from
+// mu = alpha E (c.mu), stopping on the RMS Jacobi-step change (true residual
+// confirmed) at target or after cap iterations; leaves mu in c.mu.
+template <class R>
+__device__ __forceinline__ void cluster_cg(const Cl<R>& c, int n, int lmax, R damp_r2, double target, int cap,
+                                           int& it, double& eps) {
+    const int n3 = 3 * n;
+    double* y = c.w;
+    double* r = c.w + 3 * c.M;
+    double* p = c.w + 6 * c.M;
+    double* q = c.w + 9 * c.M;
+    for (int k = threadIdx.x; k < n3; k += blockDim.x) y[k] = c.salpha[k / 3] * c.E[k];
+    cluster_matvec(c, n, lmax, damp_r2, q);
+    double ee;
+    double rr = cg_residual(c, n, y, r, p, q, &ee);
+    eps = sqrt(ee / n);
+    bool is_true = true;
+    while (true) {
+        if (!(eps <= 1.0e300)) break;  // non-finite
+        if (eps <= target || it >= cap) {
+            if (is_true) break;
+            // Accept only on the true residual of the current iterate.
+            for (int i = threadIdx.x; i < n; i += blockDim.x) {
+                const double sa = c.salpha[i];
+                set_vec(c, i, sa * y[3 * i], sa * y[3 * i + 1], sa * y[3 * i + 2]);
+            }
+            __syncthreads();
+            cluster_matvec(c, n, lmax, damp_r2, q);
+            rr = cg_residual(c, n, y, r, p, q, &ee);
+            eps = sqrt(ee / n);
+            is_true = true;
+            continue;
+        }
+        __syncthreads();
+        cluster_matvec(c, n, lmax, damp_r2, q);  // T S p
+        double pq = 0.0;
+        for (int k = threadIdx.x; k < n3; k += blockDim.x) {
+            const double qv = p[k] - c.salpha[k / 3] * q[k];
+            q[k] = qv;
+            pq += p[k] * qv;
+        }
+        pq = bsum(pq, c.red);
+        const double a = rr / pq;
+        double rr2 = 0.0, e2 = 0.0;
+        for (int k = threadIdx.x; k < n3; k += blockDim.x) {
+            const double sa = c.salpha[k / 3];
+            y[k] += a * p[k];
+            const double rv = r[k] - a * q[k];
+            r[k] = rv;
+            rr2 += rv * rv;
+            e2 += sa * sa * rv * rv;
+        }
+        bsum2(rr2, e2, c.red);
+        eps = sqrt(e2 / n);
+        const double beta = rr2 / rr;
+        rr = rr2;
+        for (int i = threadIdx.x; i < n; i += blockDim.x) {
+            const double sa = c.salpha[i];
+            for (int k = 0; k < 3; k++) p[3 * i + k] = r[3 * i + k] + beta * p[3 * i + k];
+            set_vec(c, i, sa * p[3 * i], sa * p[3 * i + 1], sa * p[3 * i + 2]);
+        }
+        it++;
+        is_true = false;
+    }
+    __syncthreads();
+    for (int k = threadIdx.x; k < n3; k += blockDim.x) c.mu[k] = c.salpha[k / 3] * y[k];
+}
+
 template <class R>
 __global__ void __launch_bounds__(512) k_batch(BatchArgs A) {
     typedef typename Vec4T<R>::type V4;
@@ -390,182 +587,16 @@ __global__ void __launch_bounds__(512) k_batch(BatchArgs A) {
             }
             continue;
         }
-        const int e0 = A.exc_off[a0];
-
-        // ---- load ------------------------------------------------------------------------
-        double cx = 0, cy = 0, cz = 0;
-        for (int i = threadIdx.x; i < n; i += blockDim.x) {
-            const int gi = a0 + i;
-            for (int k = 0; k < 3; k++) c.pos[3 * i + k] = A.pos[3 * (size_t)gi + k];
-            cx += c.pos[3 * i];
-            cy += c.pos[3 * i + 1];
-            cz += c.pos[3 * i + 2];
-            const int4 ax = A.axis[gi];
-            c.axis[i] = make_int4(ax.x, ax.y >= 0 ? ax.y - a0 : -1, ax.z >= 0 ? ax.z - a0 : -1,
-                                  ax.w >= 0 ? ax.w - a0 : -1);
-            const double al = A.alpha[gi];
-            c.alpha[i] = al;
-            c.salpha[i] = al > 0.0 ? sqrt(al) : 0.0;
-            c.eoff[i] = A.exc_off[gi] - e0;
-            unsigned long long w = 0ull;
-            for (int e = A.exc_off[gi]; e < A.exc_off[gi + 1]; e++) {
-                const int j = A.exc_j[e] - a0;
-                c.ej[e - e0] = j;
-                c.em[e - e0] = (R)A.exc_m[e];
-                c.es[e - e0] = (R)A.exc_s[e];
-                const unsigned d = (unsigned)(j - i + 32);
-                w |= d < 63u ? 1ull << d : 1ull << 63;
-            }
-            c.emask[i] = w;
-        }
-        if (threadIdx.x == 0) c.eoff[n] = A.exc_off[a0 + n] - e0;
-        cx = bsum(cx, c.red) / n;
-        cy = bsum(cy, c.red) / n;
-        cz = bsum(cz, c.red) / n;
-        for (int i = threadIdx.x; i < n; i += blockDim.x) {
-            V4 pq;
-            if (sizeof(R) == 4) {
-                pq.x = (R)(c.pos[3 * i] - cx);
-                pq.y = (R)(c.pos[3 * i + 1] - cy);
-                pq.z = (R)(c.pos[3 * i + 2] - cz);
-            } else {
-                pq.x = (R)c.pos[3 * i];
-                pq.y = (R)c.pos[3 * i + 1];
-                pq.z = (R)c.pos[3 * i + 2];
-            }
-            pq.w = (R)A.charge[a0 + i];
-            c.posq[i] = pq;
-        }
-        __syncthreads();
-
-        // ---- lab-frame dipoles (RTDF.cpp:432-571) ------------------------------------------
-        for (int i = threadIdx.x; i < n; i += blockDim.x) {
-            double Rm[3][3], sy;
-            frame_rows(c.pos, c.axis[i], i, Rm, sy);
-            const double* dm = A.dip_mol + 3 * (size_t)(a0 + i);
-            const double d0 = dm[0], d1 = sy * dm[1], d2 = dm[2];
-            double lab[3];
-            for (int k = 0; k < 3; k++) lab[k] = 0.0 + d0 * Rm[0][k] + d1 * Rm[1][k] + d2 * Rm[2][k];
-            V4 dv;
-            dv.x = (R)lab[0];
-            dv.y = (R)lab[1];
-            dv.z = (R)lab[2];
-            dv.w = (R)A.thole[a0 + i];
-            c.dipt[i] = dv;
-        }
-        __syncthreads();
-
-        // ---- permanent field (RTDF.cpp:678-746): E, mu = alpha E --------------------------
-        for (int base = 0; base < n; base += blockDim.x) {
-            const int na = min(n - base, (int)blockDim.x);
-            const Split sp = split(na, A.lmax);
-            const int i = base + sp.a;
-            R fx = 0, fy = 0, fz = 0;
-            if (sp.act) {
-                const V4 pi = c.posq[i];
-                const R ti = c.dipt[i].w;
-                for (int j = sp.l; j < n; j += sp.L) {
-                    if (j == i) continue;
-                    R m, s;
-                    pair_scales(c, i, j, m, s);
-                    if (m == R(0)) continue;
-                    const V4 pj = c.posq[j], dj = c.dipt[j];
-                    const R dx = pj.x - pi.x, dy = pj.y - pi.y, dz = pj.z - pi.z;
-                    const R r2 = dx * dx + dy * dy + dz * dz;
-                    R tx = 0, ty = 0, tz = 0;
-                    pair_fixed<R>(dx, dy, dz, r2, pj.w, dj.x, dj.y, dj.z, ti, dj.w, damp_r2, tx, ty, tz);
-                    fx += m * tx;
-                    fy += m * ty;
-                    fz += m * tz;
-                }
-            }
-            double* pt = c.part + 3 * threadIdx.x;
-            pt[0] = (double)fx;
-            pt[1] = (double)fy;
-            pt[2] = (double)fz;
-            __syncthreads();
-            if ((int)threadIdx.x < na)
-                for (int k = 0; k < 3; k++)
-                    c.E[3 * (base + threadIdx.x) + k] = split_sum(c.part, 3, k, threadIdx.x, na, sp.T);
-            __syncthreads();
-        }
-        __syncthreads();
-        for (int i = threadIdx.x; i < n; i += blockDim.x) {
-            const double al = c.alpha[i];
-            for (int k = 0; k < 3; k++) c.mu[3 * i + k] = al * c.E[3 * i + k];
-            V4 v;
-            v.x = (R)c.mu[3 * i];
-            v.y = (R)c.mu[3 * i + 1];
-            v.z = (R)c.mu[3 * i + 2];
-            v.w = c.dipt[i].w;
-            c.vec[i] = v;
-        }
-        __syncthreads();
+        cluster_load(c, A, a0, n);
+        cluster_lab(c, A, a0, n);
+        cluster_fixed_field(c, A, n, damp_r2);
 
         // ---- induced dipoles ---------------------------------------------------------------
         int it = 0;
         double eps = 1.0e50;
         const int n3 = 3 * n;
         if (A.polarization == TDP_MUTUAL) {
-            double* y = c.w;
-            double* r = c.w + 3 * c.M;
-            double* p = c.w + 6 * c.M;
-            double* q = c.w + 9 * c.M;
-            for (int k = threadIdx.x; k < n3; k += blockDim.x) y[k] = c.salpha[k / 3] * c.E[k];
-            cluster_matvec(c, n, A.lmax, damp_r2, q);
-            double ee;
-            double rr = cg_residual(c, n, y, r, p, q, &ee);
-            eps = sqrt(ee / n);
-            bool is_true = true;
-            while (true) {
-                if (!(eps <= 1.0e300)) break;  // non-finite
-                if (eps <= A.target_eps || it >= A.max_iter) {
-                    if (is_true) break;
-                    // Accept only on the true residual of the current iterate.
-                    for (int i = threadIdx.x; i < n; i += blockDim.x) {
-                        const double sa = c.salpha[i];
-                        set_vec(c, i, sa * y[3 * i], sa * y[3 * i + 1], sa * y[3 * i + 2]);
-                    }
-                    __syncthreads();
-                    cluster_matvec(c, n, A.lmax, damp_r2, q);
-                    rr = cg_residual(c, n, y, r, p, q, &ee);
-                    eps = sqrt(ee / n);
-                    is_true = true;
-                    continue;
-                }
-                __syncthreads();
-                cluster_matvec(c, n, A.lmax, damp_r2, q);  // T S p
-                double pq = 0.0;
-                for (int k = threadIdx.x; k < n3; k += blockDim.x) {
-                    const double qv = p[k] - c.salpha[k / 3] * q[k];
-                    q[k] = qv;
-                    pq += p[k] * qv;
-                }
-                pq = bsum(pq, c.red);
-                const double a = rr / pq;
-                double rr2 = 0.0, e2 = 0.0;
-                for (int k = threadIdx.x; k < n3; k += blockDim.x) {
-                    const double sa = c.salpha[k / 3];
-                    y[k] += a * p[k];
-                    const double rv = r[k] - a * q[k];
-                    r[k] = rv;
-                    rr2 += rv * rv;
-                    e2 += sa * sa * rv * rv;
-                }
-                bsum2(rr2, e2, c.red);
-                eps = sqrt(e2 / n);
-                const double beta = rr2 / rr;
-                rr = rr2;
-                for (int i = threadIdx.x; i < n; i += blockDim.x) {
-                    const double sa = c.salpha[i];
-                    for (int k = 0; k < 3; k++) p[3 * i + k] = r[3 * i + k] + beta * p[3 * i + k];
-                    set_vec(c, i, sa * p[3 * i], sa * p[3 * i + 1], sa * p[3 * i + 2]);
-                }
-                it++;
-                is_true = false;
-            }
-            __syncthreads();
-            for (int k = threadIdx.x; k < n3; k += blockDim.x) c.mu[k] = c.salpha[k / 3] * y[k];
+            cluster_cg(c, n, A.lmax, damp_r2, A.target_eps, A.max_iter, it, eps);
         } else if (A.polarization == TDP_EXTRAPOLATED) {
             // Perturbation-theory extrapolation (RTDF.cpp:853-909).
             double* hist = c.w;                               // korder slots of 3M
@@ -685,6 +716,249 @@ __global__ void __launch_bounds__(512) k_batch(BatchArgs A) {
     }
 }
 
+
+// ---------------------------------------------------------------------------
+// Reverse pass (tdp_batch_adjoint): per cluster, the chain of tdp_adjoint
+// (tdp_adjoint.cu) in one CTA -- torque-map VJP, pair VJPs, one adjoint solve
+// of the cluster's (alpha^-1 - T) system (Mutual), the permanent-field and
+// mutual-field VJPs and the rotation transpose -- from the forward's induced
+// dipoles, with every per-atom vector in shared memory.  The pair VJPs run in
+// FP64; the adjoint solve uses the form's matvec (FP32 pair arithmetic with
+// FP64 vectors in the mixed form) to 1e-12 of the right-hand side's scale.
+// ---------------------------------------------------------------------------
+struct AdjArgs {
+    const double* gF;   // n*3 dL/dF (NULL: zero)
+    const double* gE;   // per-cluster dL/dE (NULL: zero)
+    double* grads;      // n*6: dq, dalpha, dthole, dmu_mol[3]
+    int* iters;         // per-cluster adjoint CG iterations
+    double* eps;        // per-cluster final adjoint residual (Jacobi-step units)
+    int* queue;
+};
+
+// FP64 per-atom arrays of the reverse pass, after the forward's layout.
+struct AdjCl {
+    double *gF, *gT, *a8, *b5, *ct, *lab, *q, *th, *muf, *amu, *lam, *etm, *part;
+};
+__host__ __device__ inline size_t adj_extra_doubles(int M) { return (size_t)M * 38 + 8 * 512; }
+
+template <class R>
+__host__ __device__ inline size_t batch_adjoint_smem(int M, int X, int korder) {
+    return batch_smem<R>(M, X, korder) + sizeof(double) * adj_extra_doubles(M);
+}
+
+template <class R>
+__device__ AdjCl carve_adj(char* base, int M, int X, int korder) {
+    double* d = reinterpret_cast<double*>(base + batch_smem<R>(M, X, korder));
+    AdjCl g;
+    g.gF = d; d += 3 * M;
+    g.gT = d; d += 3 * M;
+    g.a8 = d; d += 8 * M;
+    g.b5 = d; d += 5 * M;
+    g.ct = d; d += M;
+    g.lab = d; d += 3 * M;
+    g.q = d; d += M;
+    g.th = d; d += M;
+    g.muf = d; d += 3 * M;
+    g.amu = d; d += 3 * M;
+    g.lam = d; d += 3 * M;
+    g.etm = d; d += 3 * M;   // 38 M so far
+    g.part = d;               // 8 per thread
+    return g;
+}
+
+// out := T x over the cluster (operand records set from x).
+template <class R>
+__device__ __forceinline__ void cluster_apply_t(const Cl<R>& c, int n, int lmax, R damp_r2, const double* x,
+                                                double* out) {
+    for (int i = threadIdx.x; i < n; i += blockDim.x) set_vec(c, i, x[3 * i], x[3 * i + 1], x[3 * i + 2]);
+    __syncthreads();
+    cluster_matvec(c, n, lmax, damp_r2, out);
+}
+
+template <class R>
+__global__ void __launch_bounds__(512) k_batch_adjoint(BatchArgs A, AdjArgs G) {
+    extern __shared__ __align__(32) char smem_raw[];
+    const Cl<R> c = carve<R>(smem_raw, A.max_atoms, A.max_exc, A.korder);
+    const AdjCl g = carve_adj<R>(smem_raw, A.max_atoms, A.max_exc, A.korder);
+    __shared__ int s_slot;
+    const R damp_r2 = (R)A.damp_r2;
+    PairParams P{};
+    P.periodic = 0;
+    P.damp_r2 = (float)A.damp_r2;
+    P.rinv4_power = (float)A.rinv4_power;
+    P.rinv4_fill = (float)A.rinv4_fill;
+    P.mutual = A.polarization == TDP_MUTUAL ? 1 : 0;
+    while (true) {
+        __syncthreads();
+        if (threadIdx.x == 0) s_slot = atomicAdd(G.queue, 1);
+        __syncthreads();
+        const int slot = s_slot;
+        if (slot >= A.num_clusters) break;
+        const int cid = A.order[slot];
+        const int a0 = A.coff[cid], n = A.coff[cid + 1] - a0;
+        if (n <= 0) {
+            if (threadIdx.x == 0) {
+                G.iters[cid] = 0;
+                G.eps[cid] = 0.0;
+            }
+            continue;
+        }
+        P.n = n;
+        cluster_load(c, A, a0, n);
+        cluster_lab(c, A, a0, n);
+        for (int i = threadIdx.x; i < n; i += blockDim.x) {
+            const int gi = a0 + i;
+            double Rm[3][3], sy;
+            frame_rows(c.pos, c.axis[i], i, Rm, sy);
+            const double* dm = A.dip_mol + 3 * (size_t)gi;
+            const double d0 = dm[0], d1 = sy * dm[1], d2 = dm[2];
+            for (int k = 0; k < 3; k++) {
+                g.lab[3 * i + k] = 0.0 + d0 * Rm[0][k] + d1 * Rm[1][k] + d2 * Rm[2][k];
+                g.muf[3 * i + k] = A.mu_out[3 * (size_t)gi + k];
+                g.gF[3 * i + k] = G.gF ? G.gF[3 * (size_t)gi + k] : 0.0;
+            }
+            g.q[i] = A.charge[gi];
+            g.th[i] = A.thole[gi];
+        }
+        const double gE = G.gE ? G.gE[cid] : 0.0;
+        // Permanent field of the forward into c.E (also sets c.mu = alpha E).
+        cluster_fixed_field(c, A, n, damp_r2);
+        for (int k = threadIdx.x; k < 3 * n; k += blockDim.x) g.etm[k] = c.E[k];
+
+        // ---- g_tau = M^T g (k_torque_vjp) -------------------------------------------------
+        for (int i = threadIdx.x; i < n; i += blockDim.x) {
+            const int4 ax = c.axis[i];
+            double o[3] = {0.0, 0.0, 0.0};
+            if (ax.x != TDP_NO_AXIS_TYPE) {
+                const int atoms[4] = {i, ax.y, ax.z, ax.w};
+                for (int role = 0; role < 4; role++) {
+                    const int at = atoms[role];
+                    if (at < 0) continue;
+                    if (role == 2 && ax.x == TDP_ZONLY) continue;
+                    if (role == 3 && !(ax.x == TDP_ZBISECT || ax.x == TDP_THREEFOLD)) continue;
+                    for (int k = 0; k < 3; k++) {
+                        const d3 e = {k == 0 ? 1.0 : 0.0, k == 1 ? 1.0 : 0.0, k == 2 ? 1.0 : 0.0};
+                        const d3 f = torque_role_force(c.pos, ax, i, role, e);
+                        o[k] += f.x * g.gF[3 * at] + f.y * g.gF[3 * at + 1] + f.z * g.gF[3 * at + 2];
+                    }
+                }
+            }
+            for (int k = 0; k < 3; k++) g.gT[3 * i + k] = o[k];
+        }
+        __syncthreads();
+        const adj::AtomData AD{c.pos, g.q, g.lab, g.muf, g.th, nullptr};
+
+        // ---- a = pair VJPs (k_pair_vjp): 8 per atom ----------------------------------------
+        for (int base = 0; base < n; base += blockDim.x) {
+            const int na = min(n - base, (int)blockDim.x);
+            const Split sp = split(na, A.lmax);
+            const int i = base + sp.a;
+            double acc[8] = {0, 0, 0, 0, 0, 0, 0, 0};
+            if (sp.act)
+                for (int j = sp.l; j < n; j += sp.L) {
+                    if (j == i) continue;
+                    R m, s;
+                    pair_scales(c, i, j, m, s);
+                    if (m == R(0) && s == R(0)) continue;
+                    adj::visit_pair(P, AD, g.gF, g.gT, gE, i, j, (double)m, (double)s, acc);
+                }
+            for (int k = 0; k < 8; k++) g.part[8 * threadIdx.x + k] = acc[k];
+            __syncthreads();
+            if ((int)threadIdx.x < na)
+                for (int k = 0; k < 8; k++)
+                    g.a8[8 * (base + threadIdx.x) + k] = split_sum(g.part, 8, k, threadIdx.x, na, sp.T);
+            __syncthreads();
+        }
+        double s2 = 0.0;
+        for (int i = threadIdx.x; i < n; i += blockDim.x)
+            for (int k = 0; k < 3; k++) {
+                const double v = g.a8[8 * i + 4 + k];
+                g.amu[3 * i + k] = v;
+                s2 += (c.alpha[i] * v) * (c.alpha[i] * v);
+            }
+        s2 = bsum(s2, c.red);
+
+        // ---- adjoint solve and the field VJPs ----------------------------------------------
+        int it = 0;
+        double eps = 0.0;
+        if (A.polarization == TDP_MUTUAL) {
+            // E + T mu of the forward, for the polarizability gradient.
+            cluster_apply_t(c, n, A.lmax, damp_r2, g.muf, g.lam);
+            for (int k = threadIdx.x; k < 3 * n; k += blockDim.x) g.etm[k] += g.lam[k];
+            // A lambda = a_mu: the forward's CG with E := a_mu, from lambda = alpha a_mu.
+            for (int i = threadIdx.x; i < n; i += blockDim.x) {
+                for (int k = 0; k < 3; k++) {
+                    c.E[3 * i + k] = g.amu[3 * i + k];
+                    c.mu[3 * i + k] = c.alpha[i] * g.amu[3 * i + k];
+                }
+                set_vec(c, i, c.mu[3 * i], c.mu[3 * i + 1], c.mu[3 * i + 2]);
+            }
+            __syncthreads();
+            const double target = fmax(sqrt(s2 / n) * 1e-12, 1e-300);
+            eps = 1.0e50;
+            cluster_cg(c, n, A.lmax, damp_r2, target, A.max_iter > 1000 ? A.max_iter : 1000, it, eps);
+            __syncthreads();
+            for (int k = threadIdx.x; k < 3 * n; k += blockDim.x) g.lam[k] = c.mu[k];
+            __syncthreads();
+            // a_mu + T lambda (into amu) for the polarizability gradient.
+            cluster_apply_t(c, n, A.lmax, damp_r2, g.lam, c.E);
+            for (int k = threadIdx.x; k < 3 * n; k += blockDim.x) g.amu[k] += c.E[k];
+        } else {
+            // Direct: mu = alpha E, so lambda = alpha a_mu and dL/dalpha = a_mu . E.
+            for (int i = threadIdx.x; i < n; i += blockDim.x)
+                for (int k = 0; k < 3; k++) g.lam[3 * i + k] = c.alpha[i] * g.amu[3 * i + k];
+        }
+        __syncthreads();
+        // b = d/d(q, lab, t) of lambda . Efix (k_fixed_vjp), c_t = d/dt of lambda^T T mu.
+        for (int base = 0; base < n; base += blockDim.x) {
+            const int na = min(n - base, (int)blockDim.x);
+            const Split sp = split(na, A.lmax);
+            const int k = base + sp.a;
+            double acc[6] = {0, 0, 0, 0, 0, 0};
+            if (sp.act)
+                for (int j = sp.l; j < n; j += sp.L) {
+                    if (j == k) continue;
+                    R m, s;
+                    pair_scales(c, k, j, m, s);
+                    if (m != R(0)) adj::fixed_vjp_visit(P, AD, g.lam, k, j, (double)m, acc);
+                    if (A.polarization == TDP_MUTUAL && s != R(0))
+                        acc[5] += adj::matvec_t_visit(P, AD, g.lam, k, j, (double)s);
+                }
+            for (int u = 0; u < 6; u++) g.part[8 * threadIdx.x + u] = acc[u];
+            __syncthreads();
+            if ((int)threadIdx.x < na) {
+                const int a = base + threadIdx.x;
+                for (int u = 0; u < 5; u++) g.b5[5 * a + u] = split_sum(g.part, 8, u, threadIdx.x, na, sp.T);
+                g.ct[a] = split_sum(g.part, 8, 5, threadIdx.x, na, sp.T);
+            }
+            __syncthreads();
+        }
+
+        // ---- rotation transpose and assembly (k_rotation_vjp, k_adjoint_assemble) ---------
+        for (int i = threadIdx.x; i < n; i += blockDim.x) {
+            const int gi = a0 + i;
+            double Rm[3][3], sy;
+            frame_rows(c.pos, c.axis[i], i, Rm, sy);
+            double gl[3];
+            for (int k = 0; k < 3; k++) gl[k] = g.a8[8 * i + 1 + k] + g.b5[5 * i + 1 + k];
+            double* o = G.grads + 6 * (size_t)gi;
+            o[0] = g.a8[8 * i] + g.b5[5 * i];
+            double ga = 0.0;
+            for (int k = 0; k < 3; k++) ga += g.amu[3 * i + k] * g.etm[3 * i + k];
+            o[1] = ga;
+            o[2] = g.a8[8 * i + 7] + g.b5[5 * i + 4] + g.ct[i];
+            for (int j = 0; j < 3; j++) {
+                const double v = Rm[j][0] * gl[0] + Rm[j][1] * gl[1] + Rm[j][2] * gl[2];
+                o[3 + j] = j == 1 ? sy * v : v;
+            }
+        }
+        if (threadIdx.x == 0) {
+            G.iters[cid] = it;
+            G.eps[cid] = eps;
+        }
+    }
+}
+
 }  // namespace
 }  // namespace tdp
 
@@ -715,6 +989,9 @@ struct tdp_batch {
     cudaEvent_t ev0 = nullptr, ev1 = nullptr;
     double last_ms = 0.0;
     bool have_results = false;
+    // Reverse pass (allocated on the first tdp_batch_adjoint).
+    AdjArgs adj{};
+    int adj_ctas = 0;
     std::string err;
 };
 
@@ -1099,6 +1376,115 @@ int tdp_batch_tile(const tdp_batch* b, int32_t* threads, int32_t* lanes, int32_t
     if (lanes) *lanes = b->tuned ? b->lmax : 0;
     if (ctas) *ctas = b->tuned ? b->ctas : 0;
     if (last_ms) *last_ms = b->last_ms;
+    return TDP_OK;
+}
+
+int tdp_batch_update_params(tdp_batch* b, const double* charges, const double* molecular_dipoles,
+                            const double* polarizabilities, const double* thole_damping, int32_t on_device) {
+    if (!b) return TDP_ERR_INVALID_ARGUMENT;
+    try {
+        const size_t n = (size_t)b->n;
+        if (n == 0) return TDP_OK;
+        if (!charges || !molecular_dipoles || !polarizabilities || !thole_damping)
+            throw TdpError{TDP_ERR_INVALID_ARGUMENT, "a per-particle array is NULL"};
+        cudaStream_t st = b->stream;
+        const cudaMemcpyKind kind = on_device ? cudaMemcpyDeviceToDevice : cudaMemcpyHostToDevice;
+        BatchArgs& a = b->args;
+        TDP_CUDA(cudaMemcpyAsync((void*)a.charge, charges, sizeof(double) * n, kind, st));
+        TDP_CUDA(cudaMemcpyAsync((void*)a.dip_mol, molecular_dipoles, sizeof(double) * 3 * n, kind, st));
+        TDP_CUDA(cudaMemcpyAsync((void*)a.alpha, polarizabilities, sizeof(double) * n, kind, st));
+        TDP_CUDA(cudaMemcpyAsync((void*)a.thole, thole_damping, sizeof(double) * n, kind, st));
+        // The damping radius follows the largest Thole factor.
+        std::vector<double> th(n);
+        if (on_device) {
+            TDP_CUDA(cudaMemcpyAsync(th.data(), thole_damping, sizeof(double) * n, cudaMemcpyDeviceToHost, st));
+            TDP_CUDA(cudaStreamSynchronize(st));
+        } else {
+            th.assign(thole_damping, thole_damping + n);
+        }
+        const double dr2 = damp_radius2(th);
+        if (dr2 != a.damp_r2) {
+            a.damp_r2 = dr2;
+            if (b->tuned) build_graph(b);
+        }
+        b->have_results = false;
+    } catch (const TdpError& e) {
+        return batch_fail(b, e);
+    }
+    return TDP_OK;
+}
+
+int tdp_batch_adjoint(tdp_batch* b, const double* dL_dF, const double* dL_dE, int32_t on_device, double* grads) {
+    if (!b || !grads) return TDP_ERR_INVALID_ARGUMENT;
+    try {
+        if (b->nc == 0 || b->n == 0) return TDP_OK;
+        if (!b->have_results) throw TdpError{TDP_ERR_INVALID_ARGUMENT, "tdp_batch_adjoint needs a previous tdp_batch_compute"};
+        if (b->polarization == TDP_EXTRAPOLATED)
+            throw TdpError{TDP_ERR_UNSUPPORTED, "tdp_batch_adjoint supports Direct and Mutual polarization"};
+        cudaStream_t st = b->stream;
+        const size_t n = (size_t)b->n;
+        const int korder = std::max(1, (int)b->extrap.size());
+        const int M = std::max(1, b->max_atoms);
+        const size_t smem = b->precision == TDP_PRECISION_DOUBLE ? batch_adjoint_smem<double>(M, b->max_exc, korder)
+                                                                 : batch_adjoint_smem<float>(M, b->max_exc, korder);
+        if (smem > b->smem_optin) {
+            char buf[200];
+            snprintf(buf, sizeof buf, "the reverse pass of the largest cluster (%d atoms) needs %zu bytes of shared "
+                     "memory; %zu available", b->max_atoms, smem, b->smem_optin);
+            throw TdpError{TDP_ERR_UNSUPPORTED, buf};
+        }
+        const void* kern = b->precision == TDP_PRECISION_DOUBLE ? (const void*)k_batch_adjoint<double>
+                                                                : (const void*)k_batch_adjoint<float>;
+        const int threads = b->tuned ? b->threads : 128;
+        const int lmax = b->tuned ? b->lmax : 8;
+        AdjArgs& g = b->adj;
+        if (!g.grads) {
+            auto& o = b->owned;
+            g.gF = dalloc<double>(3 * n, o);
+            g.gE = dalloc<double>((size_t)b->nc, o);
+            g.grads = dalloc<double>(6 * n, o);
+            g.iters = dalloc<int>((size_t)b->nc, o);
+            g.eps = dalloc<double>((size_t)b->nc, o);
+            g.queue = dalloc<int>(1, o);
+            TDP_CUDA(cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
+            int per_sm = 0;
+            TDP_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, kern, threads, smem));
+            if (per_sm < 1) throw TdpError{TDP_ERR_UNSUPPORTED, "the reverse pass does not fit an SM"};
+            b->adj_ctas = std::max(1, std::min(b->nc, per_sm * b->num_sms));
+        }
+        const cudaMemcpyKind kind = on_device ? cudaMemcpyDeviceToDevice : cudaMemcpyHostToDevice;
+        AdjArgs args = g;
+        if (dL_dF) TDP_CUDA(cudaMemcpyAsync((void*)g.gF, dL_dF, sizeof(double) * 3 * n, kind, st));
+        else args.gF = nullptr;
+        if (dL_dE) TDP_CUDA(cudaMemcpyAsync((void*)g.gE, dL_dE, sizeof(double) * b->nc, kind, st));
+        else args.gE = nullptr;
+        TDP_CUDA(cudaMemsetAsync(g.queue, 0, sizeof(int), st));
+        BatchArgs a = b->args;
+        a.lmax = lmax;
+        if (b->precision == TDP_PRECISION_DOUBLE) k_batch_adjoint<double><<<b->adj_ctas, threads, smem, st>>>(a, args);
+        else k_batch_adjoint<float><<<b->adj_ctas, threads, smem, st>>>(a, args);
+        TDP_CUDA(cudaGetLastError());
+        TDP_CUDA(cudaMemcpyAsync(grads, g.grads, sizeof(double) * 6 * n,
+                                 on_device ? cudaMemcpyDeviceToDevice : cudaMemcpyDeviceToHost, st));
+        if (!on_device) TDP_CUDA(cudaStreamSynchronize(st));
+    } catch (const TdpError& e) {
+        return batch_fail(b, e);
+    }
+    return TDP_OK;
+}
+
+int tdp_batch_adjoint_stats(tdp_batch* b, int32_t* iterations, double* epsilons) {
+    if (!b) return TDP_ERR_INVALID_ARGUMENT;
+    try {
+        if (!b->adj.grads) throw TdpError{TDP_ERR_INVALID_ARGUMENT, "no tdp_batch_adjoint yet"};
+        if (iterations && b->nc)
+            TDP_CUDA(cudaMemcpyAsync(iterations, b->adj.iters, sizeof(int) * b->nc, cudaMemcpyDeviceToHost, b->stream));
+        if (epsilons && b->nc)
+            TDP_CUDA(cudaMemcpyAsync(epsilons, b->adj.eps, sizeof(double) * b->nc, cudaMemcpyDeviceToHost, b->stream));
+        TDP_CUDA(cudaStreamSynchronize(b->stream));
+    } catch (const TdpError& e) {
+        return batch_fail(b, e);
+    }
     return TDP_OK;
 }
 

@@ -94,6 +94,10 @@ struct tdp_handle {
     Ewald* ew = nullptr;
     double total_charge = 0.0;
 
+    // Device scratch of the device-side parameter update and the adjoint's
+    // right-hand-side scale (allocated on first use).
+    double* d_pstat = nullptr;
+
     // Adjoint work buffers (allocated on first use).
     double* adj = nullptr;
     double adj_eps = 0.0;
@@ -145,6 +149,69 @@ void upload_params(tdp_handle* h) {
     d.users = dalloc<int2>(flat.size(), h->owned);
     upload(d.users_off, off.data(), sizeof(int) * (n + 1));
     upload(d.users, flat.data(), sizeof(int2) * flat.size());
+}
+
+// Per-particle parameters given on the device: sqrt(alpha), and in one CTA
+// (fixed summation order) the largest Thole factor, whether any is negative or
+// not a number, and the net charge as the pair records hold it.
+__global__ void k_param_stats(int n, int f32_charges, const double* __restrict__ alpha,
+                              const double* __restrict__ thole, const double* __restrict__ charge,
+                              double* __restrict__ salpha, double* __restrict__ out) {
+    __shared__ double s_max[1024], s_q[1024];
+    __shared__ int s_bad[1024];
+    double tmax = 0.0, qsum = 0.0;
+    int bad = 0;
+    for (int i = threadIdx.x; i < n; i += blockDim.x) {
+        const double a = alpha[i];
+        salpha[i] = a > 0.0 ? sqrt(a) : 0.0;
+        const double t = thole[i];
+        if (t < 0.0 || isnan(t)) bad = 1;
+        else tmax = fmax(tmax, t);
+        qsum += f32_charges ? (double)(float)charge[i] : charge[i];
+    }
+    s_max[threadIdx.x] = tmax;
+    s_q[threadIdx.x] = qsum;
+    s_bad[threadIdx.x] = bad;
+    __syncthreads();
+    if (threadIdx.x == 0) {
+        for (unsigned k = 1; k < blockDim.x; k++) {
+            tmax = fmax(tmax, s_max[k]);
+            qsum += s_q[k];
+            bad |= s_bad[k];
+        }
+        out[0] = tmax;
+        out[1] = bad;
+        out[2] = qsum;
+    }
+}
+
+// s2 = sum_i |alpha_i v_i|^2 over n*3 values, one CTA, fixed order.
+__global__ void k_alpha_norm2(int n, const double* __restrict__ alpha, const double* __restrict__ v,
+                              double* __restrict__ out) {
+    __shared__ double s[1024];
+    double acc = 0.0;
+    for (int k = threadIdx.x; k < 3 * n; k += blockDim.x) {
+        const double x = alpha[k / 3] * v[k];
+        acc += x * x;
+    }
+    s[threadIdx.x] = acc;
+    __syncthreads();
+    if (threadIdx.x == 0) {
+        for (unsigned k = 1; k < blockDim.x; k++) acc += s[k];
+        out[0] = acc;
+    }
+}
+
+// out = alpha v (n*3).
+__global__ void k_alpha_scale(int n, const double* __restrict__ alpha, const double* __restrict__ v,
+                              double* __restrict__ out) {
+    const int k = blockIdx.x * blockDim.x + threadIdx.x;
+    if (k < 3 * n) out[k] = alpha[k / 3] * v[k];
+}
+
+double* pstat(tdp_handle* h) {
+    if (!h->d_pstat) h->d_pstat = dalloc<double>(4, h->owned);
+    return h->d_pstat;
 }
 
 void refresh_box(tdp_handle* h) {
@@ -310,6 +377,17 @@ void stage_positions(tdp_handle* h, const void* positions, int dtype, int on_dev
         else
             launch_positions_in(d, positions, 1, h->stream);
     } else {
+        // Host coordinates are checked here, before any device work; device
+        // coordinates that are not finite surface as a non-finite solve or sum.
+        bool finite = true;
+        if (dtype == TDP_F64) {
+            const double* p = static_cast<const double*>(positions);
+            for (size_t k = 0; k < n3; k++) finite &= std::isfinite(p[k]);
+        } else {
+            const float* p = static_cast<const float*>(positions);
+            for (size_t k = 0; k < n3; k++) finite &= std::isfinite(p[k]);
+        }
+        if (!finite) throw TdpError{TDP_ERR_NON_FINITE, "a particle coordinate is not finite"};
         if (dtype == TDP_F64) {
             TDP_CUDA(cudaMemcpyAsync(d.pos, positions, n3 * 8, cudaMemcpyHostToDevice, h->stream));
         } else {
@@ -597,10 +675,13 @@ void check_flags(tdp_handle* h) {
                        "(2^23 per band sum; near-coincident particles?)"};
 }
 
+// positions == &kStaged: the coordinates are already in d.pos.
+const char kStaged = 0;
+
 void solve_at(tdp_handle* h, const void* positions, int dtype, int on_device) {
     if (positions) {
         check_box(h);
-        stage_positions(h, positions, dtype, on_device);
+        if (positions != &kStaged) stage_positions(h, positions, dtype, on_device);
         if (!h->sorted || ++h->since_sort >= h->resort_interval) sort_atoms(h);
         if (h->precision == TDP_PRECISION_DOUBLE) setup_and_solve<double>(h);
         else setup_and_solve<float>(h);
@@ -614,12 +695,13 @@ void solve_at(tdp_handle* h, const void* positions, int dtype, int on_device) {
 // derivation).  Needs the state of the last evaluation (positions, lab-frame
 // and induced dipoles, permanent field); leaves it as it was.
 template <class R>
-void run_adjoint(tdp_handle* h, const double* g_host, double gE, double* out_host) {
+void run_adjoint(tdp_handle* h, const double* g_in, double gE, double* out_dst, bool on_device) {
     Dev& d = h->d;
     cudaStream_t st = h->stream;
     const int n = h->n;
     const size_t n3 = 3 * (size_t)n;
-    if (!h->adj) h->adj = dalloc<double>(n3 * 10 + 8 * (size_t)n + 5 * (size_t)n + n + 6 * (size_t)n, h->owned);
+    if (!h->adj) h->adj = dalloc<double>(n3 * 11 + 8 * (size_t)n + 5 * (size_t)n + 2 * (size_t)n + 6 * (size_t)n,
+                                         h->owned);
     double* g = h->adj;
     double* gt = g + n3;
     double* amu = gt + n3;
@@ -634,8 +716,12 @@ void run_adjoint(tdp_handle* h, const double* g_host, double gE, double* out_hos
     double* b5 = a8 + 8 * (size_t)n;
     double* ct = b5 + 5 * (size_t)n;
     double* out = ct + n;
-    if (g_host) TDP_CUDA(cudaMemcpyAsync(g, g_host, n3 * 8, cudaMemcpyHostToDevice, st));
-    else TDP_CUDA(cudaMemsetAsync(g, 0, n3 * 8, st));
+    double* ext_v = out + 6 * (size_t)n;   // Extrapolated: E + T mu_(k-1)
+    double* galpha = ext_v + n3;           // Extrapolated: polarizability gradient
+    if (g_in)
+        TDP_CUDA(cudaMemcpyAsync(g, g_in, n3 * 8, on_device ? cudaMemcpyDeviceToDevice : cudaMemcpyHostToDevice, st));
+    else
+        TDP_CUDA(cudaMemsetAsync(g, 0, n3 * 8, st));
     TDP_CUDA(cudaMemcpyAsync(mu_fwd, d.mu, n3 * 8, cudaMemcpyDeviceToDevice, st));
     TDP_CUDA(cudaMemcpyAsync(E_fwd, d.E, n3 * 8, cudaMemcpyDeviceToDevice, st));
     launch_torque_vjp(d, g, gt, st);
@@ -644,11 +730,9 @@ void run_adjoint(tdp_handle* h, const double* g_host, double gE, double* out_hos
     if (h->polarization == TDP_MUTUAL) {
         // One solve of the same symmetric system: A lambda = a_mu.  Target:
         // 1e-12 of the RMS of alpha * a_mu (the solver's Jacobi-step units).
-        std::vector<double> ha(n3);
-        TDP_CUDA(cudaMemcpyAsync(ha.data(), amu, n3 * 8, cudaMemcpyDeviceToHost, st));
-        TDP_CUDA(cudaStreamSynchronize(st));
-        double s2 = 0.0;
-        for (size_t k = 0; k < n3; k++) s2 += (h->alpha[k / 3] * ha[k]) * (h->alpha[k / 3] * ha[k]);
+        double* ps = pstat(h);
+        k_alpha_norm2<<<1, 1024, 0, st>>>(n, d.alpha, amu, ps);
+        const double s2 = read_scalar(h, ps);
         double rms = std::sqrt(s2 / std::max(n, 1));
         int it0 = h->iterations, conv0 = h->converged, st0 = h->status, mv0 = h->matvecs;
         double eps0 = h->epsilon, tgt0 = h->target_eps;
@@ -677,14 +761,40 @@ void run_adjoint(tdp_handle* h, const double* g_host, double gE, double* out_hos
         launch_set_operand<R>(d, mu_fwd, st);
         launch_field<R>(d, 1, st);
         launch_add_field(d, E_fwd, e_tmu, st);
+    } else if (h->polarization == TDP_EXTRAPOLATED) {
+        // The extrapolation recursion backwards (see tdp_adjoint.cu): gbar in
+        // amu_tlam, alpha gbar in e_tmu; lambda, dL/dalpha and c_t accumulate.
+        const int K = (int)h->extrap.size();
+        double* gbar = amu_tlam;
+        double* agb = e_tmu;
+        TDP_CUDA(cudaMemsetAsync(lam, 0, n3 * 8, st));
+        TDP_CUDA(cudaMemsetAsync(galpha, 0, sizeof(double) * n, st));
+        TDP_CUDA(cudaMemsetAsync(ct, 0, sizeof(double) * n, st));
+        launch_lincomb(n, h->extrap[K - 1], amu, 0.0, nullptr, gbar, st);
+        for (int o = K - 1; o >= 0; o--) {
+            const double* mu_prev = d.hist + (size_t)(o - 1) * n3;
+            launch_alpha_scale(d, gbar, agb, st);
+            launch_lincomb(n, 1.0, lam, 1.0, agb, lam, st);
+            if (o == 0) {
+                launch_dot3_acc(n, gbar, E_fwd, galpha, st);
+                break;
+            }
+            launch_set_operand<R>(d, mu_prev, st);
+            launch_field<R>(d, 1, st);
+            launch_add_field(d, E_fwd, ext_v, st);
+            launch_dot3_acc(n, gbar, ext_v, galpha, st);
+            launch_adjoint_matvec_t_mu(d, agb, mu_prev, ct, true, st);
+            launch_set_operand<R>(d, agb, st);
+            launch_field<R>(d, 1, st);
+            launch_lincomb(n, h->extrap[o - 1], amu, 0.0, nullptr, ext_v, st);
+            launch_add_field(d, ext_v, gbar, st);
+        }
+        launch_adjoint_fixed(d, lam, b5, st);
+        h->adj_eps = 0.0;
+        h->adj_iterations = 0;
     } else {
         // Direct: mu = alpha E, so lambda = alpha a_mu and dL/dalpha = a_mu . E.
-        std::vector<double> ha(n3);
-        TDP_CUDA(cudaMemcpyAsync(ha.data(), amu, n3 * 8, cudaMemcpyDeviceToHost, st));
-        TDP_CUDA(cudaStreamSynchronize(st));
-        for (size_t k = 0; k < n3; k++) ha[k] *= h->alpha[k / 3];
-        TDP_CUDA(cudaMemcpyAsync(lam, ha.data(), n3 * 8, cudaMemcpyHostToDevice, st));
-        TDP_CUDA(cudaStreamSynchronize(st));
+        k_alpha_scale<<<(unsigned)((n3 + 255) / 256), 256, 0, st>>>(n, d.alpha, amu, lam);
         launch_adjoint_fixed(d, lam, b5, st);
         TDP_CUDA(cudaMemsetAsync(ct, 0, sizeof(double) * n, st));
         TDP_CUDA(cudaMemcpyAsync(amu_tlam, amu, n3 * 8, cudaMemcpyDeviceToDevice, st));
@@ -694,10 +804,26 @@ void run_adjoint(tdp_handle* h, const double* g_host, double gE, double* out_hos
     }
     launch_adjoint_split(d, a8, b5, amu, glab, st);
     launch_rotation_vjp(d, glab, gmol, st);
-    launch_adjoint_assemble(d, a8, b5, ct, amu_tlam, e_tmu, gmol, out, st);
-    TDP_CUDA(cudaMemcpyAsync(out_host, out, sizeof(double) * 6 * n, cudaMemcpyDeviceToHost, st));
-    TDP_CUDA(cudaStreamSynchronize(st));
+    launch_adjoint_assemble(d, a8, b5, ct, amu_tlam, e_tmu, gmol, out, st,
+                            h->polarization == TDP_EXTRAPOLATED ? galpha : nullptr);
+    TDP_CUDA(cudaMemcpyAsync(out_dst, out, sizeof(double) * 6 * n,
+                             on_device ? cudaMemcpyDeviceToDevice : cudaMemcpyDeviceToHost, st));
+    if (!on_device) TDP_CUDA(cudaStreamSynchronize(st));
     TDP_CUDA(cudaGetLastError());
+}
+
+int adjoint_entry(tdp_handle* h, const double* dL_dF, double dL_dE, double* grads, bool on_device) {
+    if (!h || !grads) return TDP_ERR_INVALID_ARGUMENT;
+    try {
+        if (h->n == 0) return TDP_OK;
+        if (!h->have_results) throw TdpError{TDP_ERR_INVALID_ARGUMENT, "tdp_adjoint needs a previous tdp_compute"};
+        if (h->ew) throw TdpError{TDP_ERR_UNSUPPORTED, "tdp_adjoint does not support the Ewald mode"};
+        if (h->precision == TDP_PRECISION_DOUBLE) run_adjoint<double>(h, dL_dF, dL_dE, grads, on_device);
+        else run_adjoint<float>(h, dL_dF, dL_dE, grads, on_device);
+    } catch (const TdpError& e) {
+        return fail(h, e);
+    }
+    return TDP_OK;
 }
 
 }  // namespace
@@ -705,19 +831,11 @@ void run_adjoint(tdp_handle* h, const double* g_host, double gE, double* out_hos
 extern "C" {
 
 int tdp_adjoint(tdp_handle* h, const double* dL_dF, double dL_dE, double* grads) {
-    if (!h || !grads) return TDP_ERR_INVALID_ARGUMENT;
-    try {
-        if (h->n == 0) return TDP_OK;
-        if (!h->have_results) throw TdpError{TDP_ERR_INVALID_ARGUMENT, "tdp_adjoint needs a previous tdp_compute"};
-        if (h->polarization == TDP_EXTRAPOLATED)
-            throw TdpError{TDP_ERR_UNSUPPORTED, "tdp_adjoint supports Direct and Mutual polarization"};
-        if (h->ew) throw TdpError{TDP_ERR_UNSUPPORTED, "tdp_adjoint does not support the Ewald mode"};
-        if (h->precision == TDP_PRECISION_DOUBLE) run_adjoint<double>(h, dL_dF, dL_dE, grads);
-        else run_adjoint<float>(h, dL_dF, dL_dE, grads);
-    } catch (const TdpError& e) {
-        return fail(h, e);
-    }
-    return TDP_OK;
+    return adjoint_entry(h, dL_dF, dL_dE, grads, false);
+}
+
+int tdp_adjoint_device(tdp_handle* h, const double* dL_dF, double dL_dE, double* grads) {
+    return adjoint_entry(h, dL_dF, dL_dE, grads, true);
 }
 
 int tdp_abi_version(void) { return TDP_ABI_VERSION; }
@@ -884,6 +1002,11 @@ int tdp_create(const tdp_system_desc* desc, tdp_handle** out) {
         d.pp.mutual = h->polarization == TDP_MUTUAL ? 1 : 0;
         d.pp.rinv4_power = (h->flags & TDP_FLAG_DD_FORCE_R4) ? 1.0f : 0.0f;
         d.pp.rinv4_fill = 0.0f;
+        // The lab-frame energy walk needs rInvVec[4] = 0; TDP_LAB_ENERGY=0
+        // keeps every tile pair on the general walk (for comparisons).
+        d.pp.lab_energy = (h->flags & TDP_FLAG_DD_FORCE_R4) ? 0 : 1;
+        if (const char* e = getenv("TDP_LAB_ENERGY"))
+            if (atoi(e) == 0) d.pp.lab_energy = 0;
 
         size_t rsz = h->precision == TDP_PRECISION_DOUBLE ? sizeof(double4) : sizeof(float4);
         auto& o = h->owned;
@@ -1043,6 +1166,62 @@ int tdp_update_params(tdp_handle* h, int32_t num_particles, const double* charge
     return TDP_OK;
 }
 
+int tdp_update_particle_params(tdp_handle* h, const double* charges, const double* molecular_dipoles,
+                               const double* polarizabilities, const double* thole_damping, int32_t on_device) {
+    if (!h) return TDP_ERR_INVALID_ARGUMENT;
+    try {
+        const int n = h->n;
+        if (n == 0) return TDP_OK;
+        if (!charges || !molecular_dipoles || !polarizabilities || !thole_damping)
+            throw TdpError{TDP_ERR_INVALID_ARGUMENT, "a per-particle array is NULL"};
+        if (!on_device) {
+            h->charge.assign(charges, charges + n);
+            h->dip.assign(molecular_dipoles, molecular_dipoles + 3 * (size_t)n);
+            h->alpha.assign(polarizabilities, polarizabilities + n);
+            h->thole.assign(thole_damping, thole_damping + n);
+            TDP_CUDA(cudaStreamSynchronize(h->stream));
+            upload_params(h);
+        } else {
+            // Device to device, then the derived quantities on the device; only
+            // three scalars come back (damping radius, net charge).
+            Dev& d = h->d;
+            cudaStream_t st = h->stream;
+            TDP_CUDA(cudaMemcpyAsync(d.charge, charges, sizeof(double) * n, cudaMemcpyDeviceToDevice, st));
+            TDP_CUDA(cudaMemcpyAsync(d.dip_mol, molecular_dipoles, sizeof(double) * 3 * n, cudaMemcpyDeviceToDevice,
+                                     st));
+            TDP_CUDA(cudaMemcpyAsync(d.alpha, polarizabilities, sizeof(double) * n, cudaMemcpyDeviceToDevice, st));
+            TDP_CUDA(cudaMemcpyAsync(d.thole, thole_damping, sizeof(double) * n, cudaMemcpyDeviceToDevice, st));
+            double* ps = pstat(h);
+            k_param_stats<<<1, 1024, 0, st>>>(n, h->precision == TDP_PRECISION_DOUBLE ? 0 : 1, d.alpha, d.thole,
+                                              d.charge, d.salpha, ps);
+            TDP_CUDA(cudaMemcpyAsync(h->h_scal + 8, ps, 3 * sizeof(double), cudaMemcpyDeviceToHost, st));
+            TDP_CUDA(cudaStreamSynchronize(st));
+            TDP_CUDA(cudaGetLastError());
+            const double tmax = h->h_scal[8];
+            double r2 = 0.0;
+            if (h->h_scal[9] != 0.0) r2 = INFINITY;
+            else if (tmax > 0.0) {
+                const double r = std::pow(tmax, 5.0 / 3.0) * std::cbrt(50.0) * 1.001;
+                r2 = r * r;
+            }
+            d.pp.damp_r2 = (float)r2;
+            h->total_charge = h->h_scal[10];
+            // The host copies no longer hold these parameters; a later
+            // tdp_update_params replaces them all.
+            h->charge.clear();
+            h->dip.clear();
+            h->alpha.clear();
+            h->thole.clear();
+        }
+        h->mu_prev_valid = false;
+        h->mu_prev2_valid = false;
+        h->have_results = false;
+    } catch (const TdpError& e) {
+        return fail(h, e);
+    }
+    return TDP_OK;
+}
+
 int tdp_compute(tdp_handle* h, const void* positions, int32_t pos_dtype, int32_t on_device, void* forces_accum,
                 int32_t force_dtype, double* energy, uint32_t flags) {
     if (!h) return TDP_ERR_INVALID_ARGUMENT;
@@ -1083,6 +1262,47 @@ int tdp_compute(tdp_handle* h, const void* positions, int32_t pos_dtype, int32_t
                 for (size_t k = 0; k < n3; k++) acc[k] += (float)h->h_forces[k];
             }
         }
+        check_flags(h);
+        if (energy) *energy = h->h_scal[1];
+        finish_timing(h);
+        if (h->status == TDP_STATUS_NON_FINITE)
+            throw TdpError{TDP_ERR_NON_FINITE, "the induced-dipole solve produced a non-finite residual"};
+        if ((flags & TDP_COMPUTE_REQUIRE_CONVERGENCE) && !h->converged)
+            throw TdpError{TDP_ERR_NOT_CONVERGED, "the induced dipoles did not converge"};
+    } catch (const TdpError& e) {
+        return fail(h, e);
+    }
+    return TDP_OK;
+}
+
+int tdp_compute_openmm(tdp_handle* h, const void* posq, int32_t posq_is_double, const int32_t* atom_index,
+                       int32_t padded_num_atoms, long long* force_fixed, double* energy, uint32_t flags) {
+    if (!h) return TDP_ERR_INVALID_ARGUMENT;
+    try {
+        if (h->n == 0) {
+            if (energy) *energy = 0.0;
+            h->iterations = 0;
+            h->converged = 1;
+            return TDP_OK;
+        }
+        if (!posq || !atom_index) throw TdpError{TDP_ERR_INVALID_ARGUMENT, "posq or atom_index is NULL"};
+        if (padded_num_atoms < h->n) throw TdpError{TDP_ERR_INVALID_ARGUMENT, "padded_num_atoms < num_particles"};
+        if ((flags & TDP_COMPUTE_FORCES) && !force_fixed)
+            throw TdpError{TDP_ERR_INVALID_ARGUMENT, "forces requested but force_fixed is NULL"};
+        cudaStream_t st = h->stream;
+        check_box(h);
+        launch_posq_in(h->d, posq, posq_is_double ? 1 : 0, atom_index, st);
+        solve_at(h, &kStaged, TDP_F64, 1);
+        if (h->precision == TDP_PRECISION_DOUBLE) run_energy<double>(h);
+        else run_energy<float>(h);
+        if (flags & TDP_COMPUTE_FORCES) {
+            launch_forces_out_fixed(h->d, atom_index, padded_num_atoms, force_fixed, st);
+            h->launches++;
+        }
+        if (energy) TDP_CUDA(cudaMemcpyAsync(h->h_scal + 1, h->d.energy, sizeof(double), cudaMemcpyDeviceToHost, st));
+        enqueue_flags(h);
+        TDP_CUDA(cudaStreamSynchronize(st));
+        TDP_CUDA(cudaGetLastError());
         check_flags(h);
         if (energy) *energy = h->h_scal[1];
         finish_timing(h);

@@ -28,6 +28,7 @@ struct PairParams {
     int mutual;            // polarization type is Mutual (adds the Uind-Uind terms)
     int band_tiles;        // 32-atom tiles per band of the pair kernels (1..16)
     int n_bands;           // bands covering the n_tiles real tiles
+    int lab_energy;        // 1: undamped unit-scale tile pairs take the lab-frame energy walk
 };
 
 __device__ __forceinline__ float rsqrt_r(float x) { return rsqrtf(x); }

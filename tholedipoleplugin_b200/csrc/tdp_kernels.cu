@@ -482,6 +482,44 @@ __global__ void k_positions_in(int n3, const void* __restrict__ src, int is_f32,
     dst[k] = is_f32 ? (double)((const float*)src)[k] : ((const double*)src)[k];
 }
 
+// OpenMM CUDA-platform coordinates: slot k of posq (float4 or double4, x y z q)
+// holds atom atom_index[k].
+__global__ void k_posq_in(int n, const void* __restrict__ posq, int is_double, const int* __restrict__ atom_index,
+                          double* __restrict__ dst) {
+    int k = blockIdx.x * blockDim.x + threadIdx.x;
+    if (k >= n) return;
+    const int a = atom_index[k];
+    if (a < 0 || a >= n) return;
+    double x, y, z;
+    if (is_double) {
+        const double4 p = ((const double4*)posq)[k];
+        x = p.x;
+        y = p.y;
+        z = p.z;
+    } else {
+        const float4 p = ((const float4*)posq)[k];
+        x = p.x;
+        y = p.y;
+        z = p.z;
+    }
+    dst[3 * a] = x;
+    dst[3 * a + 1] = y;
+    dst[3 * a + 2] = z;
+}
+
+// Forces added to OpenMM's 64-bit fixed-point accumulator (2^32 units per
+// force unit, component c of slot k at k + c * padded, truncated toward zero
+// as the platform converts).
+__global__ void k_forces_out_fixed(int n, const double* __restrict__ f, const int* __restrict__ atom_index,
+                                   int padded, unsigned long long* __restrict__ acc) {
+    int k = blockIdx.x * blockDim.x + threadIdx.x;
+    if (k >= n) return;
+    const int a = atom_index[k];
+    if (a < 0 || a >= n) return;
+    for (int c = 0; c < 3; c++)
+        acc[k + (size_t)c * padded] += (unsigned long long)__double2ll_rz(f[3 * a + c] * 4294967296.0);
+}
+
 // Electrostatic potential at grid points, calculateElectrostaticPotential-
 // ForParticleGridPoint (RTDF.cpp:1348-1372), FP64.
 __global__ void k_potential(int n, int ng, PairParams P, const double* __restrict__ pos,
@@ -696,6 +734,13 @@ void launch_add_forces(const Dev& d, void* acc, int is_f32, cudaStream_t st) {
 void launch_positions_in(const Dev& d, const void* src, int is_f32, cudaStream_t st) {
     int n3 = 3 * d.n;
     k_positions_in<<<nblk(n3, kVecThreads), kVecThreads, 0, st>>>(n3, src, is_f32, d.pos);
+}
+void launch_posq_in(const Dev& d, const void* posq, int is_double, const int* atom_index, cudaStream_t st) {
+    k_posq_in<<<nblk(d.n, kVecThreads), kVecThreads, 0, st>>>(d.n, posq, is_double, atom_index, d.pos);
+}
+void launch_forces_out_fixed(const Dev& d, const int* atom_index, int padded, long long* acc, cudaStream_t st) {
+    k_forces_out_fixed<<<nblk(d.n, kVecThreads), kVecThreads, 0, st>>>(d.n, d.ftotal, atom_index, padded,
+                                                                        (unsigned long long*)acc);
 }
 void launch_potential(const Dev& d, const double* grid, int ng, double* out, cudaStream_t st) {
     k_potential<<<nblk(ng, 128), 128, 0, st>>>(d.n, ng, d.pp, d.pos, d.charge, d.lab, d.mu, grid, out);

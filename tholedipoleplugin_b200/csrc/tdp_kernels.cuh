@@ -107,6 +107,8 @@ void launch_energy_done(const Dev& d, cudaStream_t st);
 void launch_torque_gather(const Dev& d, cudaStream_t st);
 void launch_add_forces(const Dev& d, void* acc, int is_f32, cudaStream_t st);
 void launch_positions_in(const Dev& d, const void* src, int is_f32, cudaStream_t st);
+void launch_posq_in(const Dev& d, const void* posq, int is_double, const int* atom_index, cudaStream_t st);
+void launch_forces_out_fixed(const Dev& d, const int* atom_index, int padded, long long* acc, cudaStream_t st);
 void launch_potential(const Dev& d, const double* grid, int ng, double* out, cudaStream_t st);
 void launch_moments(const Dev& d, const double* mass, double* scratch, double* out13, cudaStream_t st);
 
@@ -115,14 +117,23 @@ void launch_torque_vjp(const Dev& d, const double* g, double* gt, cudaStream_t s
 void launch_adjoint_pair(const Dev& d, const double* g, const double* gT, double gE, double* a8, cudaStream_t st);
 void launch_adjoint_fixed(const Dev& d, const double* lam, double* b5, cudaStream_t st);
 void launch_adjoint_matvec_t(const Dev& d, const double* lam, double* ct, cudaStream_t st);
+// ct (+)= d/dt of lam^T T(t) mu for an explicit mu (n*3); accumulate adds to ct.
+void launch_adjoint_matvec_t_mu(const Dev& d, const double* lam, const double* mu, double* ct, bool accumulate,
+                                cudaStream_t st);
+// out = ca a + cb b (n*3; b may be NULL); acc_i += a_i . b_i (per atom).
+void launch_lincomb(int n, double ca, const double* a, double cb, const double* b, double* out, cudaStream_t st);
+void launch_dot3_acc(int n, const double* a, const double* b, double* acc, cudaStream_t st);
+// out = alpha (.) v (n*3).
+void launch_alpha_scale(const Dev& d, const double* v, double* out, cudaStream_t st);
 void launch_rotation_vjp(const Dev& d, const double* glab, double* gmol, cudaStream_t st);
 void launch_adjoint_split(const Dev& d, const double* a8, const double* b5, double* amu, double* glab,
                           cudaStream_t st);
 void launch_add_field(const Dev& d, const double* base, double* out, cudaStream_t st);
 template <class R> void launch_rhs_init(const Dev& d, const double* rhs, cudaStream_t st);
 template <class R> void launch_set_operand(const Dev& d, const double* x, cudaStream_t st);
+// galpha (n, may be NULL) replaces amu_tlam . e_tmu as the polarizability gradient.
 void launch_adjoint_assemble(const Dev& d, const double* a8, const double* b5, const double* ct,
                              const double* amu_tlam, const double* e_tmu, const double* gmol, double* out,
-                             cudaStream_t st);
+                             cudaStream_t st, const double* galpha = nullptr);
 
 }  // namespace tdp

@@ -15,6 +15,11 @@
 // so calls that overlap on the GPU (on different streams, or from several
 // threads) race on it and must be serialised by the caller.  Each call writes
 // every scratch slot it later reads, so nothing needs clearing between calls.
+//
+// The array's device address is looked up once per device and kept for the
+// life of the process.  A cudaDeviceReset unloads the module and invalidates
+// that address, so the entry point must not be used on a device after the
+// host program has reset it.
 #include "tholedipole_b200.h"
 #include "tdp_common.cuh"
 
@@ -114,6 +119,9 @@ extern "C" int tdp_potential_noalloc(int32_t num_particles, const double* positi
                                      const double* total_dipoles, int32_t num_points, const double* grid,
                                      int32_t periodic, const double* box3, double* out, void* stream) {
     g_noalloc_error[0] = '\0';
+    // A non-sticky error left by the caller's earlier CUDA work would
+    // otherwise be reported below as this call's own launch failure.
+    (void)cudaGetLastError();
     if (num_particles < 0 || num_points < 0)
         return noalloc_fail(TDP_ERR_INVALID_ARGUMENT, "tdp_potential_noalloc: negative size");
     if (num_points == 0) return TDP_OK;
@@ -138,6 +146,7 @@ extern "C" int tdp_potential_noalloc(int32_t num_particles, const double* positi
             void* p = nullptr;
             cudaError_t e = cudaGetSymbolAddress(&p, g_potential_scratch);
             if (e != cudaSuccess || !p) {
+                (void)cudaGetLastError();  // leave no error of this lookup behind
                 char buf[200];
                 snprintf(buf, sizeof buf, "tdp_potential_noalloc: cudaGetSymbolAddress failed: %s",
                          cudaGetErrorString(e));

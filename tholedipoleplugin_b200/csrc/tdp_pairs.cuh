@@ -266,6 +266,113 @@ __device__ __forceinline__ void pair_energy_sides(R dx, R dy, R dz, R r2, bool y
     }
 }
 
+// pair_energy_sides<R, 3> for a pair that Thole damping does not reach (all
+// six damping factors 1), with unit scales and rInvVec[4] = 0, computed in the
+// lab frame.  With those factors the reference's QI-frame algebra
+// (RTDF.cpp:212-340) reduces to expressions in the frame's X row alone, the
+// axis its multipole algebra treats as the bond axis.  With P = m + u and
+// W = m + 2u (W = m unless Mutual), and _0 the component along X:
+//   E    = q_i q_j / r + (q_j (P_i0 + m_i0) - q_i (P_j0 + m_j0)) / (2 r^2)
+//          + (m_i.P_j + m_j.P_i - 3 (m_i0 P_j0 + m_j0 P_i0)) / (2 r^3)
+//   V_ij = (q_j/r^2 - 3 P_j0/r^3) X + P_j/r^3,  V_ji = (-q_i/r^2 - 3 P_i0/r^3) X + P_i/r^3
+//   Vd_ij, Vd_ji: the same with W in place of P
+//   S    = m_i x V_ij + m_j x V_ji + u_i x Vd_ij + u_j x Vd_ji
+//   f    = (S x X) / r + (q_i q_j / r^2 - 2 (q_i P_j0 - q_j P_i0) / r^3) X
+//   F_I -= perm(f), F_K += perm(f), tau_I = -perm(m_i x V_ij), tau_K = -perm(m_j x V_ji),
+// perm(v) = (v_y, v_z, v_x) being the permuted back rotation of :150-159.  X is
+// the frame test's (:580-593): (x^ - Z_x Z)/|.| = (d_y^2 + d_z^2, -d_x d_y,
+// -d_x d_z) / (r sqrt(d_y^2 + d_z^2)) when the y or z coordinates differ,
+// the Gram-Schmidt form otherwise.  kap = 1 (Mutual) or -1: W = P + kap u.
+template <class R>
+__device__ __forceinline__ void pair_energy_lab(R dx, R dy, R dz, R r2, bool yz_differ, const EAtom<R>& I,
+                                                const EAtom<R>& K, R kap, R& fx, R& fy, R& fz, R& tx, R& ty, R& tz,
+                                                R& gx, R& gy, R& gz, R& ux, R& uy, R& uz, R& en) {
+    const R rinv = rsqrt_r(r2);
+    const R rho2 = dy * dy + dz * dz;
+    R xx, xy, xz;
+    if (yz_differ && rho2 > R(0)) {
+        const R s = rinv * rsqrt_r(rho2);
+        xx = rho2 * s;
+        xy = -dx * dy * s;
+        xz = -dx * dz * s;
+    } else {
+        const R zx = dx * rinv, zy = dy * rinv, zz = dz * rinv;
+        xx = zx + (yz_differ ? R(1) : R(0));
+        xy = zy + (yz_differ ? R(0) : R(1));
+        xz = zz;
+        const R dt = zx * xx + zy * xy + zz * xz;
+        xx -= zx * dt;
+        xy -= zy * dt;
+        xz -= zz * dt;
+        const R n2 = xx * xx + xy * xy + xz * xz;
+        const R s = n2 > R(0) ? rsqrt_r(n2) : R(1);
+        xx *= s;
+        xy *= s;
+        xz *= s;
+    }
+    const R pix = I.mx + I.ux, piy = I.my + I.uy, piz = I.mz + I.uz;
+    const R pjx = K.mx + K.ux, pjy = K.my + K.uy, pjz = K.mz + K.uz;
+    const R qi1 = xx * I.mx + xy * I.my + xz * I.mz, ui0 = xx * I.ux + xy * I.uy + xz * I.uz;
+    const R qj1 = xx * K.mx + xy * K.my + xz * K.mz, uj0 = xx * K.ux + xy * K.uy + xz * K.uz;
+    const R pi0 = qi1 + ui0, pj0 = qj1 + uj0;
+    const R rv2 = rinv * rinv, rv3 = rv2 * rinv;
+    const R qq = I.q * K.q;
+    {
+        const R t1 = K.q * (pi0 + qi1) - I.q * (pj0 + qj1);
+        const R t2 = I.mx * pjx + I.my * pjy + I.mz * pjz + K.mx * pix + K.my * piy + K.mz * piz -
+                     R(3) * (qi1 * pj0 + qj1 * pi0);
+        en += rinv * qq + R(0.5) * (rv2 * t1 + rv3 * t2);
+    }
+    R sx, sy, sz;
+    {
+        const R a = rv2 * K.q - R(3) * rv3 * pj0;
+        const R vx = a * xx + rv3 * pjx, vy = a * xy + rv3 * pjy, vz = a * xz + rv3 * pjz;
+        sx = I.my * vz - I.mz * vy;
+        sy = I.mz * vx - I.mx * vz;
+        sz = I.mx * vy - I.my * vx;
+        tx -= sy;
+        ty -= sz;
+        tz -= sx;
+    }
+    {
+        const R b = -rv2 * I.q - R(3) * rv3 * pi0;
+        const R vx = b * xx + rv3 * pix, vy = b * xy + rv3 * piy, vz = b * xz + rv3 * piz;
+        const R cx = K.my * vz - K.mz * vy, cy = K.mz * vx - K.mx * vz, cz = K.mx * vy - K.my * vx;
+        ux -= cy;
+        uy -= cz;
+        uz -= cx;
+        sx += cx;
+        sy += cy;
+        sz += cz;
+    }
+    {
+        const R wx = pjx + kap * K.ux, wy = pjy + kap * K.uy, wz = pjz + kap * K.uz;
+        const R c = rv2 * K.q - R(3) * rv3 * (pj0 + kap * uj0);
+        const R vx = c * xx + rv3 * wx, vy = c * xy + rv3 * wy, vz = c * xz + rv3 * wz;
+        sx += I.uy * vz - I.uz * vy;
+        sy += I.uz * vx - I.ux * vz;
+        sz += I.ux * vy - I.uy * vx;
+    }
+    {
+        const R wx = pix + kap * I.ux, wy = piy + kap * I.uy, wz = piz + kap * I.uz;
+        const R c = -rv2 * I.q - R(3) * rv3 * (pi0 + kap * ui0);
+        const R vx = c * xx + rv3 * wx, vy = c * xy + rv3 * wy, vz = c * xz + rv3 * wz;
+        sx += K.uy * vz - K.uz * vy;
+        sy += K.uz * vx - K.ux * vz;
+        sz += K.ux * vy - K.uy * vx;
+    }
+    const R qf2 = rv2 * qq - R(2) * rv3 * (I.q * pj0 - K.q * pi0);
+    const R fvx = rinv * (sy * xz - sz * xy) + qf2 * xx;
+    const R fvy = rinv * (sz * xx - sx * xz) + qf2 * xy;
+    const R fvz = rinv * (sx * xy - sy * xx) + qf2 * xz;
+    fx -= fvy;
+    fy -= fvz;
+    fz -= fvx;
+    gx += fvy;
+    gy += fvz;
+    gz += fvx;
+}
+
 // One side of the pair: SIDE_I adds the force and torque on I and the pair
 // energy; otherwise the force and torque on K.
 template <class R, bool SIDE_I>

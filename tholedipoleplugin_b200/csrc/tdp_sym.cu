@@ -865,7 +865,8 @@ __device__ __forceinline__ bool yz_differ(R dy, R dz, const double2* __restrict_
     return d;
 }
 
-template <class R, bool FOLD, bool SLOW>
+// LAB (non-SLOW tile pairs beyond the damping range only): pair_energy_lab.
+template <class R, bool FOLD, bool SLOW, bool LAB = false>
 __device__ __forceinline__ void energy_walk(const PairParams& P, const double* __restrict__ pos,
                                             const double2* __restrict__ yz,
                                             const typename Vec4T<R>::type* __restrict__ sp,
@@ -885,7 +886,10 @@ __device__ __forceinline__ void energy_walk(const PairParams& P, const double* _
         R r2 = dx * dx + dy * dy + dz * dz;
         if (SLOW && skip_pair(s, lane, i, j, P.n, partners, jj, diag)) r2 = (R)INFINITY;
         const bool yzd = yz_differ<R>(dy, dz, yz, i, j, nmax);
-        if (!SLOW || !diag) {
+        if (LAB) {
+            pair_energy_lab<R>(dx, dy, dz, r2, yzd, me, other, P.mutual ? R(1) : R(-1), f[0], f[1], f[2], f[3], f[4],
+                               f[5], g[0], g[1], g[2], g[3], g[4], g[5], en);
+        } else if (!SLOW || !diag) {
             pair_energy_sides<R, 3>(dx, dy, dz, r2, yzd, me, other, R(1), R(1), damp_r2, rv4p, rv4f, P.mutual != 0,
                                     f[0], f[1], f[2], f[3], f[4], f[5], g[0], g[1], g[2], g[3], g[4], g[5], en);
         } else {
@@ -1206,6 +1210,260 @@ __device__ __forceinline__ void energy_walk_x2(const PairParams& P, const double
     }
 }
 
+// ---------------------------------------------------------------------------
+// Packed FP32 energy walk for tile pairs that no Thole damping reaches (every
+// damping factor 1), with unit scales and rInvVec[4] = 0 (the default, see
+// TDP_FLAG_DD_FORCE_R4).  It computes the reference's pair routine
+// (RTDF.cpp:129-366) in the lab frame.  With all damping factors 1 the
+// permanent and induced coefficients of calculateElectrostaticPairIxn merge
+// and every rInvVec[4] term vanishes; what is left of the quasi-internal
+// frame is its X row, the axis its multipole algebra treats as the bond axis
+// (component 0).  With P = m + u and W = m + 2u (W = m without the
+// induced-induced terms, i.e. unless Mutual), X-components written _0:
+//   E   = q_i q_j / r + (q_j (P_i0 + m_i0) - q_i (P_j0 + m_j0)) / (2 r^2)
+//         + (m_i.P_j + m_j.P_i - 3 (m_i0 P_j0 + m_j0 P_i0)) / (2 r^3)
+//   V_ij = (q_j/r^2 - 3 P_j0/r^3) X + P_j/r^3,  V_ji = (-q_i/r^2 - 3 P_i0/r^3) X + P_i/r^3
+//   Vd_ij, Vd_ji: the same with W for P
+//   S   = m_i x V_ij + m_j x V_ji + u_i x Vd_ij + u_j x Vd_ji
+//   f   = (S x X) / r + (q_i q_j / r^2 - 2 (q_i P_j0 - q_j P_i0) / r^3) X
+//   F_i -= perm(f), F_j += perm(f), tau_i = -perm(m_i x V_ij), tau_j = -perm(m_j x V_ji)
+// where perm(v) = (v_y, v_z, v_x) is the reference's permuted back rotation
+// (:150-159).  This is an exact rewrite (FP64 transcriptions of both agree to
+// rounding), with X from the frame test as there: X = (x^ - Z_x Z)/|.| when
+// the pair's y or z coordinates differ (:584), written here as
+// (d_y^2 + d_z^2, -d_x d_y, -d_x d_z) / (r sqrt(d_y^2 + d_z^2)); pairs within
+// 1e-5 nm of the x axis take the reference's test and Gram-Schmidt as is.
+// ---------------------------------------------------------------------------
+__device__ __forceinline__ f2 xneg2(f2 a) { return a ^ 0x8000000080000000ull; }
+
+__device__ __forceinline__ void cross2(f2 ax, f2 ay, f2 az, f2 bx, f2 by, f2 bz, f2& cx, f2& cy, f2& cz) {
+    cx = fma2(ay, bz, xneg2(mul2(az, by)));
+    cy = fma2(az, bx, xneg2(mul2(ax, bz)));
+    cz = fma2(ax, by, xneg2(mul2(ay, bx)));
+}
+
+// X row of formQIRotationMatrix (RTDF.cpp:580-593) for one pair, as the
+// general walk forms it.
+__device__ __forceinline__ void qi_frame_x(float dx, float dy, float dz, float rinv, bool yzd, float& xx, float& xy,
+                                           float& xz) {
+    const float zx = dx * rinv, zy = dy * rinv, zz = dz * rinv;
+    xx = zx + (yzd ? 1.0f : 0.0f);
+    xy = zy + (yzd ? 0.0f : 1.0f);
+    xz = zz;
+    const float dt = zx * xx + zy * xy + zz * xz;
+    xx -= zx * dt;
+    xy -= zy * dt;
+    xz -= zz * dt;
+    const float n2 = xx * xx + xy * xy + xz * xz;
+    const float s = n2 > 0.0f ? rsqrtf(n2) : 1.0f;
+    xx *= s;
+    xy *= s;
+    xz *= s;
+}
+
+template <bool FOLD>
+__device__ __forceinline__ void energy_walk_x2_fast(const PairParams& P, const double* __restrict__ pos,
+                                                    const double2* __restrict__ yz, const EPackedTile& T, int lane,
+                                                    int i, int jbase, float oix, float oiy, float oiz, float4 pi,
+                                                    float4 di, float4 ui, unsigned fm, bool mutual, float f[6],
+                                                    float gg[6], float& en) {
+    const int nxt = (lane + 1) & 31;
+    const int nmax = P.n_tiles * 32 - 1;
+    const f2 OX = bc2(oix), OY = bc2(oiy), OZ = bc2(oiz);
+    const float kap = mutual ? 1.0f : -1.0f;   // W = P + kap u
+    const f2 KAP = bc2(kap);
+    const f2 QI0 = bc2(pi.w), NQI0 = bc2(-pi.w);
+    const f2 MIX = bc2(di.x), MIY = bc2(di.y), MIZ = bc2(di.z);
+    const f2 UIX = bc2(ui.x), UIY = bc2(ui.y), UIZ = bc2(ui.z);
+    const float pix = di.x + ui.x, piy = di.y + ui.y, piz = di.z + ui.z;
+    const f2 PIX = bc2(pix), PIY = bc2(piy), PIZ = bc2(piz);
+    const f2 WIX = bc2(pix + kap * ui.x), WIY = bc2(piy + kap * ui.y), WIZ = bc2(piz + kap * ui.z);
+    const f2 HALF = bc2(0.5f), NTHREE = bc2(-3.0f), NTWO = bc2(-2.0f);
+    f2 Lx = 0, Ly = 0, Lz = 0, Ix = 0, Iy = 0, Iz = 0, NTx = 0, NTy = 0, NTz = 0;
+    if (FOLD) {
+        Lx = bc2(-(float)P.box[0]);
+        Ly = bc2(-(float)P.box[1]);
+        Lz = bc2(-(float)P.box[2]);
+        Ix = bc2((float)P.inv_box[0]);
+        Iy = bc2((float)P.inv_box[1]);
+        Iz = bc2((float)P.inv_box[2]);
+        NTx = bc2(-(float)(P.half_box_tol[0] * P.half_box_tol[0]));
+        NTy = bc2(-(float)(P.half_box_tol[1] * P.half_box_tol[1]));
+        NTz = bc2(-(float)(P.half_box_tol[2] * P.half_box_tol[2]));
+    }
+    f2 FX = 0, FY = 0, FZ = 0, TX = 0, TY = 0, TZ = 0, EN = 0;        // I side
+    f2 GX = 0, GY = 0, GZ = 0, UX = 0, UY = 0, UZ = 0;                // J side (packed atoms m, m + 16)
+#pragma unroll 1
+    for (int s = 0; s < 16; s++) {
+        const int m = (lane + s) & 15;
+        const float4 a = T.p0[m], b = T.p1[m], c = T.d0[m], d = T.d1[m], e = T.u0[m], h = T.u1[m];
+        f2 DX = sub2(pk2(a.x, a.y), OX), DY = sub2(pk2(a.z, a.w), OY), DZ = sub2(pk2(b.x, b.y), OZ);
+        const int ja = jbase + m, jb = ja + 16;
+        if (FOLD) {
+            f2 neg = ~0ull;
+            if (fm & 1u) {
+                DX = fold2(DX, Lx, Ix);
+                neg &= fma2(DX, DX, NTx);
+            }
+            if (fm & 2u) {
+                DY = fold2(DY, Ly, Iy);
+                neg &= fma2(DY, DY, NTy);
+            }
+            if (fm & 4u) {
+                DZ = fold2(DZ, Lz, Iz);
+                neg &= fma2(DZ, DZ, NTz);
+            }
+            const f2 flag = ~neg & 0x8000000080000000ull;
+            if (flag) {
+                const bool amb_a = (flag >> 31) & 1ull, amb_b = (flag >> 63) != 0ull;
+                float ax, bx, ay, by, az, bz;
+                un2(DX, ax, bx);
+                un2(DY, ay, by);
+                un2(DZ, az, bz);
+                if (amb_a) {
+                    d3 q = exact_delta(P, pos, i, ja);
+                    ax = (float)q.x;
+                    ay = (float)q.y;
+                    az = (float)q.z;
+                }
+                if (amb_b) {
+                    d3 q = exact_delta(P, pos, i, jb);
+                    bx = (float)q.x;
+                    by = (float)q.y;
+                    bz = (float)q.z;
+                }
+                DX = pk2(ax, bx);
+                DY = pk2(ay, by);
+                DZ = pk2(az, bz);
+            }
+        }
+        float r2a, r2b, ra, rb;
+        un2(dot2(DX, DY, DZ, DX, DY, DZ), r2a, r2b);
+        const f2 RINV = pk2(rsqrtf(r2a), rsqrtf(r2b));
+        const f2 RHO2 = fma2(DY, DY, mul2(DZ, DZ));
+        un2(RHO2, ra, rb);
+        // Frame X row (see above).
+        const f2 XS = mul2(RINV, pk2(rsqrtf(ra), rsqrtf(rb)));
+        const f2 NDXS = mul2(xneg2(DX), XS);
+        f2 XX = mul2(RHO2, XS), XY = mul2(NDXS, DY), XZ = mul2(NDXS, DZ);
+        if (ra <= 1.0e-10f || rb <= 1.0e-10f) {
+            float dxa, dxb, dya, dyb, dza, dzb, rva, rvb, xxa, xxb, xya, xyb, xza, xzb;
+            un2(DX, dxa, dxb);
+            un2(DY, dya, dyb);
+            un2(DZ, dza, dzb);
+            un2(RINV, rva, rvb);
+            un2(XX, xxa, xxb);
+            un2(XY, xya, xyb);
+            un2(XZ, xza, xzb);
+            if (ra <= 1.0e-10f) qi_frame_x(dxa, dya, dza, rva, yz_differ<float>(dya, dza, yz, i, ja, nmax), xxa, xya, xza);
+            if (rb <= 1.0e-10f) qi_frame_x(dxb, dyb, dzb, rvb, yz_differ<float>(dyb, dzb, yz, i, jb, nmax), xxb, xyb, xzb);
+            XX = pk2(xxa, xxb);
+            XY = pk2(xya, xyb);
+            XZ = pk2(xza, xzb);
+        }
+        const f2 QJ0 = pk2(b.z, b.w);
+        const f2 MJX = pk2(c.x, c.y), MJY = pk2(c.z, c.w), MJZ = pk2(d.x, d.y);
+        const f2 UJX = pk2(e.x, e.y), UJY = pk2(e.z, e.w), UJZ = pk2(h.x, h.y);
+        const f2 PJX = add2(MJX, UJX), PJY = add2(MJY, UJY), PJZ = add2(MJZ, UJZ);
+        const f2 QI1 = dot2(XX, XY, XZ, MIX, MIY, MIZ), UI0 = dot2(XX, XY, XZ, UIX, UIY, UIZ);
+        const f2 QJ1 = dot2(XX, XY, XZ, MJX, MJY, MJZ), UJ0 = dot2(XX, XY, XZ, UJX, UJY, UJZ);
+        const f2 PI0 = add2(QI1, UI0), PJ0 = add2(QJ1, UJ0);
+        const f2 rv2 = mul2(RINV, RINV), rv3 = mul2(rv2, RINV);
+        const f2 NR3X3 = mul2(NTHREE, rv3);
+        // Energy.
+        {
+            const f2 qq = mul2(QI0, QJ0);
+            const f2 t1 = fma2(QJ0, add2(PI0, QI1), mul2(NQI0, add2(PJ0, QJ1)));
+            const f2 t2 = fma2(NTHREE, fma2(QI1, PJ0, mul2(QJ1, PI0)),
+                               add2(dot2(MIX, MIY, MIZ, PJX, PJY, PJZ), dot2(MJX, MJY, MJZ, PIX, PIY, PIZ)));
+            EN = fma2(RINV, qq, fma2(HALF, fma2(rv2, t1, mul2(rv3, t2)), EN));
+        }
+        const f2 rv2QJ0 = mul2(rv2, QJ0), rv2NQI0 = mul2(rv2, NQI0);
+        f2 SX, SY, SZ;
+        {
+            // m_i x V_ij: the I torque and the first part of S.
+            const f2 aJ = fma2(NR3X3, PJ0, rv2QJ0);
+            const f2 VX = fma2(aJ, XX, mul2(rv3, PJX)), VY = fma2(aJ, XY, mul2(rv3, PJY)),
+                     VZ = fma2(aJ, XZ, mul2(rv3, PJZ));
+            cross2(MIX, MIY, MIZ, VX, VY, VZ, SX, SY, SZ);
+            TX = sub2(TX, SY);
+            TY = sub2(TY, SZ);
+            TZ = sub2(TZ, SX);
+        }
+        {
+            // m_j x V_ji: the J torque.
+            const f2 bI = fma2(NR3X3, PI0, rv2NQI0);
+            const f2 VX = fma2(bI, XX, mul2(rv3, PIX)), VY = fma2(bI, XY, mul2(rv3, PIY)),
+                     VZ = fma2(bI, XZ, mul2(rv3, PIZ));
+            f2 BX, BY, BZ;
+            cross2(MJX, MJY, MJZ, VX, VY, VZ, BX, BY, BZ);
+            UX = sub2(UX, BY);
+            UY = sub2(UY, BZ);
+            UZ = sub2(UZ, BX);
+            SX = add2(SX, BX);
+            SY = add2(SY, BY);
+            SZ = add2(SZ, BZ);
+        }
+        {
+            // u_i x Vd_ij.
+            const f2 WJX = fma2(KAP, UJX, PJX), WJY = fma2(KAP, UJY, PJY), WJZ = fma2(KAP, UJZ, PJZ);
+            const f2 cJ = fma2(NR3X3, fma2(KAP, UJ0, PJ0), rv2QJ0);
+            const f2 VX = fma2(cJ, XX, mul2(rv3, WJX)), VY = fma2(cJ, XY, mul2(rv3, WJY)),
+                     VZ = fma2(cJ, XZ, mul2(rv3, WJZ));
+            f2 CX, CY, CZ;
+            cross2(UIX, UIY, UIZ, VX, VY, VZ, CX, CY, CZ);
+            SX = add2(SX, CX);
+            SY = add2(SY, CY);
+            SZ = add2(SZ, CZ);
+        }
+        {
+            // u_j x Vd_ji.
+            const f2 dI = fma2(NR3X3, fma2(KAP, UI0, PI0), rv2NQI0);
+            const f2 VX = fma2(dI, XX, mul2(rv3, WIX)), VY = fma2(dI, XY, mul2(rv3, WIY)),
+                     VZ = fma2(dI, XZ, mul2(rv3, WIZ));
+            f2 CX, CY, CZ;
+            cross2(UJX, UJY, UJZ, VX, VY, VZ, CX, CY, CZ);
+            SX = add2(SX, CX);
+            SY = add2(SY, CY);
+            SZ = add2(SZ, CZ);
+        }
+        {
+            f2 CX, CY, CZ;
+            cross2(SX, SY, SZ, XX, XY, XZ, CX, CY, CZ);
+            const f2 qf2 = fma2(mul2(NTWO, rv3), fma2(QI0, PJ0, xneg2(mul2(QJ0, PI0))), mul2(rv2QJ0, QI0));
+            const f2 FVX = fma2(RINV, CX, mul2(qf2, XX)), FVY = fma2(RINV, CY, mul2(qf2, XY)),
+                     FVZ = fma2(RINV, CZ, mul2(qf2, XZ));
+            FX = sub2(FX, FVY);
+            FY = sub2(FY, FVZ);
+            FZ = sub2(FZ, FVX);
+            GX = add2(GX, FVY);
+            GY = add2(GY, FVZ);
+            GZ = add2(GZ, FVX);
+        }
+        GX = __shfl_sync(kFull, GX, nxt);
+        GY = __shfl_sync(kFull, GY, nxt);
+        GZ = __shfl_sync(kFull, GZ, nxt);
+        UX = __shfl_sync(kFull, UX, nxt);
+        UY = __shfl_sync(kFull, UY, nxt);
+        UZ = __shfl_sync(kFull, UZ, nxt);
+    }
+    float lo, hi;
+    const f2* Is[7] = {&FX, &FY, &FZ, &TX, &TY, &TZ, &EN};
+    float* Io[7] = {&f[0], &f[1], &f[2], &f[3], &f[4], &f[5], &en};
+#pragma unroll
+    for (int k = 0; k < 7; k++) {
+        un2(*Is[k], lo, hi);
+        *Io[k] += lo + hi;
+    }
+    const f2 Js[6] = {GX, GY, GZ, UX, UY, UZ};
+#pragma unroll
+    for (int k = 0; k < 6; k++) {
+        un2(Js[k], lo, hi);
+        const float olo = __shfl_xor_sync(kFull, lo, 16), ohi = __shfl_xor_sync(kFull, hi, 16);
+        gg[k] += lane < 16 ? lo + olo : hi + ohi;
+    }
+}
+
 // Partner pairs of a SLOW tile pair with their (M, I) scales, each side once:
 // the lane's I atom with its partners in J (the pair energy is counted on the
 // lower-index side), and atom l of J (off the diagonal) with its partners in I.
@@ -1339,7 +1597,7 @@ __global__ void __launch_bounds__(kSymThreads, 3) k_energy_sym(
                 gdx = (float)g0.dcx;
                 gdy = (float)g0.dcy;
                 gdz = (float)g0.dcz;
-                gfl = g0.fmask | (g0.fold ? 8u : 0u);
+                gfl = g0.fmask | (g0.fold ? 8u : 0u) | (g0.near ? 16u : 0u);
             }
         }
         for (int c = 0; c < 6; c++) my[c] = 0.0;
@@ -1364,6 +1622,7 @@ __global__ void __launch_bounds__(kSymThreads, 3) k_energy_sym(
                     } else {
                         g.fmask = fl & 7u;
                         g.fold = (fl >> 3) & 1u;
+                        g.near = (fl >> 4) & 1u;
                     }
                 } else {
                     g = tile_geom(P, cA, eA, cB, s_ext[Jl]);
@@ -1382,7 +1641,14 @@ __global__ void __launch_bounds__(kSymThreads, 3) k_energy_sym(
                         __syncwarp();
                         stage_epacked(s_ept[warp], lane, sp[lane], sd[lane], su[lane]);
                         __syncwarp();
-                        if (g.fold)
+                        if (!g.near && P.lab_energy) {
+                            if (g.fold)
+                                energy_walk_x2_fast<true>(P, pos, yz, s_ept[warp], lane, i, jbase, oix, oiy, oiz, pi,
+                                                          di, ui, g.fmask, P.mutual != 0, f, gg, en);
+                            else
+                                energy_walk_x2_fast<false>(P, pos, yz, s_ept[warp], lane, i, jbase, oix, oiy, oiz, pi,
+                                                           di, ui, g.fmask, P.mutual != 0, f, gg, en);
+                        } else if (g.fold)
                             energy_walk_x2<true>(P, pos, yz, s_ept[warp], lane, i, jbase, oix, oiy, oiz, pi, di, ui,
                                                  g.fmask, damp_r2, rv4p, rv4f, P.mutual != 0, f, gg, en);
                         else
@@ -1405,6 +1671,13 @@ __global__ void __launch_bounds__(kSymThreads, 3) k_energy_sym(
                                                   exc_s, g, cA, cB, lane, i, ibase, jbase, e0, e1, oix, oiy, oiz, me,
                                                   diag, damp_r2, rv4p, rv4f, f, gg, en);
                     }
+                } else if (!g.near && P.lab_energy) {
+                    if (g.fold)
+                        energy_walk<R, true, false, true>(P, pos, yz, sp, sd, su, lane, i, jbase, oix, oiy, oiz, me,
+                                                          diag, partners, damp_r2, rv4p, rv4f, f, gg, en);
+                    else
+                        energy_walk<R, false, false, true>(P, pos, yz, sp, sd, su, lane, i, jbase, oix, oiy, oiz, me,
+                                                           diag, partners, damp_r2, rv4p, rv4f, f, gg, en);
                 } else if (g.fold) {
                     energy_walk<R, true, false>(P, pos, yz, sp, sd, su, lane, i, jbase, oix, oiy, oiz, me, diag,
                                                 partners, damp_r2, rv4p, rv4f, f, gg, en);

@@ -153,6 +153,20 @@ class CudaCalcTholeDipoleForceKernel:
         self._check(self._lib.tdp_update_params(self._h, system.n, _dptr(b.q), _dptr(b.d), _dptr(b.a), _dptr(b.t),
                                                 _iptr(b.types), _iptr(b.z), _iptr(b.x), _iptr(b.y)))
 
+    def updateParticleParams(self, charges, dipoles, polarizabilities, tholes) -> None:
+        """Per-particle parameters only (axis frames and covalent maps stay):
+        host arrays, or contiguous float64 CUDA torch tensors, which then never
+        leave the device."""
+        arrs = [charges, dipoles, polarizabilities, tholes]
+        if all(getattr(a, "is_cuda", False) for a in arrs):
+            for a in arrs:
+                assert a.dtype.itemsize == 8 and a.is_contiguous()
+            rc = self._lib.tdp_update_particle_params(self._h, *[C.c_void_p(a.data_ptr()) for a in arrs], 1)
+        else:
+            hs = [np.ascontiguousarray(np.asarray(a, dtype=np.float64)) for a in arrs]
+            rc = self._lib.tdp_update_particle_params(self._h, *[h.ctypes.data_as(C.c_void_p) for h in hs], 0)
+        self._check(rc)
+
     def enableTiming(self, on: bool = True) -> None:
         self._check(self._lib.tdp_enable_timing(self._h, 1 if on else 0))
 
@@ -240,6 +254,12 @@ class CudaCalcTholeDipoleForceKernel:
         self._check(self._lib.tdp_adjoint(self._h, None if g is None else g.ctypes.data_as(C.c_void_p),
                                           float(dL_dE), _dptr(out)))
         return out
+
+    def adjoint_device(self, dL_dF_ptr: int, dL_dE: float, grads_ptr: int) -> None:
+        """tdp_adjoint on device memory: dL_dF (n*3, 0 = zero) and grads (n*6) are
+        raw CUDA pointers."""
+        self._check(self._lib.tdp_adjoint_device(self._h, C.c_void_p(dL_dF_ptr or None), float(dL_dE),
+                                                 C.c_void_p(grads_ptr)))
 
     def solverStats(self):
         it, conv, st = C.c_int32(), C.c_int32(), C.c_int32()

@@ -16,8 +16,13 @@ using namespace OpenMM;
 
 KernelImpl* CudaTholeDipoleKernelFactory::createKernelImpl(std::string name, const Platform& platform,
                                                            ContextImpl& context) const {
-    if (name == CalcTholeDipoleForceKernel::Name())
-        return new CudaCalcTholeDipoleForceKernel(name, platform, context.getSystem());
+    if (name == CalcTholeDipoleForceKernel::Name()) {
+        CudaCalcTholeDipoleForceKernel* k = new CudaCalcTholeDipoleForceKernel(name, platform, context.getSystem());
+        // The CUDA platform's "Precision" property: "double" selects the FP64
+        // form; "single" and "mixed" the mixed form.
+        if (platform.getPropertyDefaultValue("Precision") == "double") k->setPrecision(TDP_PRECISION_DOUBLE);
+        return k;
+    }
     throw OpenMMException((std::string("Tried to create kernel with illegal kernel name '") + name + "'").c_str());
 }
 

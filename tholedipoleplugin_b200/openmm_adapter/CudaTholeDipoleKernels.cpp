@@ -11,11 +11,19 @@ using OpenMM::OpenMMException;
 using OpenMM::Vec3;
 
 namespace {
-// Host platform data: positions, forces and box vectors as vectors of Vec3
-// (the layout of OpenMM's ReferencePlatform::PlatformData, which
-// ReferenceTholeDipoleKernels.cpp:45-68 reads).
+// Platform data in one of two shapes (openmm/internal/ContextImpl.h):
+// host positions, forces and box vectors as vectors of Vec3 (the layout of
+// OpenMM's ReferencePlatform::PlatformData, which
+// ReferenceTholeDipoleKernels.cpp:45-68 reads), or the CUDA platform
+// context's device buffers (posq, atom index, fixed-point forces).
+bool onDevice(OpenMM::ContextImpl& context) {
+    return *static_cast<const int*>(context.getPlatformData()) == OpenMM::kDevicePlatformData;
+}
 OpenMM::HostPlatformData& data(OpenMM::ContextImpl& context) {
     return *static_cast<OpenMM::HostPlatformData*>(context.getPlatformData());
+}
+OpenMM::DevicePlatformData& device(OpenMM::ContextImpl& context) {
+    return *static_cast<OpenMM::DevicePlatformData*>(context.getPlatformData());
 }
 static_assert(sizeof(Vec3) == 3 * sizeof(double), "Vec3 must be three packed doubles");
 }  // namespace
@@ -96,7 +104,7 @@ void CudaCalcTholeDipoleForceKernel::initialize(const OpenMM::System& system, co
 
 void CudaCalcTholeDipoleForceKernel::syncBox(OpenMM::ContextImpl& context) {
     if (!usePme_) return;
-    const Vec3* b = data(context).periodicBoxVectors;
+    const Vec3* b = onDevice(context) ? device(context).periodicBoxVectors : data(context).periodicBoxVectors;
     double box9[9];
     for (int r = 0; r < 3; r++)
         for (int c = 0; c < 3; c++) box9[3 * r + c] = b[r][c];
@@ -104,6 +112,14 @@ void CudaCalcTholeDipoleForceKernel::syncBox(OpenMM::ContextImpl& context) {
 }
 
 const double* CudaCalcTholeDipoleForceKernel::positions(OpenMM::ContextImpl& context) {
+    if (onDevice(context)) {
+        // The queries run on the coordinates of the context's buffers: one
+        // evaluation there (no forces added), after which NULL positions
+        // select them.
+        const OpenMM::DevicePlatformData& d = device(context);
+        check(tdp_compute_openmm(handle_, d.posq, d.posqIsDouble, d.atomIndex, d.paddedNumAtoms, nullptr, nullptr, 0u));
+        return nullptr;
+    }
     std::vector<Vec3>& pos = *data(context).positions;
     if ((int)pos.size() != numParticles_) throw OpenMMException("TholeDipoleForce: wrong number of positions");
     return reinterpret_cast<const double*>(pos.data());
@@ -113,9 +129,17 @@ const double* CudaCalcTholeDipoleForceKernel::positions(OpenMM::ContextImpl& con
 // the context's force array and the energy is returned.
 double CudaCalcTholeDipoleForceKernel::execute(OpenMM::ContextImpl& context, bool includeForces, bool includeEnergy) {
     syncBox(context);
-    std::vector<Vec3>& forces = *data(context).forces;
     double energy = 0.0;
     uint32_t flags = TDP_COMPUTE_ENERGY | (includeForces ? TDP_COMPUTE_FORCES : 0u);
+    if (onDevice(context)) {
+        // The CUDA platform's buffers: posq in, fixed-point forces added.
+        const OpenMM::DevicePlatformData& d = device(context);
+        check(tdp_compute_openmm(handle_, d.posq, d.posqIsDouble, d.atomIndex, d.paddedNumAtoms, d.force, &energy,
+                                 flags));
+        (void)includeEnergy;
+        return energy;
+    }
+    std::vector<Vec3>& forces = *data(context).forces;
     check(tdp_compute(handle_, positions(context), TDP_F64, 0, reinterpret_cast<double*>(forces.data()), TDP_F64,
                       &energy, flags));
     (void)includeEnergy;

@@ -6,10 +6,8 @@
 // total dipoles, potential, multipole moments, the PME-parameter query, the
 // updateParametersInContext equivalence (:255-313) and its size check.
 //
-// Input (whitespace separated): n method polarization cutoff ewald_tol eps
-// max_iter n_extrap [coefficients], 9 box numbers, then per particle: q dx dy dz
-// polarizability thole axis_type z x y n12 [atoms] n13 [atoms] mass px py pz,
-// then n_grid and grid points.  Argument 2 selects "mixed" or "double".
+// Input: the text description of driver_input.h.  Argument 2 selects "mixed"
+// or "double".
 #include <cmath>
 #include <cstdio>
 #include <cstdlib>
@@ -20,6 +18,7 @@
 
 #include "CudaTholeDipoleKernelFactory.h"
 #include "CudaTholeDipoleKernels.h"
+#include "driver_input.h"
 #include "openmm/internal/ContextImpl.h"
 
 using namespace TholeDipolePlugin;
@@ -27,83 +26,18 @@ using namespace OpenMM;
 
 extern "C" void registerTholeDipoleCudaKernelFactories();
 
-static void print_vecs(const char* tag, const std::vector<Vec3>& v) {
-    printf("%s", tag);
-    for (const Vec3& a : v) printf(" %.17g %.17g %.17g", a[0], a[1], a[2]);
-    printf("\n");
-}
-
-static void need(std::istream& in, const char* what) {
-    if (!in) {
-        fprintf(stderr, "adapter_driver: malformed input while reading %s\n", what);
-        std::exit(3);
-    }
-}
-
-static int count(std::istream& in, int lo, int hi, const char* what) {
-    int v = -1;
-    in >> v;
-    need(in, what);
-    if (v < lo || v > hi) {
-        fprintf(stderr, "adapter_driver: %s = %d outside [%d, %d]\n", what, v, lo, hi);
-        std::exit(3);
-    }
-    return v;
-}
+using tdp_driver::print_vecs;
 
 int main(int argc, char** argv) {
     if (argc < 2) return 2;
-    std::ifstream in(argv[1]);
-    if (!in) return 2;
     bool dbl = argc > 2 && std::strcmp(argv[2], "double") == 0;
-    int n = count(in, 0, 1000000, "particle count");
-    int method = count(in, 0, 1, "nonbonded method");
-    int pol = count(in, 0, 2, "polarization type");
-    double cutoff, tol, eps;
-    in >> cutoff >> tol >> eps;
-    need(in, "settings");
-    int maxIter = count(in, 0, 1000000, "max iterations");
-    int nex = count(in, 0, 64, "extrapolation coefficient count");
-    std::vector<double> ex(nex);
-    for (double& c : ex) in >> c;
-    double box[9];
-    for (double& b : box) in >> b;
-    need(in, "coefficients and box");
-    System system;
-    system.setDefaultPeriodicBoxVectors(Vec3(box[0], box[1], box[2]), Vec3(box[3], box[4], box[5]),
-                                        Vec3(box[6], box[7], box[8]));
-    TholeDipoleForce* force = new TholeDipoleForce();
-    force->setNonbondedMethod((TholeDipoleForce::NonbondedMethod)method);
-    force->setPolarizationType((TholeDipoleForce::PolarizationType)pol);
-    force->setCutoffDistance(cutoff);
-    force->setEwaldErrorTolerance(tol);
-    force->setMutualInducedTargetEpsilon(eps);
-    force->setMutualInducedMaxIterations(maxIter);
-    if (nex > 0) force->setExtrapolationCoefficients(ex);
-    std::vector<Vec3> pos(n);
-    for (int i = 0; i < n; i++) {
-        double q, pl, th, mass;
-        std::vector<double> d(3);
-        int t, z, x, y;
-        in >> q >> d[0] >> d[1] >> d[2] >> pl >> th >> t >> z >> x >> y;
-        need(in, "particle parameters");
-        int idx = force->addParticle(q, d, pl, th, t, z, x, y);
-        for (int list = 0; list < 2; list++) {
-            int k = count(in, 0, 64, "covalent list length");
-            std::vector<int> atoms(k);
-            for (int& a : atoms) in >> a;
-            need(in, "covalent atoms");
-            force->setCovalentMap(idx, list == 0 ? TholeDipoleForce::Covalent12 : TholeDipoleForce::Covalent13, atoms);
-        }
-        in >> mass >> pos[i][0] >> pos[i][1] >> pos[i][2];
-        need(in, "mass and position");
-        system.addParticle(mass);
-    }
-    int ng = count(in, 0, 100000, "grid point count");
-    std::vector<Vec3> grid(ng);
-    for (Vec3& g : grid) in >> g[0] >> g[1] >> g[2];
-    need(in, "grid points");
-    system.addForce(force);
+    tdp_driver::Input input;
+    tdp_driver::read_input(argv[1], input);
+    System& system = input.system;
+    TholeDipoleForce* force = input.force;
+    const int n = input.n;
+    const std::vector<Vec3>& pos = input.positions;
+    const std::vector<Vec3>& grid = input.grid;
 
     try {
     registerTholeDipoleCudaKernelFactories();

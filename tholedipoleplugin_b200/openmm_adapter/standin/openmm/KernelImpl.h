@@ -26,6 +26,7 @@ public:
     Kernel() {}
     explicit Kernel(KernelImpl* impl) : impl(impl) {}
     template <class T> T& getAs() { return dynamic_cast<T&>(*impl); }
+    template <class T> const T& getAs() const { return dynamic_cast<const T&>(*impl); }
     KernelImpl& getImpl() { return *impl; }
 private:
     std::shared_ptr<KernelImpl> impl;
@@ -41,6 +42,12 @@ public:
     virtual ~Platform() {}
     const std::string& getName() const { return name; }
     void registerKernelFactory(const std::string& kernel, KernelFactory* factory) { factories[kernel] = factory; }
+    // Platform properties (OpenMM's CUDA platform has e.g. "Precision").
+    void setPropertyDefaultValue(const std::string& property, const std::string& value) { props[property] = value; }
+    std::string getPropertyDefaultValue(const std::string& property) const {
+        auto it = props.find(property);
+        return it == props.end() ? std::string() : it->second;
+    }
     Kernel createKernel(const std::string& kernel, ContextImpl& context) const;
     static void registerPlatform(Platform* p);
     static int getNumPlatforms();
@@ -49,6 +56,7 @@ public:
 private:
     std::string name;
     std::map<std::string, KernelFactory*> factories;
+    std::map<std::string, std::string> props;
 };
 }  // namespace OpenMM
 #endif

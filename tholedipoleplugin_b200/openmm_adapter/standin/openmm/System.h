@@ -12,6 +12,9 @@ public:
     int getNumParticles() const { return (int)masses.size(); }
     double getParticleMass(int i) const { return masses[i]; }
     int addForce(Force* f) { forces.push_back(f); return (int)forces.size() - 1; }
+    int getNumForces() const { return (int)forces.size(); }
+    const Force& getForce(int i) const { return *forces[i]; }
+    Force& getForce(int i) { return *forces[i]; }
     void setDefaultPeriodicBoxVectors(const Vec3& a, const Vec3& b, const Vec3& c) { box[0] = a; box[1] = b; box[2] = c; }
     void getDefaultPeriodicBoxVectors(Vec3& a, Vec3& b, Vec3& c) const { a = box[0]; b = box[1]; c = box[2]; }
 private:
