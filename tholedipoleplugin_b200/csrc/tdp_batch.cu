@@ -51,6 +51,9 @@ struct BatchArgs {
     double target_eps;
     double damp_r2;
     double rinv4_power, rinv4_fill;
+    // Mixed form: 1 = permanent field and energy/force pass in FP64, FP32 only
+    // in the CG matvec; 0 = every pair pass in FP32.
+    int fp64_passes;
     const int* order;   // clusters by decreasing size
     const int* coff;    // num_clusters+1 atom offsets
     const double* pos;  // n*3
@@ -94,6 +97,8 @@ __host__ __device__ inline size_t batch_smem(int M, int X, int korder) {
     b += sizeof(int) * ((size_t)M + 1 + (size_t)X);
     b = align_up(b, 8);
     b += sizeof(R) * 2 * (size_t)X;
+    b = align_up(b, 16);
+    b += sizeof(double) * 5 * (size_t)M;            // FP64 lab dipoles, charges, Thole factors
     return align_up(b, 16);
 }
 
@@ -109,6 +114,7 @@ struct Cl {
     int4* axis;
     int *eoff, *ej;
     R *em, *es;
+    double *lab64, *q64, *th64;   // FP64 lab-frame dipoles (3 per atom), charges, Thole factors
     int M;
 };
 
@@ -143,7 +149,12 @@ __device__ Cl<R> carve(char* base, int M, int X, int korder) {
     off = align_up((size_t)(reinterpret_cast<char*>(ip) - base), 8);
     R* rp = reinterpret_cast<R*>(base + off);
     c.em = rp; rp += X;
-    c.es = rp;
+    c.es = rp; rp += X;
+    off = align_up((size_t)(reinterpret_cast<char*>(rp) - base), 16);
+    double* dd = reinterpret_cast<double*>(base + off);
+    c.lab64 = dd; dd += 3 * M;
+    c.q64 = dd; dd += M;
+    c.th64 = dd;
     return c;
 }
 
@@ -440,6 +451,9 @@ __device__ __forceinline__ void cluster_lab(const Cl<R>& c, const BatchArgs& A, 
         dv.z = (R)lab[2];
         dv.w = (R)A.thole[a0 + i];
         c.dipt[i] = dv;
+        for (int k = 0; k < 3; k++) c.lab64[3 * i + k] = lab[k];
+        c.q64[i] = A.charge[a0 + i];
+        c.th64[i] = A.thole[a0 + i];
     }
     __syncthreads();
 }
@@ -493,6 +507,64 @@ __device__ __forceinline__ void cluster_fixed_field(const Cl<R>& c, const BatchA
         c.vec[i] = v;
     }
     __syncthreads();
+}
+
+// cluster_fixed_field with FP64 pair arithmetic on the FP64 coordinates,
+// dipoles, charges and Thole factors (the mixed form's FP64 passes).
+template <class R>
+__device__ __forceinline__ void cluster_fixed_field64(const Cl<R>& c, const BatchArgs& A, int n) {
+    typedef typename Vec4T<R>::type V4;
+    const double damp_r2 = A.damp_r2;
+    for (int base = 0; base < n; base += blockDim.x) {
+        const int na = min(n - base, (int)blockDim.x);
+        const Split sp = split(na, A.lmax);
+        const int i = base + sp.a;
+        double fx = 0, fy = 0, fz = 0;
+        if (sp.act) {
+            const double pix = c.pos[3 * i], piy = c.pos[3 * i + 1], piz = c.pos[3 * i + 2];
+            const double ti = c.th64[i];
+            for (int j = sp.l; j < n; j += sp.L) {
+                if (j == i) continue;
+                R m, s;
+                pair_scales(c, i, j, m, s);
+                if (m == R(0)) continue;
+                const double dx = c.pos[3 * j] - pix, dy = c.pos[3 * j + 1] - piy, dz = c.pos[3 * j + 2] - piz;
+                const double r2 = dx * dx + dy * dy + dz * dz;
+                double tx = 0, ty = 0, tz = 0;
+                pair_fixed<double>(dx, dy, dz, r2, c.q64[j], c.lab64[3 * j], c.lab64[3 * j + 1], c.lab64[3 * j + 2],
+                                   ti, c.th64[j], damp_r2, tx, ty, tz);
+                fx += (double)m * tx;
+                fy += (double)m * ty;
+                fz += (double)m * tz;
+            }
+        }
+        double* pt = c.part + 3 * threadIdx.x;
+        pt[0] = fx;
+        pt[1] = fy;
+        pt[2] = fz;
+        __syncthreads();
+        if ((int)threadIdx.x < na)
+            for (int k = 0; k < 3; k++)
+                c.E[3 * (base + threadIdx.x) + k] = split_sum(c.part, 3, k, threadIdx.x, na, sp.T);
+        __syncthreads();
+    }
+    for (int i = threadIdx.x; i < n; i += blockDim.x) {
+        const double al = c.alpha[i];
+        for (int k = 0; k < 3; k++) c.mu[3 * i + k] = al * c.E[3 * i + k];
+        V4 v;
+        v.x = (R)c.mu[3 * i];
+        v.y = (R)c.mu[3 * i + 1];
+        v.z = (R)c.mu[3 * i + 2];
+        v.w = c.dipt[i].w;
+        c.vec[i] = v;
+    }
+    __syncthreads();
+}
+
+template <class R>
+__device__ __forceinline__ void cluster_field_any(const Cl<R>& c, const BatchArgs& A, int n, R damp_r2) {
+    if (sizeof(R) == 4 && A.fp64_passes) cluster_fixed_field64(c, A, n);
+    else cluster_fixed_field(c, A, n, damp_r2);
 }
 
 // Mutual polarization: CG in y = mu / sqrt(alpha) on (I - S T S) y = S E from
@@ -589,7 +661,7 @@ __global__ void __launch_bounds__(512) k_batch(BatchArgs A) {
         }
         cluster_load(c, A, a0, n);
         cluster_lab(c, A, a0, n);
-        cluster_fixed_field(c, A, n, damp_r2);
+        cluster_field_any(c, A, n, damp_r2);
 
         // ---- induced dipoles ---------------------------------------------------------------
         int it = 0;
@@ -642,12 +714,59 @@ __global__ void __launch_bounds__(512) k_batch(BatchArgs A) {
         double* frc = c.w;
         double* trq = c.w + 3 * c.M;
         double en = 0.0;
+        const bool e64 = sizeof(R) == 4 && A.fp64_passes;
+        const bool lab_ok = A.rinv4_power == 0.0 && A.rinv4_fill == 0.0;
         for (int base = 0; base < n; base += blockDim.x) {
             const int na = min(n - base, (int)blockDim.x);
             const Split sp = split(na, A.lmax);
             const int i = base + sp.a;
             double f[6] = {0, 0, 0, 0, 0, 0};
-            if (sp.act) {
+            if (sp.act && e64) {
+                // FP64 pair arithmetic on the FP64 records; pairs beyond the
+                // damping range with unit scales take the lab-frame form.
+                const EAtom<double> me{c.q64[i], c.lab64[3 * i], c.lab64[3 * i + 1], c.lab64[3 * i + 2],
+                                       c.mu[3 * i], c.mu[3 * i + 1], c.mu[3 * i + 2], c.th64[i]};
+                const double pix = c.pos[3 * i], piy = c.pos[3 * i + 1], piz = c.pos[3 * i + 2];
+                const bool mutual = A.polarization == TDP_MUTUAL;
+                for (int j = sp.l; j < n; j += sp.L) {
+                    if (j == i) continue;
+                    R mr, sr;
+                    pair_scales(c, i, j, mr, sr);
+                    const double m = mr, s = sr;
+                    if (m == 0.0 && s == 0.0) continue;
+                    const EAtom<double> other{c.q64[j], c.lab64[3 * j], c.lab64[3 * j + 1], c.lab64[3 * j + 2],
+                                              c.mu[3 * j], c.mu[3 * j + 1], c.mu[3 * j + 2], c.th64[j]};
+                    const double dx = c.pos[3 * j] - pix, dy = c.pos[3 * j + 1] - piy, dz = c.pos[3 * j + 2] - piz;
+                    const double r2 = dx * dx + dy * dy + dz * dz;
+                    bool yzd = fabs(dy) > 1e-5 || fabs(dz) > 1e-5;
+                    if (!yzd) yzd = (piy != c.pos[3 * j + 1]) || (piz != c.pos[3 * j + 2]);
+                    double fx = 0, fy = 0, fz = 0, tx = 0, ty = 0, tz = 0, e = 0;
+                    if (lab_ok && m == 1.0 && s == 1.0 && !(r2 < A.damp_r2)) {
+                        double gx = 0, gy = 0, gz = 0, ux = 0, uy = 0, uz = 0;
+                        const double kap = mutual ? 1.0 : -1.0;
+                        if (i < j)
+                            pair_energy_lab<double>(dx, dy, dz, r2, yzd, me, other, kap, fx, fy, fz, tx, ty, tz, gx, gy,
+                                                    gz, ux, uy, uz, e);
+                        else
+                            pair_energy_lab<double>(-dx, -dy, -dz, r2, yzd, other, me, kap, gx, gy, gz, ux, uy, uz, fx,
+                                                    fy, fz, tx, ty, tz, e);
+                        if (i > j) e = 0.0;
+                    } else if (i < j) {
+                        pair_energy<double, true>(dx, dy, dz, r2, yzd, me, other, m, s, A.damp_r2, A.rinv4_power,
+                                                  A.rinv4_fill, mutual, fx, fy, fz, tx, ty, tz, e);
+                    } else {
+                        pair_energy<double, false>(-dx, -dy, -dz, r2, yzd, other, me, m, s, A.damp_r2, A.rinv4_power,
+                                                   A.rinv4_fill, mutual, fx, fy, fz, tx, ty, tz, e);
+                    }
+                    f[0] += fx;
+                    f[1] += fy;
+                    f[2] += fz;
+                    f[3] += tx;
+                    f[4] += ty;
+                    f[5] += tz;
+                    en += e;
+                }
+            } else if (sp.act) {
                 const V4 pi = c.posq[i], di = c.dipt[i], ui = c.vec[i];
                 const EAtom<R> me{pi.w, di.x, di.y, di.z, ui.x, ui.y, ui.z, di.w};
                 const double yi = c.pos[3 * i + 1], zi = c.pos[3 * i + 2];
@@ -822,7 +941,7 @@ __global__ void __launch_bounds__(512) k_batch_adjoint(BatchArgs A, AdjArgs G) {
         }
         const double gE = G.gE ? G.gE[cid] : 0.0;
         // Permanent field of the forward into c.E (also sets c.mu = alpha E).
-        cluster_fixed_field(c, A, n, damp_r2);
+        cluster_field_any(c, A, n, damp_r2);
         for (int k = threadIdx.x; k < 3 * n; k += blockDim.x) g.etm[k] = c.E[k];
 
         // ---- g_tau = M^T g (k_torque_vjp) -------------------------------------------------
@@ -1243,6 +1362,11 @@ int tdp_batch_create(const tdp_system_desc* desc, int32_t num_clusters, const in
         const bool r4 = (desc->flags & TDP_FLAG_DD_FORCE_R4) != 0;
         a.rinv4_power = r4 ? 1.0 : 0.0;
         a.rinv4_fill = 0.0;
+        // TDP_BATCH_FP32_PASSES=1 runs every pair pass of the mixed form in
+        // FP32 (for comparisons).
+        a.fp64_passes = 1;
+        if (const char* env = getenv("TDP_BATCH_FP32_PASSES"))
+            if (atoi(env) == 1) a.fp64_passes = 0;
 
         auto& o = b->owned;
         int* d_order = dalloc<int>(num_clusters, o);
