@@ -47,12 +47,22 @@ ROOT = os.path.dirname(os.path.abspath(__file__))
 sys.path.insert(0, ROOT)
 
 NS_PER_DAY = 1e-6 * 86400.0  # per (step/s) at 1 fs
-# Algorithmic operation counts per unordered pair (reference semantics):
-# mutual-field pass (both sides) 57 FLOP + 9 FLOP minimum image;
-# energy/force/torque pair 280 FLOP; permanent-field pair 70 FLOP.
+# Algorithmic operation counts per unordered pair, counted from the reference's
+# own operation sequence (ReferenceTholeDipoleForce.cpp; +, -, *, / one FLOP
+# each, a fused multiply-add two, sqrt/exp one), minimum image included:
+#  mutual-field pass (:766-818 with getAndScaleInverseRs :646-676): delta 3,
+#    minimum image 9, r^2 5, sqrt 1, inverse powers and damping test 11, I
+#    scale 2, both sides 2 x 18 -> 66;
+#  permanent-field pair (:678-713): delta 3, minimum image 9, r 6, inverse
+#    powers 11, both sides 2 x (dot 5 + factor 3 + field 9 + scale 6) -> 75;
+#  energy/force/torque pair (:129-366, Mutual): delta 3, minimum image 9, r 6,
+#    QI frame 33, four rotations 72, inverse powers 3, Thole factors 25 + exp,
+#    interaction coefficients and terms 102, energy/force/torque sums 63,
+#    induced torques 12, induced-induced 52, QI force 9, back rotations 54,
+#    accumulation 12 -> 450.
 FLOP_MATVEC_PAIR = 66
-FLOP_ENERGY_PAIR = 280
-FLOP_FIXED_PAIR = 70
+FLOP_ENERGY_PAIR = 450
+FLOP_FIXED_PAIR = 75
 # Algorithmic HBM bytes per atom and launch: matvec 16 (posq) + 12 (operand) +
 # 12 (result) + 48 (four CG vectors); energy pass 16 (posq) + 16 (dipole,
 # thole) + 16 (induced) + 16 (raw y, z) + 56 (seven FP64 outputs).
@@ -60,6 +70,9 @@ BYTES_MATVEC_ATOM = 88
 # FP64 records of the plain form: posq 32 + operand 32 + result 24 + CG vectors 48.
 BYTES_MATVEC_ATOM_FP64 = 136
 BYTES_ENERGY_ATOM = 120
+# Solver tolerances of the timed runs (tholedipoleplugin_b200/systems.py says why).
+from tholedipoleplugin_b200.systems import BOX_SOLVER_EPS as BOX_EPS  # noqa: E402
+from tholedipoleplugin_b200.systems import CLUSTER_SOLVER_EPS as CLUSTER_EPS  # noqa: E402
 # CPU samples of the reference run on 13^3 = 2,197 waters (6,591 atoms) at the
 # density of the 32^3 box and are scaled to the full box by the pair count.
 SAMPLE_SIDE = 13
@@ -289,7 +302,9 @@ def cpu_baseline_single(n_atoms, sweeps):
     te = _ref_sample("energy")
     step, t_pass = reference_step_seconds(tf, tp, te, n_atoms, sweeps)
     ns = _sample_system().n
+    scale = (n_atoms * (n_atoms - 1)) / (ns * (ns - 1))
     return {"value": NS_PER_DAY / step, "unit": "ns/day", "cores": 1, "kind": "reference",
+            "solve_seconds": scale * (tf + sweeps * t_pass),
             "sample": (f"reference ReferenceTholeDipoleForce.cpp (compiled oracle/_ref), 1 core: permanent field "
                        f"{tf:.2f}s, one mutual-field pass {t_pass:.2f}s, energy/force pass {te - tf:.2f}s on a "
                        f"{ns}-atom water box; scaled by the pair count to {n_atoms} atoms and {sweeps} Jacobi "
@@ -330,8 +345,8 @@ def run_reference(args):
     value = cores * NS_PER_DAY / step
     base.update({
         "value": value, "ms_per_step": step * 1e3 / cores,
-        "config": {"workload": f"{n_atoms}-atom water box MD step (reference platform semantics)",
-                   "n_atoms": n_atoms, "jacobi_sweeps": sweeps},
+        "config": workload_config(args.config),
+        "solver": {"reference_jacobi_sweeps": sweeps},
         "cpu_baseline": {"value": value, "unit": "ns/day", "cores": cores, "kind": "reference",
                          "sample": (f"{cores} concurrent processes of the compiled reference; per process: "
                                     f"permanent field {tf:.2f}s, mutual-field pass {t_pass:.2f}s (mean of "
@@ -344,10 +359,10 @@ def run_reference(args):
 
 
 # Jacobi sweeps the reference's loop (RTDF.cpp:820-851) takes to an RMS dipole
-# change below 1e-6 on each seeded box, as counted by the library's Jacobi
+# change below BOX_EPS on each seeded box, as counted by the library's Jacobi
 # solver, which runs that loop sweep for sweep (the iteration count is tested
-# against the reference's): 216 waters 39, 4,096 waters 92, 32,768 waters 134
-# (the last re-measured by every default bench run, config.reference_jacobi_sweeps).
+# against the reference's); re-measured by every default bench run
+# (solver.reference_jacobi_sweeps).
 REFERENCE_JACOBI_SWEEPS = {"small": 39, "medium": 92, "large": 134}
 
 
@@ -380,14 +395,19 @@ def _ref_clusters(args):
 
 
 def run_clusters(args, rank, world, barrier, max_over_ranks, stream):
+    """The batched-cluster workload, both forms at CLUSTER_EPS: clusters/s
+    (device-resident and end to end), the tile the autotuner chose, and (rank
+    0) per-cluster errors of both forms against the FP64 oracle on a seeded
+    sample, plus the compiled reference on one core over 384 clusters."""
     import numpy as np
     import torch
     from tholedipoleplugin_b200.batch import ClusterBatch
 
-    clusters = _cluster_workload(3 + 100 * rank)
-    res = {"workload": f"{N_CLUSTERS} isolated water clusters, 4-64 waters each (seeded), NoCutoff, "
-                       "mutual polarization to 1e-6, one persistent graph-captured launch per evaluation"}
+    clusters = [c.copy(target_eps=CLUSTER_EPS) for c in _cluster_workload(3 + 100 * rank)]
+    res = {"workload": f"{N_CLUSTERS} isolated water clusters, 4-64 waters each (seeded), NoCutoff, mutual "
+                       f"polarization to {CLUSTER_EPS:g}, one persistent graph-captured launch per evaluation"}
     reps = max(5, args.steps)
+    out = {}
     for prec in ("mixed", "double"):
         with ClusterBatch(clusters, precision=prec) as b:
             b.setStream(stream.cuda_stream)
@@ -406,7 +426,6 @@ def run_clusters(args, rank, world, barrier, max_over_ranks, stream):
             s1.record(stream)
             torch.cuda.synchronize()
             t_ms = max_over_ranks(s0.elapsed_time(s1) / reps)
-            # End to end: host positions in, host forces and energies out, every call.
             hpos = torch.empty((b.n, 3), dtype=torch.float64, pin_memory=True).numpy()
             hpos[...] = b.positions
             barrier()
@@ -416,51 +435,62 @@ def run_clusters(args, rank, world, barrier, max_over_ranks, stream):
             t_e2e = max_over_ranks((time.perf_counter() - t0) / reps)
             it, ep = b.solverStats()
             tile = b.tile()
-            cand = b.tileCandidates()
-            res[prec] = {"clusters_per_s": world * N_CLUSTERS / (t_ms * 1e-3), "ms_per_launch": t_ms,
-                         "e2e_clusters_per_s": world * N_CLUSTERS / t_e2e, "n_atoms": b.n,
-                         "cg_iterations_mean": float(it.mean()), "cg_iterations_max": int(it.max()),
-                         "max_epsilon": float(ep.max()),
-                         "tile": {"threads": tile["threads"], "lanes_per_atom": tile["lanes"], "ctas": tile["ctas"]},
-                         "autotuner_ms": {f"{c['threads']}x{c['lanes']}": round(c["ms"], 4) for c in cand}}
-            if prec == "mixed":
-                e_mixed, f_mixed = b.compute()
-                offs = b.offsets
-    res["mixed_over_plain"] = res["mixed"]["clusters_per_s"] / res["double"]["clusters_per_s"]
-    # Pair work of one evaluation: every cluster's fixed field, its matvecs and its energy pass.
-    sizes = np.diff(offs).astype(np.float64)
-    pairs = float((sizes * (sizes - 1) / 2).sum())
-    res["unordered_pairs"] = pairs
+            res[prec] = {"clusters_per_s": _r(world * N_CLUSTERS / (t_ms * 1e-3)), "ms_per_launch": _r(t_ms),
+                         "e2e_clusters_per_s": _r(world * N_CLUSTERS / t_e2e),
+                         "cg_iterations_mean": _r(float(it.mean())), "cg_iterations_max": int(it.max()),
+                         "tile": f"{tile['threads']} threads x {tile['lanes']} lanes, {tile['ctas']} CTAs"}
+            out[prec] = b.compute()
+            offs = b.offsets
+    res["n_atoms"] = int(offs[-1])
+    res["mixed_over_plain"] = _r(res["mixed"]["clusters_per_s"] / res["double"]["clusters_per_s"])
+    res["forms"] = "mixed: FP32 CG matvec with FP64 refinement, FP64 permanent-field and energy passes; plain: FP64"
     if rank == 0:
         from oracle import oracle as O
-        # Per-cluster error against the FP64 oracle (converged to 1e-12) on a seeded sample.
-        sample = np.random.default_rng(0).choice(N_CLUSTERS, 32, replace=False)
-        e_rel, f_rel = [], []
-        for k in sample:
-            c = clusters[k]
-            ref = O.compute(c.copy(target_eps=1e-12, max_iter=5000), "port")
-            sl = slice(int(offs[k]), int(offs[k + 1]))
-            e_rel.append(abs(e_mixed[k] - ref.energy) / abs(ref.energy))
-            f_rel.append(rel_rms(f_mixed[sl], ref.forces))
-        res["errors_mixed_vs_fp64_oracle"] = {
-            "clusters_sampled": len(sample), "energy_rel_median": float(np.median(e_rel)),
-            "energy_rel_max": float(np.max(e_rel)), "force_rms_rel_median": float(np.median(f_rel)),
-            "force_rms_rel_max": float(np.max(f_rel)),
-            "note": "batch at the workload's 1e-6 target; oracle converged to 1e-12"}
+        sample = np.random.default_rng(0).choice(N_CLUSTERS, 48, replace=False)
+        refs = {int(k): O.compute(clusters[k].copy(target_eps=1e-12, max_iter=5000), "port") for k in sample}
+        errs = {}
+        for prec in ("mixed", "double"):
+            e_all, f_all = out[prec]
+            e_rel, f_rel = [], []
+            for k in sample:
+                ref = refs[int(k)]
+                sl = slice(int(offs[k]), int(offs[k + 1]))
+                e_rel.append(abs(e_all[k] - ref.energy) / abs(ref.energy))
+                f_rel.append(rel_rms(f_all[sl], ref.forces))
+            errs[prec] = {"energy_rel_max": _r(max(e_rel)), "energy_rel_median": _r(float(np.median(e_rel))),
+                          "force_rms_rel_max": _r(max(f_rel))}
+        errs["note"] = f"48 seeded clusters at {CLUSTER_EPS:g}; FP64 oracle converged to 1e-12"
+        res["errors_vs_fp64_oracle"] = errs
         if world == 1 and O.reference_available():
             t, m = _ref_clusters((3, 0, 384))
-            res["cpu_baseline"] = {"value": m / t, "unit": "clusters/s", "cores": 1, "kind": "reference",
-                                   "sample": f"compiled reference on the first {m} clusters of the workload, "
-                                             f"1 core, {t:.1f}s"}
+            res["cpu_baseline"] = {"value": _r(m / t), "unit": "clusters/s", "cores": 1, "kind": "reference",
+                                   "sample": f"compiled reference, first {m} clusters at 1e-6, 1 core, {t:.1f}s"}
     return res
 
-
-# ---------------------------------------------------------------------------
-# Our arm.
-# ---------------------------------------------------------------------------
 def rel_rms(a, b):
     import numpy as np
     return float(np.sqrt(np.mean((a - b) ** 2) / np.mean(b ** 2)))
+
+
+def _r(x, sig=4):
+    """x rounded to sig significant digits (keeps the JSON line short)."""
+    if x is None or not isinstance(x, (int, float)) or x == 0 or not math.isfinite(x):
+        return x
+    return float(f"{x:.{sig}g}")
+
+
+BOX = {"small": (6, 1.8643), "medium": (16, 4.968), "profile": (24, 9.936 * 24 / 32), "large": (32, 9.936)}
+
+
+def workload_config(config: str, ewald_md: bool = False) -> dict:
+    """The workload both arms report (identical dicts)."""
+    side, box = BOX[config]
+    n = 3 * side ** 3
+    kind = "Ewald mode: cutoff + smooth PME" if ewald_md else "minimum-image all-pairs (the reference's PME flag)"
+    return {"workload": f"{n}-atom rigid water box ({side ** 3} waters, {box:g} nm cubic, {kind}, mutual "
+                        f"polarization to an RMS dipole change of {BOX_EPS:g}), velocity Verlet MD, 1 fs steps",
+            "n_atoms": n, "solver_eps": BOX_EPS, "l2": "working set per pass ~10 MB, L2-resident; every step "
+                                                        "re-reads all of it"}
 
 
 def ewald_section(system, K, W, stream, world, barrier, max_over_ranks, rank):
@@ -477,7 +507,7 @@ def ewald_section(system, K, W, stream, world, barrier, max_over_ranks, rank):
     n = system.n
     res = {"workload": f"{n}-atom water box, Ewald mode: real space within {system.cutoff} nm over a 32-atom tile "
                        f"neighbour list + order-5 smooth PME (tolerance {system.ewald_tolerance}), mutual "
-                       "polarization to 1e-6, velocity Verlet 1 fs"}
+                       f"polarization to {system.target_eps:g}, velocity Verlet 1 fs"}
 
     def md_rate(precision, steps, warm):
         md = DeviceRigidWaterMD(system, precision=precision, warm_start=True, seed=11 + rank, ewald=True)
@@ -502,17 +532,17 @@ def ewald_section(system, K, W, stream, world, barrier, max_over_ranks, rank):
         t = max_over_ranks(e0.elapsed_time(e1))
         params = md.kernel.getPMEParameters()
         md.close()
-        return {"ns_per_day": world * steps / (t * 1e-3) * NS_PER_DAY, "ms_per_step": t / steps, "steps": steps,
-                "cg_iterations_mean": statistics.mean(its), "matvec_ms_per_launch": mv_ms / max(mv_n, 1),
-                "matvec_share": mv_ms / t, "energy_force_ms": en_ms / steps, "energy_force_share": en_ms / t,
-                "launches_per_step": launches / steps}, params
+        return {"ns_per_day": _r(world * steps / (t * 1e-3) * NS_PER_DAY), "ms_per_step": _r(t / steps),
+                "cg_iterations_mean": _r(statistics.mean(its)), "matvec_ms": _r(mv_ms / max(mv_n, 1)),
+                "matvec_share": _r(mv_ms / t), "energy_force_ms": _r(en_ms / steps),
+                "launches_per_step": _r(launches / steps)}, params
 
     mixed, params = md_rate("mixed", K, max(W, 3))
     plain, _ = md_rate("double", max(3, K // 2), 3)
-    res["pme"] = {"alpha_per_nm": params[0], "grid": list(params[1:]), "order": 5}
+    res["pme"] = {"alpha_per_nm": _r(params[0]), "grid": list(params[1:]), "order": 5}
     res["mixed"] = mixed
     res["plain"] = plain
-    res["md_ns_per_day_mixed_over_plain"] = mixed["ns_per_day"] / plain["ns_per_day"]
+    res["md_mixed_over_plain"] = _r(mixed["ns_per_day"] / plain["ns_per_day"])
 
     def solves_per_s(precision, reps):
         with CudaCalcTholeDipoleForceKernel(system, precision=precision, ewald=True) as k:
@@ -533,100 +563,223 @@ def ewald_section(system, K, W, stream, world, barrier, max_over_ranks, rank):
     reps = max(5, K)
     sm, im = solves_per_s("mixed", reps)
     sp, ip = solves_per_s("double", reps)
-    res["scf_solves_per_s"] = {"mixed": sm, "plain": sp, "mixed_over_plain": sm / sp,
-                               "cg_iterations": {"mixed": im, "plain": ip},
-                               "what": "rotation + permanent field + CG to 1e-6 from mu0 = alpha E (Ewald)"}
+    res["scf_solves_per_s"] = {"mixed": _r(sm), "plain": _r(sp), "mixed_over_plain": _r(sm / sp),
+                               "cg_iterations": {"mixed": im, "plain": ip}}
     if rank == 0:
-        def rel_rms(a, b):
-            return float(np.sqrt(np.mean((a - b) ** 2) / np.mean(b ** 2)))
-
         errs = {}
-        with CudaCalcTholeDipoleForceKernel(system.copy(target_eps=1e-9), precision="mixed", ewald=True) as km:
-            em, fm = km.execute(system.positions)
-            mum = km.getInducedDipoles()
         with CudaCalcTholeDipoleForceKernel(system.copy(target_eps=1e-11), precision="double", ewald=True) as kp:
             ep, fp = kp.execute(system.positions)
             mup = kp.getInducedDipoles()
-        errs["mixed_vs_plain_this_box"] = {"energy_rel": abs(em - ep) / abs(ep), "force_rms_rel": rel_rms(fm, fp),
-                                           "induced_rms_rel": rel_rms(mum, mup)}
+        for prec in ("mixed", "double"):
+            with CudaCalcTholeDipoleForceKernel(system, precision=prec, ewald=True) as km:
+                em, fm = km.execute(system.positions)
+                errs[f"{prec}_vs_fp64_tight_this_box"] = _errs(em, fm, km.getInducedDipoles(), ep, fp, mup)
         from oracle import ewald as EW
         small = S.config_small(target_eps=1e-12, max_iter=500)
         alpha, grid = EW.pme_parameters(small.cutoff, small.ewald_tolerance, small.box)
         ref = EW.Ewald(small, alpha, recip="pme", grid=grid).evaluate()
-        for prec, eps in (("mixed", 1e-9), ("double", 1e-11)):
-            with CudaCalcTholeDipoleForceKernel(small.copy(target_eps=eps), precision=prec, ewald=True) as k:
+        for prec in ("mixed", "double"):
+            with CudaCalcTholeDipoleForceKernel(small.copy(target_eps=system.target_eps), precision=prec,
+                                                ewald=True) as k:
                 e, f = k.execute(small.positions)
-                mu = k.getInducedDipoles()
-            errs[f"{prec}_vs_fp64_ewald_oracle_216_waters"] = {
-                "energy_rel": abs(e - ref.energy) / abs(ref.energy), "force_rms_rel": rel_rms(f, ref.forces),
-                "induced_rms_rel": rel_rms(mu, ref.induced)}
+                errs[f"{prec}_vs_fp64_ewald_oracle_216_waters"] = _errs(e, f, k.getInducedDipoles(), ref.energy,
+                                                                        ref.forces, ref.induced)
         res["errors"] = errs
     return res
 
 
-def run_ours(args):
+def _md_rate(system, precision, steps, warm, stream, world, barrier, max_over_ranks, rank, ewald=False,
+             clocks=None):
+    """Device-resident MD with the given form: timed steps, per-kernel times."""
+    import torch
+    from tholedipoleplugin_b200.md import DeviceRigidWaterMD
+    md = DeviceRigidWaterMD(system, precision=precision, warm_start=True, seed=11 + rank, ewald=ewald)
+    md.kernel.enableTiming(True)
+    md.step(warm)
+    torch.cuda.synchronize()
+    barrier()
+    if clocks:
+        clocks.start()
+    ev0, ev1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    r = {"mv_ms": 0.0, "mv_n": 0, "en_ms": 0.0, "fix_ms": 0.0, "launches": 0, "its": []}
+    ev0.record(stream)
+    for _ in range(steps):
+        md.step()
+        st = md.kernel.stageTimes()
+        r["mv_ms"] += st[7]
+        r["mv_n"] += int(st[6])
+        r["en_ms"] += st[8]
+        r["fix_ms"] += st[1]
+        r["launches"] += int(st[9]) + 2  # + kick-drift and kick kernels
+        r["its"].append(md.kernel.solverStats()["iterations"])
+    ev1.record(stream)
+    torch.cuda.synchronize()
+    r["clk"] = clocks.stop() if clocks else None
+    barrier()
+    r["t_ms"] = max_over_ranks(ev0.elapsed_time(ev1))
+    r["temperature"] = md.temperature()
+    r["ns_per_day"] = world * steps / (r["t_ms"] * 1e-3) * NS_PER_DAY
+    md.close()
+    del md
+    torch.cuda.empty_cache()
+    return r
+
+
+def _solves_per_s(system, precision, reps, stream, world, max_over_ranks):
+    """Cold-start SCF solves (rotation + permanent field + CG from mu = alpha E)."""
     import numpy as np
     import torch
-
     from tholedipoleplugin_b200 import _capi as A
+    from tholedipoleplugin_b200.kernel import CudaCalcTholeDipoleForceKernel
+    n = system.n
+    with CudaCalcTholeDipoleForceKernel(system, precision=precision) as k:
+        k.setStream(stream.cuda_stream)
+        dev_pos = torch.tensor(system.positions, dtype=torch.float64, device="cuda")
+        buf = np.zeros((n, 3))
+        k.solveDevice(dev_pos.data_ptr(), A.F64, buf)
+        torch.cuda.synchronize()
+        s0, s1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        s0.record(stream)
+        for _ in range(reps):
+            k.solveDevice(dev_pos.data_ptr(), A.F64, buf)
+        s1.record(stream)
+        torch.cuda.synchronize()
+        return world * reps / (max_over_ranks(s0.elapsed_time(s1)) * 1e-3), k.solverStats()["iterations"]
+
+
+def _errs(e, f, mu, e0, f0, mu0):
+    return {"energy_rel": _r(abs(e - e0) / abs(e0)), "force_rms_rel": _r(rel_rms(f, f0)),
+            "induced_rms_rel": _r(rel_rms(mu, mu0))}
+
+
+def _box_errors(system, config):
+    """Both forms at BOX_EPS against the converged FP64 answer: on this box
+    (the FP64 form solved to 1e-11), on 216 waters (the oracle solved to
+    1e-12) and, when present, on the compiled reference's 12,288-atom golden."""
+    import numpy as np
+    from oracle import oracle as O
     from tholedipoleplugin_b200 import systems as S
     from tholedipoleplugin_b200.kernel import CudaCalcTholeDipoleForceKernel
-    from tholedipoleplugin_b200.md import DeviceRigidWaterMD, HostRigidWaterMD
+
+    def run(s, prec, eps):
+        with CudaCalcTholeDipoleForceKernel(s.copy(target_eps=eps, max_iter=1000), precision=prec) as k:
+            e, f = k.execute(s.positions)
+            return e, f, k.getInducedDipoles()
+
+    out = {}
+    e0, f0, mu0 = run(system, "double", 1e-11)
+    out["this_box_vs_fp64_tight"] = {p: _errs(*run(system, p, BOX_EPS), e0, f0, mu0) for p in ("mixed", "double")}
+    small = S.config_small()
+    ref = O.compute(small.copy(target_eps=1e-12, max_iter=5000), "port")
+    out["water216_vs_fp64_oracle"] = {p: _errs(*run(small, p, BOX_EPS), ref.energy, ref.forces, ref.induced)
+                                      for p in ("mixed", "double")}
+    gpath = os.path.join(ROOT, "tests", "golden", "water12288.npz")
+    if os.path.exists(gpath):
+        g = np.load(gpath)
+        med = S.config_medium(seed=1)
+        out["water12288_vs_compiled_reference"] = {
+            p: _errs(*run(med, p, BOX_EPS), float(g["energy"]), g["forces"], g["induced"]) for p in ("mixed", "double")}
+    out["bounds"] = "energy_rel <= 1e-6, force_rms_rel <= 2e-5"
+    return out
+
+
+def adjoint_section(stream, world, max_over_ranks, reps):
+    """The differentiation workload: the force-matching loss gradient (one
+    forward and one adjoint, device-resident) on the 4,096-water box, and the
+    same over 256 clusters in one forward and one reverse launch."""
+    import numpy as np
+    import torch
+    from tholedipoleplugin_b200 import _capi as A
+    from tholedipoleplugin_b200 import systems as S
+    from tholedipoleplugin_b200.batch import ClusterBatch
+    from tholedipoleplugin_b200.kernel import CudaCalcTholeDipoleForceKernel
+
+    res = {"workload": "dL/d(q, alpha, thole, mu_mol) of a force loss: one forward + one adjoint (Mutual, "
+                       "one adjoint CG solve) per gradient"}
+    box = S.config_medium(seed=1, target_eps=BOX_EPS)
+    n = box.n
+    rng = np.random.default_rng(1)
+    for prec in ("double", "mixed"):
+        with CudaCalcTholeDipoleForceKernel(box, precision=prec) as k:
+            k.setStream(stream.cuda_stream)
+            pos = torch.tensor(box.positions, dtype=torch.float64, device="cuda")
+            frc = torch.zeros_like(pos)
+            gF = torch.tensor(rng.normal(size=(n, 3)), dtype=torch.float64, device="cuda")
+            grads = torch.empty((n, 6), dtype=torch.float64, device="cuda")
+
+            def one():
+                frc.zero_()
+                k.execute_device(pos.data_ptr(), A.F64, frc.data_ptr(), A.F64)
+                k.adjoint_device(gF.data_ptr(), 0.0, grads.data_ptr())
+
+            one()
+            torch.cuda.synchronize()
+            s0, s1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+            s0.record(stream)
+            for _ in range(reps):
+                one()
+            s1.record(stream)
+            torch.cuda.synchronize()
+            ms = max_over_ranks(s0.elapsed_time(s1) / reps)
+            res[f"box12288_{prec}"] = {"gradients_per_s": _r(world * 1e3 / ms), "ms_per_gradient": _r(ms)}
+    clusters = [c.copy(target_eps=CLUSTER_EPS) for c in _cluster_workload(3)[:256]]
+    for prec in ("double", "mixed"):
+        with ClusterBatch(clusters, precision=prec) as b:
+            b.setStream(stream.cuda_stream)
+            b.compute()
+            pos = torch.tensor(b.positions, dtype=torch.float64, device="cuda")
+            frc = torch.zeros_like(pos)
+            en = torch.zeros(b.num_clusters, dtype=torch.float64, device="cuda")
+            gF = torch.tensor(rng.normal(size=(b.n, 3)), dtype=torch.float64, device="cuda")
+            grads = torch.empty((b.n, 6), dtype=torch.float64, device="cuda")
+
+            def one():
+                b.compute_device(pos.data_ptr(), frc.data_ptr(), en.data_ptr())
+                b.adjoint_device(gF.data_ptr(), 0, grads.data_ptr())
+
+            one()
+            torch.cuda.synchronize()
+            s0, s1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+            s0.record(stream)
+            for _ in range(reps):
+                one()
+            s1.record(stream)
+            torch.cuda.synchronize()
+            ms = max_over_ranks(s0.elapsed_time(s1) / reps)
+            res[f"clusters256_{prec}"] = {"batch_gradients_per_s": _r(world * 1e3 / ms), "ms_per_batch": _r(ms)}
+    return res
+
+
+def run_ours(args):
+    import torch
+
+    from tholedipoleplugin_b200 import systems as S
+    from tholedipoleplugin_b200.kernel import CudaCalcTholeDipoleForceKernel
+    from tholedipoleplugin_b200.md import HostRigidWaterMD
 
     ranks = Ranks("nccl")
     rank, world, local = ranks.rank, ranks.world, ranks.local
     barrier, max_over_ranks = ranks.barrier, ranks.max_over_ranks
 
-    make = {"small": S.config_small, "medium": S.config_medium, "large": S.config_large,
-            "profile": lambda seed: S.water_box(24, 9.936 * 24 / 32, seed=seed, cutoff=0.9)}[args.config]
-    system = make(seed=box_seed(args.config, rank))
+    side, box_nm = BOX[args.config]
+    system = S.water_box(side, box_nm, seed=box_seed(args.config, rank), cutoff=0.9 if box_nm > 2 else 0.8,
+                         target_eps=BOX_EPS)
     n = system.n
     pairs = n * (n - 1) / 2
     K, W = args.steps, args.warmup
     stream = torch.cuda.current_stream()
 
     # ---- mixed form, device-resident MD (the headline) --------------------------------
-    md = DeviceRigidWaterMD(system, precision="mixed", warm_start=True, seed=11 + rank, ewald=args.ewald_md)
-    md.kernel.enableTiming(True)
-    md.step(W)
-    torch.cuda.synchronize()
-    barrier()
-    clocks = Clocks(local)
-    clocks.start()
-    ev0, ev1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
-    mv_ms, mv_n, en_ms, launches, its = 0.0, 0, 0.0, 0, []
-    ev0.record(stream)
-    for _ in range(K):
-        md.step()
-        st = md.kernel.stageTimes()
-        mv_ms += st[7]
-        mv_n += int(st[6])
-        en_ms += st[8]
-        launches += int(st[9]) + 2  # + kick-drift and kick kernels
-        its.append(md.kernel.solverStats()["iterations"])
-    ev1.record(stream)
-    torch.cuda.synchronize()
-    clk = clocks.stop()
-    barrier()
-    t_ms = max_over_ranks(ev0.elapsed_time(ev1))
-    value = world * K / (t_ms * 1e-3) * NS_PER_DAY
-    temperature = md.temperature()
-    md.close()
-    del md
-    torch.cuda.empty_cache()
-
+    m = _md_rate(system, "mixed", K, W, stream, world, barrier, max_over_ranks, rank, ewald=args.ewald_md,
+                 clocks=Clocks(local))
+    value = m["ns_per_day"]
     out = {"metric": "ns/day", "value": value, "unit": "ns/day", "n_gpus": world, "steps": K, "warmup": W,
-           "ms_per_step": t_ms / K, "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
-           "dtype": "f32", "data": "synthetic",
-           "config": {"workload": f"{n}-atom rigid water box ({n // 3} waters, {system.box[0]} nm cubic, "
-                                  + ("Ewald mode: cutoff + smooth PME" if args.ewald_md else "minimum-image all-pairs")
-                                  + ", mutual polarization to 1e-6), velocity Verlet 1 fs, "
-                                  "mixed form (FP32 pair arithmetic, FP64 accumulation/CG)",
-                      "n_atoms": n, "parallelism": f"replicas x{world}",
-                      "l2": "inputs+working set per pass ~ 10 MB (L2-resident); every step re-reads all of it",
-                      "solver": "CG, warm start from the previous step", "cg_iterations_mean": statistics.mean(its)},
-           "gpu_launches": launches, "clocks": clk}
-
+           "ms_per_step": m["t_ms"] / K, "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
+           "dtype": "f32", "data": "synthetic", "gpu_launches": m["launches"],
+           "config": workload_config(args.config, args.ewald_md), "clocks": m["clk"],
+           "solver": {"kind": "CG (Jacobi-preconditioned), warm start from the previous steps",
+                      "cg_iterations_mean_md": _r(statistics.mean(m["its"])),
+                      "matvecs_per_step": _r(m["mv_n"] / K), "parallelism": f"replicas x{world}"}}
     if args.no_extras:
         if rank == 0:
             print(json.dumps(out), flush=True)
@@ -647,144 +800,80 @@ def run_ours(args):
     hmd.close()
     out["e2e"] = {"value": world * K_e2e / t_e2e * NS_PER_DAY, "unit": "ns/day", "h2d_bytes_per_step": n * 3 * 8,
                   "d2h_bytes_per_step": n * 3 * 8 + 8, "steps": K_e2e,
-                  "what": "host velocity Verlet + SHAKE/RATTLE (tdp_md_host_*, host threads); tdp_compute on pinned host positions/forces"}
+                  "what": "host velocity Verlet + SHAKE/RATTLE (tdp_md_host_*); tdp_compute on pinned host "
+                          "positions and forces every step"}
 
     # ---- plain (FP64) form, same MD -------------------------------------------------
     K_pl = max(3, K // 4)
-    pmd = DeviceRigidWaterMD(system, precision="double", warm_start=True, seed=11 + rank)
-    pmd.kernel.enableTiming(True)
-    pmd.step(max(1, W // 2))
-    torch.cuda.synchronize()
-    barrier()
-    pl_mv_ms, pl_mv_n, pl_en_ms = 0.0, 0, 0.0
-    ev0.record(stream)
-    for _ in range(K_pl):
-        pmd.step()
-        st = pmd.kernel.stageTimes()
-        pl_mv_ms += st[7]
-        pl_mv_n += int(st[6])
-        pl_en_ms += st[8]
-    ev1.record(stream)
-    torch.cuda.synchronize()
-    t_pl = max_over_ranks(ev0.elapsed_time(ev1))
-    pmd.close()
-    del pmd
+    pl = _md_rate(system, "double", K_pl, max(1, W // 2), stream, world, barrier, max_over_ranks, rank)
 
-    # ---- SCF solves/s (rotation + permanent field + CG to 1e-6, cold start) ------------
-    def solves_per_s(precision, reps):
-        with CudaCalcTholeDipoleForceKernel(system, precision=precision) as k:
-            k.setStream(stream.cuda_stream)
-            dev_pos = torch.tensor(system.positions, dtype=torch.float64, device="cuda")
-            buf = np.zeros((n, 3))
-            k.solveDevice(dev_pos.data_ptr(), A.F64, buf)
-            torch.cuda.synchronize()
-            s0, s1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
-            s0.record(stream)
-            for _ in range(reps):
-                k.solveDevice(dev_pos.data_ptr(), A.F64, buf)
-            s1.record(stream)
-            torch.cuda.synchronize()
-            return reps / (s0.elapsed_time(s1) * 1e-3), k.solverStats()["iterations"]
-
+    # ---- SCF solves/s (cold start) -------------------------------------------------------
     reps = max(3, K // 4)
-    sps_mixed, it_mixed = solves_per_s("mixed", reps)
-    sps_plain, it_plain = solves_per_s("double", reps)
-    sps_mixed *= world
-    out["plain"] = {"ns_per_day": world * K_pl / (t_pl * 1e-3) * NS_PER_DAY, "ms_per_step": t_pl / K_pl,
-                    "steps": K_pl, "matvec_avg_ms": pl_mv_ms / max(pl_mv_n, 1), "energy_avg_ms": pl_en_ms / K_pl}
-    out["scf_solves_per_s"] = {"mixed": sps_mixed, "plain": world * sps_plain,
-                               "mixed_over_plain": sps_mixed / (world * sps_plain),
-                               "cg_iterations": {"mixed": it_mixed, "plain": it_plain},
-                               "what": "rotation + permanent field + CG to 1e-6 from mu0 = alpha E"}
-    out["md_ns_per_day_mixed_over_plain"] = value / out["plain"]["ns_per_day"]
+    sps_m, it_m = _solves_per_s(system, "mixed", reps, stream, world, max_over_ranks)
+    sps_p, it_p = _solves_per_s(system, "double", reps, stream, world, max_over_ranks)
 
-    # ---- Ewald mode (TDP_FLAG_EWALD): the same box with real-space cutoff + smooth PME ---------
-    out["ewald"] = ewald_section(system, K, W, stream, world, barrier, max_over_ranks, rank)
+    # ---- Ewald mode, cluster batches, adjoint ----------------------------------------------
+    ew = ewald_section(system, K, W, stream, world, barrier, max_over_ranks, rank)
+    cl = run_clusters(args, rank, world, barrier, max_over_ranks, stream)
+    adj = adjoint_section(stream, world, max_over_ranks, max(3, K // 5))
 
-    # ---- cluster batches (1024 NoCutoff clusters of 4-64 waters, one launch) -------------
-    out["clusters"] = run_clusters(args, rank, world, barrier, max_over_ranks, stream)
-
-    # ---- errors (rank 0) ---------------------------------------------------------------
     if rank == 0:
-        errs = {}
-        with CudaCalcTholeDipoleForceKernel(system.copy(target_eps=1e-9, max_iter=500), precision="mixed") as km:
-            em, fm = km.execute(system.positions)
-            mum = km.getInducedDipoles()
-        with CudaCalcTholeDipoleForceKernel(system.copy(target_eps=1e-11, max_iter=500), precision="double") as kp:
-            ep, fp = kp.execute(system.positions)
-            mup = kp.getInducedDipoles()
-        errs["mixed_vs_plain_this_box"] = {"energy_rel": abs(em - ep) / abs(ep), "force_rms_rel": rel_rms(fm, fp),
-                                           "induced_rms_rel": rel_rms(mum, mup)}
-        with CudaCalcTholeDipoleForceKernel(system, precision="mixed") as km6:
-            e6, f6 = km6.execute(system.positions)
-        errs["mixed_eps1e-6_vs_plain_tight_this_box"] = {"energy_rel": abs(e6 - ep) / abs(ep),
-                                                         "force_rms_rel": rel_rms(f6, fp)}
-        from oracle import oracle as O
-        small = S.config_small()
-        ref = O.compute(small.copy(target_eps=1e-12, max_iter=5000), "port")
-        for prec, eps in (("mixed", 1e-9), ("double", 1e-11)):
-            with CudaCalcTholeDipoleForceKernel(small.copy(target_eps=eps, max_iter=2000), precision=prec) as k:
-                e, f = k.execute(small.positions)
-                mu = k.getInducedDipoles()
-            errs[f"{prec}_vs_fp64_oracle_216_waters"] = {"energy_rel": abs(e - ref.energy) / abs(ref.energy),
-                                                        "force_rms_rel": rel_rms(f, ref.forces),
-                                                        "induced_rms_rel": rel_rms(mu, ref.induced)}
-        out["errors"] = errs
-
-        # Reference Jacobi sweeps on this box (GPU Jacobi = the reference loop).
+        errs = _box_errors(system, args.config)
         with CudaCalcTholeDipoleForceKernel(system, precision="double", solver="jacobi") as kj:
             kj.getInducedDipoles(system.positions)
             sweeps = kj.solverStats()["iterations"]
-        out["config"]["reference_jacobi_sweeps"] = sweeps
+        out["solver"]["reference_jacobi_sweeps"] = sweeps
 
-        # ---- roofline --------------------------------------------------------------------
+        # ---- roofline: the dominant kernel of the step -------------------------------------
         peaks = measured_peaks()
         fp32 = fp32_sgemm_tflops(torch)
-        mv_avg = mv_ms / max(mv_n, 1)
-        en_avg = en_ms / K
-        dominant = "energy" if en_ms >= mv_ms else "matvec"
-        if dominant == "energy":
-            flops, avg, bytes_ = pairs * FLOP_ENERGY_PAIR, en_avg, n * BYTES_ENERGY_ATOM
-            kname = "k_energy_sym<float>"
-        else:
-            flops, avg, bytes_ = pairs * FLOP_MATVEC_PAIR, mv_avg, n * BYTES_MATVEC_ATOM
-            kname = "k_field_sym<float,1>"
-        ach = flops / (avg * 1e-3) / 1e12
-        hbm_peak = peaks.get("hbm_gbs", 6650.0)
-        out["roofline"] = {"bound": "fp32", "kernel": kname, "achieved": ach, "peak": fp32, "unit": "TFLOP/s",
-                           "frac": ach / fp32, "traffic": profile_traffic(kname),
-                           "peak_source": "FP32 cuBLAS SGEMM 8192^3 (TF32 off), measured in this run",
-                           "algorithmic": f"{FLOP_ENERGY_PAIR if dominant == 'energy' else FLOP_MATVEC_PAIR} "
-                                          f"FLOP per unordered pair x {pairs:.4g} pairs per launch",
-                           "avg_launch_ms": avg,
-                           "share_of_step": (en_ms if dominant == "energy" else mv_ms) / t_ms}
-        out["roofline_hbm"] = {"bound": "hbm", "kernel": kname, "achieved": bytes_ / (avg * 1e-3) / 1e9,
-                               "peak": hbm_peak, "unit": "GB/s",
-                               "frac": bytes_ / (avg * 1e-3) / 1e9 / hbm_peak,
-                               "peak_source": "MEASURED_PEAKS.json hbm_gbs" if "hbm_gbs" in peaks else "fallback"}
-        # Plain (FP64) form: the same kernels against the FP64 rate (DGEMM measured here) and HBM.
         fp64 = fp64_dgemm_tflops(torch)
-        pmv = out["plain"]["matvec_avg_ms"]
-        pen = out["plain"]["energy_avg_ms"]
-        out["plain"]["roofline"] = {
-            "bound": "fp64", "kernel": "k_field_sym<double,1>",
-            "achieved": pairs * FLOP_MATVEC_PAIR / (pmv * 1e-3) / 1e12, "peak": fp64, "unit": "TFLOP/s",
-            "frac": pairs * FLOP_MATVEC_PAIR / (pmv * 1e-3) / 1e12 / fp64,
-            "peak_source": "FP64 cuBLAS DGEMM 4096^3, measured in this run",
-            "energy_tflops": pairs * FLOP_ENERGY_PAIR / (pen * 1e-3) / 1e12}
-        out["plain"]["roofline_hbm"] = {
-            "bound": "hbm", "kernel": "k_field_sym<double,1>",
-            "achieved": n * BYTES_MATVEC_ATOM_FP64 / (pmv * 1e-3) / 1e9, "peak": hbm_peak, "unit": "GB/s",
-            "frac": n * BYTES_MATVEC_ATOM_FP64 / (pmv * 1e-3) / 1e9 / hbm_peak}
-        out["kernels"] = {"matvec_avg_ms": mv_avg, "matvec_launches": mv_n, "matvec_share": mv_ms / t_ms,
-                          "matvec_tflops": pairs * FLOP_MATVEC_PAIR / (mv_avg * 1e-3) / 1e12,
-                          "energy_avg_ms": en_avg, "energy_share": en_ms / t_ms,
-                          "energy_tflops": pairs * FLOP_ENERGY_PAIR / (en_avg * 1e-3) / 1e12}
-        out["md_temperature_K"] = temperature
-
-        # ---- CPU baseline (N = 1 only) ------------------------------------------------------
-        if world == 1:
-            out["cpu_baseline"] = cpu_baseline_single(n, sweeps)
+        hbm_peak = peaks.get("hbm_gbs", 6650.0)
+        mv_avg = m["mv_ms"] / max(m["mv_n"], 1)
+        en_avg = m["en_ms"] / K
+        mv_tf = pairs * FLOP_MATVEC_PAIR / (mv_avg * 1e-3) / 1e12
+        en_tf = pairs * FLOP_ENERGY_PAIR / (en_avg * 1e-3) / 1e12
+        if m["en_ms"] >= m["mv_ms"]:
+            kname, ach, avg, share, flop = "k_energy_sym<float>", en_tf, en_avg, m["en_ms"] / m["t_ms"], FLOP_ENERGY_PAIR
+            bytes_ = n * BYTES_ENERGY_ATOM
+        else:
+            kname, ach, avg, share, flop = "k_field_sym<float,1>", mv_tf, mv_avg, m["mv_ms"] / m["t_ms"], FLOP_MATVEC_PAIR
+            bytes_ = n * BYTES_MATVEC_ATOM
+        out["roofline"] = {"bound": "fp32", "kernel": kname, "achieved": _r(ach), "peak": _r(fp32), "unit": "TFLOP/s",
+                           "frac": _r(ach / fp32), "traffic": profile_traffic(kname),
+                           "peak_source": "FP32 cuBLAS SGEMM 8192^3 (TF32 off), measured in this run",
+                           "algorithmic": f"{flop} FLOP per unordered pair (the reference's operation sequence) x "
+                                          f"{pairs:.4g} pairs per launch",
+                           "avg_launch_ms": _r(avg), "share_of_step": _r(share)}
+        out["roofline_hbm"] = {"bound": "hbm", "kernel": kname, "achieved": _r(bytes_ / (avg * 1e-3) / 1e9),
+                               "peak": hbm_peak, "unit": "GB/s", "frac": _r(bytes_ / (avg * 1e-3) / 1e9 / hbm_peak),
+                               "peak_source": "MEASURED_PEAKS.json hbm_gbs" if "hbm_gbs" in peaks else "fallback"}
+        pmv = pl["mv_ms"] / max(pl["mv_n"], 1)
+        pen = pl["en_ms"] / K_pl
+        out["kernels"] = {
+            "mixed": {"matvec_ms": _r(mv_avg), "matvec_tflops": _r(mv_tf), "matvec_share": _r(m["mv_ms"] / m["t_ms"]),
+                      "energy_ms": _r(en_avg), "energy_tflops": _r(en_tf), "energy_share": _r(m["en_ms"] / m["t_ms"]),
+                      "permanent_field_stage_ms": _r(m["fix_ms"] / K), "fp32_peak_tflops": _r(fp32)},
+            "plain": {"matvec_ms": _r(pmv), "matvec_tflops": _r(pairs * FLOP_MATVEC_PAIR / (pmv * 1e-3) / 1e12),
+                      "energy_ms": _r(pen), "energy_tflops": _r(pairs * FLOP_ENERGY_PAIR / (pen * 1e-3) / 1e12),
+                      "fp64_peak_tflops": _r(fp64)}}
+        out["ewald"] = ew
+        out["clusters"] = cl
+        out["adjoint"] = adj
+        out["md_temperature_K"] = _r(m["temperature"])
+        cpu = cpu_baseline_single(n, sweeps) if world == 1 else None
+        if cpu is not None:
+            out["cpu_baseline"] = {k: (_r(v) if isinstance(v, float) else v) for k, v in cpu.items()}
+        # The headline figures last, where a truncated record keeps them.
+        out["plain"] = {"ns_per_day": _r(pl["ns_per_day"]), "ms_per_step": _r(pl["t_ms"] / K_pl),
+                        "md_mixed_over_plain": _r(value / pl["ns_per_day"])}
+        out["scf_solves_per_s"] = {"mixed": _r(sps_m), "plain": _r(sps_p), "mixed_over_plain": _r(sps_m / sps_p),
+                                   "cg_iterations": {"mixed": it_m, "plain": it_p},
+                                   "what": f"cold start (mu = alpha E) to {BOX_EPS:g}: rotation, permanent field, CG"}
+        if cpu is not None:
+            out["scf_solves_per_s"]["reference_1core_solve_s"] = _r(cpu["solve_seconds"])
+            out["scf_solves_per_s"]["mixed_speedup_vs_reference_1core"] = _r(sps_m * cpu["solve_seconds"])
+        out["errors"] = errs
         print(json.dumps(out), flush=True)
     barrier()
     ranks.close()
