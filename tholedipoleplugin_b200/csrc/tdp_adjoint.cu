@@ -28,26 +28,44 @@
 // one atom's multipoles is the pair function evaluated with those multipoles
 // set to unit vectors; the Thole-factor derivative flows through the damping
 // factors and is taken with a one-direction dual number.  Damping terms are
-// recomputed in every pass rather than stored.  Every pair is visited from
-// both atoms (each thread owns one atom), so no atomics are needed.
+// recomputed in every pass rather than stored.  Pairs beyond the damping
+// range with unit scales (nearly all of a box) take the closed-form lab-frame
+// VJP (pair_vjp_lab), a few times cheaper.  Every pair is visited from both
+// atoms (each atom owns kLanes threads), so no atomics are needed.
 #include "tdp_adjoint.cuh"
 
 namespace tdp {
 namespace adj {
 
+// The per-atom reductions below give each atom kLanes consecutive threads:
+// lane l visits partners j = l, l + kLanes, ..., and the lanes' sums are
+// combined by a fixed xor-shuffle tree, so results do not depend on timing.
+constexpr int kLanes = 8;
+
+__device__ __forceinline__ double lane_sum(double v) {
+#pragma unroll
+    for (int o = kLanes / 2; o > 0; o >>= 1) v += __shfl_xor_sync(0xffffffffu, v, o, kLanes);
+    return v;
+}
+
 // a = d/d(q, lab, mu, t) of gE*E_pair + g.F_pair + gT.tau, per atom.  out: n*8.
 __global__ void k_pair_vjp(PairParams P, AtomData A, const double* __restrict__ g, const double* __restrict__ gT,
                            double gE, const int* __restrict__ exc_off, const int* __restrict__ exc_j,
                            const double* __restrict__ exc_m, const double* __restrict__ exc_s, double* __restrict__ out) {
-    int me = blockIdx.x * blockDim.x + threadIdx.x;
-    if (me >= P.n) return;
+    const int t = blockIdx.x * blockDim.x + threadIdx.x;
+    const int me = t / kLanes, l = t % kLanes;
+    const bool act = me < P.n;
     double acc[8] = {0, 0, 0, 0, 0, 0, 0, 0};
-    for (int j = 0; j < P.n; j++)
-        if (j != me) visit_pair(P, A, g, gT, gE, me, j, 1.0, 1.0, acc);
-    // Covalent scales: the pair function is linear in (mScale, iScale).
-    for (int e = exc_off[me]; e < exc_off[me + 1]; e++)
-        visit_pair(P, A, g, gT, gE, me, exc_j[e], exc_m[e] - 1.0, exc_s[e] - 1.0, acc);
-    for (int k = 0; k < 8; k++) out[8 * me + k] = acc[k];
+    if (act) {
+        for (int j = l; j < P.n; j += kLanes)
+            if (j != me) visit_pair(P, A, g, gT, gE, me, j, 1.0, 1.0, acc);
+        // Covalent scales: the pair function is linear in (mScale, iScale).
+        for (int e = exc_off[me] + l; e < exc_off[me + 1]; e += kLanes)
+            visit_pair(P, A, g, gT, gE, me, exc_j[e], exc_m[e] - 1.0, exc_s[e] - 1.0, acc);
+    }
+    for (int k = 0; k < 8; k++) acc[k] = lane_sum(acc[k]);
+    if (act && l == 0)
+        for (int k = 0; k < 8; k++) out[8 * me + k] = acc[k];
 }
 
 // b = d/d(q, lab, t) of lambda . Efix, per atom (out: n*5).  Field at i due to
@@ -55,26 +73,37 @@ __global__ void k_pair_vjp(PairParams P, AtomData A, const double* __restrict__ 
 // d = p_k - p_i.
 __global__ void k_fixed_vjp(PairParams P, AtomData A, const double* __restrict__ lam, const int* __restrict__ exc_off,
                             const int* __restrict__ exc_j, const double* __restrict__ exc_m, double* __restrict__ out) {
-    int k = blockIdx.x * blockDim.x + threadIdx.x;
-    if (k >= P.n) return;
+    const int t = blockIdx.x * blockDim.x + threadIdx.x;
+    const int k = t / kLanes, l = t % kLanes;
+    const bool act = k < P.n;
     double acc[5] = {0, 0, 0, 0, 0};
-    for (int i = 0; i < P.n; i++)
-        if (i != k) fixed_vjp_visit(P, A, lam, k, i, 1.0, acc);
-    for (int e = exc_off[k]; e < exc_off[k + 1]; e++) fixed_vjp_visit(P, A, lam, k, exc_j[e], exc_m[e] - 1.0, acc);
-    for (int c = 0; c < 5; c++) out[5 * k + c] = acc[c];
+    if (act) {
+        for (int i = l; i < P.n; i += kLanes)
+            if (i != k) fixed_vjp_visit(P, A, lam, k, i, 1.0, acc);
+        for (int e = exc_off[k] + l; e < exc_off[k + 1]; e += kLanes)
+            fixed_vjp_visit(P, A, lam, k, exc_j[e], exc_m[e] - 1.0, acc);
+    }
+    for (int c = 0; c < 5; c++) acc[c] = lane_sum(acc[c]);
+    if (act && l == 0)
+        for (int c = 0; c < 5; c++) out[5 * k + c] = acc[c];
 }
 
 // c_t = d/dt_k of lambda^T T(t) mu (RTDF.cpp:766-818), per atom.
 __global__ void k_matvec_t_vjp(PairParams P, AtomData A, const double* __restrict__ lam,
                                const int* __restrict__ exc_off, const int* __restrict__ exc_j,
                                const double* __restrict__ exc_s, double* __restrict__ out, int accumulate) {
-    int k = blockIdx.x * blockDim.x + threadIdx.x;
-    if (k >= P.n) return;
+    const int t = blockIdx.x * blockDim.x + threadIdx.x;
+    const int k = t / kLanes, l = t % kLanes;
+    const bool act = k < P.n;
     double acc = 0.0;
-    for (int j = 0; j < P.n; j++)
-        if (j != k) acc += matvec_t_visit(P, A, lam, k, j, 1.0);
-    for (int e = exc_off[k]; e < exc_off[k + 1]; e++) acc += matvec_t_visit(P, A, lam, k, exc_j[e], exc_s[e] - 1.0);
-    out[k] = accumulate ? out[k] + acc : acc;
+    if (act) {
+        for (int j = l; j < P.n; j += kLanes)
+            if (j != k) acc += matvec_t_visit(P, A, lam, k, j, 1.0);
+        for (int e = exc_off[k] + l; e < exc_off[k + 1]; e += kLanes)
+            acc += matvec_t_visit(P, A, lam, k, exc_j[e], exc_s[e] - 1.0);
+    }
+    acc = lane_sum(acc);
+    if (act && l == 0) out[k] = accumulate ? out[k] + acc : acc;
 }
 
 }  // namespace adj
@@ -210,11 +239,11 @@ static inline int nb(int n) { return (n + 127) / 128; }
 
 void launch_adjoint_pair(const Dev& d, const double* g, const double* gT, double gE, double* a8, cudaStream_t st) {
     adj::AtomData A{d.pos, d.charge, d.lab, d.mu, d.thole, d.yz};
-    adj::k_pair_vjp<<<nb(d.n), 128, 0, st>>>(d.pp, A, g, gT, gE, d.exc_off, d.exc_j, d.exc_m, d.exc_s, a8);
+    adj::k_pair_vjp<<<nb(d.n * adj::kLanes), 128, 0, st>>>(d.pp, A, g, gT, gE, d.exc_off, d.exc_j, d.exc_m, d.exc_s, a8);
 }
 void launch_adjoint_fixed(const Dev& d, const double* lam, double* b5, cudaStream_t st) {
     adj::AtomData A{d.pos, d.charge, d.lab, d.mu, d.thole, d.yz};
-    adj::k_fixed_vjp<<<nb(d.n), 128, 0, st>>>(d.pp, A, lam, d.exc_off, d.exc_j, d.exc_m, b5);
+    adj::k_fixed_vjp<<<nb(d.n * adj::kLanes), 128, 0, st>>>(d.pp, A, lam, d.exc_off, d.exc_j, d.exc_m, b5);
 }
 void launch_adjoint_matvec_t(const Dev& d, const double* lam, double* ct, cudaStream_t st) {
     launch_adjoint_matvec_t_mu(d, lam, d.mu, ct, false, st);
@@ -222,7 +251,7 @@ void launch_adjoint_matvec_t(const Dev& d, const double* lam, double* ct, cudaSt
 void launch_adjoint_matvec_t_mu(const Dev& d, const double* lam, const double* mu, double* ct, bool accumulate,
                                 cudaStream_t st) {
     adj::AtomData A{d.pos, d.charge, d.lab, mu, d.thole, d.yz};
-    adj::k_matvec_t_vjp<<<nb(d.n), 128, 0, st>>>(d.pp, A, lam, d.exc_off, d.exc_j, d.exc_s, ct, accumulate ? 1 : 0);
+    adj::k_matvec_t_vjp<<<nb(d.n * adj::kLanes), 128, 0, st>>>(d.pp, A, lam, d.exc_off, d.exc_j, d.exc_s, ct, accumulate ? 1 : 0);
 }
 
 __global__ void k_lincomb(int n3, double ca, const double* __restrict__ a, double cb, const double* __restrict__ b,

@@ -250,6 +250,89 @@ struct AtomData {
 };
 
 // Visits pair (me, j) with scales (mS, iS); accumulates d l / d(my q, lab, mu, t).
+__device__ __forceinline__ V3 cross3(V3 a, V3 b) {
+    return {a.y * b.z - a.z * b.y, a.z * b.x - a.x * b.z, a.x * b.y - a.y * b.x};
+}
+__device__ __forceinline__ double dot3(V3 a, V3 b) { return a.x * b.x + a.y * b.y + a.z * b.z; }
+__device__ __forceinline__ V3 axpy(double a, V3 x, V3 y) { return {a * x.x + y.x, a * x.y + y.y, a * x.z + y.z}; }
+__device__ __forceinline__ V3 scl(double a, V3 x) { return {a * x.x, a * x.y, a * x.z}; }
+__device__ __forceinline__ V3 add3(V3 a, V3 b) { return {a.x + b.x, a.y + b.y, a.z + b.z}; }
+__device__ __forceinline__ V3 sub3v(V3 a, V3 b) { return {a.x - b.x, a.y - b.y, a.z - b.z}; }
+// Transpose of the permuted back rotation: a . perm(v) = permT(a) . v with
+// perm(v) = (v_y, v_z, v_x).
+__device__ __forceinline__ V3 permT(V3 a) { return {a.z, a.x, a.y}; }
+
+// Closed-form VJP of the pair routine for a pair that Thole damping does not
+// reach, with unit scales and rInvVec[4] = 0: the derivatives of
+//   l = gE e + gF_I . F_I + gF_K . F_K + gT_I . tau_I + gT_K . tau_K
+// with respect to one side's (q, m_lab, mu_ind), from the lab-frame form of
+// the routine (pair_energy_lab in tdp_pairs.cuh).  With c = permT(gF_K - gF_I),
+// D = (X x c)/r, G_side = D - permT(gT_side), tau_s = G_s x m_s,
+// sigma_s = D x u_s, kap = 1 (Mutual) or -1, the loss is bilinear in the two
+// sides' multipoles and its gradient is written out term by term below.  The
+// Thole factors do not enter (their derivative is 0 here).  out[0..6]: dq,
+// dm_lab[3], du[3] of side I (side_I) or side K.
+__device__ __forceinline__ void pair_vjp_lab(V3 d, double qI, V3 mI, V3 uI, double qK, V3 mK, V3 uK, double kap,
+                                             double gE, V3 gFI, V3 gFK, V3 gTI, V3 gTK, bool side_I, double* out) {
+    const double r2 = dot3(d, d), rinv = 1.0 / sqrt(r2), rv2 = rinv * rinv, rv3 = rv2 * rinv;
+    const double rho2 = d.y * d.y + d.z * d.z;
+    const double xs = rinv / sqrt(rho2);
+    const V3 X = {rho2 * xs, -d.x * d.y * xs, -d.x * d.z * xs};
+    const V3 PI = add3(mI, uI), PK = add3(mK, uK);
+    const double QI1 = dot3(X, mI), UI0 = dot3(X, uI), QK1 = dot3(X, mK), UK0 = dot3(X, uK);
+    const double PI0 = QI1 + UI0, PK0 = QK1 + UK0;
+    const V3 cf = permT(sub3v(gFK, gFI));
+    const V3 D = scl(rinv, cross3(X, cf));
+    const double cX = dot3(cf, X);
+    const double w = 1.0 + kap;   // dW/du
+    if (side_I) {
+        const V3 GI = sub3v(D, permT(gTI)), GK = sub3v(D, permT(gTK));
+        const V3 tauK = cross3(GK, mK), sigK = cross3(D, uK);
+        const V3 WK = axpy(kap, uK, PK);
+        const double WK0 = PK0 + kap * UK0;
+        const V3 Vij = axpy(rv2 * qK - 3.0 * rv3 * PK0, X, scl(rv3, PK));
+        const V3 Vdij = axpy(rv2 * qK - 3.0 * rv3 * WK0, X, scl(rv3, WK));
+        const V3 t2 = axpy(-3.0 * rv3 * dot3(X, tauK), X, scl(rv3, tauK));
+        const V3 t4 = axpy(-3.0 * rv3 * dot3(X, sigK), X, scl(rv3, sigK));
+        const double c5 = 2.0 * rv3 * cX * qK;
+        // Energy partials.
+        const double de_q = rinv * qK - 0.5 * rv2 * (PK0 + QK1);
+        const V3 de_m = axpy(rv2 * qK - 1.5 * rv3 * (PK0 + QK1), X, scl(0.5 * rv3, add3(PK, mK)));
+        const V3 de_u = axpy(0.5 * rv2 * qK - 1.5 * rv3 * QK1, X, scl(0.5 * rv3, mK));
+        out[0] = gE * de_q - rv2 * (dot3(X, tauK) + dot3(X, sigK)) + cX * (rv2 * qK - 2.0 * rv3 * PK0);
+        const V3 gm = add3(add3(scl(gE, de_m), cross3(Vij, GI)), axpy(c5, X, add3(t2, t4)));
+        const V3 gu = add3(add3(scl(gE, de_u), cross3(Vdij, D)), axpy(c5, X, axpy(w, t4, t2)));
+        out[1] = gm.x;
+        out[2] = gm.y;
+        out[3] = gm.z;
+        out[4] = gu.x;
+        out[5] = gu.y;
+        out[6] = gu.z;
+    } else {
+        const V3 GI = sub3v(D, permT(gTI)), GK = sub3v(D, permT(gTK));
+        const V3 tauI = cross3(GI, mI), sigI = cross3(D, uI);
+        const V3 WI = axpy(kap, uI, PI);
+        const double WI0 = PI0 + kap * UI0;
+        const V3 Vji = axpy(-rv2 * qI - 3.0 * rv3 * PI0, X, scl(rv3, PI));
+        const V3 Vdji = axpy(-rv2 * qI - 3.0 * rv3 * WI0, X, scl(rv3, WI));
+        const V3 t1 = axpy(-3.0 * rv3 * dot3(X, tauI), X, scl(rv3, tauI));
+        const V3 t3 = axpy(-3.0 * rv3 * dot3(X, sigI), X, scl(rv3, sigI));
+        const double c5 = -2.0 * rv3 * cX * qI;
+        const double de_q = rinv * qI + 0.5 * rv2 * (PI0 + QI1);
+        const V3 de_m = axpy(-rv2 * qI - 1.5 * rv3 * (PI0 + QI1), X, scl(0.5 * rv3, add3(PI, mI)));
+        const V3 de_u = axpy(-0.5 * rv2 * qI - 1.5 * rv3 * QI1, X, scl(0.5 * rv3, mI));
+        out[0] = gE * de_q + rv2 * (dot3(X, tauI) + dot3(X, sigI)) + cX * (rv2 * qI + 2.0 * rv3 * PI0);
+        const V3 gm = add3(add3(scl(gE, de_m), cross3(Vji, GK)), axpy(c5, X, add3(t1, t3)));
+        const V3 gu = add3(add3(scl(gE, de_u), cross3(Vdji, D)), axpy(c5, X, axpy(w, t3, t1)));
+        out[1] = gm.x;
+        out[2] = gm.y;
+        out[3] = gm.z;
+        out[4] = gu.x;
+        out[5] = gu.y;
+        out[6] = gu.z;
+    }
+}
+
 __device__ inline void visit_pair(const PairParams& P, const AtomData& A, const double* g, const double* gT, double gE,
                            int me, int j, double mS, double iS, double* acc) {
     const bool meI = me < j;
@@ -266,6 +349,16 @@ __device__ inline void visit_pair(const PairParams& P, const AtomData& A, const 
     V3 gFI = ld(g + 3 * I), gFK = ld(g + 3 * K), gTI = ld(gT + 3 * I), gTK = ld(gT + 3 * K);
     const double rv4p = P.rinv4_power, rv4f = P.rinv4_fill;
     const double damp_r2 = P.damp_r2 == 0.0f ? 0.0 : (double)P.damp_r2;
+    const double r2 = d.x * d.x + d.y * d.y + d.z * d.z;
+    if (mS == 1.0 && iS == 1.0 && rv4p == 0.0 && rv4f == 0.0 && !(r2 < damp_r2) && yzd &&
+        d.y * d.y + d.z * d.z > 0.0) {
+        // Beyond the damping range: the closed-form lab-frame VJP (Thole derivative 0).
+        double o[7];
+        pair_vjp_lab(d, A.q[I], ld(A.lab + 3 * I), ld(A.mu + 3 * I), A.q[K], ld(A.lab + 3 * K), ld(A.mu + 3 * K),
+                     P.mutual ? 1.0 : -1.0, gE, gFI, gFK, gTI, gTK, meI, o);
+        for (int a = 0; a < 7; a++) acc[a] += o[a];
+        return;
+    }
     // Multipole derivatives: the pair function with my multipoles set to unit vectors.
     double oq = A.q[meI ? K : I];
     double om[3] = {A.lab[3 * (meI ? K : I)], A.lab[3 * (meI ? K : I) + 1], A.lab[3 * (meI ? K : I) + 2]};
@@ -326,7 +419,8 @@ __device__ __forceinline__ void fixed_vjp_visit(const PairParams& P, const AtomD
     acc[1] += m * (rr5 * ldd * d.x - rr3 * li.x);
     acc[2] += m * (rr5 * ldd * d.y - rr3 * li.y);
     acc[3] += m * (rr5 * ldd * d.z - rr3 * li.z);
-    // t_k enters f_ik and f_ki: dual number on t_k.
+    // t_k enters f_ik and f_ki (only within the damping range): dual number on t_k.
+    if (!(r2 < damp_r2)) return;
     V3 dn = {-d.x, -d.y, -d.z};
     Dual tk = mk(A.thole[k], 1.0), ti = mk(A.thole[i]);
     Dual s1 = lam_dot_field<Dual>(d, r, r2, damp_r2, ti, tk, A.q[k], labk, li, m);
