@@ -165,3 +165,33 @@ def test_warm_start_predictor(precision):
     # the constant guess of call 2, which needs fewer than a cold start.
     assert warm_it[1] < cold_it[1], (warm_it, cold_it)
     assert max(warm_it[2:]) < warm_it[1], (warm_it, cold_it)
+
+
+@pytest.mark.parametrize("precision", ["double", "mixed"])
+@pytest.mark.parametrize("method", [S.PME, S.NO_CUTOFF])
+def test_fused_warm_start_matches_separate_walks(precision, method, monkeypatch):
+    """A warm-started solve starts with one walk over the operand m + mu0
+    (E + T mu0 in one pass; covalent partners split into their M and I
+    scales).  Along a short trajectory it must give the results of the
+    separate permanent-field walk and starting matvec (TDP_FUSED_START=0) to
+    the solver tolerance, and the adjoint after such a solve must match a
+    cold one."""
+    base = S.water_box(5, 1.6 if method == S.PME else 1.55, seed=77, cutoff=0.7, method=method)
+    s = base.copy(target_eps=1e-11 if precision == "double" else 1e-9, max_iter=2000)
+    rng = np.random.default_rng(3)
+    traj = [s.positions + 0.002 * k * rng.normal(size=s.positions.shape) for k in range(4)]
+    out = {}
+    for fused in ("1", "0"):
+        monkeypatch.setenv("TDP_FUSED_START", fused)
+        with CudaCalcTholeDipoleForceKernel(s, precision=precision, warm_start=True) as k:
+            res = [k.execute(p) for p in traj]
+            out[fused] = (res, k.getInducedDipoles(), k.adjoint(np.ones((s.n, 3)), 0.5))
+    te, tf = (1e-9, 1e-8) if precision == "double" else (1e-6, 2e-5)
+    for (e1, f1), (e0, f0) in zip(out["1"][0], out["0"][0]):
+        assert rel_err(e1, e0) < te and rel_rms(f1, f0) < tf
+    assert rel_rms(out["1"][1], out["0"][1]) < tf
+    g1, g0 = out["1"][2], out["0"][2]
+    for c in range(6):
+        assert np.abs(g1[:, c] - g0[:, c]).max() <= (1e-7 if precision == "double" else 1e-4) * np.abs(g0[:, c]).max()
+    ref = O.compute(s.copy(positions=traj[-1], target_eps=1e-12, max_iter=5000), "port")
+    assert rel_err(out["1"][0][-1][0], ref.energy) < te

@@ -1013,7 +1013,9 @@ __global__ void __launch_bounds__(512) k_batch_adjoint(BatchArgs A, AdjArgs G) {
                 set_vec(c, i, c.mu[3 * i], c.mu[3 * i + 1], c.mu[3 * i + 2]);
             }
             __syncthreads();
-            const double target = fmax(sqrt(s2 / n) * 1e-12, 1e-300);
+            // 1e-12 of the right-hand side's scale in FP64; 1e-6 in the mixed
+            // form, whose true residual is limited by the FP32 matvec near 1e-7.
+            const double target = fmax(sqrt(s2 / n) * (sizeof(R) == 8 ? 1e-12 : 1e-6), 1e-300);
             eps = 1.0e50;
             cluster_cg(c, n, A.lmax, damp_r2, target, A.max_iter > 1000 ? A.max_iter : 1000, it, eps);
             __syncthreads();

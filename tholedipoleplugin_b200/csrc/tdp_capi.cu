@@ -73,6 +73,10 @@ struct tdp_handle {
     size_t stage_bytes = 0;
     bool mu_prev_valid = false;
     bool mu_prev2_valid = false;
+    // Warm-started Mutual solves start with one walk that gives E + T mu0
+    // (TDP_FUSED_START=0 keeps the separate permanent-field walk and matvec).
+    bool fused_start = true;
+    bool e_shifted = false;   // the last solve started fused: d.E holds E + T mu0, d.mu0 holds mu0
     bool have_results = false;
 
     int iterations = 0;
@@ -457,15 +461,24 @@ void matvec(tdp_handle* h) {
 // reference's Jacobi fixed point mu = alpha (E + T mu).  The stopping test is
 // the reference's epsilon: the RMS change a Jacobi step would make,
 // sqrt(sum alpha |r|^2 / N), confirmed on the true residual before returning.
+//
+// fused: the start of a warm-started solve whose single field walk left
+// E' = E + T mu0 in d.E (mu0 in d.mu0).  The starting residual then needs no
+// matvec, and the final check's matvec runs on mu - mu0:
+// E + T mu = E' + T (mu - mu0).
 template <class R>
-void solve_cg(tdp_handle* h) {
+void solve_cg(tdp_handle* h, bool fused = false) {
     Dev& d = h->d;
     cudaStream_t st = h->stream;
     const int cap = h->max_iter;
     int slot = 0;
     // Residual of the starting point (mu = alpha E, or the previous solution).
-    matvec<R>(h);
-    launch_cg_residual<R>(d, st);
+    if (fused) {
+        launch_cg_residual<R>(d, st, false);
+    } else {
+        matvec<R>(h);
+        launch_cg_residual<R>(d, st);
+    }
     launch_cg_p<R>(d, -1, slot, st);
     h->launches += 2;
     double eps = read_scalar(h, d.scal_eps + slot);
@@ -479,7 +492,7 @@ void solve_cg(tdp_handle* h) {
         }
         if (eps <= h->target_eps || it >= cap || (size_t)slot + 3 >= h->nscal) {
             if (!is_true) {
-                launch_cg_mu<R>(d, st);
+                launch_cg_mu<R>(d, st, fused ? d.mu0 : nullptr);
                 matvec<R>(h);
                 launch_cg_residual<R>(d, st);
                 launch_cg_p<R>(d, -1, ++slot, st);
@@ -566,16 +579,21 @@ void setup_and_solve(tdp_handle* h) {
     launch_pack<R>(d, st);
     launch_rotate<R>(d, st);
     record(h, 1);
+    // A warm-started Mutual CG solve takes the fused start: one walk with the
+    // operand m + mu0 gives E + T mu0 (see solve_cg).
+    const bool fused = h->polarization == TDP_MUTUAL && h->solver == TDP_SOLVER_CG &&
+                       (h->flags & TDP_FLAG_WARM_START) && h->mu_prev_valid && !h->ew && h->fused_start && d.mu0;
+    h->e_shifted = false;
     if (h->ew) {
         const double L[3] = {h->box[0], h->box[4], h->box[8]};
         ewald_prepare(h->ew, d, L, h->cutoff, h->ewald_tol, h->pme_alpha, h->pme_grid, st);
         ewald_fixed_field<R>(h->ew, d, st);
         h->launches += 3 + ewald_last_launches(h->ew);
-    } else {
+    } else if (!fused) {
         launch_field<R>(d, 0, st);
         h->launches += 4;
     }
-    launch_fixed_done<R>(d, st);
+    if (!fused) launch_fixed_done<R>(d, st);
     record(h, 2);
     if (h->polarization == TDP_DIRECT) {
         h->iterations = 0;
@@ -595,10 +613,22 @@ void setup_and_solve(tdp_handle* h) {
                     TDP_CUDA(cudaMemcpyAsync(d.mu, d.mu_prev, sizeof(double) * 3 * h->n, cudaMemcpyDeviceToDevice,
                                              st));
                 }
-                launch_warm_start<R>(d, st);
+                if (fused) {
+                    TDP_CUDA(cudaMemcpyAsync(d.mu0, d.mu, sizeof(double) * 3 * h->n, cudaMemcpyDeviceToDevice, st));
+                    launch_pack_total<R>(d, st);
+                    size_t k = kernel_begin(h, 0);
+                    launch_field<R>(d, 2, st);
+                    kernel_end(h, k);
+                    h->matvecs++;
+                    launch_fused_done<R>(d, st);
+                    h->launches += 4 + (sizeof(R) == 4 ? 1 : 0);
+                    h->e_shifted = true;
+                } else {
+                    launch_warm_start<R>(d, st);
+                }
                 h->launches += h->mu_prev2_valid ? 2 : 1;
             }
-            solve_cg<R>(h);
+            solve_cg<R>(h, fused);
         }
         const bool ok = h->status == TDP_STATUS_CONVERGED;
         std::swap(d.mu_prev, d.mu_prev2);
@@ -729,7 +759,9 @@ void run_adjoint(tdp_handle* h, const double* g_in, double gE, double* out_dst, 
     launch_adjoint_split(d, a8, nullptr, amu, nullptr, st);
     if (h->polarization == TDP_MUTUAL) {
         // One solve of the same symmetric system: A lambda = a_mu.  Target:
-        // 1e-12 of the RMS of alpha * a_mu (the solver's Jacobi-step units).
+        // 1e-12 (FP64 form) or 1e-6 (mixed form, whose true residual is
+        // itself limited by the FP32 matvec near 1e-7) of the RMS of
+        // alpha * a_mu (the solver's Jacobi-step units).
         double* ps = pstat(h);
         k_alpha_norm2<<<1, 1024, 0, st>>>(n, d.alpha, amu, ps);
         const double s2 = read_scalar(h, ps);
@@ -737,7 +769,7 @@ void run_adjoint(tdp_handle* h, const double* g_in, double gE, double* out_dst, 
         int it0 = h->iterations, conv0 = h->converged, st0 = h->status, mv0 = h->matvecs;
         double eps0 = h->epsilon, tgt0 = h->target_eps;
         int cap0 = h->max_iter;
-        h->target_eps = std::max(rms * 1e-12, 1e-300);
+        h->target_eps = std::max(rms * (h->precision == TDP_PRECISION_DOUBLE ? 1e-12 : 1e-6), 1e-300);
         h->max_iter = std::max(cap0, 1000);
         launch_rhs_init<R>(d, amu, st);
         solve_cg<R>(h);
@@ -758,7 +790,13 @@ void run_adjoint(tdp_handle* h, const double* g_in, double gE, double* out_dst, 
         launch_set_operand<R>(d, lam, st);
         launch_field<R>(d, 1, st);
         launch_add_field(d, amu, amu_tlam, st);
-        launch_set_operand<R>(d, mu_fwd, st);
+        if (h->e_shifted) {
+            // E_fwd holds E + T mu0: E + T mu = E_fwd + T (mu - mu0) (glab as scratch).
+            launch_lincomb(n, 1.0, mu_fwd, -1.0, d.mu0, glab, st);
+            launch_set_operand<R>(d, glab, st);
+        } else {
+            launch_set_operand<R>(d, mu_fwd, st);
+        }
         launch_field<R>(d, 1, st);
         launch_add_field(d, E_fwd, e_tmu, st);
     } else if (h->polarization == TDP_EXTRAPOLATED) {
@@ -1035,6 +1073,7 @@ int tdp_create(const tdp_system_desc* desc, tdp_handle** out) {
         d.mu = dalloc<double>(n3, o);
         d.mu_prev = dalloc<double>(n3, o);
         d.mu_prev2 = dalloc<double>(n3, o);
+        d.mu0 = dalloc<double>(n3, o);
         d.y = dalloc<double>(n3, o);
         d.r = dalloc<double>(n3, o);
         d.p = dalloc<double>(n3, o);
@@ -1069,6 +1108,8 @@ int tdp_create(const tdp_system_desc* desc, tdp_handle** out) {
         h->n_exc = ej.size();
         build_components(h, desc);
         if (const char* e = getenv("TDP_RESORT_INTERVAL")) h->resort_interval = std::max(1, atoi(e));
+        if (const char* e = getenv("TDP_FUSED_START"))
+            if (atoi(e) == 0) h->fused_start = false;
         d.order = dalloc<int>(d.n_pad, o);
         d.rank = dalloc<int>(n, o);
         d.pos_s = dalloc<double>(3 * (size_t)d.n_pad, o);

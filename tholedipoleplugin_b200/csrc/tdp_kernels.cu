@@ -226,19 +226,49 @@ __global__ void k_predict(size_t n3, const double* __restrict__ mu1, const doubl
     if (k < n3) mu[k] = 2.0 * mu1[k] - mu2[k];
 }
 
+// Start of a fused warm start: the operand records carry m + mu0 (mu0 in mu),
+// so one permanent-field walk gives E + T mu0 for unit-scale pairs.
+template <class R>
+__global__ void k_pack_total(int n, const int* __restrict__ rank, const double* __restrict__ lab,
+                             const double* __restrict__ mu, const double* __restrict__ thole,
+                             typename Vec4T<R>::type* __restrict__ vec) {
+    int i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= n) return;
+    store_vec<R>(vec, rank[i], ld3(lab + 3 * i) + ld3(mu + 3 * i), thole[i]);
+}
+
+// E := E_fixed + T mu0 (the fused walk's partial sums); y = mu0 / sqrt(alpha).
+__global__ void k_fused_done(int n, const int* __restrict__ rank, int nsplit, int n_pad,
+                             const double* __restrict__ partial, const double* __restrict__ salpha,
+                             const double* __restrict__ mu, double* __restrict__ E, double* __restrict__ y) {
+    int i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= n) return;
+    d3 e = sum_partial3(partial, nsplit, n_pad, rank[i]);
+    E[3 * i] = e.x;
+    E[3 * i + 1] = e.y;
+    E[3 * i + 2] = e.z;
+    d3 m = ld3(mu + 3 * i);
+    double s = salpha[i];
+    d3 yy = s > 0.0 ? m * (1.0 / s) : d3{0.0, 0.0, 0.0};
+    y[3 * i] = yy.x;
+    y[3 * i + 1] = yy.y;
+    y[3 * i + 2] = yy.z;
+}
+
 // True residual in y-space: r = sqrt(alpha)*(E + T mu) - y, with mu = sqrt(alpha)*y.
 // p = r, packs sqrt(alpha)*p; block partials of r.r and sum alpha|r|^2.
+// use_partial = 0: the field term is already included in E.
 template <class R>
 __global__ void k_cg_residual(int n, const int* __restrict__ rank, int nsplit, int n_pad, const double* __restrict__ partial,
                               const double* __restrict__ E, const double* __restrict__ salpha,
                               const double* __restrict__ thole, const double* __restrict__ y, double* __restrict__ r,
                               double* __restrict__ p, typename Vec4T<R>::type* __restrict__ vec,
-                              double* __restrict__ rr_part, double* __restrict__ eps_part) {
+                              double* __restrict__ rr_part, double* __restrict__ eps_part, int use_partial) {
     __shared__ double red[40];
     int i = blockIdx.x * blockDim.x + threadIdx.x;
     double rr = 0.0, ee = 0.0;
     if (i < n) {
-        d3 t = sum_partial3(partial, nsplit, n_pad, rank[i]);
+        d3 t = use_partial ? sum_partial3(partial, nsplit, n_pad, rank[i]) : d3{0.0, 0.0, 0.0};
         double s = salpha[i];
         d3 rv = (ld3(E + 3 * i) + t) * s - ld3(y + 3 * i);
         r[3 * i] = rv.x;
@@ -338,18 +368,18 @@ __global__ void k_cg_p(int n, const int* __restrict__ rank, int nblk, int prev, 
     }
 }
 
-// mu = sqrt(alpha) y; packs mu.
+// mu = sqrt(alpha) y; packs mu (mu - mu0 when mu0 is given).
 template <class R>
 __global__ void k_cg_mu(int n, const int* __restrict__ rank, const double* __restrict__ salpha, const double* __restrict__ thole,
                         const double* __restrict__ y, double* __restrict__ mu,
-                        typename Vec4T<R>::type* __restrict__ vec) {
+                        typename Vec4T<R>::type* __restrict__ vec, const double* __restrict__ mu0) {
     int i = blockIdx.x * blockDim.x + threadIdx.x;
     if (i >= n) return;
     d3 m = ld3(y + 3 * i) * salpha[i];
     mu[3 * i] = m.x;
     mu[3 * i + 1] = m.y;
     mu[3 * i + 2] = m.z;
-    store_vec<R>(vec, rank[i], m, thole[i]);
+    store_vec<R>(vec, rank[i], mu0 ? m - ld3(mu0 + 3 * i) : m, thole[i]);
 }
 
 // One Jacobi sweep of convergeInducedDipolesByDIIS (RTDF.cpp:838-846):
@@ -673,9 +703,20 @@ void launch_warm_start(const Dev& d, cudaStream_t st) {
                                                                      (typename Vec4T<R>::type*)d.vec_s);
 }
 template <class R>
-void launch_cg_residual(const Dev& d, cudaStream_t st) {
+void launch_cg_residual(const Dev& d, cudaStream_t st, bool use_partial) {
     k_cg_residual<R><<<d.nvb, kVecThreads, 0, st>>>(d.n, d.rank, d.nsplit, d.n_pad, d.partial, d.E, d.salpha, d.thole, d.y,
-                                                    d.r, d.p, (typename Vec4T<R>::type*)d.vec_s, d.rr_part, d.eps_part);
+                                                    d.r, d.p, (typename Vec4T<R>::type*)d.vec_s, d.rr_part, d.eps_part,
+                                                    use_partial ? 1 : 0);
+}
+template <class R>
+void launch_pack_total(const Dev& d, cudaStream_t st) {
+    k_pack_total<R><<<nblk(d.n, kVecThreads), kVecThreads, 0, st>>>(d.n, d.rank, d.lab, d.mu, d.thole,
+                                                                     (typename Vec4T<R>::type*)d.vec_s);
+}
+template <class R>
+void launch_fused_done(const Dev& d, cudaStream_t st) {
+    k_fused_done<<<nblk(d.n, kVecThreads), kVecThreads, 0, st>>>(d.n, d.rank, d.nsplit, d.n_pad, d.partial, d.salpha,
+                                                                 d.mu, d.E, d.y);
 }
 void launch_cg_q(const Dev& d, cudaStream_t st) {
     k_cg_q<<<d.nvb, kVecThreads, 0, st>>>(d.n, d.rank, d.nsplit, d.n_pad, d.partial, d.salpha, d.p, d.q, d.pq_part);
@@ -690,8 +731,9 @@ void launch_cg_p(const Dev& d, int prev, int slot, cudaStream_t st) {
                                              d.thole, d.r, d.p, (typename Vec4T<R>::type*)d.vec_s);
 }
 template <class R>
-void launch_cg_mu(const Dev& d, cudaStream_t st) {
-    k_cg_mu<R><<<d.nvb, kVecThreads, 0, st>>>(d.n, d.rank, d.salpha, d.thole, d.y, d.mu, (typename Vec4T<R>::type*)d.vec_s);
+void launch_cg_mu(const Dev& d, cudaStream_t st, const double* mu0) {
+    k_cg_mu<R><<<d.nvb, kVecThreads, 0, st>>>(d.n, d.rank, d.salpha, d.thole, d.y, d.mu, (typename Vec4T<R>::type*)d.vec_s,
+                                              mu0);
 }
 template <class R>
 void launch_jacobi(const Dev& d, cudaStream_t st) {
@@ -755,9 +797,11 @@ void launch_moments(const Dev& d, const double* mass, double* scratch, double* o
 #define TDP_INSTANTIATE2(R)                                                         \
     template void launch_fixed_done<R>(const Dev&, cudaStream_t);                   \
     template void launch_warm_start<R>(const Dev&, cudaStream_t);                   \
-    template void launch_cg_residual<R>(const Dev&, cudaStream_t);                  \
+    template void launch_cg_residual<R>(const Dev&, cudaStream_t, bool);            \
+    template void launch_pack_total<R>(const Dev&, cudaStream_t);                   \
+    template void launch_fused_done<R>(const Dev&, cudaStream_t);                   \
     template void launch_cg_p<R>(const Dev&, int, int, cudaStream_t);               \
-    template void launch_cg_mu<R>(const Dev&, cudaStream_t);                        \
+    template void launch_cg_mu<R>(const Dev&, cudaStream_t, const double*);         \
     template void launch_jacobi<R>(const Dev&, cudaStream_t);                       \
     template void launch_extrap_step<R>(const Dev&, int, cudaStream_t);             \
     template void launch_extrap_combine<R>(const Dev&, int, const double*, cudaStream_t); \

@@ -58,6 +58,7 @@ struct Dev {
     double* mu = nullptr;
     double* mu_prev = nullptr;   // the previous call's converged dipoles
     double* mu_prev2 = nullptr;  // and the call before's (warm-start predictor)
+    double* mu0 = nullptr;       // starting dipoles of a fused warm start (E then holds E + T mu0)
     double* y = nullptr;
     double* r = nullptr;
     double* p = nullptr;
@@ -92,11 +93,17 @@ template <class R> void launch_energy(const Dev& d, cudaStream_t st);
 template <class R> void launch_fixed_done(const Dev& d, cudaStream_t st);
 template <class R> void launch_warm_start(const Dev& d, cudaStream_t st);
 void launch_predict(const Dev& d, cudaStream_t st);
-template <class R> void launch_cg_residual(const Dev& d, cudaStream_t st);
+// use_partial = false: the field term is already in E (the fused start).
+template <class R> void launch_cg_residual(const Dev& d, cudaStream_t st, bool use_partial = true);
+// The start of a fused warm start: operand records m + mu0 (mu0 in d.mu), and
+// afterwards E := E + T mu0 from the walk's partial sums, y = mu0/sqrt(alpha).
+template <class R> void launch_pack_total(const Dev& d, cudaStream_t st);
+template <class R> void launch_fused_done(const Dev& d, cudaStream_t st);
 void launch_cg_q(const Dev& d, cudaStream_t st);
 void launch_cg_update(const Dev& d, int slot, cudaStream_t st);
 template <class R> void launch_cg_p(const Dev& d, int prev, int slot, cudaStream_t st);
-template <class R> void launch_cg_mu(const Dev& d, cudaStream_t st);
+// mu0 != NULL: the packed operand is mu - mu0 (the final check of a fused start).
+template <class R> void launch_cg_mu(const Dev& d, cudaStream_t st, const double* mu0 = nullptr);
 template <class R> void launch_jacobi(const Dev& d, cudaStream_t st);
 template <class R> void launch_extrap_step(const Dev& d, int k, cudaStream_t st);
 template <class R> void launch_extrap_combine(const Dev& d, int korder, const double* coef, cudaStream_t st);

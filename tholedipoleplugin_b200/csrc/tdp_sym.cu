@@ -492,14 +492,20 @@ __device__ __forceinline__ void field_partners(const PairParams& P, const double
                                                const TileGeom& g, double4 cA, double4 cB, int lane, int i, int ibase,
                                                int jbase, int e0, int e1, R oix, R oiy, R oiz, R qi,
                                                typename Vec4T<R>::type vi, bool diag, R damp_r2, R& fx, R& fy, R& fz,
-                                               R& gx, R& gy, R& gz) {
+                                               R& gx, R& gy, R& gz,
+                                               const typename Vec4T<R>::type* __restrict__ lab = nullptr) {
     typedef typename Vec4T<R>::type V4;
 #pragma unroll 1
+    // With lab (the fused start of a warm-started solve, KIND 0) the operand
+    // is P = m + mu0 and a partner pair adds M * field(q, P) + (I - M) * T mu0
+    // = M * field(q, m) + I * T mu0, with mu0 = P - m.
+    const bool fused = KIND == 0 && lab != nullptr;
     for (int e = e0; e < e1; e++) {
         unsigned off = (unsigned)(exc_j[e] - jbase);
         if (off >= 32u) continue;
         R sc = (R)(KIND == 0 ? exc_m[e] : exc_s[e]);
-        if (sc == R(0)) continue;
+        const R si = (R)exc_s[e];
+        if (sc == R(0) && (!fused || si == R(0))) continue;
         const V4 pj = sp[off], vj = sv[off];
         R dx, dy, dz;
         pair_delta<R, FOLD>(P, pos, i, jbase + off, pj.x, pj.y, pj.z, oix, oiy, oiz, dx, dy, dz);
@@ -510,6 +516,15 @@ __device__ __forceinline__ void field_partners(const PairParams& P, const double
         fx += sc * tx;
         fy += sc * ty;
         fz += sc * tz;
+        if (fused && si != sc) {
+            const V4 mj = lab[jbase + off];
+            R ux = 0, uy = 0, uz = 0;
+            pair_matvec<R, true>(dx, dy, dz, r2, vj.x - mj.x, vj.y - mj.y, vj.z - mj.z, vi.w, vj.w, damp_r2, ux, uy,
+                                 uz);
+            fx += (si - sc) * ux;
+            fy += (si - sc) * uy;
+            fz += (si - sc) * uz;
+        }
     }
     if (diag) return;
     const int jl = jbase + lane;
@@ -520,7 +535,8 @@ __device__ __forceinline__ void field_partners(const PairParams& P, const double
         const int a = exc_j[e];
         if ((unsigned)(a - ibase) >= 32u) continue;
         R sc = (R)(KIND == 0 ? exc_m[e] : exc_s[e]);
-        if (sc == R(0)) continue;
+        const R si = (R)exc_s[e];
+        if (sc == R(0) && (!fused || si == R(0))) continue;
         const V4 pa = posq[a], va = jvec[a];
         R ox, oy, oz;
         shift_into<R>(g, cA, cB, pa.x, pa.y, pa.z, ox, oy, oz);
@@ -533,6 +549,15 @@ __device__ __forceinline__ void field_partners(const PairParams& P, const double
         gx += sc * tx;
         gy += sc * ty;
         gz += sc * tz;
+        if (fused && si != sc) {
+            const V4 ma = lab[a];
+            R ux = 0, uy = 0, uz = 0;
+            pair_matvec<R, true>(dx, dy, dz, r2, va.x - ma.x, va.y - ma.y, va.z - ma.z, vl.w, va.w, damp_r2, ux, uy,
+                                 uz);
+            gx += (si - sc) * ux;
+            gy += (si - sc) * uy;
+            gz += (si - sc) * uz;
+        }
     }
 }
 
@@ -617,7 +642,7 @@ __global__ void __launch_bounds__(kSymThreads, sizeof(R) == 4 ? 4 : 3) k_field_s
     const double4* __restrict__ tctr, const double4* __restrict__ text, const double* __restrict__ pos,
     const int* __restrict__ exc_off, const int* __restrict__ exc_j, const double* __restrict__ exc_m,
     const double* __restrict__ exc_s, const int2* __restrict__ exc_tiles, int n_pad, double* __restrict__ partial,
-    FixAcc fix) {
+    FixAcc fix, const typename Vec4T<R>::type* __restrict__ lab) {
     typedef typename Vec4T<R>::type V4;
     extern __shared__ __align__(16) unsigned char smem[];
     const int BT = P.band_tiles, NA = BT * 32;
@@ -787,12 +812,12 @@ __global__ void __launch_bounds__(kSymThreads, sizeof(R) == 4 ? 4 : 3) k_field_s
                     field_partners<R, KIND, true>(P, pos, posq, jvec, sp, sv, exc_off, exc_j, exc_m, exc_s, g1, cA,
                                                   cB, lane, s1.i, s1.I * 32, jbase, s1.e0, s1.e1, s1.ox, s1.oy, s1.oz,
                                                   s1.pi.w, s1.vi, s1.diag, damp_r2, f1[0], f1[1], f1[2], g[0], g[1],
-                                                  g[2]);
+                                                  g[2], lab);
                 else
                     field_partners<R, KIND, false>(P, pos, posq, jvec, sp, sv, exc_off, exc_j, exc_m, exc_s, g1, cA,
                                                    cB, lane, s1.i, s1.I * 32, jbase, s1.e0, s1.e1, s1.ox, s1.oy,
                                                    s1.oz, s1.pi.w, s1.vi, s1.diag, damp_r2, f1[0], f1[1], f1[2], g[0],
-                                                   g[1], g[2]);
+                                                   g[1], g[2], lab);
             }
             R* acc = wacc + 3 * (Jl * 32 + lane);
             for (int c = 0; c < 3; c++) {
@@ -1766,21 +1791,26 @@ void fix_flush(const Dev& d, int ncomp, cudaStream_t st) {
 
 }  // namespace
 
+// kind 0: permanent field (operand: the lab dipoles); kind 1: mutual-field
+// matvec (operand: vec); kind 2: the start of a warm-started solve, the
+// permanent field plus T mu0 in one walk (operand vec = m + mu0, see
+// field_partners).
 template <class R>
 void launch_field(const Dev& d, int kind, cudaStream_t st) {
     typedef typename Vec4T<R>::type V4;
     const size_t smem = field_smem<R>(d.pp.band_tiles);
     // Field kernels run on the spatially sorted records.
-    if (kind == 0) {
+    if (kind == 0 || kind == 2) {
         cudaFuncSetAttribute(k_field_sym<R, 0>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
         k_field_sym<R, 0><<<band_pairs(d), kSymThreads, smem, st>>>(
-            d.pp, (const V4*)d.posq_s, (const V4*)d.dipt_s, d.tctr_s, d.text_s, d.pos_s, d.exs_off, d.exs_j, d.exs_m,
-            d.exs_s, d.exs_tiles, d.n_pad, d.partial, fix_of(d));
+            d.pp, (const V4*)d.posq_s, (const V4*)(kind == 0 ? d.dipt_s : d.vec_s), d.tctr_s, d.text_s, d.pos_s,
+            d.exs_off, d.exs_j, d.exs_m, d.exs_s, d.exs_tiles, d.n_pad, d.partial, fix_of(d),
+            kind == 2 ? (const V4*)d.dipt_s : nullptr);
     } else {
         cudaFuncSetAttribute(k_field_sym<R, 1>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
         k_field_sym<R, 1><<<band_pairs(d), kSymThreads, smem, st>>>(
             d.pp, (const V4*)d.posq_s, (const V4*)d.vec_s, d.tctr_s, d.text_s, d.pos_s, d.exs_off, d.exs_j, d.exs_m,
-            d.exs_s, d.exs_tiles, d.n_pad, d.partial, fix_of(d));
+            d.exs_s, d.exs_tiles, d.n_pad, d.partial, fix_of(d), nullptr);
     }
     if (sizeof(R) == 4) fix_flush(d, 3, st);
 }
