@@ -601,7 +601,7 @@ def _md_rate(system, precision, steps, warm, stream, world, barrier, max_over_ra
     if clocks:
         clocks.start()
     ev0, ev1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
-    r = {"mv_ms": 0.0, "mv_n": 0, "en_ms": 0.0, "fix_ms": 0.0, "launches": 0, "its": []}
+    r = {"mv_ms": 0.0, "mv_n": 0, "en_ms": 0.0, "fix_ms": 0.0, "fu_ms": 0.0, "fu_n": 0, "launches": 0, "its": []}
     ev0.record(stream)
     for _ in range(steps):
         md.step()
@@ -610,6 +610,8 @@ def _md_rate(system, precision, steps, warm, stream, world, barrier, max_over_ra
         r["mv_n"] += int(st[6])
         r["en_ms"] += st[8]
         r["fix_ms"] += st[1]
+        r["fu_n"] += int(st[10])
+        r["fu_ms"] += st[11]
         r["launches"] += int(st[9]) + 2  # + kick-drift and kick kernels
         r["its"].append(md.kernel.solverStats()["iterations"])
     ev1.record(stream)
@@ -781,6 +783,9 @@ def run_ours(args):
                       "cg_iterations_mean_md": _r(statistics.mean(m["its"])),
                       "matvecs_per_step": _r(m["mv_n"] / K), "parallelism": f"replicas x{world}"}}
     if args.no_extras:
+        out["kernels"] = {"matvec_ms": _r(m["mv_ms"] / max(1, m["mv_n"])), "energy_ms": _r(m["en_ms"] / K),
+                          "fused_start_ms": _r(m["fu_ms"] / max(1, m["fu_n"])),
+                          "permanent_field_stage_ms": _r(m["fix_ms"] / K)}
         if rank == 0:
             print(json.dumps(out), flush=True)
         ranks.close()
@@ -853,7 +858,9 @@ def run_ours(args):
         out["kernels"] = {
             "mixed": {"matvec_ms": _r(mv_avg), "matvec_tflops": _r(mv_tf), "matvec_share": _r(m["mv_ms"] / m["t_ms"]),
                       "energy_ms": _r(en_avg), "energy_tflops": _r(en_tf), "energy_share": _r(m["en_ms"] / m["t_ms"]),
-                      "permanent_field_stage_ms": _r(m["fix_ms"] / K), "fp32_peak_tflops": _r(fp32)},
+                      "permanent_field_stage_ms": _r(m["fix_ms"] / K),
+                      "fused_start_ms": _r(m["fu_ms"] / max(1, m["fu_n"])),
+                      "fused_start_share": _r(m["fu_ms"] / m["t_ms"]), "fp32_peak_tflops": _r(fp32)},
             "plain": {"matvec_ms": _r(pmv), "matvec_tflops": _r(pairs * FLOP_MATVEC_PAIR / (pmv * 1e-3) / 1e12),
                       "energy_ms": _r(pen), "energy_tflops": _r(pairs * FLOP_ENERGY_PAIR / (pen * 1e-3) / 1e12),
                       "fp64_peak_tflops": _r(fp64)}}

@@ -310,8 +310,11 @@ int tdp_adjoint_device(tdp_handle* h, const double* dL_dF, double dL_dE, double*
  * [0] pack+rotation ms, [1] permanent field ms, [2] induced-dipole solve ms,
  * [3] energy/force stage ms, [4] torque mapping ms, [5] total ms,
  * [6] mutual-field matvec launches, [7] summed matvec kernel ms,
- * [8] energy/force kernel ms, [9] kernel launches of the call. */
-#define TDP_NUM_STAGE_TIMES 10
+ * [8] energy/force kernel ms, [9] kernel launches of the call,
+ * [10] fused-start walks (0 or 1: a warm-started solve's single walk giving
+ * the permanent field plus the starting matvec), [11] their kernel ms.  The
+ * fused walk is counted in neither [6] nor [7]. */
+#define TDP_NUM_STAGE_TIMES 12
 int tdp_enable_timing(tdp_handle* h, int32_t enable);
 int tdp_stage_times(const tdp_handle* h, double* out);
 

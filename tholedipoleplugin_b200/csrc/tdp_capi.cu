@@ -71,8 +71,8 @@ struct tdp_handle {
     double* h_forces = nullptr; // pinned n*3
     double* d_stage = nullptr;  // device staging for host FP32 positions / query inputs
     size_t stage_bytes = 0;
-    bool mu_prev_valid = false;
-    bool mu_prev2_valid = false;
+    int n_hist = 0;         // valid entries of d.mu_hist
+    int predictor = 3;      // history points the warm-start predictor uses (1-4, TDP_PREDICTOR)
     // Warm-started Mutual solves start with one walk that gives E + T mu0
     // (TDP_FUSED_START=0 keeps the separate permanent-field walk and matvec).
     bool fused_start = true;
@@ -89,7 +89,7 @@ struct tdp_handle {
     bool timing = false;
     cudaEvent_t ev[6] = {nullptr, nullptr, nullptr, nullptr, nullptr, nullptr};
     std::vector<cudaEvent_t> kev;  // event pairs around matvec / energy kernels
-    std::vector<int> kev_kind;     // 0 matvec, 1 energy, per pair
+    std::vector<int> kev_kind;     // 0 matvec, 1 energy, 2 fused start, per pair
     size_t kev_used = 0;
     double stage_ms[TDP_NUM_STAGE_TIMES] = {};
     long launches = 0;
@@ -421,7 +421,8 @@ void record(tdp_handle* h, int k) {
     if (h->timing) TDP_CUDA(cudaEventRecord(h->ev[k], h->stream));
 }
 
-// Event pair around one pair-kernel launch (kind 0: matvec, 1: energy).
+// Event pair around one pair-kernel launch (kind 0: matvec, 1: energy, 2:
+// fused start).
 size_t kernel_begin(tdp_handle* h, int kind) {
     if (!h->timing) return 0;
     size_t k = h->kev_used++;
@@ -566,6 +567,12 @@ void solve_extrapolated(tdp_handle* h) {
     h->status = std::isfinite(h->epsilon) ? TDP_STATUS_CONVERGED : TDP_STATUS_NON_FINITE;
 }
 
+// Warm-start predictor weights, newest solution first: the polynomial of
+// degree nh - 1 through the last nh solutions, evaluated one step ahead
+// (binomial weights (-1)^(k) C(nh, k + 1)).
+constexpr double kPredictor[kMuHist][kMuHist] = {
+    {1.0, 0.0, 0.0, 0.0}, {2.0, -1.0, 0.0, 0.0}, {3.0, -3.0, 1.0, 0.0}, {4.0, -6.0, 4.0, -1.0}};
+
 // setup (RTDF.cpp:1117-1155): rotation, permanent field, induced dipoles.
 template <class R>
 void setup_and_solve(tdp_handle* h) {
@@ -582,7 +589,7 @@ void setup_and_solve(tdp_handle* h) {
     // A warm-started Mutual CG solve takes the fused start: one walk with the
     // operand m + mu0 gives E + T mu0 (see solve_cg).
     const bool fused = h->polarization == TDP_MUTUAL && h->solver == TDP_SOLVER_CG &&
-                       (h->flags & TDP_FLAG_WARM_START) && h->mu_prev_valid && !h->ew && h->fused_start && d.mu0;
+                       (h->flags & TDP_FLAG_WARM_START) && h->n_hist > 0 && !h->ew && h->fused_start && d.mu0;
     h->e_shifted = false;
     if (h->ew) {
         const double L[3] = {h->box[0], h->box[4], h->box[8]};
@@ -604,37 +611,34 @@ void setup_and_solve(tdp_handle* h) {
         if (h->solver == TDP_SOLVER_JACOBI) {
             solve_jacobi<R>(h);
         } else {
-            if ((h->flags & TDP_FLAG_WARM_START) && h->mu_prev_valid) {
-                // Linear extrapolation from the last two solutions when both
-                // exist (an O(dt^2) guess along a trajectory), else the last one.
-                if (h->mu_prev2_valid) {
-                    launch_predict(d, st);
-                } else {
-                    TDP_CUDA(cudaMemcpyAsync(d.mu, d.mu_prev, sizeof(double) * 3 * h->n, cudaMemcpyDeviceToDevice,
-                                             st));
-                }
+            if ((h->flags & TDP_FLAG_WARM_START) && h->n_hist > 0) {
+                // Polynomial extrapolation through the last nh solutions (exact
+                // for a trajectory of degree nh - 1 in time).
+                const int nh = std::min(h->n_hist, h->predictor);
+                launch_predict(d, nh, kPredictor[nh - 1], st);
                 if (fused) {
                     TDP_CUDA(cudaMemcpyAsync(d.mu0, d.mu, sizeof(double) * 3 * h->n, cudaMemcpyDeviceToDevice, st));
                     launch_pack_total<R>(d, st);
-                    size_t k = kernel_begin(h, 0);
+                    size_t k = kernel_begin(h, 2);
                     launch_field<R>(d, 2, st);
                     kernel_end(h, k);
-                    h->matvecs++;
                     launch_fused_done<R>(d, st);
                     h->launches += 4 + (sizeof(R) == 4 ? 1 : 0);
                     h->e_shifted = true;
                 } else {
                     launch_warm_start<R>(d, st);
                 }
-                h->launches += h->mu_prev2_valid ? 2 : 1;
+                h->launches += 1;
             }
             solve_cg<R>(h, fused);
         }
         const bool ok = h->status == TDP_STATUS_CONVERGED;
-        std::swap(d.mu_prev, d.mu_prev2);
-        TDP_CUDA(cudaMemcpyAsync(d.mu_prev, d.mu, sizeof(double) * 3 * h->n, cudaMemcpyDeviceToDevice, st));
-        h->mu_prev2_valid = ok && h->mu_prev_valid;
-        h->mu_prev_valid = ok;
+        // The oldest buffer takes this solution and moves to the front.
+        double* oldest = d.mu_hist[kMuHist - 1];
+        for (int k = kMuHist - 1; k > 0; k--) d.mu_hist[k] = d.mu_hist[k - 1];
+        d.mu_hist[0] = oldest;
+        TDP_CUDA(cudaMemcpyAsync(d.mu_hist[0], d.mu, sizeof(double) * 3 * h->n, cudaMemcpyDeviceToDevice, st));
+        h->n_hist = ok ? std::min(h->n_hist + 1, kMuHist) : 0;
     } else {
         solve_extrapolated<R>(h);
     }
@@ -679,15 +683,22 @@ void finish_timing(tdp_handle* h) {
     TDP_CUDA(cudaEventElapsedTime(&ms, h->ev[0], h->ev[5]));
     h->stage_ms[5] = ms;
     h->stage_ms[6] = h->matvecs;
-    double mv = 0.0, en = 0.0;
+    double mv = 0.0, en = 0.0, fu = 0.0;
+    int nfu = 0;
     for (size_t k = 0; k < h->kev_used; k++) {
         TDP_CUDA(cudaEventElapsedTime(&ms, h->kev[2 * k], h->kev[2 * k + 1]));
         if (h->kev_kind[k] == 0) mv += ms;
-        else en += ms;
+        else if (h->kev_kind[k] == 1) en += ms;
+        else {
+            fu += ms;
+            nfu++;
+        }
     }
     h->stage_ms[7] = mv;
     h->stage_ms[8] = en;
     h->stage_ms[9] = (double)h->launches;
+    h->stage_ms[10] = nfu;
+    h->stage_ms[11] = fu;
 }
 
 // Device-side failure flags of the last evaluation: enqueue their readback
@@ -1071,8 +1082,7 @@ int tdp_create(const tdp_system_desc* desc, tdp_handle** out) {
         d.lab = dalloc<double>(n3, o);
         d.E = dalloc<double>(n3, o);
         d.mu = dalloc<double>(n3, o);
-        d.mu_prev = dalloc<double>(n3, o);
-        d.mu_prev2 = dalloc<double>(n3, o);
+        for (int k = 0; k < kMuHist; k++) d.mu_hist[k] = dalloc<double>(n3, o);
         d.mu0 = dalloc<double>(n3, o);
         d.y = dalloc<double>(n3, o);
         d.r = dalloc<double>(n3, o);
@@ -1110,6 +1120,7 @@ int tdp_create(const tdp_system_desc* desc, tdp_handle** out) {
         if (const char* e = getenv("TDP_RESORT_INTERVAL")) h->resort_interval = std::max(1, atoi(e));
         if (const char* e = getenv("TDP_FUSED_START"))
             if (atoi(e) == 0) h->fused_start = false;
+        if (const char* e = getenv("TDP_PREDICTOR")) h->predictor = std::min(std::max(atoi(e), 1), kMuHist);
         d.order = dalloc<int>(d.n_pad, o);
         d.rank = dalloc<int>(n, o);
         d.pos_s = dalloc<double>(3 * (size_t)d.n_pad, o);
@@ -1198,8 +1209,7 @@ int tdp_update_params(tdp_handle* h, int32_t num_particles, const double* charge
         }
         TDP_CUDA(cudaStreamSynchronize(h->stream));
         upload_params(h);
-        h->mu_prev_valid = false;
-        h->mu_prev2_valid = false;
+        h->n_hist = 0;
         h->have_results = false;
     } catch (const TdpError& e) {
         return fail(h, e);
@@ -1254,8 +1264,7 @@ int tdp_update_particle_params(tdp_handle* h, const double* charges, const doubl
             h->alpha.clear();
             h->thole.clear();
         }
-        h->mu_prev_valid = false;
-        h->mu_prev2_valid = false;
+        h->n_hist = 0;
         h->have_results = false;
     } catch (const TdpError& e) {
         return fail(h, e);

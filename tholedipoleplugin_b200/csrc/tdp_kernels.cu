@@ -220,10 +220,16 @@ __global__ void k_warm_start(int n, const int* __restrict__ rank, const double* 
 }
 
 // Starting point extrapolated from the last two solutions: mu = 2 mu1 - mu2.
-__global__ void k_predict(size_t n3, const double* __restrict__ mu1, const double* __restrict__ mu2,
-                          double* __restrict__ mu) {
+__global__ void k_predict(size_t n3, int nh, const double* __restrict__ h0, const double* __restrict__ h1,
+                          const double* __restrict__ h2, const double* __restrict__ h3, double c0, double c1,
+                          double c2, double c3, double* __restrict__ mu) {
     const size_t k = blockIdx.x * (size_t)blockDim.x + threadIdx.x;
-    if (k < n3) mu[k] = 2.0 * mu1[k] - mu2[k];
+    if (k >= n3) return;
+    double v = c0 * h0[k];
+    if (nh > 1) v += c1 * h1[k];
+    if (nh > 2) v += c2 * h2[k];
+    if (nh > 3) v += c3 * h3[k];
+    mu[k] = v;
 }
 
 // Start of a fused warm start: the operand records carry m + mu0 (mu0 in mu),
@@ -693,9 +699,10 @@ void launch_fixed_done(const Dev& d, cudaStream_t st) {
                                                                      d.salpha, d.thole, d.E, d.mu, d.y,
                                                                      (typename Vec4T<R>::type*)d.vec_s);
 }
-void launch_predict(const Dev& d, cudaStream_t st) {
+void launch_predict(const Dev& d, int nh, const double* c, cudaStream_t st) {
     const size_t n3 = 3 * (size_t)d.n;
-    k_predict<<<nblk(n3, kVecThreads), kVecThreads, 0, st>>>(n3, d.mu_prev, d.mu_prev2, d.mu);
+    k_predict<<<nblk(n3, kVecThreads), kVecThreads, 0, st>>>(n3, nh, d.mu_hist[0], d.mu_hist[1], d.mu_hist[2],
+                                                              d.mu_hist[3], c[0], c[1], c[2], c[3], d.mu);
 }
 template <class R>
 void launch_warm_start(const Dev& d, cudaStream_t st) {

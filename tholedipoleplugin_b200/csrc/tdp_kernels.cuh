@@ -10,6 +10,8 @@ namespace tdp {
 // whole number of bands, nsplit partial-sum slots of the pair kernels = one per
 // band, n_eblk energy partials = one per band pair, nvb blocks of the O(N)
 // kernels).
+constexpr int kMuHist = 4;
+
 struct Dev {
     int n = 0, n_pad = 0, nsplit = 1, nvb = 1, n_eblk = 1;
     PairParams pp{};
@@ -56,8 +58,9 @@ struct Dev {
     double* lab = nullptr;
     double* E = nullptr;
     double* mu = nullptr;
-    double* mu_prev = nullptr;   // the previous call's converged dipoles
-    double* mu_prev2 = nullptr;  // and the call before's (warm-start predictor)
+    // Converged dipoles of the last kMuHist calls, newest first (warm-start
+    // predictor; the handle counts the valid ones).
+    double* mu_hist[kMuHist] = {nullptr, nullptr, nullptr, nullptr};
     double* mu0 = nullptr;       // starting dipoles of a fused warm start (E then holds E + T mu0)
     double* y = nullptr;
     double* r = nullptr;
@@ -92,7 +95,8 @@ template <class R> void launch_field(const Dev& d, int kind, cudaStream_t st);
 template <class R> void launch_energy(const Dev& d, cudaStream_t st);
 template <class R> void launch_fixed_done(const Dev& d, cudaStream_t st);
 template <class R> void launch_warm_start(const Dev& d, cudaStream_t st);
-void launch_predict(const Dev& d, cudaStream_t st);
+// mu = sum_k c[k] mu_hist[k] over the first nh history entries.
+void launch_predict(const Dev& d, int nh, const double* c, cudaStream_t st);
 // use_partial = false: the field term is already in E (the fused start).
 template <class R> void launch_cg_residual(const Dev& d, cudaStream_t st, bool use_partial = true);
 // The start of a fused warm start: operand records m + mu0 (mu0 in d.mu), and

@@ -299,7 +299,7 @@ __device__ __forceinline__ void stage_fpacked(FPackedTile& T, int lane, float4 p
 
 // Loop-invariant operands of one I atom.
 struct XSlot {
-    f2 OX, OY, OZ, VX, VY, VZ, Q;
+    f2 OX, OY, OZ, VX, VY, VZ, NQ;   // NQ = -q
     float t;
     int i;
 };
@@ -312,20 +312,21 @@ __device__ __forceinline__ XSlot xslot(int i, float ox, float oy, float oz, floa
     x.VX = bc2(v.x);
     x.VY = bc2(v.y);
     x.VZ = bc2(v.z);
-    x.Q = bc2(q);
+    x.NQ = bc2(-q);
     x.t = v.w;
     x.i = i;
     return x;
 }
 
-// One I atom against J atoms (m, m + 16): I-side sums into F*, J-side into G*.
+// One I atom against J atoms (m, m + 16): I-side sums into F*, J-side into G*,
+// both with the opposite sign of the field (the walk's caller flips them), so
+// that every term is a plain product-sum with -rr5.
 template <int KIND, bool FOLD, bool DAMP>
 __device__ __forceinline__ void xslot_pairs(const PairParams& P, const double* __restrict__ pos, const XSlot& x,
                                             int ja, f2 PX, f2 PY, f2 PZ, f2 QJ, f2 VJX, f2 VJY, f2 VJZ, float tja,
                                             float tjb, unsigned fm, f2 Lx, f2 Ly, f2 Lz, f2 Ix, f2 Iy, f2 Iz,
                                             f2 NTx, f2 NTy, f2 NTz, float damp_r2, f2& FX, f2& FY, f2& FZ,
                                             f2& GX, f2& GY, f2& GZ) {
-    const f2 THREE = bc2(3.0f), NEG = bc2(-1.0f);
     f2 DX = sub2(PX, x.OX), DY = sub2(PY, x.OY), DZ = sub2(PZ, x.OZ);
     if (FOLD) {
         // Fold the dimensions of fm.  Q = d^2 - t^2 (t = half a box minus 16
@@ -376,41 +377,43 @@ __device__ __forceinline__ void xslot_pairs(const PairParams& P, const double* _
     const f2 RINV = pk2(rsqrt_r(r2a), rsqrt_r(r2b));
     const f2 RINV2 = mul2(RINV, RINV);
     f2 RR3 = mul2(RINV, RINV2);
-    f2 RR5 = mul2(mul2(THREE, RR3), RINV2);
+    f2 NRR5 = mul2(RR3, mul2(RINV2, bc2(-3.0f)));   // -rr5
     if (DAMP) {
         if (r2a < damp_r2 || r2b < damp_r2) {
             float ra, rb, r3a, r3b, r5a, r5b;
             un2(RINV, ra, rb);
             un2(RR3, r3a, r3b);
-            un2(RR5, r5a, r5b);
+            un2(NRR5, r5a, r5b);
+            r5a = -r5a;
+            r5b = -r5b;
             damp_field<float>(r2a, ra, x.t, tja, damp_r2, r3a, r5a);
             damp_field<float>(r2b, rb, x.t, tjb, damp_r2, r3b, r5b);
             RR3 = pk2(r3a, r3b);
-            RR5 = pk2(r5a, r5b);
+            NRR5 = pk2(-r5a, -r5b);
         }
     }
-    const f2 NRR3 = mul2(RR3, NEG);
     if (KIND == 1) {
-        // pair_matvec2: f_i += (rr5 v_j.d) d - rr3 v_j;  f_j += (rr5 v_i.d) d - rr3 v_i.
-        const f2 DDJ = mul2(RR5, fma2(VJX, DX, fma2(VJY, DY, mul2(VJZ, DZ))));
-        const f2 DDI = mul2(RR5, fma2(x.VX, DX, fma2(x.VY, DY, mul2(x.VZ, DZ))));
-        FX = fma2(NRR3, VJX, fma2(DDJ, DX, FX));
-        FY = fma2(NRR3, VJY, fma2(DDJ, DY, FY));
-        FZ = fma2(NRR3, VJZ, fma2(DDJ, DZ, FZ));
-        GX = fma2(NRR3, x.VX, fma2(DDI, DX, GX));
-        GY = fma2(NRR3, x.VY, fma2(DDI, DY, GY));
-        GZ = fma2(NRR3, x.VZ, fma2(DDI, DZ, GZ));
+        // pair_matvec2 with both sums negated: -f_i += rr3 v_j - (rr5 v_j.d) d,
+        // -f_j += rr3 v_i - (rr5 v_i.d) d.
+        const f2 DDJ = mul2(NRR5, fma2(VJX, DX, fma2(VJY, DY, mul2(VJZ, DZ))));
+        const f2 DDI = mul2(NRR5, fma2(x.VX, DX, fma2(x.VY, DY, mul2(x.VZ, DZ))));
+        FX = fma2(RR3, VJX, fma2(DDJ, DX, FX));
+        FY = fma2(RR3, VJY, fma2(DDJ, DY, FY));
+        FZ = fma2(RR3, VJZ, fma2(DDJ, DZ, FZ));
+        GX = fma2(RR3, x.VX, fma2(DDI, DX, GX));
+        GY = fma2(RR3, x.VY, fma2(DDI, DY, GY));
+        GZ = fma2(RR3, x.VZ, fma2(DDI, DZ, GZ));
     } else {
         // pair_fixed2: a = rr3 q_j - rr5 m_j.d, b = rr3 q_i + rr5 m_i.d;
-        // f_i -= d a + m_j rr3 (F holds the negative);  f_j += d b - m_i rr3.
-        const f2 A = sub2(mul2(RR3, QJ), mul2(RR5, fma2(VJX, DX, fma2(VJY, DY, mul2(VJZ, DZ)))));
-        const f2 B = fma2(RR5, fma2(x.VX, DX, fma2(x.VY, DY, mul2(x.VZ, DZ))), mul2(RR3, x.Q));
+        // -f_i += d a + m_j rr3;  -f_j += m_i rr3 - d b, with nb = -b.
+        const f2 A = fma2(NRR5, fma2(VJX, DX, fma2(VJY, DY, mul2(VJZ, DZ))), mul2(RR3, QJ));
+        const f2 NB = fma2(NRR5, fma2(x.VX, DX, fma2(x.VY, DY, mul2(x.VZ, DZ))), mul2(RR3, x.NQ));
         FX = fma2(VJX, RR3, fma2(DX, A, FX));
         FY = fma2(VJY, RR3, fma2(DY, A, FY));
         FZ = fma2(VJZ, RR3, fma2(DZ, A, FZ));
-        GX = fma2(NRR3, x.VX, fma2(DX, B, GX));
-        GY = fma2(NRR3, x.VY, fma2(DY, B, GY));
-        GZ = fma2(NRR3, x.VZ, fma2(DZ, B, GZ));
+        GX = fma2(x.VX, RR3, fma2(DX, NB, GX));
+        GY = fma2(x.VY, RR3, fma2(DY, NB, GY));
+        GZ = fma2(x.VZ, RR3, fma2(DZ, NB, GZ));
     }
 }
 
@@ -451,21 +454,21 @@ __device__ __forceinline__ void field_walk_x4(const PairParams& P, const double*
         GY = __shfl_sync(kFull, GY, nxt);
         GZ = __shfl_sync(kFull, GZ, nxt);
     }
-    const float sg = KIND == 0 ? -1.0f : 1.0f;
+    // F and G hold the negated sums (xslot_pairs).
     float lo, hi;
     un2(FXA, lo, hi);
-    fa[0] += sg * (lo + hi);
+    fa[0] -= lo + hi;
     un2(FYA, lo, hi);
-    fa[1] += sg * (lo + hi);
+    fa[1] -= lo + hi;
     un2(FZA, lo, hi);
-    fa[2] += sg * (lo + hi);
+    fa[2] -= lo + hi;
     if (two) {
         un2(FXB, lo, hi);
-        fb[0] += sg * (lo + hi);
+        fb[0] -= lo + hi;
         un2(FYB, lo, hi);
-        fb[1] += sg * (lo + hi);
+        fb[1] -= lo + hi;
         un2(FZB, lo, hi);
-        fb[2] += sg * (lo + hi);
+        fb[2] -= lo + hi;
     }
     // Lane l now holds (atom l & 15, atom (l & 15) + 16); lane l ^ 16 the other copy.
     const f2 Js[3] = {GX, GY, GZ};
@@ -473,7 +476,7 @@ __device__ __forceinline__ void field_walk_x4(const PairParams& P, const double*
     for (int k = 0; k < 3; k++) {
         un2(Js[k], lo, hi);
         const float olo = __shfl_xor_sync(kFull, lo, 16), ohi = __shfl_xor_sync(kFull, hi, 16);
-        g[k] += lane < 16 ? lo + olo : hi + ohi;
+        g[k] -= lane < 16 ? lo + olo : hi + ohi;
     }
 }
 
@@ -495,11 +498,11 @@ __device__ __forceinline__ void field_partners(const PairParams& P, const double
                                                R& gx, R& gy, R& gz,
                                                const typename Vec4T<R>::type* __restrict__ lab = nullptr) {
     typedef typename Vec4T<R>::type V4;
-#pragma unroll 1
     // With lab (the fused start of a warm-started solve, KIND 0) the operand
     // is P = m + mu0 and a partner pair adds M * field(q, P) + (I - M) * T mu0
     // = M * field(q, m) + I * T mu0, with mu0 = P - m.
     const bool fused = KIND == 0 && lab != nullptr;
+#pragma unroll 1
     for (int e = e0; e < e1; e++) {
         unsigned off = (unsigned)(exc_j[e] - jbase);
         if (off >= 32u) continue;

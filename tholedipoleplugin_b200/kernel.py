@@ -268,6 +268,6 @@ class CudaCalcTholeDipoleForceKernel:
         return {"iterations": it.value, "epsilon": eps.value, "converged": conv.value, "status": st.value}
 
     def stageTimes(self) -> Sequence[float]:
-        out = np.zeros(10)
+        out = np.zeros(A.NUM_STAGE_TIMES)
         self._check(self._lib.tdp_stage_times(self._h, _dptr(out)))
         return out
