@@ -4,29 +4,36 @@
 Workload (per GPU): the 98,304-atom water box -- 32,768 rigid 3-site waters on
 a 32^3 lattice in a 9.936 nm cubic box, seeded jitter and orientations,
 minimum-image all-pairs electrostatics with Thole-damped mutual polarization
-converged to an RMS dipole change below 1e-6 e*nm -- integrated by velocity
-Verlet (1 fs, rigid waters, Maxwell-Boltzmann start at 300 K).  One "step" is
-one MD step: kick-drift-SHAKE, the full force/energy evaluation (lab-frame
-rotation, permanent field, CG solve, pair energy/force/torque, torque
-mapping) and kick-RATTLE.
+converged to an RMS dipole change below BOX_EPS (1e-7 e*nm) -- integrated by
+velocity Verlet (1 fs, rigid waters, Maxwell-Boltzmann start at 300 K).  One
+"step" is one MD step: kick-drift-SHAKE, the full force/energy evaluation
+(lab-frame rotation, permanent field, CG solve warm-started from the last
+solutions, pair energy/force/torque, torque mapping) and kick-RATTLE.
 
 Reported (one JSON line, rank 0):
   value        ns/day of the mixed form, summed over ranks (replicas; weak scaling)
   e2e          the same metric through the public C ABI with host buffers
                (positions copied in from pinned memory and forces read back
                every step, integration on the host)
-  plain        ns/day and SCF solves/s of the FP64 form; mixed solves/s beside it
-  errors       mixed vs plain on this box; both vs the FP64 oracle on 216 waters
+  plain        ns/day of the FP64 form; scf_solves_per_s: cold-start SCF
+               solves/s of both forms beside the reference's one-core solve
+  errors       both forms at the timed tolerance against a tight FP64 solve of
+               this box, the FP64 oracle on 216 waters and the compiled
+               reference's golden for the 12,288-atom box
   roofline     the dominant kernel against the FP32 issue rate of the GPU
                (FP32 SGEMM measured here); roofline_hbm: the same kernel
-               against the measured HBM copy bandwidth
+               against the measured HBM copy bandwidth; kernels: per-kernel
+               times and rates of both forms
   cpu_baseline the reference's own FP64 code (compiled oracle/_ref), 1 core,
                timed on a 6,591-atom sample and scaled to this box
+  ewald        the same box in the Ewald mode (real space + smooth PME)
   clusters     the batched-cluster workload (1024 NoCutoff water clusters of
                4-64 waters in one persistent launch): clusters/s mixed and
-               plain, device-resident and end to end, the autotuner's table,
+               plain, device-resident and end to end, the autotuner's tile,
                per-cluster errors against the FP64 oracle, and the compiled
                reference on one core over 384 of the clusters
+  adjoint      gradients/s of a force loss with respect to the particle
+               parameters, on the 12,288-atom box and on 256 clusters
 
 `--impl reference` times the reference's CPU implementation on all host cores
 instead (rank 0 only).
