@@ -82,9 +82,11 @@ extern "C" {
  * reproducible against it.  With this flag they use 1/r^4 instead. */
 #define TDP_FLAG_DD_FORCE_R4 (1u << 0)
 /* Start the Mutual CG solve from the previous calls' induced dipoles (the
- * reference restarts from mu0 = alpha*E every call): 2*mu(n-1) - mu(n-2) when
- * the last two calls converged -- along an MD trajectory a second-order
- * guess -- else mu(n-1).  The converged result is the same fixed point to the
+ * reference restarts from mu0 = alpha*E every call): the polynomial through
+ * the last converged solutions (up to three by default, TDP_PREDICTOR = 1..4
+ * at create), evaluated one call ahead.  With CG the first walk then gives the
+ * permanent field and the starting matvec together (TDP_FUSED_START=0 at create
+ * keeps them apart).  The converged result is the same fixed point to the
  * solver tolerance; only the iteration count changes. */
 #define TDP_FLAG_WARM_START (1u << 1)
 /* Ewald mode (with TDP_PME only).  The reference has no Ewald sum: its "PME"
@@ -97,9 +99,10 @@ extern "C" {
  * terms.  The fields and induced dipoles are the periodic versions of the
  * reference's (same Thole damping, M and I scales); the energy is the
  * variational one, U_perm - 1/2 mu.E_M, and the forces are its exact negative
- * gradient (Mutual polarization only, where the energy is stationary in the
- * induced dipoles; Direct and Extrapolated give TDP_ERR_UNSUPPORTED; frames
- * whose torque map is the gradient of their rotation, i.e. not ZOnly).
+ * gradient (Mutual and Direct polarization, whose energies are stationary in
+ * the induced dipoles -- Direct's functional drops the induced-induced term;
+ * Extrapolated gives TDP_ERR_UNSUPPORTED; frames whose torque map is the
+ * gradient of their rotation, i.e. not ZOnly).
  * Orthorhombic boxes only; real space, damping corrections
  * included, stops at the cutoff, where exp(-a u^3) of every pair must be
  * <= 1e-12 (cutoff^3 >= 27.63 t_max^5); tdp_adjoint is unsupported.
@@ -115,8 +118,8 @@ extern "C" {
  * reference's own forces follow its quasi-internal-frame convention and are
  * not the gradient of its energy, ReferenceTholeDipoleForce.cpp:129-366).  Runs
  * on the Ewald mode's real-space kernels with alpha = 0, no cutoff and no
- * reciprocal space; the same limits as TDP_FLAG_EWALD (Mutual polarization,
- * no ZOnly frames, no tdp_adjoint). */
+ * reciprocal space; the same limits as TDP_FLAG_EWALD (Mutual or Direct
+ * polarization, no ZOnly frames, no tdp_adjoint). */
 #define TDP_FLAG_VARIATIONAL (1u << 3)
 
 /* Flags of tdp_compute. */

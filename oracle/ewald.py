@@ -40,6 +40,10 @@ Physics (Coulomb prefactor 1, RTDF.cpp:20-21; nm, e, e*nm, nm^3):
   corrections for scaled and damped terms, at any distance; self terms
   -alpha/sqrt(pi) sum q^2 - 2 alpha^3/(3 sqrt(pi)) sum |p + mu|^2 and the
   neutralising plasma -pi Q^2 / (2 V alpha^2).
+* Direct polarization (mu = alpha E_M): the functional without the s E_damp(U_i,U_j)
+  term, whose stationary point is mu = alpha E_M; written as U(mu) minus the
+  Ewald energy of the induced dipoles alone, U(0, mu) = -1/2 mu.T mu, so its
+  forces are those of U minus those of that induced-only energy.
 * Forces are -dU/dr at the converged dipoles (the energy is stationary in
   mu); the torques p_i x (-dU/dp_i) go through the reference's torque map
   (RTDF.cpp:915-1115, via the C oracle).  Unlike the reference's own forces
@@ -520,12 +524,32 @@ class Ewald:
         return s * y, E
 
     # Energy and forces ------------------------------------------------------
+    def direct(self) -> bool:
+        return int(self.sys.polarization) == 0
+
     def evaluate(self, mu=None, E=None) -> EwaldResult:
+        """Energy functional and forces at mu (the converged dipoles when None:
+        the CG solution for Mutual, alpha E_M for Direct polarization)."""
         if mu is None:
-            mu, E = self.solve()
+            if self.direct():
+                E = self.fixed_field()
+                mu = self.pol[:, None] * E
+            else:
+                mu, E = self.solve()
         elif E is None:
             E = self.fixed_field()
-        q, p = self.q, self.lab
+        energy, forces, torque = self._energy_forces(self.q, self.lab, mu, induction=True)
+        if self.direct():
+            z = np.zeros(self.n)
+            e_uu, f_uu, _ = self._energy_forces(z, np.zeros((self.n, 3)), mu, induction=False)
+            energy -= e_uu
+            forces = forces - f_uu
+        forces = forces + map_torque(self.sys, torque)
+        return EwaldResult(energy, forces, mu, self.lab.copy(), E, self.alpha, self.grid)
+
+    def _energy_forces(self, q, p, mu, induction):
+        """Energy, pair forces and the torques on p of multipoles (q, p) with
+        induced dipoles mu (induction adds 1/2 mu.alpha^-1 mu)."""
         z = np.zeros(self.n)
         tot = p + mu
         M, S = self.M, self.S
@@ -562,12 +586,9 @@ class Ewald:
             (tot * tot).sum())
         e_plasma = -math.pi * Q * Q / (2.0 * V * self.alpha ** 2) if self.alpha > 0.0 else 0.0
         pos_mask = self.pol > 0
-        e_ind = 0.5 * float((mu[pos_mask] ** 2 / self.pol[pos_mask, None]).sum())
+        e_ind = 0.5 * float((mu[pos_mask] ** 2 / self.pol[pos_mask, None]).sum()) if induction else 0.0
         energy = e_real + e_rec + e_self + e_plasma + e_ind
-        forces = f_real + f_rec
-        torque = np.cross(p, eff)
-        forces = forces + map_torque(self.sys, torque)
-        return EwaldResult(energy, forces, mu, p.copy(), E, self.alpha, self.grid)
+        return energy, f_real + f_rec, np.cross(p, eff)
 
     def energy_at(self, mu=None):
         return self.evaluate(mu).energy

@@ -145,8 +145,8 @@ def test_ewald_mode_validation(lib):
 
 def test_gradient_modes_validation(lib):
     s = S.config_small()
-    rc, _, _ = _create(s.copy(polarization=S.DIRECT), flags=A.FLAG_EWALD)
-    assert rc == -8 and "Mutual polarization" in lib.tdp_last_error(None).decode()
+    rc, _, _ = _create(s.copy(polarization=S.EXTRAPOLATED), flags=A.FLAG_EWALD)
+    assert rc == -8 and "Mutual or Direct polarization" in lib.tdp_last_error(None).decode()
     rc, _, _ = _create(s, flags=A.FLAG_VARIATIONAL)
     assert rc == -1 and "NoCutoff mode" in lib.tdp_last_error(None).decode()
     rc, _, _ = _create(s.copy(method=S.NO_CUTOFF), flags=A.FLAG_VARIATIONAL | A.FLAG_EWALD)

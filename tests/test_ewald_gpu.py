@@ -84,11 +84,38 @@ def test_permanent_field(precision, tol):
     assert rel_rms(mu, E * s.polarizabilities[:, None]) < tol
 
 
-def test_direct_and_extrapolated_rejected():
+def test_extrapolated_rejected():
     from tholedipoleplugin_b200._capi import TdpError
-    for pol in (S.DIRECT, S.EXTRAPOLATED):
-        with pytest.raises(TdpError, match="Mutual polarization"):
-            CudaCalcTholeDipoleForceKernel(water216().copy(polarization=pol), ewald=True)
+    with pytest.raises(TdpError, match="Mutual or Direct polarization"):
+        CudaCalcTholeDipoleForceKernel(water216().copy(polarization=S.EXTRAPOLATED), ewald=True)
+
+
+@pytest.mark.parametrize("precision,e_tol,f_tol", [("double", 1e-9, 1e-8), ("mixed", 1e-6, 2e-5)])
+def test_direct_water216_matches_oracle(precision, e_tol, f_tol):
+    # Direct polarization: mu = alpha E_M, energy U_perm - 1/2 mu.E_M (the
+    # Mutual functional without the induced-induced term), forces its gradient.
+    _, ref, _, _ = oracle_pme("w216_direct", lambda: water216().copy(polarization=S.DIRECT))
+    e, f, mu, _, stats = run(water216().copy(polarization=S.DIRECT), precision, 1e-11)
+    assert stats["iterations"] == 0
+    assert rel_rms(mu, ref.induced) < f_tol
+    assert rel_err(e, ref.energy) < e_tol, (e, ref.energy)
+    assert rel_rms(f, ref.forces) < f_tol
+
+
+def test_direct_forces_are_gradient_of_gpu_energy():
+    s = S.water_box(5, 1.5525, seed=9, cutoff=0.7, polarization=S.DIRECT)
+    with CudaCalcTholeDipoleForceKernel(s, precision="double", ewald=True) as k:
+        _, f0 = k.execute(s.positions)
+        h = 1e-5
+        scale = np.abs(f0).max()
+        for i, c in [(0, 0), (0, 2), (1, 1), (2, 0), (100, 2), (374, 1)]:
+            e = []
+            for sg in (1.0, -1.0):
+                p = s.positions.copy()
+                p[i, c] += sg * h
+                e.append(k.execute(p)[0])
+            fd = -(e[0] - e[1]) / (2 * h)
+            assert abs(fd - f0[i, c]) < 1e-7 * scale, (i, c, fd, f0[i, c])
 
 
 def test_forces_are_gradient_of_gpu_energy():

@@ -177,3 +177,38 @@ def test_variational_nocutoff_oracle():
                 s2.positions[i, c] += sg * h
                 e.append(EW.variational_nocutoff(s2).energy)
             assert abs(-(e[0] - e[1]) / (2 * h) - r.forces[i, c]) < 1e-8 * scale
+
+
+def test_direct_forces_are_minus_energy_gradient(tiny_box):
+    # Direct polarization: mu = alpha E_M at every position, energy U_perm - 1/2 mu.E_M.
+    s = tiny_box.copy(polarization=S.DIRECT)
+    alpha = 9.0
+    r0 = EW.Ewald(s, alpha, recip="direct").evaluate()
+    assert rel(r0.induced, r0.fixed_field * s.polarizabilities[:, None]) < 1e-15
+    # The functional at its stationary point is U_perm - 1/2 mu.E_M.
+    perm = EW.Ewald(s.copy(polarizabilities=np.zeros(s.n)), alpha, recip="direct").evaluate().energy
+    assert abs((r0.energy - perm) - (-0.5 * (r0.induced * r0.fixed_field).sum())) < 1e-12 * abs(r0.energy)
+    h = 2e-5
+    scale = np.abs(r0.forces).max()
+    for i, c in [(0, 0), (0, 2), (1, 0), (2, 1), (4, 2), (9, 0)]:
+        e = []
+        for sg in (1.0, -1.0):
+            s2 = s.copy()
+            s2.positions[i, c] += sg * h
+            e.append(EW.Ewald(s2, alpha, recip="direct").evaluate().energy)
+        fd = -(e[0] - e[1]) / (2 * h)
+        assert abs(fd - r0.forces[i, c]) < 2e-8 * scale, (i, c, fd, r0.forces[i, c])
+
+
+def test_direct_energy_stationary_and_alpha_independent(tiny_box):
+    s = tiny_box.copy(polarization=S.DIRECT)
+    a = EW.Ewald(s, 18.0, recip="direct")
+    b = EW.Ewald(s, 21.0, recip="direct").evaluate()
+    ra = a.evaluate()
+    assert abs(ra.energy - b.energy) <= 1e-12 * abs(ra.energy)
+    assert rel(ra.forces, b.forces) < 1e-12
+    u0 = ra.energy
+    d = np.random.default_rng(2).standard_normal(ra.induced.shape) * 1e-4 * np.abs(ra.induced).max()
+    d1 = a.evaluate(ra.induced + d, ra.fixed_field).energy - u0
+    d2 = a.evaluate(ra.induced + 0.5 * d, ra.fixed_field).energy - u0
+    assert d1 > 0 and abs(d1 / d2 - 4.0) < 1e-3

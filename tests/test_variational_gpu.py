@@ -34,9 +34,10 @@ def run(s, precision, eps, variational=True):
     return e, f, mu
 
 
+@pytest.mark.parametrize("polarization", [S.MUTUAL, S.DIRECT])
 @pytest.mark.parametrize("precision,eps,e_tol,f_tol", [("double", 1e-11, 1e-9, 1e-8), ("mixed", 1e-9, 1e-6, 2e-5)])
-def test_water_cluster_matches_oracle(precision, eps, e_tol, f_tol):
-    s = cluster()
+def test_water_cluster_matches_oracle(precision, eps, e_tol, f_tol, polarization):
+    s = cluster().copy(polarization=polarization)
     ref = EW.variational_nocutoff(s)
     e, f, mu = run(s, precision, eps)
     bound = e_tol * abs(ref.energy) + (3e-7 * energy_rms_scale(s) if precision == "mixed" else 0.0)

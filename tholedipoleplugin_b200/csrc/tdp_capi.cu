@@ -652,7 +652,7 @@ void run_energy(tdp_handle* h) {
     cudaStream_t st = h->stream;
     if (h->ew) {
         size_t k = kernel_begin(h, 1);
-        ewald_energy<R>(h->ew, d, h->total_charge, st);
+        ewald_energy<R>(h->ew, d, h->total_charge, st, h->polarization == TDP_DIRECT);
         kernel_end(h, k);
         h->launches += ewald_last_launches(h->ew);
         record(h, 4);
@@ -978,12 +978,14 @@ int tdp_create(const tdp_system_desc* desc, tdp_handle** out) {
         d.nsplit = d.pp.n_bands;
         d.n_eblk = d.pp.n_bands * (d.pp.n_bands + 1) / 2;
         const bool variational = (h->flags & TDP_FLAG_VARIATIONAL) != 0;
-        // Both gradient modes rest on the energy being stationary in the induced
-        // dipoles, which holds for Mutual polarization.
-        if ((h->flags & (TDP_FLAG_VARIATIONAL | TDP_FLAG_EWALD)) && h->polarization != TDP_MUTUAL)
+        // Both gradient modes rest on an energy functional that is stationary
+        // in the induced dipoles: Mutual (mu = alpha (E + T mu)) and Direct
+        // (mu = alpha E, the functional without the induced-induced term)
+        // have one; the Extrapolated dipoles minimise none.
+        if ((h->flags & (TDP_FLAG_VARIATIONAL | TDP_FLAG_EWALD)) && h->polarization == TDP_EXTRAPOLATED)
             throw TdpError{TDP_ERR_UNSUPPORTED,
-                           "TDP_FLAG_EWALD and TDP_FLAG_VARIATIONAL need Mutual polarization (their forces are the "
-                           "gradient of an energy that is stationary in the induced dipoles)"};
+                           "TDP_FLAG_EWALD and TDP_FLAG_VARIATIONAL need Mutual or Direct polarization (their forces "
+                           "are the gradient of an energy that is stationary in the induced dipoles)"};
         if (variational) {
             if (h->method != TDP_NO_CUTOFF)
                 throw TdpError{TDP_ERR_INVALID_ARGUMENT,
@@ -1136,7 +1138,8 @@ int tdp_create(const tdp_system_desc* desc, tdp_handle** out) {
         d.exs_tiles = dalloc<int2>(d.n_pad / kTile, o);
         upload(d.coef, h->extrap.data(), sizeof(double) * h->extrap.size());
         upload_params(h);
-        if (ewald || variational) h->ew = ewald_create(d, h->precision, variational);
+        if (ewald || variational)
+            h->ew = ewald_create(d, h->precision, variational, h->polarization == TDP_DIRECT);
         TDP_CUDA(cudaMallocHost(&h->h_scal, 64 * sizeof(double)));
         TDP_CUDA(cudaMallocHost(&h->h_fixerr, sizeof(int)));
         *h->h_fixerr = 0;

@@ -1271,6 +1271,21 @@ __global__ void k_ew_pack_mu(int n, const int* __restrict__ rank, const double* 
     vec_s[rank[i]] = o;
 }
 
+// The induced dipoles' own records (Direct polarization): charge 0 and
+// permanent dipole 0, positions and Thole factors kept.
+template <class R>
+__global__ void k_ew_records0(int n_pad, const typename Vec4T<R>::type* __restrict__ posq_s,
+                              const typename Vec4T<R>::type* __restrict__ dipt_s,
+                              typename Vec4T<R>::type* __restrict__ posq0, typename Vec4T<R>::type* __restrict__ dipt0) {
+    const int k = blockIdx.x * blockDim.x + threadIdx.x;
+    if (k >= n_pad) return;
+    typename Vec4T<R>::type p = posq_s[k], t = dipt_s[k];
+    p.w = R(0);
+    t.x = t.y = t.z = R(0);
+    posq0[k] = p;
+    dipt0[k] = t;
+}
+
 // Forces and torques in index order, per-atom energy terms (self, induction).
 // The self terms cancel the erf self-interaction that reciprocal space holds
 // for every site, so they use the same (R-rounded) charges and dipoles the
@@ -1282,7 +1297,8 @@ __global__ void k_ew_finish(int n, int n_pad, const int* __restrict__ rank, cons
                             const typename Vec4T<R>::type* __restrict__ dipt_s,
                             const typename Vec4T<R>::type* __restrict__ vec_s, const double* __restrict__ lab,
                             const double* __restrict__ pol, double alpha, double selfc, int recip,
-                            double* __restrict__ fpair, double* __restrict__ torque, double* __restrict__ epart) {
+                            double* __restrict__ fpair, double* __restrict__ torque, double* __restrict__ epart,
+                            int subtract = 0) {
     __shared__ double red[40];
     const int i = blockIdx.x * blockDim.x + threadIdx.x;
     double e = 0.0;
@@ -1305,27 +1321,37 @@ __global__ void k_ew_finish(int n, int n_pad, const int* __restrict__ rank, cons
         G[0] += selfc * t.x;
         G[1] += selfc * t.y;
         G[2] += selfc * t.z;
-        fpair[3 * i] = F[0];
-        fpair[3 * i + 1] = F[1];
-        fpair[3 * i + 2] = F[2];
-        torque[3 * i] = p.y * G[2] - p.z * G[1];
-        torque[3 * i + 1] = p.z * G[0] - p.x * G[2];
-        torque[3 * i + 2] = p.x * G[1] - p.y * G[0];
         const double q = (double)posq_s[k].w;
         e = -alpha / kSqrtPi * q * q - 2.0 * alpha * alpha * alpha / (3.0 * kSqrtPi) * dot(t, t);
-        if (pol[i] > 0.0) e += 0.5 * dot(u, u) / pol[i];
+        if (subtract) {
+            // The induced dipoles' own pass: its forces come off the total;
+            // nothing acts on the permanent dipoles, and no induction term.
+            fpair[3 * i] -= F[0];
+            fpair[3 * i + 1] -= F[1];
+            fpair[3 * i + 2] -= F[2];
+        } else {
+            fpair[3 * i] = F[0];
+            fpair[3 * i + 1] = F[1];
+            fpair[3 * i + 2] = F[2];
+            torque[3 * i] = p.y * G[2] - p.z * G[1];
+            torque[3 * i + 1] = p.z * G[0] - p.x * G[2];
+            torque[3 * i + 2] = p.x * G[1] - p.y * G[0];
+            if (pol[i] > 0.0) e += 0.5 * dot(u, u) / pol[i];
+        }
     }
     e = block_sum(e, red);
     if (threadIdx.x == 0) epart[blockIdx.x] = e;
 }
 
+// *out = s + plasma, or with subtract *out -= s + plasma.
 __global__ void k_ew_energy_sum(int n_a, const double* __restrict__ a, int n_b, const double* __restrict__ b, int n_c,
-                                const double* __restrict__ c, double plasma, double* __restrict__ out) {
+                                const double* __restrict__ c, double plasma, double* __restrict__ out,
+                                int subtract = 0) {
     __shared__ double red[40];
     double s = sum_partials(a, n_a, red);
     s += sum_partials(b, n_b, red);
     s += sum_partials(c, n_c, red);
-    if (threadIdx.x == 0) *out = s + plasma;
+    if (threadIdx.x == 0) *out = subtract ? *out - (s + plasma) : s + plasma;
 }
 
 inline int nblk(size_t n, int t) { return (int)((n + t - 1) / t); }
@@ -1404,6 +1430,10 @@ struct Ewald {
     double* rec_epart = nullptr;
     int n_rec_blk = 1;
     int launches = 0;
+    // Direct polarization: records of the induced dipoles alone (positions
+    // with charge 0, then zero permanent dipoles with the Thole factors),
+    // 2 * n_pad records of the form's precision.
+    void* rec0 = nullptr;
 
     FftGrid& energy_grid() { return precision == TDP_PRECISION_DOUBLE ? it : en64; }
 
@@ -1446,11 +1476,13 @@ void influence(Ewald* e, FftGrid& g, cudaStream_t st) {
 
 }  // namespace
 
-Ewald* ewald_create(const Dev& d, int precision, bool vacuum) {
+Ewald* ewald_create(const Dev& d, int precision, bool vacuum, bool direct) {
     Ewald* e = new Ewald();
     try {
         e->precision = precision;
         e->vacuum = vacuum;
+        if (direct)
+            e->rec0 = dalloc<char>(2 * (size_t)d.n_pad * (precision == TDP_PRECISION_DOUBLE ? 32 : 16), e->owned);
         const int nt = std::max(1, d.pp.n_tiles);
         e->cap = vacuum ? nt : std::min(nt, 2048);
         e->list = dalloc<int>((size_t)nt * e->cap, e->owned);
@@ -1550,14 +1582,17 @@ namespace {
 // Reciprocal space of one density: spread (R arithmetic), then FFT,
 // convolution and inverse FFT on grid g (element type GT).
 template <class R, class GT, int KIND>
-void pme_potential(Ewald* e, const Dev& d, FftGrid& g, bool energy, cudaStream_t st) {
+void pme_potential(Ewald* e, const Dev& d, FftGrid& g, bool energy, cudaStream_t st,
+                   const typename Vec4T<R>::type* posq = nullptr, const typename Vec4T<R>::type* dipt = nullptr) {
     typedef typename Vec4T<R>::type V4;
+    if (!posq) posq = (const V4*)d.posq_s;
+    if (!dipt) dipt = (const V4*)d.dipt_s;
     const size_t ng = (size_t)e->K[0] * e->K[1] * e->K[2];
     const size_t nc = (size_t)e->K[0] * e->K[1] * (e->K[2] / 2 + 1);
     const bool fix = sizeof(R) == 4;   // the mixed form spreads into the fixed-point grid
     if (!fix) TDP_CUDA(cudaMemsetAsync(g.real, 0, ng * sizeof(double), st));
-    k_pme_spread<R, KIND><<<nblk((size_t)d.n, 128), 128, 0, st>>>(e->G, d.n, d.pos_s, (const V4*)d.posq_s,
-                                                                   (const V4*)d.dipt_s, (const V4*)d.vec_s, e->gfix,
+    k_pme_spread<R, KIND><<<nblk((size_t)d.n, 128), 128, 0, st>>>(e->G, d.n, d.pos_s, posq, dipt,
+                                                                   (const V4*)d.vec_s, e->gfix,
                                                                    fix ? nullptr : (double*)g.real);
     e->launches++;
     if (fix) {
@@ -1631,32 +1666,59 @@ void ewald_matvec(Ewald* e, const Dev& d, cudaStream_t st) {
     TDP_CUDA(cudaGetLastError());
 }
 
+namespace {
+
+// One energy/force pass over the records (posq, dipt) and the induced dipoles
+// in vec_s.  subtract = 0: forces, torques and the energy are written;
+// subtract = 1: the pass's forces and energy come off them (no torques).
 template <class R>
-void ewald_energy(Ewald* e, const Dev& d, double total_charge, cudaStream_t st) {
+void energy_pass(Ewald* e, const Dev& d, const typename Vec4T<R>::type* posq, const typename Vec4T<R>::type* dipt,
+                 double plasma, int subtract, cudaStream_t st) {
+    typedef typename Vec4T<R>::type V4;
+    k_ew_force<R><<<d.pp.n_tiles, kEwThreads, 0, st>>>(d.pp, e->E, posq, dipt, (const V4*)d.vec_s, d.tctr_s,
+                                                       d.text_s, d.pos_s, d.exs_off, d.exs_j, d.exs_m, d.exs_s,
+                                                       e->list, e->count, d.n_pad, d.partial, e->tile_energy);
+    if (!e->vacuum) {
+        FftGrid& g = e->energy_grid();
+        pme_potential<R, double, 2>(e, d, g, true, st, posq, dipt);
+        k_pme_gather<R, double, 2, true><<<nblk((size_t)d.n_pad, 128), 128, 0, st>>>(
+            e->G, d.n, d.n_pad, e->E.selfc, d.pos_s, posq, dipt, (const V4*)d.vec_s, (const double*)g.real,
+            d.partial + 6 * (size_t)d.n_pad);
+    }
+    k_ew_finish<R><<<e->n_atom_blk, kVecThreads, 0, st>>>(d.n, d.n_pad, d.rank, d.partial, posq, dipt,
+                                                          (const V4*)d.vec_s, d.lab, d.alpha, e->alpha, e->E.selfc,
+                                                          e->vacuum ? 0 : 1, d.fpair, d.torque, e->atom_epart,
+                                                          subtract);
+    k_ew_energy_sum<<<1, kVecThreads, 0, st>>>(d.pp.n_tiles, e->tile_energy, e->n_rec_blk, e->rec_epart,
+                                               e->n_atom_blk, e->atom_epart, plasma, d.energy, subtract);
+    e->launches += e->vacuum ? 3 : 4;
+}
+
+}  // namespace
+
+template <class R>
+void ewald_energy(Ewald* e, const Dev& d, double total_charge, cudaStream_t st, bool direct) {
     typedef typename Vec4T<R>::type V4;
     e->launches = 0;
     k_ew_pack_mu<R><<<nblk((size_t)d.n, kVecThreads), kVecThreads, 0, st>>>(d.n, d.rank, d.mu, d.thole, (V4*)d.vec_s);
-    const int blocks = d.pp.n_tiles;
-    k_ew_force<R><<<blocks, kEwThreads, 0, st>>>(d.pp, e->E, (const V4*)d.posq_s, (const V4*)d.dipt_s,
-                                                 (const V4*)d.vec_s, d.tctr_s, d.text_s, d.pos_s, d.exs_off, d.exs_j, d.exs_m,
-                                                 d.exs_s, e->list, e->count, d.n_pad, d.partial, e->tile_energy);
-    if (!e->vacuum) {
-        FftGrid& g = e->energy_grid();
-        pme_potential<R, double, 2>(e, d, g, true, st);
-        k_pme_gather<R, double, 2, true><<<nblk((size_t)d.n_pad, 128), 128, 0, st>>>(
-            e->G, d.n, d.n_pad, e->E.selfc, d.pos_s, (const V4*)d.posq_s, (const V4*)d.dipt_s, (const V4*)d.vec_s,
-            (const double*)g.real, d.partial + 6 * (size_t)d.n_pad);
-    }
-    k_ew_finish<R><<<e->n_atom_blk, kVecThreads, 0, st>>>(d.n, d.n_pad, d.rank, d.partial, (const V4*)d.posq_s,
-                                                          (const V4*)d.dipt_s, (const V4*)d.vec_s, d.lab, d.alpha,
-                                                          e->alpha, e->E.selfc, e->vacuum ? 0 : 1, d.fpair, d.torque,
-                                                          e->atom_epart);
+    e->launches++;
     const double V = e->box[0] * e->box[1] * e->box[2];
     const double plasma =
         e->vacuum ? 0.0 : -kPi * total_charge * total_charge / (2.0 * V * e->alpha * e->alpha);
-    k_ew_energy_sum<<<1, kVecThreads, 0, st>>>(d.pp.n_tiles, e->tile_energy, e->n_rec_blk, e->rec_epart,
-                                               e->n_atom_blk, e->atom_epart, plasma, d.energy);
-    e->launches += 6;
+    energy_pass<R>(e, d, (const V4*)d.posq_s, (const V4*)d.dipt_s, plasma, 0, st);
+    if (direct) {
+        // Direct polarization: its functional U_perm - mu.E_M + 1/2 mu alpha^-1 mu
+        // is the Mutual one minus U(0, mu), the induced dipoles' own Ewald
+        // energy (-1/2 mu.T mu), so energy and forces are the Mutual pass's
+        // minus those of a pass over the induced dipoles alone.
+        if (!e->rec0) throw TdpError{TDP_ERR_CUDA, "Ewald mode: Direct records were not allocated"};
+        V4* posq0 = (V4*)e->rec0;
+        V4* dipt0 = posq0 + d.n_pad;
+        k_ew_records0<R><<<nblk((size_t)d.n_pad, kVecThreads), kVecThreads, 0, st>>>(
+            d.n_pad, (const V4*)d.posq_s, (const V4*)d.dipt_s, posq0, dipt0);
+        e->launches++;
+        energy_pass<R>(e, d, posq0, dipt0, 0.0, 1, st);
+    }
     TDP_CUDA(cudaGetLastError());
 }
 
@@ -1664,7 +1726,7 @@ template void ewald_fixed_field<float>(Ewald*, const Dev&, cudaStream_t);
 template void ewald_fixed_field<double>(Ewald*, const Dev&, cudaStream_t);
 template void ewald_matvec<float>(Ewald*, const Dev&, cudaStream_t);
 template void ewald_matvec<double>(Ewald*, const Dev&, cudaStream_t);
-template void ewald_energy<float>(Ewald*, const Dev&, double, cudaStream_t);
-template void ewald_energy<double>(Ewald*, const Dev&, double, cudaStream_t);
+template void ewald_energy<float>(Ewald*, const Dev&, double, cudaStream_t, bool);
+template void ewald_energy<double>(Ewald*, const Dev&, double, cudaStream_t, bool);
 
 }  // namespace tdp

@@ -15,8 +15,9 @@ struct Ewald;
 // State that does not depend on the box (neighbour list, buffers of the
 // atom-side kernels); the grid is planned by ewald_prepare.
 // vacuum: the variational NoCutoff model (alpha = 0, no cutoff, every tile
-// pair in the list, no reciprocal space).
-Ewald* ewald_create(const Dev& d, int precision, bool vacuum = false);
+// pair in the list, no reciprocal space); direct: Direct polarization (the
+// energy pass needs a second set of records).
+Ewald* ewald_create(const Dev& d, int precision, bool vacuum = false, bool direct = false);
 void ewald_destroy(Ewald* e);
 
 // Chooses alpha and the grid on the first call (alpha_in > 0 and grid_in[0] > 0
@@ -34,8 +35,11 @@ template <class R> void ewald_fixed_field(Ewald* e, const Dev& d, cudaStream_t s
 // Periodic field T v of the operand in vec_s into partial slots 0 and 1.
 template <class R> void ewald_matvec(Ewald* e, const Dev& d, cudaStream_t st);
 // Energy, forces (fpair) and torques (torque) at the converged dipoles d.mu;
-// plasma = -pi Q^2 / (2 V alpha^2) is added to the energy.
-template <class R> void ewald_energy(Ewald* e, const Dev& d, double total_charge, cudaStream_t st);
+// plasma = -pi Q^2 / (2 V alpha^2) is added to the energy.  direct: the
+// Direct-polarization functional (the Mutual one minus the induced dipoles'
+// own energy), whose forces are its gradient at mu = alpha E_M.
+template <class R> void ewald_energy(Ewald* e, const Dev& d, double total_charge, cudaStream_t st,
+                                     bool direct = false);
 // Nonzero when the last neighbour-list build overflowed a row (valid after the
 // stream has been synchronised).
 int ewald_list_overflow(const Ewald* e);
