@@ -323,48 +323,36 @@ __device__ __forceinline__ void pair_energy_lab(R dx, R dy, R dz, R r2, bool yz_
                      R(3) * (qi1 * pj0 + qj1 * pi0);
         en += rinv * qq + R(0.5) * (rv2 * t1 + rv3 * t2);
     }
-    R sx, sy, sz;
+    // V_ij = a X + rv3 P_j, V_ji = b X + rv3 P_i, Vd_ij = c X + rv3 W_j,
+    // Vd_ji = d X + rv3 W_i.  In S = m_i x V_ij + m_j x V_ji + u_i x Vd_ij +
+    // u_j x Vd_ji the rv3 terms cancel pairwise (m_i x P_j + m_j x P_i +
+    // u_i x W_j + u_j x W_i = 0 for P = m + u, W = m + (1 + kap) u), so
+    // S = K x X with K = a m_i + b m_j + c u_i + d u_j, and for the unit X
+    // S x X = (K.X) X - K.
+    const R a = rv2 * K.q - R(3) * rv3 * pj0;
+    const R b = -rv2 * I.q - R(3) * rv3 * pi0;
     {
-        const R a = rv2 * K.q - R(3) * rv3 * pj0;
         const R vx = a * xx + rv3 * pjx, vy = a * xy + rv3 * pjy, vz = a * xz + rv3 * pjz;
-        sx = I.my * vz - I.mz * vy;
-        sy = I.mz * vx - I.mx * vz;
-        sz = I.mx * vy - I.my * vx;
-        tx -= sy;
-        ty -= sz;
-        tz -= sx;
+        tx -= I.mz * vx - I.mx * vz;
+        ty -= I.mx * vy - I.my * vx;
+        tz -= I.my * vz - I.mz * vy;
     }
     {
-        const R b = -rv2 * I.q - R(3) * rv3 * pi0;
         const R vx = b * xx + rv3 * pix, vy = b * xy + rv3 * piy, vz = b * xz + rv3 * piz;
-        const R cx = K.my * vz - K.mz * vy, cy = K.mz * vx - K.mx * vz, cz = K.mx * vy - K.my * vx;
-        ux -= cy;
-        uy -= cz;
-        uz -= cx;
-        sx += cx;
-        sy += cy;
-        sz += cz;
+        ux -= K.mz * vx - K.mx * vz;
+        uy -= K.mx * vy - K.my * vx;
+        uz -= K.my * vz - K.mz * vy;
     }
-    {
-        const R wx = pjx + kap * K.ux, wy = pjy + kap * K.uy, wz = pjz + kap * K.uz;
-        const R c = rv2 * K.q - R(3) * rv3 * (pj0 + kap * uj0);
-        const R vx = c * xx + rv3 * wx, vy = c * xy + rv3 * wy, vz = c * xz + rv3 * wz;
-        sx += I.uy * vz - I.uz * vy;
-        sy += I.uz * vx - I.ux * vz;
-        sz += I.ux * vy - I.uy * vx;
-    }
-    {
-        const R wx = pix + kap * I.ux, wy = piy + kap * I.uy, wz = piz + kap * I.uz;
-        const R c = -rv2 * I.q - R(3) * rv3 * (pi0 + kap * ui0);
-        const R vx = c * xx + rv3 * wx, vy = c * xy + rv3 * wy, vz = c * xz + rv3 * wz;
-        sx += K.uy * vz - K.uz * vy;
-        sy += K.uz * vx - K.ux * vz;
-        sz += K.ux * vy - K.uy * vx;
-    }
+    const R c = rv2 * K.q - R(3) * rv3 * (pj0 + kap * uj0);
+    const R d = -rv2 * I.q - R(3) * rv3 * (pi0 + kap * ui0);
+    const R kx = a * I.mx + b * K.mx + c * I.ux + d * K.ux;
+    const R ky = a * I.my + b * K.my + c * I.uy + d * K.uy;
+    const R kz = a * I.mz + b * K.mz + c * I.uz + d * K.uz;
     const R qf2 = rv2 * qq - R(2) * rv3 * (I.q * pj0 - K.q * pi0);
-    const R fvx = rinv * (sy * xz - sz * xy) + qf2 * xx;
-    const R fvy = rinv * (sz * xx - sx * xz) + qf2 * xy;
-    const R fvz = rinv * (sx * xy - sy * xx) + qf2 * xz;
+    const R cf = rinv * (kx * xx + ky * xy + kz * xz) + qf2;
+    const R fvx = cf * xx - rinv * kx;
+    const R fvy = cf * xy - rinv * ky;
+    const R fvz = cf * xz - rinv * kz;
     fx -= fvy;
     fy -= fvz;
     fz -= fvx;

@@ -1305,7 +1305,6 @@ __device__ __forceinline__ void energy_walk_x2_fast(const PairParams& P, const d
     const f2 UIX = bc2(ui.x), UIY = bc2(ui.y), UIZ = bc2(ui.z);
     const float pix = di.x + ui.x, piy = di.y + ui.y, piz = di.z + ui.z;
     const f2 PIX = bc2(pix), PIY = bc2(piy), PIZ = bc2(piz);
-    const f2 WIX = bc2(pix + kap * ui.x), WIY = bc2(piy + kap * ui.y), WIZ = bc2(piz + kap * ui.z);
     const f2 HALF = bc2(0.5f), NTHREE = bc2(-3.0f), NTWO = bc2(-2.0f);
     f2 Lx = 0, Ly = 0, Lz = 0, Ix = 0, Iy = 0, Iz = 0, NTx = 0, NTy = 0, NTz = 0;
     if (FOLD) {
@@ -1407,60 +1406,42 @@ __device__ __forceinline__ void energy_walk_x2_fast(const PairParams& P, const d
             EN = fma2(RINV, qq, fma2(HALF, fma2(rv2, t1, mul2(rv3, t2)), EN));
         }
         const f2 rv2QJ0 = mul2(rv2, QJ0), rv2NQI0 = mul2(rv2, NQI0);
-        f2 SX, SY, SZ;
+        // S = K x X with K = a m_i + b m_j + c u_i + d u_j (pair_energy_lab):
+        // the torques need m_i x V_ij and m_j x V_ji, the force only K.
+        const f2 aJ = fma2(NR3X3, PJ0, rv2QJ0);
+        const f2 bI = fma2(NR3X3, PI0, rv2NQI0);
         {
-            // m_i x V_ij: the I torque and the first part of S.
-            const f2 aJ = fma2(NR3X3, PJ0, rv2QJ0);
+            // m_i x V_ij: the I torque.
             const f2 VX = fma2(aJ, XX, mul2(rv3, PJX)), VY = fma2(aJ, XY, mul2(rv3, PJY)),
                      VZ = fma2(aJ, XZ, mul2(rv3, PJZ));
-            cross2(MIX, MIY, MIZ, VX, VY, VZ, SX, SY, SZ);
-            TX = sub2(TX, SY);
-            TY = sub2(TY, SZ);
-            TZ = sub2(TZ, SX);
+            f2 CX, CY, CZ;
+            cross2(MIX, MIY, MIZ, VX, VY, VZ, CX, CY, CZ);
+            TX = sub2(TX, CY);
+            TY = sub2(TY, CZ);
+            TZ = sub2(TZ, CX);
         }
         {
             // m_j x V_ji: the J torque.
-            const f2 bI = fma2(NR3X3, PI0, rv2NQI0);
             const f2 VX = fma2(bI, XX, mul2(rv3, PIX)), VY = fma2(bI, XY, mul2(rv3, PIY)),
                      VZ = fma2(bI, XZ, mul2(rv3, PIZ));
-            f2 BX, BY, BZ;
-            cross2(MJX, MJY, MJZ, VX, VY, VZ, BX, BY, BZ);
-            UX = sub2(UX, BY);
-            UY = sub2(UY, BZ);
-            UZ = sub2(UZ, BX);
-            SX = add2(SX, BX);
-            SY = add2(SY, BY);
-            SZ = add2(SZ, BZ);
+            f2 CX, CY, CZ;
+            cross2(MJX, MJY, MJZ, VX, VY, VZ, CX, CY, CZ);
+            UX = sub2(UX, CY);
+            UY = sub2(UY, CZ);
+            UZ = sub2(UZ, CX);
         }
         {
-            // u_i x Vd_ij.
-            const f2 WJX = fma2(KAP, UJX, PJX), WJY = fma2(KAP, UJY, PJY), WJZ = fma2(KAP, UJZ, PJZ);
             const f2 cJ = fma2(NR3X3, fma2(KAP, UJ0, PJ0), rv2QJ0);
-            const f2 VX = fma2(cJ, XX, mul2(rv3, WJX)), VY = fma2(cJ, XY, mul2(rv3, WJY)),
-                     VZ = fma2(cJ, XZ, mul2(rv3, WJZ));
-            f2 CX, CY, CZ;
-            cross2(UIX, UIY, UIZ, VX, VY, VZ, CX, CY, CZ);
-            SX = add2(SX, CX);
-            SY = add2(SY, CY);
-            SZ = add2(SZ, CZ);
-        }
-        {
-            // u_j x Vd_ji.
             const f2 dI = fma2(NR3X3, fma2(KAP, UI0, PI0), rv2NQI0);
-            const f2 VX = fma2(dI, XX, mul2(rv3, WIX)), VY = fma2(dI, XY, mul2(rv3, WIY)),
-                     VZ = fma2(dI, XZ, mul2(rv3, WIZ));
-            f2 CX, CY, CZ;
-            cross2(UJX, UJY, UJZ, VX, VY, VZ, CX, CY, CZ);
-            SX = add2(SX, CX);
-            SY = add2(SY, CY);
-            SZ = add2(SZ, CZ);
-        }
-        {
-            f2 CX, CY, CZ;
-            cross2(SX, SY, SZ, XX, XY, XZ, CX, CY, CZ);
+            const f2 KX = fma2(aJ, MIX, fma2(bI, MJX, fma2(cJ, UIX, mul2(dI, UJX))));
+            const f2 KY = fma2(aJ, MIY, fma2(bI, MJY, fma2(cJ, UIY, mul2(dI, UJY))));
+            const f2 KZ = fma2(aJ, MIZ, fma2(bI, MJZ, fma2(cJ, UIZ, mul2(dI, UJZ))));
             const f2 qf2 = fma2(mul2(NTWO, rv3), fma2(QI0, PJ0, xneg2(mul2(QJ0, PI0))), mul2(rv2QJ0, QI0));
-            const f2 FVX = fma2(RINV, CX, mul2(qf2, XX)), FVY = fma2(RINV, CY, mul2(qf2, XY)),
-                     FVZ = fma2(RINV, CZ, mul2(qf2, XZ));
+            // f = (S x X) / r + qf2 X = (rinv K.X + qf2) X - rinv K.
+            const f2 CF = fma2(RINV, dot2(KX, KY, KZ, XX, XY, XZ), qf2);
+            const f2 NRINV = xneg2(RINV);
+            const f2 FVX = fma2(CF, XX, mul2(NRINV, KX)), FVY = fma2(CF, XY, mul2(NRINV, KY)),
+                     FVZ = fma2(CF, XZ, mul2(NRINV, KZ));
             FX = sub2(FX, FVY);
             FY = sub2(FY, FVZ);
             FZ = sub2(FZ, FVX);
