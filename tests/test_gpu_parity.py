@@ -234,3 +234,33 @@ def test_fused_warm_start_matches_separate_walks(precision, method, monkeypatch)
     # Against the oracle the mixed form adds the FP32 rounding of its pair
     # sums, here on a small total (4.9 in Coulomb-prefactor-1 units).
     assert rel_err(out["1"][0][-1][0], ref.energy) < (te if precision == "double" else 2e-5)
+
+
+@pytest.mark.parametrize("precision", ["double", "mixed"])
+def test_true_residual_check_skipped_under_drift_bound(precision, monkeypatch):
+    """Warm-started solves skip the final true-residual matvec when the drift
+    bound (a multiple of the recursive residuals' sum) is below the margin to
+    the target.  The check only confirms (it does not change the dipoles), so
+    the results equal those of solves that always take it."""
+    s = S.water_box(6, 1.8643, seed=5, cutoff=0.8, target_eps=1e-7, max_iter=2000)
+    v = np.random.default_rng(7).normal(size=s.positions.shape) * 2e-4   # nm per call
+    traj = [s.positions + k * v for k in range(6)]
+    out, mv = {}, {}
+    for flag in ("0", "1"):
+        monkeypatch.setenv("TDP_TRUE_RESIDUAL", flag)
+        with CudaCalcTholeDipoleForceKernel(s, precision=precision, warm_start=True) as k:
+            k.enableTiming(True)
+            res = []
+            mv[flag] = []
+            for p in traj:
+                res.append(k.execute(p))
+                st = k.solverStats()
+                assert st["converged"] and st["epsilon"] <= s.target_eps
+                mv[flag].append(int(k.stageTimes()[6]) - st["iterations"])
+            out[flag] = res
+    # Matvecs beyond the CG iterations: with the check forced, one per warm
+    # solve; by default none once the warm start is close.
+    assert all(m == 1 for m in mv["1"][1:]), mv
+    assert all(m == 0 for m in mv["0"][2:]), mv
+    for (e0, f0), (e1, f1) in zip(out["0"], out["1"]):
+        assert rel_err(e0, e1) < 1e-12 and rel_rms(f0, f1) < 1e-12
