@@ -730,7 +730,15 @@ def adjoint_section(stream, world, max_over_ranks, reps):
             s1.record(stream)
             torch.cuda.synchronize()
             ms = max_over_ranks(s0.elapsed_time(s1) / reps)
-            res[f"box12288_{prec}"] = {"gradients_per_s": _r(world * 1e3 / ms), "ms_per_gradient": _r(ms)}
+            s0.record(stream)
+            for _ in range(reps):
+                frc.zero_()
+                k.execute_device(pos.data_ptr(), A.F64, frc.data_ptr(), A.F64)
+            s1.record(stream)
+            torch.cuda.synchronize()
+            ms_fwd = max_over_ranks(s0.elapsed_time(s1) / reps)
+            res[f"box12288_{prec}"] = {"gradients_per_s": _r(world * 1e3 / ms), "ms_per_gradient": _r(ms),
+                                       "forward_ms": _r(ms_fwd), "adjoint_ms": _r(ms - ms_fwd)}
     clusters = [c.copy(target_eps=CLUSTER_EPS) for c in _cluster_workload(3)[:256]]
     for prec in ("double", "mixed"):
         with ClusterBatch(clusters, precision=prec) as b:
@@ -755,7 +763,14 @@ def adjoint_section(stream, world, max_over_ranks, reps):
             s1.record(stream)
             torch.cuda.synchronize()
             ms = max_over_ranks(s0.elapsed_time(s1) / reps)
-            res[f"clusters256_{prec}"] = {"batch_gradients_per_s": _r(world * 1e3 / ms), "ms_per_batch": _r(ms)}
+            s0.record(stream)
+            for _ in range(reps):
+                b.compute_device(pos.data_ptr(), frc.data_ptr(), en.data_ptr())
+            s1.record(stream)
+            torch.cuda.synchronize()
+            ms_fwd = max_over_ranks(s0.elapsed_time(s1) / reps)
+            res[f"clusters256_{prec}"] = {"batch_gradients_per_s": _r(world * 1e3 / ms), "ms_per_batch": _r(ms),
+                                          "forward_ms": _r(ms_fwd), "reverse_ms": _r(ms - ms_fwd)}
     return res
 
 

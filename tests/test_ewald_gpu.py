@@ -192,3 +192,29 @@ def test_mixed_matches_plain_at_tight_tolerance():
     assert rel_err(em, ep) < 1e-6
     assert rel_rms(fm, fp) < 2e-5
     assert rel_rms(mum, mup) < 2e-5
+
+
+@pytest.mark.parametrize("precision,te,tf", [("double", 1e-9, 1e-8), ("mixed", 5e-6, 2e-5)])
+def test_fused_start_matches_separate_walks(precision, te, tf, monkeypatch):
+    # A warm-started Ewald solve starts with one permanent-field pass over the
+    # dipole records m + mu0 (real space with the partners' M/I split,
+    # reciprocal space and self term of the sum), giving E + T mu0; along a
+    # trajectory it must match the separate permanent-field pass and matvec.
+    s = water216().copy(target_eps=1e-11 if precision == "double" else 1e-9, max_iter=2000)
+    v = np.random.default_rng(12).normal(size=s.positions.shape) * 3e-4
+    traj = [s.positions + k * v for k in range(5)]
+    out = {}
+    for fused in ("1", "0"):
+        monkeypatch.setenv("TDP_FUSED_START", fused)
+        with CudaCalcTholeDipoleForceKernel(s, precision=precision, warm_start=True, ewald=True) as k:
+            k.enableTiming(True)
+            res = []
+            for p in traj:
+                res.append(k.execute(p))
+                assert k.solverStats()["converged"]
+            out[fused] = (res, int(k.stageTimes()[10]))
+    assert out["1"][1] == 1 and out["0"][1] == 0
+    for (e1, f1), (e0, f0) in zip(out["1"][0], out["0"][0]):
+        assert rel_err(e1, e0) < te and rel_rms(f1, f0) < tf
+    ref = EW.ewald(s.copy(positions=traj[-1]))
+    assert rel_err(out["1"][0][-1][0], ref.energy) < (1e-9 if precision == "double" else 1e-6)

@@ -607,13 +607,15 @@ void setup_and_solve(tdp_handle* h) {
     // A warm-started Mutual CG solve takes the fused start: one walk with the
     // operand m + mu0 gives E + T mu0 (see solve_cg).
     const bool fused = h->polarization == TDP_MUTUAL && h->solver == TDP_SOLVER_CG &&
-                       (h->flags & TDP_FLAG_WARM_START) && h->n_hist > 0 && !h->ew && h->fused_start && d.mu0;
+                       (h->flags & TDP_FLAG_WARM_START) && h->n_hist > 0 && h->fused_start && d.mu0;
     h->e_shifted = false;
     if (h->ew) {
         const double L[3] = {h->box[0], h->box[4], h->box[8]};
         ewald_prepare(h->ew, d, L, h->cutoff, h->ewald_tol, h->pme_alpha, h->pme_grid, st);
-        ewald_fixed_field<R>(h->ew, d, st);
-        h->launches += 3 + ewald_last_launches(h->ew);
+        if (!fused) {
+            ewald_fixed_field<R>(h->ew, d, st);
+            h->launches += 3 + ewald_last_launches(h->ew);
+        }
     } else if (!fused) {
         launch_field<R>(d, 0, st);
         h->launches += 4;
@@ -638,10 +640,16 @@ void setup_and_solve(tdp_handle* h) {
                     TDP_CUDA(cudaMemcpyAsync(d.mu0, d.mu, sizeof(double) * 3 * h->n, cudaMemcpyDeviceToDevice, st));
                     launch_pack_total<R>(d, st);
                     size_t k = kernel_begin(h, 2);
-                    launch_field<R>(d, 2, st);
+                    if (h->ew) {
+                        ewald_fixed_field<R>(h->ew, d, st, d.vec_s);
+                        h->launches += ewald_last_launches(h->ew);
+                    } else {
+                        launch_field<R>(d, 2, st);
+                        h->launches += 1 + (sizeof(R) == 4 ? 1 : 0);
+                    }
                     kernel_end(h, k);
                     launch_fused_done<R>(d, st);
-                    h->launches += 4 + (sizeof(R) == 4 ? 1 : 0);
+                    h->launches += 3;
                     h->e_shifted = true;
                 } else {
                     launch_warm_start<R>(d, st);

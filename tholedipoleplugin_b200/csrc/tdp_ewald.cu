@@ -266,6 +266,9 @@ __device__ __forceinline__ void ew_field_walk(const PairParams& P, const EwParam
 
 // Exceptions of slot i (covalent partners with their M and I scales), FP64:
 // erfc part within the cutoff, minus the bare term, plus the scaled, damped term.
+// lab (KIND 0 only: the fused start of a warm-started solve, whose dipole
+// records hold P = m + mu0): the partner's mu0 = P - m gets its I scale, i.e.
+// (I - M) times the damped term of mu0 is added to the M-scaled field of P.
 template <class R, int KIND>
 __device__ __forceinline__ void ew_field_exceptions(const PairParams& P, const EwParams& E,
                                                     const double* __restrict__ pos_s,
@@ -273,7 +276,8 @@ __device__ __forceinline__ void ew_field_exceptions(const PairParams& P, const E
                                                     const typename Vec4T<R>::type* __restrict__ src,
                                                     const int* __restrict__ exs_off, const int* __restrict__ exs_j,
                                                     const double* __restrict__ exs_m, const double* __restrict__ exs_s,
-                                                    int i, double ti, double& fx, double& fy, double& fz) {
+                                                    int i, double ti, double& fx, double& fy, double& fz,
+                                                    const typename Vec4T<R>::type* __restrict__ lab = nullptr) {
     const int e0 = exs_off[i], e1 = exs_off[i + 1];
     const d3 pi = ld3(pos_s + 3 * i);
     for (int e = e0; e < e1; e++) {
@@ -295,6 +299,14 @@ __device__ __forceinline__ void ew_field_exceptions(const PairParams& P, const E
         double K1 = B1 - b1 + sc * l3 * b1, K2 = B2 - b2 + sc * l5 * b2;
         double qj = KIND == 0 ? (double)posq_s[j].w : 0.0;
         pair_field_only<double>(dx, dy, dz, qj, (double)vj.x, (double)vj.y, (double)vj.z, K1, K2, fx, fy, fz);
+        if (KIND == 0 && lab) {
+            const double ds = exs_s[e] - sc;
+            if (ds != 0.0) {
+                const typename Vec4T<R>::type mj = lab[j];
+                pair_field_only<double>(dx, dy, dz, 0.0, (double)vj.x - (double)mj.x, (double)vj.y - (double)mj.y,
+                                        (double)vj.z - (double)mj.z, ds * l3 * b1, ds * l5 * b2, fx, fy, fz);
+            }
+        }
     }
 }
 
@@ -470,7 +482,8 @@ __global__ void __launch_bounds__(kEwThreads) k_ew_field(PairParams P, EwParams 
                                                          const double* __restrict__ exs_m,
                                                          const double* __restrict__ exs_s, const int* __restrict__ list,
                                                          const int* __restrict__ count, int n_pad,
-                                                         double* __restrict__ out) {
+                                                         double* __restrict__ out,
+                                                         const typename Vec4T<R>::type* __restrict__ lab) {
     typedef typename Vec4T<R>::type V4;
     __shared__ V4 s_pos[kEwWarps][32], s_vec[kEwWarps][32];
     __shared__ EwPackedTile s_pk[sizeof(R) == 4 ? kEwWarps : 1];
@@ -556,7 +569,9 @@ __global__ void __launch_bounds__(kEwThreads) k_ew_field(PairParams P, EwParams 
         fy += s_red[w][1][lane];
         fz += s_red[w][2][lane];
     }
-    if (i < P.n) ew_field_exceptions<R, KIND>(P, E, pos_s, posq_s, src, exs_off, exs_j, exs_m, exs_s, i, (double)vi.w, fx, fy, fz);
+    if (i < P.n)
+        ew_field_exceptions<R, KIND>(P, E, pos_s, posq_s, src, exs_off, exs_j, exs_m, exs_s, i, (double)vi.w, fx, fy,
+                                     fz, lab);
     else fx = fy = fz = 0.0;
     out[i] = fx;
     out[(size_t)n_pad + i] = fy;
@@ -1619,20 +1634,23 @@ void pme_potential(Ewald* e, const Dev& d, FftGrid& g, bool energy, cudaStream_t
 }
 
 template <class R, int KIND>
-void real_field(Ewald* e, const Dev& d, const void* src, cudaStream_t st) {
+void real_field(Ewald* e, const Dev& d, const void* src, cudaStream_t st, const void* lab = nullptr) {
     typedef typename Vec4T<R>::type V4;
     const int blocks = d.pp.n_tiles;
     k_ew_field<R, KIND><<<blocks, kEwThreads, 0, st>>>(d.pp, e->E, (const V4*)d.posq_s, (const V4*)src, d.tctr_s,
                                                       d.text_s, d.pos_s, d.exs_off, d.exs_j, d.exs_m, d.exs_s, e->list, e->count,
-                                                      d.n_pad, d.partial);
+                                                      d.n_pad, d.partial, (const V4*)lab);
     e->launches++;
 }
 
 }  // namespace
 
 template <class R>
-void ewald_fixed_field(Ewald* e, const Dev& d, cudaStream_t st) {
+void ewald_fixed_field(Ewald* e, const Dev& d, cudaStream_t st, const void* operand) {
     typedef typename Vec4T<R>::type V4;
+    // The dipole records: the lab-frame permanent dipoles, or (fused start)
+    // the operand P = m + mu0, whose field is E + T mu0.
+    const V4* dip = operand ? (const V4*)operand : (const V4*)d.dipt_s;
     e->launches = 0;
     TDP_CUDA(cudaMemsetAsync(e->overflow, 0, sizeof(int), st));
     k_ew_tiles<<<(d.pp.n_tiles + kEwWarps - 1) / kEwWarps, kEwThreads, 0, st>>>(d.pp, e->E, d.tctr_s, d.text_s,
@@ -1640,12 +1658,12 @@ void ewald_fixed_field(Ewald* e, const Dev& d, cudaStream_t st) {
                                                                               e->overflow);
     TDP_CUDA(cudaMemcpyAsync(e->h_overflow, e->overflow, sizeof(int), cudaMemcpyDeviceToHost, st));
     e->launches++;
-    real_field<R, 0>(e, d, d.dipt_s, st);
+    real_field<R, 0>(e, d, dip, st, operand ? d.dipt_s : nullptr);
     TDP_CUDA(cudaGetLastError());
     if (e->vacuum) return;
-    pme_potential<R, R, 0>(e, d, e->it, false, st);
+    pme_potential<R, R, 0>(e, d, e->it, false, st, nullptr, dip);
     k_pme_gather<R, R, 0, false><<<nblk((size_t)d.n_pad, 128), 128, 0, st>>>(
-        e->G, d.n, d.n_pad, e->E.selfc, d.pos_s, (const V4*)d.posq_s, (const V4*)d.dipt_s, (const V4*)d.vec_s,
+        e->G, d.n, d.n_pad, e->E.selfc, d.pos_s, (const V4*)d.posq_s, dip, (const V4*)d.vec_s,
         (const R*)e->it.real, d.partial + 3 * (size_t)d.n_pad);
     e->launches++;
     TDP_CUDA(cudaGetLastError());
@@ -1722,8 +1740,8 @@ void ewald_energy(Ewald* e, const Dev& d, double total_charge, cudaStream_t st, 
     TDP_CUDA(cudaGetLastError());
 }
 
-template void ewald_fixed_field<float>(Ewald*, const Dev&, cudaStream_t);
-template void ewald_fixed_field<double>(Ewald*, const Dev&, cudaStream_t);
+template void ewald_fixed_field<float>(Ewald*, const Dev&, cudaStream_t, const void*);
+template void ewald_fixed_field<double>(Ewald*, const Dev&, cudaStream_t, const void*);
 template void ewald_matvec<float>(Ewald*, const Dev&, cudaStream_t);
 template void ewald_matvec<double>(Ewald*, const Dev&, cudaStream_t);
 template void ewald_energy<float>(Ewald*, const Dev&, double, cudaStream_t, bool);

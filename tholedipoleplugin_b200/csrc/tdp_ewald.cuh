@@ -31,7 +31,10 @@ void ewald_params(const Ewald* e, double* alpha, int grid[3]);
 
 // Permanent field E_M of the sorted records into partial slots 0 (real
 // space) and 1 (reciprocal + self); builds the neighbour list first.
-template <class R> void ewald_fixed_field(Ewald* e, const Dev& d, cudaStream_t st);
+// operand (the fused start of a warm-started solve): dipole records
+// P = m + mu0 in place of m, giving E_M + T mu0 (covalent partners split
+// into their M and I scales).
+template <class R> void ewald_fixed_field(Ewald* e, const Dev& d, cudaStream_t st, const void* operand = nullptr);
 // Periodic field T v of the operand in vec_s into partial slots 0 and 1.
 template <class R> void ewald_matvec(Ewald* e, const Dev& d, cudaStream_t st);
 // Energy, forces (fpair) and torques (torque) at the converged dipoles d.mu;
