@@ -69,7 +69,15 @@ extern "C" {
  * RMS change a Jacobi step would make, sqrt(sum|alpha(E+T mu)-mu|^2 / N)
  * (ReferenceTholeDipoleForce.cpp:838-846), below the target epsilon.
  *  CG    : conjugate gradients on the symmetric (alpha^-1 - T) system
- *          (Jacobi-preconditioned), converging to the same fixed point.
+ *          (Jacobi-preconditioned), converging to the same fixed point.  In
+ *          the minimum-image PME mode (not TDP_FLAG_EWALD) each residual is
+ *          also preconditioned by three CG iterations on the Ewald operator
+ *          of the same box (real space within max(0.6 nm, the 1e-12 damping
+ *          range), PME tolerance 1e-3, plus the minimum-image cube's uniform
+ *          depolarising field -4 pi M / 3V), with flexible directions; a box
+ *          edge below twice that cutoff runs unpreconditioned.  At create,
+ *          TDP_PRECOND=0 keeps plain CG and TDP_PRECOND_INNER sets the inner
+ *          iterations (1-8).
  *  JACOBI: the reference's own fixed-point iteration, step for step. */
 #define TDP_SOLVER_CG 0
 #define TDP_SOLVER_JACOBI 1
@@ -316,8 +324,10 @@ int tdp_adjoint_device(tdp_handle* h, const double* dL_dF, double dL_dE, double*
  * [8] energy/force kernel ms, [9] kernel launches of the call,
  * [10] fused-start walks (0 or 1: a warm-started solve's single walk giving
  * the permanent field plus the starting matvec), [11] their kernel ms.  The
- * fused walk is counted in neither [6] nor [7]. */
-#define TDP_NUM_STAGE_TIMES 12
+ * fused walk is counted in neither [6] nor [7].  [12] preconditioner
+ * applications of the minimum-image CG (each a few matvecs of the Ewald
+ * operator of the same box), [13] their ms (counted in neither [6] nor [7]). */
+#define TDP_NUM_STAGE_TIMES 14
 int tdp_enable_timing(tdp_handle* h, int32_t enable);
 int tdp_stage_times(const tdp_handle* h, double* out);
 

@@ -26,7 +26,7 @@ FLAG_DD_FORCE_R4 = 1 << 0
 FLAG_WARM_START = 1 << 1
 FLAG_EWALD = 1 << 2
 FLAG_VARIATIONAL = 1 << 3
-NUM_STAGE_TIMES = 12
+NUM_STAGE_TIMES = 14
 COMPUTE_FORCES, COMPUTE_ENERGY, COMPUTE_REQUIRE_CONVERGENCE = 1, 2, 4
 F64, F32 = 0, 1
 DIPOLES_INDUCED, DIPOLES_LAB_PERMANENT, DIPOLES_TOTAL = 0, 1, 2

@@ -13,7 +13,7 @@ ROOT = os.path.dirname(HERE)
 CSRC = os.path.join(HERE, "csrc")
 LIB = os.path.join(HERE, "libtholedipole_b200.so")
 SOURCES = ["tdp_kernels.cu", "tdp_sym.cu", "tdp_ewald.cu", "tdp_capi.cu", "tdp_md.cu", "tdp_noalloc.cu",
-           "tdp_adjoint.cu", "tdp_batch.cu"]
+           "tdp_adjoint.cu", "tdp_batch.cu", "tdp_precond.cu"]
 # Sources whose FP32 pair arithmetic is compiled with subnormal flushing.
 FTZ = {"tdp_kernels.cu", "tdp_sym.cu", "tdp_ewald.cu", "tdp_batch.cu"}
 ARCH = ["-gencode", "arch=compute_100a,code=sm_100a"]

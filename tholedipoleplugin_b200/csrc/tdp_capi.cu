@@ -7,6 +7,7 @@
 // platforms/reference/src/ReferenceTholeDipoleKernels.cpp).
 #include "tholedipole_b200.h"
 #include "tdp_ewald.cuh"
+#include "tdp_precond.cuh"
 #include "tdp_host.h"
 #include "tdp_kernels.cuh"
 
@@ -92,13 +93,17 @@ struct tdp_handle {
     bool timing = false;
     cudaEvent_t ev[6] = {nullptr, nullptr, nullptr, nullptr, nullptr, nullptr};
     std::vector<cudaEvent_t> kev;  // event pairs around matvec / energy kernels
-    std::vector<int> kev_kind;     // 0 matvec, 1 energy, 2 fused start, per pair
+    std::vector<int> kev_kind;     // 0 matvec, 1 energy, 2 fused start, 3 preconditioner, per pair
     size_t kev_used = 0;
     double stage_ms[TDP_NUM_STAGE_TIMES] = {};
     long launches = 0;
 
     // Ewald mode (TDP_FLAG_EWALD): neighbour list, PME grid and plans.
     Ewald* ew = nullptr;
+    // Minimum-image Mutual CG: the Ewald-operator preconditioner
+    // (tdp_precond.cuh), used whenever the box holds twice its cutoff.
+    Precond* pre = nullptr;
+    int pre_applications = 0;   // B matvecs of the last evaluation
     double total_charge = 0.0;
 
     // Device scratch of the device-side parameter update and the adjoint's
@@ -425,7 +430,7 @@ void record(tdp_handle* h, int k) {
 }
 
 // Event pair around one pair-kernel launch (kind 0: matvec, 1: energy, 2:
-// fused start).
+// fused start, 3: one preconditioner application).
 size_t kernel_begin(tdp_handle* h, int kind) {
     if (!h->timing) return 0;
     size_t k = h->kev_used++;
@@ -481,9 +486,21 @@ void matvec(tdp_handle* h) {
 // one matvec); TDP_TRUE_RESIDUAL=1 at create keeps it on every solve.
 constexpr double kDriftPerStep = 1e-5;
 template <class R>
+void solve_pcg(tdp_handle* h, bool fused);
+template <class R>
 void solve_cg(tdp_handle* h, bool fused = false) {
     Dev& d = h->d;
     cudaStream_t st = h->stream;
+    if (h->pre) {
+        const double L[3] = {h->box[0], h->box[4], h->box[8]};
+        const double rc2 = 2.0 * precond_cutoff(h->pre);
+        if (L[0] >= rc2 && L[1] >= rc2 && L[2] >= rc2) {
+            precond_prepare(h->pre, d, L, st);
+            h->launches += 1;
+            solve_pcg<R>(h, fused);
+            return;
+        }
+    }
     const int cap = h->max_iter;
     int slot = 0;
     // Residual of the starting point (mu = alpha E, or the previous solution).
@@ -529,6 +546,78 @@ void solve_cg(tdp_handle* h, bool fused = false) {
         h->launches += 3;
         slot++;
         it++;
+        eps = read_scalar(h, d.scal_eps + slot);
+        eps_sum += eps;
+        is_true = false;
+    }
+    launch_cg_mu<R>(d, st);
+    h->launches += 1;
+    h->iterations = it;
+    h->epsilon = eps;
+    h->converged = (h->status == TDP_STATUS_CONVERGED) ? 1 : 0;
+}
+
+// solve_cg preconditioned by the Ewald operator of the same box
+// (tdp_precond.cuh): the same start, stopping test, drift bound and
+// true-residual check; every iteration first applies z = M(r) and steps along
+// the flexible direction p = z + beta p.  The residual r and its stopping
+// quantity are the unpreconditioned ones, so the converged dipoles are the
+// same fixed point.
+template <class R>
+void solve_pcg(tdp_handle* h, bool fused) {
+    Dev& d = h->d;
+    cudaStream_t st = h->stream;
+    const int cap = h->max_iter;
+    int slot = 0;
+    if (fused) {
+        launch_cg_residual<R>(d, st, false);
+    } else {
+        matvec<R>(h);
+        launch_cg_residual<R>(d, st);
+    }
+    launch_cg_p<R>(d, -1, slot, st);
+    h->launches += 2;
+    double eps = read_scalar(h, d.scal_eps + slot);
+    double eps_sum = eps;
+    bool is_true = true, first = true;
+    int it = 0;
+    h->status = TDP_STATUS_MAX_ITERATIONS;
+    while (true) {
+        if (!std::isfinite(eps)) {
+            h->status = TDP_STATUS_NON_FINITE;
+            break;
+        }
+        if (eps <= h->target_eps || it >= cap || (size_t)slot + 3 >= h->nscal) {
+            const bool drift_ok = eps <= h->target_eps && !h->always_true_residual &&
+                                  kDriftPerStep * eps_sum <= h->target_eps - eps;
+            if (!is_true && !drift_ok) {
+                launch_cg_mu<R>(d, st, fused ? d.mu0 : nullptr);
+                matvec<R>(h);
+                launch_cg_residual<R>(d, st);
+                launch_cg_p<R>(d, -1, ++slot, st);
+                h->launches += 3;
+                eps = read_scalar(h, d.scal_eps + slot);
+                eps_sum = eps;
+                is_true = true;
+                first = true;   // restart the directions from the true residual
+                continue;
+            }
+            if (eps <= h->target_eps) h->status = TDP_STATUS_CONVERGED;
+            break;
+        }
+        size_t k = kernel_begin(h, 3);
+        precond_apply<R>(h->pre, d, slot, first, st);
+        kernel_end(h, k);
+        h->launches += precond_last_launches(h->pre);
+        h->pre_applications++;
+        matvec<R>(h);
+        launch_cg_q(d, st);
+        launch_cg_update(d, slot, st);
+        launch_cg_p<R>(d, -1, slot + 1, st);
+        h->launches += 3;
+        slot++;
+        it++;
+        first = false;
         eps = read_scalar(h, d.scal_eps + slot);
         eps_sum += eps;
         is_true = false;
@@ -599,6 +688,7 @@ void setup_and_solve(tdp_handle* h) {
     h->matvecs = 0;
     h->launches = 0;
     h->kev_used = 0;
+    h->pre_applications = 0;
     if (d.fix_err) TDP_CUDA(cudaMemsetAsync(d.fix_err, 0, sizeof(int), st));
     record(h, 0);
     launch_pack<R>(d, st);
@@ -709,17 +799,20 @@ void finish_timing(tdp_handle* h) {
     TDP_CUDA(cudaEventElapsedTime(&ms, h->ev[0], h->ev[5]));
     h->stage_ms[5] = ms;
     h->stage_ms[6] = h->matvecs;
-    double mv = 0.0, en = 0.0, fu = 0.0;
+    double mv = 0.0, en = 0.0, fu = 0.0, pc = 0.0;
     int nfu = 0;
     for (size_t k = 0; k < h->kev_used; k++) {
         TDP_CUDA(cudaEventElapsedTime(&ms, h->kev[2 * k], h->kev[2 * k + 1]));
         if (h->kev_kind[k] == 0) mv += ms;
         else if (h->kev_kind[k] == 1) en += ms;
+        else if (h->kev_kind[k] == 3) pc += ms;
         else {
             fu += ms;
             nfu++;
         }
     }
+    h->stage_ms[12] = h->pre_applications;
+    h->stage_ms[13] = pc;
     h->stage_ms[7] = mv;
     h->stage_ms[8] = en;
     h->stage_ms[9] = (double)h->launches;
@@ -736,6 +829,8 @@ void enqueue_flags(tdp_handle* h) {
 void check_flags(tdp_handle* h) {
     if (h->ew && ewald_list_overflow(h->ew))
         throw TdpError{TDP_ERR_CUDA, "Ewald mode: a neighbour-tile list row overflowed its capacity"};
+    if (h->pre && precond_list_overflow(h->pre))
+        throw TdpError{TDP_ERR_CUDA, "CG preconditioner: a neighbour-tile list row overflowed its capacity"};
     if (h->d.fix_err && *h->h_fixerr)
         throw TdpError{TDP_ERR_NON_FINITE,
                        "a field or force sum is not finite or exceeds the fixed-point accumulator range "
@@ -1168,6 +1263,25 @@ int tdp_create(const tdp_system_desc* desc, tdp_handle** out) {
         upload_params(h);
         if (ewald || variational)
             h->ew = ewald_create(d, h->precision, variational, h->polarization == TDP_DIRECT);
+        // Minimum-image Mutual CG: preconditioned by the Ewald operator of the
+        // same box (tdp_precond.cuh).  Its real space stops at 0.6 nm or where
+        // the Thole damping of every pair is below 1e-12, whichever is longer;
+        // PME tolerance 1e-3; three inner iterations per application.
+        // TDP_PRECOND=0 at create keeps the unpreconditioned CG;
+        // TDP_PRECOND_INNER sets the inner iterations (1-8).
+        bool want_pre = h->method == TDP_PME && !ewald && h->polarization == TDP_MUTUAL &&
+                        h->solver == TDP_SOLVER_CG && n > 0;
+        if (const char* e = getenv("TDP_PRECOND"))
+            if (atoi(e) == 0) want_pre = false;
+        if (want_pre) {
+            double tmax = 0.0;
+            for (double t : h->thole) tmax = std::max(tmax, std::isfinite(t) ? t : 0.0);
+            const double rc = std::max(0.6, 1.001 * std::cbrt(27.631021115928547 * std::pow(tmax, 5.0)));
+            int inner = 3;
+            if (const char* e = getenv("TDP_PRECOND_INNER")) inner = std::min(std::max(atoi(e), 1), 8);
+            d.scal_a = dalloc<double>(nscal, o);
+            h->pre = precond_create(d, h->precision, rc, 1e-3, inner);
+        }
         TDP_CUDA(cudaMallocHost(&h->h_scal, 64 * sizeof(double)));
         TDP_CUDA(cudaMallocHost(&h->h_fixerr, sizeof(int)));
         *h->h_fixerr = 0;
@@ -1192,6 +1306,7 @@ int tdp_create(const tdp_system_desc* desc, tdp_handle** out) {
 void tdp_destroy(tdp_handle* h) {
     if (!h) return;
     if (h->ew) ewald_destroy(h->ew);
+    if (h->pre) precond_destroy(h->pre);
     for (void* p : h->owned) cudaFree(p);
     if (h->h_scal) cudaFreeHost(h->h_scal);
     if (h->h_fixerr) cudaFreeHost(h->h_fixerr);

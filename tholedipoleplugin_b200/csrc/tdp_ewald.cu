@@ -1645,6 +1645,15 @@ void real_field(Ewald* e, const Dev& d, const void* src, cudaStream_t st, const 
 
 }  // namespace
 
+void ewald_build_list(Ewald* e, const Dev& d, cudaStream_t st) {
+    TDP_CUDA(cudaMemsetAsync(e->overflow, 0, sizeof(int), st));
+    k_ew_tiles<<<(d.pp.n_tiles + kEwWarps - 1) / kEwWarps, kEwThreads, 0, st>>>(d.pp, e->E, d.tctr_s, d.text_s,
+                                                                              d.exs_tiles, e->list, e->count,
+                                                                              e->overflow);
+    TDP_CUDA(cudaMemcpyAsync(e->h_overflow, e->overflow, sizeof(int), cudaMemcpyDeviceToHost, st));
+    e->launches++;
+}
+
 template <class R>
 void ewald_fixed_field(Ewald* e, const Dev& d, cudaStream_t st, const void* operand) {
     typedef typename Vec4T<R>::type V4;
@@ -1652,12 +1661,7 @@ void ewald_fixed_field(Ewald* e, const Dev& d, cudaStream_t st, const void* oper
     // the operand P = m + mu0, whose field is E + T mu0.
     const V4* dip = operand ? (const V4*)operand : (const V4*)d.dipt_s;
     e->launches = 0;
-    TDP_CUDA(cudaMemsetAsync(e->overflow, 0, sizeof(int), st));
-    k_ew_tiles<<<(d.pp.n_tiles + kEwWarps - 1) / kEwWarps, kEwThreads, 0, st>>>(d.pp, e->E, d.tctr_s, d.text_s,
-                                                                              d.exs_tiles, e->list, e->count,
-                                                                              e->overflow);
-    TDP_CUDA(cudaMemcpyAsync(e->h_overflow, e->overflow, sizeof(int), cudaMemcpyDeviceToHost, st));
-    e->launches++;
+    ewald_build_list(e, d, st);
     real_field<R, 0>(e, d, dip, st, operand ? d.dipt_s : nullptr);
     TDP_CUDA(cudaGetLastError());
     if (e->vacuum) return;

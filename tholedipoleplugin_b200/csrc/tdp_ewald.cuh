@@ -29,6 +29,9 @@ void ewald_prepare(Ewald* e, const Dev& d, const double box[3], double cutoff, d
                    const int grid_in[3], cudaStream_t st);
 void ewald_params(const Ewald* e, double* alpha, int grid[3]);
 
+// Neighbour list of the sorted tiles within the cutoff (part of
+// ewald_fixed_field; alone for a caller that only runs matvecs).
+void ewald_build_list(Ewald* e, const Dev& d, cudaStream_t st);
 // Permanent field E_M of the sorted records into partial slots 0 (real
 // space) and 1 (reciprocal + self); builds the neighbour list first.
 // operand (the fused start of a warm-started solve): dipole records

@@ -316,13 +316,16 @@ __global__ void k_cg_q(int n, const int* __restrict__ rank, int nsplit, int n_pa
 }
 
 // a = rr/pq; y += a p; r -= a q; block partials of r.r and sum alpha|r|^2.
+// scal_a (may be NULL) keeps a for the flexible beta of a preconditioned solve.
 __global__ void k_cg_update(int n, int nblk, const double* __restrict__ scal_rr, int slot,
                             const double* __restrict__ pq_part, const double* __restrict__ salpha,
                             const double* __restrict__ p, const double* __restrict__ q, double* __restrict__ y,
-                            double* __restrict__ r, double* __restrict__ rr_part, double* __restrict__ eps_part) {
+                            double* __restrict__ r, double* __restrict__ rr_part, double* __restrict__ eps_part,
+                            double* __restrict__ scal_a) {
     __shared__ double red[40];
     double pq = sum_partials(pq_part, nblk, red);
     double a = scal_rr[slot] / pq;
+    if (scal_a && blockIdx.x == 0 && threadIdx.x == 0) scal_a[slot] = a;
     int i = blockIdx.x * blockDim.x + threadIdx.x;
     double rr = 0.0, ee = 0.0;
     if (i < n) {
@@ -730,7 +733,7 @@ void launch_cg_q(const Dev& d, cudaStream_t st) {
 }
 void launch_cg_update(const Dev& d, int slot, cudaStream_t st) {
     k_cg_update<<<d.nvb, kVecThreads, 0, st>>>(d.n, d.nvb, d.scal_rr, slot, d.pq_part, d.salpha, d.p, d.q, d.y, d.r,
-                                               d.rr_part, d.eps_part);
+                                               d.rr_part, d.eps_part, d.scal_a);
 }
 template <class R>
 void launch_cg_p(const Dev& d, int prev, int slot, cudaStream_t st) {

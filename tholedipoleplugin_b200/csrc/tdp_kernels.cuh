@@ -86,6 +86,7 @@ struct Dev {
     double* pq_part = nullptr;
     double* scal_rr = nullptr;   // per-iteration scalars
     double* scal_eps = nullptr;
+    double* scal_a = nullptr;    // CG step sizes by slot (preconditioned solves only)
     double* coef = nullptr;      // extrapolation coefficients
 };
 
