@@ -298,6 +298,15 @@ int tdp_get_pme_parameters(const tdp_handle* h, double* alpha, int32_t* nx, int3
 int tdp_solver_stats(const tdp_handle* h, int32_t* iterations, double* epsilon, int32_t* converged,
                      int32_t* status);
 
+/* The stopping quantity of every step of the last Mutual CG or Jacobi solve
+ * (the RMS change a Jacobi step would make, as tdp_solver_stats reports the
+ * final one), oldest first: the start, then one per iteration and one per
+ * true-residual check.  Copies min(capacity, *count) values into eps_out
+ * (host doubles); *count receives the number available (0 after Direct or
+ * Extrapolated polarization).  No reference counterpart: a convergence
+ * monitor of this library's solvers. */
+int tdp_solver_history(tdp_handle* h, double* eps_out, int32_t capacity, int32_t* count);
+
 /* Reverse mode of the last tdp_compute (its positions and parameters):
  * gradients of  L = dL_dE * E + sum_i dL_dF_i . F_i  (F the total force,
  * torque mapping included) with respect to every particle's charge,

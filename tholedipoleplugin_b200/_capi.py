@@ -80,6 +80,7 @@ PROTOTYPES = {
                                         C.c_int32, _dp, C.c_void_p, C.c_void_p]),
     "tdp_get_pme_parameters": (C.c_int, [C.c_void_p, _dp, _ip, _ip, _ip]),
     "tdp_solver_stats": (C.c_int, [C.c_void_p, _ip, _dp, _ip, _ip]),
+    "tdp_solver_history": (C.c_int, [C.c_void_p, _dp, C.c_int32, _ip]),
     "tdp_adjoint": (C.c_int, [C.c_void_p, C.c_void_p, C.c_double, _dp]),
     "tdp_adjoint_device": (C.c_int, [C.c_void_p, C.c_void_p, C.c_double, C.c_void_p]),
     "tdp_update_particle_params": (C.c_int, [C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p,

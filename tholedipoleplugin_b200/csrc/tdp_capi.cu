@@ -89,6 +89,7 @@ struct tdp_handle {
     int status = TDP_STATUS_CONVERGED;
     int matvecs = 0;
     size_t nscal = 0;  // capacity of the per-iteration scalar arrays
+    int eps_slots = 0; // stopping quantities the last CG / Jacobi solve left in d.scal_eps
 
     bool timing = false;
     cudaEvent_t ev[6] = {nullptr, nullptr, nullptr, nullptr, nullptr, nullptr};
@@ -552,6 +553,7 @@ void solve_cg(tdp_handle* h, bool fused = false) {
     }
     launch_cg_mu<R>(d, st);
     h->launches += 1;
+    h->eps_slots = slot + 1;
     h->iterations = it;
     h->epsilon = eps;
     h->converged = (h->status == TDP_STATUS_CONVERGED) ? 1 : 0;
@@ -624,6 +626,7 @@ void solve_pcg(tdp_handle* h, bool fused) {
     }
     launch_cg_mu<R>(d, st);
     h->launches += 1;
+    h->eps_slots = slot + 1;
     h->iterations = it;
     h->epsilon = eps;
     h->converged = (h->status == TDP_STATUS_CONVERGED) ? 1 : 0;
@@ -645,6 +648,7 @@ void solve_jacobi(tdp_handle* h) {
         if (!std::isfinite(eps)) break;
     }
     h->iterations = it;
+    h->eps_slots = it;
     h->epsilon = eps;
     h->converged = eps < h->target_eps ? 1 : 0;
     h->status = std::isfinite(eps) ? (h->converged ? TDP_STATUS_CONVERGED : TDP_STATUS_MAX_ITERATIONS)
@@ -689,6 +693,7 @@ void setup_and_solve(tdp_handle* h) {
     h->launches = 0;
     h->kev_used = 0;
     h->pre_applications = 0;
+    h->eps_slots = 0;
     if (d.fix_err) TDP_CUDA(cudaMemsetAsync(d.fix_err, 0, sizeof(int), st));
     record(h, 0);
     launch_pack<R>(d, st);
@@ -1654,6 +1659,21 @@ int tdp_solver_stats(const tdp_handle* h, int32_t* iterations, double* epsilon, 
     if (epsilon) *epsilon = h->epsilon;
     if (converged) *converged = h->converged;
     if (status) *status = h->status;
+    return TDP_OK;
+}
+
+int tdp_solver_history(tdp_handle* h, double* eps_out, int32_t capacity, int32_t* count) {
+    if (!h || (capacity > 0 && !eps_out)) return TDP_ERR_INVALID_ARGUMENT;
+    try {
+        const int m = std::min(std::max(capacity, 0), h->eps_slots);
+        if (m > 0) {
+            TDP_CUDA(cudaStreamSynchronize(h->stream));
+            TDP_CUDA(cudaMemcpy(eps_out, h->d.scal_eps, sizeof(double) * m, cudaMemcpyDeviceToHost));
+        }
+        if (count) *count = h->eps_slots;
+    } catch (const TdpError& e) {
+        return fail(h, e);
+    }
     return TDP_OK;
 }
 

@@ -267,6 +267,15 @@ class CudaCalcTholeDipoleForceKernel:
         self._check(self._lib.tdp_solver_stats(self._h, C.byref(it), C.byref(eps), C.byref(conv), C.byref(st)))
         return {"iterations": it.value, "epsilon": eps.value, "converged": conv.value, "status": st.value}
 
+    def solverHistory(self) -> np.ndarray:
+        """Stopping quantity at every step of the last Mutual solve (start,
+        iterations, true-residual checks), oldest first."""
+        cnt = C.c_int32()
+        self._check(self._lib.tdp_solver_history(self._h, None, 0, C.byref(cnt)))
+        out = np.zeros(max(cnt.value, 1))
+        self._check(self._lib.tdp_solver_history(self._h, _dptr(out), cnt.value, C.byref(cnt)))
+        return out[:cnt.value]
+
     def stageTimes(self) -> Sequence[float]:
         out = np.zeros(A.NUM_STAGE_TIMES)
         self._check(self._lib.tdp_stage_times(self._h, _dptr(out)))
