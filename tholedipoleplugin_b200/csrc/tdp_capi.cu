@@ -487,9 +487,11 @@ void matvec(tdp_handle* h) {
 // one matvec); TDP_TRUE_RESIDUAL=1 at create keeps it on every solve.
 constexpr double kDriftPerStep = 1e-5;
 template <class R>
-void solve_pcg(tdp_handle* h, bool fused);
+void solve_pcg(tdp_handle* h, bool fused, bool cold);
+// cold: the solve starts from y = sqrt(alpha) E (no warm start), which the
+// preconditioned form replaces by y = M(sqrt(alpha) E).
 template <class R>
-void solve_cg(tdp_handle* h, bool fused = false) {
+void solve_cg(tdp_handle* h, bool fused = false, bool cold = true) {
     Dev& d = h->d;
     cudaStream_t st = h->stream;
     if (h->pre) {
@@ -498,7 +500,7 @@ void solve_cg(tdp_handle* h, bool fused = false) {
         if (L[0] >= rc2 && L[1] >= rc2 && L[2] >= rc2) {
             precond_prepare(h->pre, d, L, st);
             h->launches += 1;
-            solve_pcg<R>(h, fused);
+            solve_pcg<R>(h, fused, cold && !fused);
             return;
         }
     }
@@ -564,9 +566,11 @@ void solve_cg(tdp_handle* h, bool fused = false) {
 // true-residual check; every iteration first applies z = M(r) and steps along
 // the flexible direction p = z + beta p.  The residual r and its stopping
 // quantity are the unpreconditioned ones, so the converged dipoles are the
-// same fixed point.
+// same fixed point.  A cold solve starts from y = M(b), b = sqrt(alpha) E,
+// instead of y = b: that costs one preconditioner application and saves about
+// one outer iteration.
 template <class R>
-void solve_pcg(tdp_handle* h, bool fused) {
+void solve_pcg(tdp_handle* h, bool fused, bool cold) {
     Dev& d = h->d;
     cudaStream_t st = h->stream;
     const int cap = h->max_iter;
@@ -574,6 +578,13 @@ void solve_pcg(tdp_handle* h, bool fused) {
     if (fused) {
         launch_cg_residual<R>(d, st, false);
     } else {
+        if (cold) {
+            size_t k = kernel_begin(h, 3);
+            precond_cold_start<R>(h->pre, d, st);
+            kernel_end(h, k);
+            h->launches += precond_last_launches(h->pre);
+            h->pre_applications++;
+        }
         matvec<R>(h);
         launch_cg_residual<R>(d, st);
     }
@@ -751,7 +762,7 @@ void setup_and_solve(tdp_handle* h) {
                 }
                 h->launches += 1;
             }
-            solve_cg<R>(h, fused);
+            solve_cg<R>(h, fused, !((h->flags & TDP_FLAG_WARM_START) && h->n_hist > 0));
         }
         const bool ok = h->status == TDP_STATUS_CONVERGED;
         // The oldest buffer takes this solution and moves to the front.

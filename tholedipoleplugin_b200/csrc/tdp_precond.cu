@@ -201,6 +201,37 @@ __global__ void k_pcg_p(int n, const int* __restrict__ rank, int nvb, int slot, 
     pack_vec<R>(vec, rank[i], pv * salpha[i], thole[i]);
 }
 
+// Cold start, first half: r = b = sqrt(alpha) E (the residual of y = 0) and
+// block partials of r.r for the scale of the inner solve.
+__global__ void k_pc_rhs(int n, const double* __restrict__ salpha, const double* __restrict__ E,
+                         double* __restrict__ r, double* __restrict__ rr_part) {
+    __shared__ double red[40];
+    const int i = blockIdx.x * blockDim.x + threadIdx.x;
+    double rr = 0.0;
+    if (i < n) {
+        const d3 b = ld3(E + 3 * i) * salpha[i];
+        st3(r, i, b);
+        rr = dot(b, b);
+    }
+    rr = block_sum(rr, red);
+    if (threadIdx.x == 0) rr_part[blockIdx.x] = rr;
+}
+
+// Cold start, second half: y = z = M(b); mu = sqrt(alpha) y packed as the
+// operand of the residual's matvec.
+template <class R>
+__global__ void k_pc_take(int n, const int* __restrict__ rank, const double* __restrict__ salpha,
+                          const double* __restrict__ thole, const double* __restrict__ z, double* __restrict__ y,
+                          double* __restrict__ mu, typename Vec4T<R>::type* __restrict__ vec) {
+    const int i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= n) return;
+    const d3 zv = ld3(z + 3 * i);
+    st3(y, i, zv);
+    const d3 m = zv * salpha[i];
+    st3(mu, i, m);
+    pack_vec<R>(vec, rank[i], m, thole[i]);
+}
+
 }  // namespace
 
 struct Precond {
@@ -255,8 +286,12 @@ void precond_prepare(Precond* p, const Dev& d, const double box[3], cudaStream_t
     ewald_build_list(p->ew, d, st);
 }
 
+namespace {
+
+// z = M(r) from d.r (r.r block partials in d.rr_part); with first = false
+// also the partials of z.q for the flexible beta.  Returns the launches.
 template <class R>
-void precond_apply(Precond* p, const Dev& d, int slot, bool first, cudaStream_t st) {
+int inner_solve(Precond* p, const Dev& d, bool first, cudaStream_t st) {
     typedef typename Vec4T<R>::type V4;
     const int nvb = d.nvb;
     V4* vec = (V4*)d.vec_s;
@@ -279,8 +314,28 @@ void precond_apply(Precond* p, const Dev& d, int slot, bool first, cudaStream_t 
             launches++;
         }
     }
-    k_pcg_p<R><<<nvb, kVecThreads, 0, st>>>(d.n, d.rank, nvb, slot, first ? 1 : 0, p->part, d.scal_rr, d.scal_a,
-                                            d.salpha, d.thole, p->z, d.p, vec);
+    return launches;
+}
+
+}  // namespace
+
+template <class R>
+void precond_apply(Precond* p, const Dev& d, int slot, bool first, cudaStream_t st) {
+    typedef typename Vec4T<R>::type V4;
+    int launches = inner_solve<R>(p, d, first, st);
+    k_pcg_p<R><<<d.nvb, kVecThreads, 0, st>>>(d.n, d.rank, d.nvb, slot, first ? 1 : 0, p->part, d.scal_rr, d.scal_a,
+                                              d.salpha, d.thole, p->z, d.p, (V4*)d.vec_s);
+    launches++;
+    TDP_CUDA(cudaGetLastError());
+    p->launches = launches;
+}
+
+template <class R>
+void precond_cold_start(Precond* p, const Dev& d, cudaStream_t st) {
+    typedef typename Vec4T<R>::type V4;
+    k_pc_rhs<<<d.nvb, kVecThreads, 0, st>>>(d.n, d.salpha, d.E, d.r, d.rr_part);
+    int launches = 1 + inner_solve<R>(p, d, true, st);
+    k_pc_take<R><<<d.nvb, kVecThreads, 0, st>>>(d.n, d.rank, d.salpha, d.thole, p->z, d.y, d.mu, (V4*)d.vec_s);
     launches++;
     TDP_CUDA(cudaGetLastError());
     p->launches = launches;
@@ -291,5 +346,7 @@ int precond_list_overflow(const Precond* p) { return ewald_list_overflow(p->ew);
 
 template void precond_apply<float>(Precond*, const Dev&, int, bool, cudaStream_t);
 template void precond_apply<double>(Precond*, const Dev&, int, bool, cudaStream_t);
+template void precond_cold_start<float>(Precond*, const Dev&, cudaStream_t);
+template void precond_cold_start<double>(Precond*, const Dev&, cudaStream_t);
 
 }  // namespace tdp

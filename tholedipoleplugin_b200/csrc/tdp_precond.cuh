@@ -41,6 +41,10 @@ void precond_prepare(Precond* p, const Dev& d, const double box[3], cudaStream_t
 // p = z (first) or z + beta p with the flexible beta from d.q, scal_a[slot-1]
 // and scal_rr[slot-1]; packs sqrt(alpha) p as the next matvec operand.
 template <class R> void precond_apply(Precond* p, const Dev& d, int slot, bool first, cudaStream_t st);
+// Starting point of a cold solve: y = M(b) for b = sqrt(alpha) E (instead of
+// y = b), with mu = sqrt(alpha) y packed for the residual's matvec.  Uses d.r
+// and d.rr_part as scratch.
+template <class R> void precond_cold_start(Precond* p, const Dev& d, cudaStream_t st);
 // Kernel launches of the last application (cuFFT's own not counted).
 int precond_last_launches(const Precond* p);
 // Nonzero when the last neighbour-list build overflowed (after a sync).
