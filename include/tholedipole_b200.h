@@ -74,10 +74,12 @@ extern "C" {
  *          also preconditioned by three CG iterations on the Ewald operator
  *          of the same box (real space within max(0.6 nm, the 1e-12 damping
  *          range), PME tolerance 1e-3, plus the minimum-image cube's uniform
- *          depolarising field -4 pi M / 3V), with flexible directions; a box
- *          edge below twice that cutoff runs unpreconditioned.  At create,
- *          TDP_PRECOND=0 keeps plain CG and TDP_PRECOND_INNER sets the inner
- *          iterations (1-8).
+ *          depolarising field -4 pi M / 3V), with flexible directions, from
+ *          32,768 atoms on (below that plain CG is as fast); a cold solve
+ *          starts from the preconditioned right-hand side.  A box edge below
+ *          twice that cutoff runs unpreconditioned.  At create, TDP_PRECOND=1
+ *          uses the preconditioner at any size, TDP_PRECOND=0 never, and
+ *          TDP_PRECOND_INNER sets the inner iterations (1-8).
  *  JACOBI: the reference's own fixed-point iteration, step for step. */
 #define TDP_SOLVER_CG 0
 #define TDP_SOLVER_JACOBI 1

@@ -32,6 +32,8 @@
 // range with unit scales (nearly all of a box) take the closed-form lab-frame
 // VJP (pair_vjp_lab), a few times cheaper.  Every pair is visited from both
 // atoms (each atom owns kLanes threads), so no atomics are needed.
+#include "tholedipole_b200.h"
+#include <algorithm>
 #include "tdp_adjoint.cuh"
 
 namespace tdp {
@@ -66,6 +68,137 @@ __global__ void k_pair_vjp(PairParams P, AtomData A, const double* __restrict__ 
     for (int k = 0; k < 8; k++) acc[k] = lane_sum(acc[k]);
     if (act && l == 0)
         for (int k = 0; k < 8; k++) out[8 * me + k] = acc[k];
+}
+
+// k_pair_vjp in two passes, for rInvVec[4] = 0 (the default; the closed form
+// assumes it).
+// Pass 1 (k_pair_vjp_fast): one thread per atom, J atoms staged in shared
+// memory 32 at a time; every pair beyond the damping range whose frame row is
+// regular takes the closed-form lab-frame VJP in the arithmetic T (FP32 in
+// the mixed form, FP64 in the plain form) from a displacement formed in FP64
+// with the minimum image and rounded once; per-tile sums are added in FP64.
+// The other pairs (damped or degenerate, ~0.6 % of a box) are listed in the
+// atom's row of `slow`, in index order (beyond kSlowCap they are evaluated in
+// place).  Pass 2 (k_pair_vjp_slow): one warp per atom runs the FP64 routine
+// over the listed pairs and the covalent corrections, lane l taking entries
+// l, l + 32, ..., and adds the warp's sums, reduced by a fixed shuffle tree.
+// Small systems split the J range over blockIdx.y (at most kVjpSplit
+// splits) to fill the GPU: split s keeps its own sums and slow rows, and
+// pass 2 adds the splits in order.  Both passes are deterministic.
+constexpr int kVjpTile = 32;
+constexpr int kSlowCap = 192;
+constexpr int kVjpSplit = 8;
+// The FP64 routine out of line, so that the rare overflow of a slow row does
+// not set the fast pass's register budget.
+__device__ __noinline__ void visit_pair_call(const PairParams& P, const AtomData& A, const double* g,
+                                             const double* gT, double gE, int me, int j, double* acc) {
+    visit_pair(P, A, g, gT, gE, me, j, 1.0, 1.0, acc);
+}
+template <class T>
+__global__ void __launch_bounds__(kVjpTile) k_pair_vjp_fast(PairParams P, AtomData A, const double* __restrict__ g,
+                                                           const double* __restrict__ gT, double gE,
+                                                           int* __restrict__ slow, int* __restrict__ nslow,
+                                                           double* __restrict__ part_out) {
+    typedef V3T<T> W;
+    __shared__ double s_pos[3][kVjpTile];
+    __shared__ double2 s_yz[kVjpTile];
+    __shared__ T s_q[kVjpTile];
+    __shared__ T s_v[12][kVjpTile];   // lab, mu, g, gT
+    const int me = blockIdx.x * kVjpTile + threadIdx.x;
+    const bool act = me < P.n;
+    const int mi = act ? me : 0;
+    const double px = A.pos[3 * mi], py = A.pos[3 * mi + 1], pz = A.pos[3 * mi + 2];
+    const double2 myz = A.yz ? A.yz[mi] : make_double2(py, pz);
+    const T q0 = (T)A.q[mi];
+    const W m0 = {(T)A.lab[3 * mi], (T)A.lab[3 * mi + 1], (T)A.lab[3 * mi + 2]};
+    const W u0 = {(T)A.mu[3 * mi], (T)A.mu[3 * mi + 1], (T)A.mu[3 * mi + 2]};
+    const W g0 = {(T)g[3 * mi], (T)g[3 * mi + 1], (T)g[3 * mi + 2]};
+    const W t0 = {(T)gT[3 * mi], (T)gT[3 * mi + 1], (T)gT[3 * mi + 2]};
+    const T kap = P.mutual ? T(1) : T(-1), tgE = (T)gE;
+    const double damp_r2 = P.damp_r2 == 0.0f ? 0.0 : (double)P.damp_r2;
+    double acc[8] = {0, 0, 0, 0, 0, 0, 0, 0};
+    int ns = 0;
+    const size_t sm = (size_t)blockIdx.y * P.n + mi;   // (split, atom)
+    int* row = slow + sm * kSlowCap;
+    const int ntile = (P.n + kVjpTile - 1) / kVjpTile;
+    const int tb = (int)(((long)ntile * blockIdx.y) / gridDim.y), te = (int)(((long)ntile * (blockIdx.y + 1)) / gridDim.y);
+    for (int base = tb * kVjpTile; base < te * kVjpTile && base < P.n; base += kVjpTile) {
+        __syncwarp();
+        const int js = base + threadIdx.x;
+        if (js < P.n) {
+            for (int c = 0; c < 3; c++) {
+                s_pos[c][threadIdx.x] = A.pos[3 * js + c];
+                s_v[c][threadIdx.x] = (T)A.lab[3 * js + c];
+                s_v[3 + c][threadIdx.x] = (T)A.mu[3 * js + c];
+                s_v[6 + c][threadIdx.x] = (T)g[3 * js + c];
+                s_v[9 + c][threadIdx.x] = (T)gT[3 * js + c];
+            }
+            s_yz[threadIdx.x] = A.yz ? A.yz[js] : make_double2(A.pos[3 * js + 1], A.pos[3 * js + 2]);
+            s_q[threadIdx.x] = (T)A.q[js];
+        }
+        __syncwarp();
+        if (!act) continue;
+        const int cnt = min(kVjpTile, P.n - base);
+        T part[7] = {0, 0, 0, 0, 0, 0, 0};
+        for (int jj = 0; jj < cnt; jj++) {
+            const int j = base + jj;
+            if (j == me) continue;
+            const bool meI = me < j;
+            // d = p_K - p_I with I the lower index.
+            V3 d = min_image(P, {s_pos[0][jj] - px, s_pos[1][jj] - py, s_pos[2][jj] - pz});
+            if (!meI) d = {-d.x, -d.y, -d.z};
+            const double2 yj = s_yz[jj];
+            const bool yzd = (myz.x != yj.x) || (myz.y != yj.y);
+            const double r2 = d.x * d.x + d.y * d.y + d.z * d.z;
+            if (!(r2 < damp_r2) && yzd && d.y * d.y + d.z * d.z > 0.0) {
+                const W dj = {(T)d.x, (T)d.y, (T)d.z};
+                const W mj = {s_v[0][jj], s_v[1][jj], s_v[2][jj]}, uj = {s_v[3][jj], s_v[4][jj], s_v[5][jj]};
+                const W gj = {s_v[6][jj], s_v[7][jj], s_v[8][jj]}, tj = {s_v[9][jj], s_v[10][jj], s_v[11][jj]};
+                const T qj = s_q[jj];
+                T o[7];
+                if (meI) pair_vjp_lab<T>(dj, q0, m0, u0, qj, mj, uj, kap, tgE, g0, gj, t0, tj, true, o);
+                else pair_vjp_lab<T>(dj, qj, mj, uj, q0, m0, u0, kap, tgE, gj, g0, tj, t0, false, o);
+                for (int a = 0; a < 7; a++) part[a] += o[a];
+            } else if (ns < kSlowCap) {
+                row[ns++] = j;
+            } else {
+                visit_pair_call(P, A, g, gT, gE, me, j, acc);
+            }
+        }
+        for (int a = 0; a < 7; a++) acc[a] += (double)part[a];
+    }
+    if (!act) return;
+    nslow[sm] = ns;
+    for (int k = 0; k < 8; k++) part_out[8 * sm + k] = acc[k];
+}
+
+__global__ void k_pair_vjp_slow(PairParams P, AtomData A, const double* __restrict__ g, const double* __restrict__ gT,
+                                double gE, int nsplit, const int* __restrict__ slow, const int* __restrict__ nslow,
+                                const double* __restrict__ part, const int* __restrict__ exc_off,
+                                const int* __restrict__ exc_j, const double* __restrict__ exc_m,
+                                const double* __restrict__ exc_s, double* __restrict__ out) {
+    const int me = (blockIdx.x * blockDim.x + threadIdx.x) >> 5, l = threadIdx.x & 31;
+    if (me >= P.n) return;   // whole warps leave together
+    double acc[8] = {0, 0, 0, 0, 0, 0, 0, 0};
+    for (int sp = 0; sp < nsplit; sp++) {
+        const size_t sm = (size_t)sp * P.n + me;
+        const int* row = slow + sm * kSlowCap;
+        for (int e = l; e < nslow[sm]; e += 32) visit_pair(P, A, g, gT, gE, me, row[e], 1.0, 1.0, acc);
+    }
+    // Covalent scales: the pair function is linear in (mScale, iScale).
+    for (int e = exc_off[me] + l; e < exc_off[me + 1]; e += 32)
+        visit_pair(P, A, g, gT, gE, me, exc_j[e], exc_m[e] - 1.0, exc_s[e] - 1.0, acc);
+    for (int k = 0; k < 8; k++) {
+        double v = acc[k];
+        for (int o = 16; o > 0; o >>= 1) v += __shfl_xor_sync(0xffffffffu, v, o);
+        acc[k] = v;
+    }
+    if (l == 0)
+        for (int k = 0; k < 8; k++) {
+            double v = 0.0;
+            for (int sp = 0; sp < nsplit; sp++) v += part[8 * ((size_t)sp * P.n + me) + k];
+            out[8 * me + k] = v + acc[k];
+        }
 }
 
 // b = d/d(q, lab, t) of lambda . Efix, per atom (out: n*5).  Field at i due to
@@ -237,9 +370,36 @@ __global__ void k_set_operand(int n, const int* __restrict__ rank, const double*
 // ---------------------------------------------------------------------------
 static inline int nb(int n) { return (n + 127) / 128; }
 
-void launch_adjoint_pair(const Dev& d, const double* g, const double* gT, double gE, double* a8, cudaStream_t st) {
+// Scratch of the two-pass pair VJP, per (split, atom): 8 FP64 sums, the
+// slow-pair row and its count.
+size_t adjoint_pair_scratch(int n) {
+    const size_t m = (size_t)adj::kVjpSplit * (size_t)std::max(n, 1);
+    return 8 * m + (m * (adj::kSlowCap + 1) * sizeof(int) + sizeof(double) - 1) / sizeof(double);
+}
+
+void launch_adjoint_pair(const Dev& d, const double* g, const double* gT, double gE, double* a8, int precision,
+                         double* scratch, cudaStream_t st) {
+    if (d.n <= 0) return;
     adj::AtomData A{d.pos, d.charge, d.lab, d.mu, d.thole, d.yz};
-    adj::k_pair_vjp<<<nb(d.n * adj::kLanes), 128, 0, st>>>(d.pp, A, g, gT, gE, d.exc_off, d.exc_j, d.exc_m, d.exc_s, a8);
+    if (d.pp.rinv4_power != 0.0f || d.pp.rinv4_fill != 0.0f) {
+        adj::k_pair_vjp<<<nb(d.n * adj::kLanes), 128, 0, st>>>(d.pp, A, g, gT, gE, d.exc_off, d.exc_j, d.exc_m,
+                                                                d.exc_s, a8);
+        return;
+    }
+    const int blocks = (d.n + adj::kVjpTile - 1) / adj::kVjpTile;
+    // Splits of the J range: about 16 warps per SM in total.
+    const int nsplit = std::min(adj::kVjpSplit, std::max(1, (16 * 148 + blocks - 1) / blocks));
+    const size_t m = (size_t)adj::kVjpSplit * d.n;
+    double* part = scratch;
+    int* slow = reinterpret_cast<int*>(scratch + 8 * m);
+    int* nslow = slow + m * adj::kSlowCap;
+    const dim3 grid(blocks, nsplit);
+    if (precision == TDP_PRECISION_MIXED)
+        adj::k_pair_vjp_fast<float><<<grid, adj::kVjpTile, 0, st>>>(d.pp, A, g, gT, gE, slow, nslow, part);
+    else
+        adj::k_pair_vjp_fast<double><<<grid, adj::kVjpTile, 0, st>>>(d.pp, A, g, gT, gE, slow, nslow, part);
+    adj::k_pair_vjp_slow<<<nb(32 * d.n), 128, 0, st>>>(d.pp, A, g, gT, gE, nsplit, slow, nslow, part, d.exc_off,
+                                                        d.exc_j, d.exc_m, d.exc_s, a8);
 }
 void launch_adjoint_fixed(const Dev& d, const double* lam, double* b5, cudaStream_t st) {
     adj::AtomData A{d.pos, d.charge, d.lab, d.mu, d.thole, d.yz};

@@ -55,9 +55,11 @@ template <class T> __device__ __forceinline__ T cst(double v);
 template <> __device__ __forceinline__ double cst<double>(double v) { return v; }
 template <> __device__ __forceinline__ Dual cst<Dual>(double v) { return mk(v); }
 
-struct V3 {
-    double x, y, z;
+template <class T>
+struct V3T {
+    T x, y, z;
 };
+typedef V3T<double> V3;
 __device__ __forceinline__ V3 ld(const double* p) { return {p[0], p[1], p[2]}; }
 
 // Thole factors of the pair energy routine (RTDF.cpp:204-220).
@@ -249,18 +251,27 @@ struct AtomData {
     const double2* yz;     // raw (y, z) for the QI frame test (NULL: taken from pos)
 };
 
-// Visits pair (me, j) with scales (mS, iS); accumulates d l / d(my q, lab, mu, t).
-__device__ __forceinline__ V3 cross3(V3 a, V3 b) {
+template <class T>
+__device__ __forceinline__ V3T<T> cross3(V3T<T> a, V3T<T> b) {
     return {a.y * b.z - a.z * b.y, a.z * b.x - a.x * b.z, a.x * b.y - a.y * b.x};
 }
-__device__ __forceinline__ double dot3(V3 a, V3 b) { return a.x * b.x + a.y * b.y + a.z * b.z; }
-__device__ __forceinline__ V3 axpy(double a, V3 x, V3 y) { return {a * x.x + y.x, a * x.y + y.y, a * x.z + y.z}; }
-__device__ __forceinline__ V3 scl(double a, V3 x) { return {a * x.x, a * x.y, a * x.z}; }
-__device__ __forceinline__ V3 add3(V3 a, V3 b) { return {a.x + b.x, a.y + b.y, a.z + b.z}; }
-__device__ __forceinline__ V3 sub3v(V3 a, V3 b) { return {a.x - b.x, a.y - b.y, a.z - b.z}; }
+template <class T>
+__device__ __forceinline__ T dot3(V3T<T> a, V3T<T> b) { return a.x * b.x + a.y * b.y + a.z * b.z; }
+template <class T>
+__device__ __forceinline__ V3T<T> axpy(T a, V3T<T> x, V3T<T> y) { return {a * x.x + y.x, a * x.y + y.y, a * x.z + y.z}; }
+template <class T>
+__device__ __forceinline__ V3T<T> scl(T a, V3T<T> x) { return {a * x.x, a * x.y, a * x.z}; }
+template <class T>
+__device__ __forceinline__ V3T<T> add3(V3T<T> a, V3T<T> b) { return {a.x + b.x, a.y + b.y, a.z + b.z}; }
+template <class T>
+__device__ __forceinline__ V3T<T> sub3v(V3T<T> a, V3T<T> b) { return {a.x - b.x, a.y - b.y, a.z - b.z}; }
 // Transpose of the permuted back rotation: a . perm(v) = permT(a) . v with
 // perm(v) = (v_y, v_z, v_x).
-__device__ __forceinline__ V3 permT(V3 a) { return {a.z, a.x, a.y}; }
+template <class T>
+__device__ __forceinline__ V3T<T> permT(V3T<T> a) { return {a.z, a.x, a.y}; }
+// a / sqrt(x): exact division in FP64, the reciprocal square root in FP32.
+__device__ __forceinline__ double div_sqrt(double a, double x) { return a / sqrt(x); }
+__device__ __forceinline__ float div_sqrt(float a, float x) { return a * rsqrtf(x); }
 
 // Closed-form VJP of the pair routine for a pair that Thole damping does not
 // reach, with unit scales and rInvVec[4] = 0: the derivatives of
@@ -272,36 +283,39 @@ __device__ __forceinline__ V3 permT(V3 a) { return {a.z, a.x, a.y}; }
 // sides' multipoles and its gradient is written out term by term below.  The
 // Thole factors do not enter (their derivative is 0 here).  out[0..6]: dq,
 // dm_lab[3], du[3] of side I (side_I) or side K.
-__device__ __forceinline__ void pair_vjp_lab(V3 d, double qI, V3 mI, V3 uI, double qK, V3 mK, V3 uK, double kap,
-                                             double gE, V3 gFI, V3 gFK, V3 gTI, V3 gTK, bool side_I, double* out) {
-    const double r2 = dot3(d, d), rinv = 1.0 / sqrt(r2), rv2 = rinv * rinv, rv3 = rv2 * rinv;
-    const double rho2 = d.y * d.y + d.z * d.z;
-    const double xs = rinv / sqrt(rho2);
-    const V3 X = {rho2 * xs, -d.x * d.y * xs, -d.x * d.z * xs};
-    const V3 PI = add3(mI, uI), PK = add3(mK, uK);
-    const double QI1 = dot3(X, mI), UI0 = dot3(X, uI), QK1 = dot3(X, mK), UK0 = dot3(X, uK);
-    const double PI0 = QI1 + UI0, PK0 = QK1 + UK0;
-    const V3 cf = permT(sub3v(gFK, gFI));
-    const V3 D = scl(rinv, cross3(X, cf));
-    const double cX = dot3(cf, X);
-    const double w = 1.0 + kap;   // dW/du
+template <class T>
+__device__ __forceinline__ void pair_vjp_lab(V3T<T> d, T qI, V3T<T> mI, V3T<T> uI, T qK, V3T<T> mK, V3T<T> uK, T kap,
+                                             T gE, V3T<T> gFI, V3T<T> gFK, V3T<T> gTI, V3T<T> gTK, bool side_I,
+                                             T* out) {
+    typedef V3T<T> W;
+    const T r2 = dot3(d, d), rinv = div_sqrt(T(1), r2), rv2 = rinv * rinv, rv3 = rv2 * rinv;
+    const T rho2 = d.y * d.y + d.z * d.z;
+    const T xs = div_sqrt(rinv, rho2);
+    const W X = {rho2 * xs, -d.x * d.y * xs, -d.x * d.z * xs};
+    const W PI = add3(mI, uI), PK = add3(mK, uK);
+    const T QI1 = dot3(X, mI), UI0 = dot3(X, uI), QK1 = dot3(X, mK), UK0 = dot3(X, uK);
+    const T PI0 = QI1 + UI0, PK0 = QK1 + UK0;
+    const W cf = permT(sub3v(gFK, gFI));
+    const W D = scl(rinv, cross3(X, cf));
+    const T cX = dot3(cf, X);
+    const T w = T(1) + kap;   // dW/du
     if (side_I) {
-        const V3 GI = sub3v(D, permT(gTI)), GK = sub3v(D, permT(gTK));
-        const V3 tauK = cross3(GK, mK), sigK = cross3(D, uK);
-        const V3 WK = axpy(kap, uK, PK);
-        const double WK0 = PK0 + kap * UK0;
-        const V3 Vij = axpy(rv2 * qK - 3.0 * rv3 * PK0, X, scl(rv3, PK));
-        const V3 Vdij = axpy(rv2 * qK - 3.0 * rv3 * WK0, X, scl(rv3, WK));
-        const V3 t2 = axpy(-3.0 * rv3 * dot3(X, tauK), X, scl(rv3, tauK));
-        const V3 t4 = axpy(-3.0 * rv3 * dot3(X, sigK), X, scl(rv3, sigK));
-        const double c5 = 2.0 * rv3 * cX * qK;
+        const W GI = sub3v(D, permT(gTI)), GK = sub3v(D, permT(gTK));
+        const W tauK = cross3(GK, mK), sigK = cross3(D, uK);
+        const W WK = axpy(kap, uK, PK);
+        const T WK0 = PK0 + kap * UK0;
+        const W Vij = axpy(rv2 * qK - T(3) * rv3 * PK0, X, scl(rv3, PK));
+        const W Vdij = axpy(rv2 * qK - T(3) * rv3 * WK0, X, scl(rv3, WK));
+        const W t2 = axpy(-T(3) * rv3 * dot3(X, tauK), X, scl(rv3, tauK));
+        const W t4 = axpy(-T(3) * rv3 * dot3(X, sigK), X, scl(rv3, sigK));
+        const T c5 = T(2) * rv3 * cX * qK;
         // Energy partials.
-        const double de_q = rinv * qK - 0.5 * rv2 * (PK0 + QK1);
-        const V3 de_m = axpy(rv2 * qK - 1.5 * rv3 * (PK0 + QK1), X, scl(0.5 * rv3, add3(PK, mK)));
-        const V3 de_u = axpy(0.5 * rv2 * qK - 1.5 * rv3 * QK1, X, scl(0.5 * rv3, mK));
-        out[0] = gE * de_q - rv2 * (dot3(X, tauK) + dot3(X, sigK)) + cX * (rv2 * qK - 2.0 * rv3 * PK0);
-        const V3 gm = add3(add3(scl(gE, de_m), cross3(Vij, GI)), axpy(c5, X, add3(t2, t4)));
-        const V3 gu = add3(add3(scl(gE, de_u), cross3(Vdij, D)), axpy(c5, X, axpy(w, t4, t2)));
+        const T de_q = rinv * qK - T(0.5) * rv2 * (PK0 + QK1);
+        const W de_m = axpy(rv2 * qK - T(1.5) * rv3 * (PK0 + QK1), X, scl(T(0.5) * rv3, add3(PK, mK)));
+        const W de_u = axpy(T(0.5) * rv2 * qK - T(1.5) * rv3 * QK1, X, scl(T(0.5) * rv3, mK));
+        out[0] = gE * de_q - rv2 * (dot3(X, tauK) + dot3(X, sigK)) + cX * (rv2 * qK - T(2) * rv3 * PK0);
+        const W gm = add3(add3(scl(gE, de_m), cross3(Vij, GI)), axpy(c5, X, add3(t2, t4)));
+        const W gu = add3(add3(scl(gE, de_u), cross3(Vdij, D)), axpy(c5, X, axpy(w, t4, t2)));
         out[1] = gm.x;
         out[2] = gm.y;
         out[3] = gm.z;
@@ -309,21 +323,21 @@ __device__ __forceinline__ void pair_vjp_lab(V3 d, double qI, V3 mI, V3 uI, doub
         out[5] = gu.y;
         out[6] = gu.z;
     } else {
-        const V3 GI = sub3v(D, permT(gTI)), GK = sub3v(D, permT(gTK));
-        const V3 tauI = cross3(GI, mI), sigI = cross3(D, uI);
-        const V3 WI = axpy(kap, uI, PI);
-        const double WI0 = PI0 + kap * UI0;
-        const V3 Vji = axpy(-rv2 * qI - 3.0 * rv3 * PI0, X, scl(rv3, PI));
-        const V3 Vdji = axpy(-rv2 * qI - 3.0 * rv3 * WI0, X, scl(rv3, WI));
-        const V3 t1 = axpy(-3.0 * rv3 * dot3(X, tauI), X, scl(rv3, tauI));
-        const V3 t3 = axpy(-3.0 * rv3 * dot3(X, sigI), X, scl(rv3, sigI));
-        const double c5 = -2.0 * rv3 * cX * qI;
-        const double de_q = rinv * qI + 0.5 * rv2 * (PI0 + QI1);
-        const V3 de_m = axpy(-rv2 * qI - 1.5 * rv3 * (PI0 + QI1), X, scl(0.5 * rv3, add3(PI, mI)));
-        const V3 de_u = axpy(-0.5 * rv2 * qI - 1.5 * rv3 * QI1, X, scl(0.5 * rv3, mI));
-        out[0] = gE * de_q + rv2 * (dot3(X, tauI) + dot3(X, sigI)) + cX * (rv2 * qI + 2.0 * rv3 * PI0);
-        const V3 gm = add3(add3(scl(gE, de_m), cross3(Vji, GK)), axpy(c5, X, add3(t1, t3)));
-        const V3 gu = add3(add3(scl(gE, de_u), cross3(Vdji, D)), axpy(c5, X, axpy(w, t3, t1)));
+        const W GI = sub3v(D, permT(gTI)), GK = sub3v(D, permT(gTK));
+        const W tauI = cross3(GI, mI), sigI = cross3(D, uI);
+        const W WI = axpy(kap, uI, PI);
+        const T WI0 = PI0 + kap * UI0;
+        const W Vji = axpy(-rv2 * qI - T(3) * rv3 * PI0, X, scl(rv3, PI));
+        const W Vdji = axpy(-rv2 * qI - T(3) * rv3 * WI0, X, scl(rv3, WI));
+        const W t1 = axpy(-T(3) * rv3 * dot3(X, tauI), X, scl(rv3, tauI));
+        const W t3 = axpy(-T(3) * rv3 * dot3(X, sigI), X, scl(rv3, sigI));
+        const T c5 = -T(2) * rv3 * cX * qI;
+        const T de_q = rinv * qI + T(0.5) * rv2 * (PI0 + QI1);
+        const W de_m = axpy(-rv2 * qI - T(1.5) * rv3 * (PI0 + QI1), X, scl(T(0.5) * rv3, add3(PI, mI)));
+        const W de_u = axpy(-T(0.5) * rv2 * qI - T(1.5) * rv3 * QI1, X, scl(T(0.5) * rv3, mI));
+        out[0] = gE * de_q + rv2 * (dot3(X, tauI) + dot3(X, sigI)) + cX * (rv2 * qI + T(2) * rv3 * PI0);
+        const W gm = add3(add3(scl(gE, de_m), cross3(Vji, GK)), axpy(c5, X, add3(t1, t3)));
+        const W gu = add3(add3(scl(gE, de_u), cross3(Vdji, D)), axpy(c5, X, axpy(w, t3, t1)));
         out[1] = gm.x;
         out[2] = gm.y;
         out[3] = gm.z;

@@ -878,7 +878,8 @@ void run_adjoint(tdp_handle* h, const double* g_in, double gE, double* out_dst, 
     cudaStream_t st = h->stream;
     const int n = h->n;
     const size_t n3 = 3 * (size_t)n;
-    if (!h->adj) h->adj = dalloc<double>(n3 * 11 + 8 * (size_t)n + 5 * (size_t)n + 2 * (size_t)n + 6 * (size_t)n,
+    if (!h->adj) h->adj = dalloc<double>(n3 * 11 + 8 * (size_t)n + 5 * (size_t)n + 2 * (size_t)n + 6 * (size_t)n +
+                                             adjoint_pair_scratch(n),
                                          h->owned);
     double* g = h->adj;
     double* gt = g + n3;
@@ -896,6 +897,7 @@ void run_adjoint(tdp_handle* h, const double* g_in, double gE, double* out_dst, 
     double* out = ct + n;
     double* ext_v = out + 6 * (size_t)n;   // Extrapolated: E + T mu_(k-1)
     double* galpha = ext_v + n3;           // Extrapolated: polarizability gradient
+    double* pair_scratch = galpha + n;     // split sums of the pair VJP
     if (g_in)
         TDP_CUDA(cudaMemcpyAsync(g, g_in, n3 * 8, on_device ? cudaMemcpyDeviceToDevice : cudaMemcpyHostToDevice, st));
     else
@@ -903,7 +905,7 @@ void run_adjoint(tdp_handle* h, const double* g_in, double gE, double* out_dst, 
     TDP_CUDA(cudaMemcpyAsync(mu_fwd, d.mu, n3 * 8, cudaMemcpyDeviceToDevice, st));
     TDP_CUDA(cudaMemcpyAsync(E_fwd, d.E, n3 * 8, cudaMemcpyDeviceToDevice, st));
     launch_torque_vjp(d, g, gt, st);
-    launch_adjoint_pair(d, g, gt, gE, a8, st);
+    launch_adjoint_pair(d, g, gt, gE, a8, h->precision, pair_scratch, st);
     launch_adjoint_split(d, a8, nullptr, amu, nullptr, st);
     if (h->polarization == TDP_MUTUAL) {
         // One solve of the same symmetric system: A lambda = a_mu.  Target:
@@ -1283,12 +1285,18 @@ int tdp_create(const tdp_system_desc* desc, tdp_handle** out) {
         // same box (tdp_precond.cuh).  Its real space stops at 0.6 nm or where
         // the Thole damping of every pair is below 1e-12, whichever is longer;
         // PME tolerance 1e-3; three inner iterations per application.
-        // TDP_PRECOND=0 at create keeps the unpreconditioned CG;
-        // TDP_PRECOND_INNER sets the inner iterations (1-8).
+        // It pays from about 30,000 atoms on (an all-pairs matvec grows as
+        // n^2, an application as n; measured on water boxes: 7 % slower at
+        // 12,288 atoms, even at 24,000, 1.25-1.5x faster at 41,472), so by
+        // default it is used from kPrecondMinAtoms atoms.  TDP_PRECOND=1 at
+        // create uses it at any size, TDP_PRECOND=0 never; TDP_PRECOND_INNER
+        // sets the inner iterations (1-8).
+        constexpr int kPrecondMinAtoms = 32768;
         bool want_pre = h->method == TDP_PME && !ewald && h->polarization == TDP_MUTUAL &&
-                        h->solver == TDP_SOLVER_CG && n > 0;
+                        h->solver == TDP_SOLVER_CG && n >= kPrecondMinAtoms;
         if (const char* e = getenv("TDP_PRECOND"))
-            if (atoi(e) == 0) want_pre = false;
+            want_pre = atoi(e) != 0 && h->method == TDP_PME && !ewald && h->polarization == TDP_MUTUAL &&
+                       h->solver == TDP_SOLVER_CG && n > 0;
         if (want_pre) {
             double tmax = 0.0;
             for (double t : h->thole) tmax = std::max(tmax, std::isfinite(t) ? t : 0.0);

@@ -126,7 +126,11 @@ void launch_moments(const Dev& d, const double* mass, double* scratch, double* o
 
 // Adjoint (tdp_adjoint.cu).
 void launch_torque_vjp(const Dev& d, const double* g, double* gt, cudaStream_t st);
-void launch_adjoint_pair(const Dev& d, const double* g, const double* gT, double gE, double* a8, cudaStream_t st);
+// precision: the arithmetic of the closed-form pairs (FP32 in the mixed form);
+// scratch: adjoint_pair_scratch(n) doubles.
+size_t adjoint_pair_scratch(int n);
+void launch_adjoint_pair(const Dev& d, const double* g, const double* gT, double gE, double* a8, int precision,
+                         double* scratch, cudaStream_t st);
 void launch_adjoint_fixed(const Dev& d, const double* lam, double* b5, cudaStream_t st);
 void launch_adjoint_matvec_t(const Dev& d, const double* lam, double* ct, cudaStream_t st);
 // ct (+)= d/dt of lam^T T(t) mu for an explicit mu (n*3); accumulate adds to ct.
