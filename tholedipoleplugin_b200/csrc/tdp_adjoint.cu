@@ -159,10 +159,12 @@ __global__ void __launch_bounds__(kVjpTile) k_pair_vjp_fast(PairParams P, AtomDa
                 if (meI) pair_vjp_lab<T>(dj, q0, m0, u0, qj, mj, uj, kap, tgE, g0, gj, t0, tj, true, o);
                 else pair_vjp_lab<T>(dj, qj, mj, uj, q0, m0, u0, kap, tgE, gj, g0, tj, t0, false, o);
                 for (int a = 0; a < 7; a++) part[a] += o[a];
-            } else if (ns < kSlowCap) {
-                row[ns++] = j;
             } else {
-                visit_pair_call(P, A, g, gT, gE, me, j, acc);
+                // The count goes on past the row (the list users then scan all
+                // partners of this atom).
+                if (ns < kSlowCap) row[ns] = j;
+                else visit_pair_call(P, A, g, gT, gE, me, j, acc);
+                ns++;
             }
         }
         for (int a = 0; a < 7; a++) acc[a] += (double)part[a];
@@ -183,7 +185,7 @@ __global__ void k_pair_vjp_slow(PairParams P, AtomData A, const double* __restri
     for (int sp = 0; sp < nsplit; sp++) {
         const size_t sm = (size_t)sp * P.n + me;
         const int* row = slow + sm * kSlowCap;
-        for (int e = l; e < nslow[sm]; e += 32) visit_pair(P, A, g, gT, gE, me, row[e], 1.0, 1.0, acc);
+        for (int e = l; e < min(nslow[sm], kSlowCap); e += 32) visit_pair(P, A, g, gT, gE, me, row[e], 1.0, 1.0, acc);
     }
     // Covalent scales: the pair function is linear in (mScale, iScale).
     for (int e = exc_off[me] + l; e < exc_off[me + 1]; e += 32)
@@ -204,15 +206,18 @@ __global__ void k_pair_vjp_slow(PairParams P, AtomData A, const double* __restri
 // b = d/d(q, lab, t) of lambda . Efix, per atom (out: n*5).  Field at i due to
 // k (RTDF.cpp:698-704): f_ik = -m [d (rr3 q_k - rr5 lab_k.d) + lab_k rr3],
 // d = p_k - p_i.
+// with_dual = 0: the unit-scale pairs' Thole-factor term is left to
+// k_fixed_dual_list (the covalent corrections keep theirs here).
 __global__ void k_fixed_vjp(PairParams P, AtomData A, const double* __restrict__ lam, const int* __restrict__ exc_off,
-                            const int* __restrict__ exc_j, const double* __restrict__ exc_m, double* __restrict__ out) {
+                            const int* __restrict__ exc_j, const double* __restrict__ exc_m, double* __restrict__ out,
+                            int with_dual) {
     const int t = blockIdx.x * blockDim.x + threadIdx.x;
     const int k = t / kLanes, l = t % kLanes;
     const bool act = k < P.n;
     double acc[5] = {0, 0, 0, 0, 0};
     if (act) {
         for (int i = l; i < P.n; i += kLanes)
-            if (i != k) fixed_vjp_visit(P, A, lam, k, i, 1.0, acc);
+            if (i != k) fixed_vjp_visit(P, A, lam, k, i, 1.0, acc, with_dual != 0);
         for (int e = exc_off[k] + l; e < exc_off[k + 1]; e += kLanes)
             fixed_vjp_visit(P, A, lam, k, exc_j[e], exc_m[e] - 1.0, acc);
     }
@@ -237,6 +242,139 @@ __global__ void k_matvec_t_vjp(PairParams P, AtomData A, const double* __restric
     }
     acc = lane_sum(acc);
     if (act && l == 0) out[k] = accumulate ? out[k] + acc : acc;
+}
+
+// k_fixed_vjp without the Thole-factor term, over shared-memory J tiles, one
+// thread per atom: undamped pairs in the arithmetic T (FP32 in the mixed
+// form) from an FP64 minimum-image displacement, damped pairs in FP64; the
+// covalent corrections (with their Thole term) in FP64 at the end.  The
+// J range is split over blockIdx.y as in k_pair_vjp_fast; split s writes
+// part + s * n * 5 and k_sum_splits5 adds the splits in order.
+template <class T>
+__global__ void __launch_bounds__(kVjpTile) k_fixed_vjp_fast(PairParams P, AtomData A, const double* __restrict__ lam,
+                                                            const int* __restrict__ exc_off,
+                                                            const int* __restrict__ exc_j,
+                                                            const double* __restrict__ exc_m,
+                                                            double* __restrict__ part) {
+    __shared__ double s_pos[3][kVjpTile];
+    __shared__ T s_l[3][kVjpTile];
+    const int k = blockIdx.x * kVjpTile + threadIdx.x;
+    const bool act = k < P.n;
+    const int kk = act ? k : 0;
+    const double px = A.pos[3 * kk], py = A.pos[3 * kk + 1], pz = A.pos[3 * kk + 2];
+    const double damp_r2 = (double)P.damp_r2;
+    double acc[5] = {0, 0, 0, 0, 0};
+    const int ntile = (P.n + kVjpTile - 1) / kVjpTile;
+    const int tb = (int)(((long)ntile * blockIdx.y) / gridDim.y), te = (int)(((long)ntile * (blockIdx.y + 1)) / gridDim.y);
+    for (int base = tb * kVjpTile; base < te * kVjpTile && base < P.n; base += kVjpTile) {
+        __syncwarp();
+        const int js = base + threadIdx.x;
+        if (js < P.n)
+            for (int c = 0; c < 3; c++) {
+                s_pos[c][threadIdx.x] = A.pos[3 * js + c];
+                s_l[c][threadIdx.x] = (T)lam[3 * js + c];
+            }
+        __syncwarp();
+        if (!act) continue;
+        const int cnt = min(kVjpTile, P.n - base);
+        T a0 = 0, a1 = 0, a2 = 0, a3 = 0;
+        for (int jj = 0; jj < cnt; jj++) {
+            const int i = base + jj;
+            if (i == k) continue;
+            // d = p_k - p_i
+            const V3 d = min_image(P, {px - s_pos[0][jj], py - s_pos[1][jj], pz - s_pos[2][jj]});
+            const double r2 = d.x * d.x + d.y * d.y + d.z * d.z;
+            if (r2 < damp_r2) {
+                fixed_vjp_visit(P, A, lam, k, i, 1.0, acc, false);
+                continue;
+            }
+            const T dx = (T)d.x, dy = (T)d.y, dz = (T)d.z;
+            const T ri = div_sqrt(T(1), (T)r2), ri2 = ri * ri, rr3 = ri * ri2, rr5 = T(3) * rr3 * ri2;
+            const T lx = s_l[0][jj], ly = s_l[1][jj], lz = s_l[2][jj];
+            const T ldd = lx * dx + ly * dy + lz * dz;
+            a0 -= rr3 * ldd;
+            a1 += rr5 * ldd * dx - rr3 * lx;
+            a2 += rr5 * ldd * dy - rr3 * ly;
+            a3 += rr5 * ldd * dz - rr3 * lz;
+        }
+        acc[0] += (double)a0;
+        acc[1] += (double)a1;
+        acc[2] += (double)a2;
+        acc[3] += (double)a3;
+    }
+    if (!act) return;
+    if (blockIdx.y == 0)
+        for (int e = exc_off[k]; e < exc_off[k + 1]; e++) fixed_vjp_visit(P, A, lam, k, exc_j[e], exc_m[e] - 1.0, acc);
+    double* o = part + 5 * ((size_t)blockIdx.y * P.n + k);
+    for (int c = 0; c < 5; c++) o[c] = acc[c];
+}
+
+// out[k] = sum over splits s of part[s * m + k], in split order.
+__global__ void k_sum_splits(int m, int nsplit, const double* __restrict__ part, double* __restrict__ out) {
+    const int k = blockIdx.x * blockDim.x + threadIdx.x;
+    if (k >= m) return;
+    double v = 0.0;
+    for (int s = 0; s < nsplit; s++) v += part[(size_t)s * m + k];
+    out[k] = v;
+}
+
+// Warp-per-atom passes over the damped-partner lists of the pair VJP (the
+// same pairs, within the damping range, are the only ones whose Thole factors
+// matter).  An atom whose list overflowed its row falls back to a scan of all
+// partners.  Lanes take entries l, l + 32, ... in split order; a fixed
+// shuffle tree adds them.
+__device__ __forceinline__ double warp_sum_fixed(double v) {
+    for (int o = 16; o > 0; o >>= 1) v += __shfl_xor_sync(0xffffffffu, v, o);
+    return v;
+}
+
+__device__ __forceinline__ bool list_overflow(const AdjPairList& L, int n, int k) {
+    for (int sp = 0; sp < L.nsplit; sp++)
+        if (L.nslow[(size_t)sp * n + k] > L.cap) return true;
+    return false;
+}
+
+// out[5 k + 4] += d/dt_k of lambda . Efix over the unit-scale damped pairs.
+__global__ void k_fixed_dual_list(PairParams P, AtomData A, const double* __restrict__ lam, AdjPairList L,
+                                  double* __restrict__ out) {
+    const int k = (blockIdx.x * blockDim.x + threadIdx.x) >> 5, l = threadIdx.x & 31;
+    if (k >= P.n) return;   // whole warps leave together
+    double acc = 0.0;
+    if (list_overflow(L, P.n, k)) {
+        for (int i = l; i < P.n; i += 32)
+            if (i != k) acc += fixed_vjp_dual(P, A, lam, k, i, 1.0);
+    } else {
+        for (int sp = 0; sp < L.nsplit; sp++) {
+            const size_t sk = (size_t)sp * P.n + k;
+            const int* row = L.slow + sk * L.cap;
+            for (int e = l; e < L.nslow[sk]; e += 32) acc += fixed_vjp_dual(P, A, lam, k, row[e], 1.0);
+        }
+    }
+    acc = warp_sum_fixed(acc);
+    if (l == 0) out[5 * k + 4] += acc;
+}
+
+// k_matvec_t_vjp over the damped-partner lists.
+__global__ void k_matvec_t_list(PairParams P, AtomData A, const double* __restrict__ lam, AdjPairList L,
+                                const int* __restrict__ exc_off, const int* __restrict__ exc_j,
+                                const double* __restrict__ exc_s, double* __restrict__ out, int accumulate) {
+    const int k = (blockIdx.x * blockDim.x + threadIdx.x) >> 5, l = threadIdx.x & 31;
+    if (k >= P.n) return;
+    double acc = 0.0;
+    if (list_overflow(L, P.n, k)) {
+        for (int j = l; j < P.n; j += 32)
+            if (j != k) acc += matvec_t_visit(P, A, lam, k, j, 1.0);
+    } else {
+        for (int sp = 0; sp < L.nsplit; sp++) {
+            const size_t sk = (size_t)sp * P.n + k;
+            const int* row = L.slow + sk * L.cap;
+            for (int e = l; e < L.nslow[sk]; e += 32) acc += matvec_t_visit(P, A, lam, k, row[e], 1.0);
+        }
+    }
+    for (int e = exc_off[k] + l; e < exc_off[k + 1]; e += 32)
+        acc += matvec_t_visit(P, A, lam, k, exc_j[e], exc_s[e] - 1.0);
+    acc = warp_sum_fixed(acc);
+    if (l == 0) out[k] = accumulate ? out[k] + acc : acc;
 }
 
 }  // namespace adj
@@ -378,7 +516,8 @@ size_t adjoint_pair_scratch(int n) {
 }
 
 void launch_adjoint_pair(const Dev& d, const double* g, const double* gT, double gE, double* a8, int precision,
-                         double* scratch, cudaStream_t st) {
+                         double* scratch, AdjPairList* list, cudaStream_t st) {
+    if (list) *list = AdjPairList{};
     if (d.n <= 0) return;
     adj::AtomData A{d.pos, d.charge, d.lab, d.mu, d.thole, d.yz};
     if (d.pp.rinv4_power != 0.0f || d.pp.rinv4_fill != 0.0f) {
@@ -400,18 +539,39 @@ void launch_adjoint_pair(const Dev& d, const double* g, const double* gT, double
         adj::k_pair_vjp_fast<double><<<grid, adj::kVjpTile, 0, st>>>(d.pp, A, g, gT, gE, slow, nslow, part);
     adj::k_pair_vjp_slow<<<nb(32 * d.n), 128, 0, st>>>(d.pp, A, g, gT, gE, nsplit, slow, nslow, part, d.exc_off,
                                                         d.exc_j, d.exc_m, d.exc_s, a8);
+    if (list) *list = AdjPairList{nsplit, adj::kSlowCap, slow, nslow};
 }
-void launch_adjoint_fixed(const Dev& d, const double* lam, double* b5, cudaStream_t st) {
+void launch_adjoint_fixed(const Dev& d, const double* lam, double* b5, const AdjPairList& list, int precision,
+                          double* scratch, cudaStream_t st) {
+    if (d.n <= 0) return;
     adj::AtomData A{d.pos, d.charge, d.lab, d.mu, d.thole, d.yz};
-    adj::k_fixed_vjp<<<nb(d.n * adj::kLanes), 128, 0, st>>>(d.pp, A, lam, d.exc_off, d.exc_j, d.exc_m, b5);
+    if (list.nsplit <= 0 || !scratch) {
+        adj::k_fixed_vjp<<<nb(d.n * adj::kLanes), 128, 0, st>>>(d.pp, A, lam, d.exc_off, d.exc_j, d.exc_m, b5, 1);
+        return;
+    }
+    const int blocks = (d.n + adj::kVjpTile - 1) / adj::kVjpTile;
+    const int nsplit = std::min(adj::kVjpSplit, std::max(1, (16 * 148 + blocks - 1) / blocks));
+    const dim3 grid(blocks, nsplit);
+    if (precision == TDP_PRECISION_MIXED)
+        adj::k_fixed_vjp_fast<float><<<grid, adj::kVjpTile, 0, st>>>(d.pp, A, lam, d.exc_off, d.exc_j, d.exc_m, scratch);
+    else
+        adj::k_fixed_vjp_fast<double><<<grid, adj::kVjpTile, 0, st>>>(d.pp, A, lam, d.exc_off, d.exc_j, d.exc_m, scratch);
+    adj::k_sum_splits<<<nb(5 * d.n), 128, 0, st>>>(5 * d.n, nsplit, scratch, b5);
+    adj::k_fixed_dual_list<<<nb(32 * d.n), 128, 0, st>>>(d.pp, A, lam, list, b5);
 }
-void launch_adjoint_matvec_t(const Dev& d, const double* lam, double* ct, cudaStream_t st) {
-    launch_adjoint_matvec_t_mu(d, lam, d.mu, ct, false, st);
+void launch_adjoint_matvec_t(const Dev& d, const double* lam, double* ct, const AdjPairList& list, cudaStream_t st) {
+    launch_adjoint_matvec_t_mu(d, lam, d.mu, ct, false, list, st);
 }
 void launch_adjoint_matvec_t_mu(const Dev& d, const double* lam, const double* mu, double* ct, bool accumulate,
-                                cudaStream_t st) {
+                                const AdjPairList& list, cudaStream_t st) {
+    if (d.n <= 0) return;
     adj::AtomData A{d.pos, d.charge, d.lab, mu, d.thole, d.yz};
-    adj::k_matvec_t_vjp<<<nb(d.n * adj::kLanes), 128, 0, st>>>(d.pp, A, lam, d.exc_off, d.exc_j, d.exc_s, ct, accumulate ? 1 : 0);
+    if (list.nsplit > 0)
+        adj::k_matvec_t_list<<<nb(32 * d.n), 128, 0, st>>>(d.pp, A, lam, list, d.exc_off, d.exc_j, d.exc_s, ct,
+                                                            accumulate ? 1 : 0);
+    else
+        adj::k_matvec_t_vjp<<<nb(d.n * adj::kLanes), 128, 0, st>>>(d.pp, A, lam, d.exc_off, d.exc_j, d.exc_s, ct,
+                                                                    accumulate ? 1 : 0);
 }
 
 __global__ void k_lincomb(int n3, double ca, const double* __restrict__ a, double cb, const double* __restrict__ b,

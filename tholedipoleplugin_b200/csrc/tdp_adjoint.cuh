@@ -417,8 +417,10 @@ __device__ __forceinline__ T lam_dot_field(V3 d, double r, double r2, double dam
 
 // Contribution of the pair (i, k) with M scale m to atom k's
 // d/d(q_k, lab_k, t_k) of lambda . Efix (k_fixed_vjp), added to acc[5].
+// dual = false leaves out the Thole-factor term (acc[4]); fixed_vjp_dual adds
+// it alone.
 __device__ __forceinline__ void fixed_vjp_visit(const PairParams& P, const AtomData& A, const double* lam, int k,
-                                                int i, double m, double* acc) {
+                                                int i, double m, double* acc, bool dual = true) {
     const double damp_r2 = (double)P.damp_r2;
     const double* labk = A.lab + 3 * k;
     const V3 lk = ld(lam + 3 * k);
@@ -434,12 +436,29 @@ __device__ __forceinline__ void fixed_vjp_visit(const PairParams& P, const AtomD
     acc[2] += m * (rr5 * ldd * d.y - rr3 * li.y);
     acc[3] += m * (rr5 * ldd * d.z - rr3 * li.z);
     // t_k enters f_ik and f_ki (only within the damping range): dual number on t_k.
-    if (!(r2 < damp_r2)) return;
+    if (!dual || !(r2 < damp_r2)) return;
     V3 dn = {-d.x, -d.y, -d.z};
     Dual tk = mk(A.thole[k], 1.0), ti = mk(A.thole[i]);
     Dual s1 = lam_dot_field<Dual>(d, r, r2, damp_r2, ti, tk, A.q[k], labk, li, m);
     Dual s2 = lam_dot_field<Dual>(dn, r, r2, damp_r2, tk, ti, A.q[i], A.lab + 3 * i, lk, m);
     acc[4] += s1.d + s2.d;
+}
+
+// The Thole-factor term of fixed_vjp_visit alone (zero beyond the damping range).
+__device__ __forceinline__ double fixed_vjp_dual(const PairParams& P, const AtomData& A, const double* lam, int k,
+                                                 int i, double m) {
+    const double damp_r2 = (double)P.damp_r2;
+    V3 d = min_image(P, {A.pos[3 * k] - A.pos[3 * i], A.pos[3 * k + 1] - A.pos[3 * i + 1],
+                         A.pos[3 * k + 2] - A.pos[3 * i + 2]});  // p_k - p_i
+    const double r2 = d.x * d.x + d.y * d.y + d.z * d.z;
+    if (!(r2 < damp_r2)) return 0.0;
+    const double r = sqrt(r2);
+    const V3 li = ld(lam + 3 * i), lk = ld(lam + 3 * k);
+    const V3 dn = {-d.x, -d.y, -d.z};
+    Dual tk = mk(A.thole[k], 1.0), ti = mk(A.thole[i]);
+    Dual s1 = lam_dot_field<Dual>(d, r, r2, damp_r2, ti, tk, A.q[k], A.lab + 3 * k, li, m);
+    Dual s2 = lam_dot_field<Dual>(dn, r, r2, damp_r2, tk, ti, A.q[i], A.lab + 3 * i, lk, m);
+    return s1.d + s2.d;
 }
 
 // d/dt_k of the pair (k, j) terms of lambda^T T(t) mu with I scale s

@@ -879,7 +879,7 @@ void run_adjoint(tdp_handle* h, const double* g_in, double gE, double* out_dst, 
     const int n = h->n;
     const size_t n3 = 3 * (size_t)n;
     if (!h->adj) h->adj = dalloc<double>(n3 * 11 + 8 * (size_t)n + 5 * (size_t)n + 2 * (size_t)n + 6 * (size_t)n +
-                                             adjoint_pair_scratch(n),
+                                             adjoint_pair_scratch(n) + 5 * 8 * (size_t)n,
                                          h->owned);
     double* g = h->adj;
     double* gt = g + n3;
@@ -897,7 +897,8 @@ void run_adjoint(tdp_handle* h, const double* g_in, double gE, double* out_dst, 
     double* out = ct + n;
     double* ext_v = out + 6 * (size_t)n;   // Extrapolated: E + T mu_(k-1)
     double* galpha = ext_v + n3;           // Extrapolated: polarizability gradient
-    double* pair_scratch = galpha + n;     // split sums of the pair VJP
+    double* pair_scratch = galpha + n;     // split sums and damped-partner lists of the pair VJP
+    double* fixed_scratch = pair_scratch + adjoint_pair_scratch(n);   // split sums of the fixed-field VJP
     if (g_in)
         TDP_CUDA(cudaMemcpyAsync(g, g_in, n3 * 8, on_device ? cudaMemcpyDeviceToDevice : cudaMemcpyHostToDevice, st));
     else
@@ -905,7 +906,8 @@ void run_adjoint(tdp_handle* h, const double* g_in, double gE, double* out_dst, 
     TDP_CUDA(cudaMemcpyAsync(mu_fwd, d.mu, n3 * 8, cudaMemcpyDeviceToDevice, st));
     TDP_CUDA(cudaMemcpyAsync(E_fwd, d.E, n3 * 8, cudaMemcpyDeviceToDevice, st));
     launch_torque_vjp(d, g, gt, st);
-    launch_adjoint_pair(d, g, gt, gE, a8, h->precision, pair_scratch, st);
+    AdjPairList plist;
+    launch_adjoint_pair(d, g, gt, gE, a8, h->precision, pair_scratch, &plist, st);
     launch_adjoint_split(d, a8, nullptr, amu, nullptr, st);
     if (h->polarization == TDP_MUTUAL) {
         // One solve of the same symmetric system: A lambda = a_mu.  Target:
@@ -935,8 +937,8 @@ void run_adjoint(tdp_handle* h, const double* g_in, double gE, double* out_dst, 
         TDP_CUDA(cudaMemcpyAsync(lam, d.mu, n3 * 8, cudaMemcpyDeviceToDevice, st));
         TDP_CUDA(cudaMemcpyAsync(d.mu, mu_fwd, n3 * 8, cudaMemcpyDeviceToDevice, st));
         TDP_CUDA(cudaMemcpyAsync(d.E, E_fwd, n3 * 8, cudaMemcpyDeviceToDevice, st));
-        launch_adjoint_fixed(d, lam, b5, st);
-        launch_adjoint_matvec_t(d, lam, ct, st);
+        launch_adjoint_fixed(d, lam, b5, plist, h->precision, fixed_scratch, st);
+        launch_adjoint_matvec_t(d, lam, ct, plist, st);
         launch_set_operand<R>(d, lam, st);
         launch_field<R>(d, 1, st);
         launch_add_field(d, amu, amu_tlam, st);
@@ -971,19 +973,19 @@ void run_adjoint(tdp_handle* h, const double* g_in, double gE, double* out_dst, 
             launch_field<R>(d, 1, st);
             launch_add_field(d, E_fwd, ext_v, st);
             launch_dot3_acc(n, gbar, ext_v, galpha, st);
-            launch_adjoint_matvec_t_mu(d, agb, mu_prev, ct, true, st);
+            launch_adjoint_matvec_t_mu(d, agb, mu_prev, ct, true, plist, st);
             launch_set_operand<R>(d, agb, st);
             launch_field<R>(d, 1, st);
             launch_lincomb(n, h->extrap[o - 1], amu, 0.0, nullptr, ext_v, st);
             launch_add_field(d, ext_v, gbar, st);
         }
-        launch_adjoint_fixed(d, lam, b5, st);
+        launch_adjoint_fixed(d, lam, b5, plist, h->precision, fixed_scratch, st);
         h->adj_eps = 0.0;
         h->adj_iterations = 0;
     } else {
         // Direct: mu = alpha E, so lambda = alpha a_mu and dL/dalpha = a_mu . E.
         k_alpha_scale<<<(unsigned)((n3 + 255) / 256), 256, 0, st>>>(n, d.alpha, amu, lam);
-        launch_adjoint_fixed(d, lam, b5, st);
+        launch_adjoint_fixed(d, lam, b5, plist, h->precision, fixed_scratch, st);
         TDP_CUDA(cudaMemsetAsync(ct, 0, sizeof(double) * n, st));
         TDP_CUDA(cudaMemcpyAsync(amu_tlam, amu, n3 * 8, cudaMemcpyDeviceToDevice, st));
         TDP_CUDA(cudaMemcpyAsync(e_tmu, E_fwd, n3 * 8, cudaMemcpyDeviceToDevice, st));

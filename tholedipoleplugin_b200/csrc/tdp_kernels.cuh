@@ -126,16 +126,29 @@ void launch_moments(const Dev& d, const double* mass, double* scratch, double* o
 
 // Adjoint (tdp_adjoint.cu).
 void launch_torque_vjp(const Dev& d, const double* g, double* gt, cudaStream_t st);
+// Damped (and degenerate) partners of every atom, listed by the pair VJP per
+// (split, atom) in rows of `cap` entries (a count above cap means the row
+// overflowed), reused by the fixed-field and matvec Thole VJPs; nsplit = 0:
+// no list (those passes scan all pairs).  Valid while the scratch of
+// launch_adjoint_pair is untouched.
+struct AdjPairList {
+    int nsplit = 0, cap = 0;
+    const int* slow = nullptr;
+    const int* nslow = nullptr;
+};
 // precision: the arithmetic of the closed-form pairs (FP32 in the mixed form);
-// scratch: adjoint_pair_scratch(n) doubles.
+// scratch: adjoint_pair_scratch(n) doubles; list (may be NULL) receives the
+// damped-partner lists.
 size_t adjoint_pair_scratch(int n);
 void launch_adjoint_pair(const Dev& d, const double* g, const double* gT, double gE, double* a8, int precision,
-                         double* scratch, cudaStream_t st);
-void launch_adjoint_fixed(const Dev& d, const double* lam, double* b5, cudaStream_t st);
-void launch_adjoint_matvec_t(const Dev& d, const double* lam, double* ct, cudaStream_t st);
+                         double* scratch, AdjPairList* list, cudaStream_t st);
+// scratch: 5 * 8 * n doubles (the split sums of the tiled pass), or NULL.
+void launch_adjoint_fixed(const Dev& d, const double* lam, double* b5, const AdjPairList& list, int precision,
+                          double* scratch, cudaStream_t st);
+void launch_adjoint_matvec_t(const Dev& d, const double* lam, double* ct, const AdjPairList& list, cudaStream_t st);
 // ct (+)= d/dt of lam^T T(t) mu for an explicit mu (n*3); accumulate adds to ct.
 void launch_adjoint_matvec_t_mu(const Dev& d, const double* lam, const double* mu, double* ct, bool accumulate,
-                                cudaStream_t st);
+                                const AdjPairList& list, cudaStream_t st);
 // out = ca a + cb b (n*3; b may be NULL); acc_i += a_i . b_i (per atom).
 void launch_lincomb(int n, double ca, const double* a, double cb, const double* b, double* out, cudaStream_t st);
 void launch_dot3_acc(int n, const double* a, const double* b, double* acc, cudaStream_t st);
