@@ -303,7 +303,7 @@ int tdp_solver_stats(const tdp_handle* h, int32_t* iterations, double* epsilon, 
 /* The stopping quantity of every step of the last Mutual CG or Jacobi solve
  * (the RMS change a Jacobi step would make, as tdp_solver_stats reports the
  * final one), oldest first: the start, then one per iteration and one per
- * true-residual check.  Copies min(capacity, *count) values into eps_out
+ * true-residual check.  After tdp_adjoint it is the adjoint solve's.  Copies min(capacity, *count) values into eps_out
  * (host doubles); *count receives the number available (0 after Direct or
  * Extrapolated polarization).  No reference counterpart: a convergence
  * monitor of this library's solvers. */
