@@ -220,3 +220,50 @@ def test_force_matching_gradients_256_clusters():
         pm[j] -= h
         fd = (loss_np(pp) - loss_np(pm)) / (2 * h)
         assert abs(grad[j] - fd) <= 1e-4 * abs(fd), (j, grad[j], fd)
+
+
+@pytest.mark.parametrize("name", ["random220_nocutoff", "water216_pme"])
+def test_wide_damping_overflows_damped_lists(name):
+    """Thole factors near 0.8 (damping width t_i t_j ~ 0.64) put every pair of
+    the system within the damping range, so every atom has more damped
+    partners than a row of the adjoint's damped-partner list holds: the
+    overflowing pairs are evaluated in place and the list passes of the
+    fixed-field and matvec Thole terms fall back to scanning all partners.
+    The FP64 adjoint must still match central finite differences of the oracle
+    along one direction of all six per-particle parameters (relative step 1e-5
+    of each parameter), to 1e-6 relative, and the mixed form the FP64 form to
+    1e-4 of the largest gradient of each kind."""
+    from tholedipoleplugin_b200.kernel import CudaCalcTholeDipoleForceKernel
+
+    base = (small_random_system(220, seed=41, method=S.NO_CUTOFF, box=1.6) if name == "random220_nocutoff"
+            else S.config_small())
+    rng = np.random.default_rng(12)
+    s = base.copy(target_eps=1e-12, max_iter=5000, tholes=0.8 * (1 + 0.05 * rng.uniform(-1, 1, base.n)))
+    g = rng.normal(size=(s.n, 3))
+    gE = 0.4
+    grads = {}
+    for prec in ("double", "mixed"):
+        with CudaCalcTholeDipoleForceKernel(s.copy(target_eps=1e-12 if prec == "double" else 1e-9),
+                                            precision=prec) as k:
+            k.execute(s.positions)
+            grads[prec] = k.adjoint(g, gE)
+    # Direction: every particle's (q, alpha, dipole) scaled by its own
+    # magnitude; the Thole factors all scaled by one common factor, which
+    # keeps their order (so no pair crosses the kink of min(t_i, t_j)).
+    v = rng.uniform(-1, 1, size=(s.n, 6))
+    v[:, 0] *= np.abs(s.charges)
+    v[:, 1] *= s.polarizabilities
+    v[:, 2] = 0.7 * s.tholes
+    v[:, 3:] *= np.abs(np.asarray(s.dipoles)).max()
+    h = 1e-5
+
+    def moved(sign):
+        return s.copy(charges=s.charges + sign * h * v[:, 0], polarizabilities=s.polarizabilities + sign * h * v[:, 1],
+                      tholes=s.tholes + sign * h * v[:, 2], dipoles=np.asarray(s.dipoles) + sign * h * v[:, 3:])
+
+    fd = (_loss(moved(1), g, gE) - _loss(moved(-1), g, gE)) / (2 * h)
+    dd = float(np.sum(grads["double"] * v))
+    assert abs(dd - fd) <= 1e-6 * max(abs(fd), 1e-12), (dd, fd)
+    for c in range(6):
+        scale = np.abs(grads["double"][:, c]).max()
+        assert np.abs(grads["mixed"][:, c] - grads["double"][:, c]).max() <= 1e-4 * scale
