@@ -283,7 +283,11 @@ __device__ __forceinline__ void pair_energy_sides(R dx, R dy, R dz, R r2, bool y
 // the frame test's (:580-593): (x^ - Z_x Z)/|.| = (d_y^2 + d_z^2, -d_x d_y,
 // -d_x d_z) / (r sqrt(d_y^2 + d_z^2)) when the y or z coordinates differ,
 // the Gram-Schmidt form otherwise.  kap = 1 (Mutual) or -1: W = P + kap u.
-template <class R>
+// VSUM: (tx, ty, tz) and (ux, uy, uz) receive V_ij and V_ji in place of the
+// torques.  The torque of an atom is linear in V with its own dipole fixed,
+// tau_I = -perm(m_i x sum_j V_ij), so a walk can sum V over its partners and
+// take one cross product per atom at the end.
+template <class R, bool VSUM = false>
 __device__ __forceinline__ void pair_energy_lab(R dx, R dy, R dz, R r2, bool yz_differ, const EAtom<R>& I,
                                                 const EAtom<R>& K, R kap, R& fx, R& fy, R& fz, R& tx, R& ty, R& tz,
                                                 R& gx, R& gy, R& gz, R& ux, R& uy, R& uz, R& en) {
@@ -333,15 +337,27 @@ __device__ __forceinline__ void pair_energy_lab(R dx, R dy, R dz, R r2, bool yz_
     const R b = -rv2 * I.q - R(3) * rv3 * pi0;
     {
         const R vx = a * xx + rv3 * pjx, vy = a * xy + rv3 * pjy, vz = a * xz + rv3 * pjz;
-        tx -= I.mz * vx - I.mx * vz;
-        ty -= I.mx * vy - I.my * vx;
-        tz -= I.my * vz - I.mz * vy;
+        if (VSUM) {
+            tx += vx;
+            ty += vy;
+            tz += vz;
+        } else {
+            tx -= I.mz * vx - I.mx * vz;
+            ty -= I.mx * vy - I.my * vx;
+            tz -= I.my * vz - I.mz * vy;
+        }
     }
     {
         const R vx = b * xx + rv3 * pix, vy = b * xy + rv3 * piy, vz = b * xz + rv3 * piz;
-        ux -= K.mz * vx - K.mx * vz;
-        uy -= K.mx * vy - K.my * vx;
-        uz -= K.my * vz - K.mz * vy;
+        if (VSUM) {
+            ux += vx;
+            uy += vy;
+            uz += vz;
+        } else {
+            ux -= K.mz * vx - K.mx * vz;
+            uy -= K.mx * vy - K.my * vx;
+            uz -= K.my * vz - K.mz * vy;
+        }
     }
     const R c = rv2 * K.q - R(3) * rv3 * (pj0 + kap * uj0);
     const R d = -rv2 * I.q - R(3) * rv3 * (pi0 + kap * ui0);

@@ -904,6 +904,9 @@ __device__ __forceinline__ void energy_walk(const PairParams& P, const double* _
                                             unsigned partners, R damp_r2, R rv4p, R rv4f, R f[6], R g[6], R& en) {
     const int nxt = (lane + 1) & 31;
     const int nmax = P.n_tiles * 32 - 1;
+    // LAB: the walk sums V_ij (I side) and V_ji (J side, rotating with the
+    // J atoms) and turns them into torques once at the end (pair_energy_lab).
+    R vi[3] = {0, 0, 0}, vj[3] = {0, 0, 0};
 #pragma unroll 1
     for (int s = 0; s < 32; s++) {
         const int jj = (lane + s) & 31;
@@ -915,8 +918,8 @@ __device__ __forceinline__ void energy_walk(const PairParams& P, const double* _
         if (SLOW && skip_pair(s, lane, i, j, P.n, partners, jj, diag)) r2 = (R)INFINITY;
         const bool yzd = yz_differ<R>(dy, dz, yz, i, j, nmax);
         if (LAB) {
-            pair_energy_lab<R>(dx, dy, dz, r2, yzd, me, other, P.mutual ? R(1) : R(-1), f[0], f[1], f[2], f[3], f[4],
-                               f[5], g[0], g[1], g[2], g[3], g[4], g[5], en);
+            pair_energy_lab<R, true>(dx, dy, dz, r2, yzd, me, other, P.mutual ? R(1) : R(-1), f[0], f[1], f[2], vi[0],
+                                     vi[1], vi[2], g[0], g[1], g[2], vj[0], vj[1], vj[2], en);
         } else if (!SLOW || !diag) {
             pair_energy_sides<R, 3>(dx, dy, dz, r2, yzd, me, other, R(1), R(1), damp_r2, rv4p, rv4f, P.mutual != 0,
                                     f[0], f[1], f[2], f[3], f[4], f[5], g[0], g[1], g[2], g[3], g[4], g[5], en);
@@ -936,8 +939,27 @@ __device__ __forceinline__ void energy_walk(const PairParams& P, const double* _
                 g[c] += lo ? b[c] : a[c];
             }
         }
+        if (LAB) {
+            // g[3..5] are untouched by this walk (a full rotation is the identity).
 #pragma unroll
-        for (int c = 0; c < 6; c++) g[c] = __shfl_sync(kFull, g[c], nxt);
+            for (int c = 0; c < 3; c++) {
+                g[c] = __shfl_sync(kFull, g[c], nxt);
+                vj[c] = __shfl_sync(kFull, vj[c], nxt);
+            }
+        } else {
+#pragma unroll
+            for (int c = 0; c < 6; c++) g[c] = __shfl_sync(kFull, g[c], nxt);
+        }
+    }
+    if (LAB) {
+        // tau = -perm(m x sum V): the lane's I atom, and J atom jbase + lane.
+        const typename Vec4T<R>::type mj = sd[lane];
+        f[3] -= me.mz * vi[0] - me.mx * vi[2];
+        f[4] -= me.mx * vi[1] - me.my * vi[0];
+        f[5] -= me.my * vi[2] - me.mz * vi[1];
+        g[3] -= mj.z * vj[0] - mj.x * vj[2];
+        g[4] -= mj.x * vj[1] - mj.y * vj[0];
+        g[5] -= mj.y * vj[2] - mj.z * vj[1];
     }
 }
 
@@ -1004,6 +1026,7 @@ __device__ __forceinline__ void energy_walk_x2(const PairParams& P, const double
         NTy = bc2(-(float)(P.half_box_tol[1] * P.half_box_tol[1]));
         NTz = bc2(-(float)(P.half_box_tol[2] * P.half_box_tol[2]));
     }
+    // Torques from summed V (pair_energy_lab, VSUM): TX.. sum V_ij, UX.. V_ji.
     f2 FX = 0, FY = 0, FZ = 0, TX = 0, TY = 0, TZ = 0, EN = 0;        // I side
     f2 GX = 0, GY = 0, GZ = 0, UX = 0, UY = 0, UZ = 0;                // J side (packed atoms m, m + 16)
 #pragma unroll 1
@@ -1264,11 +1287,6 @@ __device__ __forceinline__ void energy_walk_x2(const PairParams& P, const double
 // ---------------------------------------------------------------------------
 __device__ __forceinline__ f2 xneg2(f2 a) { return a ^ 0x8000000080000000ull; }
 
-__device__ __forceinline__ void cross2(f2 ax, f2 ay, f2 az, f2 bx, f2 by, f2 bz, f2& cx, f2& cy, f2& cz) {
-    cx = fma2(ay, bz, xneg2(mul2(az, by)));
-    cy = fma2(az, bx, xneg2(mul2(ax, bz)));
-    cz = fma2(ax, by, xneg2(mul2(ay, bx)));
-}
 
 // X row of formQIRotationMatrix (RTDF.cpp:580-593) for one pair, as the
 // general walk forms it.
@@ -1318,6 +1336,7 @@ __device__ __forceinline__ void energy_walk_x2_fast(const PairParams& P, const d
         NTy = bc2(-(float)(P.half_box_tol[1] * P.half_box_tol[1]));
         NTz = bc2(-(float)(P.half_box_tol[2] * P.half_box_tol[2]));
     }
+    // Torques from summed V (pair_energy_lab, VSUM): TX.. sum V_ij, UX.. V_ji.
     f2 FX = 0, FY = 0, FZ = 0, TX = 0, TY = 0, TZ = 0, EN = 0;        // I side
     f2 GX = 0, GY = 0, GZ = 0, UX = 0, UY = 0, UZ = 0;                // J side (packed atoms m, m + 16)
 #pragma unroll 1
@@ -1410,26 +1429,14 @@ __device__ __forceinline__ void energy_walk_x2_fast(const PairParams& P, const d
         // the torques need m_i x V_ij and m_j x V_ji, the force only K.
         const f2 aJ = fma2(NR3X3, PJ0, rv2QJ0);
         const f2 bI = fma2(NR3X3, PI0, rv2NQI0);
-        {
-            // m_i x V_ij: the I torque.
-            const f2 VX = fma2(aJ, XX, mul2(rv3, PJX)), VY = fma2(aJ, XY, mul2(rv3, PJY)),
-                     VZ = fma2(aJ, XZ, mul2(rv3, PJZ));
-            f2 CX, CY, CZ;
-            cross2(MIX, MIY, MIZ, VX, VY, VZ, CX, CY, CZ);
-            TX = sub2(TX, CY);
-            TY = sub2(TY, CZ);
-            TZ = sub2(TZ, CX);
-        }
-        {
-            // m_j x V_ji: the J torque.
-            const f2 VX = fma2(bI, XX, mul2(rv3, PIX)), VY = fma2(bI, XY, mul2(rv3, PIY)),
-                     VZ = fma2(bI, XZ, mul2(rv3, PIZ));
-            f2 CX, CY, CZ;
-            cross2(MJX, MJY, MJZ, VX, VY, VZ, CX, CY, CZ);
-            UX = sub2(UX, CY);
-            UY = sub2(UY, CZ);
-            UZ = sub2(UZ, CX);
-        }
+        // V_ij (I torque) and V_ji (J torque), summed; the cross products with
+        // m_i and m_j come once per atom after the walk.
+        TX = fma2(aJ, XX, fma2(rv3, PJX, TX));
+        TY = fma2(aJ, XY, fma2(rv3, PJY, TY));
+        TZ = fma2(aJ, XZ, fma2(rv3, PJZ, TZ));
+        UX = fma2(bI, XX, fma2(rv3, PIX, UX));
+        UY = fma2(bI, XY, fma2(rv3, PIY, UY));
+        UZ = fma2(bI, XZ, fma2(rv3, PIZ, UZ));
         {
             const f2 cJ = fma2(NR3X3, fma2(KAP, UJ0, PJ0), rv2QJ0);
             const f2 dI = fma2(NR3X3, fma2(KAP, UI0, PI0), rv2NQI0);
@@ -1457,20 +1464,43 @@ __device__ __forceinline__ void energy_walk_x2_fast(const PairParams& P, const d
         UZ = __shfl_sync(kFull, UZ, nxt);
     }
     float lo, hi;
-    const f2* Is[7] = {&FX, &FY, &FZ, &TX, &TY, &TZ, &EN};
-    float* Io[7] = {&f[0], &f[1], &f[2], &f[3], &f[4], &f[5], &en};
+    const f2* Is[4] = {&FX, &FY, &FZ, &EN};
+    float* Io[4] = {&f[0], &f[1], &f[2], &en};
 #pragma unroll
-    for (int k = 0; k < 7; k++) {
+    for (int k = 0; k < 4; k++) {
         un2(*Is[k], lo, hi);
         *Io[k] += lo + hi;
     }
+    float v[3];
+    const f2 Vs[3] = {TX, TY, TZ};
+#pragma unroll
+    for (int k = 0; k < 3; k++) {
+        un2(Vs[k], lo, hi);
+        v[k] = lo + hi;
+    }
+    // tau_I = -perm(m_i x sum V_ij).
+    f[3] -= di.z * v[0] - di.x * v[2];
+    f[4] -= di.x * v[1] - di.y * v[0];
+    f[5] -= di.y * v[2] - di.z * v[1];
     const f2 Js[6] = {GX, GY, GZ, UX, UY, UZ};
+    float w[6];
 #pragma unroll
     for (int k = 0; k < 6; k++) {
         un2(Js[k], lo, hi);
         const float olo = __shfl_xor_sync(kFull, lo, 16), ohi = __shfl_xor_sync(kFull, hi, 16);
-        gg[k] += lane < 16 ? lo + olo : hi + ohi;
+        w[k] = lane < 16 ? lo + olo : hi + ohi;
     }
+    gg[0] += w[0];
+    gg[1] += w[1];
+    gg[2] += w[2];
+    // Lane l now holds J atom l: tau_J = -perm(m_j x sum V_ji).
+    const int m = lane & 15, h = lane >> 4;
+    const float mjx = reinterpret_cast<const float*>(&T.d0[m])[h];
+    const float mjy = reinterpret_cast<const float*>(&T.d0[m])[2 + h];
+    const float mjz = reinterpret_cast<const float*>(&T.d1[m])[h];
+    gg[3] -= mjz * w[3] - mjx * w[5];
+    gg[4] -= mjx * w[4] - mjy * w[3];
+    gg[5] -= mjy * w[5] - mjz * w[4];
 }
 
 // Partner pairs of a SLOW tile pair with their (M, I) scales, each side once:
