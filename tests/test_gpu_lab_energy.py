@@ -5,7 +5,10 @@ Tile pairs that Thole damping cannot reach take the lab-frame form of the
 reference's pair routine (ReferenceTholeDipoleForce.cpp:129-366) unless
 TDP_LAB_ENERGY=0.  The two forms are algebraically identical, so they must
 agree to rounding: FP64 to 1e-12, FP32 within the mixed form's own rounding
-(1e-6 energy, 2e-6 forces RMS).  Both are also checked against the oracle
+(forces 2e-6 RMS; energy 1e-6 relative plus the FP32 rounding of the pair
+terms, 3e-7 sqrt(sum (q_i q_j / r_ij)^2), which matters where the total nearly
+cancels, as for the 1000-water cluster: 13.2 against a scale of several
+hundred).  Both are also checked against the oracle
 with the parity tolerances, for Mutual and Direct polarization and for a box
 whose tiles straddle the half-box (folded tile pairs)."""
 import os
@@ -56,7 +59,8 @@ def test_lab_energy_matches_general_walk_and_oracle(name, precision, lab_env):
     if precision == "double":
         assert rel_err(e1, e0) < 1e-12 and rel_rms(f1, f0) < 1e-12
     else:
-        assert rel_err(e1, e0) < 1e-6 and rel_rms(f1, f0) < 2e-6
+        c2 = energy_rms_scale(s)
+        assert abs(e1 - e0) < 1e-6 * abs(e0) + 3e-7 * c2 and rel_rms(f1, f0) < 2e-6
     ref = O.compute(s.copy(target_eps=1e-12, max_iter=5000), "port")
     if precision == "double":
         assert rel_err(e1, ref.energy) < 1e-9 and rel_rms(f1, ref.forces) < 1e-8

@@ -284,9 +284,12 @@ __device__ __forceinline__ void pair_energy_sides(R dx, R dy, R dz, R r2, bool y
 // -d_x d_z) / (r sqrt(d_y^2 + d_z^2)) when the y or z coordinates differ,
 // the Gram-Schmidt form otherwise.  kap = 1 (Mutual) or -1: W = P + kap u.
 // VSUM: (tx, ty, tz) and (ux, uy, uz) receive V_ij and V_ji in place of the
-// torques.  The torque of an atom is linear in V with its own dipole fixed,
-// tau_I = -perm(m_i x sum_j V_ij), so a walk can sum V over its partners and
-// take one cross product per atom at the end.
+// torques, and en only the charge terms.  The torque of an atom is linear in
+// V with its own dipole fixed, tau_I = -perm(m_i x sum_j V_ij), and the
+// dipole terms of the energy are 0.5 (m_i.V_ij + m_j.V_ji) (expand m.V with
+// the expressions above: E = q_i q_j / r + (q_j P_i0 - q_i P_j0) / (2 r^2)
+// + (m_i.V_ij + m_j.V_ji) / 2), so a walk can sum V over its partners and
+// take one cross product and one dot product per atom at the end.
 template <class R, bool VSUM = false>
 __device__ __forceinline__ void pair_energy_lab(R dx, R dy, R dz, R r2, bool yz_differ, const EAtom<R>& I,
                                                 const EAtom<R>& K, R kap, R& fx, R& fy, R& fz, R& tx, R& ty, R& tz,
@@ -321,7 +324,9 @@ __device__ __forceinline__ void pair_energy_lab(R dx, R dy, R dz, R r2, bool yz_
     const R pi0 = qi1 + ui0, pj0 = qj1 + uj0;
     const R rv2 = rinv * rinv, rv3 = rv2 * rinv;
     const R qq = I.q * K.q;
-    {
+    if (VSUM) {
+        en += rinv * qq + R(0.5) * rv2 * (K.q * pi0 - I.q * pj0);
+    } else {
         const R t1 = K.q * (pi0 + qi1) - I.q * (pj0 + qj1);
         const R t2 = I.mx * pjx + I.my * pjy + I.mz * pjz + K.mx * pix + K.my * piy + K.mz * piz -
                      R(3) * (qi1 * pj0 + qj1 * pi0);

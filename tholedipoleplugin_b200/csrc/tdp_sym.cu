@@ -952,8 +952,10 @@ __device__ __forceinline__ void energy_walk(const PairParams& P, const double* _
         }
     }
     if (LAB) {
-        // tau = -perm(m x sum V): the lane's I atom, and J atom jbase + lane.
+        // tau = -perm(m x sum V) and the dipole energy 0.5 m.sum V: the lane's
+        // I atom, and J atom jbase + lane.
         const typename Vec4T<R>::type mj = sd[lane];
+        en += R(0.5) * (me.mx * vi[0] + me.my * vi[1] + me.mz * vi[2] + mj.x * vj[0] + mj.y * vj[1] + mj.z * vj[2]);
         f[3] -= me.mz * vi[0] - me.mx * vi[2];
         f[4] -= me.mx * vi[1] - me.my * vi[0];
         f[5] -= me.my * vi[2] - me.mz * vi[1];
@@ -1411,18 +1413,16 @@ __device__ __forceinline__ void energy_walk_x2_fast(const PairParams& P, const d
         const f2 MJX = pk2(c.x, c.y), MJY = pk2(c.z, c.w), MJZ = pk2(d.x, d.y);
         const f2 UJX = pk2(e.x, e.y), UJY = pk2(e.z, e.w), UJZ = pk2(h.x, h.y);
         const f2 PJX = add2(MJX, UJX), PJY = add2(MJY, UJY), PJZ = add2(MJZ, UJZ);
-        const f2 QI1 = dot2(XX, XY, XZ, MIX, MIY, MIZ), UI0 = dot2(XX, XY, XZ, UIX, UIY, UIZ);
-        const f2 QJ1 = dot2(XX, XY, XZ, MJX, MJY, MJZ), UJ0 = dot2(XX, XY, XZ, UJX, UJY, UJZ);
-        const f2 PI0 = add2(QI1, UI0), PJ0 = add2(QJ1, UJ0);
+        const f2 PI0 = dot2(XX, XY, XZ, PIX, PIY, PIZ), UI0 = dot2(XX, XY, XZ, UIX, UIY, UIZ);
+        const f2 PJ0 = dot2(XX, XY, XZ, PJX, PJY, PJZ), UJ0 = dot2(XX, XY, XZ, UJX, UJY, UJZ);
         const f2 rv2 = mul2(RINV, RINV), rv3 = mul2(rv2, RINV);
         const f2 NR3X3 = mul2(NTHREE, rv3);
-        // Energy.
+        // Energy: the charge terms here; the dipole terms 0.5 (m_i.V_ij +
+        // m_j.V_ji) come from the V sums after the walk (pair_energy_lab, VSUM).
         {
             const f2 qq = mul2(QI0, QJ0);
-            const f2 t1 = fma2(QJ0, add2(PI0, QI1), mul2(NQI0, add2(PJ0, QJ1)));
-            const f2 t2 = fma2(NTHREE, fma2(QI1, PJ0, mul2(QJ1, PI0)),
-                               add2(dot2(MIX, MIY, MIZ, PJX, PJY, PJZ), dot2(MJX, MJY, MJZ, PIX, PIY, PIZ)));
-            EN = fma2(RINV, qq, fma2(HALF, fma2(rv2, t1, mul2(rv3, t2)), EN));
+            const f2 cp = fma2(QJ0, PI0, mul2(NQI0, PJ0));
+            EN = fma2(RINV, qq, fma2(mul2(HALF, rv2), cp, EN));
         }
         const f2 rv2QJ0 = mul2(rv2, QJ0), rv2NQI0 = mul2(rv2, NQI0);
         // S = K x X with K = a m_i + b m_j + c u_i + d u_j (pair_energy_lab):
@@ -1478,7 +1478,8 @@ __device__ __forceinline__ void energy_walk_x2_fast(const PairParams& P, const d
         un2(Vs[k], lo, hi);
         v[k] = lo + hi;
     }
-    // tau_I = -perm(m_i x sum V_ij).
+    // tau_I = -perm(m_i x sum V_ij); dipole energy 0.5 m_i.sum V_ij.
+    en += 0.5f * (di.x * v[0] + di.y * v[1] + di.z * v[2]);
     f[3] -= di.z * v[0] - di.x * v[2];
     f[4] -= di.x * v[1] - di.y * v[0];
     f[5] -= di.y * v[2] - di.z * v[1];
@@ -1501,6 +1502,7 @@ __device__ __forceinline__ void energy_walk_x2_fast(const PairParams& P, const d
     gg[3] -= mjz * w[3] - mjx * w[5];
     gg[4] -= mjx * w[4] - mjy * w[3];
     gg[5] -= mjy * w[5] - mjz * w[4];
+    en += 0.5f * (mjx * w[3] + mjy * w[4] + mjz * w[5]);
 }
 
 // Partner pairs of a SLOW tile pair with their (M, I) scales, each side once:
