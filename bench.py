@@ -69,6 +69,15 @@ NS_PER_DAY = 1e-6 * 86400.0  # per (step/s) at 1 fs
 #    accumulation 12 -> 450.
 FLOP_MATVEC_PAIR = 66
 FLOP_ENERGY_PAIR = 450
+# The energy kernel's own formulation for the undamped unit-scale pairs (every
+# pair but ~0.2 % of a box): the lab-frame walk with summed V, counted from its
+# operation sequence the same way: delta 3, minimum image 9, r^2 5, 1/r 1,
+# frame X row 10, P_j 3, the four X projections 20, inverse powers 3, energy
+# charge terms 9, V coefficients 4, V sums 24, W coefficients 8, K 21, charge
+# force coefficient 7, K.X coefficient 7, force vector 9, both sides' force
+# sums 6 -> 150.  The reference's sequence (450) stays the algorithmic count;
+# this one says how busy the walk keeps the FP32 pipes.
+FLOP_ENERGY_PAIR_EXECUTED = 150
 FLOP_FIXED_PAIR = 75
 # Algorithmic HBM bytes per atom and launch: matvec 16 (posq) + 12 (operand) +
 # 12 (result) + 48 (four CG vectors); energy pass 16 (posq) + 16 (dipole,
@@ -879,6 +888,13 @@ def run_ours(args):
                            "algorithmic": f"{flop} FLOP per unordered pair (the reference's operation sequence) x "
                                           f"{pairs:.4g} pairs per launch",
                            "avg_launch_ms": _r(avg), "share_of_step": _r(share)}
+        if flop == FLOP_ENERGY_PAIR:
+            # The lab-frame walk does fewer operations than the reference's
+            # sequence (frac above 1); its own count gives the pipe load.
+            ex = pairs * FLOP_ENERGY_PAIR_EXECUTED / (avg * 1e-3) / 1e12
+            out["roofline"]["executed"] = {
+                "flop_per_pair": FLOP_ENERGY_PAIR_EXECUTED, "achieved": _r(ex), "frac": _r(ex / fp32),
+                "what": "the walk's own operation count (lab-frame pair routine with summed V)"}
         out["roofline_hbm"] = {"bound": "hbm", "kernel": kname, "achieved": _r(bytes_ / (avg * 1e-3) / 1e9),
                                "peak": hbm_peak, "unit": "GB/s", "frac": _r(bytes_ / (avg * 1e-3) / 1e9 / hbm_peak),
                                "peak_source": "MEASURED_PEAKS.json hbm_gbs" if "hbm_gbs" in peaks else "fallback"}
