@@ -513,10 +513,19 @@ static inline int nb(int n) { return (n + 127) / 128; }
 
 // Scratch of the two-pass pair VJP, per (split, atom): 8 FP64 sums, the
 // slow-pair row and its count.
+// Splits of the J range of the tiled passes: about 16 warps per SM (148 SMs)
+// in total, at most kVjpSplit.
+static int vjp_splits(int n) {
+    const int blocks = (std::max(n, 1) + adj::kVjpTile - 1) / adj::kVjpTile;
+    return std::min(adj::kVjpSplit, std::max(1, (16 * 148 + blocks - 1) / blocks));
+}
+
 size_t adjoint_pair_scratch(int n) {
-    const size_t m = (size_t)adj::kVjpSplit * (size_t)std::max(n, 1);
+    const size_t m = (size_t)vjp_splits(n) * (size_t)std::max(n, 1);
     return 8 * m + (m * (adj::kSlowCap + 1) * sizeof(int) + sizeof(double) - 1) / sizeof(double);
 }
+
+size_t adjoint_fixed_scratch(int n) { return 5 * (size_t)vjp_splits(n) * (size_t)std::max(n, 1); }
 
 void launch_adjoint_pair(const Dev& d, const double* g, const double* gT, double gE, double* a8, int precision,
                          double* scratch, AdjPairList* list, cudaStream_t st) {
@@ -529,9 +538,8 @@ void launch_adjoint_pair(const Dev& d, const double* g, const double* gT, double
         return;
     }
     const int blocks = (d.n + adj::kVjpTile - 1) / adj::kVjpTile;
-    // Splits of the J range: about 16 warps per SM in total.
-    const int nsplit = std::min(adj::kVjpSplit, std::max(1, (16 * 148 + blocks - 1) / blocks));
-    const size_t m = (size_t)adj::kVjpSplit * d.n;
+    const int nsplit = vjp_splits(d.n);
+    const size_t m = (size_t)nsplit * d.n;
     double* part = scratch;
     int* slow = reinterpret_cast<int*>(scratch + 8 * m);
     int* nslow = slow + m * adj::kSlowCap;
@@ -553,7 +561,7 @@ void launch_adjoint_fixed(const Dev& d, const double* lam, double* b5, const Adj
         return;
     }
     const int blocks = (d.n + adj::kVjpTile - 1) / adj::kVjpTile;
-    const int nsplit = std::min(adj::kVjpSplit, std::max(1, (16 * 148 + blocks - 1) / blocks));
+    const int nsplit = vjp_splits(d.n);
     const dim3 grid(blocks, nsplit);
     if (precision == TDP_PRECISION_MIXED)
         adj::k_fixed_vjp_fast<float><<<grid, adj::kVjpTile, 0, st>>>(d.pp, A, lam, d.exc_off, d.exc_j, d.exc_m, scratch);

@@ -879,7 +879,7 @@ void run_adjoint(tdp_handle* h, const double* g_in, double gE, double* out_dst, 
     const int n = h->n;
     const size_t n3 = 3 * (size_t)n;
     if (!h->adj) h->adj = dalloc<double>(n3 * 11 + 8 * (size_t)n + 5 * (size_t)n + 2 * (size_t)n + 6 * (size_t)n +
-                                             adjoint_pair_scratch(n) + 5 * 8 * (size_t)n,
+                                             adjoint_pair_scratch(n) + adjoint_fixed_scratch(n),
                                          h->owned);
     double* g = h->adj;
     double* gt = g + n3;

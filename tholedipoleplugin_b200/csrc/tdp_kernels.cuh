@@ -140,9 +140,10 @@ struct AdjPairList {
 // scratch: adjoint_pair_scratch(n) doubles; list (may be NULL) receives the
 // damped-partner lists.
 size_t adjoint_pair_scratch(int n);
+size_t adjoint_fixed_scratch(int n);
 void launch_adjoint_pair(const Dev& d, const double* g, const double* gT, double gE, double* a8, int precision,
                          double* scratch, AdjPairList* list, cudaStream_t st);
-// scratch: 5 * 8 * n doubles (the split sums of the tiled pass), or NULL.
+// scratch: adjoint_fixed_scratch(n) doubles (the split sums of the tiled pass), or NULL.
 void launch_adjoint_fixed(const Dev& d, const double* lam, double* b5, const AdjPairList& list, int precision,
                           double* scratch, cudaStream_t st);
 void launch_adjoint_matvec_t(const Dev& d, const double* lam, double* ct, const AdjPairList& list, cudaStream_t st);
