@@ -83,6 +83,17 @@ def test_null_desc(lib):
     assert lib.tdp_create(None, C.byref(h)) == -1
 
 
+def test_query_argument_checks(lib):
+    # Host-side checks of the solver queries, before any device work.
+    cnt = C.c_int32(-5)
+    assert lib.tdp_solver_history(None, None, 0, C.byref(cnt)) == -1
+    it, conv, st = C.c_int32(), C.c_int32(), C.c_int32()
+    eps = C.c_double()
+    assert lib.tdp_solver_stats(None, C.byref(it), C.byref(eps), C.byref(conv), C.byref(st)) == -1
+    out = (C.c_double * 14)()
+    assert lib.tdp_stage_times(None, out) == -1
+
+
 # -- cluster batches: host validation runs before any device work ----------
 def _batch_create(clusters, offsets=None, edit=None, **kw):
     sys_, offs = S.concat_clusters(clusters)
