@@ -13,7 +13,10 @@
 // Applying B^-1 costs a few real-space walks within a short cutoff plus a
 // coarse PME grid, a small fraction of one all-pairs walk (1.2 ms against
 // 8.7 ms at 98,304 atoms, mixed form), and cuts the outer iterations there
-// from 7 to 3 from a cold start and from 5-6 to 2 per warm-started MD step.
+// from 7 to 2 from a cold start (which also begins at y = M(b), see
+// precond_cold_start) and from 5-6 to 2 per warm-started MD step.  Below about
+// 30,000 atoms an all-pairs matvec is cheap enough that plain CG is as fast,
+// so the C ABI uses it from 32,768 atoms on unless told otherwise.
 //
 // The preconditioner is z = M(r): `inner` CG iterations on B z = r from z = 0,
 // on r scaled to unit RMS (the PME grid of the mixed form is 64-bit fixed
