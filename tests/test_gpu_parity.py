@@ -108,10 +108,14 @@ def test_forces_are_added(precision):
     assert e == e2
 
 
+@pytest.mark.parametrize("name", ["ammonia_mutual", "water216", "random_pme", "random_extrap", "water_cluster"])
 @pytest.mark.parametrize("precision", ["double", "mixed"])
-def test_queries_match_oracle(precision):
-    s = SYSTEMS["ammonia_mutual"]
-    grid = np.random.default_rng(3).uniform(-0.8, 0.8, size=(33, 3))
+def test_queries_match_oracle(precision, name):
+    # Potential on a grid spanning the system (minimum image for PME), the 13
+    # multipole moments and the total dipoles (RTDF.cpp:1157-1372).
+    s = SYSTEMS[name]
+    lo, hi = s.positions.min(0) - 0.3, s.positions.max(0) + 0.3
+    grid = np.random.default_rng(3).uniform(lo, hi, size=(33, 3))
     ts = tight(s)
     with CudaCalcTholeDipoleForceKernel(s.copy(target_eps=1e-11 if precision == "double" else 1e-9,
                                                 max_iter=2000), precision=precision) as k:
