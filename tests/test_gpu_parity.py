@@ -122,10 +122,13 @@ def test_queries_match_oracle(precision, name):
         pot = k.getElectrostaticPotential(grid, s.positions)
         mom = k.getSystemMultipoleMoments(s.masses, s.positions)
         tot = k.getTotalDipoles(s.positions)
+    # Dipoles as in the induced-dipole parity checks (the solve stops at 1e-11,
+    # which leaves ~1e-9 relative in a cluster's dipoles); potential and
+    # moments sum over many sites and carry less of it.
     tol = 1e-9 if precision == "double" else 2e-5
     assert rel_rms(pot, O.potential(ts, grid, "port")) < tol
     assert rel_rms(mom, O.moments(ts, "port")) < tol
-    assert rel_rms(tot, O.total_dipoles(ts, "port")) < tol
+    assert rel_rms(tot, O.total_dipoles(ts, "port")) < (1e-8 if precision == "double" else 2e-5)
 
 
 def test_rinv4_power_flag():
