@@ -118,3 +118,20 @@ def test_preconditioned_adjoint_matches_plain_cg(precision, monkeypatch):
     for c in range(out[True].shape[1]):
         scale = np.abs(out[False][:, c]).max()
         assert np.abs(out[True][:, c] - out[False][:, c]).max() <= tol * scale
+
+
+@pytest.mark.parametrize("pre", [True, False])
+def test_solver_history(pre, monkeypatch):
+    """tdp_solver_history: the stopping quantity at the start, after every
+    iteration and after a true-residual check, oldest first; its last entry is
+    the epsilon tdp_solver_stats reports, and below the target."""
+    monkeypatch.setenv("TDP_PRECOND", "1" if pre else "0")
+    s = S.config_small().copy(target_eps=1e-9, max_iter=2000)
+    with CudaCalcTholeDipoleForceKernel(s, precision="double") as k:
+        k.execute(s.positions)
+        st = k.solverStats()
+        h = k.solverHistory()
+    assert st["converged"]
+    assert len(h) in (st["iterations"] + 1, st["iterations"] + 2)   # + the true-residual check
+    assert h[-1] == st["epsilon"] and h[-1] <= 1e-9 < h[0]
+    assert np.all(np.isfinite(h))
